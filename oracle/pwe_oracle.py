@@ -1,0 +1,429 @@
+"""complex128 restatement of the reference's paraxial (PWE) and multislice paths.
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()``
+and ``bench.py``'s CPU legs, never by the product package.
+
+Every function cites the reference file:line it restates (paths are relative
+to the reference project root).  Parity of this restatement with the
+unmodified reference is pinned by the golden fixtures in ``tests/golden``.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+BC_TYPES = ("dirichlet", "neumann", "impedance", "impedance2")
+
+
+# ---------------------------------------------------------------------------
+# Boundary-condition coefficients and step matrices
+# ---------------------------------------------------------------------------
+def bc_coefficients(k, dx, dz, dy=None, bc_type="impedance", dimension=2):
+    """μ, β and γ coefficients.
+
+    Restates ``thick_ptycho/forward_model/pwe/operators/finite_differences/
+    boundary_conditions.py:9-55``: ``a = i/(2k)``, ``μ_x = a·dz/(2dx²)``,
+    ``μ_y`` likewise in 3D (0 in 2D), ``β = μ·2ik·dx`` for the impedance
+    variants and ``γ = −1/(2ik)`` for impedance2.
+    """
+    a = 1j / (2 * k)
+    mu_x = a * (0.5 * dz / dx**2)
+    mu_y = a * (0.5 * dz / dy**2) if dimension == 3 else 0.0
+    out = {"mu_x": mu_x, "mu_y": mu_y, "beta_x": 0.0, "beta_y": 0.0, "gamma": 0.0}
+    if bc_type in ("impedance", "impedance2"):
+        out["beta_x"] = mu_x * 2j * k * dx
+        out["beta_y"] = mu_y * 2j * k * dy if dimension == 3 else 0.0
+    if bc_type == "impedance2":
+        out["gamma"] = -1 / (2j * k)
+    return out
+
+
+def laplacian_1d(nx, mu_x, mu_y=0.0):
+    """Scaled 1D second difference ``K = tridiag(μx, −2(μx+μy), μx)``.
+
+    Restates ``operator_matrices.py:36-45``.
+    """
+    e = np.ones(nx, dtype=complex)
+    return sp.diags(
+        [mu_x * e[1:], -2 * (mu_x + mu_y) * e, mu_x * e[1:]],
+        offsets=[-1, 0, 1],
+        shape=(nx, nx),
+        dtype=complex,
+    ).tolil()
+
+
+def apply_bc_1d(K, bc_type, co, dz):
+    """Boundary-row edits of K.
+
+    Restates ``operator_matrices.py:59-72`` and ``boundary_conditions.py:
+    57-94``: Dirichlet zeroes rows 0 and N−1; otherwise the Neumann edit
+    doubles ``K[0,1]`` and ``K[N−1,N−2]``, then impedance adds β to the two
+    corner diagonals and impedance2 adds ``β + γ/dz²`` there and ``−γ/dz²`` to
+    the doubled couplings.
+    """
+    K = K.tolil()
+    if bc_type == "dirichlet":
+        K[0, 1] = 0
+        K[-1, -2] = 0
+        K[0, 0] = 0
+        K[-1, -1] = 0
+        return K.tocsr()
+    K[0, 1] *= 2
+    K[-1, -2] *= 2
+    if bc_type == "impedance":
+        K[0, 0] += co["beta_x"]
+        K[-1, -1] += co["beta_x"]
+    elif bc_type == "impedance2":
+        g = co["gamma"] / dz**2
+        K[0, 0] += co["beta_x"] + g
+        K[0, 1] += -g
+        K[-1, -1] += co["beta_x"] + g
+        K[-1, -2] += -g
+    return K.tocsr()
+
+
+def step_matrices_1d(nx, co, bc_type, dz):
+    """``A = I − K``, ``B = I + K`` for 2D problems (1D transverse).
+
+    Restates ``operator_matrices.py:47-57``.
+    """
+    K = apply_bc_1d(laplacian_1d(nx, co["mu_x"], co["mu_y"]), bc_type, co, dz)
+    eye = sp.eye(nx, dtype=complex)
+    return (eye - K).tocsr(), (eye + K).tocsr()
+
+
+def step_matrices_2d(nx, ny, co, bc_type, dz):
+    """5-point step matrices for 3D problems (2D transverse).
+
+    Restates ``operator_matrices.py:75-126`` and ``boundary_conditions.py:
+    96-130``: ``A = kron(I_y, A_x) + kron(offdiag_y, −μ_y I_x)`` (``+μ_y`` for
+    B), then the y-edge rules (Dirichlet identity blocks, Neumann doubled
+    couplings, impedance ``∓β_y I`` on the first and last blocks).
+    """
+    if bc_type not in ("dirichlet", "neumann", "impedance"):
+        raise ValueError(f"3D step matrices do not support bc_type={bc_type!r}")
+    Ax, Bx = step_matrices_1d(nx, co, bc_type, dz)
+    Ix = sp.eye(nx, dtype=complex)
+    Iy = sp.eye(ny, dtype=complex)
+    off = sp.diags([1.0, 1.0], [-1, 1], shape=(ny, ny), dtype=complex)
+    Axy = (sp.kron(Iy, Ax) + sp.kron(off, -co["mu_y"] * Ix)).tolil()
+    Bxy = (sp.kron(Iy, Bx) + sp.kron(off, co["mu_y"] * Ix)).tolil()
+    if bc_type == "dirichlet":
+        Axy[:nx, :nx] = Ix
+        Axy[-nx:, -nx:] = Ix
+        Bxy[:nx, :nx] = Ix
+        Bxy[-nx:, -nx:] = Ix
+        Axy[:nx, nx : 2 * nx] *= 0
+        Axy[-nx:, -2 * nx : -nx] *= 0
+        Bxy[:nx, nx : 2 * nx] *= 0
+        Bxy[-nx:, -2 * nx : -nx] *= 0
+        return Axy.tocsr(), Bxy.tocsr()
+    Axy[:nx, nx : 2 * nx] *= 2
+    Axy[-nx:, -2 * nx : -nx] *= 2
+    Bxy[:nx, nx : 2 * nx] *= 2
+    Bxy[-nx:, -2 * nx : -nx] *= 2
+    if bc_type == "impedance":
+        Axy[:nx, :nx] -= co["beta_y"] * Ix
+        Axy[-nx:, -nx:] -= co["beta_y"] * Ix
+        Bxy[:nx, :nx] += co["beta_y"] * Ix
+        Bxy[-nx:, -nx:] += co["beta_y"] * Ix
+    return Axy.tocsr(), Bxy.tocsr()
+
+
+def probe_bc_rhs_1d(nx, co, bc_type, probe=None):
+    """Step RHS ``b`` (zero unless a probe is set for Dirichlet/impedance).
+
+    Restates ``operator_matrices.py:152-166``.
+    """
+    ubc = np.zeros(nx, dtype=complex)
+    if probe is None:
+        return ubc
+    if bc_type == "dirichlet":
+        ubc[1] += 2 * co["mu_x"] * probe[0]
+        ubc[-2] += 2 * co["mu_x"] * probe[-1]
+    elif bc_type == "impedance":
+        ubc[0] -= 2 * co["beta_x"] * probe[0]
+        ubc[-1] -= 2 * co["beta_x"] * probe[-1]
+    return ubc
+
+
+# ---------------------------------------------------------------------------
+# Object contribution C_j
+# ---------------------------------------------------------------------------
+def object_contribution(n, k, dz, grad=False, exact_ref_coeff=False, empty_space_px=0):
+    """Per-step object coefficients ``C[..., j]`` (j = 0..Nz−2).
+
+    Restates ``simulation/simulation_space/base_simulation_space.py:315-383``:
+    ``coef = (k/i)(n−1)`` (or ``(k/2i)(n²−1)`` when ``exact_ref_coeff``; with
+    ``grad`` the derivative forms ``k/i`` or ``(k/i)n``), optional zero padding
+    of the first transverse axis, then ``(dz/2)·½(coef_j + coef_{j+1})``.
+    """
+    n = np.asarray(n)
+    if grad:
+        coef = (k / 1j) * (n if exact_ref_coeff else np.ones_like(n))
+    else:
+        coef = (k / 1j) * (n - 1) if not exact_ref_coeff else (k / 2j) * (n**2 - 1)
+    if empty_space_px > 0:
+        pad = [(empty_space_px, empty_space_px)] + [(0, 0)] * (coef.ndim - 1)
+        coef = np.pad(coef, pad, mode="constant", constant_values=0.0)
+    return (dz / 2) * (coef[..., :-1] + coef[..., 1:]) / 2
+
+
+# ---------------------------------------------------------------------------
+# Slice-by-slice LU march (the reference's IterativeLU path)
+# ---------------------------------------------------------------------------
+def build_lu_factors(A, B, C2d, mode="forward"):
+    """Per-slice ``splu(A − C_j)`` and ``B + C_j`` for a mode.
+
+    Restates ``forward_model/pwe/solvers/iterative_lu.py:90-133``: reverse
+    swaps A and B (and negates b, done by the caller) and uses ``−C[:, −j]``;
+    adjoint uses ``C[:, −j]`` and conjugate-transposes both matrices; forward
+    uses ``C[:, j−1]``.
+    """
+    if mode == "reverse":
+        A, B = B, A
+    L = C2d.shape[1]
+    lus, Bs = [], []
+    for j in range(1, L + 1):
+        if mode == "reverse":
+            C = -sp.diags(C2d[:, -j])
+        elif mode == "adjoint":
+            C = sp.diags(C2d[:, -j])
+        else:
+            C = sp.diags(C2d[:, j - 1])
+        Aw = A - C
+        Bw = B + C
+        if mode == "adjoint":
+            Aw, Bw = Aw.conj().T, Bw.conj().T
+        lus.append(spla.splu(Aw.tocsc()))
+        Bs.append(Bw.tocsr())
+    return lus, Bs
+
+
+def march_with_lu(lus, Bs, b, probe, mode="forward", rhs_block=None, test_rhs=None):
+    """One probe's z-march with prebuilt factors.
+
+    Restates ``iterative_lu.py:138-197``: ``u[:,0] = probe``; per step
+    ``u_j = LU_j⁻¹(B_j u_{j−1} + b)`` with ``b = rhs_block[:, −j]`` (adjoint)
+    or ``rhs_block[:, j−1]``, overridden by the exact test boundary data when
+    given; the adjoint result is flipped along z.
+    """
+    N = Bs[0].shape[0]
+    L = len(lus)
+    if mode == "reverse":
+        b = -np.asarray(b)
+    u = np.zeros((N, L + 1), dtype=complex)
+    if probe is not None:
+        u[:, 0] = np.asarray(probe).ravel()
+    for j in range(1, L + 1):
+        bj = b
+        if rhs_block is not None:
+            bj = rhs_block[:, -j] if mode == "adjoint" else rhs_block[:, j - 1]
+        if test_rhs is not None:
+            bj = test_rhs[j - 1]
+        u[:, j] = lus[j - 1].solve(Bs[j - 1] @ u[:, j - 1] + bj)
+    if mode == "adjoint":
+        u = np.flip(u, axis=1)
+    return u
+
+
+def march(A, B, C2d, probe, mode="forward", b=None, rhs_block=None, test_rhs=None):
+    """Convenience wrapper: factorise then march one probe."""
+    lus, Bs = build_lu_factors(A, B, C2d, mode)
+    if b is None:
+        b = np.zeros(A.shape[0], dtype=complex)
+    return march_with_lu(lus, Bs, b, probe, mode, rhs_block, test_rhs)
+
+
+# ---------------------------------------------------------------------------
+# Exact discrete adjoint and gradient (no reference counterpart; the
+# reference's adjoint differs, see ``reference_grad_least_squares``)
+# ---------------------------------------------------------------------------
+def exact_adjoint(A, B, C2d, src):
+    """λ_j solving ``(A − C_j)ᴴ λ_j = src_j + (B + C_{j+1})ᴴ λ_{j+1}``.
+
+    ``src`` has shape (N, L); column j−1 is the source of slice j.  This is
+    the exact adjoint of the forward march of ``march`` (mode "forward").
+    Returns λ with shape (N, L), column j−1 holding slice j.
+    """
+    N, L = C2d.shape
+    lam = np.zeros((N, L), dtype=complex)
+    nxt = np.zeros(N, dtype=complex)
+    for j in range(L, 0, -1):
+        rhs = src[:, j - 1].copy()
+        if j < L:
+            Rn = (B + sp.diags(C2d[:, j])).conj().T
+            rhs = rhs + Rn @ nxt
+        Mj = (A - sp.diags(C2d[:, j - 1])).conj().T.tocsc()
+        lam[:, j - 1] = spla.spsolve(Mj, rhs)
+        nxt = lam[:, j - 1]
+    return lam
+
+
+def grad_c_from_adjoint(u, lam):
+    """Torch-convention gradient w.r.t. each step coefficient c_j.
+
+    ``u`` is (N, Nz), ``lam`` is (N, L).  ``∂ℓ/∂Re c + i∂ℓ/∂Im c =
+    λ_j · conj(u_j + u_{j−1})``.
+    """
+    return lam * np.conj(u[:, 1:] + u[:, :-1])
+
+
+def chain_grad_to_n(grad_c, k, dz, n=None, exact_ref_coeff=False, empty_space_px=0):
+    """Map gradients w.r.t. c_j onto the z nodes of n (torch convention).
+
+    ``c_j = (dz/4)(coef(n_{j−1}) + coef(n_j))`` so node t receives
+    ``conj((dz/4)·coef'(n_t))·(g_t + g_{t+1})`` with out-of-range terms zero.
+    """
+    if empty_space_px > 0:
+        grad_c = grad_c[empty_space_px:-empty_space_px]
+    N, L = grad_c.shape
+    acc = np.zeros((N, L + 1), dtype=complex)
+    acc[:, :-1] += grad_c
+    acc[:, 1:] += grad_c
+    if exact_ref_coeff:
+        dcoef = (k / 1j) * np.asarray(n)
+    else:
+        dcoef = (k / 1j) * np.ones((N, L + 1))
+    return np.conj((dz / 4) * dcoef) * acc
+
+
+# ---------------------------------------------------------------------------
+# Exit waves, far field, phase-retrieval projection, amplitude loss
+# ---------------------------------------------------------------------------
+def farfield_intensity(exit_waves, dimension=2, shape2d=None):
+    """``|FFT(exit)|²``, unnormalised, no shift.
+
+    Restates ``forward_model/base/base_solver.py:234-242`` (Poisson noise off).
+    """
+    if dimension == 2:
+        return np.abs(np.fft.fft(exit_waves, axis=-1)) ** 2
+    e = exit_waves.reshape(exit_waves.shape[0], *shape2d)
+    return (np.abs(np.fft.fft2(e, axes=(-2, -1))) ** 2).reshape(exit_waves.shape)
+
+
+def phase_retrieval_projection(exit_waves, data):
+    """Gerchberg–Saxton modulus projection.
+
+    Restates ``reconstruction/base_reconstructor.py:171-207``.
+    """
+    f = np.fft.fft(exit_waves, axis=-1)
+    mag = np.abs(f)
+    mag[mag == 0] = 1.0
+    return np.fft.ifft(np.sqrt(data) * (f / mag), axis=-1)
+
+
+def amplitude_loss_and_grad(exit_waves, amplitude):
+    """``ℓ = Σ(|F e| − a)²`` and its torch-convention gradient w.r.t. e."""
+    N = exit_waves.shape[-1]
+    U = np.fft.fft(exit_waves, axis=-1)
+    mag = np.abs(U)
+    loss = float(np.sum((mag - amplitude) ** 2))
+    safe = np.where(mag > 0, mag, 1.0)
+    gU = 2 * (mag - amplitude) * U / safe
+    gU = np.where(mag > 0, gU, 0)
+    return loss, N * np.fft.ifft(gU, axis=-1)
+
+
+# ---------------------------------------------------------------------------
+# Reference-compatible least-squares gradient (reproduces its B1/B2/B3)
+# ---------------------------------------------------------------------------
+def reference_grad_least_squares(A, B, C2d, u_all, exit_err, k, dz):
+    """The reference's ``compute_grad_least_squares`` for one projection.
+
+    Restates ``reconstruction/pwe_reconstructor.py:100-164`` (no reduced
+    domain): per probe an adjoint march (mode "adjoint", source = exit error
+    at the last slice), ``g = grad_A @ u`` with ``grad_A = −(diag(G) +
+    subdiag(G))`` and ``G = (dz/2)(k/i)`` (``forward_model.py:128-153``),
+    then ``grad_re −= Re(conj(g)λ)``, ``grad_im −= Re(conj(ig)λ)``.
+    ``u_all`` is (P, N, Nz), ``exit_err`` (P, N); returns two (L·N,) arrays
+    laid out z-major like the reference.
+    """
+    P, N, Nz = u_all.shape
+    L = Nz - 1
+    lus, Bs = build_lu_factors(A, B, C2d, "adjoint")
+    G = (dz / 2) * (k / 1j)
+    gre = np.zeros(L * N)
+    gim = np.zeros(L * N)
+    zero_b = np.zeros(N, dtype=complex)
+    for p in range(P):
+        rhs_block = np.zeros((N, L), dtype=complex)
+        rhs_block[:, -1] = exit_err[p]
+        bp = march_with_lu(lus, Bs, zero_b, None, "adjoint", rhs_block)
+        bp = bp[:, :-1].T.ravel()
+        uk = u_all[p][:, 1:].T  # (L, N)
+        g = -G * uk.copy()
+        g[1:] += -G * uk[:-1]
+        g = g.ravel()
+        gre -= (g.conj() * bp).real
+        gim -= ((1j * g).conj() * bp).real
+    return gre, gim
+
+
+# ---------------------------------------------------------------------------
+# Multislice (angular spectrum), 2D
+# ---------------------------------------------------------------------------
+def ms_kernel(nx_eff, dx, k, dz, remove_global_phase=True):
+    """Angular-spectrum kernel ``H = exp(i k_z dz)·exp(−ik dz)``.
+
+    Restates ``forward_model/multislice/ms_solver.py:49-72``.
+    """
+    kx = 2 * np.pi * np.fft.fftfreq(nx_eff, d=dx)
+    kz = np.sqrt(np.clip(k**2 - kx**2, 0.0, None))
+    H = np.exp(1j * kz * dz)
+    if remove_global_phase:
+        H = H * np.exp(-1j * k * dz)
+    return H.astype(np.complex128)
+
+
+def ms_forward(n, probe, k, dx, dz, n_medium=1.0):
+    """Multislice march of one probe, shape (N, Nz).
+
+    Restates ``ms_solver.py:74-78,86-88,90-159``: transmit by
+    ``exp(ik(n_z − n_med)dz)`` then propagate with H (global phase removed).
+    """
+    N, Nz = n.shape
+    H = ms_kernel(N, dx, k, dz)
+    u = np.empty((N, Nz), dtype=complex)
+    psi = np.asarray(probe, dtype=complex).copy()
+    u[:, 0] = psi
+    for z in range(Nz - 1):
+        psi = psi * np.exp(1j * k * (n[:, z] - n_medium) * dz)
+        psi = np.fft.ifft(np.fft.fft(psi) * H)
+        u[:, z + 1] = psi
+    return u
+
+
+# ---------------------------------------------------------------------------
+# Exact impedance test boundary data (the reference's known-answer tests)
+# ---------------------------------------------------------------------------
+def exact_impedance_test_rhs(x, z, k, beta_x, y=None, beta_y=0.0):
+    """Per-step test boundary data, shape (L, N).
+
+    Restates ``boundary_condition_test.py:49-114``: the analytic Neumann mode
+    sum evaluated on the boundary, ``−2β·u_exact`` on the edge rows, averaged
+    between z_{j−1} and z_j.
+    """
+    a = 1j / (2 * k)
+
+    def u_nm(n, m, xx, yy, zz):
+        return np.exp(-a * ((n**2 + m**2) * np.pi**2) * zz) * np.cos(n * np.pi * xx) * np.cos(m * np.pi * yy)
+
+    def bnd(zz):
+        if y is None:
+            ue = lambda xx: u_nm(1, 0, xx, 0, zz) + 0.5 * u_nm(2, 0, xx, 0, zz) + 0.2 * u_nm(5, 0, xx, 0, zz)  # noqa: E731
+            ubc = np.zeros(len(x), dtype=complex)
+            ubc[0] -= 2 * beta_x * ue(x[0])
+            ubc[-1] -= 2 * beta_x * ue(x[-1])
+            return ubc
+        ue = lambda xx, yy: u_nm(1, 1, xx, yy, zz) + 0.5 * u_nm(2, 2, xx, yy, zz) + 0.2 * u_nm(5, 5, xx, yy, zz)  # noqa: E731
+        ubc = np.zeros((len(x), len(y)), dtype=complex)
+        ubc[0, :] -= 2 * beta_x * ue(x[0], y)
+        ubc[-1, :] -= 2 * beta_x * ue(x[-1], y)
+        ubc[:, 0] -= 2 * beta_y * ue(x, y[0])
+        ubc[:, -1] -= 2 * beta_y * ue(x, y[-1])
+        return ubc.ravel()
+
+    return np.stack([0.5 * (bnd(z[j - 1]) + bnd(z[j])) for j in range(1, len(z))])
