@@ -1,0 +1,162 @@
+/*
+ * tpcuda.h — C ABI of libtpcuda.so, the sm_100a implementation of the
+ * thick_ptycho paraxial finite-difference (PWE) hot path.
+ *
+ * Every entry point returns an int status (TP_OK = 0); on failure
+ * tp_last_error_string() describes the last error of the calling thread.
+ * Pointers are device pointers unless stated otherwise; complex numbers are
+ * interleaved (re, im) pairs: float2 for complex64, double2 for complex128.
+ * All work is enqueued on the caller's stream; no entry point synchronises
+ * except where stated, and none allocates device memory: the caller passes
+ * workspaces sized by the *_bytes() queries.
+ *
+ * Step equation (reference iterative_lu.py:185-193, operator_matrices.py:36-72):
+ *   (A - C_j) u_j = (B + C_j) u_{j-1} + b_j,  A = I - K, B = I + K,
+ *   K = scaled tridiagonal second difference with boundary-row edits,
+ *   C_j = diag((dz/2) * 0.5 * (coef(n[:, j-1]) + coef(n[:, j]))),
+ *   coef(n) = (k/i)(n - 1)  or  (k/2i)(n^2 - 1)  (exact_ref_coeff)
+ *   (reference base_simulation_space.py:315-383).
+ */
+#ifndef TPCUDA_H
+#define TPCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define TP_API __attribute__((visibility("default")))
+#else
+#define TP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *tp_stream_t; /* = cudaStream_t */
+
+enum tp_status {
+  TP_OK = 0,
+  TP_ERR_INVALID = 1,   /* bad argument (size, null pointer, mode) */
+  TP_ERR_UNSUPPORTED = 2,
+  TP_ERR_CUDA = 3,      /* a CUDA runtime call failed */
+  TP_ERR_TIMEOUT = 4,   /* a device-side bounded wait gave up */
+  TP_ERR_WORKSPACE = 5  /* workspace too small */
+};
+
+/* Propagation modes (reference iterative_lu.py:90-133, 185-197). */
+enum tp_mode {
+  TP_MODE_FORWARD = 0,       /* (A - C_j) u_j = (B + C_j) u_{j-1} + b      */
+  TP_MODE_ADJOINT = 1,       /* reference adjoint: (A - C_s)^H, (B + C_s)^H,
+                                s = L+1-j, output flipped along z          */
+  TP_MODE_REVERSE = 2,       /* A<->B swapped, C negated, slices reversed   */
+  TP_MODE_ADJOINT_EXACT = 3  /* exact discrete adjoint of FORWARD:
+                                (A - C_s)^H l_s = e_s + (B + C_{s+1})^H l_{s+1} */
+};
+
+/* Dtype of the refractive-index array handed to tp_cn2d_factor. */
+enum tp_dtype { TP_C128 = 0, TP_C64 = 1 };
+
+/*
+ * The 2D step operator: K's interior entries and its boundary-row edits.
+ * Replaces the reference's sparse A_step/B_step (operator_matrices.py:47-72,
+ * boundary_conditions.py:57-94) and the C_j coefficients
+ * (base_simulation_space.py:315-383).  Complex values are (re, im).
+ */
+typedef struct tp_cn2d_op {
+  int32_t n;               /* transverse rows N (block_size), 4 <= N <= 2048 */
+  int32_t nz;              /* z nodes; L = nz - 1 steps                     */
+  int32_t n_obj;           /* rows of the object array (N - 2*empty_px)      */
+  int32_t empty_px;        /* zero padding of the object coefficient         */
+  int32_t exact_ref_coeff; /* coef = (k/2i)(n^2-1) instead of (k/i)(n-1)     */
+  int32_t field_is_delta;  /* the index array holds n - 1 instead of n       */
+  double k;                /* wavenumber 2*pi/lambda                         */
+  double dz;               /* z step                                         */
+  double k_off[2];         /* interior off-diagonal of K (mu_x)              */
+  double k_diag[2];        /* interior diagonal of K (-2 mu_x)               */
+  double k_d0[2];          /* K[0,0]                                          */
+  double k_dn[2];          /* K[N-1,N-1]                                      */
+  double k_01[2];          /* K[0,1]                                          */
+  double k_nm[2];          /* K[N-1,N-2]                                      */
+} tp_cn2d_op;
+
+/* Arguments of one batched march over all probes. */
+typedef struct tp_cn2d_march_args {
+  int32_t num_probes;        /* P                                             */
+  int32_t mode;              /* tp_mode; must match the factor set            */
+  const void *probes;        /* float2 (P, N) initial fields, or NULL (zero)  */
+  const void *src_shared;    /* float2 (L, N) probe-independent source, row t-1
+                                used at step t (exact test boundary data,
+                                reference boundary_condition_test.py:109-114),
+                                or NULL                                       */
+  const void *src_probe;     /* float2 (P, L, N) per-probe source (the
+                                reference's rhs_block transposed to slice-major;
+                                slice t-1 at step t, or L-t for the adjoint
+                                modes), or NULL                               */
+  const void *src_exit;      /* float2 (P, N) source applied at the first step
+                                only (exit-wave error for the adjoints), or NULL */
+  void *u_store;             /* float2 (P, nz, Npad) full field in the chunked
+                                layout (see tp_cn2d_chunked_rows), or NULL    */
+  void *exit_out;            /* float2 (P, N) last-step field, or NULL        */
+  const void *u_fwd;         /* ADJOINT_EXACT + gradient: forward full field
+                                (chunked, as written by a FORWARD march)      */
+  void *grad_c;              /* ADJOINT_EXACT: float2 (L, N) accumulator of
+                                sum_p lambda_s * conj(u_s + u_{s-1}); the caller
+                                zeroes it; row s-1 holds slice s               */
+  int32_t flags;             /* reserved, 0                                   */
+  int32_t reserved;
+} tp_cn2d_march_args;
+
+/* Rows per lane M and padded row count Npad = 32*M used for N. */
+TP_API int tp_cn2d_rows_per_lane(int32_t n, int32_t *rows_per_lane, int32_t *npad);
+
+/* Bytes of the per-slice factor workspace for (N, nz). */
+TP_API size_t tp_cn2d_factor_bytes(int32_t n, int32_t nz);
+
+/*
+ * Factorise every slice's LHS (the reference's _build_lu_factors,
+ * iterative_lu.py:103-133, and the per-mode matrix choice of :90-128) into
+ * the caller's workspace.  `n_field` is the refractive index, shape
+ * (n_obj, nz), row-major, dtype `n_dtype`.
+ */
+TP_API int tp_cn2d_factor(const tp_cn2d_op *op, const void *n_field, int32_t n_dtype, int32_t mode,
+                   void *factors, size_t factors_bytes, tp_stream_t stream);
+
+/*
+ * March all probes through the slices with a factor set of the same mode
+ * (the reference's per-probe loop iterative_lu.py:138-197 and the serial
+ * probe loop base/base_solver.py:124-143, batched).
+ */
+TP_API int tp_cn2d_march(const tp_cn2d_op *op, const void *factors, const tp_cn2d_march_args *args,
+                  tp_stream_t stream);
+
+/*
+ * Map the per-step gradient sum_p lambda_s conj(u_s + u_{s-1}) (L, N) onto the
+ * refractive-index nodes (n_obj, nz) (torch convention d/dRe + i d/dIm):
+ * g_n[x, t] = conj((dz/4) coef'(n[x,t])) * (g_c[t] + g_c[t+1]).
+ * `n_field` is needed only when exact_ref_coeff is set (else may be NULL).
+ * grad_n is float2 (n_obj, nz), row-major, overwritten.
+ */
+TP_API int tp_cn2d_grad_to_n(const tp_cn2d_op *op, const void *grad_c, const void *n_field, int32_t n_dtype,
+                      void *grad_n, tp_stream_t stream);
+
+/* Gather a chunked full field (P, nz, Npad) into the reference layout
+ * (P, N, nz) complex64. */
+TP_API int tp_cn2d_unchunk(const tp_cn2d_op *op, int32_t num_probes, const void *u_store, void *u_out,
+                    tp_stream_t stream);
+
+/* Synchronise `stream` and report device-side failures of earlier launches
+ * (a bounded wait that gave up).  Returns TP_ERR_TIMEOUT and clears the flag
+ * when one was recorded; *code receives the raw device code (0 = none). */
+TP_API int tp_device_status(tp_stream_t stream, int32_t *code);
+
+/* Message of the last failed call on this thread ("" if none). */
+TP_API const char *tp_last_error_string(void);
+
+/* Library version (major*10000 + minor*100 + patch). */
+TP_API int tp_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TPCUDA_H */

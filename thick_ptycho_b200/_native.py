@@ -1,0 +1,123 @@
+"""ctypes binding of libtpcuda.so (declared in include/tpcuda.h).
+
+The library is built in-tree by :mod:`thick_ptycho_b200.build_native`.  There
+is no fallback: if it is missing or fails to load, every GPU entry point
+raises :class:`NativeLibraryError`.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+from .build_native import LIB
+
+_lock = threading.Lock()
+_lib = None
+
+TP_OK = 0
+TP_ERR_TIMEOUT = 4
+
+MODE_FORWARD = 0
+MODE_ADJOINT = 1
+MODE_REVERSE = 2
+MODE_ADJOINT_EXACT = 3
+MODES = {"forward": MODE_FORWARD, "adjoint": MODE_ADJOINT, "reverse": MODE_REVERSE, "adjoint_exact": MODE_ADJOINT_EXACT}
+
+C128 = 0
+C64 = 1
+
+
+class NativeLibraryError(RuntimeError):
+    """libtpcuda.so is missing, failed to load, or a call returned an error."""
+
+
+class TpCn2dOp(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int32),
+        ("nz", ctypes.c_int32),
+        ("n_obj", ctypes.c_int32),
+        ("empty_px", ctypes.c_int32),
+        ("exact_ref_coeff", ctypes.c_int32),
+        ("field_is_delta", ctypes.c_int32),
+        ("k", ctypes.c_double),
+        ("dz", ctypes.c_double),
+        ("k_off", ctypes.c_double * 2),
+        ("k_diag", ctypes.c_double * 2),
+        ("k_d0", ctypes.c_double * 2),
+        ("k_dn", ctypes.c_double * 2),
+        ("k_01", ctypes.c_double * 2),
+        ("k_nm", ctypes.c_double * 2),
+    ]
+
+
+class TpCn2dMarchArgs(ctypes.Structure):
+    _fields_ = [
+        ("num_probes", ctypes.c_int32),
+        ("mode", ctypes.c_int32),
+        ("probes", ctypes.c_void_p),
+        ("src_shared", ctypes.c_void_p),
+        ("src_probe", ctypes.c_void_p),
+        ("src_exit", ctypes.c_void_p),
+        ("u_store", ctypes.c_void_p),
+        ("exit_out", ctypes.c_void_p),
+        ("u_fwd", ctypes.c_void_p),
+        ("grad_c", ctypes.c_void_p),
+        ("flags", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+# (name, restype, argtypes) of every exported symbol of include/tpcuda.h
+SIGNATURES = [
+    ("tp_cn2d_rows_per_lane", ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
+    ("tp_cn2d_factor_bytes", ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
+    ("tp_cn2d_factor", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                      ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    ("tp_cn2d_march", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_void_p, ctypes.POINTER(TpCn2dMarchArgs),
+                                     ctypes.c_void_p]),
+    ("tp_cn2d_grad_to_n", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                         ctypes.c_void_p, ctypes.c_void_p]),
+    ("tp_cn2d_unchunk", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p]),
+    ("tp_device_status", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
+    ("tp_last_error_string", ctypes.c_char_p, []),
+    ("tp_version", ctypes.c_int, []),
+]
+
+
+def lib_path() -> str:
+    return os.environ.get("TPCUDA_LIB", LIB)
+
+
+def load() -> ctypes.CDLL:
+    """Load libtpcuda.so once; raise NativeLibraryError if it is unavailable."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        path = lib_path()
+        if not os.path.exists(path):
+            raise NativeLibraryError(
+                f"{path} not found: build it with `python -m thick_ptycho_b200.build_native` "
+                "(there is no CPU fallback)"
+            )
+        try:
+            lib = ctypes.CDLL(path)
+        except OSError as e:  # pragma: no cover - depends on the machine
+            raise NativeLibraryError(f"failed to load {path}: {e}") from e
+        for name, res, args in SIGNATURES:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def check(rc: int, what: str):
+    if rc != TP_OK:
+        msg = load().tp_last_error_string().decode(errors="replace")
+        raise NativeLibraryError(f"{what} failed (status {rc}): {msg}")

@@ -1,0 +1,169 @@
+"""Batched 2D Crank–Nicolson propagation on the GPU (host side).
+
+:class:`CN2D` owns the device workspaces of one geometry and calls the C ABI
+of libtpcuda.so (``include/tpcuda.h``) on the current torch CUDA stream.
+Tensors are complex64 on the device except the refractive index, which may
+be complex128 (``n``) or complex64 holding ``n − 1`` (``is_delta=True``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional
+
+import torch
+
+from . import _native
+from .operators import BCCoefficients, normalize_bc, operator_1d
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(device) -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _c2(z: complex):
+    return (ctypes.c_double * 2)(z.real, z.imag)
+
+
+@dataclass
+class FactorSet:
+    mode: int
+    buf: torch.Tensor  # uint8 workspace
+
+
+class CN2D:
+    """One 2D geometry: N transverse rows, nz nodes (L = nz − 1 steps)."""
+
+    def __init__(self, n, nz, k, dx, dz, bc_type="impedance", empty_px=0, exact_ref_coeff=False, device=None):
+        if not torch.cuda.is_available():
+            raise _native.NativeLibraryError("CN2D needs a CUDA device (there is no CPU fallback)")
+        self.lib = _native.load()
+        self.device = torch.device(device if device is not None else "cuda")
+        self.n, self.nz, self.L = int(n), int(nz), int(nz) - 1
+        self.k, self.dx, self.dz = float(k), float(dx), float(dz)
+        self.bc_type = normalize_bc(bc_type)
+        self.empty_px = int(empty_px)
+        self.n_obj = self.n - 2 * self.empty_px
+        self.exact_ref_coeff = bool(exact_ref_coeff)
+        co = BCCoefficients.make(self.k, self.dx, self.dz, self.bc_type)
+        self.kop = operator_1d(self.n, co, self.bc_type, self.dz)
+        m = ctypes.c_int32()
+        npad = ctypes.c_int32()
+        _native.check(self.lib.tp_cn2d_rows_per_lane(self.n, ctypes.byref(m), ctypes.byref(npad)), "tp_cn2d_rows_per_lane")
+        self.rows_per_lane, self.npad = m.value, npad.value
+        self.factor_bytes = int(self.lib.tp_cn2d_factor_bytes(self.n, self.nz))
+
+    # ------------------------------------------------------------------ op
+    def op(self, is_delta=False) -> _native.TpCn2dOp:
+        o = _native.TpCn2dOp()
+        o.n, o.nz, o.n_obj, o.empty_px = self.n, self.nz, self.n_obj, self.empty_px
+        o.exact_ref_coeff = int(self.exact_ref_coeff)
+        o.field_is_delta = int(is_delta)
+        o.k, o.dz = self.k, self.dz
+        o.k_off, o.k_diag = _c2(self.kop.k_off), _c2(self.kop.k_diag)
+        o.k_d0, o.k_dn = _c2(self.kop.k_d0), _c2(self.kop.k_dn)
+        o.k_01, o.k_nm = _c2(self.kop.k_01), _c2(self.kop.k_nm)
+        return o
+
+    def _check_field(self, field: torch.Tensor):
+        if field.device != self.device and not (field.is_cuda and self.device.type == "cuda"):
+            raise ValueError("refractive index must be on the solver's device")
+        if tuple(field.shape) != (self.n_obj, self.nz):
+            raise ValueError(f"refractive index has shape {tuple(field.shape)}, expected {(self.n_obj, self.nz)}")
+        if field.dtype not in (torch.complex128, torch.complex64):
+            raise TypeError("refractive index must be complex128 or complex64")
+        return field.contiguous()
+
+    # ------------------------------------------------------------- factor
+    def new_factor_buffer(self) -> torch.Tensor:
+        return torch.empty(self.factor_bytes, dtype=torch.uint8, device=self.device)
+
+    def factor(self, field: torch.Tensor, mode="forward", is_delta=False, out: Optional[torch.Tensor] = None) -> FactorSet:
+        """Per-slice factor set of ``mode`` for the index field ``field``."""
+        field = self._check_field(field)
+        mode_i = _native.MODES[mode] if isinstance(mode, str) else int(mode)
+        buf = out if out is not None else self.new_factor_buffer()
+        dtype = _native.C128 if field.dtype == torch.complex128 else _native.C64
+        o = self.op(is_delta)
+        rc = self.lib.tp_cn2d_factor(ctypes.byref(o), _ptr(field), dtype, mode_i, _ptr(buf), buf.numel(),
+                                     _stream(self.device))
+        _native.check(rc, "tp_cn2d_factor")
+        return FactorSet(mode_i, buf)
+
+    # -------------------------------------------------------------- march
+    def march(
+        self,
+        fs: FactorSet,
+        num_probes: int,
+        probes: Optional[torch.Tensor] = None,
+        src_shared: Optional[torch.Tensor] = None,
+        src_probe: Optional[torch.Tensor] = None,
+        src_exit: Optional[torch.Tensor] = None,
+        u_store: Optional[torch.Tensor] = None,
+        exit_out: Optional[torch.Tensor] = None,
+        u_fwd: Optional[torch.Tensor] = None,
+        grad_c: Optional[torch.Tensor] = None,
+    ):
+        """One batched march; every tensor is complex64, contiguous, on device."""
+        P = int(num_probes)
+        shapes = {
+            "probes": (probes, (P, self.n)),
+            "src_shared": (src_shared, (self.L, self.n)),
+            "src_probe": (src_probe, (P, self.L, self.n)),
+            "src_exit": (src_exit, (P, self.n)),
+            "u_store": (u_store, (P, self.nz, self.npad)),
+            "exit_out": (exit_out, (P, self.n)),
+            "u_fwd": (u_fwd, None),
+            "grad_c": (grad_c, (self.L, self.n)),
+        }
+        for name, (t, shp) in shapes.items():
+            if t is None:
+                continue
+            if t.dtype != torch.complex64 or not t.is_contiguous() or not t.is_cuda:
+                raise TypeError(f"{name} must be a contiguous complex64 CUDA tensor")
+            if shp is not None and tuple(t.shape) != shp:
+                raise ValueError(f"{name} has shape {tuple(t.shape)}, expected {shp}")
+        if u_fwd is not None and (u_fwd.shape[1:] != (self.nz, self.npad) or u_fwd.shape[0] < P):
+            raise ValueError("u_fwd must be a chunked forward field (P, nz, Npad)")
+        a = _native.TpCn2dMarchArgs()
+        a.num_probes, a.mode = P, fs.mode
+        a.probes, a.src_shared, a.src_probe, a.src_exit = _ptr(probes), _ptr(src_shared), _ptr(src_probe), _ptr(src_exit)
+        a.u_store, a.exit_out, a.u_fwd, a.grad_c = _ptr(u_store), _ptr(exit_out), _ptr(u_fwd), _ptr(grad_c)
+        o = self.op()
+        rc = self.lib.tp_cn2d_march(ctypes.byref(o), _ptr(fs.buf), ctypes.byref(a), _stream(self.device))
+        _native.check(rc, "tp_cn2d_march")
+
+    # ------------------------------------------------------------ helpers
+    def new_store(self, num_probes: int) -> torch.Tensor:
+        return torch.empty((num_probes, self.nz, self.npad), dtype=torch.complex64, device=self.device)
+
+    def unchunk(self, u_store: torch.Tensor) -> torch.Tensor:
+        """Chunked (P, nz, Npad) → reference layout (P, N, nz)."""
+        P = u_store.shape[0]
+        out = torch.empty((P, self.n, self.nz), dtype=torch.complex64, device=self.device)
+        o = self.op()
+        rc = self.lib.tp_cn2d_unchunk(ctypes.byref(o), P, _ptr(u_store), _ptr(out), _stream(self.device))
+        _native.check(rc, "tp_cn2d_unchunk")
+        return out
+
+    def grad_to_n(self, grad_c: torch.Tensor, field: Optional[torch.Tensor] = None, is_delta=False) -> torch.Tensor:
+        """Σ_p λ conj(u_s + u_{s−1}) (L, N) → torch-convention gradient on n (n_obj, nz)."""
+        out = torch.empty((self.n_obj, self.nz), dtype=torch.complex64, device=self.device)
+        dtype = _native.C128
+        if field is not None:
+            field = self._check_field(field)
+            dtype = _native.C128 if field.dtype == torch.complex128 else _native.C64
+        o = self.op(is_delta)
+        rc = self.lib.tp_cn2d_grad_to_n(ctypes.byref(o), _ptr(grad_c), _ptr(field), dtype, _ptr(out), _stream(self.device))
+        _native.check(rc, "tp_cn2d_grad_to_n")
+        return out
+
+    def device_status(self):
+        code = ctypes.c_int32()
+        rc = self.lib.tp_device_status(_stream(self.device), ctypes.byref(code))
+        _native.check(rc, "tp_device_status")

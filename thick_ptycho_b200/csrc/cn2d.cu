@@ -1,0 +1,767 @@
+// 2D paraxial Crank–Nicolson march (1D transverse), batched over probes.
+//
+// Replaces the reference's per-slice sparse LU (iterative_lu.py:103-133) and
+// per-probe z-march (iterative_lu.py:138-197, base/base_solver.py:124-143).
+//
+// Step t of a march solves  M_s u_t = R_s u_{t-1} + b_t  with
+//   M_s = I - P_s,  R_s = I + P_s,  P_s = sigma * T(K + diag(c_s)),
+// where sigma = -1 for REVERSE, T = conjugate transpose for the adjoints and
+// s = t (forward) or L+1-t (backward).  For ADJOINT_EXACT the right-hand side
+// of step t uses P_{s+1} (the exact transpose of the forward recursion).
+//
+// Numerics: every coefficient is held as a deviation from the identity
+// ("1 + eps" form): x*(1+eps) is evaluated as x + x*eps.  Rounding a diagonal
+// of size ~1 to fp32 would otherwise perturb the operator by 6e-8 absolute
+// every slice, a systematic error that grows linearly with the number of
+// slices (4e-5 relative after 1023 slices at N = 2048); in this form the
+// complex64 march stays at ~3e-6 of the complex128 result.
+//
+// Tridiagonal solve (one warp per probe, 32 lanes): the N_pad = 32*M rows are
+// cut into 32 chunks of M rows, one per lane.  The last row of each chunk is
+// a separator; the M-1 interior rows are eliminated in terms of the two
+// neighbouring separators (Schur complement), which leaves a 32-unknown
+// tridiagonal system solved by 5 levels of warp-shuffle parallel cyclic
+// reduction.  Everything that depends only on the matrix (interior LU
+// factors, the two spike vectors, the PCR multipliers) is probe-independent;
+// it is computed once per slice in fp64 by cn2d_factor_kernel and streamed
+// into shared memory with bulk (TMA) copies, so each probe pays only for
+// right-hand-side work.  Data layout of one slice of the factor set (float2
+// [rows][32 lanes], row i of lane k is matrix row k*M + i):
+//   QD  [M][32]  diagonal of P_s
+//   LF  [M][32]  interior forward multipliers (row 0 unused)
+//   EP  [M][32]  interior inverse pivots minus one
+//   V   [M][32]  spike: response of the interior to the left separator
+//   W   [M][32]  spike: response of the interior to the own separator
+//   LR  [13][32] per-lane reduced-system data: M sub / super at the
+//                separator, 5 PCR alpha, 5 PCR gamma, 1/d_final - 1
+// The full field is stored in the same chunked layout (row k*M+i at offset
+// i*32+k of a slice), so every warp-wide load/store moves 256 contiguous bytes.
+
+#include <cuda_runtime.h>
+#include <stdio.h>
+
+#include "tp_common.cuh"
+#include "tp_errors.h"
+#include "tpcuda.h"
+
+namespace tp {
+
+constexpr int kLaneRecs = 13;
+constexpr int kRecMA = 0, kRecMC = 1, kRecAlpha = 2, kRecGamma = 7, kRecRDE = 12;
+constexpr int kMarchWarps = 4;
+constexpr int kMaxRowsPerLane = 64;
+constexpr int kFactorWarps = 4;
+
+// Rows-per-lane values with compiled kernels.
+static const int kRowSet[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64};
+
+__host__ __device__ inline size_t cn2d_slice_bytes(int M) {
+  size_t b = (size_t)(5 * M + kLaneRecs) * kLanes * sizeof(float2);
+  return (b + 255) & ~size_t(255);
+}
+
+static int rows_per_lane_for(int n) {
+  int need = (n + kLanes - 1) / kLanes;
+  for (int m : kRowSet)
+    if (m >= need) return m;
+  return -1;
+}
+
+// --------------------------------------------------------------------------
+// Factorisation (fp64)
+// --------------------------------------------------------------------------
+struct FactorParams {
+  int N, L, M, nz, n_obj, empty_px, exact, is_delta, dtype;
+  double sigma;
+  int conj_t;
+  double k, dz;
+  double2 k_off, k_diag, k_d0, k_dn, k_01, k_nm;
+  const void *n;
+  char *factors;
+  size_t slice_bytes;
+};
+
+__device__ __forceinline__ double2 load_n(const FactorParams &f, int row, int col) {
+  size_t idx = (size_t)row * f.nz + col;
+  if (f.dtype == TP_C128) return static_cast<const double2 *>(f.n)[idx];
+  float2 v = static_cast<const float2 *>(f.n)[idx];
+  return z2(v.x, v.y);
+}
+
+// coef(n) of base_simulation_space.py:356-360 (v = n, or n - 1 if is_delta)
+__device__ __forceinline__ double2 coef_of(const FactorParams &f, double2 v) {
+  double2 d = f.is_delta ? v : z2(v.x - 1.0, v.y);
+  if (!f.exact) return z2(f.k * d.y, -f.k * d.x);            // (k/i) d
+  double2 w = zadd(zscale(d, 2.0), zmul(d, d));               // n^2 - 1
+  return z2(0.5 * f.k * w.y, -0.5 * f.k * w.x);               // (k/2i) w
+}
+
+// C_s at matrix row g for slice index sl (0-based; nodes sl, sl+1).
+__device__ __forceinline__ double2 obj_c(const FactorParams &f, int g, int sl) {
+  int r = g - f.empty_px;
+  if (r < 0 || r >= f.n_obj) return z2(0.0, 0.0);
+  double2 c0 = coef_of(f, load_n(f, r, sl)), c1 = coef_of(f, load_n(f, r, sl + 1));
+  return zscale(zadd(c0, c1), 0.25 * f.dz);
+}
+
+__device__ __forceinline__ double2 k_sub(const FactorParams &f, int g) {  // K[g, g-1]
+  return (g == f.N - 1) ? f.k_nm : f.k_off;
+}
+__device__ __forceinline__ double2 k_sup(const FactorParams &f, int g) {  // K[g, g+1]
+  return (g == 0) ? f.k_01 : f.k_off;
+}
+__device__ __forceinline__ double2 p_diag(const FactorParams &f, int g, int sl) {
+  if (g >= f.N) return z2(0.0, 0.0);
+  double2 d = zadd((g == 0) ? f.k_d0 : ((g == f.N - 1) ? f.k_dn : f.k_diag), obj_c(f, g, sl));
+  if (f.conj_t) d = zconj(d);
+  return zscale(d, f.sigma);
+}
+__device__ __forceinline__ double2 p_sub(const FactorParams &f, int g) {  // P[g, g-1]
+  if (g < 1 || g > f.N - 1) return z2(0.0, 0.0);
+  double2 v = f.conj_t ? zconj(k_sup(f, g - 1)) : k_sub(f, g);
+  return zscale(v, f.sigma);
+}
+__device__ __forceinline__ double2 p_sup(const FactorParams &f, int g) {  // P[g, g+1]
+  if (g < 0 || g > f.N - 2) return z2(0.0, 0.0);
+  double2 v = f.conj_t ? zconj(k_sub(f, g + 1)) : k_sup(f, g);
+  return zscale(v, f.sigma);
+}
+
+// One warp per slice, one lane per chunk.
+__global__ void __launch_bounds__(kFactorWarps * 32) cn2d_factor_kernel(const FactorParams f) {
+  const int lane = threadIdx.x & 31;
+  const int sl = blockIdx.x * kFactorWarps + (threadIdx.x >> 5);
+  if (sl >= f.L) return;  // warp-uniform
+  const int M = f.M;
+  float2 *base = reinterpret_cast<float2 *>(f.factors + (size_t)sl * f.slice_bytes);
+  float2 *QD = base, *LF = base + M * 32, *EP = base + 2 * M * 32, *V = base + 3 * M * 32,
+         *W = base + 4 * M * 32, *LR = base + 5 * M * 32;
+
+  double2 pl[kMaxRowsPerLane], msl[kMaxRowsPerLane], fv[kMaxRowsPerLane];
+  const int g0 = lane * M;
+  double2 p_prev = z2(1, 0), msup_prev = z2(0, 0), fvv = z2(0, 0);
+  double2 me_a = z2(0, 0), me_d = z2(1, 0), me_c = z2(0, 0);
+  for (int i = 0; i < M; ++i) {
+    const int g = g0 + i;
+    const double2 pd = p_diag(f, g, sl);
+    QD[i * 32 + lane] = to_f2(pd);
+    const double2 md = z2(1.0 - pd.x, -pd.y);
+    const double2 msub = zneg(p_sub(f, g));
+    const double2 msup = zneg(p_sup(f, g));
+    if (i < M - 1) {
+      double2 l, p;
+      if (i == 0) {
+        l = z2(0, 0);
+        p = md;
+        fvv = zneg(msub);  // spike v forward part: -M[g0, g0-1] e_0
+      } else {
+        l = zdiv(msub, p_prev);
+        p = zsub(md, zmul(l, msup_prev));
+        fvv = zneg(zmul(l, fvv));
+      }
+      LF[i * 32 + lane] = to_f2(l);
+      EP[i * 32 + lane] = to_f2(zdiv(z2(1.0 - p.x, -p.y), p));  // 1/p - 1
+      pl[i] = p;
+      msl[i] = msup;
+      fv[i] = fvv;
+      p_prev = p;
+      msup_prev = msup;
+    } else {
+      me_d = md;
+      me_a = msub;
+      me_c = msup;
+      LF[i * 32 + lane] = make_float2(0.f, 0.f);
+      EP[i * 32 + lane] = make_float2(0.f, 0.f);
+      V[i * 32 + lane] = make_float2(0.f, 0.f);
+      W[i * 32 + lane] = make_float2(0.f, 0.f);
+    }
+  }
+  double2 v_last, w_last, v_first, w_first;
+  if (M >= 2) {
+    double2 v = zdiv(fv[M - 2], pl[M - 2]);
+    double2 w = zdiv(zneg(msl[M - 2]), pl[M - 2]);
+    V[(M - 2) * 32 + lane] = to_f2(v);
+    W[(M - 2) * 32 + lane] = to_f2(w);
+    v_last = v;
+    w_last = w;
+    for (int i = M - 3; i >= 0; --i) {
+      v = zdiv(zsub(fv[i], zmul(msl[i], v)), pl[i]);
+      w = zdiv(zneg(zmul(msl[i], w)), pl[i]);
+      V[i * 32 + lane] = to_f2(v);
+      W[i * 32 + lane] = to_f2(w);
+    }
+    v_first = v;
+    w_first = w;
+  } else {
+    v_last = z2(1, 0);
+    w_last = z2(0, 0);
+    v_first = z2(0, 0);
+    w_first = z2(1, 0);
+  }
+  // Reduced 32-unknown tridiagonal system on the separators.
+  const double2 vf_n = shfl_down_z(v_first, 1), wf_n = shfl_down_z(w_first, 1);
+  double2 ra = zmul(me_a, v_last);
+  double2 rd = zadd(me_d, zadd(zmul(me_a, w_last), lane < 31 ? zmul(me_c, vf_n) : z2(0, 0)));
+  double2 rc = lane < 31 ? zmul(me_c, wf_n) : z2(0, 0);
+  LR[kRecMA * 32 + lane] = to_f2(me_a);
+  LR[kRecMC * 32 + lane] = to_f2(lane < 31 ? me_c : z2(0, 0));
+  for (int l = 0; l < 5; ++l) {
+    const int s = 1 << l;
+    const double2 ra_m = shfl_up_z(ra, s), rd_m = shfl_up_z(rd, s), rc_m = shfl_up_z(rc, s);
+    const double2 ra_p = shfl_down_z(ra, s), rd_p = shfl_down_z(rd, s), rc_p = shfl_down_z(rc, s);
+    const double2 al = (lane >= s) ? zneg(zdiv(ra, rd_m)) : z2(0, 0);
+    const double2 ga = (lane < 32 - s) ? zneg(zdiv(rc, rd_p)) : z2(0, 0);
+    const double2 nra = zmul(al, ra_m), nrc = zmul(ga, rc_p);
+    rd = zadd(rd, zadd(zmul(al, rc_m), zmul(ga, ra_p)));
+    ra = nra;
+    rc = nrc;
+    LR[(kRecAlpha + l) * 32 + lane] = to_f2(al);
+    LR[(kRecGamma + l) * 32 + lane] = to_f2(ga);
+  }
+  LR[kRecRDE * 32 + lane] = to_f2(zdiv(z2(1.0 - rd.x, -rd.y), rd));
+}
+
+// --------------------------------------------------------------------------
+// March
+// --------------------------------------------------------------------------
+struct Spec {
+  float2 p_o;                         // interior off-diagonal of P
+  float2 sup0, sub1, supN2, subN1;    // P[0,1], P[1,0], P[N-2,N-1], P[N-1,N-2]
+  float2 d_sup0, d_sub1, d_supN2, d_subN1;  // the same minus p_o
+};
+
+struct MarchParams {
+  int N, L, nz, P, Npad;
+  int backward, flip_out, src_rev;
+  size_t slice_bytes;
+  const char *factors;
+  Spec sp;
+  const float2 *probes, *src_shared, *src_probe, *src_exit;
+  float2 *u_store, *exit_out;
+  const float2 *u_fwd;
+  float2 *grad_c;
+  int *err;
+};
+
+// U <- (I + P_s) U with P's boundary-row specials.
+template <int M, bool ALIGNED>
+__device__ __forceinline__ void cn2d_rhs(float2 (&U)[M], const float2 *__restrict__ QD, int lane,
+                                         const MarchParams &p) {
+  const float2 zero = make_float2(0.f, 0.f);
+  const float2 left = shfl_up2(U[M - 1], 1);
+  const float2 right = shfl_down2(U[0], 1);
+  float2 prev = (lane == 0) ? zero : left;
+  const float2 rlast = (lane == 31) ? zero : right;
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+    const float2 cur = U[i];
+    const float2 nxt = (i < M - 1) ? U[(i + 1) < M ? i + 1 : i] : rlast;
+    float2 r = cfma(QD[i * 32 + lane], cur, cur);
+    if constexpr (ALIGNED) {
+      r = cfma(p.sp.p_o, cadd(prev, nxt), r);
+      if (i == 0 && lane == 0) r = cfma(p.sp.d_sup0, nxt, r);
+      if ((M >= 2 ? (i == 1) : (i == 0)) && lane == (M >= 2 ? 0 : 1)) r = cfma(p.sp.d_sub1, prev, r);
+      if ((M >= 2 ? (i == M - 2) : (i == 0)) && lane == (M >= 2 ? 31 : 30)) r = cfma(p.sp.d_supN2, nxt, r);
+      if (i == M - 1 && lane == 31) r = cfma(p.sp.d_subN1, prev, r);
+    } else {
+      const int g = lane * M + i;
+      const float2 psub = (g == p.N - 1) ? p.sp.subN1 : ((g == 1) ? p.sp.sub1 : p.sp.p_o);
+      const float2 psup = (g == 0) ? p.sp.sup0 : ((g == p.N - 2) ? p.sp.supN2 : p.sp.p_o);
+      r = cfma(psub, prev, r);
+      r = cfma(psup, nxt, r);
+      if (g >= p.N) r = zero;
+    }
+    prev = cur;
+    U[i] = r;
+  }
+}
+
+// U <- M_s^{-1} U (partitioned solve with the slice's factor set F).
+template <int M, bool ALIGNED>
+__device__ __forceinline__ void cn2d_solve(float2 (&U)[M], const float2 *__restrict__ F, int lane,
+                                           const MarchParams &p) {
+  const float2 *LF = F + M * 32, *EP = F + 2 * M * 32, *V = F + 3 * M * 32, *W = F + 4 * M * 32,
+               *LR = F + 5 * M * 32;
+  if constexpr (M >= 2) {
+#pragma unroll
+    for (int i = 1; i <= M - 2; ++i) U[i] = cfnma(LF[i * 32 + lane], U[i - 1], U[i]);
+    {
+      const float2 t = U[M - 2];
+      U[M - 2] = cfma(t, EP[(M - 2) * 32 + lane], t);
+    }
+    const float2 m_o = make_float2(-p.sp.p_o.x, -p.sp.p_o.y);
+#pragma unroll
+    for (int i = M - 3; i >= 0; --i) {
+      float2 msup = m_o;
+      if (i == 0 && lane == 0) msup = make_float2(-p.sp.sup0.x, -p.sp.sup0.y);
+      if constexpr (!ALIGNED) {
+        if (lane * M + i == p.N - 2) msup = make_float2(-p.sp.supN2.x, -p.sp.supN2.y);
+      }
+      const float2 t = cfnma(msup, U[i + 1], U[i]);
+      U[i] = cfma(t, EP[i * 32 + lane], t);
+    }
+  }
+  float2 rho;
+  if constexpr (M >= 2) {
+    const float2 y0n = shfl_down2(U[0], 1);
+    rho = cfnma(LR[kRecMA * 32 + lane], U[M - 2], U[M - 1]);
+    rho = cfnma(LR[kRecMC * 32 + lane], y0n, rho);
+  } else {
+    rho = U[0];
+  }
+#pragma unroll
+  for (int l = 0; l < 5; ++l) {
+    const int s = 1 << l;
+    const float2 up = shfl_up2(rho, s), dn = shfl_down2(rho, s);
+    const float2 r2 = cfma(LR[(kRecAlpha + l) * 32 + lane], up, rho);
+    rho = cfma(LR[(kRecGamma + l) * 32 + lane], dn, r2);
+  }
+  const float2 x = cfma(rho, LR[kRecRDE * 32 + lane], rho);
+  const float2 xp = shfl_up2(x, 1);
+  if constexpr (M >= 2) {
+#pragma unroll
+    for (int i = 0; i <= M - 2; ++i) U[i] = cfma(W[i * 32 + lane], x, cfma(V[i * 32 + lane], xp, U[i]));
+  }
+  U[M - 1] = x;
+}
+
+template <int M>
+__device__ __forceinline__ void add_natural(float2 (&U)[M], const float2 *__restrict__ src, int lane, int N) {
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+    const int g = lane * M + i;
+    if (g < N) U[i] = cadd(U[i], src[g]);
+  }
+}
+
+template <int M, bool ALIGNED, bool LAGGED>
+__global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const MarchParams p) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int probe = blockIdx.x * kMarchWarps + warp;
+  const bool active = probe < p.P;
+  const size_t sb = p.slice_bytes;
+  float2 *bufs = reinterpret_cast<float2 *>(smem);
+  float2 *gacc = reinterpret_cast<float2 *>(smem + 2 * sb);  // [2][M][33]
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + 2 * sb + 2 * M * 33 * sizeof(float2));
+  const bool do_grad = LAGGED && (p.grad_c != nullptr);
+  const size_t slice_f2 = sb / sizeof(float2);
+
+  if (tid == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    fence_mbar_init();
+  }
+  if (do_grad)
+    for (int e = tid; e < 2 * M * 33; e += blockDim.x) gacc[e] = make_float2(0.f, 0.f);
+  __syncthreads();
+
+  auto slice_of = [&](int t) { return p.backward ? (p.L + 1 - t) : t; };
+  if (tid == 0) {
+    mbar_arrive_expect_tx(&mbar[1], (uint32_t)sb);
+    bulk_g2s(bufs + slice_f2, p.factors + (size_t)(slice_of(1) - 1) * sb, (uint32_t)sb, &mbar[1]);
+  }
+
+  float2 U[M];
+#pragma unroll
+  for (int i = 0; i < M; ++i) U[i] = make_float2(0.f, 0.f);
+  if (active && p.probes != nullptr) add_natural<M>(U, p.probes + (size_t)probe * p.N, lane, p.N);
+  if (active && p.u_store != nullptr) {
+    const int t0 = p.flip_out ? p.L : 0;
+    float2 *dst = p.u_store + ((size_t)probe * p.nz + t0) * p.Npad;
+#pragma unroll
+    for (int i = 0; i < M; ++i) dst[i * 32 + lane] = U[i];
+  }
+
+  uint32_t phase = 0;
+  bool ok = mbar_wait_bounded(&mbar[1], 0, p.err);
+  phase ^= 2u;
+  if (__syncthreads_or(!ok)) {
+    // Give the copy that timed out a second bounded chance to land before the
+    // CTA's shared memory is released.
+    if (tid == 0) mbar_wait_bounded(&mbar[1], 0, nullptr);
+    __syncthreads();
+    return;
+  }
+
+  for (int t = 1; t <= p.L; ++t) {
+    const int cb = t & 1;
+    const int s = slice_of(t);
+    if (tid == 0 && t < p.L) {
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&mbar[cb ^ 1], (uint32_t)sb);
+      bulk_g2s(bufs + (cb ^ 1) * slice_f2, p.factors + (size_t)(slice_of(t + 1) - 1) * sb, (uint32_t)sb,
+               &mbar[cb ^ 1]);
+    }
+    const float2 *F = bufs + cb * slice_f2;
+    if (active) {
+      if constexpr (!LAGGED) cn2d_rhs<M, ALIGNED>(U, F, lane, p);
+      if (p.src_shared != nullptr) add_natural<M>(U, p.src_shared + (size_t)(t - 1) * p.N, lane, p.N);
+      if (p.src_probe != nullptr) {
+        const int col = p.src_rev ? (p.L - t) : (t - 1);
+        add_natural<M>(U, p.src_probe + ((size_t)probe * p.L + col) * p.N, lane, p.N);
+      }
+      if (t == 1 && p.src_exit != nullptr) add_natural<M>(U, p.src_exit + (size_t)probe * p.N, lane, p.N);
+      cn2d_solve<M, ALIGNED>(U, F, lane, p);
+      if (p.u_store != nullptr) {
+        const int to = p.flip_out ? (p.L - t) : t;
+        float2 *dst = p.u_store + ((size_t)probe * p.nz + to) * p.Npad;
+#pragma unroll
+        for (int i = 0; i < M; ++i) dst[i * 32 + lane] = U[i];
+      }
+      if (t == p.L && p.exit_out != nullptr) {
+        float2 *dst = p.exit_out + (size_t)probe * p.N;
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+          const int g = lane * M + i;
+          if (g < p.N) dst[g] = U[i];
+        }
+      }
+      if (do_grad) {
+        const float2 *ua = p.u_fwd + ((size_t)probe * p.nz + s) * p.Npad;
+        const float2 *ub = ua - p.Npad;
+        float2 *ga = gacc + cb * M * 33;
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+          const float2 w = cadd(ua[i * 32 + lane], ub[i * 32 + lane]);
+          const float2 v = cmulc(U[i], w);
+          atomicAdd(&ga[i * 33 + lane].x, v.x);
+          atomicAdd(&ga[i * 33 + lane].y, v.y);
+        }
+      }
+      if constexpr (LAGGED) cn2d_rhs<M, ALIGNED>(U, F, lane, p);
+    }
+    bool good = true;
+    if (t < p.L) {
+      good = mbar_wait_bounded(&mbar[cb ^ 1], (phase >> (cb ^ 1)) & 1u, p.err);
+      phase ^= (1u << (cb ^ 1));
+    }
+    if (__syncthreads_or(!good)) {
+      // The copy waited for is the only one in flight: drain it (bounded).
+      if (tid == 0) mbar_wait_bounded(&mbar[cb ^ 1], ((phase >> (cb ^ 1)) & 1u) ^ 1u, nullptr);
+      __syncthreads();
+      return;
+    }
+    if (do_grad) {
+      float2 *ga = gacc + cb * M * 33;
+      float2 *dst = p.grad_c + (size_t)(s - 1) * p.N;
+      for (int g = tid; g < p.N; g += blockDim.x) {
+        const int i = g % M, k = g / M;
+        const float2 v = ga[i * 33 + k];
+        atomicAdd(&dst[g], v);
+        ga[i * 33 + k] = make_float2(0.f, 0.f);
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// Layout and gradient helpers
+// --------------------------------------------------------------------------
+__global__ void cn2d_unchunk_kernel(const float2 *__restrict__ st, float2 *__restrict__ out, int P, int N, int nz,
+                                    int M, int Npad) {
+  const size_t total = (size_t)P * N * nz;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    const int t = (int)(idx % nz);
+    const size_t pg = idx / nz;
+    const int g = (int)(pg % N);
+    const size_t pp = pg / N;
+    out[idx] = st[(pp * nz + t) * Npad + (size_t)(g % M) * 32 + g / M];
+  }
+}
+
+struct GradParams {
+  int N, L, nz, n_obj, empty_px, exact, is_delta, dtype;
+  double k, dz;
+  const float2 *gc;
+  const void *n;
+  float2 *gn;
+};
+
+__global__ void cn2d_grad_to_n_kernel(const GradParams q) {
+  const size_t total = (size_t)q.n_obj * q.nz;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    const int t = (int)(idx % q.nz);
+    const int x = (int)(idx / q.nz);
+    const int g = x + q.empty_px;
+    double2 acc = z2(0, 0);
+    if (t >= 1) {
+      const float2 a = q.gc[(size_t)(t - 1) * q.N + g];
+      acc = zadd(acc, z2(a.x, a.y));
+    }
+    if (t <= q.L - 1) {
+      const float2 b = q.gc[(size_t)t * q.N + g];
+      acc = zadd(acc, z2(b.x, b.y));
+    }
+    // dc/dn = (dz/4) coef'(n); coef' = k/i  or (k/i) n
+    double2 d = z2(0.0, -0.25 * q.dz * q.k);
+    if (q.exact) {
+      double2 nv;
+      if (q.dtype == TP_C128) nv = static_cast<const double2 *>(q.n)[idx];
+      else {
+        float2 f = static_cast<const float2 *>(q.n)[idx];
+        nv = z2(f.x, f.y);
+      }
+      if (q.is_delta) nv.x += 1.0;
+      d = zmul(d, nv);
+    }
+    const double2 r = zmul(zconj(d), acc);
+    q.gn[idx] = make_float2((float)r.x, (float)r.y);
+  }
+}
+
+// Device error word (timeouts of bounded waits); read by tp_device_status.
+__device__ int g_device_error;
+
+static int *device_error_ptr() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  static int *ptrs[64] = {nullptr};
+  if (dev < 0 || dev >= 64) return nullptr;
+  if (ptrs[dev] == nullptr) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_device_error) != cudaSuccess) return nullptr;
+    ptrs[dev] = static_cast<int *>(p);
+  }
+  return ptrs[dev];
+}
+
+// --------------------------------------------------------------------------
+// Host launchers
+// --------------------------------------------------------------------------
+static inline double2 hz(const double v[2]) { return make_double2(v[0], v[1]); }
+
+static int validate_op(const tp_cn2d_op *op) {
+  if (op == nullptr) return set_error(TP_ERR_INVALID, "op is NULL");
+  if (op->n < 4) return set_error(TP_ERR_INVALID, "N=%d must be >= 4", op->n);
+  if (rows_per_lane_for(op->n) < 0)
+    return set_error(TP_ERR_UNSUPPORTED, "N=%d exceeds the register-resident limit of %d rows", op->n,
+                     kLanes * kMaxRowsPerLane);
+  if (op->nz < 2) return set_error(TP_ERR_INVALID, "nz=%d must be >= 2", op->nz);
+  if (op->empty_px < 0 || op->n_obj != op->n - 2 * op->empty_px)
+    return set_error(TP_ERR_INVALID, "n_obj=%d must equal N - 2*empty_px (N=%d, empty_px=%d)", op->n_obj, op->n,
+                     op->empty_px);
+  return TP_OK;
+}
+
+static void mode_transform(int mode, double *sigma, int *conj_t) {
+  *sigma = (mode == TP_MODE_REVERSE) ? -1.0 : 1.0;
+  *conj_t = (mode == TP_MODE_ADJOINT || mode == TP_MODE_ADJOINT_EXACT) ? 1 : 0;
+}
+
+// P's off-diagonal entries (host mirror of p_sub / p_sup).
+static Spec make_spec(const tp_cn2d_op *op, int mode) {
+  double sigma;
+  int ct;
+  mode_transform(mode, &sigma, &ct);
+  auto f = [&](const double v[2], bool conj) {
+    return make_float2((float)(sigma * v[0]), (float)(sigma * (conj ? -v[1] : v[1])));
+  };
+  Spec s;
+  s.p_o = f(op->k_off, ct);
+  if (!ct) {
+    s.sup0 = f(op->k_01, false);   // P[0,1] = K[0,1]
+    s.subN1 = f(op->k_nm, false);  // P[N-1,N-2] = K[N-1,N-2]
+    s.sub1 = s.p_o;
+    s.supN2 = s.p_o;
+  } else {
+    s.sub1 = f(op->k_01, true);    // P[1,0] = conj(K[0,1])
+    s.supN2 = f(op->k_nm, true);   // P[N-2,N-1] = conj(K[N-1,N-2])
+    s.sup0 = s.p_o;
+    s.subN1 = s.p_o;
+  }
+  auto d = [&](float2 a) { return make_float2(a.x - s.p_o.x, a.y - s.p_o.y); };
+  s.d_sup0 = d(s.sup0);
+  s.d_sub1 = d(s.sub1);
+  s.d_supN2 = d(s.supN2);
+  s.d_subN1 = d(s.subN1);
+  return s;
+}
+
+template <int M, bool ALIGNED, bool LAGGED>
+static int launch_march_t(const MarchParams &mp, cudaStream_t st) {
+  auto kern = cn2d_march_kernel<M, ALIGNED, LAGGED>;
+  const size_t smem = 2 * mp.slice_bytes + 2 * (size_t)M * 33 * sizeof(float2) + 2 * sizeof(uint64_t);
+  TP_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = (mp.P + kMarchWarps - 1) / kMarchWarps;
+  kern<<<grid, kMarchWarps * 32, smem, st>>>(mp);
+  return check_cuda(cudaGetLastError(), "cn2d_march_kernel launch");
+}
+
+template <int M>
+static int launch_march_m(const MarchParams &mp, bool aligned, bool lagged, cudaStream_t st) {
+  if (aligned) return lagged ? launch_march_t<M, true, true>(mp, st) : launch_march_t<M, true, false>(mp, st);
+  return lagged ? launch_march_t<M, false, true>(mp, st) : launch_march_t<M, false, false>(mp, st);
+}
+
+static int launch_march(int M, const MarchParams &mp, bool aligned, bool lagged, cudaStream_t st) {
+  switch (M) {
+#define TP_CASE(m) \
+  case m:          \
+    return launch_march_m<m>(mp, aligned, lagged, st);
+    TP_CASE(1)
+    TP_CASE(2)
+    TP_CASE(3)
+    TP_CASE(4)
+    TP_CASE(6)
+    TP_CASE(8)
+    TP_CASE(12)
+    TP_CASE(16)
+    TP_CASE(24)
+    TP_CASE(32)
+    TP_CASE(48)
+    TP_CASE(64)
+#undef TP_CASE
+    default:
+      return set_error(TP_ERR_UNSUPPORTED, "no kernel for %d rows per lane", M);
+  }
+}
+
+}  // namespace tp
+
+using namespace tp;
+
+extern "C" int tp_cn2d_rows_per_lane(int32_t n, int32_t *rows_per_lane, int32_t *npad) {
+  const int m = rows_per_lane_for(n);
+  if (n < 4 || m < 0) return set_error(TP_ERR_UNSUPPORTED, "N=%d unsupported (4 <= N <= %d)", n, 32 * kMaxRowsPerLane);
+  if (rows_per_lane) *rows_per_lane = m;
+  if (npad) *npad = 32 * m;
+  return TP_OK;
+}
+
+extern "C" size_t tp_cn2d_factor_bytes(int32_t n, int32_t nz) {
+  const int m = rows_per_lane_for(n);
+  if (m < 0 || nz < 2) return 0;
+  return cn2d_slice_bytes(m) * (size_t)(nz - 1);
+}
+
+extern "C" int tp_cn2d_factor(const tp_cn2d_op *op, const void *n_field, int32_t n_dtype, int32_t mode,
+                              void *factors, size_t factors_bytes, tp_stream_t stream) {
+  int rc = validate_op(op);
+  if (rc) return rc;
+  if (n_field == nullptr || factors == nullptr) return set_error(TP_ERR_INVALID, "n_field/factors is NULL");
+  if (n_dtype != TP_C128 && n_dtype != TP_C64) return set_error(TP_ERR_INVALID, "bad n_dtype %d", n_dtype);
+  if (mode < TP_MODE_FORWARD || mode > TP_MODE_ADJOINT_EXACT) return set_error(TP_ERR_INVALID, "bad mode %d", mode);
+  const size_t need = tp_cn2d_factor_bytes(op->n, op->nz);
+  if (factors_bytes < need)
+    return set_error(TP_ERR_WORKSPACE, "factor workspace %zu B < required %zu B", factors_bytes, need);
+  if ((reinterpret_cast<uintptr_t>(factors) & 255u) != 0)
+    return set_error(TP_ERR_INVALID, "factor workspace must be 256-byte aligned");
+  FactorParams f{};
+  f.N = op->n;
+  f.L = op->nz - 1;
+  f.M = rows_per_lane_for(op->n);
+  f.nz = op->nz;
+  f.n_obj = op->n_obj;
+  f.empty_px = op->empty_px;
+  f.exact = op->exact_ref_coeff;
+  f.is_delta = op->field_is_delta;
+  f.dtype = n_dtype;
+  mode_transform(mode, &f.sigma, &f.conj_t);
+  f.k = op->k;
+  f.dz = op->dz;
+  f.k_off = hz(op->k_off);
+  f.k_diag = hz(op->k_diag);
+  f.k_d0 = hz(op->k_d0);
+  f.k_dn = hz(op->k_dn);
+  f.k_01 = hz(op->k_01);
+  f.k_nm = hz(op->k_nm);
+  f.n = n_field;
+  f.factors = static_cast<char *>(factors);
+  f.slice_bytes = cn2d_slice_bytes(f.M);
+  const int grid = (f.L + kFactorWarps - 1) / kFactorWarps;
+  cn2d_factor_kernel<<<grid, kFactorWarps * 32, 0, reinterpret_cast<cudaStream_t>(stream)>>>(f);
+  return check_cuda(cudaGetLastError(), "cn2d_factor_kernel launch");
+}
+
+extern "C" int tp_cn2d_march(const tp_cn2d_op *op, const void *factors, const tp_cn2d_march_args *a,
+                             tp_stream_t stream) {
+  int rc = validate_op(op);
+  if (rc) return rc;
+  if (a == nullptr || factors == nullptr) return set_error(TP_ERR_INVALID, "args/factors is NULL");
+  if (a->num_probes < 1) return set_error(TP_ERR_INVALID, "num_probes=%d", a->num_probes);
+  if (a->mode < TP_MODE_FORWARD || a->mode > TP_MODE_ADJOINT_EXACT)
+    return set_error(TP_ERR_INVALID, "bad mode %d", a->mode);
+  if ((reinterpret_cast<uintptr_t>(factors) & 255u) != 0)
+    return set_error(TP_ERR_INVALID, "factor workspace must be 256-byte aligned");
+  const bool lagged = a->mode == TP_MODE_ADJOINT_EXACT;
+  if ((a->grad_c != nullptr) != (a->u_fwd != nullptr))
+    return set_error(TP_ERR_INVALID, "grad_c and u_fwd must be given together");
+  if (a->grad_c != nullptr && !lagged)
+    return set_error(TP_ERR_INVALID, "the fused gradient needs mode TP_MODE_ADJOINT_EXACT");
+  int *err = device_error_ptr();
+  if (err == nullptr) return set_error(TP_ERR_CUDA, "cannot resolve the device error word");
+  MarchParams mp{};
+  const int M = rows_per_lane_for(op->n);
+  mp.N = op->n;
+  mp.L = op->nz - 1;
+  mp.nz = op->nz;
+  mp.P = a->num_probes;
+  mp.Npad = 32 * M;
+  mp.backward = (a->mode != TP_MODE_FORWARD) ? 1 : 0;
+  mp.flip_out = (a->mode == TP_MODE_ADJOINT) ? 1 : 0;
+  mp.src_rev = (a->mode == TP_MODE_ADJOINT || a->mode == TP_MODE_ADJOINT_EXACT) ? 1 : 0;
+  mp.slice_bytes = cn2d_slice_bytes(M);
+  mp.factors = static_cast<const char *>(factors);
+  mp.sp = make_spec(op, a->mode);
+  mp.probes = static_cast<const float2 *>(a->probes);
+  mp.src_shared = static_cast<const float2 *>(a->src_shared);
+  mp.src_probe = static_cast<const float2 *>(a->src_probe);
+  mp.src_exit = static_cast<const float2 *>(a->src_exit);
+  mp.u_store = static_cast<float2 *>(a->u_store);
+  mp.exit_out = static_cast<float2 *>(a->exit_out);
+  mp.u_fwd = static_cast<const float2 *>(a->u_fwd);
+  mp.grad_c = static_cast<float2 *>(a->grad_c);
+  mp.err = err;
+  return launch_march(M, mp, op->n == 32 * M, lagged, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int tp_cn2d_unchunk(const tp_cn2d_op *op, int32_t num_probes, const void *u_store, void *u_out,
+                               tp_stream_t stream) {
+  int rc = validate_op(op);
+  if (rc) return rc;
+  if (u_store == nullptr || u_out == nullptr || num_probes < 1) return set_error(TP_ERR_INVALID, "bad unchunk args");
+  const int M = rows_per_lane_for(op->n);
+  cn2d_unchunk_kernel<<<1184, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      static_cast<const float2 *>(u_store), static_cast<float2 *>(u_out), num_probes, op->n, op->nz, M, 32 * M);
+  return check_cuda(cudaGetLastError(), "cn2d_unchunk_kernel launch");
+}
+
+extern "C" int tp_cn2d_grad_to_n(const tp_cn2d_op *op, const void *grad_c, const void *n_field, int32_t n_dtype,
+                                 void *grad_n, tp_stream_t stream) {
+  int rc = validate_op(op);
+  if (rc) return rc;
+  if (grad_c == nullptr || grad_n == nullptr) return set_error(TP_ERR_INVALID, "grad_c/grad_n is NULL");
+  if (op->exact_ref_coeff && n_field == nullptr) return set_error(TP_ERR_INVALID, "exact_ref_coeff needs n_field");
+  GradParams q{};
+  q.N = op->n;
+  q.L = op->nz - 1;
+  q.nz = op->nz;
+  q.n_obj = op->n_obj;
+  q.empty_px = op->empty_px;
+  q.exact = op->exact_ref_coeff;
+  q.is_delta = op->field_is_delta;
+  q.dtype = n_dtype;
+  q.k = op->k;
+  q.dz = op->dz;
+  q.gc = static_cast<const float2 *>(grad_c);
+  q.n = n_field;
+  q.gn = static_cast<float2 *>(grad_n);
+  cn2d_grad_to_n_kernel<<<592, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(q);
+  return check_cuda(cudaGetLastError(), "cn2d_grad_to_n_kernel launch");
+}
+
+extern "C" int tp_device_status(tp_stream_t stream, int32_t *code) {
+  int *err = device_error_ptr();
+  if (err == nullptr) return set_error(TP_ERR_CUDA, "cannot resolve the device error word");
+  int h = 0;
+  TP_CHECK_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, reinterpret_cast<cudaStream_t>(stream)));
+  TP_CHECK_CUDA(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)));
+  if (code) *code = h;
+  if (h != 0) {
+    const int zero = 0;
+    TP_CHECK_CUDA(cudaMemcpy(err, &zero, sizeof(int), cudaMemcpyHostToDevice));
+    return set_error(TP_ERR_TIMEOUT, "a device-side bounded wait timed out (code %d)", h);
+  }
+  return TP_OK;
+}

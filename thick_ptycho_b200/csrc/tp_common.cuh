@@ -1,0 +1,115 @@
+// Shared device helpers for libtpcuda: complex arithmetic, bulk-copy (TMA)
+// staging with bounded mbarrier waits, and the error channel.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tp {
+
+constexpr int kLanes = 32;
+
+// Device-side error channel: kernels never trap; a bounded wait that gives up
+// writes a code here and returns, the host reads it after the stream syncs.
+enum DeviceError : int { kDevOk = 0, kDevMbarTimeout = 1 };
+
+// ----------------------------------------------------------------- complex64
+__device__ __forceinline__ float2 c2(float x, float y) { return make_float2(x, y); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return c2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return c2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return c2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+// a*b + c
+__device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {
+  return c2(fmaf(a.x, b.x, fmaf(-a.y, b.y, c.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, c.y)));
+}
+// c - a*b
+__device__ __forceinline__ float2 cfnma(float2 a, float2 b, float2 c) {
+  return c2(fmaf(-a.x, b.x, fmaf(a.y, b.y, c.x)), fmaf(-a.x, b.y, fmaf(-a.y, b.x, c.y)));
+}
+// a * conj(b)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+  return c2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+__device__ __forceinline__ float2 shfl_up2(float2 v, int d) {
+  return c2(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d));
+}
+__device__ __forceinline__ float2 shfl_down2(float2 v, int d) {
+  return c2(__shfl_down_sync(0xffffffffu, v.x, d), __shfl_down_sync(0xffffffffu, v.y, d));
+}
+
+// ---------------------------------------------------------------- complex128
+__host__ __device__ __forceinline__ double2 z2(double x, double y) { return make_double2(x, y); }
+__host__ __device__ __forceinline__ double2 zadd(double2 a, double2 b) { return z2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 zsub(double2 a, double2 b) { return z2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+  return z2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 zconj(double2 a) { return z2(a.x, -a.y); }
+__host__ __device__ __forceinline__ double2 zneg(double2 a) { return z2(-a.x, -a.y); }
+__host__ __device__ __forceinline__ double2 zscale(double2 a, double s) { return z2(a.x * s, a.y * s); }
+// a / b by Smith's scaling (avoids overflow of |b|^2 for extreme values)
+__host__ __device__ __forceinline__ double2 zdiv(double2 a, double2 b) {
+  if (fabs(b.x) >= fabs(b.y)) {
+    double r = b.y / b.x, d = b.x + b.y * r;
+    return z2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+  }
+  double r = b.x / b.y, d = b.x * r + b.y;
+  return z2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+}
+__device__ __forceinline__ float2 to_f2(double2 a) { return make_float2((float)a.x, (float)a.y); }
+__device__ __forceinline__ double2 shfl_up_z(double2 v, int d) {
+  return z2(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d));
+}
+__device__ __forceinline__ double2 shfl_down_z(double2 v, int d) {
+  return z2(__shfl_down_sync(0xffffffffu, v.x, d), __shfl_down_sync(0xffffffffu, v.y, d));
+}
+
+// ------------------------------------------------- bulk copy (TMA) + mbarrier
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+// Global -> shared bulk copy completing on `bar`.  dst, src 16-byte aligned,
+// bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: returns false (and records kDevMbarTimeout) after `max_iter`
+// polls.  Each try_wait already suspends the thread for a hardware-chosen
+// interval, so 1<<22 polls is far beyond any bulk copy's latency.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err,
+                                                  uint32_t max_iter = 1u << 22) {
+  for (uint32_t it = 0; it < max_iter; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  if (err) atomicExch(err, (int)kDevMbarTimeout);
+  return false;
+}
+
+}  // namespace tp
