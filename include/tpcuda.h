@@ -145,6 +145,22 @@ TP_API int tp_cn2d_grad_to_n(const tp_cn2d_op *op, const void *grad_c, const voi
 TP_API int tp_cn2d_unchunk(const tp_cn2d_op *op, int32_t num_probes, const void *u_store, void *u_out,
                     tp_stream_t stream);
 
+/*
+ * tp_cn2d_factor + tp_cn2d_march in one call that allocates nothing: the
+ * factor set lives in a 32 MiB file-scope device array instead of a caller
+ * workspace.  This entry point has no counterpart in the reference.  It is
+ * for callers that cannot allocate device memory: a host that owns the whole
+ * device budget as a pre-reserved pool and passes only input and output
+ * buffers, or a latency-bounded loop where cudaMalloc (which may synchronise
+ * the device) is not allowed.  Problems whose tp_cn2d_factor_bytes exceeds
+ * 32 MiB return TP_ERR_WORKSPACE.  Every GPU that loads the library holds the
+ * array until exit; calls share it, so calls that overlap on the GPU race.
+ * The first call on a device resolves the array's address
+ * (cudaGetSymbolAddress) and should come before any stream capture.
+ */
+TP_API int tp_cn2d_march_noalloc(const tp_cn2d_op *op, const void *n_field, int32_t n_dtype,
+                                 const tp_cn2d_march_args *args, tp_stream_t stream);
+
 /* Synchronise `stream` and report device-side failures of earlier launches
  * (a bounded wait that gave up).  Returns TP_ERR_TIMEOUT and clears the flag
  * when one was recorded; *code receives the raw device code (0 = none). */

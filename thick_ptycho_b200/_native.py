@@ -81,6 +81,8 @@ SIGNATURES = [
                                          ctypes.c_void_p, ctypes.c_void_p]),
     ("tp_cn2d_unchunk", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.c_void_p]),
+    ("tp_cn2d_march_noalloc", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_void_p, ctypes.c_int32,
+                                             ctypes.POINTER(TpCn2dMarchArgs), ctypes.c_void_p]),
     ("tp_device_status", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ("tp_last_error_string", ctypes.c_char_p, []),
     ("tp_version", ctypes.c_int, []),
