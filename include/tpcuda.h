@@ -96,7 +96,7 @@ typedef struct tp_cn2d_march_args {
   const void *src_exit;      /* float2 (P, N) source applied at the first step
                                 only (exit-wave error for the adjoints), or NULL */
   void *u_store;             /* float2 (P, nz, Npad) full field in the chunked
-                                layout (see tp_cn2d_chunked_rows), or NULL    */
+                                layout (see tp_cn2d_layout), or NULL    */
   void *exit_out;            /* float2 (P, N) last-step field, or NULL        */
   const void *u_fwd;         /* ADJOINT_EXACT + gradient: forward full field
                                 (chunked, as written by a FORWARD march)      */
@@ -107,8 +107,10 @@ typedef struct tp_cn2d_march_args {
   int32_t reserved;
 } tp_cn2d_march_args;
 
-/* Rows per lane M and padded row count Npad = 32*M used for N. */
-TP_API int tp_cn2d_rows_per_lane(int32_t n, int32_t *rows_per_lane, int32_t *npad);
+/* Partition of N rows into `chunks` chunks of `rows_per_chunk` rows (padded
+ * row count Npad = chunks * rows_per_chunk).  Chunked full fields store row
+ * k*rows_per_chunk + i of a slice at offset i*chunks + k. */
+TP_API int tp_cn2d_layout(int32_t n, int32_t *chunks, int32_t *rows_per_chunk, int32_t *npad);
 
 /* Bytes of the per-slice factor workspace for (N, nz). */
 TP_API size_t tp_cn2d_factor_bytes(int32_t n, int32_t nz);

@@ -262,6 +262,25 @@ def exact_adjoint(A, B, C2d, src):
     return lam
 
 
+def exact_adjoint_many(A, B, C2d, srcs):
+    """``exact_adjoint`` for several sources sharing one factorisation per slice.
+
+    ``srcs`` has shape (K, N, L); returns λ of the same shape.
+    """
+    K, N, L = srcs.shape
+    lam = np.zeros_like(srcs, dtype=complex)
+    nxt = np.zeros((N, K), dtype=complex)
+    for j in range(L, 0, -1):
+        rhs = srcs[:, :, j - 1].T.copy()
+        if j < L:
+            Rn = (B + sp.diags(C2d[:, j])).conj().T
+            rhs = rhs + Rn @ nxt
+        lu = spla.splu((A - sp.diags(C2d[:, j - 1])).conj().T.tocsc())
+        nxt = lu.solve(rhs)
+        lam[:, :, j - 1] = nxt.T
+    return lam
+
+
 def grad_c_from_adjoint(u, lam):
     """Torch-convention gradient w.r.t. each step coefficient c_j.
 

@@ -37,14 +37,18 @@ def test_library_exports_every_declared_symbol():
 
 def test_pure_host_queries():
     lib = _native.load()
-    m, npad = ctypes.c_int32(), ctypes.c_int32()
-    assert lib.tp_cn2d_rows_per_lane(2048, ctypes.byref(m), ctypes.byref(npad)) == 0
-    assert (m.value, npad.value) == (64, 2048)
-    assert lib.tp_cn2d_rows_per_lane(257, ctypes.byref(m), ctypes.byref(npad)) == 0
+    c, m, npad = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    args = (ctypes.byref(c), ctypes.byref(m), ctypes.byref(npad))
+    assert lib.tp_cn2d_layout(2048, *args) == 0
+    assert (c.value, m.value, npad.value) == (128, 16, 2048)          # team path
+    assert lib.tp_cn2d_layout(256, *args) == 0
+    assert (c.value, m.value, npad.value) == (32, 8, 256)             # warp path
+    assert lib.tp_cn2d_layout(257, *args) == 0
     assert npad.value >= 257 and npad.value == 32 * m.value
-    assert lib.tp_cn2d_rows_per_lane(4097, ctypes.byref(m), ctypes.byref(npad)) != 0
+    assert lib.tp_cn2d_layout(4097, *args) != 0
     assert b"4097" in lib.tp_last_error_string()
-    assert lib.tp_cn2d_factor_bytes(2048, 1024) == 1023 * 85248
+    # team slice: (5*16 + 17) * 128 * 8 bytes
+    assert lib.tp_cn2d_factor_bytes(2048, 1024) == 1023 * (5 * 16 + 17) * 128 * 8
     assert lib.tp_cn2d_factor_bytes(2048, 1) == 0
 
 

@@ -1,0 +1,99 @@
+"""GPU parity of the team path (N in {512, 1024, 2048}: 128 chunks, several
+probes per thread) against the complex128 oracle: every boundary condition
+and mode, groups of 1 and 4 probes per CTA with a partial last group, and
+the fused exact-adjoint gradient summed over hundreds of probes.
+
+Tolerances as in the other GPU tests: relative L2 ≤ 1e-5 for fields, ≤ 1e-4
+for the fp32-summed gradient.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import pwe_oracle as po
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from thick_ptycho_b200.cn2d import CN2D  # noqa: E402
+
+TOL = 1e-5
+GRAD_TOL = 1e-4
+K, DX, DZ = 4 * np.pi, 1.0, 1.0
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _field(N, nz, seed):
+    rng = np.random.default_rng(seed)
+    return 1 + 1e-3 * (rng.standard_normal((N, nz)) + 0.1j * rng.standard_normal((N, nz)))
+
+
+def _probes(N, P, seed):
+    rng = np.random.default_rng(seed)
+    x = np.arange(N)[None]
+    c = rng.uniform(0.1 * N, 0.9 * N, (P, 1))
+    return (np.exp(-((x - c) ** 2) / 64.0) * np.exp(1j * rng.uniform(0, 6.28, (P, 1)))).astype(complex)
+
+
+@pytest.mark.parametrize("bc", ["neumann", "impedance", "dirichlet", "impedance2"])
+def test_team_modes_against_oracle(bc):
+    N, nz, P = 512, 33, 3
+    n = _field(N, nz, 1)
+    probes = _probes(N, P, 2)
+    eng = CN2D(N, nz, K, DX, DZ, bc)
+    assert eng.chunks == 128
+    co = po.bc_coefficients(K, DX, DZ, bc_type=bc)
+    A, B = po.step_matrices_1d(N, co, bc, DZ)
+    C = po.object_contribution(n, K, DZ)
+    field = torch.from_numpy(n).cuda()
+    pr = torch.from_numpy(probes.astype(np.complex64)).cuda()
+    rng = np.random.default_rng(3)
+    rhs = rng.standard_normal((P, N, nz - 1)) + 1j * rng.standard_normal((P, N, nz - 1))
+    src = torch.from_numpy(np.ascontiguousarray(rhs.transpose(0, 2, 1)).astype(np.complex64)).cuda()
+    for mode, use_probe, use_src in (("forward", True, False), ("forward", True, True), ("adjoint", False, True),
+                                     ("reverse", True, False), ("adjoint", True, False)):
+        fs = eng.factor(field, mode)
+        st = eng.new_store(P)
+        eng.march(fs, P, probes=pr if use_probe else None, src_probe=src if use_src else None, u_store=st)
+        eng.device_status()
+        got = eng.unchunk(st).cpu().numpy()
+        for p in range(P):
+            ref = po.march(A, B, C, probes[p] if use_probe else None, mode, rhs_block=rhs[p] if use_src else None)
+            assert rel(got[p], ref) < TOL, (bc, mode, p, rel(got[p], ref))
+
+
+def test_team_groups_of_four_with_partial_group_and_gradient():
+    N, nz, P = 1024, 24, 457  # 115 CTAs of 4 probes, the last one partial
+    n = _field(N, nz, 5)
+    probes = _probes(N, P, 6)
+    eng = CN2D(N, nz, K, DX, DZ, "impedance")
+    co = po.bc_coefficients(K, DX, DZ, bc_type="impedance")
+    A, B = po.step_matrices_1d(N, co, "impedance", DZ)
+    C = po.object_contribution(n, K, DZ)
+    field = torch.from_numpy(n).cuda()
+    pr = torch.from_numpy(probes.astype(np.complex64)).cuda()
+    st = eng.new_store(P)
+    ex = torch.empty((P, N), dtype=torch.complex64, device="cuda")
+    eng.march(eng.factor(field, "forward"), P, probes=pr, u_store=st, exit_out=ex)
+    # exit-wave source for the adjoint: a fixed random field per probe
+    rng = np.random.default_rng(7)
+    e = (rng.standard_normal((P, N)) + 1j * rng.standard_normal((P, N))).astype(np.complex64)
+    gc = torch.zeros((nz - 1, N), dtype=torch.complex64, device="cuda")
+    eng.march(eng.factor(field, "adjoint_exact"), P, src_exit=torch.from_numpy(e).cuda(), u_fwd=st, grad_c=gc)
+    eng.device_status()
+    lus, Bs = po.build_lu_factors(A, B, C)
+    u_ref = np.array([po.march_with_lu(lus, Bs, np.zeros(N, complex), probes[p]) for p in range(P)])
+    assert rel(ex.cpu().numpy(), u_ref[:, :, -1]) < TOL
+    assert rel(eng.unchunk(st).cpu().numpy()[[0, 228, 456]], u_ref[[0, 228, 456]]) < TOL
+    srcs = np.zeros((P, N, nz - 1), dtype=complex)
+    srcs[:, :, -1] = e
+    lam = po.exact_adjoint_many(A, B, C, srcs)
+    gref = sum(po.grad_c_from_adjoint(u_ref[p], lam[p]) for p in range(P))
+    assert rel(gc.cpu().numpy().T, gref) < GRAD_TOL, rel(gc.cpu().numpy().T, gref)

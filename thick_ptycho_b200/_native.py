@@ -71,7 +71,8 @@ class TpCn2dMarchArgs(ctypes.Structure):
 
 # (name, restype, argtypes) of every exported symbol of include/tpcuda.h
 SIGNATURES = [
-    ("tp_cn2d_rows_per_lane", ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
+    ("tp_cn2d_layout", ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                      ctypes.POINTER(ctypes.c_int32)]),
     ("tp_cn2d_factor_bytes", ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
     ("tp_cn2d_factor", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                       ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),

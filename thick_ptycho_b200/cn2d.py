@@ -52,10 +52,10 @@ class CN2D:
         self.exact_ref_coeff = bool(exact_ref_coeff)
         co = BCCoefficients.make(self.k, self.dx, self.dz, self.bc_type)
         self.kop = operator_1d(self.n, co, self.bc_type, self.dz)
-        m = ctypes.c_int32()
-        npad = ctypes.c_int32()
-        _native.check(self.lib.tp_cn2d_rows_per_lane(self.n, ctypes.byref(m), ctypes.byref(npad)), "tp_cn2d_rows_per_lane")
-        self.rows_per_lane, self.npad = m.value, npad.value
+        c, m, npad = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        rc = self.lib.tp_cn2d_layout(self.n, ctypes.byref(c), ctypes.byref(m), ctypes.byref(npad))
+        _native.check(rc, "tp_cn2d_layout")
+        self.chunks, self.rows_per_chunk, self.npad = c.value, m.value, npad.value
         self.factor_bytes = int(self.lib.tp_cn2d_factor_bytes(self.n, self.nz))
 
     # ------------------------------------------------------------------ op

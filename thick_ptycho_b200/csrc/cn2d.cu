@@ -40,25 +40,19 @@
 #include <cuda_runtime.h>
 #include <stdio.h>
 
+#include "cn2d_internal.cuh"
 #include "tp_common.cuh"
 #include "tp_errors.h"
 #include "tpcuda.h"
 
 namespace tp {
 
-constexpr int kLaneRecs = 13;
+// Warp path: 32 chunks (one per lane), 5 PCR levels, 13 records per chunk.
 constexpr int kRecMA = 0, kRecMC = 1, kRecAlpha = 2, kRecGamma = 7, kRecRDE = 12;
 constexpr int kMarchWarps = 4;
-constexpr int kMaxRowsPerLane = 64;
-constexpr int kFactorWarps = 4;
 
-// Rows-per-lane values with compiled kernels.
+// Rows-per-lane values of the warp path with compiled kernels.
 static const int kRowSet[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64};
-
-__host__ __device__ inline size_t cn2d_slice_bytes(int M) {
-  size_t b = (size_t)(5 * M + kLaneRecs) * kLanes * sizeof(float2);
-  return (b + 255) & ~size_t(255);
-}
 
 static int rows_per_lane_for(int n) {
   int need = (n + kLanes - 1) / kLanes;
@@ -67,19 +61,43 @@ static int rows_per_lane_for(int n) {
   return -1;
 }
 
+int partition_for(int n, Partition *pt) {
+  if (n == 512 || n == 1024 || n == 2048) {
+    pt->C = kTeamChunks;
+    pt->M = n / kTeamChunks;
+    pt->team = 1;
+    pt->levels = 7;
+  } else {
+    const int m = rows_per_lane_for(n);
+    if (n < 4 || m < 0)
+      return set_error(TP_ERR_UNSUPPORTED, "N=%d unsupported (4 <= N <= %d)", n, kWarpChunks * kMaxRowsPerLane);
+    pt->C = kWarpChunks;
+    pt->M = m;
+    pt->team = 0;
+    pt->levels = 5;
+  }
+  pt->nrec = 3 + 2 * pt->levels;
+  return TP_OK;
+}
+
+int team_spike_rows(const tp_cn2d_op *op, int M) {
+  const double b = hypot(op->k_off[0], op->k_off[1]);
+  const double d0 = hypot(1.0 - op->k_diag[0], op->k_diag[1]);
+  if (b == 0.0) return 1;
+  const double disc = d0 * d0 - 4.0 * b * b;
+  if (disc <= 0.0) return M - 1;
+  const double rho = (d0 - sqrt(disc)) / (2.0 * b);
+  if (!(rho > 0.0) || rho >= 0.5) return M - 1;
+  int t = (int)ceil(log(1e-10) / log(rho)) + 2;
+  if (t < 1) t = 1;
+  if (t > M - 1) t = M - 1;
+  return t;
+}
+
 // --------------------------------------------------------------------------
 // Factorisation (fp64)
 // --------------------------------------------------------------------------
-struct FactorParams {
-  int N, L, M, nz, n_obj, empty_px, exact, is_delta, dtype;
-  double sigma;
-  int conj_t;
-  double k, dz;
-  double2 k_off, k_diag, k_d0, k_dn, k_01, k_nm;
-  const void *n;
-  char *factors;
-  size_t slice_bytes;
-};
+
 
 __device__ __forceinline__ double2 load_n(const FactorParams &f, int row, int col) {
   size_t idx = (size_t)row * f.nz + col;
@@ -127,24 +145,24 @@ __device__ __forceinline__ double2 p_sup(const FactorParams &f, int g) {  // P[g
   return zscale(v, f.sigma);
 }
 
-// One warp per slice, one lane per chunk.
-__global__ void __launch_bounds__(kFactorWarps * 32) cn2d_factor_kernel(const FactorParams f) {
-  const int lane = threadIdx.x & 31;
-  const int sl = blockIdx.x * kFactorWarps + (threadIdx.x >> 5);
-  if (sl >= f.L) return;  // warp-uniform
-  const int M = f.M;
+// One block of C threads per slice, one thread per chunk.
+__global__ void __launch_bounds__(128) cn2d_factor_kernel(const FactorParams f) {
+  extern __shared__ double2 fsm[];  // [5][C]: ra, rd, rc, v_first, w_first
+  const int c = threadIdx.x;
+  const int sl = blockIdx.x;
+  const int M = f.M, C = f.C;
   float2 *base = reinterpret_cast<float2 *>(f.factors + (size_t)sl * f.slice_bytes);
-  float2 *QD = base, *LF = base + M * 32, *EP = base + 2 * M * 32, *V = base + 3 * M * 32,
-         *W = base + 4 * M * 32, *LR = base + 5 * M * 32;
+  float2 *QD = base, *LF = base + M * C, *EP = base + 2 * M * C, *V = base + 3 * M * C, *W = base + 4 * M * C,
+         *LR = base + 5 * M * C;
 
   double2 pl[kMaxRowsPerLane], msl[kMaxRowsPerLane], fv[kMaxRowsPerLane];
-  const int g0 = lane * M;
+  const int g0 = c * M;
   double2 p_prev = z2(1, 0), msup_prev = z2(0, 0), fvv = z2(0, 0);
   double2 me_a = z2(0, 0), me_d = z2(1, 0), me_c = z2(0, 0);
   for (int i = 0; i < M; ++i) {
     const int g = g0 + i;
     const double2 pd = p_diag(f, g, sl);
-    QD[i * 32 + lane] = to_f2(pd);
+    QD[i * C + c] = to_f2(pd);
     const double2 md = z2(1.0 - pd.x, -pd.y);
     const double2 msub = zneg(p_sub(f, g));
     const double2 msup = zneg(p_sup(f, g));
@@ -159,8 +177,8 @@ __global__ void __launch_bounds__(kFactorWarps * 32) cn2d_factor_kernel(const Fa
         p = zsub(md, zmul(l, msup_prev));
         fvv = zneg(zmul(l, fvv));
       }
-      LF[i * 32 + lane] = to_f2(l);
-      EP[i * 32 + lane] = to_f2(zdiv(z2(1.0 - p.x, -p.y), p));  // 1/p - 1
+      LF[i * C + c] = to_f2(l);
+      EP[i * C + c] = to_f2(zdiv(z2(1.0 - p.x, -p.y), p));  // 1/p - 1
       pl[i] = p;
       msl[i] = msup;
       fv[i] = fvv;
@@ -170,25 +188,30 @@ __global__ void __launch_bounds__(kFactorWarps * 32) cn2d_factor_kernel(const Fa
       me_d = md;
       me_a = msub;
       me_c = msup;
-      LF[i * 32 + lane] = make_float2(0.f, 0.f);
-      EP[i * 32 + lane] = make_float2(0.f, 0.f);
-      V[i * 32 + lane] = make_float2(0.f, 0.f);
-      W[i * 32 + lane] = make_float2(0.f, 0.f);
+      LF[i * C + c] = make_float2(0.f, 0.f);
+      EP[i * C + c] = make_float2(0.f, 0.f);
+      V[i * C + c] = make_float2(0.f, 0.f);
+      W[i * C + c] = make_float2(0.f, 0.f);
     }
   }
   double2 v_last, w_last, v_first, w_first;
+  bool trunc_bad = false;
+  const double thr = 1e-9;
   if (M >= 2) {
     double2 v = zdiv(fv[M - 2], pl[M - 2]);
     double2 w = zdiv(zneg(msl[M - 2]), pl[M - 2]);
-    V[(M - 2) * 32 + lane] = to_f2(v);
-    W[(M - 2) * 32 + lane] = to_f2(w);
+    V[(M - 2) * C + c] = to_f2(v);
+    W[(M - 2) * C + c] = to_f2(w);
+    if (M - 2 >= f.trunc && hypot(v.x, v.y) > thr) trunc_bad = true;
     v_last = v;
     w_last = w;
     for (int i = M - 3; i >= 0; --i) {
       v = zdiv(zsub(fv[i], zmul(msl[i], v)), pl[i]);
       w = zdiv(zneg(zmul(msl[i], w)), pl[i]);
-      V[i * 32 + lane] = to_f2(v);
-      W[i * 32 + lane] = to_f2(w);
+      V[i * C + c] = to_f2(v);
+      W[i * C + c] = to_f2(w);
+      if (i >= f.trunc && hypot(v.x, v.y) > thr) trunc_bad = true;
+      if (i < M - 1 - f.trunc && hypot(w.x, w.y) > thr) trunc_bad = true;
     }
     v_first = v;
     w_first = w;
@@ -198,50 +221,48 @@ __global__ void __launch_bounds__(kFactorWarps * 32) cn2d_factor_kernel(const Fa
     v_first = z2(0, 0);
     w_first = z2(1, 0);
   }
-  // Reduced 32-unknown tridiagonal system on the separators.
-  const double2 vf_n = shfl_down_z(v_first, 1), wf_n = shfl_down_z(w_first, 1);
+  if (trunc_bad && f.err != nullptr) atomicOr(f.err, (int)kDevSpikeTruncation);
+  // Reduced C-unknown tridiagonal system on the separators.
+  fsm[3 * C + c] = v_first;
+  fsm[4 * C + c] = w_first;
+  __syncthreads();
+  const double2 vf_n = (c < C - 1) ? fsm[3 * C + c + 1] : z2(0, 0);
+  const double2 wf_n = (c < C - 1) ? fsm[4 * C + c + 1] : z2(0, 0);
   double2 ra = zmul(me_a, v_last);
-  double2 rd = zadd(me_d, zadd(zmul(me_a, w_last), lane < 31 ? zmul(me_c, vf_n) : z2(0, 0)));
-  double2 rc = lane < 31 ? zmul(me_c, wf_n) : z2(0, 0);
-  LR[kRecMA * 32 + lane] = to_f2(me_a);
-  LR[kRecMC * 32 + lane] = to_f2(lane < 31 ? me_c : z2(0, 0));
-  for (int l = 0; l < 5; ++l) {
+  double2 rd = zadd(me_d, zadd(zmul(me_a, w_last), c < C - 1 ? zmul(me_c, vf_n) : z2(0, 0)));
+  double2 rc = c < C - 1 ? zmul(me_c, wf_n) : z2(0, 0);
+  LR[0 * C + c] = to_f2(me_a);
+  LR[1 * C + c] = to_f2(c < C - 1 ? me_c : z2(0, 0));
+  for (int l = 0; l < f.levels; ++l) {
     const int s = 1 << l;
-    const double2 ra_m = shfl_up_z(ra, s), rd_m = shfl_up_z(rd, s), rc_m = shfl_up_z(rc, s);
-    const double2 ra_p = shfl_down_z(ra, s), rd_p = shfl_down_z(rd, s), rc_p = shfl_down_z(rc, s);
-    const double2 al = (lane >= s) ? zneg(zdiv(ra, rd_m)) : z2(0, 0);
-    const double2 ga = (lane < 32 - s) ? zneg(zdiv(rc, rd_p)) : z2(0, 0);
+    fsm[c] = ra;
+    fsm[C + c] = rd;
+    fsm[2 * C + c] = rc;
+    __syncthreads();
+    const bool hm = c >= s, hp = c + s < C;
+    const double2 ra_m = hm ? fsm[c - s] : z2(0, 0), rd_m = hm ? fsm[C + c - s] : z2(1, 0),
+                  rc_m = hm ? fsm[2 * C + c - s] : z2(0, 0);
+    const double2 ra_p = hp ? fsm[c + s] : z2(0, 0), rd_p = hp ? fsm[C + c + s] : z2(1, 0),
+                  rc_p = hp ? fsm[2 * C + c + s] : z2(0, 0);
+    __syncthreads();
+    const double2 al = hm ? zneg(zdiv(ra, rd_m)) : z2(0, 0);
+    const double2 ga = hp ? zneg(zdiv(rc, rd_p)) : z2(0, 0);
     const double2 nra = zmul(al, ra_m), nrc = zmul(ga, rc_p);
     rd = zadd(rd, zadd(zmul(al, rc_m), zmul(ga, ra_p)));
     ra = nra;
     rc = nrc;
-    LR[(kRecAlpha + l) * 32 + lane] = to_f2(al);
-    LR[(kRecGamma + l) * 32 + lane] = to_f2(ga);
+    LR[rec_alpha(f.levels, l) * C + c] = to_f2(al);
+    LR[rec_gamma(f.levels, l) * C + c] = to_f2(ga);
   }
-  LR[kRecRDE * 32 + lane] = to_f2(zdiv(z2(1.0 - rd.x, -rd.y), rd));
+  LR[rec_rde(f.levels) * C + c] = to_f2(zdiv(z2(1.0 - rd.x, -rd.y), rd));
 }
 
 // --------------------------------------------------------------------------
 // March
 // --------------------------------------------------------------------------
-struct Spec {
-  float2 p_o;                         // interior off-diagonal of P
-  float2 sup0, sub1, supN2, subN1;    // P[0,1], P[1,0], P[N-2,N-1], P[N-1,N-2]
-  float2 d_sup0, d_sub1, d_supN2, d_subN1;  // the same minus p_o
-};
 
-struct MarchParams {
-  int N, L, nz, P, Npad;
-  int backward, flip_out, src_rev;
-  size_t slice_bytes;
-  const char *factors;
-  Spec sp;
-  const float2 *probes, *src_shared, *src_probe, *src_exit;
-  float2 *u_store, *exit_out;
-  const float2 *u_fwd;
-  float2 *grad_c;
-  int *err;
-};
+
+
 
 // U <- (I + P_s) U with P's boundary-row specials.
 template <int M, bool ALIGNED>
@@ -459,14 +480,15 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
 // Layout and gradient helpers
 // --------------------------------------------------------------------------
 __global__ void cn2d_unchunk_kernel(const float2 *__restrict__ st, float2 *__restrict__ out, int P, int N, int nz,
-                                    int M, int Npad) {
+                                    int M, int C) {
+  const size_t Npad = (size_t)C * M;
   const size_t total = (size_t)P * N * nz;
   for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
     const int t = (int)(idx % nz);
     const size_t pg = idx / nz;
     const int g = (int)(pg % N);
     const size_t pp = pg / N;
-    out[idx] = st[(pp * nz + t) * Npad + (size_t)(g % M) * 32 + g / M];
+    out[idx] = st[(pp * nz + t) * Npad + (size_t)(g % M) * C + g / M];
   }
 }
 
@@ -534,9 +556,8 @@ static inline double2 hz(const double v[2]) { return make_double2(v[0], v[1]); }
 static int validate_op(const tp_cn2d_op *op) {
   if (op == nullptr) return set_error(TP_ERR_INVALID, "op is NULL");
   if (op->n < 4) return set_error(TP_ERR_INVALID, "N=%d must be >= 4", op->n);
-  if (rows_per_lane_for(op->n) < 0)
-    return set_error(TP_ERR_UNSUPPORTED, "N=%d exceeds the register-resident limit of %d rows", op->n,
-                     kLanes * kMaxRowsPerLane);
+  Partition pt;
+  if (partition_for(op->n, &pt) != TP_OK) return TP_ERR_UNSUPPORTED;
   if (op->nz < 2) return set_error(TP_ERR_INVALID, "nz=%d must be >= 2", op->nz);
   if (op->empty_px < 0 || op->n_obj != op->n - 2 * op->empty_px)
     return set_error(TP_ERR_INVALID, "n_obj=%d must equal N - 2*empty_px (N=%d, empty_px=%d)", op->n_obj, op->n,
@@ -621,18 +642,20 @@ static int launch_march(int M, const MarchParams &mp, bool aligned, bool lagged,
 
 using namespace tp;
 
-extern "C" int tp_cn2d_rows_per_lane(int32_t n, int32_t *rows_per_lane, int32_t *npad) {
-  const int m = rows_per_lane_for(n);
-  if (n < 4 || m < 0) return set_error(TP_ERR_UNSUPPORTED, "N=%d unsupported (4 <= N <= %d)", n, 32 * kMaxRowsPerLane);
-  if (rows_per_lane) *rows_per_lane = m;
-  if (npad) *npad = 32 * m;
+extern "C" int tp_cn2d_layout(int32_t n, int32_t *chunks, int32_t *rows_per_chunk, int32_t *npad) {
+  Partition pt;
+  int rc = partition_for(n, &pt);
+  if (rc) return rc;
+  if (chunks) *chunks = pt.C;
+  if (rows_per_chunk) *rows_per_chunk = pt.M;
+  if (npad) *npad = pt.C * pt.M;
   return TP_OK;
 }
 
 extern "C" size_t tp_cn2d_factor_bytes(int32_t n, int32_t nz) {
-  const int m = rows_per_lane_for(n);
-  if (m < 0 || nz < 2) return 0;
-  return cn2d_slice_bytes(m) * (size_t)(nz - 1);
+  Partition pt;
+  if (nz < 2 || partition_for(n, &pt) != TP_OK) return 0;
+  return slice_bytes(pt) * (size_t)(nz - 1);
 }
 
 extern "C" int tp_cn2d_factor(const tp_cn2d_op *op, const void *n_field, int32_t n_dtype, int32_t mode,
@@ -647,10 +670,19 @@ extern "C" int tp_cn2d_factor(const tp_cn2d_op *op, const void *n_field, int32_t
     return set_error(TP_ERR_WORKSPACE, "factor workspace %zu B < required %zu B", factors_bytes, need);
   if ((reinterpret_cast<uintptr_t>(factors) & 255u) != 0)
     return set_error(TP_ERR_INVALID, "factor workspace must be 256-byte aligned");
+  Partition pt;
+  rc = partition_for(op->n, &pt);
+  if (rc) return rc;
+  int *err = device_error_ptr();
+  if (err == nullptr) return set_error(TP_ERR_CUDA, "cannot resolve the device error word");
   FactorParams f{};
   f.N = op->n;
   f.L = op->nz - 1;
-  f.M = rows_per_lane_for(op->n);
+  f.C = pt.C;
+  f.M = pt.M;
+  f.levels = pt.levels;
+  f.nrec = pt.nrec;
+  f.trunc = pt.team ? team_spike_rows(op, pt.M) : pt.M - 1;
   f.nz = op->nz;
   f.n_obj = op->n_obj;
   f.empty_px = op->empty_px;
@@ -668,9 +700,10 @@ extern "C" int tp_cn2d_factor(const tp_cn2d_op *op, const void *n_field, int32_t
   f.k_nm = hz(op->k_nm);
   f.n = n_field;
   f.factors = static_cast<char *>(factors);
-  f.slice_bytes = cn2d_slice_bytes(f.M);
-  const int grid = (f.L + kFactorWarps - 1) / kFactorWarps;
-  cn2d_factor_kernel<<<grid, kFactorWarps * 32, 0, reinterpret_cast<cudaStream_t>(stream)>>>(f);
+  f.slice_bytes = slice_bytes(pt);
+  f.err = err;
+  const size_t smem = 5 * (size_t)pt.C * sizeof(double2);
+  cn2d_factor_kernel<<<f.L, pt.C, smem, reinterpret_cast<cudaStream_t>(stream)>>>(f);
   return check_cuda(cudaGetLastError(), "cn2d_factor_kernel launch");
 }
 
@@ -689,19 +722,22 @@ extern "C" int tp_cn2d_march(const tp_cn2d_op *op, const void *factors, const tp
     return set_error(TP_ERR_INVALID, "grad_c and u_fwd must be given together");
   if (a->grad_c != nullptr && !lagged)
     return set_error(TP_ERR_INVALID, "the fused gradient needs mode TP_MODE_ADJOINT_EXACT");
+  Partition pt;
+  rc = partition_for(op->n, &pt);
+  if (rc) return rc;
   int *err = device_error_ptr();
   if (err == nullptr) return set_error(TP_ERR_CUDA, "cannot resolve the device error word");
   MarchParams mp{};
-  const int M = rows_per_lane_for(op->n);
   mp.N = op->n;
   mp.L = op->nz - 1;
   mp.nz = op->nz;
   mp.P = a->num_probes;
-  mp.Npad = 32 * M;
+  mp.Npad = pt.C * pt.M;
   mp.backward = (a->mode != TP_MODE_FORWARD) ? 1 : 0;
   mp.flip_out = (a->mode == TP_MODE_ADJOINT) ? 1 : 0;
   mp.src_rev = (a->mode == TP_MODE_ADJOINT || a->mode == TP_MODE_ADJOINT_EXACT) ? 1 : 0;
-  mp.slice_bytes = cn2d_slice_bytes(M);
+  mp.trunc = pt.team ? team_spike_rows(op, pt.M) : pt.M - 1;
+  mp.slice_bytes = slice_bytes(pt);
   mp.factors = static_cast<const char *>(factors);
   mp.sp = make_spec(op, a->mode);
   mp.probes = static_cast<const float2 *>(a->probes);
@@ -713,7 +749,8 @@ extern "C" int tp_cn2d_march(const tp_cn2d_op *op, const void *factors, const tp
   mp.u_fwd = static_cast<const float2 *>(a->u_fwd);
   mp.grad_c = static_cast<float2 *>(a->grad_c);
   mp.err = err;
-  return launch_march(M, mp, op->n == 32 * M, lagged, reinterpret_cast<cudaStream_t>(stream));
+  if (pt.team) return launch_team_march(pt, mp, lagged, reinterpret_cast<cudaStream_t>(stream));
+  return launch_march(pt.M, mp, op->n == pt.C * pt.M, lagged, reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" int tp_cn2d_unchunk(const tp_cn2d_op *op, int32_t num_probes, const void *u_store, void *u_out,
@@ -721,9 +758,11 @@ extern "C" int tp_cn2d_unchunk(const tp_cn2d_op *op, int32_t num_probes, const v
   int rc = validate_op(op);
   if (rc) return rc;
   if (u_store == nullptr || u_out == nullptr || num_probes < 1) return set_error(TP_ERR_INVALID, "bad unchunk args");
-  const int M = rows_per_lane_for(op->n);
+  Partition pt;
+  rc = partition_for(op->n, &pt);
+  if (rc) return rc;
   cn2d_unchunk_kernel<<<1184, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-      static_cast<const float2 *>(u_store), static_cast<float2 *>(u_out), num_probes, op->n, op->nz, M, 32 * M);
+      static_cast<const float2 *>(u_store), static_cast<float2 *>(u_out), num_probes, op->n, op->nz, pt.M, pt.C);
   return check_cuda(cudaGetLastError(), "cn2d_unchunk_kernel launch");
 }
 
@@ -761,6 +800,10 @@ extern "C" int tp_device_status(tp_stream_t stream, int32_t *code) {
   if (h != 0) {
     const int zero = 0;
     TP_CHECK_CUDA(cudaMemcpy(err, &zero, sizeof(int), cudaMemcpyHostToDevice));
+    if (h & kDevSpikeTruncation)
+      return set_error(TP_ERR_UNSUPPORTED,
+                       "the factorised matrices have slowly decaying spikes beyond the kept rows (code %d): "
+                       "results of the team path are inaccurate for this operator", h);
     return set_error(TP_ERR_TIMEOUT, "a device-side bounded wait timed out (code %d)", h);
   }
   return TP_OK;

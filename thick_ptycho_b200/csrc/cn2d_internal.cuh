@@ -1,0 +1,92 @@
+// Internal declarations shared by the 2D Crank–Nicolson translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "tp_common.cuh"
+#include "tpcuda.h"
+
+namespace tp {
+
+// The matrix rows are cut into C chunks of M rows (N_pad = C*M); chunk k's
+// row i is matrix row k*M + i.  Two kernel families:
+//   warp path  (C = 32):  one warp per probe, any 4 <= N <= 2048;
+//   team path  (C = 128): a 4-warp CTA per group of Q probes, N in {512, 1024, 2048}.
+constexpr int kWarpChunks = 32;
+constexpr int kTeamChunks = 128;
+constexpr int kMaxRowsPerLane = 64;
+
+struct Partition {
+  int C;      // chunks
+  int M;      // rows per chunk
+  int team;   // 1 = team path
+  int levels; // log2(C): PCR levels of the reduced system
+  int nrec;   // per-chunk reduced-system records: MA, MC, alpha[levels], gamma[levels], RDE
+};
+
+__host__ __device__ inline int rec_alpha(int levels, int l) { return 2 + l; }
+__host__ __device__ inline int rec_gamma(int levels, int l) { return 2 + levels + l; }
+__host__ __device__ inline int rec_rde(int levels) { return 2 + 2 * levels; }
+
+// Global factor set of one slice: QD, LF, EP, V, W ([M][C] float2 each) then
+// the records ([nrec][C] float2), padded to 256 bytes.
+__host__ __device__ inline size_t slice_bytes(const Partition &pt) {
+  size_t b = (size_t)(5 * pt.M + pt.nrec) * pt.C * sizeof(float2);
+  return (b + 255) & ~size_t(255);
+}
+
+int partition_for(int n, Partition *pt);  // TP_OK or an error code
+
+// Device error codes (bit flags) recorded instead of trapping.
+enum DeviceErrorBits : int { kDevSpikeTruncation = 2 };
+
+struct FactorParams {
+  int N, L, nz, n_obj, empty_px, exact, is_delta, dtype;
+  int C, M, levels, nrec;
+  int trunc;  // spike rows the march keeps (V rows [0,T), W rows [M-1-T, M-1))
+  double sigma;
+  int conj_t;
+  double k, dz;
+  double2 k_off, k_diag, k_d0, k_dn, k_01, k_nm;
+  const void *n;
+  char *factors;
+  size_t slice_bytes;
+  int *err;
+};
+
+// P's off-diagonals: interior value and the four boundary entries (+ deltas).
+struct Spec {
+  float2 p_o;
+  float2 sup0, sub1, supN2, subN1;
+  float2 d_sup0, d_sub1, d_supN2, d_subN1;
+};
+
+struct MarchParams {
+  int N, L, nz, P, Npad;
+  int backward, flip_out, src_rev;
+  int trunc;                 // team path: spike rows kept in shared memory
+  size_t slice_bytes;        // global factor-set stride
+  size_t smem_slice_bytes;   // team path: shared-memory slice size
+  const char *factors;
+  Spec sp;
+  const float2 *probes, *src_shared, *src_probe, *src_exit;
+  float2 *u_store, *exit_out;
+  const float2 *u_fwd;
+  float2 *grad_c;
+  int *err;
+};
+
+// Spike rows kept by the team path for operator `op` with M rows per chunk:
+// the inverse of a diagonally dominant tridiagonal matrix decays like rho^d,
+// rho = (d0 - sqrt(d0^2 - 4 b^2)) / (2 b) with b the off-diagonal and d0 the
+// diagonal magnitude of the free-space matrix; keep rows until rho^T < 1e-10
+// (plus two).  The factor kernel verifies the choice on the actual matrices.
+int team_spike_rows(const tp_cn2d_op *op, int M);
+
+// Team-path launcher (cn2d_team.cu).
+int launch_team_march(const Partition &pt, MarchParams &mp, bool lagged, cudaStream_t st);
+size_t team_smem_bytes(const Partition &pt, int trunc, int Q, bool grad);
+
+}  // namespace tp

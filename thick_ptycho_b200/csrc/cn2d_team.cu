@@ -1,0 +1,362 @@
+// Team path of the 2D Crank–Nicolson march: N in {512, 1024, 2048}.
+//
+// One CTA of 4 warps (128 threads) marches a group of Q probes.  Thread c
+// owns chunk c (M = N/128 consecutive rows) of every probe of the group, so
+// each factor value read from shared memory serves Q probes and the Q
+// recurrences of a thread are independent (instruction-level parallelism
+// where the warp path has one dependent chain).  The 128 separators of each
+// probe form a tridiagonal system solved by 7 levels of parallel cyclic
+// reduction through shared memory.  Only the first and last T rows of the
+// spike vectors are staged (they decay geometrically; T is chosen from the
+// operator and verified when factorising).
+//
+// Exact-adjoint gradient: the Q probes' contributions lambda*conj(u_s+u_{s-1})
+// are summed in registers, stored once per CTA in shared memory and flushed
+// with one vector atomic per row, so no shared-memory atomics are needed.
+#include "cn2d_internal.cuh"
+#include "tp_errors.h"
+
+namespace tp {
+
+constexpr int kTeamThreads = kTeamChunks;  // one thread per chunk
+constexpr int kTeamLevels = 7;
+
+__host__ __device__ inline size_t team_slice_smem(int M, int T) {
+  return (size_t)(3 * M + 2 * T + 3 + 2 * kTeamLevels) * kTeamChunks * sizeof(float2);
+}
+
+size_t team_smem_bytes(const Partition &pt, int trunc, int Q, bool grad) {
+  return 2 * team_slice_smem(pt.M, trunc) + 6 * (size_t)Q * kTeamChunks * sizeof(float2) +
+         (grad ? (size_t)pt.M * (kTeamChunks + 1) * sizeof(float2) : 0) + 2 * sizeof(uint64_t);
+}
+
+// Issue the bulk copies of one slice's factor set (QD|LF|EP, V head, W tail, records).
+__device__ __forceinline__ void team_issue(float2 *dst, const char *slice, int M, int T, uint64_t *bar) {
+  constexpr int C = kTeamChunks;
+  const uint32_t row = C * sizeof(float2);
+  const uint32_t b_main = 3 * M * row, b_sp = T * row, b_rec = (3 + 2 * kTeamLevels) * row;
+  mbar_arrive_expect_tx(bar, b_main + 2 * b_sp + b_rec);
+  char *d = reinterpret_cast<char *>(dst);
+  bulk_g2s(d, slice, b_main, bar);
+  bulk_g2s(d + b_main, slice + (size_t)3 * M * row, b_sp, bar);
+  bulk_g2s(d + b_main + b_sp, slice + (size_t)(4 * M + (M - 1 - T)) * row, b_sp, bar);
+  bulk_g2s(d + b_main + 2 * b_sp, slice + (size_t)5 * M * row, b_rec, bar);
+}
+
+// U <- (I + P_s) U for the Q probes (boundary rows: chunk 0 rows 0,1 and
+// chunk C-1 rows M-2, M-1).
+template <int M, int Q>
+__device__ __forceinline__ void team_rhs(float2 (&U)[Q][M], const float2 *__restrict__ QD, float2 *XL, float2 *XF,
+                                         int c, const Spec &sp) {
+  constexpr int C = kTeamChunks;
+  const float2 zero = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    XL[q * C + c] = U[q][M - 1];
+    XF[q * C + c] = U[q][0];
+  }
+  __syncthreads();
+  float2 prev[Q], right[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    prev[q] = (c > 0) ? XL[q * C + c - 1] : zero;
+    right[q] = (c < C - 1) ? XF[q * C + c + 1] : zero;
+  }
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+    const float2 qd = QD[i * C + c];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const float2 cur = U[q][i];
+      const float2 nxt = (i < M - 1) ? U[q][(i + 1) < M ? i + 1 : i] : right[q];
+      float2 r = cfma(qd, cur, cur);
+      r = cfma(sp.p_o, cadd(prev[q], nxt), r);
+      if (i == 0 && c == 0) r = cfma(sp.d_sup0, nxt, r);
+      if (i == 1 && c == 0) r = cfma(sp.d_sub1, prev[q], r);
+      if (i == M - 2 && c == C - 1) r = cfma(sp.d_supN2, nxt, r);
+      if (i == M - 1 && c == C - 1) r = cfma(sp.d_subN1, prev[q], r);
+      prev[q] = cur;
+      U[q][i] = r;
+    }
+  }
+}
+
+// U <- M_s^{-1} U with the staged factor slice F.
+template <int M, int Q>
+__device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__restrict__ F, int T, float2 *Y0,
+                                           float2 *R0, float2 *R1, float2 *XS, int c, const Spec &sp) {
+  constexpr int C = kTeamChunks;
+  const float2 zero = make_float2(0.f, 0.f);
+  const float2 *LF = F + M * C, *EP = F + 2 * M * C, *VH = F + 3 * M * C, *WT = VH + T * C, *LR = WT + T * C;
+#pragma unroll
+  for (int i = 1; i <= M - 2; ++i) {
+    const float2 lf = LF[i * C + c];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) U[q][i] = cfnma(lf, U[q][i - 1], U[q][i]);
+  }
+  {
+    const float2 ep = EP[(M - 2) * C + c];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const float2 t = U[q][M - 2];
+      U[q][M - 2] = cfma(t, ep, t);
+    }
+  }
+#pragma unroll
+  for (int i = M - 3; i >= 0; --i) {
+    const float2 ep = EP[i * C + c];
+    const float2 msup = (i == 0 && c == 0) ? make_float2(-sp.sup0.x, -sp.sup0.y) : make_float2(-sp.p_o.x, -sp.p_o.y);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const float2 t = cfnma(msup, U[q][i + 1], U[q][i]);
+      U[q][i] = cfma(t, ep, t);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < Q; ++q) Y0[q * C + c] = U[q][0];
+  __syncthreads();
+  float2 rho[Q];
+  {
+    const float2 ma = LR[0 * C + c], mc = LR[1 * C + c];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const float2 y0n = (c < C - 1) ? Y0[q * C + c + 1] : zero;
+      rho[q] = cfnma(mc, y0n, cfnma(ma, U[q][M - 2], U[q][M - 1]));
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < kTeamLevels; ++l) {
+    const int s = 1 << l;
+    float2 *Rb = (l & 1) ? R1 : R0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) Rb[q * C + c] = rho[q];
+    __syncthreads();
+    const float2 al = LR[(2 + l) * C + c], ga = LR[(2 + kTeamLevels + l) * C + c];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const float2 up = (c >= s) ? Rb[q * C + c - s] : zero;
+      const float2 dn = (c + s < C) ? Rb[q * C + c + s] : zero;
+      rho[q] = cfma(ga, dn, cfma(al, up, rho[q]));
+    }
+  }
+  float2 x[Q], xp[Q];
+  {
+    const float2 rde = LR[(2 + 2 * kTeamLevels) * C + c];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      x[q] = cfma(rho[q], rde, rho[q]);
+      XS[q * C + c] = x[q];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < Q; ++q) xp[q] = (c > 0) ? XS[q * C + c - 1] : zero;
+  const int wlo = M - 1 - T;
+#pragma unroll
+  for (int i = 0; i <= M - 2; ++i) {
+    if (i < T) {
+      const float2 v = VH[i * C + c];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) U[q][i] = cfma(v, xp[q], U[q][i]);
+    }
+    if (i >= wlo) {
+      const float2 w = WT[(i - wlo) * C + c];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) U[q][i] = cfma(w, x[q], U[q][i]);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < Q; ++q) U[q][M - 1] = x[q];
+}
+
+template <int M, int Q, bool LAGGED>
+__global__ void __launch_bounds__(kTeamThreads, 1) cn2d_team_kernel(const MarchParams p) {
+  constexpr int C = kTeamChunks;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int c = threadIdx.x;
+  const int T = p.trunc;
+  const size_t ss = p.smem_slice_bytes;
+  float2 *bufs = reinterpret_cast<float2 *>(smem);
+  float2 *XL = reinterpret_cast<float2 *>(smem + 2 * ss);
+  float2 *XF = XL + Q * C, *Y0 = XF + Q * C, *R0 = Y0 + Q * C, *R1 = R0 + Q * C, *XS = R1 + Q * C;
+  const bool do_grad = LAGGED && (p.grad_c != nullptr);
+  float2 *GB = XS + Q * C;  // [M][C+1], only with the gradient
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(GB + (do_grad ? M * (C + 1) : 0));
+  const size_t ssf = ss / sizeof(float2);
+  const int p0 = blockIdx.x * Q;
+
+  if (c == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto slice_of = [&](int t) { return p.backward ? (p.L + 1 - t) : t; };
+  if (c == 0) team_issue(bufs + ssf, p.factors + (size_t)(slice_of(1) - 1) * p.slice_bytes, M, T, &mbar[1]);
+
+  float2 U[Q][M];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+#pragma unroll
+    for (int i = 0; i < M; ++i) U[q][i] = make_float2(0.f, 0.f);
+    if (p.probes != nullptr && p0 + q < p.P) {
+      const float2 *src = p.probes + (size_t)(p0 + q) * p.N + c * M;
+#pragma unroll
+      for (int i = 0; i < M; ++i) U[q][i] = src[i];
+    }
+  }
+  if (p.u_store != nullptr) {
+    const int t0 = p.flip_out ? p.L : 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      if (p0 + q >= p.P) continue;
+      float2 *dst = p.u_store + ((size_t)(p0 + q) * p.nz + t0) * p.Npad;
+#pragma unroll
+      for (int i = 0; i < M; ++i) dst[i * C + c] = U[q][i];
+    }
+  }
+
+  uint32_t phase = 0;
+  {
+    const bool ok = mbar_wait_bounded(&mbar[1], 0, p.err);
+    phase ^= 2u;
+    if (__syncthreads_or(!ok)) {
+      if (c == 0) mbar_wait_bounded(&mbar[1], 0, nullptr);
+      __syncthreads();
+      return;
+    }
+  }
+
+  for (int t = 1; t <= p.L; ++t) {
+    const int cb = t & 1;
+    const int s = slice_of(t);
+    if (c == 0 && t < p.L) {
+      fence_proxy_async_smem();
+      team_issue(bufs + (cb ^ 1) * ssf, p.factors + (size_t)(slice_of(t + 1) - 1) * p.slice_bytes, M, T,
+                 &mbar[cb ^ 1]);
+    }
+    const float2 *F = bufs + cb * ssf;
+    if constexpr (!LAGGED) team_rhs<M, Q>(U, F, XL, XF, c, p.sp);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      if (p0 + q >= p.P) continue;
+      const int g0 = c * M;
+      if (p.src_shared != nullptr) {
+        const float2 *src = p.src_shared + (size_t)(t - 1) * p.N + g0;
+#pragma unroll
+        for (int i = 0; i < M; ++i) U[q][i] = cadd(U[q][i], src[i]);
+      }
+      if (p.src_probe != nullptr) {
+        const int col = p.src_rev ? (p.L - t) : (t - 1);
+        const float2 *src = p.src_probe + ((size_t)(p0 + q) * p.L + col) * p.N + g0;
+#pragma unroll
+        for (int i = 0; i < M; ++i) U[q][i] = cadd(U[q][i], src[i]);
+      }
+      if (t == 1 && p.src_exit != nullptr) {
+        const float2 *src = p.src_exit + (size_t)(p0 + q) * p.N + g0;
+#pragma unroll
+        for (int i = 0; i < M; ++i) U[q][i] = cadd(U[q][i], src[i]);
+      }
+    }
+    team_solve<M, Q>(U, F, T, Y0, R0, R1, XS, c, p.sp);
+    if (p.u_store != nullptr) {
+      const int to = p.flip_out ? (p.L - t) : t;
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        if (p0 + q >= p.P) continue;
+        float2 *dst = p.u_store + ((size_t)(p0 + q) * p.nz + to) * p.Npad;
+#pragma unroll
+        for (int i = 0; i < M; ++i) dst[i * C + c] = U[q][i];
+      }
+    }
+    if (t == p.L && p.exit_out != nullptr) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        if (p0 + q >= p.P) continue;
+        float2 *dst = p.exit_out + (size_t)(p0 + q) * p.N + c * M;
+#pragma unroll
+        for (int i = 0; i < M; ++i) dst[i] = U[q][i];
+      }
+    }
+    if (do_grad) {
+      // GB is free: every thread finished the previous step's flush before
+      // passing this step's first barrier.
+#pragma unroll
+      for (int i = 0; i < M; ++i) {
+        float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+          if (p0 + q >= p.P) continue;
+          const float2 *ua = p.u_fwd + ((size_t)(p0 + q) * p.nz + s) * p.Npad + i * C + c;
+          const float2 w = cadd(ua[0], ua[-(ptrdiff_t)p.Npad]);
+          acc = cadd(acc, cmulc(U[q][i], w));
+        }
+        GB[i * (C + 1) + c] = acc;
+      }
+    }
+    if constexpr (LAGGED) team_rhs<M, Q>(U, F, XL, XF, c, p.sp);
+    bool good = true;
+    if (t < p.L) {
+      good = mbar_wait_bounded(&mbar[cb ^ 1], (phase >> (cb ^ 1)) & 1u, p.err);
+      phase ^= (1u << (cb ^ 1));
+    }
+    if (__syncthreads_or(!good)) {
+      if (c == 0) mbar_wait_bounded(&mbar[cb ^ 1], ((phase >> (cb ^ 1)) & 1u) ^ 1u, nullptr);
+      __syncthreads();
+      return;
+    }
+    if (do_grad) {
+      float2 *dst = p.grad_c + (size_t)(s - 1) * p.N;
+      for (int g = c; g < p.N; g += kTeamThreads) {
+        const int i = g % M, k = g / M;
+        atomicAdd(&dst[g], GB[i * (C + 1) + k]);
+      }
+    }
+  }
+}
+
+template <int M, int Q, bool LAGGED>
+static int launch_team_t(const Partition &pt, MarchParams &mp, cudaStream_t st) {
+  auto kern = cn2d_team_kernel<M, Q, LAGGED>;
+  const bool grad = LAGGED && mp.grad_c != nullptr;
+  const size_t smem = team_smem_bytes(pt, mp.trunc, Q, grad);
+  TP_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = (mp.P + Q - 1) / Q;
+  kern<<<grid, kTeamThreads, smem, st>>>(mp);
+  return check_cuda(cudaGetLastError(), "cn2d_team_kernel launch");
+}
+
+template <int M, bool LAGGED>
+static int launch_team_q(const Partition &pt, MarchParams &mp, int Q, cudaStream_t st) {
+  if (Q == 4) return launch_team_t<M, 4, LAGGED>(pt, mp, st);
+  if (Q == 2) return launch_team_t<M, 2, LAGGED>(pt, mp, st);
+  return launch_team_t<M, 1, LAGGED>(pt, mp, st);
+}
+
+int launch_team_march(const Partition &pt, MarchParams &mp, bool lagged, cudaStream_t st) {
+  mp.smem_slice_bytes = team_slice_smem(pt.M, mp.trunc);
+  // Probes per CTA: enough CTAs to cover the SMs, then the largest group that fits.
+  int dev = 0, sms = 148, max_smem = 232448;
+  TP_CHECK_CUDA(cudaGetDevice(&dev));
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const bool grad = lagged && mp.grad_c != nullptr;
+  int Q = 4;
+  while (Q > 1 && ((mp.P + Q - 1) / Q < (sms * 3) / 4 || team_smem_bytes(pt, mp.trunc, Q, grad) > (size_t)max_smem))
+    Q /= 2;
+  if (team_smem_bytes(pt, mp.trunc, Q, grad) > (size_t)max_smem)
+    return set_error(TP_ERR_UNSUPPORTED, "team march needs %zu B of shared memory (> %d)",
+                     team_smem_bytes(pt, mp.trunc, Q, grad), max_smem);
+  switch (pt.M) {
+    case 4:
+      return lagged ? launch_team_q<4, true>(pt, mp, Q, st) : launch_team_q<4, false>(pt, mp, Q, st);
+    case 8:
+      return lagged ? launch_team_q<8, true>(pt, mp, Q, st) : launch_team_q<8, false>(pt, mp, Q, st);
+    case 16:
+      return lagged ? launch_team_q<16, true>(pt, mp, Q, st) : launch_team_q<16, false>(pt, mp, Q, st);
+    default:
+      return set_error(TP_ERR_UNSUPPORTED, "no team kernel for %d rows per chunk", pt.M);
+  }
+}
+
+}  // namespace tp

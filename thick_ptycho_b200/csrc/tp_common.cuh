@@ -108,7 +108,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
                                                   uint32_t max_iter = 1u << 22) {
   for (uint32_t it = 0; it < max_iter; ++it)
     if (mbar_try_wait(bar, parity)) return true;
-  if (err) atomicExch(err, (int)kDevMbarTimeout);
+  if (err) atomicOr(err, (int)kDevMbarTimeout);
   return false;
 }
 
