@@ -469,7 +469,7 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
       for (int g = tid; g < p.N; g += blockDim.x) {
         const int i = g % M, k = g / M;
         const float2 v = ga[i * 33 + k];
-        atomicAdd(&dst[g], v);
+        asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(&dst[g]), "f"(v.x), "f"(v.y) : "memory");
         ga[i * 33 + k] = make_float2(0.f, 0.f);
       }
     }

@@ -1,7 +1,10 @@
 // Team path of the 2D Crank–Nicolson march: N in {512, 1024, 2048}.
 //
-// One CTA of 4 warps (128 threads) marches a group of Q probes.  Thread c
-// owns chunk c (M = N/128 consecutive rows) of every probe of the group, so
+// A team of 4 warps (128 threads) marches a group of Q probes; a CTA holds TM
+// teams that share the staged factor slice (so an SM runs 4*TM warps while
+// holding one copy of the factors) and synchronise among themselves with
+// named barriers.  Thread c of a team owns chunk c (M = N/128 consecutive
+// rows) of every probe of its group, so
 // each factor value read from shared memory serves Q probes and the Q
 // recurrences of a thread are independent (instruction-level parallelism
 // where the warp path has one dependent chain).  The 128 separators of each
@@ -11,23 +14,37 @@
 // operator and verified when factorising).
 //
 // Exact-adjoint gradient: the Q probes' contributions lambda*conj(u_s+u_{s-1})
-// are summed in registers, stored once per CTA in shared memory and flushed
-// with one vector atomic per row, so no shared-memory atomics are needed.
+// are summed in registers, combined across the CTA's teams in shared memory
+// and flushed with one fire-and-forget vector reduction per row and CTA.
 #include "cn2d_internal.cuh"
+#include <stdio.h>
+#include <stdlib.h>
+
 #include "tp_errors.h"
 
 namespace tp {
 
-constexpr int kTeamThreads = kTeamChunks;  // one thread per chunk
+constexpr int kTeamThreads = kTeamChunks;  // threads per team: one per chunk
 constexpr int kTeamLevels = 7;
+
+// Barrier among the 128 threads of one team (ids 1..TM; 0 is __syncthreads).
+__device__ __forceinline__ void team_sync(int team) {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + team), "r"(kTeamThreads) : "memory");
+}
+__device__ __forceinline__ void red_add_v2(float2 *addr, float2 v) {
+  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(addr), "f"(v.x), "f"(v.y) : "memory");
+}
+__device__ __forceinline__ void red_add_shared(float *addr, float v) {
+  asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(smem_addr(addr)), "f"(v) : "memory");
+}
 
 __host__ __device__ inline size_t team_slice_smem(int M, int T) {
   return (size_t)(3 * M + 2 * T + 3 + 2 * kTeamLevels) * kTeamChunks * sizeof(float2);
 }
 
-size_t team_smem_bytes(const Partition &pt, int trunc, int Q, bool grad) {
-  return 2 * team_slice_smem(pt.M, trunc) + 6 * (size_t)Q * kTeamChunks * sizeof(float2) +
-         (grad ? (size_t)pt.M * (kTeamChunks + 1) * sizeof(float2) : 0) + 2 * sizeof(uint64_t);
+size_t team_smem_bytes(const Partition &pt, int trunc, int Q, int TM, bool grad) {
+  return 2 * team_slice_smem(pt.M, trunc) + 6 * (size_t)TM * Q * kTeamChunks * sizeof(float2) +
+         (grad ? 2 * (size_t)pt.M * (kTeamChunks + 1) * sizeof(float2) : 0) + 2 * sizeof(uint64_t);
 }
 
 // Issue the bulk copies of one slice's factor set (QD|LF|EP, V head, W tail, records).
@@ -47,7 +64,7 @@ __device__ __forceinline__ void team_issue(float2 *dst, const char *slice, int M
 // chunk C-1 rows M-2, M-1).
 template <int M, int Q>
 __device__ __forceinline__ void team_rhs(float2 (&U)[Q][M], const float2 *__restrict__ QD, float2 *XL, float2 *XF,
-                                         int c, const Spec &sp) {
+                                         int c, int team, const Spec &sp) {
   constexpr int C = kTeamChunks;
   const float2 zero = make_float2(0.f, 0.f);
 #pragma unroll
@@ -55,7 +72,7 @@ __device__ __forceinline__ void team_rhs(float2 (&U)[Q][M], const float2 *__rest
     XL[q * C + c] = U[q][M - 1];
     XF[q * C + c] = U[q][0];
   }
-  __syncthreads();
+  team_sync(team);
   float2 prev[Q], right[Q];
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
@@ -84,7 +101,7 @@ __device__ __forceinline__ void team_rhs(float2 (&U)[Q][M], const float2 *__rest
 // U <- M_s^{-1} U with the staged factor slice F.
 template <int M, int Q>
 __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__restrict__ F, int T, float2 *Y0,
-                                           float2 *R0, float2 *R1, float2 *XS, int c, const Spec &sp) {
+                                           float2 *R0, float2 *R1, float2 *XS, int c, int team, const Spec &sp) {
   constexpr int C = kTeamChunks;
   const float2 zero = make_float2(0.f, 0.f);
   const float2 *LF = F + M * C, *EP = F + 2 * M * C, *VH = F + 3 * M * C, *WT = VH + T * C, *LR = WT + T * C;
@@ -114,7 +131,7 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
   }
 #pragma unroll
   for (int q = 0; q < Q; ++q) Y0[q * C + c] = U[q][0];
-  __syncthreads();
+  team_sync(team);
   float2 rho[Q];
   {
     const float2 ma = LR[0 * C + c], mc = LR[1 * C + c];
@@ -130,7 +147,7 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
     float2 *Rb = (l & 1) ? R1 : R0;
 #pragma unroll
     for (int q = 0; q < Q; ++q) Rb[q * C + c] = rho[q];
-    __syncthreads();
+    team_sync(team);
     const float2 al = LR[(2 + l) * C + c], ga = LR[(2 + kTeamLevels + l) * C + c];
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
@@ -148,7 +165,7 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
       XS[q * C + c] = x[q];
     }
   }
-  __syncthreads();
+  team_sync(team);
 #pragma unroll
   for (int q = 0; q < Q; ++q) xp[q] = (c > 0) ? XS[q * C + c - 1] : zero;
   const int wlo = M - 1 - T;
@@ -169,30 +186,35 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
   for (int q = 0; q < Q; ++q) U[q][M - 1] = x[q];
 }
 
-template <int M, int Q, bool LAGGED>
-__global__ void __launch_bounds__(kTeamThreads, 1) cn2d_team_kernel(const MarchParams p) {
+template <int M, int Q, int TM, bool LAGGED>
+__global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const MarchParams p) {
   constexpr int C = kTeamChunks;
+  constexpr int NT = kTeamThreads * TM;
   extern __shared__ __align__(128) unsigned char smem[];
-  const int c = threadIdx.x;
+  const int tid = threadIdx.x;
+  const int team = tid / kTeamThreads;
+  const int c = tid % kTeamThreads;
   const int T = p.trunc;
   const size_t ss = p.smem_slice_bytes;
   float2 *bufs = reinterpret_cast<float2 *>(smem);
-  float2 *XL = reinterpret_cast<float2 *>(smem + 2 * ss);
+  float2 *XL = reinterpret_cast<float2 *>(smem + 2 * ss) + (size_t)team * 6 * Q * C;
   float2 *XF = XL + Q * C, *Y0 = XF + Q * C, *R0 = Y0 + Q * C, *R1 = R0 + Q * C, *XS = R1 + Q * C;
   const bool do_grad = LAGGED && (p.grad_c != nullptr);
-  float2 *GB = XS + Q * C;  // [M][C+1], only with the gradient
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(GB + (do_grad ? M * (C + 1) : 0));
+  float2 *GB = reinterpret_cast<float2 *>(smem + 2 * ss) + (size_t)TM * 6 * Q * C;  // [2][M][C+1]
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(GB + (do_grad ? 2 * M * (C + 1) : 0));
   const size_t ssf = ss / sizeof(float2);
-  const int p0 = blockIdx.x * Q;
+  const int p0 = (blockIdx.x * TM + team) * Q;
 
-  if (c == 0) {
+  if (tid == 0) {
     mbar_init(&mbar[0], 1);
     mbar_init(&mbar[1], 1);
     fence_mbar_init();
   }
+  if (do_grad)
+    for (int e = tid; e < 2 * M * (C + 1); e += NT) GB[e] = make_float2(0.f, 0.f);
   __syncthreads();
   auto slice_of = [&](int t) { return p.backward ? (p.L + 1 - t) : t; };
-  if (c == 0) team_issue(bufs + ssf, p.factors + (size_t)(slice_of(1) - 1) * p.slice_bytes, M, T, &mbar[1]);
+  if (tid == 0) team_issue(bufs + ssf, p.factors + (size_t)(slice_of(1) - 1) * p.slice_bytes, M, T, &mbar[1]);
 
   float2 U[Q][M];
 #pragma unroll
@@ -221,7 +243,7 @@ __global__ void __launch_bounds__(kTeamThreads, 1) cn2d_team_kernel(const MarchP
     const bool ok = mbar_wait_bounded(&mbar[1], 0, p.err);
     phase ^= 2u;
     if (__syncthreads_or(!ok)) {
-      if (c == 0) mbar_wait_bounded(&mbar[1], 0, nullptr);
+      if (tid == 0) mbar_wait_bounded(&mbar[1], 0, nullptr);
       __syncthreads();
       return;
     }
@@ -230,13 +252,13 @@ __global__ void __launch_bounds__(kTeamThreads, 1) cn2d_team_kernel(const MarchP
   for (int t = 1; t <= p.L; ++t) {
     const int cb = t & 1;
     const int s = slice_of(t);
-    if (c == 0 && t < p.L) {
+    if (tid == 0 && t < p.L) {
       fence_proxy_async_smem();
       team_issue(bufs + (cb ^ 1) * ssf, p.factors + (size_t)(slice_of(t + 1) - 1) * p.slice_bytes, M, T,
                  &mbar[cb ^ 1]);
     }
     const float2 *F = bufs + cb * ssf;
-    if constexpr (!LAGGED) team_rhs<M, Q>(U, F, XL, XF, c, p.sp);
+    if constexpr (!LAGGED) team_rhs<M, Q>(U, F, XL, XF, c, team, p.sp);
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       if (p0 + q >= p.P) continue;
@@ -258,7 +280,7 @@ __global__ void __launch_bounds__(kTeamThreads, 1) cn2d_team_kernel(const MarchP
         for (int i = 0; i < M; ++i) U[q][i] = cadd(U[q][i], src[i]);
       }
     }
-    team_solve<M, Q>(U, F, T, Y0, R0, R1, XS, c, p.sp);
+    team_solve<M, Q>(U, F, T, Y0, R0, R1, XS, c, team, p.sp);
     if (p.u_store != nullptr) {
       const int to = p.flip_out ? (p.L - t) : t;
 #pragma unroll
@@ -279,81 +301,118 @@ __global__ void __launch_bounds__(kTeamThreads, 1) cn2d_team_kernel(const MarchP
       }
     }
     if (do_grad) {
-      // GB is free: every thread finished the previous step's flush before
-      // passing this step's first barrier.
+      // GB[cb] was zeroed by the flush two steps ago, which every thread
+      // finished before passing the previous step's closing barrier.
+      float2 w[Q][M];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const bool ok = p0 + q < p.P;
+        const float2 *ua = p.u_fwd + ((size_t)(ok ? p0 + q : 0) * p.nz + s) * p.Npad + c;
+#pragma unroll
+        for (int i = 0; i < M; ++i) w[q][i] = ok ? cadd(ua[i * C], ua[i * C - (ptrdiff_t)p.Npad]) : make_float2(0.f, 0.f);
+      }
+      float2 *gb = GB + cb * M * (C + 1);
 #pragma unroll
       for (int i = 0; i < M; ++i) {
         float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-          if (p0 + q >= p.P) continue;
-          const float2 *ua = p.u_fwd + ((size_t)(p0 + q) * p.nz + s) * p.Npad + i * C + c;
-          const float2 w = cadd(ua[0], ua[-(ptrdiff_t)p.Npad]);
-          acc = cadd(acc, cmulc(U[q][i], w));
+        for (int q = 0; q < Q; ++q) acc = cadd(acc, cmulc(U[q][i], w[q][i]));
+        if constexpr (TM == 1) {
+          gb[i * (C + 1) + c] = acc;
+        } else {
+          red_add_shared(&gb[i * (C + 1) + c].x, acc.x);
+          red_add_shared(&gb[i * (C + 1) + c].y, acc.y);
         }
-        GB[i * (C + 1) + c] = acc;
       }
     }
-    if constexpr (LAGGED) team_rhs<M, Q>(U, F, XL, XF, c, p.sp);
+    if constexpr (LAGGED) team_rhs<M, Q>(U, F, XL, XF, c, team, p.sp);
     bool good = true;
     if (t < p.L) {
       good = mbar_wait_bounded(&mbar[cb ^ 1], (phase >> (cb ^ 1)) & 1u, p.err);
       phase ^= (1u << (cb ^ 1));
     }
     if (__syncthreads_or(!good)) {
-      if (c == 0) mbar_wait_bounded(&mbar[cb ^ 1], ((phase >> (cb ^ 1)) & 1u) ^ 1u, nullptr);
+      if (tid == 0) mbar_wait_bounded(&mbar[cb ^ 1], ((phase >> (cb ^ 1)) & 1u) ^ 1u, nullptr);
       __syncthreads();
       return;
     }
     if (do_grad) {
       float2 *dst = p.grad_c + (size_t)(s - 1) * p.N;
-      for (int g = c; g < p.N; g += kTeamThreads) {
+      float2 *gb = GB + cb * M * (C + 1);
+      for (int g = tid; g < p.N; g += NT) {
         const int i = g % M, k = g / M;
-        atomicAdd(&dst[g], GB[i * (C + 1) + k]);
+        red_add_v2(&dst[g], gb[i * (C + 1) + k]);
+        if constexpr (TM > 1) gb[i * (C + 1) + k] = make_float2(0.f, 0.f);
       }
     }
   }
 }
 
-template <int M, int Q, bool LAGGED>
+template <int M, int Q, int TM, bool LAGGED>
 static int launch_team_t(const Partition &pt, MarchParams &mp, cudaStream_t st) {
-  auto kern = cn2d_team_kernel<M, Q, LAGGED>;
+  auto kern = cn2d_team_kernel<M, Q, TM, LAGGED>;
   const bool grad = LAGGED && mp.grad_c != nullptr;
-  const size_t smem = team_smem_bytes(pt, mp.trunc, Q, grad);
+  const size_t smem = team_smem_bytes(pt, mp.trunc, Q, TM, grad);
   TP_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int grid = (mp.P + Q - 1) / Q;
-  kern<<<grid, kTeamThreads, smem, st>>>(mp);
+  const int grid = (mp.P + Q * TM - 1) / (Q * TM);
+  kern<<<grid, kTeamThreads * TM, smem, st>>>(mp);
   return check_cuda(cudaGetLastError(), "cn2d_team_kernel launch");
 }
 
 template <int M, bool LAGGED>
-static int launch_team_q(const Partition &pt, MarchParams &mp, int Q, cudaStream_t st) {
-  if (Q == 4) return launch_team_t<M, 4, LAGGED>(pt, mp, st);
-  if (Q == 2) return launch_team_t<M, 2, LAGGED>(pt, mp, st);
-  return launch_team_t<M, 1, LAGGED>(pt, mp, st);
+static int launch_team_qt(const Partition &pt, MarchParams &mp, int Q, int TM, cudaStream_t st) {
+  if (TM == 1 && Q == 4) return launch_team_t<M, 4, 1, LAGGED>(pt, mp, st);
+  if (TM == 1 && Q == 2) return launch_team_t<M, 2, 1, LAGGED>(pt, mp, st);
+  if (TM == 1 && Q == 1) return launch_team_t<M, 1, 1, LAGGED>(pt, mp, st);
+  if (TM == 2 && Q == 2) return launch_team_t<M, 2, 2, LAGGED>(pt, mp, st);
+  if (TM == 2 && Q == 1) return launch_team_t<M, 1, 2, LAGGED>(pt, mp, st);
+  if (TM == 4 && Q == 1) return launch_team_t<M, 1, 4, LAGGED>(pt, mp, st);
+  return set_error(TP_ERR_UNSUPPORTED, "no team kernel for Q=%d, TM=%d", Q, TM);
+}
+
+// (teams per CTA, probes per thread) for K probes per CTA.
+static void team_shape(int K, int *TM, int *Q) {
+  const char *env = getenv("TPCUDA_TEAM_SHAPE");  // "TM,Q" override for tuning sweeps
+  if (env != nullptr && sscanf(env, "%d,%d", TM, Q) == 2 && *TM * *Q == K) return;
+  if (K >= 4) {
+    *TM = 2;
+    *Q = 2;
+  } else if (K == 2) {
+    *TM = 2;
+    *Q = 1;
+  } else {
+    *TM = 1;
+    *Q = 1;
+  }
 }
 
 int launch_team_march(const Partition &pt, MarchParams &mp, bool lagged, cudaStream_t st) {
   mp.smem_slice_bytes = team_slice_smem(pt.M, mp.trunc);
-  // Probes per CTA: enough CTAs to cover the SMs, then the largest group that fits.
   int dev = 0, sms = 148, max_smem = 232448;
   TP_CHECK_CUDA(cudaGetDevice(&dev));
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   const bool grad = lagged && mp.grad_c != nullptr;
-  int Q = 4;
-  while (Q > 1 && ((mp.P + Q - 1) / Q < (sms * 3) / 4 || team_smem_bytes(pt, mp.trunc, Q, grad) > (size_t)max_smem))
-    Q /= 2;
-  if (team_smem_bytes(pt, mp.trunc, Q, grad) > (size_t)max_smem)
+  // Probes per CTA: one CTA per SM (the factor double buffer fills most of
+  // an SM's shared memory), so K = ceil(P / SMs) rounded up to 1, 2 or 4.
+  int K = 1;
+  while (K < 4 && (mp.P + K - 1) / K > sms) K *= 2;
+  int TM, Q;
+  team_shape(K, &TM, &Q);
+  while (team_smem_bytes(pt, mp.trunc, Q, TM, grad) > (size_t)max_smem && TM * Q > 1) {
+    if (TM > 1) TM /= 2;
+    else Q /= 2;
+  }
+  if (team_smem_bytes(pt, mp.trunc, Q, TM, grad) > (size_t)max_smem)
     return set_error(TP_ERR_UNSUPPORTED, "team march needs %zu B of shared memory (> %d)",
-                     team_smem_bytes(pt, mp.trunc, Q, grad), max_smem);
+                     team_smem_bytes(pt, mp.trunc, Q, TM, grad), max_smem);
   switch (pt.M) {
     case 4:
-      return lagged ? launch_team_q<4, true>(pt, mp, Q, st) : launch_team_q<4, false>(pt, mp, Q, st);
+      return lagged ? launch_team_qt<4, true>(pt, mp, Q, TM, st) : launch_team_qt<4, false>(pt, mp, Q, TM, st);
     case 8:
-      return lagged ? launch_team_q<8, true>(pt, mp, Q, st) : launch_team_q<8, false>(pt, mp, Q, st);
+      return lagged ? launch_team_qt<8, true>(pt, mp, Q, TM, st) : launch_team_qt<8, false>(pt, mp, Q, TM, st);
     case 16:
-      return lagged ? launch_team_q<16, true>(pt, mp, Q, st) : launch_team_q<16, false>(pt, mp, Q, st);
+      return lagged ? launch_team_qt<16, true>(pt, mp, Q, TM, st) : launch_team_qt<16, false>(pt, mp, Q, TM, st);
     default:
       return set_error(TP_ERR_UNSUPPORTED, "no team kernel for %d rows per chunk", pt.M);
   }

@@ -115,4 +115,7 @@ CONFIG1 = Workload("2d-fwd-adj-2048x1024-p512", 2, 2048, 1024, 512, 3, 8.0, 200,
 CONFIG2 = Workload("3d-forward-256x256x256-p64", 3, 256, 256, 8, 16, 12.0, 400, 1)
 CONFIG3 = Workload("2d-grad-1024x512-p256", 2, 1024, 512, 256, 4, 8.0, 300, 0)
 CONFIG4 = Workload("3d-recon-192x192x192-p256", 3, 192, 192, 16, 10, 12.0, 600, 1)
-CONFIGS = {w.name: w for w in (CONFIG0, CONFIG1, CONFIG2, CONFIG3, CONFIG4)}
+# Reduced-depth case of the CONFIG1 kernels (same N and probe count, 128 nodes):
+# small enough for full profiler captures, larger than L2 (1.07 GB field).
+PROFILE1 = Workload("2d-fwd-adj-2048x128-p512", 2, 2048, 128, 512, 3, 8.0, 200, 0)
+CONFIGS = {w.name: w for w in (CONFIG0, CONFIG1, CONFIG2, CONFIG3, CONFIG4, PROFILE1)}
