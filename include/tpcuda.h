@@ -109,7 +109,10 @@ typedef struct tp_cn2d_march_args {
 
 /* Partition of N rows into `chunks` chunks of `rows_per_chunk` rows (padded
  * row count Npad = chunks * rows_per_chunk).  Chunked full fields store row
- * k*rows_per_chunk + i of a slice at offset i*chunks + k. */
+ * k*rows_per_chunk + i of a slice at offset i*chunks + k when chunks == 32,
+ * and in row pairs, at offset ((i/2)*chunks + k)*2 + i%2, when chunks == 128
+ * (N in {512, 1024, 2048}; these sizes need purely imaginary off-diagonals
+ * of K, which every paraxial operator has). */
 TP_API int tp_cn2d_layout(int32_t n, int32_t *chunks, int32_t *rows_per_chunk, int32_t *npad);
 
 /* Bytes of the per-slice factor workspace for (N, nz). */

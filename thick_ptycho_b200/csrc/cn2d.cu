@@ -88,7 +88,7 @@ int team_spike_rows(const tp_cn2d_op *op, int M) {
   if (disc <= 0.0) return M - 1;
   const double rho = (d0 - sqrt(disc)) / (2.0 * b);
   if (!(rho > 0.0) || rho >= 0.5) return M - 1;
-  int t = (int)ceil(log(1e-10) / log(rho)) + 2;
+  int t = (int)ceil(log(1e-9) / log(rho)) + 1;
   if (t < 1) t = 1;
   if (t > M - 1) t = M - 1;
   return t;
@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
 // Layout and gradient helpers
 // --------------------------------------------------------------------------
 __global__ void cn2d_unchunk_kernel(const float2 *__restrict__ st, float2 *__restrict__ out, int P, int N, int nz,
-                                    int M, int C) {
+                                    int M, int C, int pair) {
   const size_t Npad = (size_t)C * M;
   const size_t total = (size_t)P * N * nz;
   for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
@@ -488,7 +488,9 @@ __global__ void cn2d_unchunk_kernel(const float2 *__restrict__ st, float2 *__res
     const size_t pg = idx / nz;
     const int g = (int)(pg % N);
     const size_t pp = pg / N;
-    out[idx] = st[(pp * nz + t) * Npad + (size_t)(g % M) * C + g / M];
+    const int i = g % M, k = g / M;
+    const size_t off = pair ? ((size_t)(i >> 1) * C + k) * 2 + (i & 1) : (size_t)i * C + k;
+    out[idx] = st[(pp * nz + t) * Npad + off];
   }
 }
 
@@ -749,7 +751,13 @@ extern "C" int tp_cn2d_march(const tp_cn2d_op *op, const void *factors, const tp
   mp.u_fwd = static_cast<const float2 *>(a->u_fwd);
   mp.grad_c = static_cast<float2 *>(a->grad_c);
   mp.err = err;
-  if (pt.team) return launch_team_march(pt, mp, lagged, reinterpret_cast<cudaStream_t>(stream));
+  if (pt.team) {
+    if (op->k_off[0] != 0.0 || op->k_01[0] != 0.0 || op->k_nm[0] != 0.0)
+      return set_error(TP_ERR_UNSUPPORTED,
+                       "N=%d uses the team kernels, which need purely imaginary off-diagonals of K "
+                       "(mu = i dz/(4 k dx^2))", op->n);
+    return launch_team_march(pt, mp, lagged, reinterpret_cast<cudaStream_t>(stream));
+  }
   return launch_march(pt.M, mp, op->n == pt.C * pt.M, lagged, reinterpret_cast<cudaStream_t>(stream));
 }
 
@@ -762,7 +770,7 @@ extern "C" int tp_cn2d_unchunk(const tp_cn2d_op *op, int32_t num_probes, const v
   rc = partition_for(op->n, &pt);
   if (rc) return rc;
   cn2d_unchunk_kernel<<<1184, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-      static_cast<const float2 *>(u_store), static_cast<float2 *>(u_out), num_probes, op->n, op->nz, pt.M, pt.C);
+      static_cast<const float2 *>(u_store), static_cast<float2 *>(u_out), num_probes, op->n, op->nz, pt.M, pt.C, pt.team);
   return check_cuda(cudaGetLastError(), "cn2d_unchunk_kernel launch");
 }
 

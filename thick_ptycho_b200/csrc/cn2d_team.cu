@@ -38,6 +38,19 @@ __device__ __forceinline__ void red_add_shared(float *addr, float v) {
   asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(smem_addr(addr)), "f"(v) : "memory");
 }
 
+// b * i * z for real b (the off-diagonal of P is purely imaginary: i*dz/(4k dx^2)).
+__device__ __forceinline__ float2 imul_acc(float b, float2 z, float2 acc) {
+  return make_float2(fmaf(-b, z.y, acc.x), fmaf(b, z.x, acc.y));
+}
+
+// Chunked team layout: rows are stored in pairs, so thread c's rows 2j, 2j+1
+// are one 16-byte vector at offset (j*C + c)*2 of a slice.
+__device__ __forceinline__ void store_pairs(float2 *dst, const float2 *U, int M, int c) {
+#pragma unroll 8
+  for (int j = 0; j < M / 2; ++j)
+    reinterpret_cast<float4 *>(dst)[j * kTeamChunks + c] = make_float4(U[2 * j].x, U[2 * j].y, U[2 * j + 1].x, U[2 * j + 1].y);
+}
+
 __host__ __device__ inline size_t team_slice_smem(int M, int T) {
   return (size_t)(3 * M + 2 * T + 3 + 2 * kTeamLevels) * kTeamChunks * sizeof(float2);
 }
@@ -87,7 +100,7 @@ __device__ __forceinline__ void team_rhs(float2 (&U)[Q][M], const float2 *__rest
       const float2 cur = U[q][i];
       const float2 nxt = (i < M - 1) ? U[q][(i + 1) < M ? i + 1 : i] : right[q];
       float2 r = cfma(qd, cur, cur);
-      r = cfma(sp.p_o, cadd(prev[q], nxt), r);
+      r = imul_acc(sp.p_o.y, cadd(prev[q], nxt), r);
       if (i == 0 && c == 0) r = cfma(sp.d_sup0, nxt, r);
       if (i == 1 && c == 0) r = cfma(sp.d_sub1, prev[q], r);
       if (i == M - 2 && c == C - 1) r = cfma(sp.d_supN2, nxt, r);
@@ -122,10 +135,11 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
 #pragma unroll
   for (int i = M - 3; i >= 0; --i) {
     const float2 ep = EP[i * C + c];
-    const float2 msup = (i == 0 && c == 0) ? make_float2(-sp.sup0.x, -sp.sup0.y) : make_float2(-sp.p_o.x, -sp.p_o.y);
+    // t = U[i] - M[i,i+1] U[i+1] = U[i] + P[i,i+1] U[i+1]; P[0,1] is the only special entry here.
+    const float bsup = (i == 0 && c == 0) ? sp.sup0.y : sp.p_o.y;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-      const float2 t = cfnma(msup, U[q][i + 1], U[q][i]);
+      const float2 t = imul_acc(bsup, U[q][i + 1], U[q][i]);
       U[q][i] = cfma(t, ep, t);
     }
   }
@@ -232,9 +246,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       if (p0 + q >= p.P) continue;
-      float2 *dst = p.u_store + ((size_t)(p0 + q) * p.nz + t0) * p.Npad;
-#pragma unroll
-      for (int i = 0; i < M; ++i) dst[i * C + c] = U[q][i];
+      store_pairs(p.u_store + ((size_t)(p0 + q) * p.nz + t0) * p.Npad, U[q], M, c);
     }
   }
 
@@ -286,9 +298,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         if (p0 + q >= p.P) continue;
-        float2 *dst = p.u_store + ((size_t)(p0 + q) * p.nz + to) * p.Npad;
-#pragma unroll
-        for (int i = 0; i < M; ++i) dst[i * C + c] = U[q][i];
+        store_pairs(p.u_store + ((size_t)(p0 + q) * p.nz + to) * p.Npad, U[q], M, c);
       }
     }
     if (t == p.L && p.exit_out != nullptr) {
@@ -307,21 +317,30 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         const bool ok = p0 + q < p.P;
-        const float2 *ua = p.u_fwd + ((size_t)(ok ? p0 + q : 0) * p.nz + s) * p.Npad + c;
+        const float4 *ua =
+            reinterpret_cast<const float4 *>(p.u_fwd + ((size_t)(ok ? p0 + q : 0) * p.nz + s) * p.Npad) + c;
+        const float4 *ub = ua - p.Npad / 2;
 #pragma unroll
-        for (int i = 0; i < M; ++i) w[q][i] = ok ? cadd(ua[i * C], ua[i * C - (ptrdiff_t)p.Npad]) : make_float2(0.f, 0.f);
+        for (int j = 0; j < M / 2; ++j) {
+          const float4 a = ok ? ua[j * C] : make_float4(0.f, 0.f, 0.f, 0.f);
+          const float4 b = ok ? ub[j * C] : make_float4(0.f, 0.f, 0.f, 0.f);
+          w[q][2 * j] = make_float2(a.x + b.x, a.y + b.y);
+          w[q][2 * j + 1] = make_float2(a.z + b.z, a.w + b.w);
+        }
       }
-      float2 *gb = GB + cb * M * (C + 1);
+      float *gr = reinterpret_cast<float *>(GB) + cb * 2 * M * (C + 1);  // [re|im][M][C+1]
+      float *gi = gr + M * (C + 1);
 #pragma unroll
       for (int i = 0; i < M; ++i) {
         float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
         for (int q = 0; q < Q; ++q) acc = cadd(acc, cmulc(U[q][i], w[q][i]));
         if constexpr (TM == 1) {
-          gb[i * (C + 1) + c] = acc;
+          gr[i * (C + 1) + c] = acc.x;
+          gi[i * (C + 1) + c] = acc.y;
         } else {
-          red_add_shared(&gb[i * (C + 1) + c].x, acc.x);
-          red_add_shared(&gb[i * (C + 1) + c].y, acc.y);
+          red_add_shared(&gr[i * (C + 1) + c], acc.x);
+          red_add_shared(&gi[i * (C + 1) + c], acc.y);
         }
       }
     }
@@ -338,11 +357,15 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
     }
     if (do_grad) {
       float2 *dst = p.grad_c + (size_t)(s - 1) * p.N;
-      float2 *gb = GB + cb * M * (C + 1);
+      float *gr = reinterpret_cast<float *>(GB) + cb * 2 * M * (C + 1);
+      float *gi = gr + M * (C + 1);
       for (int g = tid; g < p.N; g += NT) {
-        const int i = g % M, k = g / M;
-        red_add_v2(&dst[g], gb[i * (C + 1) + k]);
-        if constexpr (TM > 1) gb[i * (C + 1) + k] = make_float2(0.f, 0.f);
+        const int e = (g % M) * (C + 1) + g / M;
+        red_add_v2(&dst[g], make_float2(gr[e], gi[e]));
+        if constexpr (TM > 1) {
+          gr[e] = 0.f;
+          gi[e] = 0.f;
+        }
       }
     }
   }
