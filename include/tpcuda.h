@@ -103,7 +103,20 @@ typedef struct tp_cn2d_march_args {
   void *grad_c;              /* ADJOINT_EXACT: float2 (L, N) accumulator of
                                 sum_p lambda_s * conj(u_s + u_{s-1}); the caller
                                 zeroes it; row s-1 holds slice s               */
-  int32_t flags;             /* reserved, 0                                   */
+  /* Partial marches (checkpointed gradients).  All zero = one march over all
+   * L steps storing every slice at its own index. */
+  int32_t t_begin, t_end;    /* step range [t_begin, t_end], 1-based; 0 = 1 / L */
+  const void *state_in;      /* float2 (P, Npad) chunked state before t_begin
+                                (overrides probes), or NULL                   */
+  void *state_out;           /* float2 (P, Npad) chunked state after t_end (for
+                                ADJOINT_EXACT: the next step's right-hand side),
+                                or NULL                                        */
+  int32_t store_slices;      /* slices per probe in u_store (0 = nz)          */
+  int32_t store_every;       /* 0 or 1: state after step t at index t - store_base;
+                                S > 1: only when t % S == 0, at index t / S    */
+  int32_t store_base;
+  int32_t ufwd_slices;       /* slices per probe in u_fwd (0 = nz)             */
+  int32_t ufwd_base;         /* u_fwd index of forward slice s is s - ufwd_base */
   int32_t reserved;
 } tp_cn2d_march_args;
 

@@ -55,7 +55,7 @@ def test_pure_host_queries():
 def test_struct_layout_matches_header():
     # tp_cn2d_op: 6 int32 + 2 double + 6 complex doubles
     assert ctypes.sizeof(_native.TpCn2dOp) == 6 * 4 + 2 * 8 + 12 * 8
-    assert ctypes.sizeof(_native.TpCn2dMarchArgs) == 8 + 8 * 8 + 8
+    assert ctypes.sizeof(_native.TpCn2dMarchArgs) == 8 + 8 * 8 + 8 + 2 * 8 + 6 * 4
 
 
 @pytest.mark.parametrize("bc", ["neumann", "impedance", "dirichlet", "impedance2"])

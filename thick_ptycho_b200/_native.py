@@ -64,7 +64,15 @@ class TpCn2dMarchArgs(ctypes.Structure):
         ("exit_out", ctypes.c_void_p),
         ("u_fwd", ctypes.c_void_p),
         ("grad_c", ctypes.c_void_p),
-        ("flags", ctypes.c_int32),
+        ("t_begin", ctypes.c_int32),
+        ("t_end", ctypes.c_int32),
+        ("state_in", ctypes.c_void_p),
+        ("state_out", ctypes.c_void_p),
+        ("store_slices", ctypes.c_int32),
+        ("store_every", ctypes.c_int32),
+        ("store_base", ctypes.c_int32),
+        ("ufwd_slices", ctypes.c_int32),
+        ("ufwd_base", ctypes.c_int32),
         ("reserved", ctypes.c_int32),
     ]
 

@@ -108,18 +108,35 @@ class CN2D:
         exit_out: Optional[torch.Tensor] = None,
         u_fwd: Optional[torch.Tensor] = None,
         grad_c: Optional[torch.Tensor] = None,
+        t_begin: int = 0,
+        t_end: int = 0,
+        state_in: Optional[torch.Tensor] = None,
+        state_out: Optional[torch.Tensor] = None,
+        store_every: int = 0,
+        store_base: int = 0,
+        ufwd_base: int = 0,
     ):
-        """One batched march; every tensor is complex64, contiguous, on device."""
+        """One batched march; every tensor is complex64, contiguous, on device.
+
+        ``u_store`` is (P, S, Npad) with S slices per probe: the state after
+        step t goes to index ``t − store_base`` (or ``t / store_every`` when
+        ``store_every > 1``, only for multiples).  ``u_fwd`` is (≥P, S', Npad)
+        with forward slice s at index ``s − ufwd_base``.  ``t_begin..t_end``
+        restricts the steps; ``state_in``/``state_out`` (P, Npad) carry the
+        state across partial marches.
+        """
         P = int(num_probes)
         shapes = {
             "probes": (probes, (P, self.n)),
             "src_shared": (src_shared, (self.L, self.n)),
             "src_probe": (src_probe, (P, self.L, self.n)),
             "src_exit": (src_exit, (P, self.n)),
-            "u_store": (u_store, (P, self.nz, self.npad)),
+            "u_store": (u_store, None),
             "exit_out": (exit_out, (P, self.n)),
             "u_fwd": (u_fwd, None),
             "grad_c": (grad_c, (self.L, self.n)),
+            "state_in": (state_in, (P, self.npad)),
+            "state_out": (state_out, (P, self.npad)),
         }
         for name, (t, shp) in shapes.items():
             if t is None:
@@ -128,19 +145,28 @@ class CN2D:
                 raise TypeError(f"{name} must be a contiguous complex64 CUDA tensor")
             if shp is not None and tuple(t.shape) != shp:
                 raise ValueError(f"{name} has shape {tuple(t.shape)}, expected {shp}")
-        if u_fwd is not None and (u_fwd.shape[1:] != (self.nz, self.npad) or u_fwd.shape[0] < P):
-            raise ValueError("u_fwd must be a chunked forward field (P, nz, Npad)")
+        if u_fwd is not None and (u_fwd.dim() != 3 or u_fwd.shape[2] != self.npad or u_fwd.shape[0] < P):
+            raise ValueError("u_fwd must be a chunked forward field (P, slices, Npad)")
+        if u_store is not None and (u_store.dim() != 3 or u_store.shape[0] != P or u_store.shape[2] != self.npad):
+            raise ValueError("u_store must be a chunked field (P, slices, Npad)")
         a = _native.TpCn2dMarchArgs()
         a.num_probes, a.mode = P, fs.mode
         a.probes, a.src_shared, a.src_probe, a.src_exit = _ptr(probes), _ptr(src_shared), _ptr(src_probe), _ptr(src_exit)
         a.u_store, a.exit_out, a.u_fwd, a.grad_c = _ptr(u_store), _ptr(exit_out), _ptr(u_fwd), _ptr(grad_c)
+        a.t_begin, a.t_end = int(t_begin), int(t_end)
+        a.state_in, a.state_out = _ptr(state_in), _ptr(state_out)
+        a.store_slices = 0 if u_store is None else int(u_store.shape[1])
+        a.store_every, a.store_base = int(store_every), int(store_base)
+        a.ufwd_slices = 0 if u_fwd is None else int(u_fwd.shape[1])
+        a.ufwd_base = int(ufwd_base)
         o = self.op()
         rc = self.lib.tp_cn2d_march(ctypes.byref(o), _ptr(fs.buf), ctypes.byref(a), _stream(self.device))
         _native.check(rc, "tp_cn2d_march")
 
     # ------------------------------------------------------------ helpers
-    def new_store(self, num_probes: int) -> torch.Tensor:
-        return torch.empty((num_probes, self.nz, self.npad), dtype=torch.complex64, device=self.device)
+    def new_store(self, num_probes: int, slices: Optional[int] = None) -> torch.Tensor:
+        s = self.nz if slices is None else int(slices)
+        return torch.empty((num_probes, s, self.npad), dtype=torch.complex64, device=self.device)
 
     def unchunk(self, u_store: torch.Tensor) -> torch.Tensor:
         """Chunked (P, nz, Npad) → reference layout (P, N, nz)."""

@@ -380,16 +380,21 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
   auto slice_of = [&](int t) { return p.backward ? (p.L + 1 - t) : t; };
   if (tid == 0) {
     mbar_arrive_expect_tx(&mbar[1], (uint32_t)sb);
-    bulk_g2s(bufs + slice_f2, p.factors + (size_t)(slice_of(1) - 1) * sb, (uint32_t)sb, &mbar[1]);
+    bulk_g2s(bufs + slice_f2, p.factors + (size_t)(slice_of(p.t0) - 1) * sb, (uint32_t)sb, &mbar[1]);
   }
 
   float2 U[M];
 #pragma unroll
   for (int i = 0; i < M; ++i) U[i] = make_float2(0.f, 0.f);
-  if (active && p.probes != nullptr) add_natural<M>(U, p.probes + (size_t)probe * p.N, lane, p.N);
-  if (active && p.u_store != nullptr) {
-    const int t0 = p.flip_out ? p.L : 0;
-    float2 *dst = p.u_store + ((size_t)probe * p.nz + t0) * p.Npad;
+  if (active && p.state_in != nullptr) {
+    const float2 *src = p.state_in + (size_t)probe * p.Npad;
+#pragma unroll
+    for (int i = 0; i < M; ++i) U[i] = src[i * 32 + lane];
+  } else if (active && p.probes != nullptr && p.t0 == 1) {
+    add_natural<M>(U, p.probes + (size_t)probe * p.N, lane, p.N);
+  }
+  if (active && p.u_store != nullptr && store_index(p, p.t0 - 1) >= 0) {
+    float2 *dst = p.u_store + ((size_t)probe * p.store_slices + store_index(p, p.t0 - 1)) * p.Npad;
 #pragma unroll
     for (int i = 0; i < M; ++i) dst[i * 32 + lane] = U[i];
   }
@@ -405,10 +410,10 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
     return;
   }
 
-  for (int t = 1; t <= p.L; ++t) {
-    const int cb = t & 1;
+  for (int t = p.t0; t <= p.t1; ++t) {
+    const int cb = (t - p.t0 + 1) & 1;
     const int s = slice_of(t);
-    if (tid == 0 && t < p.L) {
+    if (tid == 0 && t < p.t1) {
       fence_proxy_async_smem();
       mbar_arrive_expect_tx(&mbar[cb ^ 1], (uint32_t)sb);
       bulk_g2s(bufs + (cb ^ 1) * slice_f2, p.factors + (size_t)(slice_of(t + 1) - 1) * sb, (uint32_t)sb,
@@ -424,9 +429,8 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
       }
       if (t == 1 && p.src_exit != nullptr) add_natural<M>(U, p.src_exit + (size_t)probe * p.N, lane, p.N);
       cn2d_solve<M, ALIGNED>(U, F, lane, p);
-      if (p.u_store != nullptr) {
-        const int to = p.flip_out ? (p.L - t) : t;
-        float2 *dst = p.u_store + ((size_t)probe * p.nz + to) * p.Npad;
+      if (p.u_store != nullptr && store_index(p, t) >= 0) {
+        float2 *dst = p.u_store + ((size_t)probe * p.store_slices + store_index(p, t)) * p.Npad;
 #pragma unroll
         for (int i = 0; i < M; ++i) dst[i * 32 + lane] = U[i];
       }
@@ -439,7 +443,7 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
         }
       }
       if (do_grad) {
-        const float2 *ua = p.u_fwd + ((size_t)probe * p.nz + s) * p.Npad;
+        const float2 *ua = p.u_fwd + ((size_t)probe * p.ufwd_slices + (s - p.ufwd_base)) * p.Npad;
         const float2 *ub = ua - p.Npad;
         float2 *ga = gacc + cb * M * 33;
 #pragma unroll
@@ -453,7 +457,7 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
       if constexpr (LAGGED) cn2d_rhs<M, ALIGNED>(U, F, lane, p);
     }
     bool good = true;
-    if (t < p.L) {
+    if (t < p.t1) {
       good = mbar_wait_bounded(&mbar[cb ^ 1], (phase >> (cb ^ 1)) & 1u, p.err);
       phase ^= (1u << (cb ^ 1));
     }
@@ -473,6 +477,11 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
         ga[i * 33 + k] = make_float2(0.f, 0.f);
       }
     }
+  }
+  if (active && p.state_out != nullptr) {
+    float2 *dst = p.state_out + (size_t)probe * p.Npad;
+#pragma unroll
+    for (int i = 0; i < M; ++i) dst[i * 32 + lane] = U[i];
   }
 }
 
@@ -751,6 +760,18 @@ extern "C" int tp_cn2d_march(const tp_cn2d_op *op, const void *factors, const tp
   mp.u_fwd = static_cast<const float2 *>(a->u_fwd);
   mp.grad_c = static_cast<float2 *>(a->grad_c);
   mp.err = err;
+  mp.t0 = a->t_begin > 0 ? a->t_begin : 1;
+  mp.t1 = a->t_end > 0 ? a->t_end : mp.L;
+  if (mp.t0 > mp.t1 || mp.t1 > mp.L) return set_error(TP_ERR_INVALID, "bad step range [%d, %d] (L=%d)", mp.t0, mp.t1, mp.L);
+  if (mp.flip_out && (mp.t0 != 1 || mp.t1 != mp.L) && a->u_store != nullptr)
+    return set_error(TP_ERR_INVALID, "the flipped ADJOINT store needs the full step range");
+  mp.state_in = static_cast<const float2 *>(a->state_in);
+  mp.state_out = static_cast<float2 *>(a->state_out);
+  mp.store_slices = a->store_slices > 0 ? a->store_slices : op->nz;
+  mp.store_every = a->store_every;
+  mp.store_base = a->store_base;
+  mp.ufwd_slices = a->ufwd_slices > 0 ? a->ufwd_slices : op->nz;
+  mp.ufwd_base = a->ufwd_base;
   if (pt.team) {
     if (op->k_off[0] != 0.0 || op->k_01[0] != 0.0 || op->k_nm[0] != 0.0)
       return set_error(TP_ERR_UNSUPPORTED,

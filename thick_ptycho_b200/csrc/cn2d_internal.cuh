@@ -76,7 +76,24 @@ struct MarchParams {
   const float2 *u_fwd;
   float2 *grad_c;
   int *err;
+  int t0, t1;                   // step range
+  const float2 *state_in;       // chunked (P, Npad) or null
+  float2 *state_out;
+  int store_slices, store_every, store_base;
+  int ufwd_slices, ufwd_base;
 };
+
+// Index in u_store of the state after step t (t0-1 = the initial state), or -1.
+__host__ __device__ inline int store_index(const MarchParams &p, int t) {
+  int idx;
+  if (p.store_every > 1) {
+    if (t % p.store_every != 0) return -1;
+    idx = t / p.store_every;
+  } else {
+    idx = p.flip_out ? (p.L - t) : (t - p.store_base);
+  }
+  return (idx >= 0 && idx < p.store_slices) ? idx : -1;
+}
 
 // Spike rows kept by the team path for operator `op` with M rows per chunk:
 // the inverse of a diagonally dominant tridiagonal matrix decays like rho^d,

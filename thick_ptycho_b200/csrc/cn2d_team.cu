@@ -228,25 +228,34 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
     for (int e = tid; e < 2 * M * (C + 1); e += NT) GB[e] = make_float2(0.f, 0.f);
   __syncthreads();
   auto slice_of = [&](int t) { return p.backward ? (p.L + 1 - t) : t; };
-  if (tid == 0) team_issue(bufs + ssf, p.factors + (size_t)(slice_of(1) - 1) * p.slice_bytes, M, T, &mbar[1]);
+  if (tid == 0) team_issue(bufs + ssf, p.factors + (size_t)(slice_of(p.t0) - 1) * p.slice_bytes, M, T, &mbar[1]);
 
   float2 U[Q][M];
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
 #pragma unroll
     for (int i = 0; i < M; ++i) U[q][i] = make_float2(0.f, 0.f);
-    if (p.probes != nullptr && p0 + q < p.P) {
+    if (p0 + q >= p.P) continue;
+    if (p.state_in != nullptr) {
+      const float4 *src = reinterpret_cast<const float4 *>(p.state_in + (size_t)(p0 + q) * p.Npad) + c;
+#pragma unroll
+      for (int j = 0; j < M / 2; ++j) {
+        const float4 v = src[j * C];
+        U[q][2 * j] = make_float2(v.x, v.y);
+        U[q][2 * j + 1] = make_float2(v.z, v.w);
+      }
+    } else if (p.probes != nullptr && p.t0 == 1) {
       const float2 *src = p.probes + (size_t)(p0 + q) * p.N + c * M;
 #pragma unroll
       for (int i = 0; i < M; ++i) U[q][i] = src[i];
     }
   }
-  if (p.u_store != nullptr) {
-    const int t0 = p.flip_out ? p.L : 0;
+  if (p.u_store != nullptr && store_index(p, p.t0 - 1) >= 0) {
+    const int idx = store_index(p, p.t0 - 1);
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       if (p0 + q >= p.P) continue;
-      store_pairs(p.u_store + ((size_t)(p0 + q) * p.nz + t0) * p.Npad, U[q], M, c);
+      store_pairs(p.u_store + ((size_t)(p0 + q) * p.store_slices + idx) * p.Npad, U[q], M, c);
     }
   }
 
@@ -261,10 +270,10 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
     }
   }
 
-  for (int t = 1; t <= p.L; ++t) {
-    const int cb = t & 1;
+  for (int t = p.t0; t <= p.t1; ++t) {
+    const int cb = (t - p.t0 + 1) & 1;
     const int s = slice_of(t);
-    if (tid == 0 && t < p.L) {
+    if (tid == 0 && t < p.t1) {
       fence_proxy_async_smem();
       team_issue(bufs + (cb ^ 1) * ssf, p.factors + (size_t)(slice_of(t + 1) - 1) * p.slice_bytes, M, T,
                  &mbar[cb ^ 1]);
@@ -293,12 +302,12 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
       }
     }
     team_solve<M, Q>(U, F, T, Y0, R0, R1, XS, c, team, p.sp);
-    if (p.u_store != nullptr) {
-      const int to = p.flip_out ? (p.L - t) : t;
+    if (p.u_store != nullptr && store_index(p, t) >= 0) {
+      const int idx = store_index(p, t);
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         if (p0 + q >= p.P) continue;
-        store_pairs(p.u_store + ((size_t)(p0 + q) * p.nz + to) * p.Npad, U[q], M, c);
+        store_pairs(p.u_store + ((size_t)(p0 + q) * p.store_slices + idx) * p.Npad, U[q], M, c);
       }
     }
     if (t == p.L && p.exit_out != nullptr) {
@@ -318,7 +327,8 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
       for (int q = 0; q < Q; ++q) {
         const bool ok = p0 + q < p.P;
         const float4 *ua =
-            reinterpret_cast<const float4 *>(p.u_fwd + ((size_t)(ok ? p0 + q : 0) * p.nz + s) * p.Npad) + c;
+            reinterpret_cast<const float4 *>(p.u_fwd + ((size_t)(ok ? p0 + q : 0) * p.ufwd_slices + (s - p.ufwd_base)) *
+                                                           p.Npad) + c;
         const float4 *ub = ua - p.Npad / 2;
 #pragma unroll
         for (int j = 0; j < M / 2; ++j) {
@@ -346,7 +356,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
     }
     if constexpr (LAGGED) team_rhs<M, Q>(U, F, XL, XF, c, team, p.sp);
     bool good = true;
-    if (t < p.L) {
+    if (t < p.t1) {
       good = mbar_wait_bounded(&mbar[cb ^ 1], (phase >> (cb ^ 1)) & 1u, p.err);
       phase ^= (1u << (cb ^ 1));
     }
@@ -367,6 +377,13 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
           gi[e] = 0.f;
         }
       }
+    }
+  }
+  if (p.state_out != nullptr) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      if (p0 + q >= p.P) continue;
+      store_pairs(p.state_out + (size_t)(p0 + q) * p.Npad, U[q], M, c);
     }
   }
 }

@@ -12,7 +12,8 @@ Gradients follow torch's complex convention ``∂ℓ/∂Re + i ∂ℓ/∂Im``.
 
 from __future__ import annotations
 
-from typing import Optional
+import math
+from typing import Optional, Union
 
 import numpy as np
 import torch
@@ -47,9 +48,14 @@ class PWEGradient2D:
 
     ``geometry`` is a reference ``SimulationSpace2D`` or a
     :class:`~thick_ptycho_b200.geometry.SimulationGeometry`.
+
+    ``checkpoint``: ``"sqrt"`` keeps the field every ⌈√L⌉ slices during the
+    forward march and recomputes each segment before its adjoint sweep
+    (memory ∝ √L per probe, one extra forward march); ``None`` keeps every
+    slice (memory ∝ L, fastest); an int sets the checkpoint spacing.
     """
 
-    def __init__(self, geometry, bc_type="impedance", device=None):
+    def __init__(self, geometry, bc_type="impedance", device=None, checkpoint: Union[str, int, None] = None):
         self.geometry = geometry
         self.engine = CN2D(
             geometry.block_size, geometry.nz, geometry.k, geometry.dx, geometry.dz, bc_type,
@@ -57,31 +63,81 @@ class PWEGradient2D:
             exact_ref_coeff=bool(getattr(geometry, "exact_ref_coeff", False)), device=device,
         )
         self.device = self.engine.device
+        L = self.engine.L
+        if checkpoint == "sqrt":
+            self.ckpt = max(1, math.ceil(math.sqrt(L)))
+        elif checkpoint is None or checkpoint == 0:
+            self.ckpt = 0
+        else:
+            self.ckpt = int(checkpoint)
+        if self.ckpt >= L:
+            self.ckpt = 0
         self._ff = self.engine.new_factor_buffer()
         self._fa = self.engine.new_factor_buffer()
-        self._store = None
-        self._grad_c = torch.empty((self.engine.L, self.engine.n), dtype=torch.complex64, device=self.device)
+        self._bufs = {}
+        self._grad_c = torch.empty((L, self.engine.n), dtype=torch.complex64, device=self.device)
 
-    def _store_for(self, P):
-        if self._store is None or self._store.shape[0] != P:
-            self._store = self.engine.new_store(P)
-        return self._store
+    def _buf(self, name, P, slices):
+        b = self._bufs.get(name)
+        if b is None or b.shape[0] != P or b.shape[1] != slices:
+            b = self.engine.new_store(P, slices)
+            self._bufs[name] = b
+        return b
+
+    def field_bytes(self, P) -> int:
+        """Device bytes of the stored forward field for P probes."""
+        e = self.engine
+        if not self.ckpt:
+            return P * e.nz * e.npad * 8
+        return P * (e.L // self.ckpt + 1 + self.ckpt + 1 + 2) * e.npad * 8
 
     def forward(self, field: torch.Tensor, probes: torch.Tensor, is_delta=False, exit_out=None):
-        """Forward march storing the full field; returns (factor set, exit)."""
+        """Forward march keeping the field (every slice, or the checkpoints)."""
         P = probes.shape[0]
-        fs = self.engine.factor(field, "forward", is_delta, out=self._ff)
-        ex = exit_out if exit_out is not None else torch.empty((P, self.engine.n), dtype=torch.complex64, device=self.device)
-        self.engine.march(fs, P, probes=probes, u_store=self._store_for(P), exit_out=ex)
+        e = self.engine
+        fs = e.factor(field, "forward", is_delta, out=self._ff)
+        ex = exit_out if exit_out is not None else torch.empty((P, e.n), dtype=torch.complex64, device=self.device)
+        if not self.ckpt:
+            e.march(fs, P, probes=probes, u_store=self._buf("full", P, e.nz), exit_out=ex)
+        else:
+            ck = self._buf("ckpt", P, e.L // self.ckpt + 1)
+            e.march(fs, P, probes=probes, u_store=ck, store_every=self.ckpt, exit_out=ex)
+        self._fs_fwd = fs
         return ex
 
     def backward(self, field: torch.Tensor, exit_grad: torch.Tensor, is_delta=False) -> torch.Tensor:
-        """Exact adjoint from the exit-wave gradient; returns ∂ℓ/∂n (n_obj, nz)."""
+        """Exact adjoint from the exit-wave gradient; returns ∂ℓ/∂n (n_obj, nz).
+
+        Must follow :meth:`forward` with the same field (it reuses the kept
+        field and, when checkpointing, the forward factor set).
+        """
         P = exit_grad.shape[0]
-        fa = self.engine.factor(field, "adjoint_exact", is_delta, out=self._fa)
+        e = self.engine
+        fa = e.factor(field, "adjoint_exact", is_delta, out=self._fa)
         self._grad_c.zero_()
-        self.engine.march(fa, P, src_exit=exit_grad.contiguous(), u_fwd=self._store_for(P), grad_c=self._grad_c)
-        return self.engine.grad_to_n(self._grad_c, field if self.engine.exact_ref_coeff else None, is_delta)
+        src = exit_grad.contiguous()
+        if not self.ckpt:
+            e.march(fa, P, src_exit=src, u_fwd=self._buf("full", P, e.nz), grad_c=self._grad_c)
+        else:
+            S, L = self.ckpt, e.L
+            ck = self._bufs["ckpt"]
+            seg = self._buf("segment", P, S + 1)
+            state = [self._buf("state0", P, 1)[:, 0], self._buf("state1", P, 1)[:, 0]]
+            start = self._buf("start", P, 1)[:, 0]
+            nseg = -(-L // S)
+            first = True
+            for k in reversed(range(nseg)):
+                a, b = k * S, min(k * S + S, L)
+                start.copy_(ck[:, a // S])
+                # recompute u_a .. u_b of this segment (indices 0 .. b - a)
+                e.march(self._fs_fwd, P, t_begin=a + 1, t_end=b, state_in=start, u_store=seg, store_base=a)
+                # adjoint steps for slices b .. a+1 (step t = L + 1 - s)
+                e.march(fa, P, t_begin=L + 1 - b, t_end=L - a, src_exit=src if first else None,
+                        state_in=None if first else state[0], state_out=state[1], u_fwd=seg, ufwd_base=a,
+                        grad_c=self._grad_c)
+                state.reverse()
+                first = False
+        return e.grad_to_n(self._grad_c, field if e.exact_ref_coeff else None, is_delta)
 
     def loss_and_grad(self, n, probes, amplitude, grad_out: Optional[torch.Tensor] = None):
         """One forward + adjoint pass: ``(loss, ∂loss/∂n)``.
