@@ -51,6 +51,18 @@ __device__ __forceinline__ void store_pairs(float2 *dst, const float2 *U, int M,
     reinterpret_cast<float4 *>(dst)[j * kTeamChunks + c] = make_float4(U[2 * j].x, U[2 * j].y, U[2 * j + 1].x, U[2 * j + 1].y);
 }
 
+// Load thread c's M rows of one stored slice (row pairs).
+template <int M>
+__device__ __forceinline__ void load_pairs(float2 (&dst)[M], const float2 *slice, int c) {
+  const float4 *src = reinterpret_cast<const float4 *>(slice) + c;
+#pragma unroll
+  for (int j = 0; j < M / 2; ++j) {
+    const float4 v = src[j * kTeamChunks];
+    dst[2 * j] = make_float2(v.x, v.y);
+    dst[2 * j + 1] = make_float2(v.z, v.w);
+  }
+}
+
 __host__ __device__ inline size_t team_slice_smem(int M, int T) {
   return (size_t)(3 * M + 2 * T + 3 + 2 * kTeamLevels) * kTeamChunks * sizeof(float2);
 }
@@ -259,6 +271,18 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
     }
   }
 
+  // Gradient: the forward slice u_s of the current step is kept from the
+  // previous step (u_prev); only u_{s-1} is read, issued at the start of the
+  // step so that its latency overlaps the solve.
+  float2 u_prev[Q][M], u_new[Q][M];
+  if (do_grad) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int pq = (p0 + q < p.P) ? p0 + q : p.P - 1;
+      load_pairs<M>(u_prev[q], p.u_fwd + ((size_t)pq * p.ufwd_slices + (slice_of(p.t0) - p.ufwd_base)) * p.Npad, c);
+    }
+  }
+
   uint32_t phase = 0;
   {
     const bool ok = mbar_wait_bounded(&mbar[1], 0, p.err);
@@ -279,6 +303,13 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
                  &mbar[cb ^ 1]);
     }
     const float2 *F = bufs + cb * ssf;
+    if (do_grad) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int pq = (p0 + q < p.P) ? p0 + q : p.P - 1;
+        load_pairs<M>(u_new[q], p.u_fwd + ((size_t)pq * p.ufwd_slices + (s - 1 - p.ufwd_base)) * p.Npad, c);
+      }
+    }
     if constexpr (!LAGGED) team_rhs<M, Q>(U, F, XL, XF, c, team, p.sp);
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
@@ -325,17 +356,11 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
       float2 w[Q][M];
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
-        const bool ok = p0 + q < p.P;
-        const float4 *ua =
-            reinterpret_cast<const float4 *>(p.u_fwd + ((size_t)(ok ? p0 + q : 0) * p.ufwd_slices + (s - p.ufwd_base)) *
-                                                           p.Npad) + c;
-        const float4 *ub = ua - p.Npad / 2;
+        const bool ok = p0 + q < p.P;  // padded probes contribute nothing
 #pragma unroll
-        for (int j = 0; j < M / 2; ++j) {
-          const float4 a = ok ? ua[j * C] : make_float4(0.f, 0.f, 0.f, 0.f);
-          const float4 b = ok ? ub[j * C] : make_float4(0.f, 0.f, 0.f, 0.f);
-          w[q][2 * j] = make_float2(a.x + b.x, a.y + b.y);
-          w[q][2 * j + 1] = make_float2(a.z + b.z, a.w + b.w);
+        for (int i = 0; i < M; ++i) {
+          w[q][i] = ok ? cadd(u_prev[q][i], u_new[q][i]) : make_float2(0.f, 0.f);
+          u_prev[q][i] = u_new[q][i];
         }
       }
       float *gr = reinterpret_cast<float *>(GB) + cb * 2 * M * (C + 1);  // [re|im][M][C+1]
@@ -401,12 +426,14 @@ static int launch_team_t(const Partition &pt, MarchParams &mp, cudaStream_t st) 
 
 template <int M, bool LAGGED>
 static int launch_team_qt(const Partition &pt, MarchParams &mp, int Q, int TM, cudaStream_t st) {
-  if (TM == 1 && Q == 4) return launch_team_t<M, 4, 1, LAGGED>(pt, mp, st);
-  if (TM == 1 && Q == 2) return launch_team_t<M, 2, 1, LAGGED>(pt, mp, st);
   if (TM == 1 && Q == 1) return launch_team_t<M, 1, 1, LAGGED>(pt, mp, st);
-  if (TM == 2 && Q == 2) return launch_team_t<M, 2, 2, LAGGED>(pt, mp, st);
   if (TM == 2 && Q == 1) return launch_team_t<M, 1, 2, LAGGED>(pt, mp, st);
   if (TM == 4 && Q == 1) return launch_team_t<M, 1, 4, LAGGED>(pt, mp, st);
+  if constexpr (!LAGGED) {
+    if (TM == 1 && Q == 4) return launch_team_t<M, 4, 1, LAGGED>(pt, mp, st);
+    if (TM == 1 && Q == 2) return launch_team_t<M, 2, 1, LAGGED>(pt, mp, st);
+    if (TM == 2 && Q == 2) return launch_team_t<M, 2, 2, LAGGED>(pt, mp, st);
+  }
   return set_error(TP_ERR_UNSUPPORTED, "no team kernel for Q=%d, TM=%d", Q, TM);
 }
 
@@ -438,7 +465,14 @@ int launch_team_march(const Partition &pt, MarchParams &mp, bool lagged, cudaStr
   int K = 1;
   while (K < 4 && (mp.P + K - 1) / K > sms) K *= 2;
   int TM, Q;
-  team_shape(K, &TM, &Q);
+  if (lagged) {
+    // one probe per thread: the kept and prefetched forward slices need 2M
+    // complex registers per probe on top of the state
+    TM = K;
+    Q = 1;
+  } else {
+    team_shape(K, &TM, &Q);
+  }
   while (team_smem_bytes(pt, mp.trunc, Q, TM, grad) > (size_t)max_smem && TM * Q > 1) {
     if (TM > 1) TM /= 2;
     else Q /= 2;
