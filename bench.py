@@ -229,7 +229,7 @@ def run_ours(a):
     amp_d = torch.from_numpy(amp).to(dev)
     ex = torch.empty((P, N), dtype=torch.complex64, device=dev)
     store = eng.new_store(P)
-    gc = torch.empty((L, N), dtype=torch.complex64, device=dev)
+    gc = eng.new_grad_buffer()
     ff_buf, fa_buf = eng.new_factor_buffer(), eng.new_factor_buffer()
     stream = torch.cuda.current_stream(dev)
     ev = {k: [] for k in ("fwd", "adj")}

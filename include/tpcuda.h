@@ -100,8 +100,9 @@ typedef struct tp_cn2d_march_args {
   void *exit_out;            /* float2 (P, N) last-step field, or NULL        */
   const void *u_fwd;         /* ADJOINT_EXACT + gradient: forward full field
                                 (chunked, as written by a FORWARD march)      */
-  void *grad_c;              /* ADJOINT_EXACT: float2 (L, N) accumulator of
-                                sum_p lambda_s * conj(u_s + u_{s-1}); the caller
+  void *grad_c;              /* ADJOINT_EXACT: float2 (L, Npad) accumulator of
+                                sum_p lambda_s * conj(u_s + u_{s-1}) in the
+                                chunked layout of tp_cn2d_layout; the caller
                                 zeroes it; row s-1 holds slice s               */
   /* Partial marches (checkpointed gradients).  All zero = one march over all
    * L steps storing every slice at its own index. */
@@ -149,7 +150,8 @@ TP_API int tp_cn2d_march(const tp_cn2d_op *op, const void *factors, const tp_cn2
                   tp_stream_t stream);
 
 /*
- * Map the per-step gradient sum_p lambda_s conj(u_s + u_{s-1}) (L, N) onto the
+ * Map the per-step gradient sum_p lambda_s conj(u_s + u_{s-1}) (L, Npad,
+ * chunked layout as written by tp_cn2d_march) onto the
  * refractive-index nodes (n_obj, nz) (torch convention d/dRe + i d/dIm):
  * g_n[x, t] = conj((dz/4) coef'(n[x,t])) * (g_c[t] + g_c[t+1]).
  * `n_field` is needed only when exact_ref_coeff is set (else may be NULL).

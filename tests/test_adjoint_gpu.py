@@ -72,12 +72,12 @@ def _gpu_grad(k, dx, dz, n, probes, amp, bc, N, nz):
     mag = U.abs()
     a = torch.from_numpy(amp).cuda()
     ge = N * torch.fft.ifft(2 * (mag - a) * U / mag, dim=-1)
-    gc = torch.zeros((nz - 1, N), dtype=torch.complex64, device="cuda")
+    gc = eng.new_grad_buffer()
     lam_st = eng.new_store(P)
     eng.march(fa, P, src_exit=ge.to(torch.complex64).contiguous(), u_store=lam_st, u_fwd=st, grad_c=gc)
     gn = eng.grad_to_n(gc)
     eng.device_status()
-    return gc.cpu().numpy().T, gn.cpu().numpy(), eng, lam_st
+    return eng.unchunk_rows(gc).cpu().numpy().T, gn.cpu().numpy(), eng, lam_st
 
 
 @pytest.mark.parametrize("bc", ["impedance", "neumann", "dirichlet"])

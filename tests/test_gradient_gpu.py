@@ -128,7 +128,7 @@ def test_reference_gradient_agreement(golden):
     pr = torch.from_numpy(g["probes"].astype(np.complex64)).cuda()
     pg.forward(field, pr)
     pg.backward(field, torch.from_numpy(g["exit_error"].astype(np.complex64)).cuda())
-    per_step = np.conj((dz / 2) * (k / 1j)) * pg._grad_c.cpu().numpy().T  # gradient w.r.t. a node-local step term
+    per_step = np.conj((dz / 2) * (k / 1j)) * pg.step_gradient().cpu().numpy().T  # gradient w.r.t. a node-local step term
     ref = (g["grad_re"] + 1j * g["grad_im"]).reshape(nz - 1, N).T
     cos = np.real(np.vdot(per_step, ref)) / np.linalg.norm(per_step) / np.linalg.norm(ref)
     assert cos >= 0.98, cos

@@ -134,7 +134,7 @@ class CN2D:
             "u_store": (u_store, None),
             "exit_out": (exit_out, (P, self.n)),
             "u_fwd": (u_fwd, None),
-            "grad_c": (grad_c, (self.L, self.n)),
+            "grad_c": (grad_c, (self.L, self.npad)),
             "state_in": (state_in, (P, self.npad)),
             "state_out": (state_out, (P, self.npad)),
         }
@@ -177,8 +177,27 @@ class CN2D:
         _native.check(rc, "tp_cn2d_unchunk")
         return out
 
+    def chunk_index(self) -> torch.Tensor:
+        """Offsets of matrix rows 0..N−1 within one chunked slice (Npad)."""
+        if getattr(self, "_chunk_idx", None) is None:
+            g = torch.arange(self.n)
+            i, k = g % self.rows_per_chunk, g // self.rows_per_chunk
+            if self.chunks == 128:
+                off = ((i // 2) * self.chunks + k) * 2 + (i % 2)
+            else:
+                off = i * self.chunks + k
+            self._chunk_idx = off.to(self.device)
+        return self._chunk_idx
+
+    def unchunk_rows(self, x: torch.Tensor) -> torch.Tensor:
+        """(..., Npad) chunked → (..., N) natural row order."""
+        return x.index_select(-1, self.chunk_index())
+
+    def new_grad_buffer(self) -> torch.Tensor:
+        return torch.zeros((self.L, self.npad), dtype=torch.complex64, device=self.device)
+
     def grad_to_n(self, grad_c: torch.Tensor, field: Optional[torch.Tensor] = None, is_delta=False) -> torch.Tensor:
-        """Σ_p λ conj(u_s + u_{s−1}) (L, N) → torch-convention gradient on n (n_obj, nz)."""
+        """Σ_p λ conj(u_s + u_{s−1}) (L, Npad chunked) → torch-convention gradient on n (n_obj, nz)."""
         out = torch.empty((self.n_obj, self.nz), dtype=torch.complex64, device=self.device)
         dtype = _native.C128
         if field is not None:

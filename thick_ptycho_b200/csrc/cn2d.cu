@@ -468,12 +468,13 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
       return;
     }
     if (do_grad) {
+      // gradient buffer in the chunked layout: row k*M + i at offset i*32 + k
       float2 *ga = gacc + cb * M * 33;
-      float2 *dst = p.grad_c + (size_t)(s - 1) * p.N;
-      for (int g = tid; g < p.N; g += blockDim.x) {
-        const int i = g % M, k = g / M;
+      float2 *dst = p.grad_c + (size_t)(s - 1) * p.Npad;
+      for (int e = tid; e < p.Npad; e += blockDim.x) {
+        const int i = e / 32, k = e % 32;
         const float2 v = ga[i * 33 + k];
-        asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(&dst[g]), "f"(v.x), "f"(v.y) : "memory");
+        asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(&dst[e]), "f"(v.x), "f"(v.y) : "memory");
         ga[i * 33 + k] = make_float2(0.f, 0.f);
       }
     }
@@ -505,6 +506,7 @@ __global__ void cn2d_unchunk_kernel(const float2 *__restrict__ st, float2 *__res
 
 struct GradParams {
   int N, L, nz, n_obj, empty_px, exact, is_delta, dtype;
+  int M, C, pair, Npad;
   double k, dz;
   const float2 *gc;
   const void *n;
@@ -517,13 +519,15 @@ __global__ void cn2d_grad_to_n_kernel(const GradParams q) {
     const int t = (int)(idx % q.nz);
     const int x = (int)(idx / q.nz);
     const int g = x + q.empty_px;
+    const int i = g % q.M, k = g / q.M;
+    const size_t off = q.pair ? ((size_t)(i >> 1) * q.C + k) * 2 + (i & 1) : (size_t)i * q.C + k;
     double2 acc = z2(0, 0);
     if (t >= 1) {
-      const float2 a = q.gc[(size_t)(t - 1) * q.N + g];
+      const float2 a = q.gc[(size_t)(t - 1) * q.Npad + off];
       acc = zadd(acc, z2(a.x, a.y));
     }
     if (t <= q.L - 1) {
-      const float2 b = q.gc[(size_t)t * q.N + g];
+      const float2 b = q.gc[(size_t)t * q.Npad + off];
       acc = zadd(acc, z2(b.x, b.y));
     }
     // dc/dn = (dz/4) coef'(n); coef' = k/i  or (k/i) n
@@ -801,7 +805,14 @@ extern "C" int tp_cn2d_grad_to_n(const tp_cn2d_op *op, const void *grad_c, const
   if (rc) return rc;
   if (grad_c == nullptr || grad_n == nullptr) return set_error(TP_ERR_INVALID, "grad_c/grad_n is NULL");
   if (op->exact_ref_coeff && n_field == nullptr) return set_error(TP_ERR_INVALID, "exact_ref_coeff needs n_field");
+  Partition pt;
+  rc = partition_for(op->n, &pt);
+  if (rc) return rc;
   GradParams q{};
+  q.M = pt.M;
+  q.C = pt.C;
+  q.pair = pt.team;
+  q.Npad = pt.C * pt.M;
   q.N = op->n;
   q.L = op->nz - 1;
   q.nz = op->nz;

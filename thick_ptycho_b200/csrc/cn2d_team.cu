@@ -14,8 +14,9 @@
 // operator and verified when factorising).
 //
 // Exact-adjoint gradient: the Q probes' contributions lambda*conj(u_s+u_{s-1})
-// are summed in registers, combined across the CTA's teams in shared memory
-// and flushed with one fire-and-forget vector reduction per row and CTA.
+// are summed in registers and added to the chunked gradient buffer with
+// fire-and-forget 16-byte vector reductions (one per row pair), coalesced
+// across the team; no shared-memory accumulator or flush stage is needed.
 #include "cn2d_internal.cuh"
 #include <stdio.h>
 #include <stdlib.h>
@@ -34,8 +35,9 @@ __device__ __forceinline__ void team_sync(int team) {
 __device__ __forceinline__ void red_add_v2(float2 *addr, float2 v) {
   asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(addr), "f"(v.x), "f"(v.y) : "memory");
 }
-__device__ __forceinline__ void red_add_shared(float *addr, float v) {
-  asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(smem_addr(addr)), "f"(v) : "memory");
+__device__ __forceinline__ void red_add_v4(float4 *addr, float4 v) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+               : "memory");
 }
 
 // b * i * z for real b (the off-diagonal of P is purely imaginary: i*dz/(4k dx^2)).
@@ -68,8 +70,8 @@ __host__ __device__ inline size_t team_slice_smem(int M, int T) {
 }
 
 size_t team_smem_bytes(const Partition &pt, int trunc, int Q, int TM, bool grad) {
-  return 2 * team_slice_smem(pt.M, trunc) + 6 * (size_t)TM * Q * kTeamChunks * sizeof(float2) +
-         (grad ? 2 * (size_t)pt.M * (kTeamChunks + 1) * sizeof(float2) : 0) + 2 * sizeof(uint64_t);
+  (void)grad;
+  return 2 * team_slice_smem(pt.M, trunc) + 6 * (size_t)TM * Q * kTeamChunks * sizeof(float2) + 2 * sizeof(uint64_t);
 }
 
 // Issue the bulk copies of one slice's factor set (QD|LF|EP, V head, W tail, records).
@@ -226,8 +228,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
   float2 *XL = reinterpret_cast<float2 *>(smem + 2 * ss) + (size_t)team * 6 * Q * C;
   float2 *XF = XL + Q * C, *Y0 = XF + Q * C, *R0 = Y0 + Q * C, *R1 = R0 + Q * C, *XS = R1 + Q * C;
   const bool do_grad = LAGGED && (p.grad_c != nullptr);
-  float2 *GB = reinterpret_cast<float2 *>(smem + 2 * ss) + (size_t)TM * 6 * Q * C;  // [2][M][C+1]
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(GB + (do_grad ? 2 * M * (C + 1) : 0));
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(reinterpret_cast<float2 *>(smem + 2 * ss) + (size_t)TM * 6 * Q * C);
   const size_t ssf = ss / sizeof(float2);
   const int p0 = (blockIdx.x * TM + team) * Q;
 
@@ -236,8 +237,6 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
     mbar_init(&mbar[1], 1);
     fence_mbar_init();
   }
-  if (do_grad)
-    for (int e = tid; e < 2 * M * (C + 1); e += NT) GB[e] = make_float2(0.f, 0.f);
   __syncthreads();
   auto slice_of = [&](int t) { return p.backward ? (p.L + 1 - t) : t; };
   if (tid == 0) team_issue(bufs + ssf, p.factors + (size_t)(slice_of(p.t0) - 1) * p.slice_bytes, M, T, &mbar[1]);
@@ -351,33 +350,26 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
       }
     }
     if (do_grad) {
-      // GB[cb] was zeroed by the flush two steps ago, which every thread
-      // finished before passing the previous step's closing barrier.
-      float2 w[Q][M];
+      float4 *gdst = reinterpret_cast<float4 *>(p.grad_c + (size_t)(s - 1) * p.Npad) + c;
 #pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        const bool ok = p0 + q < p.P;  // padded probes contribute nothing
+      for (int j = 0; j < M / 2; ++j) {
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-        for (int i = 0; i < M; ++i) {
-          w[q][i] = ok ? cadd(u_prev[q][i], u_new[q][i]) : make_float2(0.f, 0.f);
-          u_prev[q][i] = u_new[q][i];
+        for (int q = 0; q < Q; ++q) {
+          if (p0 + q >= p.P) continue;  // padded probes contribute nothing
+          const float2 a = cmulc(U[q][2 * j], cadd(u_prev[q][2 * j], u_new[q][2 * j]));
+          const float2 b = cmulc(U[q][2 * j + 1], cadd(u_prev[q][2 * j + 1], u_new[q][2 * j + 1]));
+          acc.x += a.x;
+          acc.y += a.y;
+          acc.z += b.x;
+          acc.w += b.y;
         }
+        red_add_v4(gdst + j * C, acc);
       }
-      float *gr = reinterpret_cast<float *>(GB) + cb * 2 * M * (C + 1);  // [re|im][M][C+1]
-      float *gi = gr + M * (C + 1);
 #pragma unroll
-      for (int i = 0; i < M; ++i) {
-        float2 acc = make_float2(0.f, 0.f);
+      for (int q = 0; q < Q; ++q)
 #pragma unroll
-        for (int q = 0; q < Q; ++q) acc = cadd(acc, cmulc(U[q][i], w[q][i]));
-        if constexpr (TM == 1) {
-          gr[i * (C + 1) + c] = acc.x;
-          gi[i * (C + 1) + c] = acc.y;
-        } else {
-          red_add_shared(&gr[i * (C + 1) + c], acc.x);
-          red_add_shared(&gi[i * (C + 1) + c], acc.y);
-        }
-      }
+        for (int i = 0; i < M; ++i) u_prev[q][i] = u_new[q][i];
     }
     if constexpr (LAGGED) team_rhs<M, Q>(U, F, XL, XF, c, team, p.sp);
     bool good = true;
@@ -389,19 +381,6 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
       if (tid == 0) mbar_wait_bounded(&mbar[cb ^ 1], ((phase >> (cb ^ 1)) & 1u) ^ 1u, nullptr);
       __syncthreads();
       return;
-    }
-    if (do_grad) {
-      float2 *dst = p.grad_c + (size_t)(s - 1) * p.N;
-      float *gr = reinterpret_cast<float *>(GB) + cb * 2 * M * (C + 1);
-      float *gi = gr + M * (C + 1);
-      for (int g = tid; g < p.N; g += NT) {
-        const int e = (g % M) * (C + 1) + g / M;
-        red_add_v2(&dst[g], make_float2(gr[e], gi[e]));
-        if constexpr (TM > 1) {
-          gr[e] = 0.f;
-          gi[e] = 0.f;
-        }
-      }
     }
   }
   if (p.state_out != nullptr) {

@@ -75,7 +75,7 @@ class PWEGradient2D:
         self._ff = self.engine.new_factor_buffer()
         self._fa = self.engine.new_factor_buffer()
         self._bufs = {}
-        self._grad_c = torch.empty((L, self.engine.n), dtype=torch.complex64, device=self.device)
+        self._grad_c = self.engine.new_grad_buffer()
 
     def _buf(self, name, P, slices):
         b = self._bufs.get(name)
@@ -138,6 +138,10 @@ class PWEGradient2D:
                 state.reverse()
                 first = False
         return e.grad_to_n(self._grad_c, field if e.exact_ref_coeff else None, is_delta)
+
+    def step_gradient(self) -> torch.Tensor:
+        """Σ_p λ_s conj(u_s + u_{s−1}) of the last backward pass, (L, N) natural rows."""
+        return self.engine.unchunk_rows(self._grad_c)
 
     def loss_and_grad(self, n, probes, amplitude, grad_out: Optional[torch.Tensor] = None):
         """One forward + adjoint pass: ``(loss, ∂loss/∂n)``.
