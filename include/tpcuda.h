@@ -181,6 +181,50 @@ TP_API int tp_cn2d_unchunk(const tp_cn2d_op *op, int32_t num_probes, const void 
 TP_API int tp_cn2d_march_noalloc(const tp_cn2d_op *op, const void *n_field, int32_t n_dtype,
                                  const tp_cn2d_march_args *args, tp_stream_t stream);
 
+/* ---------------------------------------------------------------- FFT heads
+ * Shared-memory mixed-radix FFTs: n = 2^a 3^b 5^c, n <= 4096; rows of n
+ * complex64 values, numpy conventions (forward unnormalised, inverse 1/n). */
+
+/* Batched 1D FFT of `batch` rows (in may equal out). Replaces numpy.fft.fft /
+ * ifft of base/base_solver.py:234-242 and base_reconstructor.py:191,205. */
+TP_API int tp_fft1d(int32_t n, int32_t batch, const void *in, void *out, int32_t inverse, tp_stream_t stream);
+
+/* Far-field intensities |FFT(exit)|^2 (float32, unnormalised, no shift):
+ * base/base_solver.py:234-242 without the Poisson noise. */
+TP_API int tp_farfield_intensity(int32_t n, int32_t batch, const void *exit_waves, float *intensity,
+                                 tp_stream_t stream);
+
+/* Amplitude loss sum (|F e| - a)^2 of exit waves e (batch, n) against the
+ * measured amplitudes a = sqrt(I) (float32), and its gradient w.r.t. e in
+ * torch's convention, F^H[2(|Fe| - a) Fe/|Fe|] = 2n (e - P_GS(e)) with P_GS
+ * the reference's modulus projection (base_reconstructor.py:171-207).
+ * *loss_out is accumulated (the caller zeroes it). */
+TP_API int tp_amplitude_residual(int32_t n, int32_t batch, const void *exit_waves, const float *amplitude,
+                                 void *grad_out, double *loss_out, tp_stream_t stream);
+
+/* ----------------------------------------------------------- multislice
+ * Angular-spectrum multislice of forward_model/multislice/ms_solver.py:49-159:
+ * u_{z+1} = IFFT(H . FFT(T_z u_z)), T_z = exp(i k (n[:,z] - n_medium) dz),
+ * H = exp(i (k_z - k) dz), k_z = sqrt(max(k^2 - k_x^2, 0)). */
+typedef struct tp_ms2d_op {
+  int32_t n;             /* transverse points, 2^a 3^b 5^c <= 4096 */
+  int32_t nz;            /* z nodes (L = nz - 1 steps) */
+  double k, dx, dz;
+  double n_medium[2];    /* background index (re, im) */
+} tp_ms2d_op;
+
+/* Transmission table T (L, n) complex64 from the index n (n, nz), dtype TP_C128/TP_C64. */
+TP_API int tp_ms2d_transmission(const tp_ms2d_op *op, const void *n_field, int32_t n_dtype, void *trans,
+                                tp_stream_t stream);
+/* March P probes (P, n); u_store (P, nz, n) or NULL; exit_out (P, n) or NULL. */
+TP_API int tp_ms2d_march(const tp_ms2d_op *op, const void *trans, const void *probes, int32_t num_probes,
+                         void *u_store, void *exit_out, tp_stream_t stream);
+/* Adjoint march from the exit-wave gradient src_exit (P, n) with the forward
+ * field u_fwd (P, nz, n); accumulates grad_t (L, n) += sum_p conj(T_z u_z) g_z,
+ * g_z = IFFT(conj(H) FFT(lambda_{z+1})).  d loss/d n[:, z] = conj(i k dz) grad_t[z]. */
+TP_API int tp_ms2d_backward(const tp_ms2d_op *op, const void *trans, const void *u_fwd, const void *src_exit,
+                            int32_t num_probes, void *grad_t, tp_stream_t stream);
+
 /* Synchronise `stream` and report device-side failures of earlier launches
  * (a bounded wait that gave up).  Returns TP_ERR_TIMEOUT and clears the flag
  * when one was recorded; *code receives the raw device code (0 = none). */

@@ -77,6 +77,17 @@ class TpCn2dMarchArgs(ctypes.Structure):
     ]
 
 
+class TpMs2dOp(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int32),
+        ("nz", ctypes.c_int32),
+        ("k", ctypes.c_double),
+        ("dx", ctypes.c_double),
+        ("dz", ctypes.c_double),
+        ("n_medium", ctypes.c_double * 2),
+    ]
+
+
 # (name, restype, argtypes) of every exported symbol of include/tpcuda.h
 SIGNATURES = [
     ("tp_cn2d_layout", ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
@@ -92,6 +103,18 @@ SIGNATURES = [
                                        ctypes.c_void_p]),
     ("tp_cn2d_march_noalloc", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_void_p, ctypes.c_int32,
                                              ctypes.POINTER(TpCn2dMarchArgs), ctypes.c_void_p]),
+    ("tp_fft1d", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                ctypes.c_void_p]),
+    ("tp_farfield_intensity", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p]),
+    ("tp_amplitude_residual", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("tp_ms2d_transmission", ctypes.c_int, [ctypes.POINTER(TpMs2dOp), ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                                            ctypes.c_void_p]),
+    ("tp_ms2d_march", ctypes.c_int, [ctypes.POINTER(TpMs2dOp), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("tp_ms2d_backward", ctypes.c_int, [ctypes.POINTER(TpMs2dOp), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
     ("tp_device_status", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ("tp_last_error_string", ctypes.c_char_p, []),
     ("tp_version", ctypes.c_int, []),

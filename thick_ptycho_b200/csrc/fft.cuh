@@ -1,0 +1,173 @@
+// Shared-memory mixed-radix (8, 4, 2, 3, 5) Stockham FFT for one CTA.
+//
+// A transform of length n = 2^a 3^b 5^c lives in shared memory; each pass of
+// radix R reads R values with stride n/R, applies the twiddles
+// W_{Ns R}^{r k} (k = j mod Ns, Ns = product of the previous radices), does
+// an R-point DFT in registers and writes them with stride Ns (autosort, so
+// the result is in natural order without a bit-reversal pass).  Twiddles
+// W_n^t = exp(-2 pi i t / n) are computed once per CTA in fp64 into shared
+// memory.  Forward transforms are unnormalised and inverse transforms are
+// scaled by 1/n, as numpy.fft.
+#pragma once
+
+#include "tp_common.cuh"
+
+namespace tp {
+
+constexpr int kFftMaxPasses = 12;
+constexpr int kFftMaxN = 4096;
+
+struct FftPlan {
+  int n;
+  int npass;
+  int radix[kFftMaxPasses];
+};
+
+// Host: radices of n (8s first, then 4, 2, 3, 5); npass = 0 if unsupported.
+inline FftPlan make_fft_plan(int n) {
+  FftPlan p{};
+  p.n = n;
+  int m = n, k = 0;
+  if (n < 1 || n > kFftMaxN) return p;
+  while (m % 8 == 0 && k < kFftMaxPasses) { p.radix[k++] = 8; m /= 8; }
+  while (m % 4 == 0 && k < kFftMaxPasses) { p.radix[k++] = 4; m /= 4; }
+  while (m % 2 == 0 && k < kFftMaxPasses) { p.radix[k++] = 2; m /= 2; }
+  while (m % 3 == 0 && k < kFftMaxPasses) { p.radix[k++] = 3; m /= 3; }
+  while (m % 5 == 0 && k < kFftMaxPasses) { p.radix[k++] = 5; m /= 5; }
+  p.npass = (m == 1) ? k : 0;
+  return p;
+}
+
+__device__ __forceinline__ void fft_twiddles(float2 *tw, int n, int tid, int nth) {
+  for (int t = tid; t < n; t += nth) {
+    double s, c;
+    sincospi(-2.0 * (double)t / (double)n, &s, &c);
+    tw[t] = make_float2((float)c, (float)s);
+  }
+}
+
+// R-point DFT in place (sign = -1 forward, +1 inverse).
+template <int R>
+__device__ __forceinline__ void dft_small(float2 (&v)[8], float sign);
+
+template <>
+__device__ __forceinline__ void dft_small<2>(float2 (&v)[8], float) {
+  const float2 a = v[0], b = v[1];
+  v[0] = cadd(a, b);
+  v[1] = csub(a, b);
+}
+
+// multiply by sign*i
+__device__ __forceinline__ float2 mul_si(float2 z, float sign) { return make_float2(-sign * z.y, sign * z.x); }
+
+template <>
+__device__ __forceinline__ void dft_small<4>(float2 (&v)[8], float sign) {
+  const float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+  const float2 b0 = cadd(v[1], v[3]), b1 = mul_si(csub(v[1], v[3]), sign);
+  v[0] = cadd(a0, b0);
+  v[2] = csub(a0, b0);
+  v[1] = cadd(a1, b1);
+  v[3] = csub(a1, b1);
+}
+
+template <>
+__device__ __forceinline__ void dft_small<8>(float2 (&v)[8], float sign) {
+  const float h = 0.70710678118654752440f;  // 1/sqrt(2)
+  float2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+  // 4-point DFTs of the even and odd samples
+  float2 a0 = cadd(e[0], e[2]), a1 = csub(e[0], e[2]), b0 = cadd(e[1], e[3]), b1 = mul_si(csub(e[1], e[3]), sign);
+  e[0] = cadd(a0, b0); e[2] = csub(a0, b0); e[1] = cadd(a1, b1); e[3] = csub(a1, b1);
+  a0 = cadd(o[0], o[2]); a1 = csub(o[0], o[2]); b0 = cadd(o[1], o[3]); b1 = mul_si(csub(o[1], o[3]), sign);
+  o[0] = cadd(a0, b0); o[2] = csub(a0, b0); o[1] = cadd(a1, b1); o[3] = csub(a1, b1);
+  // twiddles W8^k = exp(sign * i * pi k / 4)
+  const float2 w1 = make_float2(h, sign * h), w3 = make_float2(-h, sign * h);
+  o[1] = cmul(o[1], w1);
+  o[2] = mul_si(o[2], sign);
+  o[3] = cmul(o[3], w3);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    v[k] = cadd(e[k], o[k]);
+    v[k + 4] = csub(e[k], o[k]);
+  }
+}
+
+template <>
+__device__ __forceinline__ void dft_small<3>(float2 (&v)[8], float sign) {
+  const float s3 = 0.86602540378443864676f;  // sin(2 pi / 3)
+  const float2 t = cadd(v[1], v[2]);
+  const float2 d = mul_si(csub(v[1], v[2]), sign * s3);
+  const float2 m = make_float2(v[0].x - 0.5f * t.x, v[0].y - 0.5f * t.y);
+  v[0] = cadd(v[0], t);
+  v[1] = cadd(m, d);
+  v[2] = csub(m, d);
+}
+
+template <>
+__device__ __forceinline__ void dft_small<5>(float2 (&v)[8], float sign) {
+  const float c1 = 0.30901699437494742410f, c2 = -0.80901699437494742410f;  // cos(2pi/5), cos(4pi/5)
+  const float s1 = 0.95105651629515357212f, s2 = 0.58778525229247312917f;   // sin(2pi/5), sin(4pi/5)
+  const float2 a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+  const float2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+  const float2 x0 = v[0];
+  const float2 m1 = make_float2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
+  const float2 m2 = make_float2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
+  const float2 n1 = mul_si(make_float2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y), sign);
+  const float2 n2 = mul_si(make_float2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y), sign);
+  v[0] = cadd(x0, cadd(a1, a2));
+  v[1] = cadd(m1, n1);
+  v[4] = csub(m1, n1);
+  v[2] = cadd(m2, n2);
+  v[3] = csub(m2, n2);
+}
+
+template <int R>
+__device__ __forceinline__ void fft_pass(const float2 *a, float2 *b, int n, int Ns, const float2 *tw, float sign,
+                                         int nb, int tid, int nth) {
+  const int T = n / R;
+  const int step = n / (Ns * R);
+  for (int w = tid; w < nb * T; w += nth) {
+    const int bi = w / T, j = w - bi * T;
+    const float2 *src = a + bi * n;
+    float2 *dst = b + bi * n;
+    const int k = j % Ns;
+    float2 v[8];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[j + r * T];
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      const float2 t = tw[(r * k * step) % n];
+      v[r] = cmul(v[r], make_float2(t.x, sign < 0 ? t.y : -t.y));
+    }
+    dft_small<R>(v, sign);
+    const int idx = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[idx + r * Ns] = v[r];
+  }
+}
+
+// nb transforms of length pl.n stored back to back in `a` (scratch `b` of
+// the same size).  Returns the buffer holding the result (a or b).  Ends
+// with __syncthreads().
+__device__ __forceinline__ float2 *fft_block(float2 *a, float2 *b, const FftPlan &pl, const float2 *tw, bool inverse,
+                                             int nb, int tid, int nth) {
+  const float sign = inverse ? 1.f : -1.f;
+  int Ns = 1;
+  for (int ps = 0; ps < pl.npass; ++ps) {
+    const int R = pl.radix[ps];
+    switch (R) {
+      case 8: fft_pass<8>(a, b, pl.n, Ns, tw, sign, nb, tid, nth); break;
+      case 4: fft_pass<4>(a, b, pl.n, Ns, tw, sign, nb, tid, nth); break;
+      case 2: fft_pass<2>(a, b, pl.n, Ns, tw, sign, nb, tid, nth); break;
+      case 3: fft_pass<3>(a, b, pl.n, Ns, tw, sign, nb, tid, nth); break;
+      default: fft_pass<5>(a, b, pl.n, Ns, tw, sign, nb, tid, nth); break;
+    }
+    __syncthreads();
+    float2 *t = a;
+    a = b;
+    b = t;
+    Ns *= R;
+  }
+  return a;
+}
+
+}  // namespace tp

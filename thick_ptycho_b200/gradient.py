@@ -18,6 +18,7 @@ from typing import Optional, Union
 import numpy as np
 import torch
 
+from . import heads
 from .cn2d import CN2D
 
 
@@ -31,16 +32,10 @@ def amplitude_residual(exit_waves: torch.Tensor, amplitude: torch.Tensor):
     """Loss ``Σ(|F e| − a)²`` and its gradient w.r.t. e (torch convention).
 
     Equals ``2N(e − P_GS(e))`` with P_GS the reference's modulus projection
-    (``base_reconstructor.py:171-207``).  Computed in complex128.
+    (``base_reconstructor.py:171-207``); one fused libtpcuda kernel
+    (FFT, residual, inverse FFT) per row group.
     """
-    n = exit_waves.shape[-1]
-    U = torch.fft.fft(exit_waves.to(torch.complex128), dim=-1)
-    mag = U.abs()
-    a = amplitude.to(torch.float64)
-    loss = torch.sum((mag - a) ** 2)
-    safe = torch.where(mag > 0, mag, torch.ones_like(mag))
-    gU = torch.where(mag > 0, 2 * (mag - a) / safe, torch.zeros_like(mag)) * U
-    return loss, (n * torch.fft.ifft(gU, dim=-1)).to(torch.complex64)
+    return heads.amplitude_residual(exit_waves.contiguous(), amplitude)
 
 
 class PWEGradient2D:

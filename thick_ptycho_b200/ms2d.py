@@ -1,0 +1,166 @@
+"""Angular-spectrum multislice on the GPU (2D), drop-in for the reference's
+``MSForwardModelSolver`` (``forward_model/multislice/ms_solver.py:8-159``).
+
+The index field enters through a transmission table ``T_z = exp(ik(n_z −
+n_med)dz)`` built once per ``n`` in fp64; every probe is then marched through
+all slices inside one CTA (field in shared memory, FFTs by libtpcuda's
+mixed-radix shared-memory FFT).  :class:`MSFunction` gives the exit waves
+with the hand-written adjoint march as its backward.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _native, heads
+
+
+def _stream(device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _ptr(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+class MS2D:
+    """Multislice engine for one geometry (n transverse points, nz nodes)."""
+
+    def __init__(self, n, nz, k, dx, dz, n_medium=1.0, device=None):
+        if not torch.cuda.is_available():
+            raise _native.NativeLibraryError("MS2D needs a CUDA device (there is no CPU fallback)")
+        self.lib = _native.load()
+        self.device = torch.device(device if device is not None else "cuda")
+        self.n, self.nz, self.L = int(n), int(nz), int(nz) - 1
+        o = _native.TpMs2dOp()
+        o.n, o.nz, o.k, o.dx, o.dz = self.n, self.nz, float(k), float(dx), float(dz)
+        nm = complex(n_medium)
+        o.n_medium = (ctypes.c_double * 2)(nm.real, nm.imag)
+        self._op = o
+        self.k, self.dz = float(k), float(dz)
+
+    def transmission(self, field: torch.Tensor) -> torch.Tensor:
+        if tuple(field.shape) != (self.n, self.nz):
+            raise ValueError(f"index field has shape {tuple(field.shape)}, expected {(self.n, self.nz)}")
+        field = field.contiguous()
+        dt = _native.C128 if field.dtype == torch.complex128 else _native.C64
+        T = torch.empty((self.L, self.n), dtype=torch.complex64, device=self.device)
+        _native.check(self.lib.tp_ms2d_transmission(ctypes.byref(self._op), _ptr(field), dt, _ptr(T), _stream(self.device)),
+                      "tp_ms2d_transmission")
+        return T
+
+    def march(self, T, probes, u_store=None, exit_out=None):
+        P = probes.shape[0]
+        _native.check(self.lib.tp_ms2d_march(ctypes.byref(self._op), _ptr(T), _ptr(probes.contiguous()), P, _ptr(u_store),
+                                             _ptr(exit_out), _stream(self.device)), "tp_ms2d_march")
+
+    def backward(self, T, u_fwd, src_exit, grad_t):
+        P = src_exit.shape[0]
+        _native.check(self.lib.tp_ms2d_backward(ctypes.byref(self._op), _ptr(T), _ptr(u_fwd), _ptr(src_exit.contiguous()),
+                                                P, _ptr(grad_t), _stream(self.device)), "tp_ms2d_backward")
+
+    def grad_to_n(self, grad_t: torch.Tensor) -> torch.Tensor:
+        """(L, n) accumulator → torch-convention ∂loss/∂n of shape (n, nz)."""
+        g = torch.zeros((self.n, self.nz), dtype=torch.complex64, device=self.device)
+        g[:, :-1] = (np.conj(1j * self.k * self.dz) * grad_t).T
+        return g
+
+
+class MSFunction(torch.autograd.Function):
+    """``exit = MS(n)`` with the adjoint multislice march as backward."""
+
+    @staticmethod
+    def forward(ctx, field, probes, engine: MS2D):
+        P = probes.shape[0]
+        T = engine.transmission(field.detach())
+        st = torch.empty((P, engine.nz, engine.n), dtype=torch.complex64, device=engine.device)
+        ex = torch.empty((P, engine.n), dtype=torch.complex64, device=engine.device)
+        engine.march(T, probes.detach().to(torch.complex64), u_store=st, exit_out=ex)
+        ctx.save_for_backward(field)
+        ctx.engine, ctx.T, ctx.st = engine, T, st
+        return ex
+
+    @staticmethod
+    def backward(ctx, grad_exit):
+        (field,) = ctx.saved_tensors
+        e = ctx.engine
+        gt = torch.zeros((e.L, e.n), dtype=torch.complex64, device=e.device)
+        e.backward(ctx.T, ctx.st, grad_exit.to(torch.complex64).contiguous(), gt)
+        return e.grad_to_n(gt).to(field.dtype), None, None
+
+
+class MSGpuSolver:
+    """Drop-in for ``MSForwardModelSolver`` (2D) running on one B200."""
+
+    def __init__(self, simulation_space, ptycho_probes, results_dir="", use_logging=False, verbose=False, log=None,
+                 device=None):
+        ss = simulation_space
+        if ss.dimension == 3:
+            raise NotImplementedError("3D simulation space is not yet implemented for MSForwardModelSolver.")
+        self.simulation_space = ss
+        self.probes = ptycho_probes
+        self.verbose = verbose
+        self.effective_shape = tuple(ss.effective_shape)
+        self.block_size = ss.block_size
+        self.nz = ss.nz
+        self.nx_eff = getattr(ss, "effective_nx", ss.nx)
+        self.num_probes = ss.num_probes
+        self.num_projections = ss.num_projections
+        self.probe_angles = ss.probe_angles
+        self.num_angles = len(self.probe_angles)
+        self.n_medium = complex(getattr(ss, "n_medium", 1.0))
+        self.solver_type = self.__class__.__name__
+        self.engine = MS2D(self.nx_eff, self.nz, ss.k, ss.dx, ss.dz, self.n_medium, device=device)
+        self.device = self.engine.device
+
+    def reset_cache(self):
+        """Nothing is cached across calls (the transmission is rebuilt per ``n``)."""
+
+    def _field(self, n):
+        if n is None:
+            n = self.simulation_space.refractive_index_empty
+        if isinstance(n, torch.Tensor):
+            return n.to(self.device)
+        return torch.from_numpy(np.ascontiguousarray(n, dtype=np.complex128)).to(self.device)
+
+    def solve(self, n=None, mode="forward", rhs_block=None, probes=None, **kwargs) -> np.ndarray:
+        """All probes, shape (proj, angle, probes, nx, nz) complex128 (``base/base_solver.py:84-154``)."""
+        assert mode in {"forward", "adjoint", "reverse"}, f"Invalid mode: {mode!r}"
+        if mode != "forward":
+            raise AssertionError(f"Invalid mode: {mode}")  # the reference's MS accepts forward only here
+        probes = self.probes if probes is None else probes
+        count = self.num_angles * self.num_probes
+        T = self.engine.transmission(self._field(n))
+        pr = torch.from_numpy(np.ascontiguousarray(probes).reshape(count, self.nx_eff).astype(np.complex64)).to(self.device)
+        st = torch.empty((count, self.nz, self.nx_eff), dtype=torch.complex64, device=self.device)
+        self.engine.march(T, pr, u_store=st)
+        u = st.permute(0, 2, 1).cpu().numpy().astype(np.complex128)
+        out = np.zeros((self.num_projections, self.num_angles, self.num_probes, *self.effective_shape), dtype=complex)
+        out[0] = u.reshape(self.num_angles, self.num_probes, *self.effective_shape)
+        return out
+
+    def _solve_single_probe(self, scan_idx=0, proj_idx=0, n=None, mode="forward", probe=None, **kwargs):
+        assert mode in {"forward", "backward"}, f"Invalid mode: {mode}"
+        if probe is None:
+            probe = np.zeros(self.nx_eff, dtype=complex)
+        T = self.engine.transmission(self._field(n))
+        pr = torch.from_numpy(np.asarray(probe, dtype=np.complex64).reshape(1, -1)).to(self.device)
+        st = torch.empty((1, self.nz, self.nx_eff), dtype=torch.complex64, device=self.device)
+        self.engine.march(T, pr, u_store=st)
+        return st[0].T.cpu().numpy().astype(np.complex128)
+
+    def get_exit_waves(self, u=None) -> np.ndarray:
+        return u[..., -1].reshape((self.simulation_space.total_scans, self.simulation_space.block_size))
+
+    def get_farfield_intensities(self, u=None, exit_waves=None, poisson_noise=True) -> np.ndarray:
+        """``|FFT(exit)|²`` computed on the GPU (``base/base_solver.py:213-249``)."""
+        exit_waves = self.get_exit_waves(u=u) if exit_waves is None else exit_waves
+        ex = torch.from_numpy(np.ascontiguousarray(exit_waves).astype(np.complex64)).to(self.device)
+        inten = heads.farfield_intensity(ex).cpu().numpy().astype(np.float64)
+        if poisson_noise:
+            inten = np.random.poisson(inten)
+        return inten.reshape((self.simulation_space.total_scans, self.simulation_space.block_size))
