@@ -113,7 +113,10 @@ struct MsParams {
   float2 *grad_t;  // backward: (L, n) accumulator of sum_p conj(T_z u_z) g_z
 };
 
-// T_z[x] = exp(i k (n[x,z] - n_medium) dz), z = 0..L-1 (ms_solver.py:86-88)
+// T_z[x] - 1 with T_z[x] = exp(i k (n[x,z] - n_medium) dz), z = 0..L-1
+// (ms_solver.py:86-88).  The table holds the deviation from one, computed in
+// fp64 (expm1, -2 sin^2): T is 1 + O(k dn dz) and rounding it to fp32 every
+// slice would bias the march.
 __global__ void ms_transmission_kernel(const MsParams q, float2 *__restrict__ trans) {
   const size_t total = (size_t)q.L * q.n;
   for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
@@ -128,94 +131,133 @@ __global__ void ms_transmission_kernel(const MsParams q, float2 *__restrict__ tr
       nr = v.x;
       ni = v.y;
     }
-    const double ph = q.k * (nr - q.nmr) * q.dz, at = exp(-q.k * (ni - q.nmi) * q.dz);
-    double s, c;
+    const double ph = q.k * (nr - q.nmr) * q.dz, am1 = expm1(-q.k * (ni - q.nmi) * q.dz);
+    double s, c, sh, ch;
     sincos(ph, &s, &c);
-    trans[idx] = make_float2((float)(at * c), (float)(at * s));
+    sincos(0.5 * ph, &sh, &ch);
+    // e^a (c + i s) - 1 = (e^a - 1) c + (c - 1) + i e^a s,  c - 1 = -2 sin^2(ph/2)
+    trans[idx] = make_float2((float)(am1 * c - 2.0 * sh * sh), (float)((am1 + 1.0) * s));
   }
 }
 
-// H[j] = exp(i (kz - k) dz), kz = sqrt(max(k^2 - kx^2, 0)), kx = 2 pi fftfreq(n, dx) (ms_solver.py:49-72)
+// H[j] - 1 with H[j] = exp(i (kz - k) dz), kz = sqrt(max(k^2 - kx^2, 0)),
+// kx = 2 pi fftfreq(n, dx) (ms_solver.py:49-72); fp64, kept as the deviation
+// from one like the transmission.
 __device__ __forceinline__ void ms_kernel_H(float2 *H, const MsParams &q, int tid, int nth) {
   for (int j = tid; j < q.n; j += nth) {
     const int f = (j < (q.n + 1) / 2) ? j : j - q.n;
     const double kx = 2.0 * 3.14159265358979323846 * (double)f / ((double)q.n * q.dx);
     const double kz = sqrt(fmax(q.k * q.k - kx * kx, 0.0));
-    double s, c;
-    sincos((kz - q.k) * q.dz, &s, &c);
-    H[j] = make_float2((float)c, (float)s);
+    const double th = (kz - q.k) * q.dz;
+    double s, c, sh, ch;
+    sincos(th, &s, &c);
+    sincos(0.5 * th, &sh, &ch);
+    H[j] = make_float2((float)(-2.0 * sh * sh), (float)s);
   }
 }
 
 // One CTA marches `rows` probes through all slices (the field stays in
-// shared memory): psi <- IFFT(H . FFT(T_z . psi)).
+// shared memory).  Each slice is evaluated in delta form,
+//   X = psi + (T_z - 1) psi,   psi' = X + IFFT((H - 1) . FFT(X)),
+// so the FFT round-off scales with the small update instead of the field
+// (the same reason the CN march keeps "1 + eps" coefficients).  X stays in
+// registers: a thread owns elements tid + j*nth, j < kMsElems.
+constexpr int kMsElems = 32;  // rows * n <= kMsElems * kFftThreads
+
 __global__ void __launch_bounds__(kFftThreads) ms_march_kernel(const FftPlan pl, const MsParams q, int rows) {
   extern __shared__ __align__(16) float2 fsm[];
   const int n = q.n, tid = threadIdx.x, nth = blockDim.x;
   float2 *tw = fsm, *H = tw + n, *a = H + n, *b = a + rows * n;
   const int p0 = blockIdx.x * rows;
   const int nb = min(rows, q.P - p0);
+  const int tot = nb * n;
   fft_twiddles(tw, n, tid, nth);
   ms_kernel_H(H, q, tid, nth);
-  for (int e = tid; e < nb * n; e += nth) {
-    const float2 v = q.probes[(size_t)p0 * n + e];
-    a[e] = v;
-    if (q.u_store) q.u_store[((size_t)(p0 + e / n) * q.nz) * n + e % n] = v;
+  float2 X[kMsElems];
+#pragma unroll
+  for (int j = 0; j < kMsElems; ++j) {
+    const int e = tid + j * nth;
+    if (e < tot) {
+      X[j] = q.probes[(size_t)p0 * n + e];
+      if (q.u_store) q.u_store[((size_t)(p0 + e / n) * q.nz) * n + e % n] = X[j];
+    }
   }
   __syncthreads();
+  const float s = 1.f / (float)n;
   for (int z = 0; z < q.L; ++z) {
     const float2 *Tz = q.trans + (size_t)z * n;
-    for (int e = tid; e < nb * n; e += nth) a[e] = cmul(a[e], Tz[e % n]);
+#pragma unroll
+    for (int j = 0; j < kMsElems; ++j) {
+      const int e = tid + j * nth;
+      if (e < tot) {
+        X[j] = cfma(Tz[e % n], X[j], X[j]);
+        a[e] = X[j];
+      }
+    }
     __syncthreads();
     float2 *F = fft_block(a, b, pl, tw, false, nb, tid, nth);
     float2 *o = (F == a) ? b : a;
-    for (int e = tid; e < nb * n; e += nth) F[e] = cmul(F[e], H[e % n]);
+    for (int e = tid; e < tot; e += nth) F[e] = cmul(F[e], H[e % n]);
     __syncthreads();
     float2 *R = fft_block(F, o, pl, tw, true, nb, tid, nth);
-    const float s = 1.f / (float)n;
-    float2 *nxt = (R == a) ? a : b;  // keep the state in `a`
-    for (int e = tid; e < nb * n; e += nth) {
-      const float2 v = make_float2(R[e].x * s, R[e].y * s);
-      a[e] = v;
-      if (q.u_store) q.u_store[((size_t)(p0 + e / n) * q.nz + z + 1) * n + e % n] = v;
-      if (z == q.L - 1 && q.exit_out) q.exit_out[(size_t)p0 * n + e] = v;
+#pragma unroll
+    for (int j = 0; j < kMsElems; ++j) {
+      const int e = tid + j * nth;
+      if (e < tot) {
+        X[j] = make_float2(fmaf(R[e].x, s, X[j].x), fmaf(R[e].y, s, X[j].y));
+        if (q.u_store) q.u_store[((size_t)(p0 + e / n) * q.nz + z + 1) * n + e % n] = X[j];
+        if (z == q.L - 1 && q.exit_out) q.exit_out[(size_t)p0 * n + e] = X[j];
+      }
     }
-    (void)nxt;
     __syncthreads();
   }
 }
 
-// Adjoint march: g_z = IFFT(conj(H) . FFT(lambda_{z+1})); grad_t[z] += sum_p
-// conj(T_z u_z) g_z; lambda_z = conj(T_z) g_z, from lambda_{nz-1} = src_exit.
+// Adjoint march (delta form as the forward): g = lambda + IFFT(conj(H - 1) .
+// FFT(lambda)); grad_t[z] += sum_p g conj(T_z u_z); lambda <- conj(T_z) g,
+// from lambda = src_exit at the exit plane.
 __global__ void __launch_bounds__(kFftThreads) ms_backward_kernel(const FftPlan pl, const MsParams q, int rows) {
   extern __shared__ __align__(16) float2 fsm[];
   const int n = q.n, tid = threadIdx.x, nth = blockDim.x;
   float2 *tw = fsm, *H = tw + n, *a = H + n, *b = a + rows * n;
   const int p0 = blockIdx.x * rows;
   const int nb = min(rows, q.P - p0);
+  const int tot = nb * n;
   fft_twiddles(tw, n, tid, nth);
   ms_kernel_H(H, q, tid, nth);
-  for (int e = tid; e < nb * n; e += nth) a[e] = q.src_exit[(size_t)p0 * n + e];
+  float2 X[kMsElems];
+#pragma unroll
+  for (int j = 0; j < kMsElems; ++j) {
+    const int e = tid + j * nth;
+    if (e < tot) {
+      X[j] = q.src_exit[(size_t)p0 * n + e];
+      a[e] = X[j];
+    }
+  }
   __syncthreads();
+  const float s = 1.f / (float)n;
   for (int z = q.L - 1; z >= 0; --z) {
     float2 *F = fft_block(a, b, pl, tw, false, nb, tid, nth);
     float2 *o = (F == a) ? b : a;
-    for (int e = tid; e < nb * n; e += nth) F[e] = cmulc(F[e], H[e % n]);
+    for (int e = tid; e < tot; e += nth) F[e] = cmulc(F[e], H[e % n]);
     __syncthreads();
     float2 *G = fft_block(F, o, pl, tw, true, nb, tid, nth);
-    const float s = 1.f / (float)n;
     const float2 *Tz = q.trans + (size_t)z * n;
-    for (int x = tid; x < n; x += nth) {
-      const float2 t = Tz[x];
-      float2 acc = make_float2(0.f, 0.f);
-      for (int r = 0; r < nb; ++r) {
-        const float2 g = make_float2(G[r * n + x].x * s, G[r * n + x].y * s);
-        const float2 u = q.u_fwd[((size_t)(p0 + r) * q.nz + z) * n + x];
-        acc = cadd(acc, cmulc(g, cmul(t, u)));  // g * conj(T u)
-        a[r * n + x] = cmulc(g, t);              // conj(T) g
+    // g = X + s*G ; contribution g conj(T u); X <- conj(T) g = g + conj(T-1) g
+#pragma unroll
+    for (int j = 0; j < kMsElems; ++j) {
+      const int e = tid + j * nth;
+      if (e < tot) {
+        const float2 g = make_float2(fmaf(G[e].x, s, X[j].x), fmaf(G[e].y, s, X[j].y));
+        const float2 tm1 = Tz[e % n];
+        const float2 u = q.u_fwd[((size_t)(p0 + e / n) * q.nz + z) * n + e % n];
+        const float2 tu = cfma(tm1, u, u);
+        const float2 c = cmulc(g, tu);
+        float2 *dst = q.grad_t + (size_t)z * n + e % n;
+        asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(dst), "f"(c.x), "f"(c.y) : "memory");
+        X[j] = cadd(g, cmulc(g, tm1));
+        a[e] = X[j];
       }
-      float2 *dst = q.grad_t + (size_t)z * n + x;
-      asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(dst), "f"(acc.x), "f"(acc.y) : "memory");
     }
     __syncthreads();
   }
@@ -312,9 +354,12 @@ extern "C" int tp_ms2d_transmission(const tp_ms2d_op *op, const void *n_field, i
 }
 
 static int ms_rows(int n) {
-  // probes per CTA: the two field buffers of every probe plus H and the
-  // twiddles must fit in 200 KB of shared memory
-  int r = (200 * 1024 / (int)sizeof(float2) - 2 * n) / (2 * n);
+  // probes per CTA: every thread keeps kMsElems field values in registers,
+  // and the two FFT buffers per probe plus H and the twiddles must fit in
+  // 200 KB of shared memory
+  int r = (kMsElems * kFftThreads) / n;
+  const int rs = (200 * 1024 / (int)sizeof(float2) - 2 * n) / (2 * n);
+  if (rs < r) r = rs;
   if (r > 4) r = 4;
   return r;
 }

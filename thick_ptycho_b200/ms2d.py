@@ -1,8 +1,8 @@
 """Angular-spectrum multislice on the GPU (2D), drop-in for the reference's
 ``MSForwardModelSolver`` (``forward_model/multislice/ms_solver.py:8-159``).
 
-The index field enters through a transmission table ``T_z = exp(ik(n_z −
-n_med)dz)`` built once per ``n`` in fp64; every probe is then marched through
+The index field enters through a transmission table (``T_z − 1`` with
+``T_z = exp(ik(n_z − n_med)dz)``) built once per ``n`` in fp64; every probe is then marched through
 all slices inside one CTA (field in shared memory, FFTs by libtpcuda's
 mixed-radix shared-memory FFT).  :class:`MSFunction` gives the exit waves
 with the hand-written adjoint march as its backward.
