@@ -225,6 +225,50 @@ TP_API int tp_ms2d_march(const tp_ms2d_op *op, const void *trans, const void *pr
 TP_API int tp_ms2d_backward(const tp_ms2d_op *op, const void *trans, const void *u_fwd, const void *src_exit,
                             int32_t num_probes, void *grad_t, tp_stream_t stream);
 
+/* ------------------------------------------------------------------- 3D
+ * 3D problems (2D transverse, N = nf*nb rows, index i = b*nf + f, the
+ * flattening of kron(I_y, A_x) in operator_matrices.py:75-99): each slice is
+ * solved by FFT-preconditioned BiCGStab in delta form (see cn3d.cu), batched
+ * over probes, fp64 inner products.  Replaces the per-slice SuperLU of the 2D
+ * operator (iterative_lu.py:103-133) and the per-probe march (:138-197). */
+typedef struct tp_cn3d_op {
+  int32_t nf, nb, nz;        /* fast / block transverse sizes, z nodes          */
+  int32_t exact_ref_coeff;   /* coef = (k/2i)(n^2-1) instead of (k/i)(n-1)       */
+  int32_t field_is_delta;    /* the index array holds n - 1                     */
+  int32_t reserved;
+  double k, dz;
+  double mu_x[2], mu_y[2];   /* interior couplings of K (preconditioner symbol) */
+  const void *kc, *kw, *ke, *ks, *kn;  /* device float2 (N) diagonals of K:
+                                (K x)_i = c x_i + w x_{i-1} + e x_{i+1}
+                                        + s x_{i-nf} + n x_{i+nf}               */
+} tp_cn3d_op;
+
+typedef struct tp_cn3d_march_args {
+  int32_t num_probes, mode;  /* tp_mode                                          */
+  int32_t max_iter;          /* BiCGStab iterations per solve (0 = 20)           */
+  int32_t precond;           /* 1: periodic FFT preconditioner (when nf, nb are
+                                2^a 3^b 5^c and tile), 0: none                  */
+  int32_t host_check;        /* 1: stop launching iterations once all probes of
+                                a slice converged (synchronises the stream)     */
+  int32_t reserved;
+  double tol;                /* relative residual per solve (0 = 1e-6)           */
+  const void *probes;        /* float2 (P, N) initial fields, or NULL            */
+  const void *src_shared;    /* float2 (L, N) probe-independent source by step   */
+  const void *src_exit;      /* float2 (P, N) source at the first step, or NULL  */
+  void *u_store;             /* float2 (P, nz, N) or NULL                        */
+  void *exit_out;            /* float2 (P, N) or NULL                            */
+  const void *u_fwd;         /* ADJOINT_EXACT gradient: forward field (P, nz, N) */
+  void *grad_c;              /* ADJOINT_EXACT: float2 (L, N) accumulator of
+                                sum_p lambda_s conj(u_s + u_{s-1}); caller zeroes */
+  int32_t *stats;            /* device int32[4]: total iterations, solves, solves
+                                whose true residual exceeded 10 tol, largest
+                                iteration count; accumulated; or NULL            */
+} tp_cn3d_march_args;
+
+TP_API size_t tp_cn3d_workspace_bytes(int32_t n_total, int32_t num_probes);
+TP_API int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t n_dtype, const tp_cn3d_march_args *args,
+                         void *workspace, size_t workspace_bytes, tp_stream_t stream);
+
 /* Synchronise `stream` and report device-side failures of earlier launches
  * (a bounded wait that gave up).  Returns TP_ERR_TIMEOUT and clears the flag
  * when one was recorded; *code receives the raw device code (0 = none). */

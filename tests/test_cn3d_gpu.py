@@ -1,0 +1,208 @@
+"""Batched 3D (5-point, BiCGStab) march against the reference's golden
+vectors and the complex128 oracle (sparse LU per slice).
+
+Tolerances: fields ≤ 2e-5 relative L2 against complex128 (BiCGStab stopped at
+a 1e-6 relative residual, complex64 vectors, FP64 dot products); exact-adjoint
+gradients ≤ 1e-4 relative L2 against the oracle's discrete adjoint.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import pwe_oracle as po
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from thick_ptycho_b200 import SimulationGeometry  # noqa: E402
+from thick_ptycho_b200.cn3d import CN3D  # noqa: E402
+from thick_ptycho_b200.solver import PWEGpuSolver  # noqa: E402
+
+TOL = 2e-5
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def c64(x):
+    return torch.from_numpy(np.ascontiguousarray(x).astype(np.complex64)).cuda()
+
+
+def run(eng, n, P, mode="forward", **kw):
+    store = eng.new_store(P)
+    eng.march(torch.from_numpy(np.ascontiguousarray(n.reshape(eng.N, eng.nz))).cuda(), P, mode, u_store=store,
+              tol=kw.pop("tol", 1e-6), **kw)
+    return store.permute(0, 2, 1).cpu().numpy().astype(np.complex128)  # (P, N, nz)
+
+
+@pytest.mark.parametrize("bc", ["neumann", "impedance", "dirichlet"])
+@pytest.mark.parametrize("nx", [8, 16])
+def test_kat3d_golden(golden, bc, nx):
+    g = golden("kat3d")
+    key = f"{bc}_{nx}"
+    N, nz, dz, dx, dy, k = (int(g[key + "_nx"]), int(g[key + "_nz"]), float(g[key + "_dz"]), float(g[key + "_dx"]),
+                            float(g[key + "_dy"]), float(g[key + "_k"]))
+    eng = CN3D(N, N, nz, k, dx, dy, dz, bc)
+    n = np.ones((N * N, nz), dtype=complex)
+    kw = {}
+    if key + "_test_rhs" in g:
+        kw["src_shared"] = c64(g[key + "_test_rhs"])
+    u = run(eng, n, 1, probes=c64(g[key + "_probe"].reshape(1, -1)), **kw)[0]
+    assert rel(u.reshape(N, N, nz), g[key + "_u"]) < TOL
+    st = eng.read_stats()
+    assert st["failed"] == 0 and st["solves"] == nz - 1
+
+
+@pytest.mark.parametrize("bc", ["neumann", "impedance", "dirichlet"])
+def test_random3d_golden(golden, bc):
+    g = golden("random3d")
+    N, nz, dz, dx, dy, k = (int(g["nx"]), int(g["nz"]), float(g["dz"]), float(g["dx"]), float(g["dy"]), float(g["k"]))
+    eng = CN3D(N, N, nz, k, dx, dy, dz, bc)
+    P = g["probes"].shape[0]
+    u = run(eng, g["n"], P, probes=c64(g["probes"].reshape(P, -1)))
+    for p in range(P):
+        assert rel(u[p].reshape(N, N, nz), g[f"{bc}_forward"][p]) < TOL, p
+    # the reference adjoint reads rhs_block column -j at step j and flips its output
+    src = c64(g["rhs_block"][:, ::-1].T)
+    lam = run(eng, g["n"], 1, "adjoint", src_shared=src)[0]
+    assert rel(lam, g[f"{bc}_adjoint"]) < TOL
+
+
+def _field(rng, N, nz, scale=5e-3):
+    return 1 + scale * (rng.standard_normal((N, nz)) + 0.2j * rng.standard_normal((N, nz)))
+
+
+def _gauss(nf, nb, centres, w):
+    f = np.arange(nf)[None, :]
+    b = np.arange(nb)[:, None]
+    return np.array([np.exp(-((f - cf) ** 2 + (b - cb) ** 2) / w**2).ravel() for cf, cb in centres]).astype(complex)
+
+
+@pytest.mark.parametrize("bc", ["impedance", "neumann", "dirichlet"])
+@pytest.mark.parametrize("precond", [True, False])
+def test_fft_preconditioned_against_oracle(bc, precond):
+    """64×64 transverse (FFT preconditioner active), 12 nodes, 6 probes."""
+    rng = np.random.default_rng(11)
+    nf = nb = 64
+    nz, k, dx, dz, P = 12, 2 * np.pi / 0.5, 1.0, 1.0, 6
+    n = _field(rng, nf * nb, nz)
+    probes = _gauss(nf, nb, rng.uniform(20, 44, (P, 2)), 8.0)
+    eng = CN3D(nf, nb, nz, k, dx, dx, dz, bc)
+    u = run(eng, n, P, probes=c64(probes), precond=precond)
+    st = eng.read_stats()
+    assert st["failed"] == 0
+    co = po.bc_coefficients(k, dx, dz, dy=dx, bc_type=bc, dimension=3)
+    A, B = po.step_matrices_2d(nf, nb, co, bc, dz)
+    C = po.object_contribution(n, k, dz)
+    for p in (0, 3, 5):
+        ref = po.march(A, B, C, probes[p])
+        assert rel(u[p], ref) < TOL, (p, rel(u[p], ref))
+
+
+def test_reverse_mode_against_oracle():
+    rng = np.random.default_rng(3)
+    nf = nb = 32
+    nz, k, P = 9, 4 * np.pi, 3
+    n = _field(rng, nf * nb, nz)
+    probes = _gauss(nf, nb, rng.uniform(10, 22, (P, 2)), 5.0)
+    eng = CN3D(nf, nb, nz, k, 1.0, 1.0, 1.0, "impedance")
+    u = run(eng, n, P, "reverse", probes=c64(probes))
+    co = po.bc_coefficients(k, 1.0, 1.0, dy=1.0, bc_type="impedance", dimension=3)
+    A, B = po.step_matrices_2d(nf, nb, co, "impedance", 1.0)
+    C = po.object_contribution(n, k, 1.0)
+    for p in range(P):
+        assert rel(u[p], po.march(A, B, C, probes[p], "reverse")) < TOL
+
+
+@pytest.mark.parametrize("exact", [False, True])
+def test_exact_adjoint_gradient_against_oracle(exact):
+    rng = np.random.default_rng(21)
+    nf = nb = 32
+    nz, k, dz, P = 10, 4 * np.pi, 1.0, 4
+    N = nf * nb
+    n = _field(rng, N, nz)
+    probes = _gauss(nf, nb, rng.uniform(10, 22, (P, 2)), 5.0)
+    eng = CN3D(nf, nb, nz, k, 1.0, 1.0, dz, "impedance", exact_ref_coeff=exact)
+    field = torch.from_numpy(n).cuda()
+    store = eng.new_store(P)
+    eng.march(field, P, "forward", probes=c64(probes), u_store=store, tol=1e-7)
+    srcs = rng.standard_normal((P, N)) + 1j * rng.standard_normal((P, N))
+    gc = torch.zeros((nz - 1, N), dtype=torch.complex64, device="cuda")
+    eng.march(field, P, "adjoint_exact", src_exit=c64(srcs), u_fwd=store, grad_c=gc, tol=1e-7)
+    gn = eng.grad_to_n(gc, field).cpu().numpy()
+
+    co = po.bc_coefficients(k, 1.0, dz, dy=1.0, bc_type="impedance", dimension=3)
+    A, B = po.step_matrices_2d(nf, nb, co, "impedance", dz)
+    C = po.object_contribution(n, k, dz, exact_ref_coeff=exact)
+    u = np.array([po.march(A, B, C, probes[p]) for p in range(P)])
+    src = np.zeros((P, N, nz - 1), dtype=complex)
+    src[:, :, -1] = srcs
+    lam = po.exact_adjoint_many(A, B, C, src)
+    gcr = sum(po.grad_c_from_adjoint(u[p], lam[p]) for p in range(P))
+    assert rel(gc.cpu().numpy().T, gcr) < 1e-4
+    gnr = po.chain_grad_to_n(gcr, k, dz, n=n, exact_ref_coeff=exact)
+    assert rel(gn, gnr) < 1e-4
+
+
+def test_src_shared_and_src_exit_adjoint():
+    """ADJOINT_EXACT with a shared per-step source and an exit source together."""
+    rng = np.random.default_rng(8)
+    nf = nb = 16
+    nz, k, P = 7, 4 * np.pi, 2
+    N = nf * nb
+    n = _field(rng, N, nz)
+    eng = CN3D(nf, nb, nz, k, 1.0, 1.0, 1.0, "neumann")
+    sh = rng.standard_normal((nz - 1, N)) + 1j * rng.standard_normal((nz - 1, N))
+    ex = rng.standard_normal((P, N)) + 1j * rng.standard_normal((P, N))
+    store = eng.new_store(P)
+    # shared source rows are in step order: step t solves slice L+1-t
+    eng.march(torch.from_numpy(n).cuda(), P, "adjoint_exact", src_exit=c64(ex), src_shared=c64(sh[::-1]),
+              u_store=store, tol=1e-7)
+    lam = store.permute(0, 2, 1).cpu().numpy()
+    co = po.bc_coefficients(k, 1.0, 1.0, dy=1.0, bc_type="neumann", dimension=3)
+    A, B = po.step_matrices_2d(nf, nb, co, "neumann", 1.0)
+    C = po.object_contribution(n, k, 1.0)
+    src = np.repeat(sh.T[None], P, axis=0).astype(complex)
+    src[:, :, -1] += ex
+    ref = po.exact_adjoint_many(A, B, C, src)
+    for p in range(P):
+        # node t holds step t, i.e. slice L+1-t (node 0 holds the zero start state)
+        assert rel(lam[p][:, 1:][:, ::-1], ref[p]) < TOL
+
+
+def test_dropin_solver_3d():
+    geo = SimulationGeometry.grid_3d(24, 10, 0.5, 2, 8)
+    rng = np.random.default_rng(2)
+    n = 1 + 2e-3 * (rng.standard_normal(geo.effective_shape) + 0.1j * rng.standard_normal(geo.effective_shape))
+    N = geo.block_size
+    centres = [(8 + 8 * (p // 2), 8 + 8 * (p % 2)) for p in range(geo.num_probes)]
+    probes = _gauss(geo.effective_shape[0], geo.effective_shape[1], centres, 4.0).reshape(
+        1, geo.num_probes, *geo.effective_shape[:2])
+    s = PWEGpuSolver(geo, probes, bc_type="impedance")
+    u = s.solve(n=n)
+    assert u.shape == (1, 1, geo.num_probes, *geo.effective_shape)
+    nf = geo.effective_shape[0]
+    co = po.bc_coefficients(geo.k, geo.dx, geo.dz, dy=geo.dy, bc_type="impedance", dimension=3)
+    A, B = po.step_matrices_2d(nf, nf, co, "impedance", geo.dz)
+    C = po.object_contribution(n, geo.k, geo.dz).reshape(N, -1)
+    for p in range(geo.num_probes):
+        ref = po.march(A, B, C, probes[0, p].ravel())
+        assert rel(u[0, 0, p].reshape(N, -1), ref) < TOL
+    rhs = rng.standard_normal((N, geo.nz - 1)) + 1j * rng.standard_normal((N, geo.nz - 1))
+    lam = s._solve_single_probe(n=n, mode="adjoint", rhs_block=rhs)
+    assert rel(lam, po.march(A, B, C, None, "adjoint", rhs_block=rhs)) < TOL
+
+
+def test_rejects_bad_arguments():
+    eng = CN3D(8, 8, 4, 4 * np.pi, 1.0, 1.0, 1.0, "impedance")
+    f = torch.ones((64, 4), dtype=torch.complex128, device="cuda")
+    with pytest.raises(ValueError):
+        eng.march(f, 2, probes=torch.zeros((2, 63), dtype=torch.complex64, device="cuda"))
+    with pytest.raises(Exception, match="gradient"):
+        eng.march(f, 1, "forward", u_fwd=eng.new_store(1),
+                  grad_c=torch.zeros((3, 64), dtype=torch.complex64, device="cuda"))

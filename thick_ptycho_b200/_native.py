@@ -88,6 +88,28 @@ class TpMs2dOp(ctypes.Structure):
     ]
 
 
+class TpCn3dOp(ctypes.Structure):
+    _fields_ = [
+        ("nf", ctypes.c_int32), ("nb", ctypes.c_int32), ("nz", ctypes.c_int32),
+        ("exact_ref_coeff", ctypes.c_int32), ("field_is_delta", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("k", ctypes.c_double), ("dz", ctypes.c_double),
+        ("mu_x", ctypes.c_double * 2), ("mu_y", ctypes.c_double * 2),
+        ("kc", ctypes.c_void_p), ("kw", ctypes.c_void_p), ("ke", ctypes.c_void_p), ("ks", ctypes.c_void_p),
+        ("kn", ctypes.c_void_p),
+    ]
+
+
+class TpCn3dMarchArgs(ctypes.Structure):
+    _fields_ = [
+        ("num_probes", ctypes.c_int32), ("mode", ctypes.c_int32), ("max_iter", ctypes.c_int32),
+        ("precond", ctypes.c_int32), ("host_check", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("tol", ctypes.c_double),
+        ("probes", ctypes.c_void_p), ("src_shared", ctypes.c_void_p), ("src_exit", ctypes.c_void_p),
+        ("u_store", ctypes.c_void_p), ("exit_out", ctypes.c_void_p), ("u_fwd", ctypes.c_void_p),
+        ("grad_c", ctypes.c_void_p), ("stats", ctypes.c_void_p),
+    ]
+
+
 # (name, restype, argtypes) of every exported symbol of include/tpcuda.h
 SIGNATURES = [
     ("tp_cn2d_layout", ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
@@ -115,6 +137,9 @@ SIGNATURES = [
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("tp_ms2d_backward", ctypes.c_int, [ctypes.POINTER(TpMs2dOp), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                         ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
+    ("tp_cn3d_workspace_bytes", ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
+    ("tp_cn3d_march", ctypes.c_int, [ctypes.POINTER(TpCn3dOp), ctypes.c_void_p, ctypes.c_int32,
+                                     ctypes.POINTER(TpCn3dMarchArgs), ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
     ("tp_device_status", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ("tp_last_error_string", ctypes.c_char_p, []),
     ("tp_version", ctypes.c_int, []),

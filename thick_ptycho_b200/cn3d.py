@@ -1,0 +1,163 @@
+"""Batched 3D Crank–Nicolson propagation on the GPU (host side).
+
+:class:`CN3D` holds the 5-point operator of one 3D geometry (restated from the
+reference's ``operator_matrices.py:75-126`` / ``boundary_conditions.py:96-130``
+in :func:`operators.operator_2d_diagonals`) and calls ``tp_cn3d_march``:
+every slice is solved by FFT-preconditioned BiCGStab in delta form, all probes
+at once.  Vectors follow the reference's flattening of (nx, ny) arrays.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _native
+from .operators import BCCoefficients, normalize_bc, operator_2d_diagonals
+
+
+def _ptr(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _c2(z: complex):
+    return (ctypes.c_double * 2)(z.real, z.imag)
+
+
+class CN3D:
+    """One 3D geometry: nx × ny transverse (N = nx·ny), nz nodes."""
+
+    def __init__(self, nx, ny, nz, k, dx, dy, dz, bc_type="impedance", exact_ref_coeff=False, device=None):
+        if not torch.cuda.is_available():
+            raise _native.NativeLibraryError("CN3D needs a CUDA device (there is no CPU fallback)")
+        self.lib = _native.load()
+        self.device = torch.device(device if device is not None else "cuda")
+        self.nx, self.ny, self.nz, self.L = int(nx), int(ny), int(nz), int(nz) - 1
+        self.N = self.nx * self.ny
+        self.k, self.dz = float(k), float(dz)
+        self.bc_type = normalize_bc(bc_type)
+        self.exact_ref_coeff = bool(exact_ref_coeff)
+        co = BCCoefficients.make(self.k, dx, dz, self.bc_type, dy=dy, dimension=3)
+        diags = operator_2d_diagonals(self.nx, self.ny, co, self.bc_type)
+        self._diags = [torch.from_numpy(d.astype(np.complex64)).to(self.device) for d in diags]
+        self.co = co
+        self._ws = None
+        self._ws_P = None
+        self.stats = torch.zeros(4, dtype=torch.int32, device=self.device)
+
+    def op(self, is_delta=False) -> _native.TpCn3dOp:
+        o = _native.TpCn3dOp()
+        o.nf, o.nb, o.nz = self.nx, self.ny, self.nz
+        o.exact_ref_coeff, o.field_is_delta = int(self.exact_ref_coeff), int(is_delta)
+        o.k, o.dz = self.k, self.dz
+        o.mu_x, o.mu_y = _c2(self.co.mu_x), _c2(self.co.mu_y)
+        o.kc, o.kw, o.ke, o.ks, o.kn = (ctypes.c_void_p(d.data_ptr()) for d in self._diags)
+        return o
+
+    def workspace(self, P):
+        if self._ws is None or self._ws_P != P:
+            nbytes = int(self.lib.tp_cn3d_workspace_bytes(self.N, P))
+            self._ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            self._ws_P = P
+        return self._ws
+
+    def new_store(self, P):
+        return torch.empty((P, self.nz, self.N), dtype=torch.complex64, device=self.device)
+
+    def march(self, field: torch.Tensor, num_probes: int, mode="forward", probes=None, src_shared=None, src_exit=None,
+              u_store=None, exit_out=None, u_fwd=None, grad_c=None, tol=1e-6, max_iter=20, precond=True,
+              host_check=True, is_delta=False):
+        """One batched march; tensors complex64 (field complex128/complex64 (N, nz))."""
+        P = int(num_probes)
+        field = field.reshape(self.N, self.nz).contiguous()
+        mode_i = _native.MODES[mode] if isinstance(mode, str) else int(mode)
+        for name, t, shp in (("probes", probes, (P, self.N)), ("src_shared", src_shared, (self.L, self.N)),
+                             ("src_exit", src_exit, (P, self.N)), ("u_store", u_store, (P, self.nz, self.N)),
+                             ("exit_out", exit_out, (P, self.N)), ("grad_c", grad_c, (self.L, self.N))):
+            if t is not None and (t.dtype != torch.complex64 or not t.is_contiguous() or tuple(t.shape) != shp):
+                raise ValueError(f"{name} must be a contiguous complex64 tensor of shape {shp}")
+        a = _native.TpCn3dMarchArgs()
+        a.num_probes, a.mode, a.max_iter, a.precond, a.host_check = P, mode_i, int(max_iter), int(precond), int(host_check)
+        a.tol = float(tol)
+        a.probes, a.src_shared, a.src_exit = _ptr(probes), _ptr(src_shared), _ptr(src_exit)
+        a.u_store, a.exit_out, a.u_fwd, a.grad_c = _ptr(u_store), _ptr(exit_out), _ptr(u_fwd), _ptr(grad_c)
+        a.stats = ctypes.c_void_p(self.stats.data_ptr())
+        ws = self.workspace(P)
+        dt = _native.C128 if field.dtype == torch.complex128 else _native.C64
+        o = self.op(is_delta)
+        rc = self.lib.tp_cn3d_march(ctypes.byref(o), _ptr(field), dt, ctypes.byref(a), _ptr(ws), ws.numel(),
+                                    ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
+        _native.check(rc, "tp_cn3d_march")
+
+    def read_stats(self, reset=True):
+        """(total iterations, solves, failed solves, max iterations per solve)."""
+        s = self.stats.cpu().tolist()
+        if reset:
+            self.stats.zero_()
+        return {"iterations": s[0], "solves": s[1], "failed": s[2], "max_iterations": s[3]}
+
+    def grad_to_n(self, grad_c: torch.Tensor, field=None, is_delta=False) -> torch.Tensor:
+        """Σ_p λ conj(u_s + u_{s−1}) (L, N) → torch-convention ∂/∂n (N, nz)."""
+        acc = torch.zeros((self.N, self.nz), dtype=torch.complex128, device=self.device)
+        g = grad_c.to(torch.complex128).T
+        acc[:, :-1] += g
+        acc[:, 1:] += g
+        d = (self.dz / 4) * (self.k / 1j)
+        if self.exact_ref_coeff:
+            f = field.reshape(self.N, self.nz).to(torch.complex128)
+            nn = f + 1 if is_delta else f
+            return (np.conj(d) * torch.conj(nn) * acc).to(torch.complex64)
+        return (np.conj(d) * acc).to(torch.complex64)
+
+
+class PWEGradient3D:
+    """Amplitude-loss gradient of a 3D geometry, all probes batched
+    (far field ``|FFT2(exit)|``; forward + exact adjoint by :class:`CN3D`)."""
+
+    def __init__(self, geometry, bc_type="impedance", device=None, tol=1e-6, max_iter=20, precond=True):
+        self.geometry = geometry
+        self.engine = CN3D(geometry.effective_shape[0], geometry.effective_shape[1], geometry.nz, geometry.k,
+                           geometry.dx, getattr(geometry, "dy", geometry.dx), geometry.dz, bc_type,
+                           exact_ref_coeff=bool(getattr(geometry, "exact_ref_coeff", False)), device=device)
+        self.device = self.engine.device
+        self.kw = dict(tol=tol, max_iter=max_iter, precond=precond)
+        self._store = None
+
+    def forward(self, field, probes):
+        e = self.engine
+        P = probes.shape[0]
+        if self._store is None or self._store.shape[0] != P:
+            self._store = e.new_store(P)
+        ex = torch.empty((P, e.N), dtype=torch.complex64, device=self.device)
+        e.march(field, P, "forward", probes=probes.reshape(P, e.N).contiguous(), u_store=self._store, exit_out=ex,
+                **self.kw)
+        return ex
+
+    def backward(self, field, exit_grad):
+        e = self.engine
+        P = exit_grad.shape[0]
+        gc = torch.zeros((e.L, e.N), dtype=torch.complex64, device=self.device)
+        e.march(field, P, "adjoint_exact", src_exit=exit_grad.reshape(P, e.N).contiguous(), u_fwd=self._store,
+                grad_c=gc, **self.kw)
+        self.grad_c = gc
+        return e.grad_to_n(gc, field)
+
+    def loss_and_grad(self, n, probes, amplitude):
+        e = self.engine
+        field = torch.as_tensor(np.ascontiguousarray(n) if not isinstance(n, torch.Tensor) else n).to(
+            self.device, torch.complex128)
+        pr = torch.as_tensor(np.ascontiguousarray(probes) if not isinstance(probes, torch.Tensor) else probes).to(
+            self.device, torch.complex64).reshape(-1, e.N)
+        amp = torch.as_tensor(np.ascontiguousarray(amplitude) if not isinstance(amplitude, torch.Tensor) else amplitude).to(
+            self.device, torch.float64).reshape(-1, e.nx, e.ny)
+        ex = self.forward(field, pr).reshape(-1, e.nx, e.ny)
+        U = torch.fft.fft2(ex.to(torch.complex128))
+        mag = U.abs()
+        loss = torch.sum((mag - amp) ** 2)
+        gU = torch.where(mag > 0, 2 * (mag - amp) / torch.where(mag > 0, mag, torch.ones_like(mag)), torch.zeros_like(mag)) * U
+        ge = (e.N * torch.fft.ifft2(gU)).to(torch.complex64).reshape(-1, e.N)
+        g = self.backward(field, ge)
+        return float(loss.item()), g.reshape(e.nx, e.ny, e.nz)

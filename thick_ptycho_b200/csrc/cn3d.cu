@@ -1,0 +1,575 @@
+// 3D paraxial Crank–Nicolson march (2D transverse, 5-point operator), batched
+// over probes, each slice solved by FFT-preconditioned BiCGStab.
+//
+// Replaces the reference's per-slice sparse LU of the 2D operator
+// (iterative_lu.py:103-133 with operator_matrices.py:75-126) and its
+// per-probe z-march (iterative_lu.py:138-197).
+//
+// Step s solves (I - P_s) u_new = (I + P_r) u + b, P = sigma*T(K + diag(c_s)),
+// in delta form: (I - P_s) d = (P_r + P_s) u + b, u_new = u + d.  The update d
+// is O(|P| |u|) ~ 4e-2 |u|, so the Krylov tolerance and the complex64
+// round-off act on the small update, not on u (the same "1 + eps" reason as
+// the 2D kernels).  BiCGStab (van der Vorst) runs on every probe of the batch
+// at once: all vectors are (P, N) complex64, inner products are accumulated
+// in fp64 per probe, and a probe stops updating once ||r|| <= tol ||rhs||;
+// after the iterations each solve is judged by its true residual
+// ||rhs - (I - P_s) d||.  Preconditioner: the periodic 5-point operator
+// diagonalised by a 2D FFT (libtpcuda's shared-memory FFT), applied as
+// IFFT2(FFT2(v) / (1 - sigma*T K_per(kf, kb))),
+// K_per = mu_x (2 cos kf - 2) + mu_y (2 cos kb - 2).
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "fft.cuh"
+#include "tp_common.cuh"
+#include "tp_errors.h"
+#include "tpcuda.h"
+
+namespace tp {
+
+constexpr int k3Threads = 256;
+
+struct C3Params {
+  int nf, nb, N, nz, L, P;
+  int exact, is_delta, dtype, conj_t;
+  double sigma, k, dz;
+  double2 mu_x, mu_y;  // preconditioner symbol coefficients (sigma and T applied)
+  const void *field;
+  const float2 *kc, *kw, *ke, *ks, *kn;  // diagonals of sigma*T(K)
+};
+
+// Per-probe BiCGStab scalars (fp64).
+struct __align__(16) Krylov {
+  double2 rho_prev, rho_cur, alpha, omega;
+  double2 acc_r0v, acc_ts, acc_r0r;
+  double acc_tt, acc_rr, bnorm2, res2;
+  int done, iters, pad0, pad1;
+};
+
+// stats[0] total iterations, [1] solves, [2] solves whose true residual
+// exceeded the tolerance, [3] largest iteration count of one solve.
+enum { kStatIters = 0, kStatSolves = 1, kStatFailed = 2, kStatMaxIters = 3 };
+
+__device__ __forceinline__ double2 load_field(const C3Params &q, size_t idx) {
+  if (q.dtype == TP_C128) return static_cast<const double2 *>(q.field)[idx];
+  const float2 v = static_cast<const float2 *>(q.field)[idx];
+  return z2(v.x, v.y);
+}
+
+// coef(n) of base_simulation_space.py:356-360
+__device__ __forceinline__ double2 coef3(const C3Params &q, double2 v) {
+  const double2 d = q.is_delta ? v : z2(v.x - 1.0, v.y);
+  if (!q.exact) return z2(q.k * d.y, -q.k * d.x);
+  const double2 w = zadd(zscale(d, 2.0), zmul(d, d));
+  return z2(0.5 * q.k * w.y, -0.5 * q.k * w.x);
+}
+
+// sigma*T(K) diagonals from K's (T = conjugate transpose for the adjoints).
+__global__ void c3_diag_kernel(int N, int nf, double sigma, int conj_t, const float2 *kc, const float2 *kw,
+                               const float2 *ke, const float2 *ks, const float2 *kn, float2 *oc, float2 *ow,
+                               float2 *oe, float2 *os, float2 *on) {
+  const float sg = (float)sigma;
+  auto tf = [&](float2 v) { return make_float2(sg * v.x, sg * (conj_t ? -v.y : v.y)); };
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const float2 z = make_float2(0.f, 0.f);
+    oc[i] = tf(kc[i]);
+    if (!conj_t) {
+      ow[i] = tf(kw[i]);
+      oe[i] = tf(ke[i]);
+      os[i] = tf(ks[i]);
+      on[i] = tf(kn[i]);
+    } else {
+      ow[i] = (i >= 1) ? tf(ke[i - 1]) : z;
+      oe[i] = (i + 1 < N) ? tf(kw[i + 1]) : z;
+      os[i] = (i >= nf) ? tf(kn[i - nf]) : z;
+      on[i] = (i + nf < N) ? tf(ks[i + nf]) : z;
+    }
+  }
+}
+
+// cd[i] = sigma*T(K)_c[i] + sigma*T(c_s(i)) for slice s (1-based), fp64 -> fp32.
+__global__ void c3_center_kernel(const C3Params q, int s, float2 *__restrict__ cd) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
+    const size_t base = (size_t)i * q.nz;
+    const double2 c = zscale(zadd(coef3(q, load_field(q, base + s - 1)), coef3(q, load_field(q, base + s))), 0.25 * q.dz);
+    const double2 v = zscale(q.conj_t ? zconj(c) : c, q.sigma);
+    const float2 k = q.kc[i];
+    cd[i] = make_float2((float)(k.x + v.x), (float)(k.y + v.y));
+  }
+}
+
+__device__ __forceinline__ float2 apply_P(const C3Params &q, const float2 *__restrict__ cd, const float2 *__restrict__ x,
+                                          int i) {
+  float2 r = cmul(cd[i], x[i]);
+  const int f = i % q.nf;
+  if (f > 0) r = cfma(q.kw[i], x[i - 1], r);
+  if (f < q.nf - 1) r = cfma(q.ke[i], x[i + 1], r);
+  if (i >= q.nf) r = cfma(q.ks[i], x[i - q.nf], r);
+  if (i + q.nf < q.N) r = cfma(q.kn[i], x[i + q.nf], r);
+  return r;
+}
+
+__device__ __forceinline__ void block_reduce_add(double v, double *dst, double *red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) red[w] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int j = 0; j < (int)(blockDim.x >> 5); ++j) s += red[j];
+    atomicAdd(dst, s);
+  }
+  __syncthreads();
+}
+
+// Grid (chunks, P).  r = r0 = rhs = (P_l + P_r) u + src; x = p = v = 0.
+__global__ void __launch_bounds__(k3Threads) c3_init_kernel(const C3Params q, const float2 *__restrict__ cdl,
+                                                            const float2 *__restrict__ cdr, const float2 *__restrict__ u,
+                                                            int use_u, const float2 *__restrict__ src,
+                                                            const float2 *__restrict__ shared, float2 *x, float2 *r,
+                                                            float2 *r0, float2 *p, float2 *v, Krylov *K) {
+  __shared__ double red[k3Threads / 32];
+  const int pr = blockIdx.y;
+  const size_t off = (size_t)pr * q.N;
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
+    float2 b = use_u ? cadd(apply_P(q, cdl, u + off, i), apply_P(q, cdr, u + off, i)) : make_float2(0.f, 0.f);
+    if (src != nullptr) b = cadd(b, src[off + i]);
+    if (shared != nullptr) b = cadd(b, shared[i]);
+    r[off + i] = b;
+    r0[off + i] = b;
+    const float2 z = make_float2(0.f, 0.f);
+    x[off + i] = z;
+    p[off + i] = z;
+    v[off + i] = z;
+    acc += (double)b.x * b.x + (double)b.y * b.y;
+  }
+  block_reduce_add(acc, &K[pr].bnorm2, red);
+}
+
+// Per probe: start (first = 1) or commit an iteration.
+__global__ void c3_scalar_kernel(Krylov *K, int P, double tol2, int first, int *stats) {
+  const int pr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pr >= P) return;
+  Krylov &k = K[pr];
+  if (first) {
+    k.rho_prev = z2(1, 0);
+    k.rho_cur = z2(k.bnorm2, 0.0);  // <r0, r0>
+    k.alpha = z2(1, 0);
+    k.omega = z2(1, 0);
+    k.iters = 0;
+    k.done = (k.bnorm2 == 0.0) ? 1 : 0;
+  } else if (!k.done) {
+    const double den = k.acc_r0v.x * k.acc_r0v.x + k.acc_r0v.y * k.acc_r0v.y;
+    k.alpha = den > 0.0 ? zdiv(k.rho_cur, k.acc_r0v) : z2(0, 0);
+    k.omega = (k.acc_tt > 0.0) ? zscale(k.acc_ts, 1.0 / k.acc_tt) : z2(0, 0);
+    k.rho_prev = k.rho_cur;
+    k.rho_cur = k.acc_r0r;
+    k.iters += 1;
+    const double om2 = k.omega.x * k.omega.x + k.omega.y * k.omega.y;
+    const double rp2 = k.rho_prev.x * k.rho_prev.x + k.rho_prev.y * k.rho_prev.y;
+    if (k.acc_rr <= tol2 * k.bnorm2 || om2 == 0.0 || rp2 == 0.0) k.done = 1;
+  }
+  k.acc_r0v = k.acc_ts = k.acc_r0r = z2(0, 0);
+  k.acc_tt = 0.0;
+  k.acc_rr = 0.0;
+  (void)stats;
+}
+
+// Forward row FFTs of the preconditioner input, formed on the fly:
+//   mode 0: p := r + beta (p - omega v)  (p updated in place), input p
+//   mode 1: s := r - alpha v             (s written),          input s
+// Grid (nb / rpc, P).
+__global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan pl, const C3Params q, int mode,
+                                                                 const float2 *r, float2 *p, const float2 *v, float2 *s,
+                                                                 float2 *hat, const Krylov *K, int rpc, int fft_on) {
+  extern __shared__ __align__(16) float2 fsm[];
+  const int n = q.nf, pr = blockIdx.y;
+  const Krylov &k = K[pr];
+  if (k.done) return;
+  float2 *tw = fsm, *a = tw + n, *b = a + rpc * n;
+  const size_t off = (size_t)pr * q.N + (size_t)blockIdx.x * rpc * n;
+  const int tot = rpc * n;
+  if (fft_on) fft_twiddles(tw, n, threadIdx.x, blockDim.x);
+  if (mode == 0) {
+    const double den = k.rho_prev.x * k.rho_prev.x + k.rho_prev.y * k.rho_prev.y;
+    const double2 beta = den > 0.0 ? zmul(zdiv(k.rho_cur, k.rho_prev), zdiv(k.alpha, k.omega)) : z2(0, 0);
+    const float2 bt = to_f2(beta), om = to_f2(k.omega);
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+      const float2 pv = cfma(bt, cfnma(om, v[off + e], p[off + e]), r[off + e]);
+      p[off + e] = pv;
+      if (fft_on) a[e] = pv;
+      else hat[off + e] = pv;
+    }
+  } else {
+    const double den = k.acc_r0v.x * k.acc_r0v.x + k.acc_r0v.y * k.acc_r0v.y;
+    const double2 alpha = den > 0.0 ? zdiv(k.rho_cur, k.acc_r0v) : z2(0, 0);
+    const float2 al = to_f2(alpha);
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+      const float2 sv = cfnma(al, v[off + e], r[off + e]);
+      s[off + e] = sv;
+      if (fft_on) a[e] = sv;
+      else hat[off + e] = sv;
+    }
+  }
+  if (!fft_on) return;
+  __syncthreads();
+  const float2 *res = fft_block(a, b, pl, tw, false, rpc, threadIdx.x, blockDim.x);
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) hat[off + e] = res[e];
+}
+
+// Column FFTs, division by the symbol, inverse column FFTs (in place on hat).
+// Grid (nf / cpc, P): a CTA transposes cpc columns of length nb into smem.
+__global__ void __launch_bounds__(k3Threads) c3_prec_cols_kernel(const FftPlan pl, const C3Params q, float2 *hat,
+                                                                 const Krylov *K, int cpc) {
+  extern __shared__ __align__(16) float2 fsm[];
+  const int nb = q.nb, nf = q.nf, pr = blockIdx.y;
+  if (K[pr].done) return;
+  float2 *tw = fsm, *a = tw + nb, *b = a + cpc * nb;
+  const int f0 = blockIdx.x * cpc;
+  float2 *base = hat + (size_t)pr * q.N;
+  fft_twiddles(tw, nb, threadIdx.x, blockDim.x);
+  for (int e = threadIdx.x; e < cpc * nb; e += blockDim.x) {
+    const int c = e % cpc, bb = e / cpc;  // coalesced over c
+    a[c * nb + bb] = base[(size_t)bb * nf + f0 + c];
+  }
+  __syncthreads();
+  float2 *F = fft_block(a, b, pl, tw, false, cpc, threadIdx.x, blockDim.x);
+  float2 *o = (F == a) ? b : a;
+  for (int e = threadIdx.x; e < cpc * nb; e += blockDim.x) {
+    const int c = e / nb, bb = e % nb;
+    double sf, cf, sb, cbv;
+    sincospi(2.0 * (double)(f0 + c) / (double)nf, &sf, &cf);
+    sincospi(2.0 * (double)bb / (double)nb, &sb, &cbv);
+    const double ax = 2.0 * cf - 2.0, ay = 2.0 * cbv - 2.0;
+    const double2 lam = z2(1.0 - (q.mu_x.x * ax + q.mu_y.x * ay), -(q.mu_x.y * ax + q.mu_y.y * ay));
+    F[e] = cmul(F[e], to_f2(zdiv(z2(1, 0), lam)));
+  }
+  __syncthreads();
+  float2 *R = fft_block(F, o, pl, tw, true, cpc, threadIdx.x, blockDim.x);
+  for (int e = threadIdx.x; e < cpc * nb; e += blockDim.x) {
+    const int c = e % cpc, bb = e / cpc;
+    base[(size_t)bb * nf + f0 + c] = R[c * nb + bb];
+  }
+}
+
+// Inverse row FFTs (scaled 1/(nf nb)) of hat into out.
+__global__ void __launch_bounds__(k3Threads) c3_prec_rows_inv_kernel(const FftPlan pl, const C3Params q,
+                                                                     const float2 *hat, float2 *out, const Krylov *K,
+                                                                     int rpc) {
+  extern __shared__ __align__(16) float2 fsm[];
+  const int n = q.nf, pr = blockIdx.y;
+  if (K[pr].done) return;
+  float2 *tw = fsm, *a = tw + n, *b = a + rpc * n;
+  const size_t off = (size_t)pr * q.N + (size_t)blockIdx.x * rpc * n;
+  const int tot = rpc * n;
+  fft_twiddles(tw, n, threadIdx.x, blockDim.x);
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) a[e] = hat[off + e];
+  __syncthreads();
+  const float2 *res = fft_block(a, b, pl, tw, true, rpc, threadIdx.x, blockDim.x);
+  const float sc = 1.f / ((float)q.nf * (float)q.nb);
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) out[off + e] = make_float2(res[e].x * sc, res[e].y * sc);
+}
+
+// out = (I - P) y with fused fp64 dots: which 0: acc_r0v += <r0, out>;
+// which 1: acc_ts += <out, s>, acc_tt += <out, out>.
+__global__ void __launch_bounds__(k3Threads) c3_matvec_kernel(const C3Params q, const float2 *__restrict__ cd,
+                                                              const float2 *__restrict__ y, float2 *__restrict__ out,
+                                                              const float2 *__restrict__ r0, const float2 *__restrict__ s,
+                                                              Krylov *K, int which) {
+  __shared__ double red[k3Threads / 32];
+  const int pr = blockIdx.y;
+  if (K[pr].done) return;
+  const size_t off = (size_t)pr * q.N;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
+    const float2 t = csub(y[off + i], apply_P(q, cd, y + off, i));
+    out[off + i] = t;
+    const float2 c = (which == 0) ? r0[off + i] : s[off + i];
+    if (which == 0) {  // conj(r0) t
+      a0 += (double)c.x * t.x + (double)c.y * t.y;
+      a1 += (double)c.x * t.y - (double)c.y * t.x;
+    } else {  // conj(t) s, |t|^2
+      a0 += (double)t.x * c.x + (double)t.y * c.y;
+      a1 += (double)t.x * c.y - (double)t.y * c.x;
+      a2 += (double)t.x * t.x + (double)t.y * t.y;
+    }
+  }
+  Krylov &k = K[pr];
+  if (which == 0) {
+    block_reduce_add(a0, &k.acc_r0v.x, red);
+    block_reduce_add(a1, &k.acc_r0v.y, red);
+  } else {
+    block_reduce_add(a0, &k.acc_ts.x, red);
+    block_reduce_add(a1, &k.acc_ts.y, red);
+    block_reduce_add(a2, &k.acc_tt, red);
+  }
+}
+
+// omega = <t,s>/<t,t>; x += alpha y + omega z; r = s - omega t; accumulate
+// <r0, r> and ||r||^2 for the next iteration.
+__global__ void __launch_bounds__(k3Threads) c3_update_kernel(const C3Params q, float2 *x, float2 *r,
+                                                              const float2 *__restrict__ r0, const float2 *__restrict__ y,
+                                                              const float2 *__restrict__ z, const float2 *__restrict__ s,
+                                                              const float2 *__restrict__ t, Krylov *K) {
+  __shared__ double red[k3Threads / 32];
+  const int pr = blockIdx.y;
+  Krylov &k = K[pr];
+  if (k.done) return;
+  const size_t off = (size_t)pr * q.N;
+  const double den = k.acc_r0v.x * k.acc_r0v.x + k.acc_r0v.y * k.acc_r0v.y;
+  const double2 alpha = den > 0.0 ? zdiv(k.rho_cur, k.acc_r0v) : z2(0, 0);
+  const double2 omega = (k.acc_tt > 0.0) ? zscale(k.acc_ts, 1.0 / k.acc_tt) : z2(0, 0);
+  const float2 al = to_f2(alpha), om = to_f2(omega);
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
+    x[off + i] = cfma(om, z[off + i], cfma(al, y[off + i], x[off + i]));
+    const float2 rv = cfnma(om, t[off + i], s[off + i]);
+    r[off + i] = rv;
+    const float2 c = r0[off + i];
+    a0 += (double)c.x * rv.x + (double)c.y * rv.y;
+    a1 += (double)c.x * rv.y - (double)c.y * rv.x;
+    a2 += (double)rv.x * rv.x + (double)rv.y * rv.y;
+  }
+  block_reduce_add(a0, &k.acc_r0r.x, red);
+  block_reduce_add(a1, &k.acc_r0r.y, red);
+  block_reduce_add(a2, &k.acc_rr, red);
+}
+
+// True residual of each solve: res2 = ||rhs - (I - P) d||^2 (rhs = r0, d = x),
+// then u += d.  Grid (chunks, P).
+__global__ void __launch_bounds__(k3Threads) c3_finish_kernel(const C3Params q, const float2 *__restrict__ cd,
+                                                              const float2 *__restrict__ x, const float2 *__restrict__ r0,
+                                                              float2 *u, Krylov *K) {
+  __shared__ double red[k3Threads / 32];
+  const int pr = blockIdx.y;
+  const size_t off = (size_t)pr * q.N;
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
+    const float2 mx = csub(x[off + i], apply_P(q, cd, x + off, i));
+    const float2 d = csub(r0[off + i], mx);
+    acc += (double)d.x * d.x + (double)d.y * d.y;
+    u[off + i] = cadd(u[off + i], x[off + i]);
+  }
+  block_reduce_add(acc, &K[pr].res2, red);
+}
+
+// pending[0] += number of probes still iterating (the caller zeroes it).
+__global__ void c3_pending_kernel(const Krylov *K, int P, int *pending) {
+  const int pr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pr < P && !K[pr].done) atomicAdd(pending, 1);
+}
+
+__global__ void c3_stats_kernel(Krylov *K, int P, double tol2, int *stats) {
+  const int pr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pr >= P) return;
+  Krylov &k = K[pr];
+  atomicAdd(&stats[kStatIters], k.iters);
+  atomicAdd(&stats[kStatSolves], 1);
+  atomicMax(&stats[kStatMaxIters], k.iters);
+  // the true residual may exceed the recursive one by round-off; allow 10x
+  if (k.res2 > 100.0 * tol2 * k.bnorm2) atomicAdd(&stats[kStatFailed], 1);
+  k.res2 = 0.0;
+  k.bnorm2 = 0.0;
+}
+
+// Store the state (P, N) into slice `t` of u_store (P, nz, N) and/or exit.
+__global__ void c3_store_kernel(int N, int P, int nz, int t, const float2 *__restrict__ u, float2 *u_store,
+                                float2 *exit_out) {
+  const size_t total = (size_t)P * N;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t pr = e / N, i = e % N;
+    if (u_store) u_store[(pr * nz + t) * N + i] = u[e];
+    if (exit_out) exit_out[e] = u[e];
+  }
+}
+
+// grad_c[s-1][i] += sum_p lambda_p[i] conj(u_p,s[i] + u_p,s-1[i])  (no atomics:
+// one thread owns element i and loops over the probes).
+__global__ void c3_grad_kernel(int N, int P, int nz, int s, const float2 *__restrict__ lam,
+                               const float2 *__restrict__ u_fwd, float2 *grad_c) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    float2 acc = make_float2(0.f, 0.f);
+    for (int pr = 0; pr < P; ++pr) {
+      const float2 w = cadd(u_fwd[((size_t)pr * nz + s) * N + i], u_fwd[((size_t)pr * nz + s - 1) * N + i]);
+      acc = cadd(acc, cmulc(lam[(size_t)pr * N + i], w));
+    }
+    float2 g = grad_c[(size_t)(s - 1) * N + i];
+    grad_c[(size_t)(s - 1) * N + i] = cadd(g, acc);
+  }
+}
+
+// ------------------------------------------------------------------ host
+struct C3Work {
+  float2 *u, *x, *r, *r0, *p, *v, *s, *y, *z, *t, *hat;
+  float2 *cdl, *cdr;
+  float2 *dc, *dw, *de, *ds, *dn;
+  Krylov *K;
+  int *pending;
+  size_t bytes;
+};
+
+static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+static C3Work c3_layout(char *base, int N, int P) {
+  C3Work w{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char *ptr = base ? base + off : nullptr;
+    off += align256(bytes);
+    return ptr;
+  };
+  const size_t vec = (size_t)P * N * sizeof(float2);
+  float2 **vecs[] = {&w.u, &w.x, &w.r, &w.r0, &w.p, &w.v, &w.s, &w.y, &w.z, &w.t, &w.hat};
+  for (float2 **v : vecs) *v = reinterpret_cast<float2 *>(take(vec));
+  float2 **diag[] = {&w.cdl, &w.cdr, &w.dc, &w.dw, &w.de, &w.ds, &w.dn};
+  for (float2 **d : diag) *d = reinterpret_cast<float2 *>(take((size_t)N * sizeof(float2)));
+  w.K = reinterpret_cast<Krylov *>(take((size_t)P * sizeof(Krylov)));
+  w.pending = reinterpret_cast<int *>(take(sizeof(int)));
+  w.bytes = off;
+  return w;
+}
+
+static int fft_rows_of(int n) {
+  int r = 4096 / n;
+  if (r > 16) r = 16;
+  return r < 1 ? 1 : r;
+}
+
+}  // namespace tp
+
+using namespace tp;
+
+extern "C" size_t tp_cn3d_workspace_bytes(int32_t n_total, int32_t num_probes) {
+  if (n_total < 1 || num_probes < 1) return 0;
+  return c3_layout(nullptr, n_total, num_probes).bytes;
+}
+
+extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t n_dtype, const tp_cn3d_march_args *a,
+                             void *workspace, size_t workspace_bytes, tp_stream_t stream) {
+  if (op == nullptr || a == nullptr || n_field == nullptr || workspace == nullptr)
+    return set_error(TP_ERR_INVALID, "tp_cn3d_march: NULL argument");
+  const int nf = op->nf, nb = op->nb, N = nf * nb, P = a->num_probes, nz = op->nz, L = nz - 1;
+  if (nf < 2 || nb < 2 || nz < 2 || P < 1) return set_error(TP_ERR_INVALID, "bad 3D sizes nf=%d nb=%d nz=%d P=%d", nf, nb, nz, P);
+  if (a->mode < TP_MODE_FORWARD || a->mode > TP_MODE_ADJOINT_EXACT) return set_error(TP_ERR_INVALID, "bad mode");
+  if ((a->grad_c != nullptr) != (a->u_fwd != nullptr) || (a->grad_c != nullptr && a->mode != TP_MODE_ADJOINT_EXACT))
+    return set_error(TP_ERR_INVALID, "the gradient needs TP_MODE_ADJOINT_EXACT with u_fwd and grad_c");
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255u) != 0) return set_error(TP_ERR_INVALID, "workspace must be 256-byte aligned");
+  C3Work w = c3_layout(static_cast<char *>(workspace), N, P);
+  if (workspace_bytes < w.bytes) return set_error(TP_ERR_WORKSPACE, "3D workspace %zu B < %zu B", workspace_bytes, w.bytes);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+
+  C3Params q{};
+  q.nf = nf;
+  q.nb = nb;
+  q.N = N;
+  q.nz = nz;
+  q.L = L;
+  q.P = P;
+  q.exact = op->exact_ref_coeff;
+  q.is_delta = op->field_is_delta;
+  q.dtype = n_dtype;
+  q.conj_t = (a->mode == TP_MODE_ADJOINT || a->mode == TP_MODE_ADJOINT_EXACT) ? 1 : 0;
+  q.sigma = (a->mode == TP_MODE_REVERSE) ? -1.0 : 1.0;
+  q.k = op->k;
+  q.dz = op->dz;
+  auto tr = [&](const double v[2]) { return z2(q.sigma * v[0], q.sigma * (q.conj_t ? -v[1] : v[1])); };
+  q.mu_x = tr(op->mu_x);
+  q.mu_y = tr(op->mu_y);
+  q.field = n_field;
+  q.kc = w.dc;
+  q.kw = w.dw;
+  q.ke = w.de;
+  q.ks = w.ds;
+  q.kn = w.dn;
+
+  const FftPlan pf = make_fft_plan(nf), pb = make_fft_plan(nb);
+  const int fft_on = a->precond != 0 && pf.npass > 0 && pb.npass > 0;
+  const int rpc = fft_rows_of(nf), cpc = fft_rows_of(nb);
+  const bool tiles_ok = (nb % rpc == 0) && (nf % cpc == 0);
+  const int use_fft = fft_on && tiles_ok;
+  const size_t smem_rows = (size_t)(nf + 2 * rpc * nf) * sizeof(float2);
+  const size_t smem_cols = (size_t)(nb + 2 * cpc * nb) * sizeof(float2);
+  if (use_fft) {
+    TP_CHECK_CUDA(cudaFuncSetAttribute(c3_prec_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
+    TP_CHECK_CUDA(cudaFuncSetAttribute(c3_prec_rows_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
+    TP_CHECK_CUDA(cudaFuncSetAttribute(c3_prec_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cols));
+  }
+  const int rows_cta = use_fft ? rpc : 1;
+  const int max_iter = a->max_iter > 0 ? a->max_iter : 20;
+  const double tol2 = (a->tol > 0 ? a->tol : 1e-6) * (a->tol > 0 ? a->tol : 1e-6);
+  int *stats = a->stats;
+
+  const int eb = 296;
+  c3_diag_kernel<<<eb, 256, 0, st>>>(N, nf, q.sigma, q.conj_t, static_cast<const float2 *>(op->kc),
+                                     static_cast<const float2 *>(op->kw), static_cast<const float2 *>(op->ke),
+                                     static_cast<const float2 *>(op->ks), static_cast<const float2 *>(op->kn), w.dc, w.dw,
+                                     w.de, w.ds, w.dn);
+  // initial state
+  TP_CHECK_CUDA(cudaMemsetAsync(w.u, 0, (size_t)P * N * sizeof(float2), st));
+  if (a->probes != nullptr)
+    TP_CHECK_CUDA(cudaMemcpyAsync(w.u, a->probes, (size_t)P * N * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+  TP_CHECK_CUDA(cudaMemsetAsync(w.K, 0, (size_t)P * sizeof(Krylov), st));
+  const bool backward = a->mode != TP_MODE_FORWARD;
+  const bool flip = a->mode == TP_MODE_ADJOINT;
+  float2 *ust = static_cast<float2 *>(a->u_store);
+  if (ust) c3_store_kernel<<<eb, 256, 0, st>>>(N, P, nz, flip ? L : 0, w.u, ust, nullptr);
+  const dim3 vgrid((N + 256 * 8 - 1) / (256 * 8), P);
+  const int pgrid = (P + 127) / 128;
+  for (int t = 1; t <= L; ++t) {
+    const int s = backward ? (L + 1 - t) : t;
+    c3_center_kernel<<<eb, 256, 0, st>>>(q, s, w.cdl);
+    const float2 *cdr = w.cdl;
+    int use_u = 1;
+    if (a->mode == TP_MODE_ADJOINT_EXACT) {
+      if (t == 1) use_u = 0;  // lambda_{L+1} = 0
+      else {
+        c3_center_kernel<<<eb, 256, 0, st>>>(q, s + 1, w.cdr);
+        cdr = w.cdr;
+      }
+    }
+    const float2 *src = (t == 1) ? static_cast<const float2 *>(a->src_exit) : nullptr;
+    const float2 *shared = a->src_shared ? static_cast<const float2 *>(a->src_shared) + (size_t)(t - 1) * N : nullptr;
+    c3_init_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, cdr, w.u, use_u, src, shared, w.x, w.r, w.r0, w.p, w.v, w.K);
+    c3_scalar_kernel<<<pgrid, 128, 0, st>>>(w.K, P, tol2, 1, stats);
+    for (int it = 0; it < max_iter; ++it) {
+      // p = r + beta (p - omega v); y = Prec(p); v = M y
+      c3_prec_rows_kernel<<<dim3(nb / rows_cta, P), k3Threads, use_fft ? smem_rows : 0, st>>>(
+          pf, q, 0, w.r, w.p, w.v, w.s, use_fft ? w.hat : w.y, w.K, rows_cta, use_fft);
+      if (use_fft) {
+        c3_prec_cols_kernel<<<dim3(nf / cpc, P), k3Threads, smem_cols, st>>>(pb, q, w.hat, w.K, cpc);
+        c3_prec_rows_inv_kernel<<<dim3(nb / rpc, P), k3Threads, smem_rows, st>>>(pf, q, w.hat, w.y, w.K, rpc);
+      }
+      c3_matvec_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, w.y, w.v, w.r0, w.s, w.K, 0);
+      // s = r - alpha v; z = Prec(s); t = M z
+      c3_prec_rows_kernel<<<dim3(nb / rows_cta, P), k3Threads, use_fft ? smem_rows : 0, st>>>(
+          pf, q, 1, w.r, w.p, w.v, w.s, use_fft ? w.hat : w.z, w.K, rows_cta, use_fft);
+      if (use_fft) {
+        c3_prec_cols_kernel<<<dim3(nf / cpc, P), k3Threads, smem_cols, st>>>(pb, q, w.hat, w.K, cpc);
+        c3_prec_rows_inv_kernel<<<dim3(nb / rpc, P), k3Threads, smem_rows, st>>>(pf, q, w.hat, w.z, w.K, rpc);
+      }
+      c3_matvec_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K, 1);
+      c3_update_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.x, w.r, w.r0, w.y, w.z, w.s, w.t, w.K);
+      c3_scalar_kernel<<<pgrid, 128, 0, st>>>(w.K, P, tol2, 0, stats);
+      if (a->host_check && it + 1 < max_iter) {
+        // stop launching iterations once every probe has converged
+        TP_CHECK_CUDA(cudaMemsetAsync(w.pending, 0, sizeof(int), st));
+        c3_pending_kernel<<<pgrid, 128, 0, st>>>(w.K, P, w.pending);
+        int pending = 0;
+        TP_CHECK_CUDA(cudaMemcpyAsync(&pending, w.pending, sizeof(int), cudaMemcpyDeviceToHost, st));
+        TP_CHECK_CUDA(cudaStreamSynchronize(st));
+        if (pending == 0) break;
+      }
+    }
+    c3_finish_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, w.x, w.r0, w.u, w.K);
+    if (stats) c3_stats_kernel<<<pgrid, 128, 0, st>>>(w.K, P, tol2, stats);
+    else TP_CHECK_CUDA(cudaMemsetAsync(w.K, 0, (size_t)P * sizeof(Krylov), st));
+    const int to = flip ? (L - t) : t;
+    if (ust || (t == L && a->exit_out))
+      c3_store_kernel<<<eb, 256, 0, st>>>(N, P, nz, to, w.u, ust, (t == L) ? static_cast<float2 *>(a->exit_out) : nullptr);
+    if (a->grad_c)
+      c3_grad_kernel<<<eb, 256, 0, st>>>(N, P, nz, s, w.u, static_cast<const float2 *>(a->u_fwd),
+                                         static_cast<float2 *>(a->grad_c));
+  }
+  return check_cuda(cudaGetLastError(), "tp_cn3d_march launches");
+}

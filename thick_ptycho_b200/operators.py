@@ -106,3 +106,60 @@ def operator_1d(n, co: BCCoefficients, bc_type: str, dz: float) -> Operator1D:
         c01 += -g
         cnm += -g
     return Operator1D(n, complex(mu), complex(diag), complex(d0), complex(dn), complex(c01), complex(cnm))
+
+
+def operator_2d_diagonals(nx, ny, co: BCCoefficients, bc_type: str):
+    """The 5 diagonals of the 3D (2D-transverse) scaled Laplacian K, K = I − A.
+
+    Restates ``operator_matrices.py:75-126`` and ``boundary_conditions.py:
+    96-130`` row by row.  The operator acts on vectors of length nx·ny with
+    index ``i = b·nx + f`` (``f`` the fast index of ``kron(I_y, A_x)``); the
+    1D part carries the x-edge rules (Dirichlet zero rows, Neumann doubled
+    couplings, impedance ``+β_x``) and the block part the y-edge rules
+    (Dirichlet identity blocks, doubled block couplings, impedance ``+β_y``).
+    Returns ``(center, west, east, south, north)`` complex128 arrays of
+    length nx·ny: ``(K x)_i = c_i x_i + w_i x_{i−1} + e_i x_{i+1} + s_i x_{i−nx}
+    + n_i x_{i+nx}`` (coefficients are zero where the neighbour is absent).
+    """
+    if bc_type not in ("dirichlet", "neumann", "impedance"):
+        raise ValueError(f"3D operators support dirichlet, neumann and impedance, not {bc_type!r}")
+    mux, muy = co.mu_x, co.mu_y
+    f = np.tile(np.arange(nx), ny)
+    b = np.repeat(np.arange(ny), nx)
+    N = nx * ny
+    center = np.full(N, -2 * (mux + muy), dtype=complex)
+    west = np.where(f > 0, mux, 0).astype(complex)
+    east = np.where(f < nx - 1, mux, 0).astype(complex)
+    south = np.where(b > 0, muy, 0).astype(complex)
+    north = np.where(b < ny - 1, muy, 0).astype(complex)
+    fe0, fe1 = f == 0, f == nx - 1
+    be0, be1 = b == 0, b == ny - 1
+    if bc_type == "dirichlet":
+        # 1D Dirichlet rows of A_x: K rows f = 0, nx-1 lose the x part and the diagonal
+        center[fe0 | fe1] = 0
+        east[fe0] = 0
+        west[fe1] = 0
+        # 2D Dirichlet: first/last blocks become identity rows of A (K rows zero)
+        for arr in (center, west, east, south, north):
+            arr[be0 | be1] = 0
+        return center, west, east, south, north
+    east[fe0] *= 2
+    west[fe1] *= 2
+    if bc_type == "impedance":
+        center[fe0 | fe1] += co.beta_x
+    north[be0] *= 2
+    south[be1] *= 2
+    if bc_type == "impedance":
+        center[be0 | be1] += co.beta_y
+    return center, west, east, south, north
+
+
+def transpose_diagonals(nx, center, west, east, south, north):
+    """Diagonals of Kᵀ (the neighbour coefficients move to the neighbour's row)."""
+    N = len(center)
+    w2, e2, s2, n2 = (np.zeros(N, complex) for _ in range(4))
+    w2[1:] = east[:-1]
+    e2[:-1] = west[1:]
+    s2[nx:] = north[:-nx]
+    n2[:-nx] = south[nx:]
+    return center.copy(), w2, e2, s2, n2

@@ -12,6 +12,11 @@ iterative_lu.py:36-197``, ``pwe/solvers/base_solver.py:29-209``,
 * ``_solve_single_probe`` → the same march for one probe with an optional
   ``rhs_block`` (the reconstructor's adjoint and step-size solves).
 
+3D simulation spaces (2D transverse, ``iterative_lu.py`` on the 5-point
+operators of ``operator_matrices.py:75-126``) run through ``tp_cn3d_march``:
+no factorisation is cached (each slice is an FFT-preconditioned BiCGStab
+solve to ``tol``), so the mode cache holds only the device copy of n.
+
 Inputs and outputs are NumPy arrays as in the reference (complex128 out); the
 arithmetic is complex64 with fp64 factorisation.  The ``*_device`` methods
 take and return torch CUDA tensors for callers that keep data on the GPU.
@@ -28,6 +33,7 @@ import torch
 
 from . import _native
 from .cn2d import CN2D
+from .cn3d import CN3D
 from .operators import normalize_bc
 
 _MODES = ("forward", "adjoint", "reverse", "adjoint_exact")
@@ -42,7 +48,7 @@ class _ModeCache:
 
 
 class PWEGpuSolver:
-    """Slice-by-slice Crank–Nicolson PWE solver on one B200 (2D problems)."""
+    """Slice-by-slice Crank–Nicolson PWE solver on one B200 (2D and 3D problems)."""
 
     def __init__(
         self,
@@ -55,6 +61,8 @@ class PWEGpuSolver:
         log=None,
         test_bcs=None,
         device=None,
+        tol=1e-6,
+        max_iter=20,
     ):
         ss = simulation_space
         self.simulation_space = ss
@@ -76,19 +84,30 @@ class PWEGpuSolver:
         self.solver_type = self.__class__.__name__
         self.test_bcs = test_bcs
         self.bc_type = normalize_bc(bc_type)
-        if ss.dimension != 2:
-            raise NotImplementedError("PWEGpuSolver currently handles 2D simulation spaces")
-        self.engine = CN2D(
-            self.block_size,
-            self.nz,
-            ss.k,
-            ss.dx,
-            ss.dz,
-            bc_type=self.bc_type,
-            empty_px=int(getattr(ss, "empty_space_px", 0) or 0),
-            exact_ref_coeff=bool(getattr(ss, "exact_ref_coeff", False)),
-            device=device,
-        )
+        self.dimension = int(ss.dimension)
+        empty_px = int(getattr(ss, "empty_space_px", 0) or 0)
+        if self.dimension == 2:
+            self.engine = CN2D(
+                self.block_size,
+                self.nz,
+                ss.k,
+                ss.dx,
+                ss.dz,
+                bc_type=self.bc_type,
+                empty_px=empty_px,
+                exact_ref_coeff=bool(getattr(ss, "exact_ref_coeff", False)),
+                device=device,
+            )
+        elif self.dimension == 3:
+            if empty_px > 0:
+                # the reference pads only axis 0 of a 3D coefficient array (base_simulation_space.py:363-376)
+                raise NotImplementedError("3D simulation spaces with empty_space_px > 0 are not supported")
+            self.engine = CN3D(self.effective_shape[0], self.effective_shape[1], self.nz, ss.k, ss.dx,
+                               getattr(ss, "dy", ss.dx), ss.dz, bc_type=self.bc_type,
+                               exact_ref_coeff=bool(getattr(ss, "exact_ref_coeff", False)), device=device)
+            self.krylov = dict(tol=tol, max_iter=max_iter)
+        else:
+            raise ValueError(f"dimension must be 2 or 3, not {ss.dimension}")
         self.device = self.engine.device
         self.create_projection_cache()
 
@@ -120,7 +139,7 @@ class PWEGpuSolver:
             n = self.simulation_space.refractive_index_empty
         field = self._field_device(self.get_projected_obj(n, proj_idx=proj_idx))
         cache = self.projection_cache[proj_idx][mode]
-        cache.factors = self.engine.factor(field, mode)
+        cache.factors = self.engine.factor(field, mode) if self.dimension == 2 else field
         cache.n_ref = n
 
     def _get_or_construct_cache(self, n, mode, proj_idx=0, scan_idx=0):
@@ -148,6 +167,25 @@ class PWEGpuSolver:
         rows = [np.asarray(self.test_bcs.test_exact_impedance_rhs_step(j)).ravel() for j in range(1, self.nz)]
         return torch.from_numpy(np.stack(rows).astype(np.complex64)).to(self.device)
 
+    def _step_source(self, rhs_block, mode) -> torch.Tensor:
+        """``rhs_block`` (block_size·(nz−1)) as the (L, N) source of each march step
+        (the adjoint reads column −j at step j, ``iterative_lu.py:172-176``)."""
+        rb = np.asarray(rhs_block).reshape(self.block_size, self.nz - 1)
+        if mode in ("adjoint", "adjoint_exact"):
+            rb = rb[:, ::-1]
+        return torch.from_numpy(np.ascontiguousarray(rb.T).astype(np.complex64)).to(self.device)
+
+    def _march3d(self, field, count, mode, probes, src_shared, store, exit_w):
+        self.engine.march(field, count, mode, probes=probes, src_shared=src_shared, u_store=store, exit_out=exit_w,
+                          **self.krylov)
+
+    def _unstore(self, store) -> torch.Tensor:
+        """Device store → (P, *effective_shape) complex64."""
+        if self.dimension == 2:
+            return self.engine.unchunk(store)
+        P = store.shape[0]
+        return store.permute(0, 2, 1).reshape(P, *self.effective_shape)
+
     def _probes_device(self, probes, count) -> torch.Tensor:
         if isinstance(probes, torch.Tensor):
             t = probes.to(self.device, torch.complex64)
@@ -159,8 +197,9 @@ class PWEGpuSolver:
     def solve_device(self, n=None, mode="forward", rhs_block=None, probes=None, proj_idx=0, full_field=True):
         """Batched march of every (angle, probe) for one projection.
 
-        Returns ``(u_store, exit)``: the chunked full field (A·P, nz, Npad)
-        (or None) and the last-step field (A·P, N), complex64 on the device.
+        Returns ``(u_store, exit)``: the full field (2D: chunked (A·P, nz,
+        Npad); 3D: (A·P, nz, N)) or None, and the last-step field (A·P, N),
+        complex64 on the device.
         """
         if mode not in _MODES:
             raise AssertionError(f"Invalid mode: {mode!r}")
@@ -173,14 +212,14 @@ class PWEGpuSolver:
         fs = self.projection_cache[proj_idx][mode].factors
         src_shared = self._test_bc_source()
         if src_shared is None and rhs_block is not None:
-            rb = np.asarray(rhs_block).reshape(self.block_size, self.nz - 1)
-            if mode in ("adjoint", "adjoint_exact"):
-                rb = rb[:, ::-1]
-            src_shared = torch.from_numpy(np.ascontiguousarray(rb.T).astype(np.complex64)).to(self.device)
+            src_shared = self._step_source(rhs_block, mode)
         pr = self._probes_device(probes, count)
         store = self.engine.new_store(count) if full_field else None
         exit_w = torch.empty((count, self.block_size), dtype=torch.complex64, device=self.device)
-        self.engine.march(fs, count, probes=pr, src_shared=src_shared, u_store=store, exit_out=exit_w)
+        if self.dimension == 3:
+            self._march3d(fs, count, mode, pr, src_shared, store, exit_w)
+        else:
+            self.engine.march(fs, count, probes=pr, src_shared=src_shared, u_store=store, exit_out=exit_w)
         return store, exit_w
 
     def solve(self, n=None, mode="forward", rhs_block=None, probes=None, **kwargs) -> np.ndarray:
@@ -194,7 +233,7 @@ class PWEGpuSolver:
         out = np.zeros((self.num_projections, self.num_angles, self.num_probes, *self.effective_shape), dtype=complex)
         for proj_idx in range(self.num_projections):
             store, _ = self.solve_device(n=n, mode=mode, rhs_block=rhs_block, probes=probes, proj_idx=proj_idx)
-            u = self.engine.unchunk(store).cpu().numpy().astype(np.complex128)
+            u = self._unstore(store).cpu().numpy().astype(np.complex128)
             out[proj_idx] = u.reshape(self.num_angles, self.num_probes, *self.effective_shape)
         if self.verbose:
             self._log(f"[{self.solver_type}] solved {self.num_projections * self.num_angles * self.num_probes} "
@@ -212,12 +251,17 @@ class PWEGpuSolver:
         pr = None if probe is None else self._probes_device(probe, 1)
         src_shared = self._test_bc_source()
         src_probe = None
-        if src_shared is None and rhs_block is not None:
-            rb = np.asarray(rhs_block).reshape(self.block_size, self.nz - 1)
-            src_probe = torch.from_numpy(np.ascontiguousarray(rb.T).astype(np.complex64)).to(self.device)[None]
         store = self.engine.new_store(1)
-        self.engine.march(fs, 1, probes=pr, src_shared=src_shared, src_probe=src_probe, u_store=store)
-        return self.engine.unchunk(store)[0].cpu().numpy().astype(np.complex128)
+        if self.dimension == 3:
+            if src_shared is None and rhs_block is not None:
+                src_shared = self._step_source(rhs_block, mode)
+            self._march3d(fs, 1, mode, pr, src_shared, store, None)
+        else:
+            if src_shared is None and rhs_block is not None:
+                rb = np.asarray(rhs_block).reshape(self.block_size, self.nz - 1)
+                src_probe = torch.from_numpy(np.ascontiguousarray(rb.T).astype(np.complex64)).to(self.device)[None]
+            self.engine.march(fs, 1, probes=pr, src_shared=src_shared, src_probe=src_probe, u_store=store)
+        return self._unstore(store)[0].reshape(self.block_size, self.nz).cpu().numpy().astype(np.complex128)
 
     # --------------------------------------------------------------- outputs
     def get_gradient(self, n):
