@@ -430,10 +430,13 @@ static C3Work c3_layout(char *base, int N, int P) {
   return w;
 }
 
-static int fft_rows_of(int n) {
+// FFT rows per CTA: at most 16 and 4096 elements, and a divisor of the row count.
+static int fft_rows_of(int n, int rows) {
   int r = 4096 / n;
   if (r > 16) r = 16;
-  return r < 1 ? 1 : r;
+  if (r < 1) r = 1;
+  while (rows % r != 0) --r;
+  return r;
 }
 
 }  // namespace tp
@@ -454,6 +457,8 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   if (a->mode < TP_MODE_FORWARD || a->mode > TP_MODE_ADJOINT_EXACT) return set_error(TP_ERR_INVALID, "bad mode");
   if ((a->grad_c != nullptr) != (a->u_fwd != nullptr) || (a->grad_c != nullptr && a->mode != TP_MODE_ADJOINT_EXACT))
     return set_error(TP_ERR_INVALID, "the gradient needs TP_MODE_ADJOINT_EXACT with u_fwd and grad_c");
+  if (a->mode == TP_MODE_ADJOINT_EXACT && a->probes != nullptr)
+    return set_error(TP_ERR_INVALID, "TP_MODE_ADJOINT_EXACT starts from lambda = 0 (probes must be NULL)");
   if ((reinterpret_cast<uintptr_t>(workspace) & 255u) != 0) return set_error(TP_ERR_INVALID, "workspace must be 256-byte aligned");
   C3Work w = c3_layout(static_cast<char *>(workspace), N, P);
   if (workspace_bytes < w.bytes) return set_error(TP_ERR_WORKSPACE, "3D workspace %zu B < %zu B", workspace_bytes, w.bytes);
@@ -485,9 +490,8 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
 
   const FftPlan pf = make_fft_plan(nf), pb = make_fft_plan(nb);
   const int fft_on = a->precond != 0 && pf.npass > 0 && pb.npass > 0;
-  const int rpc = fft_rows_of(nf), cpc = fft_rows_of(nb);
-  const bool tiles_ok = (nb % rpc == 0) && (nf % cpc == 0);
-  const int use_fft = fft_on && tiles_ok;
+  const int rpc = fft_rows_of(nf, nb), cpc = fft_rows_of(nb, nf);
+  const int use_fft = fft_on;
   const size_t smem_rows = (size_t)(nf + 2 * rpc * nf) * sizeof(float2);
   const size_t smem_cols = (size_t)(nb + 2 * cpc * nb) * sizeof(float2);
   if (use_fft) {
