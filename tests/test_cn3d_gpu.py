@@ -104,17 +104,23 @@ def test_fft_preconditioned_against_oracle(bc, precond):
         assert rel(u[p], ref) < TOL, (p, rel(u[p], ref))
 
 
-def test_reverse_mode_against_oracle():
+@pytest.mark.parametrize("bc,dz", [("neumann", 1.0), ("impedance", 0.5)])
+def test_reverse_mode_against_oracle(bc, dz):
+    """Reverse (σ = −1) march.  With impedance edges the reversed corner
+    diagonal is 1 + Kc = 1 − dz/dx + O(μ): at dz = dx it is ≈ −0.08i, the
+    corner amplification per step is |1 − Kc|/|1 + Kc| ≈ 25, and complex64
+    round-off grows like 25^L (the complex128 march is no reference there);
+    dz = dx/2 keeps the amplification at ≈ 3."""
     rng = np.random.default_rng(3)
     nf = nb = 32
     nz, k, P = 9, 4 * np.pi, 3
     n = _field(rng, nf * nb, nz)
     probes = _gauss(nf, nb, rng.uniform(10, 22, (P, 2)), 5.0)
-    eng = CN3D(nf, nb, nz, k, 1.0, 1.0, 1.0, "impedance")
+    eng = CN3D(nf, nb, nz, k, 1.0, 1.0, dz, bc)
     u = run(eng, n, P, "reverse", probes=c64(probes))
-    co = po.bc_coefficients(k, 1.0, 1.0, dy=1.0, bc_type="impedance", dimension=3)
-    A, B = po.step_matrices_2d(nf, nb, co, "impedance", 1.0)
-    C = po.object_contribution(n, k, 1.0)
+    co = po.bc_coefficients(k, 1.0, dz, dy=1.0, bc_type=bc, dimension=3)
+    A, B = po.step_matrices_2d(nf, nb, co, bc, dz)
+    C = po.object_contribution(n, k, dz)
     for p in range(P):
         assert rel(u[p], po.march(A, B, C, probes[p], "reverse")) < TOL
 
