@@ -42,7 +42,7 @@ UNIT = "probe·slice/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--config", default="2d-fwd-adj-2048x1024-p512")
@@ -60,27 +60,48 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    """nvidia-smi samples (every 50 ms) of SM clock and throttle reasons.
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    Started before the warm-up so that the sampler is running when the timed
+    region begins; ``begin()``/``end()`` mark the timed region on the host
+    clock and ``summary()`` keeps the rows whose nvidia-smi timestamp falls
+    inside it (widened to the whole run, and said so, when the timed region
+    is shorter than one sampling interval)."""
+
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "100"],
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
+
+    def wait_first(self, limit_s=5.0):
+        """Block until the sampler has written one row (or `limit_s` passes)."""
+        t = time.time()
+        while self.proc is not None and time.time() - t < limit_s:
+            if os.path.getsize(self.path) > 0:
+                return
+            time.sleep(0.02)
+
+    def begin(self):
+        self.t0 = time.time()
+
+    def end(self):
+        self.t1 = time.time()
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -90,22 +111,45 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
+    @staticmethod
+    def _stamp(s):
+        import datetime
+
+        try:
+            return datetime.datetime.strptime(s.strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
+
     def summary(self):
         try:
-            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+            rows = [[x.strip() for x in r.split(",")] for r in open(self.path).read().strip().splitlines() if r.strip()]
         except Exception:
             rows = []
         finally:
             if self.path and os.path.exists(self.path):
                 os.unlink(self.path)
+        rows = [r for r in rows if len(r) >= 10]
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        window = "timed"
+        sel = rows
+        if self.t0 is not None and self.t1 is not None:
+            sel = [r for r in rows if (ts := self._stamp(r[0])) is not None and self.t0 <= ts <= self.t1]
+            if not sel:
+                sel, window = rows, "whole run (timed region shorter than the 50 ms sampling interval)"
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+
+        sm = [v for v in (num(r[2]) for r in sel) if v is not None]
+        mx = [v for v in (num(r[3]) for r in sel) if v is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and r[5 + i].strip() == "Active"})
+        reasons = sorted({names[i] for r in sel for i in range(4) if r[6 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(sel), "window": window}
 
 
 # --------------------------------------------------------------------------
@@ -260,14 +304,16 @@ def run_ours(a):
             dist.all_reduce(torch.view_as_real(g))
         return g
 
-    for _ in range(a.warmup):
-        step(False)
-    eng.device_status()
-    torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
     with ClockSampler(local) as clk:
+        clk.wait_first()
+        for _ in range(a.warmup):
+            step(False)
+        eng.device_status()
         torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clk.begin()
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
@@ -275,6 +321,7 @@ def run_ours(a):
             step(True)
         t1.record(stream)
         torch.cuda.synchronize()
+        clk.end()
         if dist is not None:
             dist.barrier()
     eng.device_status()
