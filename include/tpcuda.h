@@ -231,6 +231,8 @@ TP_API int tp_ms2d_backward(const tp_ms2d_op *op, const void *trans, const void 
  * solved by FFT-preconditioned BiCGStab in delta form (see cn3d.cu), batched
  * over probes, fp64 inner products.  Replaces the per-slice SuperLU of the 2D
  * operator (iterative_lu.py:103-133) and the per-probe march (:138-197). */
+struct tp_cnn_model;
+
 typedef struct tp_cn3d_op {
   int32_t nf, nb, nz;        /* fast / block transverse sizes, z nodes          */
   int32_t exact_ref_coeff;   /* coef = (k/2i)(n^2-1) instead of (k/i)(n-1)       */
@@ -247,7 +249,9 @@ typedef struct tp_cn3d_march_args {
   int32_t num_probes, mode;  /* tp_mode                                          */
   int32_t max_iter;          /* BiCGStab iterations per solve (0 = 20)           */
   int32_t precond;           /* 1: periodic FFT preconditioner (when nf, nb are
-                                2^a 3^b 5^c and tile), 0: none                  */
+                                2^a 3^b 5^c and tile), 0: none, 2: the FFT
+                                preconditioner with the learned per-pixel
+                                correction of `model` (not REVERSE)             */
   int32_t host_check;        /* 1: stop launching iterations once all probes of
                                 a slice converged (synchronises the stream)     */
   int32_t reserved;
@@ -262,12 +266,84 @@ typedef struct tp_cn3d_march_args {
                                 sum_p lambda_s conj(u_s + u_{s-1}); caller zeroes */
   int32_t *stats;            /* device int32[4]: total iterations, solves, solves
                                 whose true residual exceeded 10 tol, largest
-                                iteration count; accumulated; or NULL            */
+                                iteration count; accumulated; or NULL.  A
+                                caller of the learned form re-runs the march
+                                with precond = 1 when stats[2] grew (fallback) */
+  const struct tp_cnn_model *model;  /* precond == 2: the network            */
+  void *learned_ws;          /* precond == 2: tp_cn3d_learned_ws_bytes, 256-B aligned */
+  size_t learned_ws_bytes;
+  /* Training pairs (no counterpart in the reference): at every step t with
+   * t % train_every == 0, index k = t/train_every - 1 receives a vector x and
+   * z0 = M0^{-1} v with (I - P_s) x = v, M0^{-1} the plain FFT preconditioner
+   * (train_z0 and train_sol, (P, N) each), and the object diagonal
+   * sigma*T(c_s) of the slice (train_diag, (N)).  train_kind 0: v is the
+   * step's right-hand side and x its converged update; 1: x is uniform
+   * complex white noise (a counter hash of step, probe and row) and
+   * v = (I - P_s) x exactly. */
+  void *train_z0, *train_sol, *train_diag;
+  int32_t train_every;       /* 0 = no training pairs                           */
+  int32_t train_kind;
 } tp_cn3d_march_args;
 
 TP_API size_t tp_cn3d_workspace_bytes(int32_t n_total, int32_t num_probes);
+TP_API size_t tp_cn3d_learned_ws_bytes(int32_t nf, int32_t nb, int32_t num_probes);
 TP_API int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t n_dtype, const tp_cn3d_march_args *args,
                          void *workspace, size_t workspace_bytes, tp_stream_t stream);
+
+/* ------------------------------------------------ learned 3D preconditioner
+ * The reference has no learned component; these entry points are this
+ * library's own addition to the 3D path (the north-star "learned" form).
+ * A four-layer 3x3 CNN (bf16 weights, fp32 accumulation on the tcgen05
+ * tensor cores) maps the object diagonal d of one slice to a 13-tap complex
+ * filter per pixel; the learned preconditioner is y = z + sum_t F_t(x) z(x + o_t)
+ * with z the plain FFT-preconditioned vector, taps o_t = (0,0), (0,-1), (0,1),
+ * (-1,0), (1,0), (-1,-1), (-1,1), (1,-1), (1,1), (0,-2), (0,2), (-2,0), (2,0)
+ * as (row, column) offsets of the nb x nf image (vector index b*nf + f).
+ *
+ * Activations use a padded-linear bf16 layout (one-pixel zero border around
+ * each image, images back to back, channels in chunks of 8); buffers sized by
+ * tp_cnn_act_bytes must be zeroed once before first use (only interior pixels
+ * are ever written).  Weights of a layer with cin inputs and 32 outputs:
+ * bf16 [9 taps (row-major 3x3)][cin/8][32][8]. */
+typedef struct tp_cnn_model {
+  const void *w[4];     /* layers 16->32, 32->32, 32->32, 32->32 (26 used)   */
+  const float *b[4];    /* fp32 biases (32 each) or NULL                      */
+  float kappa;          /* scale of the d features                            */
+  float out_scale;      /* the filter is out_scale * (last layer + bias)      */
+} tp_cnn_model;
+
+enum tp_conv_epilogue {
+  TP_CONV_RELU = 0,     /* out = relu(conv + b), bf16 32 channels             */
+  TP_CONV_MASK = 1,     /* out = conv * (aux > 0) (ReLU backward), bf16       */
+  TP_CONV_FILTER = 2    /* out = out_scale (conv + b) as float2 (13, batch*nf*nb) */
+};
+
+TP_API size_t tp_cnn_act_bytes(int32_t nf, int32_t nb, int32_t batch, int32_t channels);
+/* 16 feature channels of `batch` diagonals d (float2 (batch, nf*nb)). */
+TP_API int tp_cnn_features(int32_t nf, int32_t nb, int32_t batch, const void *diag, float kappa, void *feat,
+                           tp_stream_t stream);
+/* One 3x3 layer, cin in {16, 32} (TP_CONV_RELU) or 32 (MASK, FILTER). */
+TP_API int tp_conv3x3_bf16(int32_t nf, int32_t nb, int32_t batch, int32_t cin, int32_t epilogue, const void *in,
+                           const void *weights, const float *bias, const void *aux, void *out, float out_scale,
+                           tp_stream_t stream);
+/* dw[tap][c][o] += sum_q x[q+o_tap][c] dy[q][o] (fp32 (9, cin, 32)); db[o] += sum_q dy[q][o] (db may be NULL). */
+TP_API int tp_conv3x3_wgrad(int32_t nf, int32_t nb, int32_t batch, int32_t cin, const void *x, const void *dy,
+                            float *dw, float *db, tp_stream_t stream);
+/* y_v = z_v + sum_t F_t z_v(x + o_t) for nvec vectors (nvec, nf*nb) float2;
+ * vector v uses filter image v / per_image (per_image = 0: image 0 for all);
+ * conj != 0 applies conj(F) (the adjoint modes). */
+TP_API int tp_cnn_filter_apply(int32_t nf, int32_t nb, int32_t nvec, int32_t per_image, int32_t conj,
+                               const void *filt, const void *z, void *y, tp_stream_t stream);
+/* Last-layer gradient (bf16, 32 channels, padded-linear) of
+ * sum_v |y_v - t_v|^2 s_v given e_v = s_v (y_v - t_v):
+ * 2 out_scale conj(z_v(x+o_t)) e_v(x) summed over the per_image vectors of
+ * each of the nimg filter images. */
+TP_API int tp_cnn_filter_grad(int32_t nf, int32_t nb, int32_t nimg, int32_t per_image, const void *z, const void *e,
+                              float out_scale, void *dy, tp_stream_t stream);
+/* Whole forward (features, 4 layers) of `batch` diagonals into the filter. */
+TP_API size_t tp_cnn_forward_ws_bytes(int32_t nf, int32_t nb, int32_t batch);
+TP_API int tp_cnn_forward(int32_t nf, int32_t nb, int32_t batch, const tp_cnn_model *model, const void *diag,
+                          void *ws, size_t ws_bytes, void *filt, tp_stream_t stream);
 
 /* Synchronise `stream` and report device-side failures of earlier launches
  * (a bounded wait that gave up).  Returns TP_ERR_TIMEOUT and clears the flag

@@ -107,8 +107,24 @@ class TpCn3dMarchArgs(ctypes.Structure):
         ("probes", ctypes.c_void_p), ("src_shared", ctypes.c_void_p), ("src_exit", ctypes.c_void_p),
         ("u_store", ctypes.c_void_p), ("exit_out", ctypes.c_void_p), ("u_fwd", ctypes.c_void_p),
         ("grad_c", ctypes.c_void_p), ("stats", ctypes.c_void_p),
+        ("model", ctypes.c_void_p), ("learned_ws", ctypes.c_void_p), ("learned_ws_bytes", ctypes.c_size_t),
+        ("train_z0", ctypes.c_void_p), ("train_sol", ctypes.c_void_p), ("train_diag", ctypes.c_void_p),
+        ("train_every", ctypes.c_int32), ("train_kind", ctypes.c_int32),
     ]
 
+
+class TpCnnModel(ctypes.Structure):
+    _fields_ = [
+        ("w", ctypes.c_void_p * 4),
+        ("b", ctypes.c_void_p * 4),
+        ("kappa", ctypes.c_float),
+        ("out_scale", ctypes.c_float),
+    ]
+
+
+CONV_RELU = 0
+CONV_MASK = 1
+CONV_FILTER = 2
 
 # (name, restype, argtypes) of every exported symbol of include/tpcuda.h
 SIGNATURES = [
@@ -138,8 +154,21 @@ SIGNATURES = [
     ("tp_ms2d_backward", ctypes.c_int, [ctypes.POINTER(TpMs2dOp), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                         ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
     ("tp_cn3d_workspace_bytes", ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
+    ("tp_cn3d_learned_ws_bytes", ctypes.c_size_t, [ctypes.c_int32] * 3),
     ("tp_cn3d_march", ctypes.c_int, [ctypes.POINTER(TpCn3dOp), ctypes.c_void_p, ctypes.c_int32,
                                      ctypes.POINTER(TpCn3dMarchArgs), ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    ("tp_cnn_act_bytes", ctypes.c_size_t, [ctypes.c_int32] * 4),
+    ("tp_cnn_features", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_float,
+                                       ctypes.c_void_p, ctypes.c_void_p]),
+    ("tp_conv3x3_bf16", ctypes.c_int, [ctypes.c_int32] * 5 + [ctypes.c_void_p] * 5 + [ctypes.c_float, ctypes.c_void_p]),
+    ("tp_conv3x3_wgrad", ctypes.c_int, [ctypes.c_int32] * 4 + [ctypes.c_void_p] * 5),
+    ("tp_cnn_filter_apply", ctypes.c_int, [ctypes.c_int32] * 5 + [ctypes.c_void_p] * 4),
+    ("tp_cnn_filter_grad", ctypes.c_int, [ctypes.c_int32] * 4 + [ctypes.c_void_p] * 2 + [ctypes.c_float] +
+     [ctypes.c_void_p] * 2),
+    ("tp_cnn_forward_ws_bytes", ctypes.c_size_t, [ctypes.c_int32] * 3),
+    ("tp_cnn_forward", ctypes.c_int, [ctypes.c_int32] * 3 + [ctypes.POINTER(TpCnnModel), ctypes.c_void_p,
+                                                             ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                                                             ctypes.c_void_p]),
     ("tp_device_status", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ("tp_last_error_string", ctypes.c_char_p, []),
     ("tp_version", ctypes.c_int, []),

@@ -46,7 +46,10 @@ class CN3D:
         self.co = co
         self._ws = None
         self._ws_P = None
+        self._lws = None
+        self._lws_P = None
         self.stats = torch.zeros(4, dtype=torch.int32, device=self.device)
+        self.fallbacks = 0
 
     def op(self, is_delta=False) -> _native.TpCn3dOp:
         o = _native.TpCn3dOp()
@@ -64,13 +67,56 @@ class CN3D:
             self._ws_P = P
         return self._ws
 
+    def learned_workspace(self, P):
+        if self._lws is None or self._lws_P != P:
+            nbytes = int(self.lib.tp_cn3d_learned_ws_bytes(self.nx, self.ny, P))
+            self._lws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            self._lws_P = P
+        return self._lws
+
     def new_store(self, P):
         return torch.empty((P, self.nz, self.N), dtype=torch.complex64, device=self.device)
 
     def march(self, field: torch.Tensor, num_probes: int, mode="forward", probes=None, src_shared=None, src_exit=None,
               u_store=None, exit_out=None, u_fwd=None, grad_c=None, tol=1e-6, max_iter=20, precond=True,
-              host_check=True, is_delta=False):
-        """One batched march; tensors complex64 (field complex128/complex64 (N, nz))."""
+              host_check=True, is_delta=False, model=None, train=None, train_every=0, fallback=True):
+        """One batched march; tensors complex64 (field complex128/complex64 (N, nz)).
+
+        ``precond``: True/"fft" (periodic FFT preconditioner), False/"none", or
+        "learned" (FFT preconditioner with the per-pixel correction of
+        ``model``, a :class:`learned.LearnedPreconditioner`).  With "learned"
+        and ``fallback``, a march in which any solve missed its tolerance
+        (judged by the true residual) is re-run with the plain FFT
+        preconditioner; ``self.fallbacks`` counts such re-runs.  ``train`` is a
+        :class:`learned.TrainingPairs` whose buffers receive the pair of every
+        ``train_every``-th step (see :func:`generate_pairs`)."""
+        if precond == "learned":
+            if model is None:
+                raise ValueError('precond="learned" needs a model')
+            if fallback:
+                before = int(self.stats[2].item())
+                self._march(field, num_probes, mode, probes, src_shared, src_exit, u_store, exit_out, u_fwd, grad_c, tol,
+                            max_iter, 2, host_check, is_delta, model, train, train_every)
+                if int(self.stats[2].item()) > before:
+                    self.fallbacks += 1
+                    if grad_c is not None:
+                        raise RuntimeError("learned adjoint solve missed its tolerance; re-run with precond=True "
+                                           "(the gradient accumulator already holds a partial sum)")
+                    self._march(field, num_probes, mode, probes, src_shared, src_exit, u_store, exit_out, u_fwd,
+                                grad_c, tol, max_iter, 1, host_check, is_delta, None, train, train_every)
+                return
+            code = 2
+        elif precond in (True, "fft", 1):
+            code = 1
+        elif precond in (False, "none", 0, None):
+            code = 0
+        else:
+            raise ValueError(f"unknown preconditioner {precond!r}")
+        self._march(field, num_probes, mode, probes, src_shared, src_exit, u_store, exit_out, u_fwd, grad_c, tol,
+                    max_iter, code, host_check, is_delta, model, train, train_every)
+
+    def _march(self, field, num_probes, mode, probes, src_shared, src_exit, u_store, exit_out, u_fwd, grad_c, tol,
+               max_iter, precond, host_check, is_delta, model, train, train_every):
         P = int(num_probes)
         field = field.reshape(self.N, self.nz).contiguous()
         mode_i = _native.MODES[mode] if isinstance(mode, str) else int(mode)
@@ -85,6 +131,19 @@ class CN3D:
         a.probes, a.src_shared, a.src_exit = _ptr(probes), _ptr(src_shared), _ptr(src_exit)
         a.u_store, a.exit_out, a.u_fwd, a.grad_c = _ptr(u_store), _ptr(exit_out), _ptr(u_fwd), _ptr(grad_c)
         a.stats = ctypes.c_void_p(self.stats.data_ptr())
+        if precond == 2:
+            lws = self.learned_workspace(P)
+            mdl = model.model()
+            a.model = ctypes.cast(ctypes.pointer(mdl), ctypes.c_void_p)
+            a.learned_ws, a.learned_ws_bytes = _ptr(lws), lws.numel()
+        if train is not None and train_every > 0:
+            S = self.L // int(train_every)
+            if tuple(train.z0.shape) != (S, P, self.N) or tuple(train.sol.shape) != (S, P, self.N) or \
+                    tuple(train.diag.shape) != (S, self.N):
+                raise ValueError(f"training buffers must be ({S}, {P}, {self.N}) and ({S}, {self.N})")
+            a.train_z0, a.train_sol, a.train_diag = _ptr(train.z0), _ptr(train.sol), _ptr(train.diag)
+            a.train_every = int(train_every)
+            a.train_kind = 1 if train.kind == "noise" else 0
         ws = self.workspace(P)
         dt = _native.C128 if field.dtype == torch.complex128 else _native.C64
         o = self.op(is_delta)
@@ -161,3 +220,27 @@ class PWEGradient3D:
         ge = (e.N * torch.fft.ifft2(gU)).to(torch.complex64).reshape(-1, e.N)
         g = self.backward(field, ge)
         return float(loss.item()), g.reshape(e.nx, e.ny, e.nz)
+
+
+def generate_pairs(engine: CN3D, field, probes, every=1, tol=1e-6, max_iter=20, mode="forward", kind="rhs"):
+    """Training pairs from a plain FFT-preconditioned march over `field`:
+    every `every`-th step gives, per probe, z0 = M0⁻¹ v and x with
+    (I − P_s) x = v, and the slice's object diagonal (see
+    :class:`learned.TrainingPairs`).  kind "rhs": v is the step's right-hand
+    side and x its converged update; kind "noise": x is white noise and
+    v = (I − P_s) x, which exposes the correction to every spatial frequency
+    (the Krylov search directions are rougher than the right-hand sides)."""
+    from .learned import TrainingPairs
+
+    if kind not in ("rhs", "noise"):
+        raise ValueError(f"unknown pair kind {kind!r}")
+    P = probes.shape[0]
+    S = engine.L // int(every)
+    N = engine.N
+    dev = engine.device
+    pairs = TrainingPairs(engine.nx, engine.ny, torch.empty((S, P, N), dtype=torch.complex64, device=dev),
+                          torch.empty((S, P, N), dtype=torch.complex64, device=dev),
+                          torch.empty((S, N), dtype=torch.complex64, device=dev), kind)
+    engine.march(field, P, mode, probes=probes, tol=tol, max_iter=max_iter, precond=True, train=pairs,
+                 train_every=every)
+    return pairs

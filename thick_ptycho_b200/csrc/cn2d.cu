@@ -550,7 +550,7 @@ __global__ void cn2d_grad_to_n_kernel(const GradParams q) {
 // Device error word (timeouts of bounded waits); read by tp_device_status.
 __device__ int g_device_error;
 
-static int *device_error_ptr() {
+int *device_error_ptr() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
   static int *ptrs[64] = {nullptr};

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include "cnn_internal.cuh"
 #include "fft.cuh"
 #include "tp_common.cuh"
 #include "tp_errors.h"
@@ -179,19 +180,25 @@ __global__ void c3_scalar_kernel(Krylov *K, int P, double tol2, int first, int *
 // Forward row FFTs of the preconditioner input, formed on the fly:
 //   mode 0: p := r + beta (p - omega v)  (p updated in place), input p
 //   mode 1: s := r - alpha v             (s written),          input s
+//   mode 2: input r as is (K may be NULL: every probe is transformed)
 // Grid (nb / rpc, P).
 __global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan pl, const C3Params q, int mode,
                                                                  const float2 *r, float2 *p, const float2 *v, float2 *s,
                                                                  float2 *hat, const Krylov *K, int rpc, int fft_on) {
   extern __shared__ __align__(16) float2 fsm[];
   const int n = q.nf, pr = blockIdx.y;
-  const Krylov &k = K[pr];
-  if (k.done) return;
+  if (K != nullptr && K[pr].done) return;
   float2 *tw = fsm, *a = tw + n, *b = a + rpc * n;
   const size_t off = (size_t)pr * q.N + (size_t)blockIdx.x * rpc * n;
   const int tot = rpc * n;
   if (fft_on) fft_twiddles(tw, n, threadIdx.x, blockDim.x);
-  if (mode == 0) {
+  if (mode == 2) {
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+      if (fft_on) a[e] = r[off + e];
+      else hat[off + e] = r[off + e];
+    }
+  } else if (mode == 0) {
+    const Krylov &k = K[pr];
     const double den = k.rho_prev.x * k.rho_prev.x + k.rho_prev.y * k.rho_prev.y;
     const double2 beta = den > 0.0 ? zmul(zdiv(k.rho_cur, k.rho_prev), zdiv(k.alpha, k.omega)) : z2(0, 0);
     const float2 bt = to_f2(beta), om = to_f2(k.omega);
@@ -202,6 +209,7 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan p
       else hat[off + e] = pv;
     }
   } else {
+    const Krylov &k = K[pr];
     const double den = k.acc_r0v.x * k.acc_r0v.x + k.acc_r0v.y * k.acc_r0v.y;
     const double2 alpha = den > 0.0 ? zdiv(k.rho_cur, k.acc_r0v) : z2(0, 0);
     const float2 al = to_f2(alpha);
@@ -224,7 +232,7 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_cols_kernel(const FftPlan p
                                                                  const Krylov *K, int cpc) {
   extern __shared__ __align__(16) float2 fsm[];
   const int nb = q.nb, nf = q.nf, pr = blockIdx.y;
-  if (K[pr].done) return;
+  if (K != nullptr && K[pr].done) return;
   float2 *tw = fsm, *a = tw + nb, *b = a + cpc * nb;
   const int f0 = blockIdx.x * cpc;
   float2 *base = hat + (size_t)pr * q.N;
@@ -259,7 +267,7 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_inv_kernel(const FftPl
                                                                      int rpc) {
   extern __shared__ __align__(16) float2 fsm[];
   const int n = q.nf, pr = blockIdx.y;
-  if (K[pr].done) return;
+  if (K != nullptr && K[pr].done) return;
   float2 *tw = fsm, *a = tw + n, *b = a + rpc * n;
   const size_t off = (size_t)pr * q.N + (size_t)blockIdx.x * rpc * n;
   const int tot = rpc * n;
@@ -399,6 +407,52 @@ __global__ void c3_grad_kernel(int N, int P, int nz, int s, const float2 *__rest
   }
 }
 
+// Learned correction of the preconditioned vector: out = z + sum_t F_t z(x + o_t)
+// (conj(F) in the adjoint modes).  Grid (chunks, P).
+__global__ void __launch_bounds__(k3Threads) c3_filter_kernel(const C3Params q, const float2 *__restrict__ F,
+                                                              const float2 *__restrict__ z, float2 *out,
+                                                              const Krylov *K) {
+  const int pr = blockIdx.y;
+  if (K != nullptr && K[pr].done) return;
+  const size_t off = (size_t)pr * q.N;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
+    const int b = i / q.nf, f = i - b * q.nf;
+    out[off + i] = filter_apply_px(F, 0, (size_t)q.N, z + off, q.nb, q.nf, b, f, q.conj_t);
+  }
+}
+
+// out = (I - P_s) x (no inner products): right-hand sides of the white-noise
+// training pairs.  Grid (chunks, P).
+__global__ void __launch_bounds__(k3Threads) c3_apply_a_kernel(const C3Params q, const float2 *__restrict__ cd,
+                                                               const float2 *__restrict__ x, float2 *out) {
+  const size_t off = (size_t)blockIdx.y * q.N;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x)
+    out[off + i] = csub(x[off + i], apply_P(q, cd, x + off, i));
+}
+
+// x = uniform complex white noise in [-1, 1]^2 from a counter hash of
+// (step, probe, row): reproducible, independent of the launch shape.
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__global__ void c3_noise_kernel(int N, int P, int step, float2 *x) {
+  const size_t total = (size_t)P * N;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const uint64_t h = mix64(((uint64_t)step << 40) ^ (uint64_t)e);
+    const float a = (float)(h >> 40) * (1.f / 16777216.f), b = (float)((h >> 16) & 0xFFFFFFu) * (1.f / 16777216.f);
+    x[e] = make_float2(2.f * a - 1.f, 2.f * b - 1.f);
+  }
+}
+
+// out[i] = cd[i] - kc[i]: the object part sigma*T(c_s) of the slice's diagonal.
+__global__ void c3_diag_diff_kernel(int N, const float2 *__restrict__ cd, const float2 *__restrict__ kc, float2 *out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+    out[i] = make_float2(cd[i].x - kc[i].x, cd[i].y - kc[i].y);
+}
+
 // ------------------------------------------------------------------ host
 struct C3Work {
   float2 *u, *x, *r, *r0, *p, *v, *s, *y, *z, *t, *hat;
@@ -439,9 +493,39 @@ static int fft_rows_of(int n, int rows) {
   return r;
 }
 
+// Learned-preconditioner workspace: the CNN activations of one slice, the
+// slice's filter (13, N) and the plain-preconditioned vectors (P, N).
+struct C3Learned {
+  char *cnn;
+  float2 *F, *zt;
+  size_t cnn_bytes, bytes;
+};
+
+static C3Learned c3_learned_layout(char *base, int nf, int nb, int P) {
+  C3Learned l{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char *ptr = base ? base + off : nullptr;
+    off += align256(bytes);
+    return ptr;
+  };
+  const size_t N = (size_t)nf * nb;
+  l.cnn_bytes = cnn_forward_ws_bytes(conv_geom(nb, nf, 1));
+  l.cnn = take(l.cnn_bytes);
+  l.F = reinterpret_cast<float2 *>(take((size_t)kFilterTaps * N * sizeof(float2)));
+  l.zt = reinterpret_cast<float2 *>(take((size_t)P * N * sizeof(float2)));
+  l.bytes = off;
+  return l;
+}
+
 }  // namespace tp
 
 using namespace tp;
+
+extern "C" size_t tp_cn3d_learned_ws_bytes(int32_t nf, int32_t nb, int32_t num_probes) {
+  if (nf < 1 || nb < 1 || num_probes < 1) return 0;
+  return c3_learned_layout(nullptr, nf, nb, num_probes).bytes;
+}
 
 extern "C" size_t tp_cn3d_workspace_bytes(int32_t n_total, int32_t num_probes) {
   if (n_total < 1 || num_probes < 1) return 0;
@@ -490,6 +574,21 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
 
   const FftPlan pf = make_fft_plan(nf), pb = make_fft_plan(nb);
   const int fft_on = a->precond != 0 && pf.npass > 0 && pb.npass > 0;
+  const bool learned = a->precond == 2;
+  C3Learned lw{};
+  if (learned) {
+    if (a->model == nullptr || a->learned_ws == nullptr)
+      return set_error(TP_ERR_INVALID, "learned preconditioner: NULL model or workspace");
+    if (!fft_on) return set_error(TP_ERR_UNSUPPORTED, "learned preconditioner needs FFT-plannable nf, nb (got %d, %d)", nf, nb);
+    if (a->mode == TP_MODE_REVERSE) return set_error(TP_ERR_UNSUPPORTED, "learned preconditioner: REVERSE mode is not supported");
+    if ((reinterpret_cast<uintptr_t>(a->learned_ws) & 255u) != 0)
+      return set_error(TP_ERR_INVALID, "learned workspace must be 256-byte aligned");
+    lw = c3_learned_layout(static_cast<char *>(a->learned_ws), nf, nb, P);
+    if (a->learned_ws_bytes < lw.bytes)
+      return set_error(TP_ERR_WORKSPACE, "learned workspace %zu B < %zu B", a->learned_ws_bytes, lw.bytes);
+  }
+  if (a->train_every > 0 && (a->train_z0 == nullptr || a->train_sol == nullptr || a->train_diag == nullptr))
+    return set_error(TP_ERR_INVALID, "train_every needs train_z0, train_sol and train_diag");
   const int rpc = fft_rows_of(nf, nb), cpc = fft_rows_of(nb, nf);
   const int use_fft = fft_on;
   const size_t smem_rows = (size_t)(nf + 2 * rpc * nf) * sizeof(float2);
@@ -509,6 +608,9 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
                                      static_cast<const float2 *>(op->kw), static_cast<const float2 *>(op->ke),
                                      static_cast<const float2 *>(op->ks), static_cast<const float2 *>(op->kn), w.dc, w.dw,
                                      w.de, w.ds, w.dn);
+  // the CNN activations' zero borders are never written by the kernels
+  if (learned) TP_CHECK_CUDA(cudaMemsetAsync(lw.cnn, 0, lw.cnn_bytes, st));
+  const ConvGeom g1 = conv_geom(nb, nf, 1);
   // initial state
   TP_CHECK_CUDA(cudaMemsetAsync(w.u, 0, (size_t)P * N * sizeof(float2), st));
   if (a->probes != nullptr)
@@ -534,6 +636,10 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     }
     const float2 *src = (t == 1) ? static_cast<const float2 *>(a->src_exit) : nullptr;
     const float2 *shared = a->src_shared ? static_cast<const float2 *>(a->src_shared) + (size_t)(t - 1) * N : nullptr;
+    if (learned) {
+      const int rc = cnn_forward(g1, *a->model, w.cdl, 0, w.dc, lw.cnn, lw.F, st);
+      if (rc != TP_OK) return rc;
+    }
     c3_init_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, cdr, w.u, use_u, src, shared, w.x, w.r, w.r0, w.p, w.v, w.K);
     c3_scalar_kernel<<<pgrid, 128, 0, st>>>(w.K, P, tol2, 1, stats);
     for (int it = 0; it < max_iter; ++it) {
@@ -542,7 +648,9 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
           pf, q, 0, w.r, w.p, w.v, w.s, use_fft ? w.hat : w.y, w.K, rows_cta, use_fft);
       if (use_fft) {
         c3_prec_cols_kernel<<<dim3(nf / cpc, P), k3Threads, smem_cols, st>>>(pb, q, w.hat, w.K, cpc);
-        c3_prec_rows_inv_kernel<<<dim3(nb / rpc, P), k3Threads, smem_rows, st>>>(pf, q, w.hat, w.y, w.K, rpc);
+        c3_prec_rows_inv_kernel<<<dim3(nb / rpc, P), k3Threads, smem_rows, st>>>(pf, q, w.hat, learned ? lw.zt : w.y,
+                                                                                  w.K, rpc);
+        if (learned) c3_filter_kernel<<<vgrid, k3Threads, 0, st>>>(q, lw.F, lw.zt, w.y, w.K);
       }
       c3_matvec_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, w.y, w.v, w.r0, w.s, w.K, 0);
       // s = r - alpha v; z = Prec(s); t = M z
@@ -550,7 +658,9 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
           pf, q, 1, w.r, w.p, w.v, w.s, use_fft ? w.hat : w.z, w.K, rows_cta, use_fft);
       if (use_fft) {
         c3_prec_cols_kernel<<<dim3(nf / cpc, P), k3Threads, smem_cols, st>>>(pb, q, w.hat, w.K, cpc);
-        c3_prec_rows_inv_kernel<<<dim3(nb / rpc, P), k3Threads, smem_rows, st>>>(pf, q, w.hat, w.z, w.K, rpc);
+        c3_prec_rows_inv_kernel<<<dim3(nb / rpc, P), k3Threads, smem_rows, st>>>(pf, q, w.hat, learned ? lw.zt : w.z,
+                                                                                  w.K, rpc);
+        if (learned) c3_filter_kernel<<<vgrid, k3Threads, 0, st>>>(q, lw.F, lw.zt, w.z, w.K);
       }
       c3_matvec_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K, 1);
       c3_update_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.x, w.r, w.r0, w.y, w.z, w.s, w.t, w.K);
@@ -566,6 +676,30 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
       }
     }
     c3_finish_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, w.x, w.r0, w.u, w.K);
+    if (a->train_every > 0 && t % a->train_every == 0) {
+      // training pair of this step: z0 = M0^{-1} v and x with (I - P_s) x = v,
+      // v the step's right-hand side r0 and x its converged update
+      // (train_kind 0), or x white noise and v = (I - P_s) x (train_kind 1);
+      // plus the slice's object diagonal
+      const size_t k = (size_t)(t / a->train_every - 1);
+      float2 *tz = static_cast<float2 *>(a->train_z0) + k * P * N;
+      float2 *tx = static_cast<float2 *>(a->train_sol) + k * P * N;
+      const float2 *v = w.r0;
+      if (a->train_kind == 1) {
+        c3_noise_kernel<<<eb, 256, 0, st>>>(N, P, t, tx);
+        c3_apply_a_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, tx, w.t);
+        v = w.t;
+      } else {
+        TP_CHECK_CUDA(cudaMemcpyAsync(tx, w.x, (size_t)P * N * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+      }
+      c3_prec_rows_kernel<<<dim3(nb / rows_cta, P), k3Threads, use_fft ? smem_rows : 0, st>>>(
+          pf, q, 2, v, w.p, w.v, w.s, use_fft ? w.hat : tz, nullptr, rows_cta, use_fft);
+      if (use_fft) {
+        c3_prec_cols_kernel<<<dim3(nf / cpc, P), k3Threads, smem_cols, st>>>(pb, q, w.hat, nullptr, cpc);
+        c3_prec_rows_inv_kernel<<<dim3(nb / rpc, P), k3Threads, smem_rows, st>>>(pf, q, w.hat, tz, nullptr, rpc);
+      }
+      c3_diag_diff_kernel<<<eb, 256, 0, st>>>(N, w.cdl, w.dc, static_cast<float2 *>(a->train_diag) + k * N);
+    }
     if (stats) c3_stats_kernel<<<pgrid, 128, 0, st>>>(w.K, P, tol2, stats);
     else TP_CHECK_CUDA(cudaMemsetAsync(w.K, 0, (size_t)P * sizeof(Krylov), st));
     const int to = flip ? (L - t) : t;
