@@ -177,21 +177,61 @@ __global__ void c3_scalar_kernel(Krylov *K, int P, double tol2, int first, int *
   (void)stats;
 }
 
+// FFT of `rows` transforms of length n in shared memory: the compile-time plan
+// when N > 0, else the runtime plan `pl`.
+template <int N>
+__device__ __forceinline__ float2 *fft_rows(float2 *a, float2 *b, const FftPlan &pl, const float2 *tw, bool inverse,
+                                            int rows) {
+  if constexpr (N > 0) return fft_block_fixed<N>(a, b, tw, inverse, rows, threadIdx.x, blockDim.x);
+  else return fft_block(a, b, pl, tw, inverse, rows, threadIdx.x, blockDim.x);
+}
+
+__device__ __forceinline__ void load_twiddles(float2 *tw, const float2 *__restrict__ twg, int n) {
+  for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twg[t];
+}
+
+// Twiddle table W_n^t = exp(-2 pi i t / n) (fp64 sincospi, rounded once).
+__global__ void c3_twiddle_kernel(int n, float2 *tw) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    double sv, cv;
+    sincospi(-2.0 * (double)t / (double)n, &sv, &cv);
+    tw[t] = make_float2((float)cv, (float)sv);
+  }
+}
+
+// Inverse of the periodic symbol, scaled by 1/(nf nb) (the normalisation of
+// the inverse 2D transform), transposed: sym[f * nb + b] =
+// 1 / ((1 - mu_x (2 cos(2 pi f/nf) - 2) - mu_y (2 cos(2 pi b/nb) - 2)) nf nb).
+__global__ void c3_symbol_kernel(const C3Params q, float2 *sym) {
+  const double sc = 1.0 / ((double)q.nf * (double)q.nb);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < q.N; e += gridDim.x * blockDim.x) {
+    const int f = e / q.nb, bb = e - f * q.nb;
+    double sf, cf, sb, cbv;
+    sincospi(2.0 * (double)f / (double)q.nf, &sf, &cf);
+    sincospi(2.0 * (double)bb / (double)q.nb, &sb, &cbv);
+    const double ax = 2.0 * cf - 2.0, ay = 2.0 * cbv - 2.0;
+    const double2 lam = z2(1.0 - (q.mu_x.x * ax + q.mu_y.x * ay), -(q.mu_x.y * ax + q.mu_y.y * ay));
+    sym[e] = to_f2(zscale(zdiv(z2(1, 0), lam), sc));
+  }
+}
+
 // Forward row FFTs of the preconditioner input, formed on the fly:
 //   mode 0: p := r + beta (p - omega v)  (p updated in place), input p
 //   mode 1: s := r - alpha v             (s written),          input s
 //   mode 2: input r as is (K may be NULL: every probe is transformed)
 // Grid (nb / rpc, P).
+template <int NF>
 __global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan pl, const C3Params q, int mode,
                                                                  const float2 *r, float2 *p, const float2 *v, float2 *s,
-                                                                 float2 *hat, const Krylov *K, int rpc, int fft_on) {
+                                                                 float2 *hat, const Krylov *K, int rpc, int fft_on,
+                                                                 const float2 *twg) {
   extern __shared__ __align__(16) float2 fsm[];
-  const int n = q.nf, pr = blockIdx.y;
+  const int n = NF > 0 ? NF : q.nf, pr = blockIdx.y;
   if (K != nullptr && K[pr].done) return;
   float2 *tw = fsm, *a = tw + n, *b = a + rpc * n;
   const size_t off = (size_t)pr * q.N + (size_t)blockIdx.x * rpc * n;
   const int tot = rpc * n;
-  if (fft_on) fft_twiddles(tw, n, threadIdx.x, blockDim.x);
+  if (fft_on) load_twiddles(tw, twg, n);
   if (mode == 2) {
     for (int e = threadIdx.x; e < tot; e += blockDim.x) {
       if (fft_on) a[e] = r[off + e];
@@ -222,61 +262,57 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan p
   }
   if (!fft_on) return;
   __syncthreads();
-  const float2 *res = fft_block(a, b, pl, tw, false, rpc, threadIdx.x, blockDim.x);
+  const float2 *res = fft_rows<NF>(a, b, pl, tw, false, rpc);
   for (int e = threadIdx.x; e < tot; e += blockDim.x) hat[off + e] = res[e];
 }
 
-// Column FFTs, division by the symbol, inverse column FFTs (in place on hat).
-// Grid (nf / cpc, P): a CTA transposes cpc columns of length nb into smem.
+// Column FFTs, multiplication by the (scaled) inverse symbol, inverse column
+// FFTs (in place on hat).  Grid (nf / cpc, P): a CTA transposes cpc columns of
+// length nb into smem.
+template <int NB>
 __global__ void __launch_bounds__(k3Threads) c3_prec_cols_kernel(const FftPlan pl, const C3Params q, float2 *hat,
-                                                                 const Krylov *K, int cpc) {
+                                                                 const Krylov *K, int cpc, const float2 *twg,
+                                                                 const float2 *__restrict__ sym) {
   extern __shared__ __align__(16) float2 fsm[];
-  const int nb = q.nb, nf = q.nf, pr = blockIdx.y;
+  const int nb = NB > 0 ? NB : q.nb, nf = q.nf, pr = blockIdx.y;
   if (K != nullptr && K[pr].done) return;
   float2 *tw = fsm, *a = tw + nb, *b = a + cpc * nb;
   const int f0 = blockIdx.x * cpc;
   float2 *base = hat + (size_t)pr * q.N;
-  fft_twiddles(tw, nb, threadIdx.x, blockDim.x);
+  load_twiddles(tw, twg, nb);
   for (int e = threadIdx.x; e < cpc * nb; e += blockDim.x) {
     const int c = e % cpc, bb = e / cpc;  // coalesced over c
     a[c * nb + bb] = base[(size_t)bb * nf + f0 + c];
   }
   __syncthreads();
-  float2 *F = fft_block(a, b, pl, tw, false, cpc, threadIdx.x, blockDim.x);
+  float2 *F = fft_rows<NB>(a, b, pl, tw, false, cpc);
   float2 *o = (F == a) ? b : a;
-  for (int e = threadIdx.x; e < cpc * nb; e += blockDim.x) {
-    const int c = e / nb, bb = e % nb;
-    double sf, cf, sb, cbv;
-    sincospi(2.0 * (double)(f0 + c) / (double)nf, &sf, &cf);
-    sincospi(2.0 * (double)bb / (double)nb, &sb, &cbv);
-    const double ax = 2.0 * cf - 2.0, ay = 2.0 * cbv - 2.0;
-    const double2 lam = z2(1.0 - (q.mu_x.x * ax + q.mu_y.x * ay), -(q.mu_x.y * ax + q.mu_y.y * ay));
-    F[e] = cmul(F[e], to_f2(zdiv(z2(1, 0), lam)));
-  }
+  const float2 *sy = sym + (size_t)f0 * nb;
+  for (int e = threadIdx.x; e < cpc * nb; e += blockDim.x) F[e] = cmul(F[e], sy[e]);
   __syncthreads();
-  float2 *R = fft_block(F, o, pl, tw, true, cpc, threadIdx.x, blockDim.x);
+  float2 *R = fft_rows<NB>(F, o, pl, tw, true, cpc);
   for (int e = threadIdx.x; e < cpc * nb; e += blockDim.x) {
     const int c = e % cpc, bb = e / cpc;
     base[(size_t)bb * nf + f0 + c] = R[c * nb + bb];
   }
 }
 
-// Inverse row FFTs (scaled 1/(nf nb)) of hat into out.
+// Inverse row FFTs of hat into out (the 1/(nf nb) scale is in the symbol).
+template <int NF>
 __global__ void __launch_bounds__(k3Threads) c3_prec_rows_inv_kernel(const FftPlan pl, const C3Params q,
                                                                      const float2 *hat, float2 *out, const Krylov *K,
-                                                                     int rpc) {
+                                                                     int rpc, const float2 *twg) {
   extern __shared__ __align__(16) float2 fsm[];
-  const int n = q.nf, pr = blockIdx.y;
+  const int n = NF > 0 ? NF : q.nf, pr = blockIdx.y;
   if (K != nullptr && K[pr].done) return;
   float2 *tw = fsm, *a = tw + n, *b = a + rpc * n;
   const size_t off = (size_t)pr * q.N + (size_t)blockIdx.x * rpc * n;
   const int tot = rpc * n;
-  fft_twiddles(tw, n, threadIdx.x, blockDim.x);
+  load_twiddles(tw, twg, n);
   for (int e = threadIdx.x; e < tot; e += blockDim.x) a[e] = hat[off + e];
   __syncthreads();
-  const float2 *res = fft_block(a, b, pl, tw, true, rpc, threadIdx.x, blockDim.x);
-  const float sc = 1.f / ((float)q.nf * (float)q.nb);
-  for (int e = threadIdx.x; e < tot; e += blockDim.x) out[off + e] = make_float2(res[e].x * sc, res[e].y * sc);
+  const float2 *res = fft_rows<NF>(a, b, pl, tw, true, rpc);
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) out[off + e] = res[e];
 }
 
 // out = (I - P) y with fused fp64 dots: which 0: acc_r0v += <r0, out>;
@@ -408,16 +444,36 @@ __global__ void c3_grad_kernel(int N, int P, int nz, int s, const float2 *__rest
 }
 
 // Learned correction of the preconditioned vector: out = z + sum_t F_t z(x + o_t)
-// (conj(F) in the adjoint modes).  Grid (chunks, P).
+// (conj(F) in the adjoint modes).  A thread owns one pixel for
+// kFilterProbes probes, so each filter value is read once per pixel group.
+// Grid (N / 256, P / kFilterProbes).
+constexpr int kFilterProbes = 8;
 __global__ void __launch_bounds__(k3Threads) c3_filter_kernel(const C3Params q, const float2 *__restrict__ F,
                                                               const float2 *__restrict__ z, float2 *out,
                                                               const Krylov *K) {
-  const int pr = blockIdx.y;
-  if (K != nullptr && K[pr].done) return;
-  const size_t off = (size_t)pr * q.N;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
-    const int b = i / q.nf, f = i - b * q.nf;
-    out[off + i] = filter_apply_px(F, 0, (size_t)q.N, z + off, q.nb, q.nf, b, f, q.conj_t);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= q.N) return;
+  const int b = i / q.nf, f = i - b * q.nf;
+  float2 w[kFilterTaps];
+  int o[kFilterTaps];
+#pragma unroll
+  for (int t = 0; t < kFilterTaps; ++t) {
+    const int bb = b + filter_tap_dy(t), ff = f + filter_tap_dx(t);
+    const bool in = bb >= 0 && bb < q.nb && ff >= 0 && ff < q.nf;
+    float2 v = in ? F[(size_t)t * q.N + i] : make_float2(0.f, 0.f);
+    if (q.conj_t) v.y = -v.y;
+    w[t] = v;
+    o[t] = in ? (bb * q.nf + ff) : i;
+  }
+  const int p0 = blockIdx.y * kFilterProbes;
+#pragma unroll 1
+  for (int pr = p0; pr < p0 + kFilterProbes && pr < q.P; ++pr) {
+    if (K != nullptr && K[pr].done) continue;
+    const float2 *zp = z + (size_t)pr * q.N;
+    float2 acc = zp[i];
+#pragma unroll
+    for (int t = 0; t < kFilterTaps; ++t) acc = cfma(w[t], zp[o[t]], acc);
+    out[(size_t)pr * q.N + i] = acc;
   }
 }
 
@@ -458,6 +514,7 @@ struct C3Work {
   float2 *u, *x, *r, *r0, *p, *v, *s, *y, *z, *t, *hat;
   float2 *cdl, *cdr;
   float2 *dc, *dw, *de, *ds, *dn;
+  float2 *sym, *twf, *twb;  // preconditioner symbol (N) and twiddle tables
   Krylov *K;
   int *pending;
   size_t bytes;
@@ -476,12 +533,46 @@ static C3Work c3_layout(char *base, int N, int P) {
   const size_t vec = (size_t)P * N * sizeof(float2);
   float2 **vecs[] = {&w.u, &w.x, &w.r, &w.r0, &w.p, &w.v, &w.s, &w.y, &w.z, &w.t, &w.hat};
   for (float2 **v : vecs) *v = reinterpret_cast<float2 *>(take(vec));
-  float2 **diag[] = {&w.cdl, &w.cdr, &w.dc, &w.dw, &w.de, &w.ds, &w.dn};
+  float2 **diag[] = {&w.cdl, &w.cdr, &w.dc, &w.dw, &w.de, &w.ds, &w.dn, &w.sym};
   for (float2 **d : diag) *d = reinterpret_cast<float2 *>(take((size_t)N * sizeof(float2)));
+  w.twf = reinterpret_cast<float2 *>(take((size_t)kFftMaxN * sizeof(float2)));
+  w.twb = reinterpret_cast<float2 *>(take((size_t)kFftMaxN * sizeof(float2)));
   w.K = reinterpret_cast<Krylov *>(take((size_t)P * sizeof(Krylov)));
   w.pending = reinterpret_cast<int *>(take(sizeof(int)));
   w.bytes = off;
   return w;
+}
+
+using RowsKernel = void (*)(const FftPlan, const C3Params, int, const float2 *, float2 *, const float2 *, float2 *,
+                           float2 *, const Krylov *, int, int, const float2 *);
+using ColsKernel = void (*)(const FftPlan, const C3Params, float2 *, const Krylov *, int, const float2 *,
+                           const float2 *);
+using InvKernel = void (*)(const FftPlan, const C3Params, const float2 *, float2 *, const Krylov *, int, const float2 *);
+struct PrecKernels {
+  RowsKernel rows;
+  ColsKernel cols;
+  InvKernel inv;
+};
+
+template <int NF, int NB>
+static PrecKernels prec_kernels_t() {
+  return {c3_prec_rows_kernel<NF>, c3_prec_cols_kernel<NB>, c3_prec_rows_inv_kernel<NF>};
+}
+
+// Square transverse grids of the common sizes get compile-time FFT plans.
+static PrecKernels prec_kernels(int nf, int nb) {
+  if (nf == nb) {
+    switch (nf) {
+      case 32: return prec_kernels_t<32, 32>();
+      case 64: return prec_kernels_t<64, 64>();
+      case 128: return prec_kernels_t<128, 128>();
+      case 192: return prec_kernels_t<192, 192>();
+      case 256: return prec_kernels_t<256, 256>();
+      case 512: return prec_kernels_t<512, 512>();
+      default: break;
+    }
+  }
+  return prec_kernels_t<0, 0>();
 }
 
 // FFT rows per CTA: at most 16 and 4096 elements, and a divisor of the row count.
@@ -593,10 +684,12 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   const int use_fft = fft_on;
   const size_t smem_rows = (size_t)(nf + 2 * rpc * nf) * sizeof(float2);
   const size_t smem_cols = (size_t)(nb + 2 * cpc * nb) * sizeof(float2);
+  // kernels of the preconditioner: compile-time FFT plans for the common sizes
+  PrecKernels pk = prec_kernels(nf, nb);
   if (use_fft) {
-    TP_CHECK_CUDA(cudaFuncSetAttribute(c3_prec_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
-    TP_CHECK_CUDA(cudaFuncSetAttribute(c3_prec_rows_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
-    TP_CHECK_CUDA(cudaFuncSetAttribute(c3_prec_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cols));
+    TP_CHECK_CUDA(cudaFuncSetAttribute(pk.rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
+    TP_CHECK_CUDA(cudaFuncSetAttribute(pk.inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
+    TP_CHECK_CUDA(cudaFuncSetAttribute(pk.cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cols));
   }
   const int rows_cta = use_fft ? rpc : 1;
   const int max_iter = a->max_iter > 0 ? a->max_iter : 20;
@@ -604,6 +697,21 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   int *stats = a->stats;
 
   const int eb = 296;
+  if (use_fft) {
+    c3_twiddle_kernel<<<(nf + 255) / 256, 256, 0, st>>>(nf, w.twf);
+    c3_twiddle_kernel<<<(nb + 255) / 256, 256, 0, st>>>(nb, w.twb);
+    c3_symbol_kernel<<<eb, 256, 0, st>>>(q, w.sym);
+  }
+  // M0^{-1} in -> out (mode 0/1/2 input of the row kernel; Kp NULL = all probes)
+  auto precondition = [&](int mode, const float2 *rin, float2 *out, const Krylov *Kp) {
+    pk.rows<<<dim3(nb / rows_cta, P), k3Threads, use_fft ? smem_rows : 0, st>>>(
+        pf, q, mode, rin, w.p, w.v, w.s, use_fft ? w.hat : out, Kp, rows_cta, use_fft, w.twf);
+    if (use_fft) {
+      pk.cols<<<dim3(nf / cpc, P), k3Threads, smem_cols, st>>>(pb, q, w.hat, Kp, cpc, w.twb, w.sym);
+      pk.inv<<<dim3(nb / rpc, P), k3Threads, smem_rows, st>>>(pf, q, w.hat, out, Kp, rpc, w.twf);
+    }
+  };
+  const dim3 fgrid((N + k3Threads - 1) / k3Threads, (P + kFilterProbes - 1) / kFilterProbes);
   c3_diag_kernel<<<eb, 256, 0, st>>>(N, nf, q.sigma, q.conj_t, static_cast<const float2 *>(op->kc),
                                      static_cast<const float2 *>(op->kw), static_cast<const float2 *>(op->ke),
                                      static_cast<const float2 *>(op->ks), static_cast<const float2 *>(op->kn), w.dc, w.dw,
@@ -644,24 +752,12 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     c3_scalar_kernel<<<pgrid, 128, 0, st>>>(w.K, P, tol2, 1, stats);
     for (int it = 0; it < max_iter; ++it) {
       // p = r + beta (p - omega v); y = Prec(p); v = M y
-      c3_prec_rows_kernel<<<dim3(nb / rows_cta, P), k3Threads, use_fft ? smem_rows : 0, st>>>(
-          pf, q, 0, w.r, w.p, w.v, w.s, use_fft ? w.hat : w.y, w.K, rows_cta, use_fft);
-      if (use_fft) {
-        c3_prec_cols_kernel<<<dim3(nf / cpc, P), k3Threads, smem_cols, st>>>(pb, q, w.hat, w.K, cpc);
-        c3_prec_rows_inv_kernel<<<dim3(nb / rpc, P), k3Threads, smem_rows, st>>>(pf, q, w.hat, learned ? lw.zt : w.y,
-                                                                                  w.K, rpc);
-        if (learned) c3_filter_kernel<<<vgrid, k3Threads, 0, st>>>(q, lw.F, lw.zt, w.y, w.K);
-      }
+      precondition(0, w.r, learned ? lw.zt : w.y, w.K);
+      if (learned) c3_filter_kernel<<<fgrid, k3Threads, 0, st>>>(q, lw.F, lw.zt, w.y, w.K);
       c3_matvec_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, w.y, w.v, w.r0, w.s, w.K, 0);
       // s = r - alpha v; z = Prec(s); t = M z
-      c3_prec_rows_kernel<<<dim3(nb / rows_cta, P), k3Threads, use_fft ? smem_rows : 0, st>>>(
-          pf, q, 1, w.r, w.p, w.v, w.s, use_fft ? w.hat : w.z, w.K, rows_cta, use_fft);
-      if (use_fft) {
-        c3_prec_cols_kernel<<<dim3(nf / cpc, P), k3Threads, smem_cols, st>>>(pb, q, w.hat, w.K, cpc);
-        c3_prec_rows_inv_kernel<<<dim3(nb / rpc, P), k3Threads, smem_rows, st>>>(pf, q, w.hat, learned ? lw.zt : w.z,
-                                                                                  w.K, rpc);
-        if (learned) c3_filter_kernel<<<vgrid, k3Threads, 0, st>>>(q, lw.F, lw.zt, w.z, w.K);
-      }
+      precondition(1, w.r, learned ? lw.zt : w.z, w.K);
+      if (learned) c3_filter_kernel<<<fgrid, k3Threads, 0, st>>>(q, lw.F, lw.zt, w.z, w.K);
       c3_matvec_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K, 1);
       c3_update_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.x, w.r, w.r0, w.y, w.z, w.s, w.t, w.K);
       c3_scalar_kernel<<<pgrid, 128, 0, st>>>(w.K, P, tol2, 0, stats);
@@ -692,12 +788,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
       } else {
         TP_CHECK_CUDA(cudaMemcpyAsync(tx, w.x, (size_t)P * N * sizeof(float2), cudaMemcpyDeviceToDevice, st));
       }
-      c3_prec_rows_kernel<<<dim3(nb / rows_cta, P), k3Threads, use_fft ? smem_rows : 0, st>>>(
-          pf, q, 2, v, w.p, w.v, w.s, use_fft ? w.hat : tz, nullptr, rows_cta, use_fft);
-      if (use_fft) {
-        c3_prec_cols_kernel<<<dim3(nf / cpc, P), k3Threads, smem_cols, st>>>(pb, q, w.hat, nullptr, cpc);
-        c3_prec_rows_inv_kernel<<<dim3(nb / rpc, P), k3Threads, smem_rows, st>>>(pf, q, w.hat, tz, nullptr, rpc);
-      }
+      precondition(2, v, tz, nullptr);
       c3_diag_diff_kernel<<<eb, 256, 0, st>>>(N, w.cdl, w.dc, static_cast<float2 *>(a->train_diag) + k * N);
     }
     if (stats) c3_stats_kernel<<<pgrid, 128, 0, st>>>(w.K, P, tol2, stats);

@@ -145,6 +145,64 @@ __device__ __forceinline__ void fft_pass(const float2 *a, float2 *b, int n, int 
   }
 }
 
+// ------------------------------------------------------ fixed-size plans
+// The same passes with the length and the radix sequence known at compile
+// time, so that every index division and modulo is by a constant.  Used by
+// the 3D preconditioner for the common transverse sizes.
+template <int N, int Ns, int R>
+__device__ __forceinline__ void fft_pass_fixed(const float2 *a, float2 *b, const float2 *tw, float sign, int nb, int tid,
+                                               int nth) {
+  constexpr int T = N / R;
+  constexpr int step = N / (Ns * R);
+  for (int w = tid; w < nb * T; w += nth) {
+    const int bi = w / T, j = w - bi * T;
+    const float2 *src = a + bi * N;
+    float2 *dst = b + bi * N;
+    const int k = j % Ns;
+    float2 v[8];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[j + r * T];
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      const float2 t = tw[(r * k * step) % N];
+      v[r] = cmul(v[r], make_float2(t.x, sign < 0 ? t.y : -t.y));
+    }
+    dft_small<R>(v, sign);
+    const int idx = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[idx + r * Ns] = v[r];
+  }
+}
+
+template <int N, int Ns, int R, int... Rest>
+__device__ __forceinline__ float2 *fft_run_fixed(float2 *a, float2 *b, const float2 *tw, float sign, int nb, int tid,
+                                                 int nth) {
+  fft_pass_fixed<N, Ns, R>(a, b, tw, sign, nb, tid, nth);
+  __syncthreads();
+  if constexpr (sizeof...(Rest) == 0) {
+    return b;
+  } else {
+    return fft_run_fixed<N, Ns * R, Rest...>(b, a, tw, sign, nb, tid, nth);
+  }
+}
+
+// Lengths with a compile-time plan (radices 8s first, then 4, 2, 3).
+__host__ __device__ constexpr bool fft_fixed_size(int n) {
+  return n == 32 || n == 64 || n == 128 || n == 192 || n == 256 || n == 512;
+}
+
+template <int N>
+__device__ __forceinline__ float2 *fft_block_fixed(float2 *a, float2 *b, const float2 *tw, bool inverse, int nb,
+                                                   int tid, int nth) {
+  const float sign = inverse ? 1.f : -1.f;
+  if constexpr (N == 32) return fft_run_fixed<32, 1, 8, 4>(a, b, tw, sign, nb, tid, nth);
+  else if constexpr (N == 64) return fft_run_fixed<64, 1, 8, 8>(a, b, tw, sign, nb, tid, nth);
+  else if constexpr (N == 128) return fft_run_fixed<128, 1, 8, 8, 2>(a, b, tw, sign, nb, tid, nth);
+  else if constexpr (N == 192) return fft_run_fixed<192, 1, 8, 8, 3>(a, b, tw, sign, nb, tid, nth);
+  else if constexpr (N == 256) return fft_run_fixed<256, 1, 8, 8, 4>(a, b, tw, sign, nb, tid, nth);
+  else return fft_run_fixed<512, 1, 8, 8, 8>(a, b, tw, sign, nb, tid, nth);
+}
+
 // nb transforms of length pl.n stored back to back in `a` (scratch `b` of
 // the same size).  Returns the buffer holding the result (a or b).  Ends
 // with __syncthreads().
