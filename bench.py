@@ -10,6 +10,11 @@ field + amplitude-loss residual + exact-adjoint march with the fused probe
 gradient + mapping onto the index nodes.  The full field (8.6 GB) is far
 larger than L2, so no explicit flush is needed between steps.
 
+The same line carries ``learned_vs_plain_3d``: forward + exact-adjoint
+probe·slice solves/s of the 3D BiCGStab march (256 x 256 x 256 nodes, 64
+probes) with the plain FFT preconditioner and with the learned correction,
+after training the network on solver-generated pairs of another field.
+
 ``--impl reference`` times the CPU restatement of the reference's
 IterativeLU path (per-slice sparse LU, per-probe march, reference adjoint)
 on the host cores instead.
@@ -47,6 +52,10 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--config", default="2d-fwd-adj-2048x1024-p512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-3d", action="store_true", help="skip the 3D learned-vs-plain section")
+    ap.add_argument("--case", choices=("headline", "3d-march-small"), default="headline",
+                    help="3d-march-small: a few learned 3D forward marches (256 x 256 x 5 nodes, 64 probes), "
+                         "a small profiler target for the conv and FFT kernels")
     return ap.parse_args()
 
 
@@ -236,6 +245,85 @@ def run_reference(a):
 
 
 # --------------------------------------------------------------------------
+# 3D: learned vs plain FFT-preconditioned BiCGStab (fwd + exact adjoint)
+# --------------------------------------------------------------------------
+def bench_learned_3d(dev, reps=2, train_probes=40, train_steps=1500):
+    """fwd + adj probe·slice solves/s of the plain and the learned 3D forms.
+
+    Workload: 256 x 256 transverse x 256 nodes, 64 probes (8 x 8 raster,
+    stride 16, waist 12), δn = 400 seeded ellipsoids + 1e-6 i, impedance
+    edges, BiCGStab to a 1e-6 relative residual per solve.  One step = a
+    forward march storing the full field + an exact-adjoint march with the
+    fused gradient, all 64 probes batched.  The network is trained first on
+    solver-generated white-noise pairs (every slice of a different seeded
+    field, `train_probes` probes); training time is reported, not timed.
+    """
+    import torch
+
+    from thick_ptycho_b200.cn3d import CN3D, generate_pairs
+    from thick_ptycho_b200.learned import LearnedPreconditioner, default_kappa
+    from thick_ptycho_b200.workloads import CONFIG2, ellipsoid_field_3d
+
+    w = CONFIG2
+    geo = w.geometry()
+    nz, P, n = w.nz, w.num_probes, w.nx
+    N, L = n * n, nz - 1
+    eng = CN3D(n, n, nz, geo.k, 1.0, 1.0, 1.0, "impedance", device=dev)
+    field = torch.from_numpy((1 - w.delta_n()).reshape(N, nz)).to(dev)
+    probes = torch.from_numpy(w.probes(geo).reshape(P, N).astype(np.complex64)).to(dev)
+    stream = torch.cuda.current_stream(dev)
+
+    t0 = time.perf_counter()
+    ftrain = torch.from_numpy((1 - ellipsoid_field_3d(n, n, nz, w.n_shapes, 1001)).reshape(N, nz)).to(dev)
+    pairs = generate_pairs(eng, ftrain, probes[:train_probes].contiguous(), every=1, kind="noise")
+    del ftrain
+    model = LearnedPreconditioner(n, n, default_kappa(geo.k, 1.0, 5e-4), device=dev, seed=0)
+    model.train(pairs, steps=train_steps, slices_per_batch=2, lr=1e-3)
+    torch.cuda.synchronize(dev)
+    train_s = time.perf_counter() - t0
+    npairs = pairs.count
+    del pairs
+    torch.cuda.empty_cache()
+
+    store = eng.new_store(P)
+    ex = torch.empty((P, N), dtype=torch.complex64, device=dev)
+    grad = torch.zeros((L, N), dtype=torch.complex64, device=dev)
+    out = {}
+    exits = {}
+    for name, pc in (("plain", True), ("learned", "learned")):
+        ms = []
+        eng.read_stats()
+        for rep in range(reps + 1):
+            if rep == 1:
+                eng.read_stats()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            grad.zero_()
+            e0.record(stream)
+            eng.march(field, P, "forward", probes=probes, u_store=store, exit_out=ex, precond=pc, model=model)
+            eng.march(field, P, "adjoint_exact", src_exit=ex, u_fwd=store, grad_c=grad, precond=pc, model=model)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            if rep >= 1:
+                ms.append(e0.elapsed_time(e1))
+        st = eng.read_stats()
+        t = statistics.median(ms)
+        exits[name] = ex.clone()
+        out[name] = {"value": P * L / (t / 1e3), "ms_per_step": t,
+                     "krylov_iterations_per_solve": st["iterations"] / max(st["solves"], 1),
+                     "failed_solves": st["failed"]}
+    diff = float(torch.linalg.vector_norm(exits["learned"] - exits["plain"]) / torch.linalg.vector_norm(exits["plain"]))
+    return {
+        "workload": w.name, "metric": "probe·slice solves/s fwd+adj (3D BiCGStab, exact adjoint + gradient)",
+        "unit": UNIT, "plain": out["plain"], "learned": out["learned"],
+        "learned_over_plain": out["learned"]["value"] / out["plain"]["value"],
+        "exit_rel_diff_learned_vs_plain": diff, "fallbacks": eng.fallbacks,
+        "training": {"pairs": npairs, "kind": "white-noise pairs (x, (I - P_s) x) of a different seeded field",
+                     "steps": train_steps, "seconds": train_s, "not_timed": True},
+    }
+
+
+# --------------------------------------------------------------------------
 # GPU leg
 # --------------------------------------------------------------------------
 def run_ours(a):
@@ -380,9 +468,12 @@ def run_ours(a):
                          "peak_kind": kind, "traffic": None,
                          "algorithmic_bytes_per_launch": dom_bytes},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": a.steps * 5,
+            # per step: 2 factorisations, 2 marches, the amplitude residual, the node mapping
+            "gpu_launches": a.steps * 6,
             "clocks": clk.summary(),
         }
+        if world == 1 and not a.no_3d:
+            line["learned_vs_plain_3d"] = bench_learned_3d(dev)
         if world == 1 and not a.no_cpu_baseline:
             v, tf, tp, wall = cpu_rate(N, nz, P, 1, 2)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
@@ -395,10 +486,44 @@ def run_ours(a):
         dist.destroy_process_group()
 
 
+def run_case_3d_small(a):
+    """`steps` learned 3D forward marches on 256 x 256 x 5 nodes, 64 probes (config-2 probes and
+    ellipsoid distribution), after `warmup` untimed ones; an untrained network (seeded)."""
+    import torch
+
+    from thick_ptycho_b200.cn3d import CN3D
+    from thick_ptycho_b200.learned import LearnedPreconditioner, default_kappa
+    from thick_ptycho_b200.workloads import CONFIG2, ellipsoid_field_3d
+
+    w = CONFIG2
+    nz = 5
+    geo = w.geometry()
+    dev = torch.device("cuda", 0)
+    eng = CN3D(w.nx, w.nx, nz, geo.k, 1.0, 1.0, 1.0, "impedance", device=dev)
+    P = w.num_probes
+    probes = torch.from_numpy(w.probes(geo).reshape(P, -1).astype(np.complex64)).to(dev)
+    field = torch.from_numpy((1 - ellipsoid_field_3d(w.nx, w.nx, nz, 10, w.seed)).reshape(-1, nz)).to(dev)
+    model = LearnedPreconditioner(w.nx, w.nx, default_kappa(geo.k, 1.0, 5e-4), device=dev, seed=0)
+    ex = torch.empty((P, eng.N), dtype=torch.complex64, device=dev)
+    ms = []
+    for i in range(a.warmup + a.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.march(field, P, "forward", probes=probes, exit_out=ex, precond="learned", model=model)
+        e1.record()
+        torch.cuda.synchronize()
+        if i >= a.warmup:
+            ms.append(e0.elapsed_time(e1))
+    print(json.dumps({"case": "3d-march-small", "ms_per_march": statistics.median(ms) if ms else None,
+                      "stats": eng.read_stats()}), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.case == "3d-march-small":
+        run_case_3d_small(a)
     else:
         run_ours(a)
 
