@@ -178,12 +178,25 @@ __global__ void c3_scalar_kernel(Krylov *K, int P, double tol2, int first, int *
 }
 
 // FFT of `rows` transforms of length n in shared memory: the compile-time plan
-// when N > 0, else the runtime plan `pl`.
+// in the padded layout when N > 0, else the runtime plan `pl` (unpadded).
 template <int N>
 __device__ __forceinline__ float2 *fft_rows(float2 *a, float2 *b, const FftPlan &pl, const float2 *tw, bool inverse,
                                             int rows) {
-  if constexpr (N > 0) return fft_block_fixed<N>(a, b, tw, inverse, rows, threadIdx.x, blockDim.x);
+  if constexpr (N > 0) return fft_block_padded<N>(a, b, tw, inverse, rows, threadIdx.x, blockDim.x);
   else return fft_block(a, b, pl, tw, inverse, rows, threadIdx.x, blockDim.x);
+}
+
+// Shared-memory slot of element i of transform bi (length n).
+template <int N>
+__device__ __forceinline__ int fslot(int bi, int i, int n) {
+  if constexpr (N > 0) return bi * FftPad<N>::S + fft_pad(i);
+  else return bi * n + i;
+}
+// Shared-memory slots per transform.
+template <int N>
+__host__ __device__ constexpr int fstride(int n) {
+  if constexpr (N > 0) return FftPad<N>::S;
+  else return n;
 }
 
 __device__ __forceinline__ void load_twiddles(float2 *tw, const float2 *__restrict__ twg, int n) {
@@ -228,13 +241,14 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan p
   extern __shared__ __align__(16) float2 fsm[];
   const int n = NF > 0 ? NF : q.nf, pr = blockIdx.y;
   if (K != nullptr && K[pr].done) return;
-  float2 *tw = fsm, *a = tw + n, *b = a + rpc * n;
+  float2 *tw = fsm, *a = tw + n, *b = a + rpc * fstride<NF>(n);
   const size_t off = (size_t)pr * q.N + (size_t)blockIdx.x * rpc * n;
   const int tot = rpc * n;
+  auto slot = [&](int e) { return fslot<NF>(e / n, e % n, n); };
   if (fft_on) load_twiddles(tw, twg, n);
   if (mode == 2) {
     for (int e = threadIdx.x; e < tot; e += blockDim.x) {
-      if (fft_on) a[e] = r[off + e];
+      if (fft_on) a[slot(e)] = r[off + e];
       else hat[off + e] = r[off + e];
     }
   } else if (mode == 0) {
@@ -245,7 +259,7 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan p
     for (int e = threadIdx.x; e < tot; e += blockDim.x) {
       const float2 pv = cfma(bt, cfnma(om, v[off + e], p[off + e]), r[off + e]);
       p[off + e] = pv;
-      if (fft_on) a[e] = pv;
+      if (fft_on) a[slot(e)] = pv;
       else hat[off + e] = pv;
     }
   } else {
@@ -256,14 +270,14 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan p
     for (int e = threadIdx.x; e < tot; e += blockDim.x) {
       const float2 sv = cfnma(al, v[off + e], r[off + e]);
       s[off + e] = sv;
-      if (fft_on) a[e] = sv;
+      if (fft_on) a[slot(e)] = sv;
       else hat[off + e] = sv;
     }
   }
   if (!fft_on) return;
   __syncthreads();
   const float2 *res = fft_rows<NF>(a, b, pl, tw, false, rpc);
-  for (int e = threadIdx.x; e < tot; e += blockDim.x) hat[off + e] = res[e];
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) hat[off + e] = res[slot(e)];
 }
 
 // Column FFTs, multiplication by the (scaled) inverse symbol, inverse column
@@ -276,24 +290,28 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_cols_kernel(const FftPlan p
   extern __shared__ __align__(16) float2 fsm[];
   const int nb = NB > 0 ? NB : q.nb, nf = q.nf, pr = blockIdx.y;
   if (K != nullptr && K[pr].done) return;
-  float2 *tw = fsm, *a = tw + nb, *b = a + cpc * nb;
+  float2 *tw = fsm, *a = tw + nb, *b = a + cpc * fstride<NB>(nb);
   const int f0 = blockIdx.x * cpc;
   float2 *base = hat + (size_t)pr * q.N;
   load_twiddles(tw, twg, nb);
   for (int e = threadIdx.x; e < cpc * nb; e += blockDim.x) {
     const int c = e % cpc, bb = e / cpc;  // coalesced over c
-    a[c * nb + bb] = base[(size_t)bb * nf + f0 + c];
+    a[fslot<NB>(c, bb, nb)] = base[(size_t)bb * nf + f0 + c];
   }
   __syncthreads();
   float2 *F = fft_rows<NB>(a, b, pl, tw, false, cpc);
   float2 *o = (F == a) ? b : a;
   const float2 *sy = sym + (size_t)f0 * nb;
-  for (int e = threadIdx.x; e < cpc * nb; e += blockDim.x) F[e] = cmul(F[e], sy[e]);
+  for (int e = threadIdx.x; e < cpc * nb; e += blockDim.x) {
+    const int c = e / nb, bb = e - c * nb;
+    const int sl = fslot<NB>(c, bb, nb);
+    F[sl] = cmul(F[sl], sy[e]);
+  }
   __syncthreads();
   float2 *R = fft_rows<NB>(F, o, pl, tw, true, cpc);
   for (int e = threadIdx.x; e < cpc * nb; e += blockDim.x) {
     const int c = e % cpc, bb = e / cpc;
-    base[(size_t)bb * nf + f0 + c] = R[c * nb + bb];
+    base[(size_t)bb * nf + f0 + c] = R[fslot<NB>(c, bb, nb)];
   }
 }
 
@@ -305,14 +323,15 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_inv_kernel(const FftPl
   extern __shared__ __align__(16) float2 fsm[];
   const int n = NF > 0 ? NF : q.nf, pr = blockIdx.y;
   if (K != nullptr && K[pr].done) return;
-  float2 *tw = fsm, *a = tw + n, *b = a + rpc * n;
+  float2 *tw = fsm, *a = tw + n, *b = a + rpc * fstride<NF>(n);
   const size_t off = (size_t)pr * q.N + (size_t)blockIdx.x * rpc * n;
   const int tot = rpc * n;
+  auto slot = [&](int e) { return fslot<NF>(e / n, e % n, n); };
   load_twiddles(tw, twg, n);
-  for (int e = threadIdx.x; e < tot; e += blockDim.x) a[e] = hat[off + e];
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) a[slot(e)] = hat[off + e];
   __syncthreads();
   const float2 *res = fft_rows<NF>(a, b, pl, tw, true, rpc);
-  for (int e = threadIdx.x; e < tot; e += blockDim.x) out[off + e] = res[e];
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) out[off + e] = res[slot(e)];
 }
 
 // out = (I - P) y with fused fp64 dots: which 0: acc_r0v += <r0, out>;
@@ -552,11 +571,12 @@ struct PrecKernels {
   RowsKernel rows;
   ColsKernel cols;
   InvKernel inv;
+  int fixed;  // compile-time plans in the padded shared-memory layout
 };
 
 template <int NF, int NB>
 static PrecKernels prec_kernels_t() {
-  return {c3_prec_rows_kernel<NF>, c3_prec_cols_kernel<NB>, c3_prec_rows_inv_kernel<NF>};
+  return {c3_prec_rows_kernel<NF>, c3_prec_cols_kernel<NB>, c3_prec_rows_inv_kernel<NF>, NF > 0 ? 1 : 0};
 }
 
 // Square transverse grids of the common sizes get compile-time FFT plans.
@@ -682,10 +702,11 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     return set_error(TP_ERR_INVALID, "train_every needs train_z0, train_sol and train_diag");
   const int rpc = fft_rows_of(nf, nb), cpc = fft_rows_of(nb, nf);
   const int use_fft = fft_on;
-  const size_t smem_rows = (size_t)(nf + 2 * rpc * nf) * sizeof(float2);
-  const size_t smem_cols = (size_t)(nb + 2 * cpc * nb) * sizeof(float2);
   // kernels of the preconditioner: compile-time FFT plans for the common sizes
   PrecKernels pk = prec_kernels(nf, nb);
+  const int srow_f = pk.fixed ? nf + nf / 8 + 1 : nf, srow_b = pk.fixed ? nb + nb / 8 + 1 : nb;
+  const size_t smem_rows = (size_t)(nf + 2 * rpc * srow_f) * sizeof(float2);
+  const size_t smem_cols = (size_t)(nb + 2 * cpc * srow_b) * sizeof(float2);
   if (use_fft) {
     TP_CHECK_CUDA(cudaFuncSetAttribute(pk.rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
     TP_CHECK_CUDA(cudaFuncSetAttribute(pk.inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));

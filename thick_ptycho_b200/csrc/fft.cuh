@@ -186,6 +186,55 @@ __device__ __forceinline__ float2 *fft_run_fixed(float2 *a, float2 *b, const flo
   }
 }
 
+// Padded shared-memory layout of the fixed-size transforms: element i of a
+// transform sits at i + i/8 (one spare slot per 8 elements) and transform bi
+// starts at bi * S, S = N + N/8 + 1.  The Stockham writes of the early passes
+// (stride R elements) and column transposes (stride S) then spread over the
+// shared-memory banks instead of hitting a few of them.
+template <int N>
+struct FftPad {
+  static constexpr int S = N + N / 8 + 1;
+};
+__device__ __forceinline__ int fft_pad(int i) { return i + (i >> 3); }
+
+template <int N, int Ns, int R>
+__device__ __forceinline__ void fft_pass_padded(const float2 *a, float2 *b, const float2 *tw, float sign, int nb, int tid,
+                                                int nth) {
+  constexpr int T = N / R;
+  constexpr int step = N / (Ns * R);
+  constexpr int S = FftPad<N>::S;
+  for (int w = tid; w < nb * T; w += nth) {
+    const int bi = w / T, j = w - bi * T;
+    const float2 *src = a + bi * S;
+    float2 *dst = b + bi * S;
+    const int k = j % Ns;
+    float2 v[8];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[fft_pad(j + r * T)];
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      const float2 t = tw[(r * k * step) % N];
+      v[r] = cmul(v[r], make_float2(t.x, sign < 0 ? t.y : -t.y));
+    }
+    dft_small<R>(v, sign);
+    const int idx = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[fft_pad(idx + r * Ns)] = v[r];
+  }
+}
+
+template <int N, int Ns, int R, int... Rest>
+__device__ __forceinline__ float2 *fft_run_padded(float2 *a, float2 *b, const float2 *tw, float sign, int nb, int tid,
+                                                  int nth) {
+  fft_pass_padded<N, Ns, R>(a, b, tw, sign, nb, tid, nth);
+  __syncthreads();
+  if constexpr (sizeof...(Rest) == 0) {
+    return b;
+  } else {
+    return fft_run_padded<N, Ns * R, Rest...>(b, a, tw, sign, nb, tid, nth);
+  }
+}
+
 // Lengths with a compile-time plan (radices 8s first, then 4, 2, 3).
 __host__ __device__ constexpr bool fft_fixed_size(int n) {
   return n == 32 || n == 64 || n == 128 || n == 192 || n == 256 || n == 512;
@@ -201,6 +250,19 @@ __device__ __forceinline__ float2 *fft_block_fixed(float2 *a, float2 *b, const f
   else if constexpr (N == 192) return fft_run_fixed<192, 1, 8, 8, 3>(a, b, tw, sign, nb, tid, nth);
   else if constexpr (N == 256) return fft_run_fixed<256, 1, 8, 8, 4>(a, b, tw, sign, nb, tid, nth);
   else return fft_run_fixed<512, 1, 8, 8, 8>(a, b, tw, sign, nb, tid, nth);
+}
+
+// The fixed-size transforms in the padded layout (FftPad).
+template <int N>
+__device__ __forceinline__ float2 *fft_block_padded(float2 *a, float2 *b, const float2 *tw, bool inverse, int nb,
+                                                    int tid, int nth) {
+  const float sign = inverse ? 1.f : -1.f;
+  if constexpr (N == 32) return fft_run_padded<32, 1, 8, 4>(a, b, tw, sign, nb, tid, nth);
+  else if constexpr (N == 64) return fft_run_padded<64, 1, 8, 8>(a, b, tw, sign, nb, tid, nth);
+  else if constexpr (N == 128) return fft_run_padded<128, 1, 8, 8, 2>(a, b, tw, sign, nb, tid, nth);
+  else if constexpr (N == 192) return fft_run_padded<192, 1, 8, 8, 3>(a, b, tw, sign, nb, tid, nth);
+  else if constexpr (N == 256) return fft_run_padded<256, 1, 8, 8, 4>(a, b, tw, sign, nb, tid, nth);
+  else return fft_run_padded<512, 1, 8, 8, 8>(a, b, tw, sign, nb, tid, nth);
 }
 
 // nb transforms of length pl.n stored back to back in `a` (scratch `b` of
