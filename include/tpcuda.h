@@ -181,6 +181,21 @@ TP_API int tp_cn2d_unchunk(const tp_cn2d_op *op, int32_t num_probes, const void 
 TP_API int tp_cn2d_march_noalloc(const tp_cn2d_op *op, const void *n_field, int32_t n_dtype,
                                  const tp_cn2d_march_args *args, tp_stream_t stream);
 
+/*
+ * The reference's NLCG pieces on stored chunked fields (P, nz, Npad) of a
+ * FORWARD march (u_store) and a reference ADJOINT march (lam_store), with its
+ * constant gradient operator grad_A = -(diag(G) + subdiag(G)), G = (dz/2)(k/i)
+ * (forward_model.py:128-153).  Both need exact_ref_coeff = 0 and empty_px = 0.
+ */
+/* compute_grad_least_squares (pwe_reconstructor.py:100-164): grad_re, grad_im
+ * float32 (L*N), z-major like the reference's vector form; overwritten. */
+TP_API int tp_cn2d_ref_gradient(const tp_cn2d_op *op, int32_t num_probes, const void *u_store,
+                                const void *lam_store, float *grad_re, float *grad_im, tp_stream_t stream);
+/* The per-probe source grad_A @ u_p of compute_alphak (pwe_reconstructor.py:
+ * 166-219) as float2 (P, L, N), the src_probe layout of tp_cn2d_march. */
+TP_API int tp_cn2d_alpha_source(const tp_cn2d_op *op, int32_t num_probes, const void *u_store, void *src,
+                                tp_stream_t stream);
+
 /* ---------------------------------------------------------------- FFT heads
  * Shared-memory mixed-radix FFTs: n = 2^a 3^b 5^c, n <= 4096; rows of n
  * complex64 values, numpy conventions (forward unnormalised, inverse 1/n). */

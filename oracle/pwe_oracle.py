@@ -381,6 +381,71 @@ def reference_grad_least_squares(A, B, C2d, u_all, exit_err, k, dz):
     return gre, gim
 
 
+def reference_alphak(A, B, C2d, u_all, probes, grad_E, d, k, dz, imaginary=False):
+    """The reference's ``compute_alphak`` (``pwe_reconstructor.py:166-219``).
+
+    Per probe: the source ``grad_A @ u`` (times i for the imaginary part),
+    a forward solve that starts from the probe itself, and
+    ``δp = −δu_L · d_L`` (plain dot product over the last slice); the step is
+    ``−vdot(d, grad_E) / Σ_p |δp|²``.
+    """
+    P, N, Nz = u_all.shape
+    L = Nz - 1
+    G = (dz / 2) * (k / 1j)
+    lus, Bs = build_lu_factors(A, B, C2d, "forward")
+    den = 0.0
+    for p in range(P):
+        uk = u_all[p][:, 1:].T  # (L, N): vector-form blocks
+        g = -G * uk.copy()
+        g[1:] += -G * uk[:-1]
+        if imaginary:
+            g = 1j * g
+        du = march_with_lu(lus, Bs, np.zeros(N, dtype=complex), probes[p], "forward", g.T)
+        dp = -(du[:, -1] @ d[-N:])
+        den += abs(dp) ** 2
+    num = np.vdot(d, grad_E)
+    return -(num / den) if den > 0 else 0.0
+
+
+def reference_betak(g, g_old):
+    """``compute_betak`` (``pwe_reconstructor.py:221-228``): min(FR, max(PR, 0))."""
+    nrm = np.vdot(g_old, g_old)
+    pr = np.vdot(g, g - g_old) / nrm
+    fr = np.vdot(g, g) / nrm
+    return min(fr, max(pr, 0))
+
+
+def reference_nlcg(A, B, n0, probes, data, k, dz, iters, phase_retrieval=True):
+    """``ReconstructorPWE.reconstruct`` (``pwe_reconstructor.py:229-368``) for one
+    projection and angle, computed step sizes, no regularisation, constant
+    gradient operator (``exact_ref_coeff`` off).  Returns (n, residuals)."""
+    nk = np.array(n0, dtype=complex)
+    N, Nz = nk.shape
+    L = Nz - 1
+    P = probes.shape[0]
+    residual = []
+    d_re = d_im = g_re_old = g_im_old = None
+    for i in range(iters):
+        C = object_contribution(nk, k, dz)
+        lus, Bs = build_lu_factors(A, B, C, "forward")
+        u = np.stack([march_with_lu(lus, Bs, np.zeros(N, dtype=complex), probes[p], "forward") for p in range(P)])
+        ex = u[:, :, -1]
+        err = ex - (phase_retrieval_projection(ex, data) if phase_retrieval else data)
+        residual.append(float(np.sqrt(np.mean(np.abs(err) ** 2))))
+        g_re, g_im = reference_grad_least_squares(A, B, C, u, err, k, dz)
+        if i == 0:
+            d_re, g_re_old = -g_re, g_re
+            d_im, g_im_old = -g_im, g_im
+        a_re = reference_alphak(A, B, C, u, probes, g_re, d_re, k, dz)
+        a_im = reference_alphak(A, B, C, u, probes, g_im, d_im, k, dz, imaginary=True)
+        nk[:, 1:] += (a_re * d_re).reshape(L, N).T + 1j * (a_im * d_im).reshape(L, N).T
+        b_re = reference_betak(g_re, g_re_old)
+        b_im = reference_betak(g_im, g_im_old)
+        d_re, g_re_old = -g_re + b_re * d_re, g_re
+        d_im, g_im_old = -g_im + b_im * d_im, g_im
+    return nk, residual
+
+
 # ---------------------------------------------------------------------------
 # Multislice (angular spectrum), 2D
 # ---------------------------------------------------------------------------

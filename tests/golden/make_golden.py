@@ -212,6 +212,29 @@ def gradient_reference():
 
 
 # ---------------------------------------------------------------------------
+# 4b. Reference NLCG reconstruction (pwe_reconstructor.py:166-368)
+# ---------------------------------------------------------------------------
+def nlcg_reference():
+    """n after 1, 2 and 3 iterations of ReconstructorPWE.reconstruct (phase
+    retrieval, computed step sizes) from the same start, and the residuals."""
+    ss = small_space_2d(nz=16)
+    rng = np.random.default_rng(2024)
+    probes = create_ptycho_probes(ss)
+    n_true = 1 + 1e-3 * (rng.standard_normal((ss.nx, ss.nz)) + 0.05j * np.abs(rng.standard_normal((ss.nx, ss.nz))))
+    fwd = PWEIterativeLUSolver(ss, probes, bc_type="impedance")
+    data = fwd.get_farfield_intensities(fwd.solve(n=n_true), poisson_noise=False)
+    n0 = (1 + 2e-4 * rng.standard_normal((ss.nx, ss.nz))).astype(complex)
+    out = {"n0": n0, "data": data, "probes": np.asarray(probes)[0], **sim_params(ss)}
+    for iters in (1, 2, 3):
+        rec = ReconstructorPWE(ss, data, phase_retrieval=True, solver_type="iterative", bc_type="impedance",
+                               verbose=False)
+        nk, _, residual = rec.reconstruct(max_iters=iters, n_initial=n0.copy())
+        out[f"n_{iters}"] = np.asarray(nk)
+        out[f"residual_{iters}"] = np.asarray(residual)
+    save("nlcg_ref", **out)
+
+
+# ---------------------------------------------------------------------------
 # 5. Random small 3D cases and scan orders
 # ---------------------------------------------------------------------------
 def random_3d():
@@ -265,5 +288,6 @@ if __name__ == "__main__":
     random_2d()
     config0_reference()
     gradient_reference()
+    nlcg_reference()
     kat_3d()
     random_3d()

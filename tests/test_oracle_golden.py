@@ -190,3 +190,16 @@ def test_oracle_exact_adjoint_matches_finite_differences():
             fd = (loss(n + e) - loss(n - e)) / (2 * h)
             an = gn[x, t].real if part == "re" else gn[x, t].imag
             assert abs(fd - an) <= 1e-5 * max(abs(an), 1e-3 * np.abs(gn).max()), (x, t, part, fd, an)
+
+
+def test_reference_nlcg_iterations(golden):
+    """The restated NLCG loop against ReconstructorPWE.reconstruct run for 1, 2, 3 iterations."""
+    g = golden("nlcg_ref")
+    k, dz, dx, N = float(g["k"]), float(g["dz"]), float(g["dx"]), int(g["nx"])
+    co = po.bc_coefficients(k, dx, dz, bc_type="impedance")
+    A, B = po.step_matrices_1d(N, co, "impedance", dz)
+    for it in (1, 2, 3):
+        nk, res = po.reference_nlcg(A, B, g["n0"], g["probes"], g["data"], k, dz, it)
+        ref = g[f"n_{it}"]
+        assert np.linalg.norm(nk - ref) <= 1e-9 * np.linalg.norm(ref - g["n0"]), it
+        assert np.allclose(res, g[f"residual_{it}"], rtol=1e-9, atol=0)

@@ -141,6 +141,10 @@ SIGNATURES = [
                                        ctypes.c_void_p]),
     ("tp_cn2d_march_noalloc", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_void_p, ctypes.c_int32,
                                              ctypes.POINTER(TpCn2dMarchArgs), ctypes.c_void_p]),
+    ("tp_cn2d_ref_gradient", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("tp_cn2d_alpha_source", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_void_p]),
     ("tp_fft1d", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                 ctypes.c_void_p]),
     ("tp_farfield_intensity", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,

@@ -16,6 +16,17 @@ import torch
 from . import _native
 
 
+def fft_plannable(n: int) -> bool:
+    """True when libtpcuda's shared-memory FFT handles length n (2^a 3^b 5^c ≤ 4096)."""
+    n = int(n)
+    if n < 1 or n > 4096:
+        return False
+    for f in (2, 3, 5):
+        while n % f == 0:
+            n //= f
+    return n == 1
+
+
 def _stream(t: torch.Tensor):
     return ctypes.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
 
