@@ -312,15 +312,17 @@ def chain_grad_to_n(grad_c, k, dz, n=None, exact_ref_coeff=False, empty_space_px
 # ---------------------------------------------------------------------------
 # Exit waves, far field, phase-retrieval projection, amplitude loss
 # ---------------------------------------------------------------------------
-def farfield_intensity(exit_waves, dimension=2, shape2d=None):
-    """``|FFT(exit)|²``, unnormalised, no shift.
+def farfield_intensity(exit_waves, dimension=2):
+    """``|FFT(exit)|²`` without noise.
 
-    Restates ``forward_model/base/base_solver.py:234-242`` (Poisson noise off).
+    Restates ``forward_model/base/base_solver.py:213-249``: 2D, the FFT of each
+    exit wave; 3D, ``fft2`` over the last two axes of the (total_scans,
+    block_size) exit-wave array — the reference transforms across the scan
+    index and the flattened pixels, and this restates it as it is.
     """
     if dimension == 2:
         return np.abs(np.fft.fft(exit_waves, axis=-1)) ** 2
-    e = exit_waves.reshape(exit_waves.shape[0], *shape2d)
-    return (np.abs(np.fft.fft2(e, axes=(-2, -1))) ** 2).reshape(exit_waves.shape)
+    return np.abs(np.fft.fft2(exit_waves, axes=(-2, -1))) ** 2
 
 
 def phase_retrieval_projection(exit_waves, data):

@@ -212,6 +212,25 @@ def gradient_reference():
 
 
 # ---------------------------------------------------------------------------
+# 4a. Far-field intensities of 2D and 3D spaces (base/base_solver.py:213-249)
+# ---------------------------------------------------------------------------
+def farfield_reference():
+    from types import SimpleNamespace
+
+    from thick_ptycho.forward_model.base.base_solver import BaseForwardModelSolver
+
+    rng = np.random.default_rng(77)
+    out = {}
+    for dim, scans, block in ((2, 5, 40), (3, 4, 36)):
+        obj = SimpleNamespace(simulation_space=SimpleNamespace(dimension=dim, total_scans=scans, block_size=block))
+        ex = rng.standard_normal((scans, block)) + 1j * rng.standard_normal((scans, block))
+        out[f"ex_{dim}d"] = ex
+        out[f"intensity_{dim}d"] = BaseForwardModelSolver.get_farfield_intensities(obj, exit_waves=ex,
+                                                                                  poisson_noise=False)
+    save("farfield_ref", **out)
+
+
+# ---------------------------------------------------------------------------
 # 4b. Reference NLCG reconstruction (pwe_reconstructor.py:166-368)
 # ---------------------------------------------------------------------------
 def nlcg_reference():
@@ -288,6 +307,7 @@ if __name__ == "__main__":
     random_2d()
     config0_reference()
     gradient_reference()
+    farfield_reference()
     nlcg_reference()
     kat_3d()
     random_3d()

@@ -203,3 +203,11 @@ def test_reference_nlcg_iterations(golden):
         ref = g[f"n_{it}"]
         assert np.linalg.norm(nk - ref) <= 1e-9 * np.linalg.norm(ref - g["n0"]), it
         assert np.allclose(res, g[f"residual_{it}"], rtol=1e-9, atol=0)
+
+
+def test_farfield_2d_and_3d(golden):
+    """Far-field intensities of the unmodified reference (3D: fft2 over scans x pixels, as it does)."""
+    g = golden("farfield_ref")
+    for dim in (2, 3):
+        assert np.allclose(po.farfield_intensity(g[f"ex_{dim}d"], dimension=dim), g[f"intensity_{dim}d"],
+                           rtol=1e-12, atol=1e-12)

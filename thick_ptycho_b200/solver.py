@@ -281,13 +281,41 @@ class PWEGpuSolver:
         """``u[..., −1]`` as (total_scans, block_size) (``base/base_solver.py:194-211``)."""
         return u[..., -1].reshape((self.simulation_space.total_scans, self.block_size))
 
-    def get_farfield_intensities(self, u=None, exit_waves=None, poisson_noise=True) -> np.ndarray:
-        """``|FFT(exit)|²`` with optional Poisson noise (``base/base_solver.py:213-249``)."""
+    def get_farfield_intensities(self, u=None, exit_waves=None, poisson_noise=True,
+                                 generator: Optional[torch.Generator] = None) -> np.ndarray:
+        """``|FFT(exit)|²`` with optional Poisson noise (``base/base_solver.py:213-249``), on the GPU.
+
+        2D: FFT of each exit wave (libtpcuda's FFT head when the length is
+        2^a 3^b 5^c ≤ 4096, else cuFFT through torch).  3D: as the reference,
+        ``fft2`` over the last two axes of the (total_scans, block_size)
+        exit-wave array.  Poisson noise is drawn on the device from
+        `generator` (the reference draws from numpy's unseeded global RNG);
+        noisy intensities are returned as int64 like ``numpy.random.poisson``.
+        """
+        from . import heads
+
         exit_waves = self.get_exit_waves(u=u) if exit_waves is None else exit_waves
-        intensities = np.abs(np.fft.fft(exit_waves)) ** 2
+        ex = torch.as_tensor(np.ascontiguousarray(exit_waves)).to(self.device, torch.complex64)
+        ex = ex.reshape(self.simulation_space.total_scans, self.block_size).contiguous()
+        if self.dimension == 2 and heads.fft_plannable(self.block_size):
+            inten = heads.farfield_intensity(ex).to(torch.float64)
+        elif self.dimension == 2:
+            inten = torch.fft.fft(ex.to(torch.complex128), dim=-1).abs() ** 2
+        else:
+            inten = torch.fft.fft2(ex.to(torch.complex128), dim=(-2, -1)).abs() ** 2
         if poisson_noise:
-            intensities = np.random.poisson(intensities)
-        return intensities.reshape((self.simulation_space.total_scans, self.block_size))
+            inten = torch.poisson(inten, generator=generator).to(torch.int64)
+        return inten.cpu().numpy().reshape((self.simulation_space.total_scans, self.block_size))
+
+    def save_simulated_data(self, path, n=None, poisson_noise=True, generator: Optional[torch.Generator] = None):
+        """Forward-simulate and write ``{intensity, exit_waves}`` in the
+        reference's ``simulated_data.npz`` format (``generate_data.py:185-197``,
+        read back by ``reconstruct_sample.py:62-67``)."""
+        u = self.solve(n=n)
+        exit_waves = self.get_exit_waves(u)
+        data = self.get_farfield_intensities(exit_waves=exit_waves, poisson_noise=poisson_noise, generator=generator)
+        np.savez_compressed(path, intensity=data, exit_waves=exit_waves)
+        return data, exit_waves
 
     def device_status(self):
         """Raise if a device-side bounded wait of an earlier launch timed out."""
