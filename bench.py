@@ -53,9 +53,10 @@ def parse():
     ap.add_argument("--config", default="2d-fwd-adj-2048x1024-p512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-3d", action="store_true", help="skip the 3D learned-vs-plain section")
-    ap.add_argument("--case", choices=("headline", "3d-march-small"), default="headline",
+    ap.add_argument("--case", choices=("headline", "3d-march-small", "3d-recon"), default="headline",
                     help="3d-march-small: a few learned 3D forward marches (256 x 256 x 5 nodes, 64 probes), "
-                         "a small profiler target for the conv and FFT kernels")
+                         "a small profiler target for the conv and FFT kernels; 3d-recon: `steps` gradient-descent "
+                         "iterations of the 3D reconstruction (192 x 192 x 192, 256 probes), plain vs learned")
     return ap.parse_args()
 
 
@@ -518,12 +519,79 @@ def run_case_3d_small(a):
                       "stats": eng.read_stats()}), flush=True)
 
 
+def run_case_3d_recon(a):
+    """3D reconstruction, 192 x 192 transverse x 192 nodes, 256 probes (16 x 16 raster, stride 10,
+    waist 12), ground truth δn = 600 seeded ellipsoids + 1e-6 i, data = |FFT2(exit)| of the truth;
+    `steps` gradient-descent iterations from δn = 0 with the plain FFT preconditioner and with the
+    learned one in the forward and adjoint marches (network trained on white-noise pairs of another
+    seeded field, not timed).  Reports fwd+adj probe·slice/s of each run, Krylov iterations per
+    solve, the loss histories, the final δn error against the truth and learned vs plain."""
+    import torch
+
+    from thick_ptycho_b200 import heads
+    from thick_ptycho_b200.cn3d import CN3D, PWEGradient3D, generate_pairs
+    from thick_ptycho_b200.learned import LearnedPreconditioner, default_kappa
+    from thick_ptycho_b200.reconstruct import gradient_descent_3d
+    from thick_ptycho_b200.workloads import CONFIG4, ellipsoid_field_3d
+
+    w = CONFIG4
+    geo = w.geometry()
+    dev = torch.device("cuda", 0)
+    n, nz, P = w.nx, w.nz, w.num_probes
+    N, L = n * n, nz - 1
+    dn_true = w.delta_n().reshape(N, nz)
+    probes = torch.from_numpy(w.probes(geo).reshape(P, N).astype(np.complex64)).to(dev)
+    truth = PWEGradient3D(geo, device=dev)
+    ex = truth.forward(torch.from_numpy(1 - dn_true).to(dev), probes)
+    amp = heads.fft2_last(ex.reshape(P, n, n).contiguous()).abs().to(torch.float64)
+    del truth, ex
+    t0 = time.perf_counter()
+    eng = CN3D(n, n, nz, geo.k, 1.0, 1.0, 1.0, "impedance", device=dev)
+    pairs = generate_pairs(eng, torch.from_numpy((1 - ellipsoid_field_3d(n, n, nz, w.n_shapes, 1001)).reshape(N, nz)).to(dev),
+                           probes[:40].contiguous(), every=1, kind="noise")
+    model = LearnedPreconditioner(n, n, default_kappa(geo.k, 1.0, 5e-4), device=dev, seed=0)
+    model.train(pairs, steps=1500, slices_per_batch=2, lr=1e-3)
+    torch.cuda.synchronize(dev)
+    train_s = time.perf_counter() - t0
+    del pairs, eng
+    torch.cuda.empty_cache()
+    n0 = np.ones((N, nz), dtype=complex)
+    res = {}
+    for name, pc in (("plain", True), ("learned", "learned")):
+        g3 = PWEGradient3D(geo, device=dev, precond=pc, model=model)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record()
+        nk, losses, its = gradient_descent_3d(g3, n0, probes, amp, iters=a.steps)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+        dn = (1 - nk).cpu().numpy()  # the reference PWE index convention n = 1 − δn
+        res[name] = {"value": a.steps * P * L / (ms / 1e3), "unit": UNIT, "ms_total": ms,
+                     "krylov_iterations_per_solve": float(np.mean(its)), "loss_first": losses[0],
+                     "loss_last": losses[-1],
+                     "delta_n_rel_error_vs_truth": float(np.linalg.norm(dn - dn_true) / np.linalg.norm(dn_true)),
+                     "fallbacks": g3.engine.fallbacks, "_n": nk}
+    diff = float(torch.linalg.vector_norm(res["learned"]["_n"] - res["plain"]["_n"]) /
+                 torch.linalg.vector_norm(res["plain"]["_n"] - torch.from_numpy(n0).to(dev)))
+    for r in res.values():
+        r.pop("_n")
+    print(json.dumps({"case": "3d-recon", "workload": w.name, "iterations": a.steps,
+                      "metric": "probe·slice solves/s fwd+adj (3D gradient descent)", "plain": res["plain"],
+                      "learned": res["learned"], "learned_over_plain": res["learned"]["value"] / res["plain"]["value"],
+                      "n_diff_learned_vs_plain_rel_update": diff,
+                      "training": {"seconds": train_s, "pairs": 191 * 40, "steps": 1500, "not_timed": True}}),
+          flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
     elif a.case == "3d-march-small":
         run_case_3d_small(a)
+    elif a.case == "3d-recon":
+        run_case_3d_recon(a)
     else:
         run_ours(a)
 

@@ -107,3 +107,40 @@ def test_learned_march_against_oracle_and_iterations(trained, mode):
             assert np.linalg.norm(got[p] - ref) <= 2e-5 * np.linalg.norm(ref), (pc, p)
     assert eng.fallbacks == 0
     assert its["learned"] <= its[True], its
+
+
+def test_gradient_descent_learned_matches_plain(trained):
+    """Config-4-style reconstruction at small size: gradient descent on the 3D
+    amplitude loss with the learned preconditioner in the forward and the
+    adjoint marches lowers the loss as the plain run does (final losses within
+    1 %) and needs no more Krylov iterations.  The trajectories are compared
+    at the level the Krylov tolerance allows: at δn = 0 the gradient is a small
+    difference of large per-probe terms, and a 1e-6 relative residual per
+    solve moves it by ~1.6 % (measured between the plain FFT-preconditioned and
+    the unpreconditioned march as well), so after 4 steps the two n differ by
+    ~8 % of the total update; the bound is 15 %."""
+    from types import SimpleNamespace
+
+    from thick_ptycho_b200 import heads
+    from thick_ptycho_b200.cn3d import PWEGradient3D
+    from thick_ptycho_b200.reconstruct import gradient_descent_3d
+
+    _, model, _ = trained
+    geo = SimpleNamespace(effective_shape=(NF, NB, NZ), nz=NZ, k=K, dx=1.0, dy=1.0, dz=1.0, exact_ref_coeff=False)
+    P = 4
+    probes = torch.from_numpy(_probes(P, 6).astype(np.complex64)).cuda()
+    truth = PWEGradient3D(geo)
+    ex = truth.forward(torch.from_numpy(_index(505)).cuda(), probes)
+    amp = heads.fft2_last(ex.reshape(P, NF, NB).contiguous()).abs().to(torch.float64)
+    n0 = np.ones((NF * NB, NZ), dtype=complex)
+    runs = {}
+    for pc in (True, "learned"):
+        g3 = PWEGradient3D(geo, precond=pc, model=model)
+        n, losses, its = gradient_descent_3d(g3, n0, probes, amp, iters=4)
+        assert losses[-1] < 0.95 * losses[0], (pc, losses)
+        assert g3.engine.fallbacks == 0
+        runs[pc] = (n.cpu().numpy(), sum(its), losses[-1])
+    assert abs(runs["learned"][2] - runs[True][2]) <= 1e-2 * runs[True][2]
+    diff = np.linalg.norm(runs["learned"][0] - runs[True][0]) / np.linalg.norm(runs[True][0] - n0)
+    assert diff <= 0.15, diff
+    assert runs["learned"][1] <= runs[True][1], (runs["learned"][1], runs[True][1])

@@ -174,15 +174,17 @@ class CN3D:
 
 class PWEGradient3D:
     """Amplitude-loss gradient of a 3D geometry, all probes batched
-    (far field ``|FFT2(exit)|``; forward + exact adjoint by :class:`CN3D`)."""
+    (far field ``|FFT2(exit)|`` of each probe's nx × ny exit wave; forward +
+    exact adjoint by :class:`CN3D`; ``precond="learned"`` with a
+    :class:`learned.LearnedPreconditioner` uses the learned correction in both)."""
 
-    def __init__(self, geometry, bc_type="impedance", device=None, tol=1e-6, max_iter=20, precond=True):
+    def __init__(self, geometry, bc_type="impedance", device=None, tol=1e-6, max_iter=20, precond=True, model=None):
         self.geometry = geometry
         self.engine = CN3D(geometry.effective_shape[0], geometry.effective_shape[1], geometry.nz, geometry.k,
                            geometry.dx, getattr(geometry, "dy", geometry.dx), geometry.dz, bc_type,
                            exact_ref_coeff=bool(getattr(geometry, "exact_ref_coeff", False)), device=device)
         self.device = self.engine.device
-        self.kw = dict(tol=tol, max_iter=max_iter, precond=precond)
+        self.kw = dict(tol=tol, max_iter=max_iter, precond=precond, model=model)
         self._store = None
 
     def forward(self, field, probes):
@@ -212,12 +214,21 @@ class PWEGradient3D:
             self.device, torch.complex64).reshape(-1, e.N)
         amp = torch.as_tensor(np.ascontiguousarray(amplitude) if not isinstance(amplitude, torch.Tensor) else amplitude).to(
             self.device, torch.float64).reshape(-1, e.nx, e.ny)
-        ex = self.forward(field, pr).reshape(-1, e.nx, e.ny)
-        U = torch.fft.fft2(ex.to(torch.complex128))
-        mag = U.abs()
+        from . import heads
+
+        ex = self.forward(field, pr).reshape(-1, e.nx, e.ny).contiguous()
+        if heads.fft_plannable(e.nx) and heads.fft_plannable(e.ny):
+            U = heads.fft2_last(ex)
+        else:
+            U = torch.fft.fft2(ex)
+        mag = U.abs().to(torch.float64)
         loss = torch.sum((mag - amp) ** 2)
-        gU = torch.where(mag > 0, 2 * (mag - amp) / torch.where(mag > 0, mag, torch.ones_like(mag)), torch.zeros_like(mag)) * U
-        ge = (e.N * torch.fft.ifft2(gU)).to(torch.complex64).reshape(-1, e.N)
+        safe = torch.where(mag > 0, mag, torch.ones_like(mag))
+        gU = (torch.where(mag > 0, 2 * (mag - amp) / safe, torch.zeros_like(mag)).to(torch.float32) * U).contiguous()
+        if heads.fft_plannable(e.nx) and heads.fft_plannable(e.ny):
+            ge = (e.N * heads.fft2_last(gU, inverse=True)).reshape(-1, e.N).contiguous()
+        else:
+            ge = (e.N * torch.fft.ifft2(gU)).reshape(-1, e.N).contiguous()
         g = self.backward(field, ge)
         return float(loss.item()), g.reshape(e.nx, e.ny, e.nz)
 

@@ -47,6 +47,20 @@ def fft1d(x: torch.Tensor, inverse: bool = False, out: torch.Tensor = None) -> t
     return out
 
 
+def fft2_last(x: torch.Tensor, inverse: bool = False) -> torch.Tensor:
+    """2D FFT over the last two axes (numpy conventions) with the 1D FFT head:
+    a pass along the last axis, a transpose, a pass along the other axis and a
+    transpose back.  Both lengths must be 2^a 3^b 5^c ≤ 4096."""
+    _check(x, "x")
+    n0, n1 = x.shape[-2], x.shape[-1]
+    if not (fft_plannable(n0) and fft_plannable(n1)):
+        raise ValueError(f"fft2_last needs 2^a 3^b 5^c <= 4096 lengths, got {n0} x {n1}")
+    y = fft1d(x, inverse)
+    yt = y.transpose(-1, -2).contiguous()
+    z = fft1d(yt, inverse)
+    return z.transpose(-1, -2).contiguous()
+
+
 def farfield_intensity(exit_waves: torch.Tensor) -> torch.Tensor:
     """``|FFT(exit)|²`` along the last axis, float32."""
     _check(exit_waves, "exit_waves")

@@ -162,3 +162,27 @@ class ReconstructorPWEGpu:
             d_re, g_re_old = -g_re + b_re * d_re, g_re
             d_im, g_im_old = -g_im + b_im * d_im, g_im
         return nk.cpu().numpy(), residual
+
+
+def gradient_descent_3d(grad3d, n0, probes, amplitude, iters=20, step=None, max_update=5e-5):
+    """Gradient descent on the 3D amplitude loss with :class:`cn3d.PWEGradient3D`:
+    ``n ← n − η ∂loss/∂n`` (torch convention ∂/∂Re + i ∂/∂Im).  ``η`` is `step`,
+    or chosen at the first iteration so that the largest update is `max_update`.
+    Returns (n, losses, Krylov iterations per solve of each iteration)."""
+    eng = grad3d.engine
+    n = torch.as_tensor(np.ascontiguousarray(n0) if not isinstance(n0, torch.Tensor) else n0)
+    n = n.to(eng.device, torch.complex128).reshape(eng.N, eng.nz).clone()
+    eta = step
+    losses, its = [], []
+    eng.read_stats()
+    for _ in range(iters):
+        loss, g = grad3d.loss_and_grad(n, probes, amplitude)
+        st = eng.read_stats()
+        losses.append(loss)
+        its.append(st["iterations"] / max(st["solves"], 1))
+        g = g.reshape(eng.N, eng.nz).to(torch.complex128)
+        if eta is None:
+            gmax = float(g.abs().max())
+            eta = max_update / gmax if gmax > 0 else 0.0
+        n -= eta * g
+    return n, losses, its
