@@ -240,6 +240,20 @@ TP_API int tp_ms2d_march(const tp_ms2d_op *op, const void *trans, const void *pr
 TP_API int tp_ms2d_backward(const tp_ms2d_op *op, const void *trans, const void *u_fwd, const void *src_exit,
                             int32_t num_probes, void *grad_t, tp_stream_t stream);
 
+/* Multislice 3PIE reconstruction (reconstruction/ms_reconstructor.py:40-190):
+ * `iters` epochs over the probes in scan order, each probe's forward march,
+ * modulus constraint and slice-by-slice back-propagation update applied to
+ * the estimate in place (sequential, as the reference; one CTA).
+ * data: float (P, n) far-field intensities when phase_retrieval != 0, else
+ * float2 (P, n) known exit waves.  n_est: double2 (n, nz) row-major, the
+ * starting estimate in, the result out.  loss: double (iters), the rms of
+ * (corrected - modelled) exit waves per epoch.  Workspace:
+ * tp_ms2d_3pie_workspace_bytes(n, nz). */
+TP_API size_t tp_ms2d_3pie_workspace_bytes(int32_t n, int32_t nz);
+TP_API int tp_ms2d_3pie(const tp_ms2d_op *op, const void *probes, int32_t num_probes, const void *data,
+                        int32_t phase_retrieval, int32_t iters, double alpha_obj, void *n_est, double *loss,
+                        void *workspace, size_t workspace_bytes, tp_stream_t stream);
+
 /* ------------------------------------------------------------------- 3D
  * 3D problems (2D transverse, N = nf*nb rows, index i = b*nf + f, the
  * flattening of kron(I_y, A_x) in operator_matrices.py:75-99): each slice is

@@ -482,6 +482,45 @@ def ms_forward(n, probe, k, dx, dz, n_medium=1.0):
     return u
 
 
+def ms_3pie(probes, data, k, dx, dz, nz, iters, alpha_obj=1.0, n_medium=1.0, phase_retrieval=True):
+    """Multislice 3PIE reconstruction (``reconstruction/ms_reconstructor.py:40-190``).
+
+    Epochs over the probes in scan order; per probe: multislice forward from
+    the current estimate, modulus constraint on the exit wave
+    (``phase = F ψ / (|F ψ| + 1e-12)``), then from the detector plane back to
+    the entrance, for every slice z (last to first): ``ψ ← F⁻¹(conj(H) F ψ)``,
+    ``ψ ← ψ · conj(T_z)``, ``δψ = ψ − u_z`` and
+    ``n_z += (α/(it+1)) conj(u_z) δψ / (max|u_z|² + 1e-12) / (i k dz)``
+    (the estimate changes in place, probe after probe).  Returns (n, loss
+    per epoch) with loss = rms of (corrected − modelled) exit waves.
+    """
+    P, N = probes.shape
+    n_est = n_medium * np.ones((N, nz), dtype=complex)
+    H = ms_kernel(N, dx, k, dz)
+    loss = []
+    for it in range(iters):
+        err = np.zeros((P, N), dtype=complex)
+        for p in range(P):
+            u = ms_forward(n_est, probes[p], k, dx, dz, n_medium)
+            ex = u[:, -1]
+            if phase_retrieval:
+                f = np.fft.fft(ex)
+                corr = np.fft.ifft(np.sqrt(data[p]) * (f / (np.abs(f) + 1e-12)))
+            else:
+                corr = data[p]
+            err[p] = corr - ex
+            psi = corr
+            step = alpha_obj / (it + 1)
+            for z in reversed(range(nz)):
+                psi = np.fft.ifft(np.fft.fft(psi) * np.conj(H))
+                psi = psi * np.conj(np.exp(1j * k * (n_est[:, z] - n_medium) * dz))
+                dpsi = psi - u[:, z]
+                scale = np.max(np.abs(u[:, z]) ** 2) + 1e-12
+                n_est[:, z] = n_est[:, z] + step * (np.conj(u[:, z]) * dpsi / scale) / (1j * k * dz)
+        loss.append(float(np.sqrt(np.mean(np.abs(err) ** 2))))
+    return n_est, loss
+
+
 # ---------------------------------------------------------------------------
 # Exact impedance test boundary data (the reference's known-answer tests)
 # ---------------------------------------------------------------------------

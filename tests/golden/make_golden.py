@@ -254,6 +254,38 @@ def nlcg_reference():
 
 
 # ---------------------------------------------------------------------------
+# 4c. Reference multislice 3PIE reconstruction (ms_reconstructor.py:40-190)
+# ---------------------------------------------------------------------------
+def ms3pie_reference():
+    """n after 1 and 2 epochs of ReconstructorMS.reconstruct (phase retrieval,
+    alpha_obj = 0.1: with 1 the reference's update diverges on this problem)
+    on a 40-pixel-wide space (a length the GPU FFT plans)."""
+    from thick_ptycho.reconstruction.ms_reconstructor import ReconstructorMS
+
+    cfg = SimulationConfig(
+        probe_config=ProbeConfig(type=ProbeType.GAUSSIAN, wave_length=0.5, diameter=12.0),
+        scan_points=4, step_size_px=5, pad_factor=2.0, nz=16,
+        spatial_limits=Limits(x=(0.0, 33.0), z=(0.0, 15.0), units="meters"), use_logging=False,
+    )
+    ss = create_simulation_space(cfg)
+    assert ss.nx == 40, ss.nx
+    probes = create_ptycho_probes(ss)
+    # a smooth object: its scattering stays inside the probes' band, so the
+    # modulus projection never takes its phase from round-off (a white-noise
+    # object scatters into frequencies where the model's spectrum is zero)
+    n_true = 1 + blob_field_2d(ss.nx, ss.nz, 4, 31, sigma=(3.0, 6.0), amplitude=(-1e-3, 1e-3), absorption=1e-5)
+    ms = MSForwardModelSolver(ss, probes)
+    data = ms.get_farfield_intensities(ms.solve(n=n_true), poisson_noise=False)
+    out = {"data": data, "probes": np.asarray(probes)[0], "n_medium": complex(ss.n_medium), **sim_params(ss)}
+    for iters in (1, 2):
+        rec = ReconstructorMS(ss, data, phase_retrieval=True, verbose=False)
+        n_est, loss = rec.reconstruct(max_iters=iters, alpha_obj=0.1)
+        out[f"n_{iters}"] = np.asarray(n_est)
+        out[f"loss_{iters}"] = np.asarray(loss)
+    save("ms3pie_ref", **out)
+
+
+# ---------------------------------------------------------------------------
 # 5. Random small 3D cases and scan orders
 # ---------------------------------------------------------------------------
 def random_3d():
@@ -309,5 +341,6 @@ if __name__ == "__main__":
     gradient_reference()
     farfield_reference()
     nlcg_reference()
+    ms3pie_reference()
     kat_3d()
     random_3d()

@@ -121,3 +121,21 @@ def test_multislice_adjoint_gradient():
             an = g[xx, t].real if part == 0 else g[xx, t].imag
             assert abs(fd - an) <= 1e-3 * max(abs(fd), 1e-2 * scale), (xx, t, part, fd, an)
     assert np.all(g[:, -1] == 0)  # the last plane does not enter the multislice model
+
+
+def test_ms_3pie_against_reference_golden(golden):
+    """The multislice 3PIE kernel against ReconstructorMS.reconstruct (1 and 2 epochs).
+    Tolerance: complex64 fields and FFTs against the reference's complex128,
+    measured relative to the total update ‖n_k − 1‖: ≤ 1e-4 (1 epoch), ≤ 3e-4 (2)."""
+    from thick_ptycho_b200.ms2d import ReconstructorMSGpu
+
+    g = golden("ms3pie_ref")
+    N, nz = int(g["nx"]), int(g["nz"])
+    rec = ReconstructorMSGpu(N, nz, float(g["k"]), float(g["dx"]), float(g["dz"]), g["data"], g["probes"],
+                             phase_retrieval=True, n_medium=complex(g["n_medium"]))
+    for it, tol in ((1, 1e-4), (2, 3e-4)):
+        n, loss = rec.reconstruct(max_iters=it, alpha_obj=0.1)
+        ref = g[f"n_{it}"]
+        err = np.linalg.norm(n - ref) / np.linalg.norm(ref - 1)
+        assert err <= tol, (it, err)
+        assert np.allclose(loss, g[f"loss_{it}"], rtol=tol, atol=0), (loss, g[f"loss_{it}"])

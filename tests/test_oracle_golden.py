@@ -211,3 +211,14 @@ def test_farfield_2d_and_3d(golden):
     for dim in (2, 3):
         assert np.allclose(po.farfield_intensity(g[f"ex_{dim}d"], dimension=dim), g[f"intensity_{dim}d"],
                            rtol=1e-12, atol=1e-12)
+
+
+def test_ms_3pie_epochs(golden):
+    """The restated multislice 3PIE loop against ReconstructorMS.reconstruct (1 and 2 epochs)."""
+    g = golden("ms3pie_ref")
+    k, dx, dz, nz = float(g["k"]), float(g["dx"]), float(g["dz"]), int(g["nz"])
+    for it in (1, 2):
+        n, loss = po.ms_3pie(g["probes"], g["data"], k, dx, dz, nz, it, alpha_obj=0.1, n_medium=complex(g["n_medium"]))
+        ref = g[f"n_{it}"]
+        assert np.linalg.norm(n - ref) <= 1e-9 * np.linalg.norm(ref - 1), it
+        assert np.allclose(loss, g[f"loss_{it}"], rtol=1e-9, atol=0)

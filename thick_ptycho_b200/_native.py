@@ -157,6 +157,10 @@ SIGNATURES = [
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("tp_ms2d_backward", ctypes.c_int, [ctypes.POINTER(TpMs2dOp), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                         ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
+    ("tp_ms2d_3pie_workspace_bytes", ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
+    ("tp_ms2d_3pie", ctypes.c_int, [ctypes.POINTER(TpMs2dOp), ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                                    ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
     ("tp_cn3d_workspace_bytes", ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
     ("tp_cn3d_learned_ws_bytes", ctypes.c_size_t, [ctypes.c_int32] * 3),
     ("tp_cn3d_march", ctypes.c_int, [ctypes.POINTER(TpCn3dOp), ctypes.c_void_p, ctypes.c_int32,

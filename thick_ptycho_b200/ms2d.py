@@ -164,3 +164,40 @@ class MSGpuSolver:
         if poisson_noise:
             inten = np.random.poisson(inten)
         return inten.reshape((self.simulation_space.total_scans, self.simulation_space.block_size))
+
+
+class ReconstructorMSGpu:
+    """Multislice 3PIE reconstruction (``reconstruction/ms_reconstructor.py:40-190``) on the GPU.
+
+    Same arguments and results as the reference's ``ReconstructorMS``:
+    ``reconstruct(max_iters, alpha_obj)`` returns the estimate (nx, nz)
+    complex128 and the per-epoch rms exit-wave error.  The update is
+    sequential over probes, as the reference's, and runs in one kernel
+    (``tp_ms2d_3pie``).  ``data``: (P, N) far-field intensities with
+    ``phase_retrieval`` (else known exit waves); ``probes``: (P, N).
+    """
+
+    def __init__(self, n, nz, k, dx, dz, data, probes, phase_retrieval=True, n_medium=1.0, device=None):
+        self.engine = MS2D(n, nz, k, dx, dz, n_medium=n_medium, device=device)
+        e = self.engine
+        self.n_medium = complex(n_medium)
+        self.phase_retrieval = bool(phase_retrieval)
+        dt = torch.float32 if phase_retrieval else torch.complex64
+        self.data = torch.as_tensor(np.ascontiguousarray(data)).to(e.device, dt).reshape(-1, e.n).contiguous()
+        self.probes = torch.as_tensor(np.ascontiguousarray(probes)).to(e.device, torch.complex64).reshape(-1, e.n)
+        self.probes = self.probes.contiguous()
+        self.ws = torch.empty(int(e.lib.tp_ms2d_3pie_workspace_bytes(e.n, e.nz)), dtype=torch.uint8, device=e.device)
+
+    def reconstruct(self, max_iters=10, alpha_obj=1.0, refractive_index=None):
+        e = self.engine
+        if refractive_index is None:
+            n0 = self.n_medium * np.ones((e.n, e.nz), dtype=complex)
+        else:
+            n0 = np.array(refractive_index, dtype=complex)
+        n_est = torch.from_numpy(n0).to(e.device).contiguous()
+        loss = torch.zeros(max(int(max_iters), 1), dtype=torch.float64, device=e.device)
+        rc = e.lib.tp_ms2d_3pie(ctypes.byref(e._op), _ptr(self.probes), self.probes.shape[0], _ptr(self.data),
+                                int(self.phase_retrieval), int(max_iters), float(alpha_obj), _ptr(n_est), _ptr(loss),
+                                _ptr(self.ws), self.ws.numel(), _stream(e.device))
+        _native.check(rc, "tp_ms2d_3pie")
+        return n_est.cpu().numpy(), loss[: int(max_iters)].cpu().numpy().tolist()
