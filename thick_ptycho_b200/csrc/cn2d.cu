@@ -233,6 +233,7 @@ __global__ void __launch_bounds__(128) cn2d_factor_kernel(const FactorParams f) 
   double2 rc = c < C - 1 ? zmul(me_c, wf_n) : z2(0, 0);
   LR[0 * C + c] = to_f2(me_a);
   LR[1 * C + c] = to_f2(c < C - 1 ? me_c : z2(0, 0));
+  double amax = 0.0;  // largest PCR coefficient of this chunk
   for (int l = 0; l < f.levels; ++l) {
     const int s = 1 << l;
     fsm[c] = ra;
@@ -253,7 +254,10 @@ __global__ void __launch_bounds__(128) cn2d_factor_kernel(const FactorParams f) 
     rc = nrc;
     LR[rec_alpha(f.levels, l) * C + c] = to_f2(al);
     LR[rec_gamma(f.levels, l) * C + c] = to_f2(ga);
+    amax = fmax(amax, fmax(hypot(al.x, al.y), hypot(ga.x, ga.y)));
   }
+  // non-negative floats order like their bit patterns
+  if (f.coupling != nullptr) atomicMax(f.coupling, __float_as_uint((float)fmin(amax, 3.0e38)));
   LR[rec_rde(f.levels) * C + c] = to_f2(zdiv(z2(1.0 - rd.x, -rd.y), rd));
 }
 
@@ -670,7 +674,7 @@ extern "C" int tp_cn2d_layout(int32_t n, int32_t *chunks, int32_t *rows_per_chun
 extern "C" size_t tp_cn2d_factor_bytes(int32_t n, int32_t nz) {
   Partition pt;
   if (nz < 2 || partition_for(n, &pt) != TP_OK) return 0;
-  return slice_bytes(pt) * (size_t)(nz - 1);
+  return slice_bytes(pt) * (size_t)(nz - 1) + kFactorTailBytes;
 }
 
 extern "C" int tp_cn2d_factor(const tp_cn2d_op *op, const void *n_field, int32_t n_dtype, int32_t mode,
@@ -716,7 +720,9 @@ extern "C" int tp_cn2d_factor(const tp_cn2d_op *op, const void *n_field, int32_t
   f.n = n_field;
   f.factors = static_cast<char *>(factors);
   f.slice_bytes = slice_bytes(pt);
+  f.coupling = reinterpret_cast<unsigned *>(f.factors + (size_t)f.L * f.slice_bytes);
   f.err = err;
+  TP_CHECK_CUDA(cudaMemsetAsync(f.coupling, 0, sizeof(unsigned), reinterpret_cast<cudaStream_t>(stream)));
   const size_t smem = 5 * (size_t)pt.C * sizeof(double2);
   cn2d_factor_kernel<<<f.L, pt.C, smem, reinterpret_cast<cudaStream_t>(stream)>>>(f);
   return check_cuda(cudaGetLastError(), "cn2d_factor_kernel launch");
@@ -763,6 +769,7 @@ extern "C" int tp_cn2d_march(const tp_cn2d_op *op, const void *factors, const tp
   mp.exit_out = static_cast<float2 *>(a->exit_out);
   mp.u_fwd = static_cast<const float2 *>(a->u_fwd);
   mp.grad_c = static_cast<float2 *>(a->grad_c);
+  mp.coupling = reinterpret_cast<const unsigned *>(mp.factors + (size_t)mp.L * mp.slice_bytes);
   mp.err = err;
   mp.t0 = a->t_begin > 0 ? a->t_begin : 1;
   mp.t1 = a->t_end > 0 ? a->t_end : mp.L;

@@ -31,11 +31,18 @@ __host__ __device__ inline int rec_gamma(int levels, int l) { return 2 + levels 
 __host__ __device__ inline int rec_rde(int levels) { return 2 + 2 * levels; }
 
 // Global factor set of one slice: QD, LF, EP, V, W ([M][C] float2 each) then
-// the records ([nrec][C] float2), padded to 256 bytes.
+// the records ([nrec][C] float2), padded to 256 bytes.  The workspace of a
+// factorisation holds L slices and then kFactorTailBytes: the largest PCR
+// coefficient of all slices (float bits), which the team march reads.
 __host__ __device__ inline size_t slice_bytes(const Partition &pt) {
   size_t b = (size_t)(5 * pt.M + pt.nrec) * pt.C * sizeof(float2);
   return (b + 255) & ~size_t(255);
 }
+
+constexpr size_t kFactorTailBytes = 256;
+// Below this bound the reduced (separator) system is diagonal to far beneath
+// fp32 round-off and the team march skips its PCR levels.
+constexpr float kPcrSkipBound = 1e-12f;
 
 int partition_for(int n, Partition *pt);  // TP_OK or an error code
 
@@ -53,6 +60,7 @@ struct FactorParams {
   const void *n;
   char *factors;
   size_t slice_bytes;
+  unsigned *coupling;  // max |alpha|, |gamma| of the PCR records (float bits), atomically maxed
   int *err;
 };
 
@@ -75,6 +83,7 @@ struct MarchParams {
   float2 *u_store, *exit_out;
   const float2 *u_fwd;
   float2 *grad_c;
+  const unsigned *coupling;     // the factor set's PCR coupling bound (float bits), or NULL
   int *err;
   int t0, t1;                   // step range
   const float2 *state_in;       // chunked (P, Npad) or null

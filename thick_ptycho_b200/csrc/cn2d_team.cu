@@ -128,7 +128,8 @@ __device__ __forceinline__ void team_rhs(float2 (&U)[Q][M], const float2 *__rest
 // U <- M_s^{-1} U with the staged factor slice F.
 template <int M, int Q>
 __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__restrict__ F, int T, float2 *Y0,
-                                           float2 *R0, float2 *R1, float2 *XS, int c, int team, const Spec &sp) {
+                                           float2 *R0, float2 *R1, float2 *XS, int c, int team, const Spec &sp,
+                                           bool pcr) {
   constexpr int C = kTeamChunks;
   const float2 zero = make_float2(0.f, 0.f);
   const float2 *LF = F + M * C, *EP = F + 2 * M * C, *VH = F + 3 * M * C, *WT = VH + T * C, *LR = WT + T * C;
@@ -169,8 +170,11 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
       rho[q] = cfnma(mc, y0n, cfnma(ma, U[q][M - 2], U[q][M - 1]));
     }
   }
+  // PCR on the separators; skipped when the factorisation found every
+  // coupling coefficient below kPcrSkipBound (the reduced system is then
+  // diagonal to far beneath fp32 round-off: x = rho / rd)
 #pragma unroll
-  for (int l = 0; l < kTeamLevels; ++l) {
+  for (int l = 0; l < (pcr ? kTeamLevels : 0); ++l) {
     const int s = 1 << l;
     float2 *Rb = (l & 1) ? R1 : R0;
 #pragma unroll
@@ -231,6 +235,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
   uint64_t *mbar = reinterpret_cast<uint64_t *>(reinterpret_cast<float2 *>(smem + 2 * ss) + (size_t)TM * 6 * Q * C);
   const size_t ssf = ss / sizeof(float2);
   const int p0 = (blockIdx.x * TM + team) * Q;
+  const bool pcr = p.coupling == nullptr || __uint_as_float(__ldg(p.coupling)) >= kPcrSkipBound;
 
   if (tid == 0) {
     mbar_init(&mbar[0], 1);
@@ -331,7 +336,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
         for (int i = 0; i < M; ++i) U[q][i] = cadd(U[q][i], src[i]);
       }
     }
-    team_solve<M, Q>(U, F, T, Y0, R0, R1, XS, c, team, p.sp);
+    team_solve<M, Q>(U, F, T, Y0, R0, R1, XS, c, team, p.sp, pcr);
     if (p.u_store != nullptr && store_index(p, t) >= 0) {
       const int idx = store_index(p, t);
 #pragma unroll
