@@ -47,7 +47,6 @@ def test_pure_host_queries():
     assert npad.value >= 257 and npad.value == 32 * m.value
     assert lib.tp_cn2d_layout(4097, *args) != 0
     assert b"4097" in lib.tp_last_error_string()
-    # team slice: (5*16 + 17) * 128 * 8 bytes
     # 1023 slices of (5 M + 17 records) x 128 chunks float2, then a 256-byte tail (the PCR coupling bound)
     assert lib.tp_cn2d_factor_bytes(2048, 1024) == 1023 * (5 * 16 + 17) * 128 * 8 + 256
     assert lib.tp_cn2d_factor_bytes(2048, 1) == 0
