@@ -314,7 +314,19 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
         load_pairs<M>(u_new[q], p.u_fwd + ((size_t)pq * p.ufwd_slices + (s - 1 - p.ufwd_base)) * p.Npad, c);
       }
     }
-    if constexpr (!LAGGED) team_rhs<M, Q>(U, F, XL, XF, c, team, p.sp);
+    // Forward and reference-adjoint steps use the Cayley form of the step:
+    // with M = I - P, (I + P) = 2I - M commutes with M^{-1}, so
+    // M^{-1}((I + P) u + b) = 2 M^{-1}(u + b/2) - u.  The right-hand-side
+    // stencil and its neighbour exchange drop out; the step keeps u in
+    // registers and ends with one fused multiply-subtract per row.
+    float2 u_old[Q][M];
+    if constexpr (!LAGGED) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q)
+#pragma unroll
+        for (int i = 0; i < M; ++i) u_old[q][i] = U[q][i];
+    }
+    const float sw = LAGGED ? 1.f : 0.5f;  // source weight
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       if (p0 + q >= p.P) continue;
@@ -322,21 +334,28 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
       if (p.src_shared != nullptr) {
         const float2 *src = p.src_shared + (size_t)(t - 1) * p.N + g0;
 #pragma unroll
-        for (int i = 0; i < M; ++i) U[q][i] = cadd(U[q][i], src[i]);
+        for (int i = 0; i < M; ++i) U[q][i] = caxpy(sw, src[i], U[q][i]);
       }
       if (p.src_probe != nullptr) {
         const int col = p.src_rev ? (p.L - t) : (t - 1);
         const float2 *src = p.src_probe + ((size_t)(p0 + q) * p.L + col) * p.N + g0;
 #pragma unroll
-        for (int i = 0; i < M; ++i) U[q][i] = cadd(U[q][i], src[i]);
+        for (int i = 0; i < M; ++i) U[q][i] = caxpy(sw, src[i], U[q][i]);
       }
       if (t == 1 && p.src_exit != nullptr) {
         const float2 *src = p.src_exit + (size_t)(p0 + q) * p.N + g0;
 #pragma unroll
-        for (int i = 0; i < M; ++i) U[q][i] = cadd(U[q][i], src[i]);
+        for (int i = 0; i < M; ++i) U[q][i] = caxpy(sw, src[i], U[q][i]);
       }
     }
     team_solve<M, Q>(U, F, T, Y0, R0, R1, XS, c, team, p.sp, pcr);
+    if constexpr (!LAGGED) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q)
+#pragma unroll
+        for (int i = 0; i < M; ++i)
+          U[q][i] = make_float2(fmaf(2.f, U[q][i].x, -u_old[q][i].x), fmaf(2.f, U[q][i].y, -u_old[q][i].y));
+    }
     if (p.u_store != nullptr && store_index(p, t) >= 0) {
       const int idx = store_index(p, t);
 #pragma unroll

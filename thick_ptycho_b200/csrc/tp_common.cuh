@@ -28,6 +28,8 @@ __device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {
 __device__ __forceinline__ float2 cfnma(float2 a, float2 b, float2 c) {
   return c2(fmaf(-a.x, b.x, fmaf(a.y, b.y, c.x)), fmaf(-a.x, b.y, fmaf(-a.y, b.x, c.y)));
 }
+// s*a + c for real s
+__device__ __forceinline__ float2 caxpy(float s, float2 a, float2 c) { return c2(fmaf(s, a.x, c.x), fmaf(s, a.y, c.y)); }
 // a * conj(b)
 __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
   return c2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
