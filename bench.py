@@ -6,9 +6,10 @@ plus one adjoint CN step of one probe = one probe·slice), for the 2D batched
 workload N = 2048 transverse × Nz = 1024 nodes × 512 probes (stride 3 px),
 δn = 200 seeded Gaussian blobs + 1e-5 i, Gaussian probes (waist 8 px).
 One step = factorise (forward and adjoint) + forward march storing the full
-field + amplitude-loss residual + exact-adjoint march with the fused probe
-gradient + mapping onto the index nodes.  The full field (8.6 GB) is far
-larger than L2, so no explicit flush is needed between steps.
+field (as the pair sums u_s + u_{s-1} the gradient contracts with) +
+amplitude-loss residual + exact-adjoint march with the fused probe gradient +
+mapping onto the index nodes.  The full field (8.6 GB) is far larger than
+L2, so no explicit flush is needed between steps.
 
 The same line carries ``learned_vs_plain_3d``: forward + exact-adjoint
 probe·slice solves/s of the 3D BiCGStab march (256 x 256 x 256 nodes, 64
@@ -372,7 +373,7 @@ def run_ours(a):
         if record:
             e0 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-        eng.march(ff, P, probes=pr, u_store=store, exit_out=ex)
+        eng.march(ff, P, probes=pr, u_store=store, exit_out=ex, store_sums=True)
         if record:
             e1 = torch.cuda.Event(enable_timing=True)
             e1.record(stream)
@@ -382,7 +383,7 @@ def run_ours(a):
         if record:
             e2 = torch.cuda.Event(enable_timing=True)
             e2.record(stream)
-        eng.march(fa, P, src_exit=ge, u_fwd=store, grad_c=gc)
+        eng.march(fa, P, src_exit=ge, u_fwd=store, grad_c=gc, store_sums=True)
         if record:
             e3 = torch.cuda.Event(enable_timing=True)
             e3.record(stream)

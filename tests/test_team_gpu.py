@@ -98,3 +98,62 @@ def test_team_groups_of_four_with_partial_group_and_gradient():
     gref = sum(po.grad_c_from_adjoint(u_ref[p], lam[p]) for p in range(P))
     got = eng.unchunk_rows(gc).cpu().numpy().T
     assert rel(got, gref) < GRAD_TOL, rel(got, gref)
+
+
+def test_team_pair_sums_store_and_cayley_adjoint():
+    """store_sums: the forward store holds u_t + u_{t-1}; the exact adjoint
+    reading those sums (one slice per step, Cayley-form step) gives the same
+    lambda and gradient as the two-slice form and as the oracle."""
+    from thick_ptycho_b200._native import NativeLibraryError
+
+    N, nz, P = 1024, 24, 9
+    n = _field(N, nz, 11)
+    probes = _probes(N, P, 12)
+    eng = CN2D(N, nz, K, DX, DZ, "impedance")
+    co = po.bc_coefficients(K, DX, DZ, bc_type="impedance")
+    A, B = po.step_matrices_1d(N, co, "impedance", DZ)
+    C = po.object_contribution(n, K, DZ)
+    field = torch.from_numpy(n).cuda()
+    pr = torch.from_numpy(probes.astype(np.complex64)).cuda()
+    ff = eng.factor(field, "forward")
+    st, sums = eng.new_store(P), eng.new_store(P)
+    eng.march(ff, P, probes=pr, u_store=st)
+    eng.march(ff, P, probes=pr, u_store=sums, store_sums=True)
+    eng.device_status()
+    u = eng.unchunk(st).cpu().numpy()
+    w = eng.unchunk(sums).cpu().numpy()
+    assert rel(w[:, :, 1:], u[:, :, 1:] + u[:, :, :-1]) < 1e-6
+    rng = np.random.default_rng(13)
+    e = torch.from_numpy((rng.standard_normal((P, N)) + 1j * rng.standard_normal((P, N))).astype(np.complex64)).cuda()
+    fa = eng.factor(field, "adjoint_exact")
+    g1, g2 = eng.new_grad_buffer(), eng.new_grad_buffer()
+    s1 = torch.empty((P, eng.npad), dtype=torch.complex64, device="cuda")
+    s2 = torch.empty_like(s1)
+    eng.march(fa, P, src_exit=e, u_fwd=st, grad_c=g1, state_out=s1)
+    eng.march(fa, P, src_exit=e, u_fwd=sums, grad_c=g2, state_out=s2, store_sums=True)
+    eng.device_status()
+    assert rel(s2.cpu().numpy(), s1.cpu().numpy()) < TOL
+    got = eng.unchunk_rows(g2).cpu().numpy().T
+    assert rel(got, eng.unchunk_rows(g1).cpu().numpy().T) < TOL
+    lus, Bs = po.build_lu_factors(A, B, C)
+    u_ref = np.array([po.march_with_lu(lus, Bs, np.zeros(N, complex), probes[p]) for p in range(P)])
+    srcs = np.zeros((P, N, nz - 1), dtype=complex)
+    srcs[:, :, -1] = e.cpu().numpy()
+    lam = po.exact_adjoint_many(A, B, C, srcs)
+    gref = sum(po.grad_c_from_adjoint(u_ref[p], lam[p]) for p in range(P))
+    assert rel(got, gref) < GRAD_TOL, rel(got, gref)
+    # exact adjoint without a gradient (Cayley step): the stored lambda
+    # (index t holds slice L+1-t) against the oracle
+    lam_st = eng.new_store(P)
+    eng.march(fa, P, src_exit=e, u_store=lam_st)
+    eng.device_status()
+    lg = eng.unchunk(lam_st).cpu().numpy()
+    for p in range(P):
+        assert rel(lg[p][:, 1:][:, ::-1], lam[p]) < TOL, (p, rel(lg[p][:, 1:][:, ::-1], lam[p]))
+    # checkpoint stores keep states; the warp path (N = 256) has no pair sums
+    with pytest.raises(NativeLibraryError):
+        eng.march(ff, P, probes=pr, u_store=eng.new_store(P, 4), store_every=8, store_sums=True)
+    small = CN2D(256, nz, K, DX, DZ, "impedance")
+    with pytest.raises(NativeLibraryError):
+        small.march(small.factor(torch.from_numpy(n[:256]).cuda(), "forward"), 1, u_store=small.new_store(1),
+                    store_sums=True)

@@ -73,7 +73,7 @@ class TpCn2dMarchArgs(ctypes.Structure):
         ("store_base", ctypes.c_int32),
         ("ufwd_slices", ctypes.c_int32),
         ("ufwd_base", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("store_sums", ctypes.c_int32),
     ]
 
 

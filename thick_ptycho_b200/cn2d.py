@@ -115,6 +115,7 @@ class CN2D:
         store_every: int = 0,
         store_base: int = 0,
         ufwd_base: int = 0,
+        store_sums: bool = False,
     ):
         """One batched march; every tensor is complex64, contiguous, on device.
 
@@ -123,7 +124,10 @@ class CN2D:
         ``store_every > 1``, only for multiples).  ``u_fwd`` is (≥P, S', Npad)
         with forward slice s at index ``s − ufwd_base``.  ``t_begin..t_end``
         restricts the steps; ``state_in``/``state_out`` (P, Npad) carry the
-        state across partial marches.
+        state across partial marches.  ``store_sums`` (team path, N in
+        {512, 1024, 2048}): a forward march stores ``u_t + u_{t−1}`` (what the
+        exact-adjoint gradient contracts with) instead of ``u_t``, and an
+        exact-adjoint march reads ``u_fwd`` as those sums.
         """
         P = int(num_probes)
         shapes = {
@@ -159,6 +163,7 @@ class CN2D:
         a.store_every, a.store_base = int(store_every), int(store_base)
         a.ufwd_slices = 0 if u_fwd is None else int(u_fwd.shape[1])
         a.ufwd_base = int(ufwd_base)
+        a.store_sums = 1 if store_sums else 0
         o = self.op()
         rc = self.lib.tp_cn2d_march(ctypes.byref(o), _ptr(fs.buf), ctypes.byref(a), _stream(self.device))
         _native.check(rc, "tp_cn2d_march")

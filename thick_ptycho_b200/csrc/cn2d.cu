@@ -783,6 +783,16 @@ extern "C" int tp_cn2d_march(const tp_cn2d_op *op, const void *factors, const tp
   mp.store_base = a->store_base;
   mp.ufwd_slices = a->ufwd_slices > 0 ? a->ufwd_slices : op->nz;
   mp.ufwd_base = a->ufwd_base;
+  mp.store_sums = a->store_sums;
+  if (a->store_sums != 0) {
+    if (a->store_sums != 1) return set_error(TP_ERR_INVALID, "store_sums=%d (0 or 1)", a->store_sums);
+    if (a->mode != TP_MODE_FORWARD && a->mode != TP_MODE_ADJOINT_EXACT)
+      return set_error(TP_ERR_INVALID, "store_sums needs mode FORWARD or ADJOINT_EXACT");
+    if (a->mode == TP_MODE_FORWARD && a->store_every > 1)
+      return set_error(TP_ERR_INVALID, "store_sums cannot keep checkpoints (store_every=%d)", a->store_every);
+    if (!pt.team)
+      return set_error(TP_ERR_UNSUPPORTED, "store_sums needs the team path (N in {512, 1024, 2048}), N=%d", op->n);
+  }
   if (pt.team) {
     if (op->k_off[0] != 0.0 || op->k_01[0] != 0.0 || op->k_nm[0] != 0.0)
       return set_error(TP_ERR_UNSUPPORTED,

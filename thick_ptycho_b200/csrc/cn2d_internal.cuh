@@ -90,6 +90,7 @@ struct MarchParams {
   float2 *state_out;
   int store_slices, store_every, store_base;
   int ufwd_slices, ufwd_base;
+  int store_sums;               // FORWARD: u_store gets u_t + u_{t-1}; ADJOINT_EXACT: u_fwd holds them
 };
 
 // Index in u_store of the state after step t (t0-1 = the initial state), or -1.

@@ -52,6 +52,14 @@ __device__ __forceinline__ void store_pairs(float2 *dst, const float2 *U, int M,
   for (int j = 0; j < M / 2; ++j)
     reinterpret_cast<float4 *>(dst)[j * kTeamChunks + c] = make_float4(U[2 * j].x, U[2 * j].y, U[2 * j + 1].x, U[2 * j + 1].y);
 }
+// Same layout, storing U + V (the pair sum u_t + u_{t-1} of the gradient).
+__device__ __forceinline__ void store_pair_sums(float2 *dst, const float2 *U, const float2 *V, int M, int c) {
+#pragma unroll 8
+  for (int j = 0; j < M / 2; ++j) {
+    const float2 a = cadd(U[2 * j], V[2 * j]), b = cadd(U[2 * j + 1], V[2 * j + 1]);
+    reinterpret_cast<float4 *>(dst)[j * kTeamChunks + c] = make_float4(a.x, a.y, b.x, b.y);
+  }
+}
 
 // Load thread c's M rows of one stored slice (row pairs).
 template <int M>
@@ -218,8 +226,14 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
   for (int q = 0; q < Q; ++q) U[q][M - 1] = x[q];
 }
 
-template <int M, int Q, int TM, bool LAGGED>
+// LAGGED: exact-adjoint order (solve, gradient, then the right-hand side of
+// the same slice).  SUMS (LAGGED only): that step in Cayley form, with u_fwd
+// (when given) holding the pair sums u_s + u_{s-1} written by a forward march
+// with store_sums, so one forward slice is read per step and the registers of
+// the second serve the Cayley step.
+template <int M, int Q, int TM, bool LAGGED, bool SUMS>
 __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const MarchParams p) {
+  static_assert(LAGGED || !SUMS, "SUMS selects the exact-adjoint Cayley step");
   constexpr int C = kTeamChunks;
   constexpr int NT = kTeamThreads * TM;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -266,7 +280,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
       for (int i = 0; i < M; ++i) U[q][i] = src[i];
     }
   }
-  if (p.u_store != nullptr && store_index(p, p.t0 - 1) >= 0) {
+  if (p.u_store != nullptr && !p.store_sums && store_index(p, p.t0 - 1) >= 0) {
     const int idx = store_index(p, p.t0 - 1);
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
@@ -277,9 +291,10 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
 
   // Gradient: the forward slice u_s of the current step is kept from the
   // previous step (u_prev); only u_{s-1} is read, issued at the start of the
-  // step so that its latency overlaps the solve.
+  // step so that its latency overlaps the solve.  With SUMS the one slice
+  // read is the pair sum itself.
   float2 u_prev[Q][M], u_new[Q][M];
-  if (do_grad) {
+  if (do_grad && !SUMS) {
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       const int pq = (p0 + q < p.P) ? p0 + q : p.P - 1;
@@ -311,14 +326,17 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         const int pq = (p0 + q < p.P) ? p0 + q : p.P - 1;
-        load_pairs<M>(u_new[q], p.u_fwd + ((size_t)pq * p.ufwd_slices + (s - 1 - p.ufwd_base)) * p.Npad, c);
+        const int ix = SUMS ? s - p.ufwd_base : s - 1 - p.ufwd_base;
+        load_pairs<M>(u_new[q], p.u_fwd + ((size_t)pq * p.ufwd_slices + ix) * p.Npad, c);
       }
     }
     // Forward and reference-adjoint steps use the Cayley form of the step:
     // with M = I - P, (I + P) = 2I - M commutes with M^{-1}, so
     // M^{-1}((I + P) u + b) = 2 M^{-1}(u + b/2) - u.  The right-hand-side
     // stencil and its neighbour exchange drop out; the step keeps u in
-    // registers and ends with one fused multiply-subtract per row.
+    // registers and ends with one fused multiply-subtract per row.  The
+    // exact-adjoint step (I + P) M^{-1} v = 2 M^{-1} v - v (SUMS) keeps the
+    // solve's input v = u + b instead.
     float2 u_old[Q][M];
     if constexpr (!LAGGED) {
 #pragma unroll
@@ -348,6 +366,12 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
         for (int i = 0; i < M; ++i) U[q][i] = caxpy(sw, src[i], U[q][i]);
       }
     }
+    if constexpr (SUMS) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q)
+#pragma unroll
+        for (int i = 0; i < M; ++i) u_old[q][i] = U[q][i];
+    }
     team_solve<M, Q>(U, F, T, Y0, R0, R1, XS, c, team, p.sp, pcr);
     if constexpr (!LAGGED) {
 #pragma unroll
@@ -361,7 +385,9 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         if (p0 + q >= p.P) continue;
-        store_pairs(p.u_store + ((size_t)(p0 + q) * p.store_slices + idx) * p.Npad, U[q], M, c);
+        float2 *dst = p.u_store + ((size_t)(p0 + q) * p.store_slices + idx) * p.Npad;
+        if (!LAGGED && p.store_sums) store_pair_sums(dst, U[q], u_old[q], M, c);
+        else store_pairs(dst, U[q], M, c);
       }
     }
     if (t == p.L && p.exit_out != nullptr) {
@@ -381,8 +407,10 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
           if (p0 + q >= p.P) continue;  // padded probes contribute nothing
-          const float2 a = cmulc(U[q][2 * j], cadd(u_prev[q][2 * j], u_new[q][2 * j]));
-          const float2 b = cmulc(U[q][2 * j + 1], cadd(u_prev[q][2 * j + 1], u_new[q][2 * j + 1]));
+          const float2 wa = SUMS ? u_new[q][2 * j] : cadd(u_prev[q][2 * j], u_new[q][2 * j]);
+          const float2 wb = SUMS ? u_new[q][2 * j + 1] : cadd(u_prev[q][2 * j + 1], u_new[q][2 * j + 1]);
+          const float2 a = cmulc(U[q][2 * j], wa);
+          const float2 b = cmulc(U[q][2 * j + 1], wb);
           acc.x += a.x;
           acc.y += a.y;
           acc.z += b.x;
@@ -390,12 +418,22 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
         }
         red_add_v4(gdst + j * C, acc);
       }
+      if constexpr (!SUMS) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+#pragma unroll
+          for (int i = 0; i < M; ++i) u_prev[q][i] = u_new[q][i];
+      }
+    }
+    if constexpr (SUMS) {
 #pragma unroll
       for (int q = 0; q < Q; ++q)
 #pragma unroll
-        for (int i = 0; i < M; ++i) u_prev[q][i] = u_new[q][i];
+        for (int i = 0; i < M; ++i)
+          U[q][i] = make_float2(fmaf(2.f, U[q][i].x, -u_old[q][i].x), fmaf(2.f, U[q][i].y, -u_old[q][i].y));
+    } else if constexpr (LAGGED) {
+      team_rhs<M, Q>(U, F, XL, XF, c, team, p.sp);
     }
-    if constexpr (LAGGED) team_rhs<M, Q>(U, F, XL, XF, c, team, p.sp);
     bool good = true;
     if (t < p.t1) {
       good = mbar_wait_bounded(&mbar[cb ^ 1], (phase >> (cb ^ 1)) & 1u, p.err);
@@ -416,9 +454,9 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
   }
 }
 
-template <int M, int Q, int TM, bool LAGGED>
+template <int M, int Q, int TM, bool LAGGED, bool SUMS>
 static int launch_team_t(const Partition &pt, MarchParams &mp, cudaStream_t st) {
-  auto kern = cn2d_team_kernel<M, Q, TM, LAGGED>;
+  auto kern = cn2d_team_kernel<M, Q, TM, LAGGED, SUMS>;
   const bool grad = LAGGED && mp.grad_c != nullptr;
   const size_t smem = team_smem_bytes(pt, mp.trunc, Q, TM, grad);
   TP_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -427,15 +465,15 @@ static int launch_team_t(const Partition &pt, MarchParams &mp, cudaStream_t st) 
   return check_cuda(cudaGetLastError(), "cn2d_team_kernel launch");
 }
 
-template <int M, bool LAGGED>
+template <int M, bool LAGGED, bool SUMS>
 static int launch_team_qt(const Partition &pt, MarchParams &mp, int Q, int TM, cudaStream_t st) {
-  if (TM == 1 && Q == 1) return launch_team_t<M, 1, 1, LAGGED>(pt, mp, st);
-  if (TM == 2 && Q == 1) return launch_team_t<M, 1, 2, LAGGED>(pt, mp, st);
-  if (TM == 4 && Q == 1) return launch_team_t<M, 1, 4, LAGGED>(pt, mp, st);
+  if (TM == 1 && Q == 1) return launch_team_t<M, 1, 1, LAGGED, SUMS>(pt, mp, st);
+  if (TM == 2 && Q == 1) return launch_team_t<M, 1, 2, LAGGED, SUMS>(pt, mp, st);
+  if (TM == 4 && Q == 1) return launch_team_t<M, 1, 4, LAGGED, SUMS>(pt, mp, st);
   if constexpr (!LAGGED) {
-    if (TM == 1 && Q == 4) return launch_team_t<M, 4, 1, LAGGED>(pt, mp, st);
-    if (TM == 1 && Q == 2) return launch_team_t<M, 2, 1, LAGGED>(pt, mp, st);
-    if (TM == 2 && Q == 2) return launch_team_t<M, 2, 2, LAGGED>(pt, mp, st);
+    if (TM == 1 && Q == 4) return launch_team_t<M, 4, 1, LAGGED, SUMS>(pt, mp, st);
+    if (TM == 1 && Q == 2) return launch_team_t<M, 2, 1, LAGGED, SUMS>(pt, mp, st);
+    if (TM == 2 && Q == 2) return launch_team_t<M, 2, 2, LAGGED, SUMS>(pt, mp, st);
   }
   return set_error(TP_ERR_UNSUPPORTED, "no team kernel for Q=%d, TM=%d", Q, TM);
 }
@@ -483,13 +521,22 @@ int launch_team_march(const Partition &pt, MarchParams &mp, bool lagged, cudaStr
   if (team_smem_bytes(pt, mp.trunc, Q, TM, grad) > (size_t)max_smem)
     return set_error(TP_ERR_UNSUPPORTED, "team march needs %zu B of shared memory (> %d)",
                      team_smem_bytes(pt, mp.trunc, Q, TM, grad), max_smem);
+  // Exact adjoint in Cayley form unless a gradient reads plain forward slices
+  // (two per step: not enough registers for the Cayley state as well).
+  const bool sums = lagged && (mp.u_fwd == nullptr || mp.store_sums);
   switch (pt.M) {
     case 4:
-      return lagged ? launch_team_qt<4, true>(pt, mp, Q, TM, st) : launch_team_qt<4, false>(pt, mp, Q, TM, st);
+      return !lagged ? launch_team_qt<4, false, false>(pt, mp, Q, TM, st)
+             : sums  ? launch_team_qt<4, true, true>(pt, mp, Q, TM, st)
+                     : launch_team_qt<4, true, false>(pt, mp, Q, TM, st);
     case 8:
-      return lagged ? launch_team_qt<8, true>(pt, mp, Q, TM, st) : launch_team_qt<8, false>(pt, mp, Q, TM, st);
+      return !lagged ? launch_team_qt<8, false, false>(pt, mp, Q, TM, st)
+             : sums  ? launch_team_qt<8, true, true>(pt, mp, Q, TM, st)
+                     : launch_team_qt<8, true, false>(pt, mp, Q, TM, st);
     case 16:
-      return lagged ? launch_team_qt<16, true>(pt, mp, Q, TM, st) : launch_team_qt<16, false>(pt, mp, Q, TM, st);
+      return !lagged ? launch_team_qt<16, false, false>(pt, mp, Q, TM, st)
+             : sums  ? launch_team_qt<16, true, true>(pt, mp, Q, TM, st)
+                     : launch_team_qt<16, true, false>(pt, mp, Q, TM, st);
     default:
       return set_error(TP_ERR_UNSUPPORTED, "no team kernel for %d rows per chunk", pt.M);
   }

@@ -67,6 +67,9 @@ class PWEGradient2D:
             self.ckpt = int(checkpoint)
         if self.ckpt >= L:
             self.ckpt = 0
+        # team path: the kept field holds the pair sums u_s + u_{s-1}, so the
+        # exact-adjoint march reads one slice per step and runs in Cayley form
+        self.sums = self.engine.chunks == 128
         self._ff = self.engine.new_factor_buffer()
         self._fa = self.engine.new_factor_buffer()
         self._bufs = {}
@@ -93,7 +96,7 @@ class PWEGradient2D:
         fs = e.factor(field, "forward", is_delta, out=self._ff)
         ex = exit_out if exit_out is not None else torch.empty((P, e.n), dtype=torch.complex64, device=self.device)
         if not self.ckpt:
-            e.march(fs, P, probes=probes, u_store=self._buf("full", P, e.nz), exit_out=ex)
+            e.march(fs, P, probes=probes, u_store=self._buf("full", P, e.nz), exit_out=ex, store_sums=self.sums)
         else:
             ck = self._buf("ckpt", P, e.L // self.ckpt + 1)
             e.march(fs, P, probes=probes, u_store=ck, store_every=self.ckpt, exit_out=ex)
@@ -112,7 +115,8 @@ class PWEGradient2D:
         self._grad_c.zero_()
         src = exit_grad.contiguous()
         if not self.ckpt:
-            e.march(fa, P, src_exit=src, u_fwd=self._buf("full", P, e.nz), grad_c=self._grad_c)
+            e.march(fa, P, src_exit=src, u_fwd=self._buf("full", P, e.nz), grad_c=self._grad_c,
+                    store_sums=self.sums)
         else:
             S, L = self.ckpt, e.L
             ck = self._bufs["ckpt"]
@@ -125,11 +129,12 @@ class PWEGradient2D:
                 a, b = k * S, min(k * S + S, L)
                 start.copy_(ck[:, a // S])
                 # recompute u_a .. u_b of this segment (indices 0 .. b - a)
-                e.march(self._fs_fwd, P, t_begin=a + 1, t_end=b, state_in=start, u_store=seg, store_base=a)
+                e.march(self._fs_fwd, P, t_begin=a + 1, t_end=b, state_in=start, u_store=seg, store_base=a,
+                        store_sums=self.sums)
                 # adjoint steps for slices b .. a+1 (step t = L + 1 - s)
                 e.march(fa, P, t_begin=L + 1 - b, t_end=L - a, src_exit=src if first else None,
                         state_in=None if first else state[0], state_out=state[1], u_fwd=seg, ufwd_base=a,
-                        grad_c=self._grad_c)
+                        grad_c=self._grad_c, store_sums=self.sums)
                 state.reverse()
                 first = False
         return e.grad_to_n(self._grad_c, field if e.exact_ref_coeff else None, is_delta)
