@@ -6,7 +6,7 @@ plus one adjoint CN step of one probe = one probe·slice), for the 2D batched
 workload N = 2048 transverse × Nz = 1024 nodes × 512 probes (stride 3 px),
 δn = 200 seeded Gaussian blobs + 1e-5 i, Gaussian probes (waist 8 px).
 One step = factorise (forward and adjoint) + forward march storing the full
-field (as the pair sums u_s + u_{s-1} the gradient contracts with) +
+field (as the half pair sums (u_s + u_{s-1})/2 the gradient contracts with) +
 amplitude-loss residual + exact-adjoint march with the fused probe gradient +
 mapping onto the index nodes.  The full field (8.6 GB) is far larger than
 L2, so no explicit flush is needed between steps.

@@ -119,11 +119,11 @@ typedef struct tp_cn2d_march_args {
   int32_t ufwd_slices;       /* slices per probe in u_fwd (0 = nz)             */
   int32_t ufwd_base;         /* u_fwd index of forward slice s is s - ufwd_base */
   int32_t store_sums;        /* 0, or 1 (N in {512, 1024, 2048} only): FORWARD
-                                stores the pair sums u_t + u_{t-1} the gradient
-                                needs instead of u_t (the initial state is not
-                                stored; needs store_every <= 1); ADJOINT_EXACT
-                                reads u_fwd as such sums (one slice per step
-                                instead of two)                               */
+                                stores the half pair sums (u_t + u_{t-1})/2 the
+                                gradient contracts with instead of u_t (the
+                                initial state is not stored; needs
+                                store_every <= 1); ADJOINT_EXACT reads u_fwd as
+                                such sums (one slice per step instead of two) */
 } tp_cn2d_march_args;
 
 /* Partition of N rows into `chunks` chunks of `rows_per_chunk` rows (padded

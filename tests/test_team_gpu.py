@@ -101,7 +101,7 @@ def test_team_groups_of_four_with_partial_group_and_gradient():
 
 
 def test_team_pair_sums_store_and_cayley_adjoint():
-    """store_sums: the forward store holds u_t + u_{t-1}; the exact adjoint
+    """store_sums: the forward store holds (u_t + u_{t-1})/2; the exact adjoint
     reading those sums (one slice per step, Cayley-form step) gives the same
     lambda and gradient as the two-slice form and as the oracle."""
     from thick_ptycho_b200._native import NativeLibraryError
@@ -122,7 +122,7 @@ def test_team_pair_sums_store_and_cayley_adjoint():
     eng.device_status()
     u = eng.unchunk(st).cpu().numpy()
     w = eng.unchunk(sums).cpu().numpy()
-    assert rel(w[:, :, 1:], u[:, :, 1:] + u[:, :, :-1]) < 1e-6
+    assert rel(w[:, :, 1:], 0.5 * (u[:, :, 1:] + u[:, :, :-1])) < 1e-6
     rng = np.random.default_rng(13)
     e = torch.from_numpy((rng.standard_normal((P, N)) + 1j * rng.standard_normal((P, N))).astype(np.complex64)).cuda()
     fa = eng.factor(field, "adjoint_exact")

@@ -125,9 +125,10 @@ class CN2D:
         with forward slice s at index ``s − ufwd_base``.  ``t_begin..t_end``
         restricts the steps; ``state_in``/``state_out`` (P, Npad) carry the
         state across partial marches.  ``store_sums`` (team path, N in
-        {512, 1024, 2048}): a forward march stores ``u_t + u_{t−1}`` (what the
-        exact-adjoint gradient contracts with) instead of ``u_t``, and an
-        exact-adjoint march reads ``u_fwd`` as those sums.
+        {512, 1024, 2048}): a forward march stores ``(u_t + u_{t−1})/2`` (the
+        exact-adjoint gradient contracts with the pair sum; the half sum is
+        the Cayley step's solve result, stored at no extra cost) instead of
+        ``u_t``, and an exact-adjoint march reads ``u_fwd`` as those.
         """
         P = int(num_probes)
         shapes = {

@@ -52,14 +52,6 @@ __device__ __forceinline__ void store_pairs(float2 *dst, const float2 *U, int M,
   for (int j = 0; j < M / 2; ++j)
     reinterpret_cast<float4 *>(dst)[j * kTeamChunks + c] = make_float4(U[2 * j].x, U[2 * j].y, U[2 * j + 1].x, U[2 * j + 1].y);
 }
-// Same layout, storing U + V (the pair sum u_t + u_{t-1} of the gradient).
-__device__ __forceinline__ void store_pair_sums(float2 *dst, const float2 *U, const float2 *V, int M, int c) {
-#pragma unroll 8
-  for (int j = 0; j < M / 2; ++j) {
-    const float2 a = cadd(U[2 * j], V[2 * j]), b = cadd(U[2 * j + 1], V[2 * j + 1]);
-    reinterpret_cast<float4 *>(dst)[j * kTeamChunks + c] = make_float4(a.x, a.y, b.x, b.y);
-  }
-}
 
 // Load thread c's M rows of one stored slice (row pairs).
 template <int M>
@@ -228,9 +220,9 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
 
 // LAGGED: exact-adjoint order (solve, gradient, then the right-hand side of
 // the same slice).  SUMS (LAGGED only): that step in Cayley form, with u_fwd
-// (when given) holding the pair sums u_s + u_{s-1} written by a forward march
-// with store_sums, so one forward slice is read per step and the registers of
-// the second serve the Cayley step.
+// (when given) holding the half pair sums (u_s + u_{s-1})/2 written by a
+// forward march with store_sums, so one forward slice is read per step and
+// the registers of the second serve the Cayley step.
 template <int M, int Q, int TM, bool LAGGED, bool SUMS>
 __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const MarchParams p) {
   static_assert(LAGGED || !SUMS, "SUMS selects the exact-adjoint Cayley step");
@@ -336,7 +328,9 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
     // stencil and its neighbour exchange drop out; the step keeps u in
     // registers and ends with one fused multiply-subtract per row.  The
     // exact-adjoint step (I + P) M^{-1} v = 2 M^{-1} v - v (SUMS) keeps the
-    // solve's input v = u + b instead.
+    // solve's input v = u + b instead.  In the forward step the solve result
+    // x = M^{-1}(u_{t-1} + b/2) is exactly (u_t + u_{t-1})/2, the half pair
+    // sum the gradient contracts with: store_sums stores x itself.
     float2 u_old[Q][M];
     if constexpr (!LAGGED) {
 #pragma unroll
@@ -373,21 +367,26 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
         for (int i = 0; i < M; ++i) u_old[q][i] = U[q][i];
     }
     team_solve<M, Q>(U, F, T, Y0, R0, R1, XS, c, team, p.sp, pcr);
+    const int sidx = p.u_store != nullptr ? store_index(p, t) : -1;
     if constexpr (!LAGGED) {
+      if (p.store_sums && sidx >= 0) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+          if (p0 + q >= p.P) continue;
+          store_pairs(p.u_store + ((size_t)(p0 + q) * p.store_slices + sidx) * p.Npad, U[q], M, c);
+        }
+      }
 #pragma unroll
       for (int q = 0; q < Q; ++q)
 #pragma unroll
         for (int i = 0; i < M; ++i)
           U[q][i] = make_float2(fmaf(2.f, U[q][i].x, -u_old[q][i].x), fmaf(2.f, U[q][i].y, -u_old[q][i].y));
     }
-    if (p.u_store != nullptr && store_index(p, t) >= 0) {
-      const int idx = store_index(p, t);
+    if (sidx >= 0 && (LAGGED || !p.store_sums)) {
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         if (p0 + q >= p.P) continue;
-        float2 *dst = p.u_store + ((size_t)(p0 + q) * p.store_slices + idx) * p.Npad;
-        if (!LAGGED && p.store_sums) store_pair_sums(dst, U[q], u_old[q], M, c);
-        else store_pairs(dst, U[q], M, c);
+        store_pairs(p.u_store + ((size_t)(p0 + q) * p.store_slices + sidx) * p.Npad, U[q], M, c);
       }
     }
     if (t == p.L && p.exit_out != nullptr) {
@@ -416,6 +415,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
           acc.z += b.x;
           acc.w += b.y;
         }
+        if constexpr (SUMS) acc = make_float4(2.f * acc.x, 2.f * acc.y, 2.f * acc.z, 2.f * acc.w);  // half sums
         red_add_v4(gdst + j * C, acc);
       }
       if constexpr (!SUMS) {
@@ -478,20 +478,15 @@ static int launch_team_qt(const Partition &pt, MarchParams &mp, int Q, int TM, c
   return set_error(TP_ERR_UNSUPPORTED, "no team kernel for Q=%d, TM=%d", Q, TM);
 }
 
-// (teams per CTA, probes per thread) for K probes per CTA.
+// (teams per CTA, probes per thread) for K probes per CTA: one probe per
+// thread (K teams) unless overridden.  With the Cayley step 4 teams x 1 probe
+// time 2.75 ms per forward march at N = 2048 x 1023 slices x 512 probes
+// against 2.84 ms for 2 x 2.
 static void team_shape(int K, int *TM, int *Q) {
   const char *env = getenv("TPCUDA_TEAM_SHAPE");  // "TM,Q" override for tuning sweeps
   if (env != nullptr && sscanf(env, "%d,%d", TM, Q) == 2 && *TM * *Q == K) return;
-  if (K >= 4) {
-    *TM = 2;
-    *Q = 2;
-  } else if (K == 2) {
-    *TM = 2;
-    *Q = 1;
-  } else {
-    *TM = 1;
-    *Q = 1;
-  }
+  *TM = K;
+  *Q = 1;
 }
 
 int launch_team_march(const Partition &pt, MarchParams &mp, bool lagged, cudaStream_t st) {

@@ -67,7 +67,7 @@ class PWEGradient2D:
             self.ckpt = int(checkpoint)
         if self.ckpt >= L:
             self.ckpt = 0
-        # team path: the kept field holds the pair sums u_s + u_{s-1}, so the
+        # team path: the kept field holds the half pair sums (u_s + u_{s-1})/2, so the
         # exact-adjoint march reads one slice per step and runs in Cayley form
         self.sums = self.engine.chunks == 128
         self._ff = self.engine.new_factor_buffer()
