@@ -125,9 +125,10 @@ __device__ __forceinline__ void team_rhs(float2 (&U)[Q][M], const float2 *__rest
   }
 }
 
-// U <- M_s^{-1} U with the staged factor slice F.
-template <int M, int Q>
-__device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__restrict__ F, int T, float2 *Y0,
+// U <- M_s^{-1} U with the staged factor slice F (T spike rows staged: a
+// compile-time count, so the spike corrections touch only those rows).
+template <int M, int Q, int T>
+__device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__restrict__ F, float2 *Y0,
                                            float2 *R0, float2 *R1, float2 *XS, int c, int team, const Spec &sp,
                                            bool pcr) {
   constexpr int C = kTeamChunks;
@@ -200,7 +201,7 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
   team_sync(team);
 #pragma unroll
   for (int q = 0; q < Q; ++q) xp[q] = (c > 0) ? XS[q * C + c - 1] : zero;
-  const int wlo = M - 1 - T;
+  constexpr int wlo = M - 1 - T;
 #pragma unroll
   for (int i = 0; i <= M - 2; ++i) {
     if (i < T) {
@@ -218,12 +219,13 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
   for (int q = 0; q < Q; ++q) U[q][M - 1] = x[q];
 }
 
-// LAGGED: exact-adjoint order (solve, gradient, then the right-hand side of
-// the same slice).  SUMS (LAGGED only): that step in Cayley form, with u_fwd
+// TS: spike rows staged per slice (>= the rows the factorisation found
+// significant).  LAGGED: exact-adjoint order (solve, gradient, then the
+// right-hand side of the same slice).  SUMS (LAGGED only): that step in Cayley form, with u_fwd
 // (when given) holding the half pair sums (u_s + u_{s-1})/2 written by a
 // forward march with store_sums, so one forward slice is read per step and
 // the registers of the second serve the Cayley step.
-template <int M, int Q, int TM, bool LAGGED, bool SUMS>
+template <int M, int Q, int TM, bool LAGGED, bool SUMS, int TS>
 __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const MarchParams p) {
   static_assert(LAGGED || !SUMS, "SUMS selects the exact-adjoint Cayley step");
   constexpr int C = kTeamChunks;
@@ -232,7 +234,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
   const int tid = threadIdx.x;
   const int team = tid / kTeamThreads;
   const int c = tid % kTeamThreads;
-  const int T = p.trunc;
+  constexpr int T = TS;  // the host sets p.trunc = TS
   const size_t ss = p.smem_slice_bytes;
   float2 *bufs = reinterpret_cast<float2 *>(smem);
   float2 *XL = reinterpret_cast<float2 *>(smem + 2 * ss) + (size_t)team * 6 * Q * C;
@@ -366,7 +368,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
 #pragma unroll
         for (int i = 0; i < M; ++i) u_old[q][i] = U[q][i];
     }
-    team_solve<M, Q>(U, F, T, Y0, R0, R1, XS, c, team, p.sp, pcr);
+    team_solve<M, Q, T>(U, F, Y0, R0, R1, XS, c, team, p.sp, pcr);
     const int sidx = p.u_store != nullptr ? store_index(p, t) : -1;
     if constexpr (!LAGGED) {
       if (p.store_sums && sidx >= 0) {
@@ -454,9 +456,10 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
   }
 }
 
-template <int M, int Q, int TM, bool LAGGED, bool SUMS>
+template <int M, int Q, int TM, bool LAGGED, bool SUMS, int TS>
 static int launch_team_t(const Partition &pt, MarchParams &mp, cudaStream_t st) {
-  auto kern = cn2d_team_kernel<M, Q, TM, LAGGED, SUMS>;
+  auto kern = cn2d_team_kernel<M, Q, TM, LAGGED, SUMS, TS>;
+  if (mp.trunc != TS) return set_error(TP_ERR_INVALID, "team march staged %d spike rows, kernel has %d", mp.trunc, TS);
   const bool grad = LAGGED && mp.grad_c != nullptr;
   const size_t smem = team_smem_bytes(pt, mp.trunc, Q, TM, grad);
   TP_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -465,17 +468,25 @@ static int launch_team_t(const Partition &pt, MarchParams &mp, cudaStream_t st) 
   return check_cuda(cudaGetLastError(), "cn2d_team_kernel launch");
 }
 
-template <int M, bool LAGGED, bool SUMS>
+template <int M, bool LAGGED, bool SUMS, int TS>
 static int launch_team_qt(const Partition &pt, MarchParams &mp, int Q, int TM, cudaStream_t st) {
-  if (TM == 1 && Q == 1) return launch_team_t<M, 1, 1, LAGGED, SUMS>(pt, mp, st);
-  if (TM == 2 && Q == 1) return launch_team_t<M, 1, 2, LAGGED, SUMS>(pt, mp, st);
-  if (TM == 4 && Q == 1) return launch_team_t<M, 1, 4, LAGGED, SUMS>(pt, mp, st);
+  if (TM == 1 && Q == 1) return launch_team_t<M, 1, 1, LAGGED, SUMS, TS>(pt, mp, st);
+  if (TM == 2 && Q == 1) return launch_team_t<M, 1, 2, LAGGED, SUMS, TS>(pt, mp, st);
+  if (TM == 4 && Q == 1) return launch_team_t<M, 1, 4, LAGGED, SUMS, TS>(pt, mp, st);
   if constexpr (!LAGGED) {
-    if (TM == 1 && Q == 4) return launch_team_t<M, 4, 1, LAGGED, SUMS>(pt, mp, st);
-    if (TM == 1 && Q == 2) return launch_team_t<M, 2, 1, LAGGED, SUMS>(pt, mp, st);
-    if (TM == 2 && Q == 2) return launch_team_t<M, 2, 2, LAGGED, SUMS>(pt, mp, st);
+    if (TM == 2 && Q == 2) return launch_team_t<M, 2, 2, LAGGED, SUMS, TS>(pt, mp, st);
   }
   return set_error(TP_ERR_UNSUPPORTED, "no team kernel for Q=%d, TM=%d", Q, TM);
+}
+
+// Exact adjoint in Cayley form unless a gradient reads plain forward slices
+// (two per step: not enough registers for the Cayley state as well).
+template <int M, int TS>
+static int launch_team_m(const Partition &pt, MarchParams &mp, bool lagged, int Q, int TM, cudaStream_t st) {
+  const bool sums = lagged && (mp.u_fwd == nullptr || mp.store_sums);
+  if (!lagged) return launch_team_qt<M, false, false, TS>(pt, mp, Q, TM, st);
+  return sums ? launch_team_qt<M, true, true, TS>(pt, mp, Q, TM, st)
+              : launch_team_qt<M, true, false, TS>(pt, mp, Q, TM, st);
 }
 
 // (teams per CTA, probes per thread) for K probes per CTA: one probe per
@@ -490,6 +501,10 @@ static void team_shape(int K, int *TM, int *Q) {
 }
 
 int launch_team_march(const Partition &pt, MarchParams &mp, bool lagged, cudaStream_t st) {
+  // Spike rows staged: a compile-time count >= the rows the factorisation
+  // keeps (the factor set holds all M rows; extra rows only add accuracy).
+  if (pt.M == 16) mp.trunc = mp.trunc <= 8 ? 8 : 15;
+  else mp.trunc = pt.M - 1;
   mp.smem_slice_bytes = team_slice_smem(pt.M, mp.trunc);
   int dev = 0, sms = 148, max_smem = 232448;
   TP_CHECK_CUDA(cudaGetDevice(&dev));
@@ -516,22 +531,14 @@ int launch_team_march(const Partition &pt, MarchParams &mp, bool lagged, cudaStr
   if (team_smem_bytes(pt, mp.trunc, Q, TM, grad) > (size_t)max_smem)
     return set_error(TP_ERR_UNSUPPORTED, "team march needs %zu B of shared memory (> %d)",
                      team_smem_bytes(pt, mp.trunc, Q, TM, grad), max_smem);
-  // Exact adjoint in Cayley form unless a gradient reads plain forward slices
-  // (two per step: not enough registers for the Cayley state as well).
-  const bool sums = lagged && (mp.u_fwd == nullptr || mp.store_sums);
   switch (pt.M) {
     case 4:
-      return !lagged ? launch_team_qt<4, false, false>(pt, mp, Q, TM, st)
-             : sums  ? launch_team_qt<4, true, true>(pt, mp, Q, TM, st)
-                     : launch_team_qt<4, true, false>(pt, mp, Q, TM, st);
+      return launch_team_m<4, 3>(pt, mp, lagged, Q, TM, st);
     case 8:
-      return !lagged ? launch_team_qt<8, false, false>(pt, mp, Q, TM, st)
-             : sums  ? launch_team_qt<8, true, true>(pt, mp, Q, TM, st)
-                     : launch_team_qt<8, true, false>(pt, mp, Q, TM, st);
+      return launch_team_m<8, 7>(pt, mp, lagged, Q, TM, st);
     case 16:
-      return !lagged ? launch_team_qt<16, false, false>(pt, mp, Q, TM, st)
-             : sums  ? launch_team_qt<16, true, true>(pt, mp, Q, TM, st)
-                     : launch_team_qt<16, true, false>(pt, mp, Q, TM, st);
+      return mp.trunc == 8 ? launch_team_m<16, 8>(pt, mp, lagged, Q, TM, st)
+                           : launch_team_m<16, 15>(pt, mp, lagged, Q, TM, st);
     default:
       return set_error(TP_ERR_UNSUPPORTED, "no team kernel for %d rows per chunk", pt.M);
   }
