@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--config", default="2d-fwd-adj-2048x1024-p512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-3d", action="store_true", help="skip the 3D learned-vs-plain section")
-    ap.add_argument("--case", choices=("headline", "3d-march-small", "3d-recon"), default="headline",
+    ap.add_argument("--case", choices=("headline", "3d-march-small", "3d-recon", "3d-ms"), default="headline",
                     help="3d-march-small: a few learned 3D forward marches (256 x 256 x 5 nodes, 64 probes), "
                          "a small profiler target for the conv and FFT kernels; 3d-recon: `steps` gradient-descent "
                          "iterations of the 3D reconstruction (192 x 192 x 192, 256 probes), plain vs learned")
@@ -520,6 +520,57 @@ def run_case_3d_small(a):
                       "stats": eng.read_stats()}), flush=True)
 
 
+def run_case_3d_ms(a):
+    """3D multislice (the reference's multislice is 2D only) on the 256 x 256 x 256-node,
+    64-probe geometry with n = 1 + δn (400 seeded ellipsoids): forward march to the exit
+    plane, forward march keeping the field, adjoint march with the gradient; CUDA-event
+    medians over `steps` after `warmup`, plus the complex128 numpy restatement timed on one
+    probe for 8 slices."""
+    import torch
+
+    from oracle import pwe_oracle as po
+    from thick_ptycho_b200.ms3d import MS3D
+    from thick_ptycho_b200.workloads import CONFIG2
+
+    w = CONFIG2
+    geo = w.geometry()
+    dev = torch.device("cuda", 0)
+    nx, nz, P = w.nx, w.nz, w.num_probes
+    n = 1 + w.delta_n()
+    eng = MS3D(nx, nx, nz, geo.k, 1.0, 1.0, 1.0, device=dev)
+    T = eng.transmission(torch.from_numpy(n.reshape(-1, nz)).to(dev))
+    probes_np = w.probes(geo).reshape(P, -1).astype(np.complex64)
+    probes = torch.from_numpy(probes_np).to(dev)
+    ex = torch.empty((P, eng.N), dtype=torch.complex64, device=dev)
+    st = torch.empty((P, nz, eng.N), dtype=torch.complex64, device=dev)
+    gt = torch.zeros((eng.L, eng.N), dtype=torch.complex64, device=dev)
+    rng = np.random.default_rng(3)
+    src = torch.from_numpy((rng.standard_normal((P, eng.N)) + 1j * rng.standard_normal((P, eng.N))).astype(np.complex64)).to(dev)
+    runs = {"forward_exit": lambda: eng.march(T, probes, exit_out=ex),
+            "forward_store": lambda: eng.march(T, probes, u_store=st, exit_out=ex),
+            "adjoint_grad": lambda: eng.backward(T, st, src, gt)}
+    ms = {k: [] for k in runs}
+    for i in range(a.warmup + a.steps):
+        for key, fn in runs.items():
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            if i >= a.warmup:
+                ms[key].append(e0.elapsed_time(e1))
+    med = {k: statistics.median(v) for k, v in ms.items()}
+    ps = P * eng.L
+    t0 = time.perf_counter()
+    po.ms_forward_3d(n[:, :, :9], probes_np[0].reshape(nx, nx).astype(complex), geo.k, 1.0, 1.0, 1.0)
+    cpu_s = (time.perf_counter() - t0) / 8
+    print(json.dumps({"case": "3d-ms", "workload": f"3d-ms-{nx}x{nx}x{nz}-p{P}", "ms": med,
+                      "probe_slices_per_s": {k: ps / (v * 1e-3) for k, v in med.items()},
+                      "fwd_adj_probe_slices_per_s": ps / ((med["forward_store"] + med["adjoint_grad"]) * 1e-3),
+                      "cpu_oracle_s_per_probe_slice": cpu_s,
+                      "launches_per_march": 2 * eng.L + 1 + 3}), flush=True)
+
+
 def run_case_3d_recon(a):
     """3D reconstruction, 192 x 192 transverse x 192 nodes, 256 probes (16 x 16 raster, stride 10,
     waist 12), ground truth δn = 600 seeded ellipsoids + 1e-6 i, data = |FFT2(exit)| of the truth;
@@ -593,6 +644,8 @@ def main():
         run_case_3d_small(a)
     elif a.case == "3d-recon":
         run_case_3d_recon(a)
+    elif a.case == "3d-ms":
+        run_case_3d_ms(a)
     else:
         run_ours(a)
 

@@ -259,6 +259,40 @@ TP_API int tp_ms2d_3pie(const tp_ms2d_op *op, const void *probes, int32_t num_pr
                         int32_t phase_retrieval, int32_t iters, double alpha_obj, void *n_est, double *loss,
                         void *workspace, size_t workspace_bytes, tp_stream_t stream);
 
+/* ---------------------------------------------------- 3D multislice
+ * The propagator of tp_ms2d_* on an (n1, n2) transverse grid (the
+ * reference's multislice solver is 2D only, ms_solver.py:28-31):
+ * u_{z+1} = IFFT2(H . FFT2(T_z u_z)), H = exp(i (k_z - k) dz),
+ * k_z = sqrt(max(k^2 - k1^2 - k2^2, 0)), k1 = 2 pi fftfreq(n1, d1),
+ * k2 = 2 pi fftfreq(n2, d2).  Element (a, b) of a slice is at a * n2 + b
+ * (the C-order flattening of the reference's (nx, ny) arrays); the index
+ * field is (n1 * n2, nz). */
+typedef struct tp_ms3d_op {
+  int32_t n1, n2;        /* transverse grid, each 2^a 3^b 5^c <= 4096 */
+  int32_t nz;            /* z nodes (L = nz - 1 steps) */
+  int32_t reserved;
+  double k, d1, d2, dz;
+  double n_medium[2];    /* background index (re, im) */
+} tp_ms3d_op;
+
+/* Workspace of tp_ms3d_march / tp_ms3d_backward for P probes (the field and
+ * spectrum work buffers, (H - 1)/N and the twiddles). */
+TP_API size_t tp_ms3d_workspace_bytes(int32_t n1, int32_t n2, int32_t num_probes);
+/* Transmission table T - 1, (L, n1 * n2) complex64, from the index field. */
+TP_API int tp_ms3d_transmission(const tp_ms3d_op *op, const void *n_field, int32_t n_dtype, void *trans,
+                                tp_stream_t stream);
+/* March P probes (P, n1 * n2); u_store (P, nz, n1 * n2) or NULL; exit_out
+ * (P, n1 * n2) or NULL.  Two kernels per slice (row pass, column pass). */
+TP_API int tp_ms3d_march(const tp_ms3d_op *op, const void *trans, const void *probes, int32_t num_probes,
+                         void *u_store, void *exit_out, void *workspace, size_t workspace_bytes,
+                         tp_stream_t stream);
+/* Adjoint march from src_exit (P, n1 * n2) with the forward field u_fwd
+ * (P, nz, n1 * n2): grad_t (L, n1 * n2) += sum_p conj(T_z u_z) g_z,
+ * g_z = IFFT2(conj(H) FFT2(lambda_{z+1})); d loss/d n[:, z] = conj(i k dz) grad_t[z]. */
+TP_API int tp_ms3d_backward(const tp_ms3d_op *op, const void *trans, const void *u_fwd, const void *src_exit,
+                            int32_t num_probes, void *grad_t, void *workspace, size_t workspace_bytes,
+                            tp_stream_t stream);
+
 /* ------------------------------------------------------------------- 3D
  * 3D problems (2D transverse, N = nf*nb rows, index i = b*nf + f, the
  * flattening of kron(I_y, A_x) in operator_matrices.py:75-99): each slice is

@@ -482,6 +482,31 @@ def ms_forward(n, probe, k, dx, dz, n_medium=1.0):
     return u
 
 
+def ms_kernel_3d(n1, n2, d1, d2, k, dz):
+    """3D angular-spectrum kernel: ``ms_kernel`` with kx² replaced by
+    k1² + k2² over the (n1, n2) grid (``ms_solver.py:49-72`` made 2D in the
+    transverse plane; the reference itself has no 3D multislice)."""
+    k1 = 2 * np.pi * np.fft.fftfreq(n1, d=d1)[:, None]
+    k2 = 2 * np.pi * np.fft.fftfreq(n2, d=d2)[None, :]
+    kz = np.sqrt(np.clip(k**2 - k1**2 - k2**2, 0.0, None))
+    return np.exp(1j * kz * dz) * np.exp(-1j * k * dz)
+
+
+def ms_forward_3d(n, probe, k, d1, d2, dz, n_medium=1.0):
+    """3D multislice march of one probe: n (n1, n2, Nz), probe (n1, n2) →
+    u (n1, n2, Nz).  Same steps as :func:`ms_forward` with ``fft2``."""
+    n1, n2, Nz = n.shape
+    H = ms_kernel_3d(n1, n2, d1, d2, k, dz)
+    u = np.empty((n1, n2, Nz), dtype=complex)
+    psi = np.asarray(probe, dtype=complex).copy()
+    u[:, :, 0] = psi
+    for z in range(Nz - 1):
+        psi = psi * np.exp(1j * k * (n[:, :, z] - n_medium) * dz)
+        psi = np.fft.ifft2(np.fft.fft2(psi) * H)
+        u[:, :, z + 1] = psi
+    return u
+
+
 def ms_3pie(probes, data, k, dx, dz, nz, iters, alpha_obj=1.0, n_medium=1.0, phase_retrieval=True):
     """Multislice 3PIE reconstruction (``reconstruction/ms_reconstructor.py:40-190``).
 

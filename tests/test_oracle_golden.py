@@ -222,3 +222,20 @@ def test_ms_3pie_epochs(golden):
         ref = g[f"n_{it}"]
         assert np.linalg.norm(n - ref) <= 1e-9 * np.linalg.norm(ref - 1), it
         assert np.allclose(loss, g[f"loss_{it}"], rtol=1e-9, atol=0)
+
+
+def test_ms_3d_reduces_to_reference_2d_multislice(golden):
+    """The 3D multislice restatement (the reference has none) pinned to the
+    reference's own 2D MSForwardModelSolver: an object and probe constant
+    along the second transverse axis keep only its zero frequency, where the
+    3D kernel equals the 2D one, so every line of the 3D field must equal the
+    reference's 2D field."""
+    g = golden("random2d")
+    k, dx, dz = float(g["k"]), float(g["dx"]), float(g["dz"])
+    n2 = 4
+    n3 = np.repeat(g["n"][:, None, :], n2, axis=1)
+    for p in range(4):
+        pr3 = np.repeat(g["probes"][p][:, None], n2, axis=1)
+        u3 = po.ms_forward_3d(n3, pr3, k, dx, 0.7, dz)
+        for j in range(n2):
+            assert rel(u3[:, j, :], g["ms_forward"][p]) < RTOL, (p, j)

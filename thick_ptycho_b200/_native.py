@@ -88,6 +88,20 @@ class TpMs2dOp(ctypes.Structure):
     ]
 
 
+class TpMs3dOp(ctypes.Structure):
+    _fields_ = [
+        ("n1", ctypes.c_int32),
+        ("n2", ctypes.c_int32),
+        ("nz", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("k", ctypes.c_double),
+        ("d1", ctypes.c_double),
+        ("d2", ctypes.c_double),
+        ("dz", ctypes.c_double),
+        ("n_medium", ctypes.c_double * 2),
+    ]
+
+
 class TpCn3dOp(ctypes.Structure):
     _fields_ = [
         ("nf", ctypes.c_int32), ("nb", ctypes.c_int32), ("nz", ctypes.c_int32),
@@ -161,6 +175,15 @@ SIGNATURES = [
     ("tp_ms2d_3pie", ctypes.c_int, [ctypes.POINTER(TpMs2dOp), ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
                                     ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_void_p,
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    ("tp_ms3d_workspace_bytes", ctypes.c_size_t, [ctypes.c_int32] * 3),
+    ("tp_ms3d_transmission", ctypes.c_int, [ctypes.POINTER(TpMs3dOp), ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                                            ctypes.c_void_p]),
+    ("tp_ms3d_march", ctypes.c_int, [ctypes.POINTER(TpMs3dOp), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                     ctypes.c_void_p]),
+    ("tp_ms3d_backward", ctypes.c_int, [ctypes.POINTER(TpMs3dOp), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                        ctypes.c_void_p]),
     ("tp_cn3d_workspace_bytes", ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
     ("tp_cn3d_learned_ws_bytes", ctypes.c_size_t, [ctypes.c_int32] * 3),
     ("tp_cn3d_march", ctypes.c_int, [ctypes.POINTER(TpCn3dOp), ctypes.c_void_p, ctypes.c_int32,

@@ -177,32 +177,6 @@ __global__ void c3_scalar_kernel(Krylov *K, int P, double tol2, int first, int *
   (void)stats;
 }
 
-// FFT of `rows` transforms of length n in shared memory: the compile-time plan
-// in the padded layout when N > 0, else the runtime plan `pl` (unpadded).
-template <int N>
-__device__ __forceinline__ float2 *fft_rows(float2 *a, float2 *b, const FftPlan &pl, const float2 *tw, bool inverse,
-                                            int rows) {
-  if constexpr (N > 0) return fft_block_padded<N>(a, b, tw, inverse, rows, threadIdx.x, blockDim.x);
-  else return fft_block(a, b, pl, tw, inverse, rows, threadIdx.x, blockDim.x);
-}
-
-// Shared-memory slot of element i of transform bi (length n).
-template <int N>
-__device__ __forceinline__ int fslot(int bi, int i, int n) {
-  if constexpr (N > 0) return bi * FftPad<N>::S + fft_pad(i);
-  else return bi * n + i;
-}
-// Shared-memory slots per transform.
-template <int N>
-__host__ __device__ constexpr int fstride(int n) {
-  if constexpr (N > 0) return FftPad<N>::S;
-  else return n;
-}
-
-__device__ __forceinline__ void load_twiddles(float2 *tw, const float2 *__restrict__ twg, int n) {
-  for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twg[t];
-}
-
 // Twiddle table W_n^t = exp(-2 pi i t / n) (fp64 sincospi, rounded once).
 __global__ void c3_twiddle_kernel(int n, float2 *tw) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {

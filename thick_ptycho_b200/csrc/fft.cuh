@@ -6,8 +6,8 @@
 // an R-point DFT in registers and writes them with stride Ns (autosort, so
 // the result is in natural order without a bit-reversal pass).  Twiddles
 // W_n^t = exp(-2 pi i t / n) are computed once per CTA in fp64 into shared
-// memory.  Forward transforms are unnormalised and inverse transforms are
-// scaled by 1/n, as numpy.fft.
+// memory.  Both directions are unnormalised (the inverse is n times
+// numpy.fft.ifft); callers fold the 1/n into an adjacent multiply.
 #pragma once
 
 #include "tp_common.cuh"
@@ -288,6 +288,33 @@ __device__ __forceinline__ float2 *fft_block(float2 *a, float2 *b, const FftPlan
     Ns *= R;
   }
   return a;
+}
+
+// FFT of `rows` transforms of length n in shared memory: the compile-time
+// plan in the padded layout when N > 0, else the runtime plan `pl`
+// (unpadded).  Whole-CTA call.
+template <int N>
+__device__ __forceinline__ float2 *fft_rows(float2 *a, float2 *b, const FftPlan &pl, const float2 *tw, bool inverse,
+                                            int rows) {
+  if constexpr (N > 0) return fft_block_padded<N>(a, b, tw, inverse, rows, threadIdx.x, blockDim.x);
+  else return fft_block(a, b, pl, tw, inverse, rows, threadIdx.x, blockDim.x);
+}
+
+// Shared-memory slot of element i of transform bi (length n).
+template <int N>
+__device__ __forceinline__ int fslot(int bi, int i, int n) {
+  if constexpr (N > 0) return bi * FftPad<N>::S + fft_pad(i);
+  else return bi * n + i;
+}
+// Shared-memory slots per transform.
+template <int N>
+__host__ __device__ constexpr int fstride(int n) {
+  if constexpr (N > 0) return FftPad<N>::S;
+  else return n;
+}
+
+__device__ __forceinline__ void load_twiddles(float2 *tw, const float2 *__restrict__ twg, int n) {
+  for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twg[t];
 }
 
 }  // namespace tp

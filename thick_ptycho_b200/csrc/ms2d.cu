@@ -265,6 +265,22 @@ __global__ void __launch_bounds__(kFftThreads) ms_backward_kernel(const FftPlan 
 
 static size_t fft_smem(int n, int rows, int extra) { return (size_t)(extra * n + 2 * rows * n) * sizeof(float2); }
 
+int ms_transmission_launch(int n_total, int nz, double k, double dz, double nmr, double nmi, const void *field,
+                           int dtype, float2 *trans, cudaStream_t st) {
+  MsParams q{};
+  q.n = n_total;
+  q.nz = nz;
+  q.L = nz - 1;
+  q.k = k;
+  q.dz = dz;
+  q.nmr = nmr;
+  q.nmi = nmi;
+  q.field = field;
+  q.dtype = dtype;
+  ms_transmission_kernel<<<592, 256, 0, st>>>(q, trans);
+  return check_cuda(cudaGetLastError(), "ms_transmission_kernel launch");
+}
+
 static int fft_launch_setup(const void *kern, size_t smem) {
   return check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                     "cudaFuncSetAttribute(fft)");
@@ -347,10 +363,8 @@ extern "C" int tp_ms2d_transmission(const tp_ms2d_op *op, const void *n_field, i
   int rc = ms_params(op, &q);
   if (rc) return rc;
   if (!n_field || !trans) return set_error(TP_ERR_INVALID, "n_field/trans is NULL");
-  q.field = n_field;
-  q.dtype = n_dtype;
-  ms_transmission_kernel<<<592, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(q, static_cast<float2 *>(trans));
-  return check_cuda(cudaGetLastError(), "ms_transmission_kernel launch");
+  return ms_transmission_launch(q.n, q.nz, q.k, q.dz, q.nmr, q.nmi, n_field, n_dtype, static_cast<float2 *>(trans),
+                                reinterpret_cast<cudaStream_t>(stream));
 }
 
 static int ms_rows(int n) {

@@ -94,13 +94,17 @@ class MSFunction(torch.autograd.Function):
 
 
 class MSGpuSolver:
-    """Drop-in for ``MSForwardModelSolver`` (2D) running on one B200."""
+    """Drop-in for ``MSForwardModelSolver`` running on one B200.
+
+    2D as the reference; a 3D simulation space (which the reference rejects,
+    ``ms_solver.py:28-31``) runs the 3D propagator of :mod:`.ms3d`, with
+    fields of shape (proj, angle, probes, nx, ny, nz).
+    """
 
     def __init__(self, simulation_space, ptycho_probes, results_dir="", use_logging=False, verbose=False, log=None,
                  device=None):
         ss = simulation_space
-        if ss.dimension == 3:
-            raise NotImplementedError("3D simulation space is not yet implemented for MSForwardModelSolver.")
+        self.dimension = int(getattr(ss, "dimension", 2))
         self.simulation_space = ss
         self.probes = ptycho_probes
         self.verbose = verbose
@@ -114,7 +118,16 @@ class MSGpuSolver:
         self.num_angles = len(self.probe_angles)
         self.n_medium = complex(getattr(ss, "n_medium", 1.0))
         self.solver_type = self.__class__.__name__
-        self.engine = MS2D(self.nx_eff, self.nz, ss.k, ss.dx, ss.dz, self.n_medium, device=device)
+        if self.dimension == 3:
+            from .ms3d import MS3D
+
+            ny_eff = getattr(ss, "effective_ny", self.nx_eff)
+            self.engine = MS3D(self.nx_eff, ny_eff, self.nz, ss.k, ss.dx, getattr(ss, "dy", ss.dx), ss.dz,
+                               self.n_medium, device=device)
+            self.block = self.nx_eff * ny_eff
+        else:
+            self.engine = MS2D(self.nx_eff, self.nz, ss.k, ss.dx, ss.dz, self.n_medium, device=device)
+            self.block = self.nx_eff
         self.device = self.engine.device
 
     def reset_cache(self):
@@ -124,8 +137,10 @@ class MSGpuSolver:
         if n is None:
             n = self.simulation_space.refractive_index_empty
         if isinstance(n, torch.Tensor):
-            return n.to(self.device)
-        return torch.from_numpy(np.ascontiguousarray(n, dtype=np.complex128)).to(self.device)
+            f = n.to(self.device)
+        else:
+            f = torch.from_numpy(np.ascontiguousarray(n, dtype=np.complex128)).to(self.device)
+        return f.reshape(self.block, self.nz)
 
     def solve(self, n=None, mode="forward", rhs_block=None, probes=None, **kwargs) -> np.ndarray:
         """All probes, shape (proj, angle, probes, nx, nz) complex128 (``base/base_solver.py:84-154``)."""
@@ -135,8 +150,8 @@ class MSGpuSolver:
         probes = self.probes if probes is None else probes
         count = self.num_angles * self.num_probes
         T = self.engine.transmission(self._field(n))
-        pr = torch.from_numpy(np.ascontiguousarray(probes).reshape(count, self.nx_eff).astype(np.complex64)).to(self.device)
-        st = torch.empty((count, self.nz, self.nx_eff), dtype=torch.complex64, device=self.device)
+        pr = torch.from_numpy(np.ascontiguousarray(probes).reshape(count, self.block).astype(np.complex64)).to(self.device)
+        st = torch.empty((count, self.nz, self.block), dtype=torch.complex64, device=self.device)
         self.engine.march(T, pr, u_store=st)
         u = st.permute(0, 2, 1).cpu().numpy().astype(np.complex128)
         out = np.zeros((self.num_projections, self.num_angles, self.num_probes, *self.effective_shape), dtype=complex)
@@ -146,21 +161,30 @@ class MSGpuSolver:
     def _solve_single_probe(self, scan_idx=0, proj_idx=0, n=None, mode="forward", probe=None, **kwargs):
         assert mode in {"forward", "backward"}, f"Invalid mode: {mode}"
         if probe is None:
-            probe = np.zeros(self.nx_eff, dtype=complex)
+            probe = np.zeros(self.block, dtype=complex)
         T = self.engine.transmission(self._field(n))
         pr = torch.from_numpy(np.asarray(probe, dtype=np.complex64).reshape(1, -1)).to(self.device)
-        st = torch.empty((1, self.nz, self.nx_eff), dtype=torch.complex64, device=self.device)
+        st = torch.empty((1, self.nz, self.block), dtype=torch.complex64, device=self.device)
         self.engine.march(T, pr, u_store=st)
-        return st[0].T.cpu().numpy().astype(np.complex128)
+        return st[0].T.cpu().numpy().astype(np.complex128).reshape(*self.effective_shape)
 
     def get_exit_waves(self, u=None) -> np.ndarray:
         return u[..., -1].reshape((self.simulation_space.total_scans, self.simulation_space.block_size))
 
     def get_farfield_intensities(self, u=None, exit_waves=None, poisson_noise=True) -> np.ndarray:
-        """``|FFT(exit)|²`` computed on the GPU (``base/base_solver.py:213-249``)."""
+        """``|FFT(exit)|²`` computed on the GPU (``base/base_solver.py:213-249``); in 3D,
+        as the reference's base solver, ``fft2`` over the last two axes of the
+        (total_scans, block_size) exit-wave array."""
         exit_waves = self.get_exit_waves(u=u) if exit_waves is None else exit_waves
         ex = torch.from_numpy(np.ascontiguousarray(exit_waves).astype(np.complex64)).to(self.device)
-        inten = heads.farfield_intensity(ex).cpu().numpy().astype(np.float64)
+        if self.dimension == 3:
+            ex = ex.reshape(self.simulation_space.total_scans, self.simulation_space.block_size)
+            if heads.fft_plannable(ex.shape[0]) and heads.fft_plannable(ex.shape[1]):
+                inten = (heads.fft2_last(ex).abs() ** 2).cpu().numpy().astype(np.float64)
+            else:
+                inten = (torch.fft.fft2(ex.to(torch.complex128), dim=(-2, -1)).abs() ** 2).cpu().numpy()
+        else:
+            inten = heads.farfield_intensity(ex).cpu().numpy().astype(np.float64)
         if poisson_noise:
             inten = np.random.poisson(inten)
         return inten.reshape((self.simulation_space.total_scans, self.simulation_space.block_size))
