@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--config", default="2d-fwd-adj-2048x1024-p512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-3d", action="store_true", help="skip the 3D learned-vs-plain section")
+    ap.add_argument("--ms-nz", type=int, default=0, help="3d-ms case: use the first N z nodes only")
     ap.add_argument("--case", choices=("headline", "3d-march-small", "3d-recon", "3d-ms"), default="headline",
                     help="3d-march-small: a few learned 3D forward marches (256 x 256 x 5 nodes, 64 probes), "
                          "a small profiler target for the conv and FFT kernels; 3d-recon: `steps` gradient-descent "
@@ -537,6 +538,9 @@ def run_case_3d_ms(a):
     dev = torch.device("cuda", 0)
     nx, nz, P = w.nx, w.nz, w.num_probes
     n = 1 + w.delta_n()
+    if a.ms_nz:  # fewer slices of the same field (small profiling captures)
+        nz = int(a.ms_nz)
+        n = np.ascontiguousarray(n[:, :, :nz])
     eng = MS3D(nx, nx, nz, geo.k, 1.0, 1.0, 1.0, device=dev)
     T = eng.transmission(torch.from_numpy(n.reshape(-1, nz)).to(dev))
     probes_np = w.probes(geo).reshape(P, -1).astype(np.complex64)

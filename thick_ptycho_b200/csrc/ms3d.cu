@@ -77,24 +77,37 @@ __global__ void ms3_kernel_h_kernel(int n1, int n2, double k, double d1, double 
   }
 }
 
+// Rows (columns) per CTA of the compile-time plans: at most 16 and 4096 elements.
+__host__ __device__ constexpr int ms3_fixed_per_cta(int n) { return 4096 / n > 16 ? 16 : 4096 / n; }
+
 // Row pass of slice z (phase selects start / step, forward / adjoint).
-// Grid (n1 / rpc, P): a CTA owns rpc rows of one probe.
+// Grid (n1 / rpc, P): a CTA owns rpc rows of one probe.  The spectrum rows
+// (into a) and the step's third operand (T_{z+1} forward, u_z adjoint, into
+// the unpadded buffer c) are copied asynchronously at entry; with a
+// compile-time plan (N2 > 0, rpc = ms3_fixed_per_cta(N2)) every thread owns
+// EPT fixed elements whose field and T_z values are loaded into registers at
+// entry too, so all loads overlap the inverse FFT.
 template <int N2>
 __global__ void __launch_bounds__(kMs3Threads) ms3_rows_kernel(const FftPlan pl, const Ms3Params q, int phase, int z,
-                                                               int rpc) {
+                                                               int rpc_rt) {
   extern __shared__ __align__(16) float2 fsm[];
-  const int n = N2 > 0 ? N2 : q.n2, pr = blockIdx.y;
-  float2 *tw = fsm, *a = tw + n, *b = a + rpc * fstride<N2>(n);
+  constexpr bool FIX = N2 > 0;
+  constexpr int RPC = FIX ? ms3_fixed_per_cta(N2 > 0 ? N2 : 1) : 1;
+  constexpr int EPT = FIX ? RPC * N2 / kMs3Threads : 1;
+  const int n = FIX ? N2 : q.n2, pr = blockIdx.y;
+  const int rpc = FIX ? RPC : rpc_rt;
+  float2 *tw = fsm, *a = tw + n, *b = a + rpc * fstride<N2>(n), *cbuf = b + rpc * fstride<N2>(n);
   const size_t pbase = (size_t)pr * q.N;
   const int g0 = blockIdx.x * rpc * n;  // first element of the CTA's rows within the slice
   const int tot = rpc * n;
+  const int tid = threadIdx.x;
   auto slot = [&](int e) { return fslot<N2>(e / n, e % n, n); };
   load_twiddles(tw, q.tw2, n);
   float2 *out = a;  // the buffer transformed forward into W at the end
   bool fwd_fft = true;
   if (phase == kMs3FwdStart) {
     const float2 *T0 = q.trans;
-    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+    for (int e = tid; e < tot; e += kMs3Threads) {
       const int g = g0 + e;
       const float2 v = q.probes[pbase + g];
       q.psi[pbase + g] = v;
@@ -102,50 +115,74 @@ __global__ void __launch_bounds__(kMs3Threads) ms3_rows_kernel(const FftPlan pl,
       a[slot(e)] = cfma(T0[g], v, v);
     }
   } else if (phase == kMs3BwdStart) {
-    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+    for (int e = tid; e < tot; e += kMs3Threads) {
       const int g = g0 + e;
       const float2 v = q.src_exit[pbase + g];
       q.psi[pbase + g] = v;
       a[slot(e)] = v;
     }
   } else {
-    for (int e = threadIdx.x; e < tot; e += blockDim.x) a[slot(e)] = q.W[pbase + g0 + e];
+    const float2 *Tz = q.trans + (size_t)z * q.N;
+    const bool last = (phase == kMs3FwdStep) && (z + 1 == q.L);
+    const float2 *third = phase == kMs3FwdStep ? (last ? nullptr : q.trans + (size_t)(z + 1) * q.N + g0)
+                                               : q.u_fwd + ((size_t)pr * q.nz + z) * q.N + g0;
+    for (int e = tid; e < tot; e += kMs3Threads) {
+      cp_async8(&a[slot(e)], &q.W[pbase + g0 + e]);
+      if (third) cp_async8(&cbuf[e], &third[e]);
+    }
+    float2 pz[EPT], tz[EPT];
+    if constexpr (FIX) {
+#pragma unroll
+      for (int j = 0; j < EPT; ++j) {
+        const int g = g0 + tid + j * kMs3Threads;
+        pz[j] = q.psi[pbase + g];
+        tz[j] = Tz[g];
+      }
+    }
+    cp_async_wait_all();
     __syncthreads();
     const float2 *R = fft_rows<N2>(a, b, pl, tw, true, rpc);
     out = (R == a) ? b : a;
-    const float2 *Tz = q.trans + (size_t)z * q.N;
     if (phase == kMs3FwdStep) {
       // psi_{z+1} = X_z + IFFT2((H-1) FFT2 X_z), X_z = psi_z + (T_z - 1) psi_z
-      const bool last = (z + 1 == q.L);
-      const float2 *Tn = last ? nullptr : q.trans + (size_t)(z + 1) * q.N;
-      for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+      float2 *us = q.u_store ? q.u_store + ((size_t)pr * q.nz + z + 1) * q.N : nullptr;
+      auto one = [&](int e, float2 pv, float2 tm1) {
         const int g = g0 + e;
-        const float2 pz = q.psi[pbase + g];
-        const float2 v = cadd(cfma(Tz[g], pz, pz), R[slot(e)]);
+        const float2 v = cadd(cfma(tm1, pv, pv), R[slot(e)]);
         q.psi[pbase + g] = v;
-        if (q.u_store) q.u_store[((size_t)pr * q.nz + z + 1) * q.N + g] = v;
+        if (us) us[g] = v;
         if (last) {
           if (q.exit_out) q.exit_out[pbase + g] = v;
         } else {
-          out[slot(e)] = cfma(Tn[g], v, v);
+          out[slot(e)] = cfma(cbuf[e], v, v);  // X_{z+1} = psi_{z+1} T_{z+1}
         }
+      };
+      if constexpr (FIX) {
+#pragma unroll
+        for (int j = 0; j < EPT; ++j) one(tid + j * kMs3Threads, pz[j], tz[j]);
+      } else {
+        for (int e = tid; e < tot; e += kMs3Threads) one(e, q.psi[pbase + g0 + e], Tz[g0 + e]);
       }
       fwd_fft = !last;
     } else {
       // g_z = lambda_{z+1} + IFFT2(conj(H-1) FFT2 lambda_{z+1});
       // grad_t[z] += g_z conj(T_z u_z);  lambda_z = conj(T_z) g_z
       float2 *gt = q.grad_t + (size_t)z * q.N;
-      const float2 *uz = q.u_fwd + ((size_t)pr * q.nz + z) * q.N;
-      for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+      auto one = [&](int e, float2 lam1, float2 tm1) {
         const int g = g0 + e;
-        const float2 gv = cadd(q.psi[pbase + g], R[slot(e)]);
-        const float2 tm1 = Tz[g];
-        const float2 u = uz[g];
+        const float2 gv = cadd(lam1, R[slot(e)]);
+        const float2 u = cbuf[e];  // u_z
         const float2 c = cmulc(gv, cfma(tm1, u, u));
         asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(gt + g), "f"(c.x), "f"(c.y) : "memory");
         const float2 lam = cadd(gv, cmulc(gv, tm1));
         q.psi[pbase + g] = lam;
         if (z > 0) out[slot(e)] = lam;
+      };
+      if constexpr (FIX) {
+#pragma unroll
+        for (int j = 0; j < EPT; ++j) one(tid + j * kMs3Threads, pz[j], tz[j]);
+      } else {
+        for (int e = tid; e < tot; e += kMs3Threads) one(e, q.psi[pbase + g0 + e], Tz[g0 + e]);
       }
       fwd_fft = z > 0;
     }
@@ -154,36 +191,55 @@ __global__ void __launch_bounds__(kMs3Threads) ms3_rows_kernel(const FftPlan pl,
   __syncthreads();
   float2 *scratch = (out == a) ? b : a;
   const float2 *F = fft_rows<N2>(out, scratch, pl, tw, false, rpc);
-  for (int e = threadIdx.x; e < tot; e += blockDim.x) q.W[pbase + g0 + e] = F[slot(e)];
+  for (int e = tid; e < tot; e += kMs3Threads) q.W[pbase + g0 + e] = F[slot(e)];
 }
 
 // Column pass: FFT along a, times (H - 1)/N (conjugated for the adjoint),
-// inverse FFT along a, in place on W.  Grid (n2 / cpc, P).
+// inverse FFT along a, in place on W.  Grid (n2 / cpc, P).  The columns are
+// copied asynchronously and, with a compile-time plan, the CTA's (H - 1)/N
+// block is loaded into registers under the forward FFT.
 template <int N1>
 __global__ void __launch_bounds__(kMs3Threads) ms3_cols_kernel(const FftPlan pl, const Ms3Params q, int conj_h,
-                                                               int cpc) {
+                                                               int cpc_rt) {
   extern __shared__ __align__(16) float2 fsm[];
-  const int n = N1 > 0 ? N1 : q.n1, pr = blockIdx.y;
+  constexpr bool FIX = N1 > 0;
+  constexpr int CPC = FIX ? ms3_fixed_per_cta(N1 > 0 ? N1 : 1) : 1;
+  constexpr int EPT = FIX ? CPC * N1 / kMs3Threads : 1;
+  const int n = FIX ? N1 : q.n1, pr = blockIdx.y;
+  const int cpc = FIX ? CPC : cpc_rt;
+  const int tid = threadIdx.x;
   float2 *tw = fsm, *a = tw + n, *b = a + cpc * fstride<N1>(n);
   const int b0 = blockIdx.x * cpc;
   float2 *base = q.W + (size_t)pr * q.N;
+  const float2 *h = q.hm1t + (size_t)b0 * n;
   load_twiddles(tw, q.tw1, n);
-  for (int e = threadIdx.x; e < cpc * n; e += blockDim.x) {
+  for (int e = tid; e < cpc * n; e += kMs3Threads) {
     const int c = e % cpc, r = e / cpc;  // coalesced over c
-    a[fslot<N1>(c, r, n)] = base[(size_t)r * q.n2 + b0 + c];
+    cp_async8(&a[fslot<N1>(c, r, n)], &base[(size_t)r * q.n2 + b0 + c]);
   }
+  float2 hv[EPT];
+  if constexpr (FIX) {
+#pragma unroll
+    for (int j = 0; j < EPT; ++j) hv[j] = h[tid + j * kMs3Threads];
+  }
+  cp_async_wait_all();
   __syncthreads();
   float2 *F = fft_rows<N1>(a, b, pl, tw, false, cpc);
   float2 *o = (F == a) ? b : a;
-  const float2 *h = q.hm1t + (size_t)b0 * n;
-  for (int e = threadIdx.x; e < cpc * n; e += blockDim.x) {
+  auto mul = [&](int e, float2 hh) {
     const int c = e / n, r = e - c * n;
     const int sl = fslot<N1>(c, r, n);
-    F[sl] = conj_h ? cmulc(F[sl], h[e]) : cmul(F[sl], h[e]);
+    F[sl] = conj_h ? cmulc(F[sl], hh) : cmul(F[sl], hh);
+  };
+  if constexpr (FIX) {
+#pragma unroll
+    for (int j = 0; j < EPT; ++j) mul(tid + j * kMs3Threads, hv[j]);
+  } else {
+    for (int e = tid; e < cpc * n; e += kMs3Threads) mul(e, h[e]);
   }
   __syncthreads();
   const float2 *R = fft_rows<N1>(F, o, pl, tw, true, cpc);
-  for (int e = threadIdx.x; e < cpc * n; e += blockDim.x) {
+  for (int e = tid; e < cpc * n; e += kMs3Threads) {
     const int c = e % cpc, r = e / cpc;
     base[(size_t)r * q.n2 + b0 + c] = R[fslot<N1>(c, r, n)];
   }
@@ -286,11 +342,16 @@ static int ms3_run(const tp_ms3d_op *op, Ms3Params q, bool backward, void *works
                                                                                            op->d2, op->dz, w.hm1t);
   TP_CHECK_CUDA(cudaGetLastError());
   const FftPlan p1 = make_fft_plan(n1), p2 = make_fft_plan(n2);
-  const Ms3Rows rows = pick_rows(n2);
-  const Ms3Cols cols = pick_cols(n1);
-  const int srow = fft_fixed_size(n2) ? n2 + n2 / 8 + 1 : n2, scol = fft_fixed_size(n1) ? n1 + n1 / 8 + 1 : n1;
-  const int rpc = ms3_per_cta(n2, n1), cpc = ms3_per_cta(n1, n2);
-  const size_t smem_r = (size_t)(n2 + 2 * rpc * srow) * sizeof(float2);
+  // compile-time plans (padded layout, fixed transforms per CTA) where the
+  // other axis splits into whole CTAs, else the runtime plan
+  const bool fix_r = fft_fixed_size(n2) && n1 % ms3_fixed_per_cta(n2) == 0;
+  const bool fix_c = fft_fixed_size(n1) && n2 % ms3_fixed_per_cta(n1) == 0;
+  const Ms3Rows rows = fix_r ? pick_rows(n2) : ms3_rows_of<0>();
+  const Ms3Cols cols = fix_c ? pick_cols(n1) : ms3_cols_of<0>();
+  const int srow = fix_r ? n2 + n2 / 8 + 1 : n2, scol = fix_c ? n1 + n1 / 8 + 1 : n1;
+  const int rpc = fix_r ? ms3_fixed_per_cta(n2) : ms3_per_cta(n2, n1);
+  const int cpc = fix_c ? ms3_fixed_per_cta(n1) : ms3_per_cta(n1, n2);
+  const size_t smem_r = (size_t)(n2 + 2 * rpc * srow + rpc * n2) * sizeof(float2);
   const size_t smem_c = (size_t)(n1 + 2 * cpc * scol) * sizeof(float2);
   TP_CHECK_CUDA(cudaFuncSetAttribute(rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_r));
   TP_CHECK_CUDA(cudaFuncSetAttribute(cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c));
