@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-3d", action="store_true", help="skip the 3D learned-vs-plain section")
     ap.add_argument("--ms-nz", type=int, default=0, help="3d-ms case: use the first N z nodes only")
-    ap.add_argument("--case", choices=("headline", "3d-march-small", "3d-recon", "3d-ms"), default="headline",
+    ap.add_argument("--case", choices=("headline", "3d-march-small", "3d-recon", "3d-ms", "pit"), default="headline",
                     help="3d-march-small: a few learned 3D forward marches (256 x 256 x 5 nodes, 64 probes), "
                          "a small profiler target for the conv and FFT kernels; 3d-recon: `steps` gradient-descent "
                          "iterations of the 3D reconstruction (192 x 192 x 192, 256 probes), plain vs learned")
@@ -575,6 +575,56 @@ def run_case_3d_ms(a):
                       "launches_per_march": 2 * eng.L + 1 + 3}), flush=True)
 
 
+def run_case_pit(a):
+    """PiT space-time GMRES (the reference's PWEFullPinTSolver) on the GPU: config 0
+    (N = 256, nz = 128, 32 probes) and the config-1 geometry (N = 2048, nz = 1024) with
+    8 probes; CUDA-event medians of `steps` solves after `warmup`, Arnoldi steps per
+    probe, and the complex128 restatement of the reference's solver (scipy GMRES,
+    splu blocks) timed on two config-0 probes on one host core."""
+    import torch
+
+    from oracle import pwe_oracle as po
+    from thick_ptycho_b200.cn2d import CN2D
+    from thick_ptycho_b200.pit import PiT2D
+    from thick_ptycho_b200.workloads import CONFIG0, CONFIG1
+
+    dev = torch.device("cuda", 0)
+    out = {"case": "pit"}
+    for w, P in ((CONFIG0, 32), (CONFIG1, 8)):
+        geo = w.geometry()
+        n = 1 - w.delta_n()
+        probes = w.probes(geo)[:P]
+        eng = CN2D(w.nx, w.nz, geo.k, 1.0, 1.0, "impedance", device=dev)
+        pit = PiT2D(eng)
+        field = torch.from_numpy(n).to(dev)
+        pr = torch.from_numpy(probes.astype(np.complex64)).to(dev)
+        ms = []
+        for i in range(a.warmup + a.steps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            pit.solve(field, probes=pr)
+            e1.record()
+            torch.cuda.synchronize()
+            if i >= a.warmup:
+                ms.append(e0.elapsed_time(e1))
+        med = statistics.median(ms)
+        out[f"{w.nx}x{w.nz}-p{P}"] = {"ms_per_solve": med, "arnoldi_steps": sorted(set(pit.iters)),
+                                       "max_resid": max(pit.resid),
+                                       "probe_slices_per_s": P * (w.nz - 1) / (med * 1e-3)}
+    w = CONFIG0
+    geo = w.geometry()
+    co = po.bc_coefficients(geo.k, 1.0, 1.0, bc_type="impedance")
+    A, B = po.step_matrices_1d(w.nx, co, "impedance", 1.0)
+    C = po.object_contribution(1 - w.delta_n(), geo.k, 1.0)
+    t0 = time.perf_counter()
+    _, its = po.pit_solve(A, B, C, w.probes(geo)[:2])
+    cpu = (time.perf_counter() - t0) / 2
+    out["cpu_reference_restatement"] = {"s_per_probe": cpu, "gmres_iterations": its, "cores": 1,
+                                        "sample": "config 0, 2 probes (preconditioner set-up included)"}
+    print(json.dumps(out), flush=True)
+
+
 def run_case_3d_recon(a):
     """3D reconstruction, 192 x 192 transverse x 192 nodes, 256 probes (16 x 16 raster, stride 10,
     waist 12), ground truth δn = 600 seeded ellipsoids + 1e-6 i, data = |FFT2(exit)| of the truth;
@@ -650,6 +700,8 @@ def main():
         run_case_3d_recon(a)
     elif a.case == "3d-ms":
         run_case_3d_ms(a)
+    elif a.case == "pit":
+        run_case_pit(a)
     else:
         run_ours(a)
 

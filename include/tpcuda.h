@@ -259,6 +259,42 @@ TP_API int tp_ms2d_3pie(const tp_ms2d_op *op, const void *probes, int32_t num_pr
                         int32_t phase_retrieval, int32_t iters, double alpha_obj, void *n_est, double *loss,
                         void *workspace, size_t workspace_bytes, tp_stream_t stream);
 
+/* ------------------------------------------------ PiT space-time solve
+ * The full-system form of the 2D march (full_pint.py:71-275,
+ * _pint_utils.py:27-205): the L = nz - 1 steps as one block-bidiagonal
+ * system M u = b, M = diag(A - C_j) - subdiag(B + C_j), b = [B u_0 + rhs_0,
+ * rhs_1, ...] (the probe enters through B alone, as in the reference's
+ * full-system solvers), solved by restarted GMRES right-preconditioned with
+ * the alpha-circulant R = Gamma^-1 F blockdiag((A - w_j B)^-1) F* Gamma of the
+ * free-space A, B, in its flexible form (u = u_0 + Z s with z_j = R v_j).
+ * All probes' Krylov spaces are built together.
+ * Replaces PWEFullPinTSolver._solve_single_probe_impl for the forward mode. */
+typedef struct tp_pit_args {
+  int32_t num_probes;      /* P                                                */
+  int32_t restart;         /* Krylov vectors per cycle (0 = 20, scipy's
+                              default), <= 64                                  */
+  int32_t max_cycles;      /* restart cycles (0 = 1000)                        */
+  int32_t reserved;
+  double alpha;            /* circulant parameter (0 = 1e-2, the reference's)  */
+  double rtol, atol;       /* stop at ||b - M u|| <= max(atol, rtol ||b||)
+                              (0 = 1e-5 / 1e-8, the reference's gmres call)    */
+  const void *probes;      /* float2 (P, N) initial fields u_0, or NULL         */
+  const void *rhs;         /* float2 (P, nz-1, N) added to b (slice-major), or
+                              NULL                                             */
+  void *u;                 /* float2 (P, nz-1, N): u_1 .. u_L, the initial
+                              guess in (zeros for none), the solution out      */
+  int32_t *iters;          /* host (P) or NULL: Arnoldi steps per probe          */
+  double *resid;           /* host (P) or NULL: final ||b - M u|| per probe      */
+} tp_pit_args;
+
+/* Workspace bytes of tp_pit_solve (0 if unsupported). */
+TP_API size_t tp_pit_workspace_bytes(int32_t n, int32_t nz, int32_t num_probes, int32_t restart);
+/* Solve for every probe; op as for tp_cn2d_factor (its K and object fields);
+ * n_field (n_obj, nz) of dtype n_dtype.  nz - 1 <= 2048.  Synchronises the
+ * stream (the GMRES control flow runs on the host). */
+TP_API int tp_pit_solve(const tp_cn2d_op *op, const void *n_field, int32_t n_dtype, const tp_pit_args *args,
+                        void *workspace, size_t workspace_bytes, tp_stream_t stream);
+
 /* ---------------------------------------------------- 3D multislice
  * The propagator of tp_ms2d_* on an (n1, n2) transverse grid (the
  * reference's multislice solver is 2D only, ms_solver.py:28-31):

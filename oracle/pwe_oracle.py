@@ -238,6 +238,107 @@ def march(A, B, C2d, probe, mode="forward", b=None, rhs_block=None, test_rhs=Non
 
 
 # ---------------------------------------------------------------------------
+# Space-time (parallel-in-time) solve: the reference's PWEFullPinTSolver
+# ---------------------------------------------------------------------------
+def pit_matvec(A, B, C2d, v):
+    """Space-time operator ``M v``: slice j gets ``(A − C_j) v_j − (B + C_j) v_{j−1}``
+    (vectors slice-major, ``v[j·N + i]``).  Restates ``_pint_utils.py:27-54``
+    (forward mode), which pairs the subdiagonal of row j with ``C[:, j]``."""
+    N, L = C2d.shape
+    V = np.reshape(v, (N, L), order="F")
+    U = (A @ V) - C2d * V
+    U[:, 1:] -= B @ V[:, :-1] + C2d[:, 1:] * V[:, :-1]
+    return np.reshape(U, (N * L,), order="F")
+
+
+class PiTPreconditionerOracle:
+    """α-block-circulant preconditioner of ``_pint_utils.py:57-205``.
+
+    ``ω_j = α^{1/L} e^{2πij/L}``, ``γ_j = α^{j/L}`` (``setup``, :150-163);
+    blocks ``splu(A − ω_j B)`` of the free-space A, B (``factorize_blocks``,
+    :175-205; the solver never calls ``update``, so C does not enter); apply
+    (forward, :91-104): scale by γ, ``ifft`` along z (ortho), block solves,
+    ``fft`` along z (ortho), divide by γ.
+    """
+
+    def __init__(self, A, B, L, alpha):
+        from scipy.fft import fft, ifft
+
+        self._fft, self._ifft = fft, ifft
+        self.N, self.L = A.shape[0], L
+        self.omegas = np.exp(2j * np.pi * np.arange(L) / L) * alpha ** (1.0 / L)
+        self.gamma = (alpha ** (np.arange(L) / L)).astype(np.complex128)
+        A, B = A.tocsr(), B.tocsr()
+        self.lus = [spla.splu((A - w * B).astype(np.complex128).tocsc()) for w in self.omegas]
+
+    def apply(self, v):
+        X = np.asarray(v, dtype=np.complex128).reshape(self.L, self.N)
+        X = self.gamma[:, None] * X
+        Xh = self._ifft(X, axis=0, norm="ortho")
+        for j in range(self.L):
+            Xh[j, :] = self.lus[j].solve(Xh[j, :])
+        Y = self._fft(Xh, axis=0, norm="ortho")
+        return (Y / self.gamma[:, None]).ravel()
+
+
+def pit_rhs(B, probe, L, b_step=None):
+    """Stacked right-hand side ``[B u_0 + b, 0, …, 0]`` of the full-system
+    solvers (``forward_model.py:155-192``): the probe enters through B alone,
+    without ``C_0 u_0`` (the reference's full-system form)."""
+    N = B.shape[0]
+    b0 = B @ np.asarray(probe, dtype=complex).ravel()
+    if b_step is not None:
+        b0 = b0 + b_step
+    return np.concatenate([b0, np.zeros(N * (L - 1), dtype=complex)])
+
+
+def full_system_solve(A, B, C2d, b):
+    """Direct solve of the space-time system ``M u = b`` (slice-major b and u):
+    ``M = kron(I, A) − kron(S, B) − diag(C) − subdiag(C)`` with S the
+    subdiagonal shift, factorised once — ``PWEFullLUSolver``
+    (``full_lu.py:72-172`` with ``forward_model.py:108-153,194-209``)."""
+    N, L = C2d.shape
+    S = sp.diags([np.ones(L - 1)], [-1], shape=(L, L), format="csr", dtype=complex)
+    M = sp.kron(sp.eye(L, format="csr"), A) - sp.kron(S, B)
+    cf = C2d.T.ravel()
+    M = M - sp.diags(cf) - sp.diags([cf[N:]], [-N], shape=M.shape)
+    return spla.spsolve(M.tocsc(), b)
+
+
+def pit_solve(A, B, C2d, probes, alpha=1e-2, atol=1e-8, rtol=1e-5, restart=20, warm_start=True):
+    """``PWEFullPinTSolver.solve`` for a probe stack: right-preconditioned GMRES
+    on ``M R y = b``, ``u = R y`` (``full_pint.py:179-275``; scipy's ``gmres``
+    with the reference's ``atol`` and its default ``rtol`` and ``restart``).
+    With ``warm_start`` each probe starts from the previous probe's ``y``, as
+    the reference's per-mode ``u0_cache`` does within one ``solve``.
+    Returns ``u`` (P, N, L+1) with the probe as column 0, and the GMRES
+    iteration counts."""
+    N, L = C2d.shape
+    R = PiTPreconditionerOracle(A, B, L, alpha)
+    M = spla.LinearOperator((N * L, N * L), dtype=np.complex128,
+                            matvec=lambda y: pit_matvec(A, B, C2d, R.apply(y)))
+    out = np.zeros((len(probes), N, L + 1), dtype=complex)
+    its = []
+    y0 = None
+    for p, probe in enumerate(probes):
+        b = pit_rhs(B, probe, L)
+        count = [0]
+
+        def cb(_r):
+            count[0] += 1
+
+        y, info = spla.gmres(M, b, atol=atol, rtol=rtol, restart=restart, x0=y0, callback=cb,
+                             callback_type="pr_norm")
+        u = R.apply(y).reshape(L, N).T
+        out[p, :, 0] = np.asarray(probe).ravel()
+        out[p, :, 1:] = u
+        its.append(count[0])
+        if warm_start:
+            y0 = y
+    return out, its
+
+
+# ---------------------------------------------------------------------------
 # Exact discrete adjoint and gradient (no reference counterpart; the
 # reference's adjoint differs, see ``reference_grad_least_squares``)
 # ---------------------------------------------------------------------------

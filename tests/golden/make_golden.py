@@ -3,7 +3,10 @@
 Run in a container that holds the reference checkout (read-only) at
 ``REF`` below::
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py [/path/to/reference [section ...]]
+
+With section names (the function names below) only those fixtures are
+regenerated.
 
 The reference is imported as-is; its two display-only imports (matplotlib,
 scikit-image) are satisfied by the stub packages in ``tests/golden/refstubs``.
@@ -288,6 +291,24 @@ def ms3pie_reference():
 # ---------------------------------------------------------------------------
 # 5. Random small 3D cases and scan orders
 # ---------------------------------------------------------------------------
+def pit_reference():
+    """PWEFullPinTSolver (full_pint.py): α-circulant right-preconditioned GMRES
+    on the space-time system, defaults (α = 1e-2, atol = 1e-8) and α = 0.1, on
+    the random 2D case; the FullLU solution of the same system beside it."""
+    from thick_ptycho.forward_model import PWEFullPinTSolver
+
+    g = np.load(os.path.join(HERE, "random2d.npz"))
+    ss = small_space_2d()
+    probes = create_ptycho_probes(ss)
+    n = g["n"]
+    out = {"n": n, "probes": probes[0], **sim_params(ss)}
+    for bc in ("neumann", "impedance", "dirichlet"):
+        out[f"pit_{bc}"] = PWEFullPinTSolver(ss, probes, bc_type=bc).solve(n=n)[0, 0]
+        out[f"pit_{bc}_alpha01"] = PWEFullPinTSolver(ss, probes, bc_type=bc, alpha=0.1).solve(n=n)[0, 0]
+        out[f"fulllu_{bc}"] = PWEFullLUSolver(ss, probes, bc_type=bc).solve(n=n)[0, 0]
+    save("pit2d", **out)
+
+
 def random_3d():
     rng = np.random.default_rng(77)
     cfg = SimulationConfig(
@@ -334,13 +355,9 @@ def geometry():
 
 
 if __name__ == "__main__":
-    geometry()
-    kat_2d()
-    random_2d()
-    config0_reference()
-    gradient_reference()
-    farfield_reference()
-    nlcg_reference()
-    ms3pie_reference()
-    kat_3d()
-    random_3d()
+    sections = [geometry, kat_2d, random_2d, config0_reference, gradient_reference, farfield_reference,
+                nlcg_reference, ms3pie_reference, kat_3d, random_3d, pit_reference]
+    wanted = set(sys.argv[2:])
+    for fn in sections:
+        if not wanted or fn.__name__ in wanted:
+            fn()

@@ -239,3 +239,24 @@ def test_ms_3d_reduces_to_reference_2d_multislice(golden):
         u3 = po.ms_forward_3d(n3, pr3, k, dx, 0.7, dz)
         for j in range(n2):
             assert rel(u3[:, j, :], g["ms_forward"][p]) < RTOL, (p, j)
+
+
+@pytest.mark.parametrize("bc", ["neumann", "impedance", "dirichlet"])
+def test_pit_gmres_matches_reference(golden, bc):
+    """The restated α-circulant PiT GMRES against PWEFullPinTSolver.solve (both
+    α), both against the FullLU solution of the same space-time system, and the
+    restated direct solve against FullLU itself."""
+    g = golden("pit2d")
+    N, dz, dx, k = int(g["nx"]), float(g["dz"]), float(g["dx"]), float(g["k"])
+    co = po.bc_coefficients(k, dx, dz, bc_type=bc)
+    A, B = po.step_matrices_1d(N, co, bc, dz)
+    C = po.object_contribution(g["n"], k, dz)
+    for alpha, key in ((1e-2, f"pit_{bc}"), (0.1, f"pit_{bc}_alpha01")):
+        u, its = po.pit_solve(A, B, C, g["probes"], alpha=alpha)
+        assert rel(u, g[key]) < RTOL, (alpha, rel(u, g[key]))
+        assert max(its) <= 10
+        assert rel(u, g[f"fulllu_{bc}"]) < 2e-5
+    L = C.shape[1]
+    for p in range(g["probes"].shape[0]):
+        x = po.full_system_solve(A, B, C, po.pit_rhs(B, g["probes"][p], L))
+        assert rel(x.reshape(L, N).T, g[f"fulllu_{bc}"][p][:, 1:]) < RTOL

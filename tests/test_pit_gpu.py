@@ -1,0 +1,93 @@
+"""GPU parity of the PiT space-time solve (the reference's PWEFullPinTSolver):
+against golden vectors of the unmodified reference (both α), the FullLU
+solution of the same system, the oracle's direct solve at N = 256 with a
+prime L = 127 (Bluestein z-DFT), a replaced right-hand side, and the warm
+start.
+
+Tolerances: the reference stops GMRES at ||r|| ≤ max(1e-8, 1e-5 ||b||); its
+own solutions sit ~1e-6 from the direct solve.  The GPU solve (complex64,
+fp64 Gram–Schmidt) must land within 2e-5 of both.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import pwe_oracle as po
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from thick_ptycho_b200 import SimulationGeometry  # noqa: E402
+from thick_ptycho_b200.pit import PWEGpuPiTSolver  # noqa: E402
+from thick_ptycho_b200.workloads import CONFIG0  # noqa: E402
+
+TOL = 2e-5
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _geo(g, num_probes):
+    return SimulationGeometry(dimension=2, nx=int(g["nx"]), nz=int(g["nz"]), dx=float(g["dx"]), dz=float(g["dz"]),
+                              k=float(g["k"]), num_probes=num_probes)
+
+
+@pytest.mark.parametrize("bc", ["neumann", "impedance", "dirichlet"])
+def test_pit_against_reference_golden(golden, bc):
+    g = golden("pit2d")
+    probes = g["probes"][None]
+    for alpha, key in ((1e-2, f"pit_{bc}"), (0.1, f"pit_{bc}_alpha01")):
+        s = PWEGpuPiTSolver(_geo(g, 4), probes, bc_type=bc, alpha=alpha)
+        u = s.solve(n=g["n"])[0, 0]
+        assert u.shape == g[key].shape
+        assert rel(u, g[key]) < TOL, (alpha, rel(u, g[key]))
+        assert rel(u, g[f"fulllu_{bc}"]) < TOL, (alpha, rel(u, g[f"fulllu_{bc}"]))
+        assert max(s.gmres_iterations) <= 12, s.gmres_iterations
+        assert max(s.pit.resid) <= 2e-5 * max(np.linalg.norm(probes[0], axis=1))
+
+
+def test_pit_config0_prime_steps_against_oracle():
+    """N = 256, nz = 128 (L = 127, prime: Bluestein length 256), 32 probes."""
+    w = CONFIG0
+    geo = w.geometry()
+    dn = w.delta_n()
+    probes = w.probes(geo)
+    s = PWEGpuPiTSolver(geo, probes[None], bc_type="impedance")
+    u = s.solve(n=1 - dn)[0, 0]
+    co = po.bc_coefficients(geo.k, 1.0, 1.0, bc_type="impedance")
+    A, B = po.step_matrices_1d(w.nx, co, "impedance", 1.0)
+    C = po.object_contribution(1 - dn, geo.k, 1.0)
+    L = w.nz - 1
+    for p in (0, 17, 31):
+        ref = po.full_system_solve(A, B, C, po.pit_rhs(B, probes[p], L)).reshape(L, w.nx).T
+        assert rel(u[p][:, 1:], ref) < TOL, (p, rel(u[p][:, 1:], ref))
+        assert np.array_equal(u[p][:, 0], probes[p].astype(np.complex64).astype(complex))
+    assert max(s.gmres_iterations) <= 20, s.gmres_iterations
+
+
+def test_pit_rhs_block_and_warm_start(golden):
+    g = golden("pit2d")
+    N, nz = int(g["nx"]), int(g["nz"])
+    L = nz - 1
+    co = po.bc_coefficients(float(g["k"]), float(g["dx"]), float(g["dz"]), bc_type="impedance")
+    A, B = po.step_matrices_1d(N, co, "impedance", float(g["dz"]))
+    C = po.object_contribution(g["n"], float(g["k"]), float(g["dz"]))
+    rng = np.random.default_rng(9)
+    rhs = rng.standard_normal((N, L)) + 1j * rng.standard_normal((N, L))
+    s = PWEGpuPiTSolver(_geo(g, 4), g["probes"][None], bc_type="impedance")
+    n = g["n"]
+    u = s._solve_single_probe(n=n, probe=g["probes"][0], rhs_block=rhs.ravel(order="F"))
+    ref = po.full_system_solve(A, B, C, rhs.T.ravel())
+    assert rel(u[:, 1:], ref.reshape(L, N).T) < TOL
+    # the same n object again: warm start from the last solution
+    u1 = s.solve(n=n)[0, 0]
+    it1 = list(s.gmres_iterations)
+    u2 = s.solve(n=n)[0, 0]
+    assert rel(u2, u1) < TOL and max(s.gmres_iterations) <= max(it1)
+    with pytest.raises(NotImplementedError):
+        s.solve(n=n, mode="adjoint")

@@ -6,6 +6,10 @@ Public entry points:
   (same constructor, ``solve``, ``_solve_single_probe``,
   ``prepare_solver_caches``, ``reset_cache``, ``get_gradient``,
   ``get_exit_waves``, ``get_farfield_intensities``).
+* :class:`PWEGpuPiTSolver` -- drop-in for ``PWEFullPinTSolver`` (the
+  α-circulant preconditioned space-time GMRES, 2D forward mode).
+* :class:`MSGpuSolver` -- drop-in for ``MSForwardModelSolver`` (2D, and 3D
+  spaces, which the reference rejects).
 * :class:`CN2D` -- batched 2D Crank–Nicolson propagation on device tensors.
 * :class:`SimulationGeometry` -- the geometry attributes the solvers read.
 
@@ -25,6 +29,14 @@ def __getattr__(name):
         from .solver import PWEGpuSolver
 
         return PWEGpuSolver
+    if name == "PWEGpuPiTSolver":
+        from .pit import PWEGpuPiTSolver
+
+        return PWEGpuPiTSolver
+    if name == "MSGpuSolver":
+        from .ms2d import MSGpuSolver
+
+        return MSGpuSolver
     if name == "CN2D":
         from .cn2d import CN2D
 

@@ -88,6 +88,23 @@ class TpMs2dOp(ctypes.Structure):
     ]
 
 
+class TpPitArgs(ctypes.Structure):
+    _fields_ = [
+        ("num_probes", ctypes.c_int32),
+        ("restart", ctypes.c_int32),
+        ("max_cycles", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("alpha", ctypes.c_double),
+        ("rtol", ctypes.c_double),
+        ("atol", ctypes.c_double),
+        ("probes", ctypes.c_void_p),
+        ("rhs", ctypes.c_void_p),
+        ("u", ctypes.c_void_p),
+        ("iters", ctypes.POINTER(ctypes.c_int32)),
+        ("resid", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
 class TpMs3dOp(ctypes.Structure):
     _fields_ = [
         ("n1", ctypes.c_int32),
@@ -176,6 +193,9 @@ SIGNATURES = [
                                     ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_void_p,
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
     ("tp_ms3d_workspace_bytes", ctypes.c_size_t, [ctypes.c_int32] * 3),
+    ("tp_pit_workspace_bytes", ctypes.c_size_t, [ctypes.c_int32] * 4),
+    ("tp_pit_solve", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_void_p, ctypes.c_int32,
+                                    ctypes.POINTER(TpPitArgs), ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
     ("tp_ms3d_transmission", ctypes.c_int, [ctypes.POINTER(TpMs3dOp), ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
                                             ctypes.c_void_p]),
     ("tp_ms3d_march", ctypes.c_int, [ctypes.POINTER(TpMs3dOp), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,

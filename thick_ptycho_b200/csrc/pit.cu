@@ -1,0 +1,720 @@
+// Parallel-in-time (PiT) space-time solve of the 2D paraxial march
+// (forward_model/pwe/solvers/full_pint.py:71-275 with
+// solvers/utils/_pint_utils.py:27-205).
+//
+// The L = nz - 1 Crank-Nicolson steps form one block-bidiagonal system
+//   M u = b,  M = diag(A - C_j) - subdiag(B + C_j),  b = [B u_0, 0, ..., 0]
+// (the full-system form: the probe enters through B alone).  It is solved by
+// restarted GMRES right-preconditioned with the alpha-circulant
+// R = Gamma^-1 F blockdiag((A - w_j B)^-1) F* Gamma: Gamma = diag(alpha^{j/L}),
+// F the unitary DFT along z, w_j = alpha^{1/L} e^{2 pi i j/L}, and A, B the
+// free-space step matrices (the reference's solver never updates them with C).
+//
+// B200 mapping: every probe's GMRES runs at once (batched Arnoldi); the
+// space-time matvec is one stencil kernel; the z-DFT of arbitrary length L is
+// Bluestein's chirp-z on the shared-memory FFT (length M, a power of two
+// >= 2L - 1); the L shifted tridiagonal block solves are one thread per
+// (probe, frequency) on fp64-built LU factors; the Gram-Schmidt inner
+// products (classical, twice) and norms accumulate in fp64.  The host loop
+// (Givens rotations, least squares) runs in double complex on the CPU; each
+// Arnoldi step reads back (j + 2) numbers per probe.
+//
+// The Krylov form is flexible GMRES: the preconditioned vectors z_j = R v_j
+// are kept and u = u_0 + Z s is built from them.  In exact arithmetic this is
+// the reference's right-preconditioned GMRES (u = R y); in fp32 it keeps the
+// solution consistent with the Arnoldi relation M Z = V H, whereas forming
+// R y at the end adds R's rounding (the z-DFTs and block solves) to the
+// residual: at N = 256, L = 127 that floor (~7e-5 ||b||) sat above the
+// reference's 1e-5 ||b|| tolerance and the restarts never met it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <vector>
+
+#include "fft.cuh"
+#include "tp_errors.h"
+#include "tpcuda.h"
+
+namespace tp {
+
+constexpr int kPitThreads = 256;
+constexpr int kPitMaxRestart = 64;
+constexpr int kPitDotGroup = 8;  // basis vectors per inner-product launch
+
+// K's tridiagonal from the 2D operator (fp32 copies for the stencils).
+struct PitK {
+  int N;
+  float2 off, diag, d0, dn, k01, knm;
+  __device__ __forceinline__ float2 sub(int i) const { return i == N - 1 ? knm : off; }  // K[i, i-1]
+  __device__ __forceinline__ float2 sup(int i) const { return i == 0 ? k01 : off; }      // K[i, i+1]
+  __device__ __forceinline__ float2 dia(int i) const { return i == 0 ? d0 : (i == N - 1 ? dn : diag); }
+};
+struct PitKd {  // the same in fp64 (block factorisation)
+  int N;
+  double2 off, diag, d0, dn, k01, knm;
+  __device__ __forceinline__ double2 sub(int i) const { return i == N - 1 ? knm : off; }
+  __device__ __forceinline__ double2 sup(int i) const { return i == 0 ? k01 : off; }
+  __device__ __forceinline__ double2 dia(int i) const { return i == 0 ? d0 : (i == N - 1 ? dn : diag); }
+};
+
+// (K v)_i of slice v (length N).
+__device__ __forceinline__ float2 pit_kv(const PitK &K, const float2 *v, int i) {
+  float2 r = cmul(K.dia(i), v[i]);
+  if (i > 0) r = cfma(K.sub(i), v[i - 1], r);
+  if (i < K.N - 1) r = cfma(K.sup(i), v[i + 1], r);
+  return r;
+}
+
+// ------------------------------------------------------------------ object
+struct PitObj {
+  int N, nz, L, n_obj, empty_px, exact, is_delta, dtype;
+  double k, dz;
+  const void *n;
+};
+
+__device__ __forceinline__ double2 pit_coef(const PitObj &o, double2 v) {
+  const double2 d = o.is_delta ? v : z2(v.x - 1.0, v.y);
+  if (!o.exact) return z2(o.k * d.y, -o.k * d.x);      // (k/i) (n - 1)
+  const double2 w = zadd(zscale(d, 2.0), zmul(d, d));  // n^2 - 1
+  return z2(0.5 * o.k * w.y, -0.5 * o.k * w.x);        // (k/2i) (n^2 - 1)
+}
+
+// C[j][i] = (dz/2) * (coef(n[r, j]) + coef(n[r, j+1])) / 2, r = i - empty_px
+// (base_simulation_space.py:315-383), slice-major (L, N).
+__global__ void pit_object_kernel(const PitObj o, float2 *__restrict__ C) {
+  const size_t total = (size_t)o.L * o.N;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(e / o.N), i = (int)(e % o.N);
+    const int r = i - o.empty_px;
+    double2 c = z2(0.0, 0.0);
+    if (r >= 0 && r < o.n_obj) {
+      auto ld = [&](int col) {
+        const size_t idx = (size_t)r * o.nz + col;
+        if (o.dtype == TP_C128) return static_cast<const double2 *>(o.n)[idx];
+        const float2 v = static_cast<const float2 *>(o.n)[idx];
+        return z2(v.x, v.y);
+      };
+      c = zscale(zadd(pit_coef(o, ld(j)), pit_coef(o, ld(j + 1))), 0.25 * o.dz);
+    }
+    C[e] = to_f2(c);
+  }
+}
+
+// ------------------------------------------------------------------ matvec
+// out = M v for the active probes: slice j gets
+// (A - C_j) v_j - (B + C_j) v_{j-1}, A = I - K, B = I + K (_pint_utils.py:27-54).
+__global__ void pit_matvec_kernel(const PitK K, int L, int P, const float2 *__restrict__ C,
+                                  const float2 *__restrict__ v, float2 *__restrict__ out, const int *active) {
+  const int N = K.N;
+  const size_t per = (size_t)L * N, total = per * P;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const int p = (int)(e / per);
+    if (active != nullptr && !active[p]) continue;
+    const size_t rem = e - (size_t)p * per;
+    const int j = (int)(rem / N), i = (int)(rem % N);
+    const float2 *vs = v + (size_t)p * per + (size_t)j * N;
+    const float2 c = C[(size_t)j * N + i];
+    const float2 x = vs[i];
+    float2 r = csub(csub(x, pit_kv(K, vs, i)), cmul(c, x));
+    if (j > 0) {
+      const float2 *ws = vs - N;
+      const float2 y = ws[i];
+      r = csub(r, cadd(cadd(y, pit_kv(K, ws, i)), cmul(c, y)));
+    }
+    out[e] = r;
+  }
+}
+
+// b[p] = [B u_0 + rhs_0, rhs_1, ...]: u_0 = probes[p] (or zero), rhs (P, L, N) or zero.
+__global__ void pit_rhs_kernel(const PitK K, int L, int P, const float2 *__restrict__ probes,
+                               const float2 *__restrict__ rhs, float2 *__restrict__ b) {
+  const int N = K.N;
+  const size_t per = (size_t)L * N, total = per * P;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const int p = (int)(e / per);
+    const size_t rem = e - (size_t)p * per;
+    float2 r = rhs ? rhs[e] : make_float2(0.f, 0.f);
+    if (rem < (size_t)N && probes != nullptr) {
+      const int i = (int)rem;
+      const float2 *u0 = probes + (size_t)p * N;
+      r = cadd(r, cadd(u0[i], pit_kv(K, u0, i)));
+    }
+    b[e] = r;
+  }
+}
+
+// ------------------------------------------------------------ preconditioner
+// Tables: gamma_j = alpha^{j/L}; chirp c_n = exp(-i pi n^2 / L) (n^2 taken
+// mod 2L in integers so the fp64 angle stays small); the Bluestein kernel
+// b_m = conj(c_m) for |m| < L wrapped into [0, M); twiddles of length M.
+__global__ void pit_tables_kernel(int L, int M, double alpha, float *gamma, float2 *chirp, float2 *bker, float2 *tw) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (int j = tid; j < L; j += nth) {
+    gamma[j] = (float)pow(alpha, (double)j / (double)L);
+    const long long m = ((long long)j * j) % (2LL * L);
+    double s, c;
+    sincospi(-(double)m / (double)L, &s, &c);
+    chirp[j] = make_float2((float)c, (float)s);
+  }
+  for (int m = tid; m < M; m += nth) {
+    int n = -1;
+    if (m < L) n = m;
+    else if (m > M - L) n = M - m;
+    float2 v = make_float2(0.f, 0.f);
+    if (n >= 0) {
+      const long long q = ((long long)n * n) % (2LL * L);
+      double s, c;
+      sincospi((double)q / (double)L, &s, &c);  // conj(c_n)
+      v = make_float2((float)c, (float)s);
+    }
+    bker[m] = v;
+    double s, c;
+    sincospi(-2.0 * (double)m / (double)M, &s, &c);
+    tw[m] = make_float2((float)c, (float)s);
+  }
+}
+
+// Unitary DFT along z by Bluestein's chirp-z, cpc columns per CTA.
+//   INV (into the block domain): x_j = gamma_j v[p][j][i] (slice-major in),
+//     out Xh[p][i][k] = (1/sqrt L) sum_j x_j e^{+2 pi i jk/L}   (i-major out)
+//   !INV (back):  x_k = Xh[p][i][k],
+//     out[p][j][i] = (1/sqrt L) sum_k x_k e^{-2 pi i jk/L} / gamma_j
+// The inverse direction is conj(DFT(conj x)).  Grid (ceil(N/cpc), P).
+template <bool INV>
+__global__ void __launch_bounds__(kPitThreads) pit_zdft_kernel(const FftPlan pl, int N, int L, int cpc,
+                                                               const float2 *__restrict__ in, float2 *__restrict__ out,
+                                                               const float *__restrict__ gamma,
+                                                               const float2 *__restrict__ chirp,
+                                                               const float2 *__restrict__ bhat,
+                                                               const float2 *__restrict__ twg, const int *active) {
+  extern __shared__ __align__(16) float2 zsm[];
+  const int M = pl.n, p = blockIdx.y, i0 = blockIdx.x * cpc;
+  if (active != nullptr && !active[p]) return;
+  float2 *tw = zsm, *a = tw + M, *b = a + cpc * M;
+  load_twiddles(tw, twg, M);
+  const size_t per = (size_t)L * N;
+  for (int e = threadIdx.x; e < cpc * M; e += blockDim.x) a[e] = make_float2(0.f, 0.f);
+  __syncthreads();
+  if (INV) {
+    for (int e = threadIdx.x; e < cpc * L; e += blockDim.x) {
+      const int q = e % cpc, j = e / cpc;  // coalesced over q
+      if (i0 + q >= N) continue;
+      const float2 v = in[(size_t)p * per + (size_t)j * N + i0 + q];
+      const float g = gamma[j];
+      a[q * M + j] = cmul(make_float2(g * v.x, -g * v.y), chirp[j]);  // conj(x) c_j
+    }
+  } else {
+    for (int e = threadIdx.x; e < cpc * L; e += blockDim.x) {
+      const int q = e / L, k = e % L;  // coalesced over k
+      if (i0 + q >= N) continue;
+      a[q * M + k] = cmul(in[(size_t)p * per + (size_t)(i0 + q) * L + k], chirp[k]);
+    }
+  }
+  __syncthreads();
+  float2 *F = fft_block(a, b, pl, tw, false, cpc, threadIdx.x, blockDim.x);
+  float2 *o = (F == a) ? b : a;
+  for (int e = threadIdx.x; e < cpc * M; e += blockDim.x) F[e] = cmul(F[e], bhat[e % M]);
+  __syncthreads();
+  const float2 *R = fft_block(F, o, pl, tw, true, cpc, threadIdx.x, blockDim.x);
+  const float sc = 1.f / ((float)M * sqrtf((float)L));
+  if (INV) {
+    for (int e = threadIdx.x; e < cpc * L; e += blockDim.x) {
+      const int q = e / L, k = e % L;
+      if (i0 + q >= N) continue;
+      const float2 X = cmul(R[q * M + k], chirp[k]);
+      out[(size_t)p * per + (size_t)(i0 + q) * L + k] = make_float2(sc * X.x, -sc * X.y);  // conj
+    }
+  } else {
+    for (int e = threadIdx.x; e < cpc * L; e += blockDim.x) {
+      const int q = e % cpc, j = e / cpc;
+      if (i0 + q >= N) continue;
+      const float2 X = cmul(R[q * M + j], chirp[j]);
+      const float s = sc / gamma[j];
+      out[(size_t)p * per + (size_t)j * N + i0 + q] = make_float2(s * X.x, s * X.y);
+    }
+  }
+}
+
+// LU factors of the L blocks (A - w_k B) = (1 - w_k) I - (1 + w_k) K, fp64
+// Thomas elimination, stored as float4 (m_i, 1/d_i) at [i][k].
+__global__ void pit_factor_kernel(const PitKd K, int L, double alpha_root, float4 *__restrict__ F) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= L) return;
+  double s, c;
+  sincospi(2.0 * (double)k / (double)L, &s, &c);
+  const double2 w = z2(alpha_root * c, alpha_root * s);
+  const double2 omw = z2(1.0 - w.x, -w.y), opw = z2(1.0 + w.x, w.y);
+  auto dval = [&](int i) { return zsub(omw, zmul(opw, K.dia(i))); };
+  double2 d = dval(0);
+  double2 dinv = zdiv(z2(1.0, 0.0), d);
+  F[k] = make_float4(0.f, 0.f, (float)dinv.x, (float)dinv.y);
+  for (int i = 1; i < K.N; ++i) {
+    const double2 a = zneg(zmul(opw, K.sub(i)));          // row i, column i-1
+    const double2 cprev = zneg(zmul(opw, K.sup(i - 1)));  // row i-1, column i
+    const double2 m = zmul(a, dinv);
+    d = zsub(dval(i), zmul(m, cprev));
+    dinv = zdiv(z2(1.0, 0.0), d);
+    F[(size_t)i * L + k] = make_float4((float)m.x, (float)m.y, (float)dinv.x, (float)dinv.y);
+  }
+}
+
+// Block solves in place on Xh (P, N, L): thread (p, k) solves along i.
+__global__ void pit_block_solve_kernel(const PitK K, int L, int P, double alpha_root, const float4 *__restrict__ F,
+                                       float2 *__restrict__ Xh, const int *active) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= L * P) return;
+  const int p = t / L, k = t % L;
+  if (active != nullptr && !active[p]) return;
+  const int N = K.N;
+  double s, c;
+  sincospi(2.0 * (double)k / (double)L, &s, &c);
+  const float2 opw = make_float2((float)(1.0 + alpha_root * c), (float)(alpha_root * s));
+  float2 *x = Xh + (size_t)p * N * L + k;
+  float2 y = x[0];
+  for (int i = 1; i < N; ++i) {
+    const float4 f = F[(size_t)i * L + k];
+    y = cfnma(make_float2(f.x, f.y), y, x[(size_t)i * L]);
+    x[(size_t)i * L] = y;
+  }
+  {
+    const float4 f = F[(size_t)(N - 1) * L + k];
+    y = cmul(y, make_float2(f.z, f.w));
+    x[(size_t)(N - 1) * L] = y;
+  }
+  for (int i = N - 2; i >= 0; --i) {
+    const float4 f = F[(size_t)i * L + k];
+    const float2 ci = cmul(make_float2(-opw.x, -opw.y), K.sup(i));  // row i, column i+1
+    y = cmul(cfnma(ci, y, x[(size_t)i * L]), make_float2(f.z, f.w));
+    x[(size_t)i * L] = y;
+  }
+}
+
+// ------------------------------------------------------------------ Krylov
+// h[p][r0 + r] += <V_{r0+r}[p], w[p]> (fp64) for r < min(kPitDotGroup, nv - r0).
+__global__ void __launch_bounds__(kPitThreads) pit_dots_kernel(size_t n, int P, const float2 *__restrict__ V,
+                                                               size_t vstride, int r0, int nv,
+                                                               const float2 *__restrict__ w, double2 *h, int hld,
+                                                               const int *active) {
+  const int p = blockIdx.y;
+  if (active != nullptr && !active[p]) return;
+  __shared__ double red[kPitThreads / 32][2 * kPitDotGroup];
+  double acc[2 * kPitDotGroup];
+#pragma unroll
+  for (int r = 0; r < 2 * kPitDotGroup; ++r) acc[r] = 0.0;
+  const int cnt = min(kPitDotGroup, nv - r0);
+  const float2 *wp = w + (size_t)p * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const float2 x = wp[e];
+#pragma unroll
+    for (int r = 0; r < kPitDotGroup; ++r) {
+      if (r < cnt) {
+        const float2 v = V[(size_t)(r0 + r) * vstride + (size_t)p * n + e];
+        acc[2 * r] += (double)v.x * x.x + (double)v.y * x.y;  // conj(v) x
+        acc[2 * r + 1] += (double)v.x * x.y - (double)v.y * x.x;
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int r = 0; r < 2 * kPitDotGroup; ++r) {
+    double v = acc[r];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) red[wid][r] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * cnt) {
+    double s = 0.0;
+    for (int q = 0; q < kPitThreads / 32; ++q) s += red[q][threadIdx.x];
+    double *dst = reinterpret_cast<double *>(&h[(size_t)p * hld + r0 + (threadIdx.x >> 1)]) + (threadIdx.x & 1);
+    atomicAdd(dst, s);
+  }
+}
+
+// w[p] += sign * sum_{r < nv} coef[p][r] V_r[p]  (coef fp64, per probe)
+__global__ void __launch_bounds__(kPitThreads) pit_combine_kernel(size_t n, int P, const float2 *__restrict__ V,
+                                                                  size_t vstride, int nv,
+                                                                  const double2 *__restrict__ coef, int cld,
+                                                                  float sign, float2 *__restrict__ w,
+                                                                  const int *active) {
+  const int p = blockIdx.y;
+  if (active != nullptr && !active[p]) return;
+  __shared__ float2 cf[kPitMaxRestart + 1];
+  for (int r = threadIdx.x; r < nv; r += blockDim.x) {
+    const double2 c = coef[(size_t)p * cld + r];
+    cf[r] = make_float2((float)(sign * c.x), (float)(sign * c.y));
+  }
+  __syncthreads();
+  float2 *wp = w + (size_t)p * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    float2 acc = wp[e];
+    for (int r = 0; r < nv; ++r) acc = cfma(cf[r], V[(size_t)r * vstride + (size_t)p * n + e], acc);
+    wp[e] = acc;
+  }
+}
+
+// nrm[p] += ||x[p]||^2 (fp64)
+__global__ void __launch_bounds__(kPitThreads) pit_norm_kernel(size_t n, int P, const float2 *__restrict__ x,
+                                                               double *nrm, const int *active) {
+  const int p = blockIdx.y;
+  if (active != nullptr && !active[p]) return;
+  __shared__ double red[kPitThreads / 32];
+  double acc = 0.0;
+  const float2 *xp = x + (size_t)p * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const float2 v = xp[e];
+    acc += (double)v.x * v.x + (double)v.y * v.y;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int q = 0; q < kPitThreads / 32; ++q) s += red[q];
+    atomicAdd(&nrm[p], s);
+  }
+}
+
+// out[p] = s[p] * x[p]   |   out[p] = x[p] - y[p] (s == NULL)
+__global__ void pit_scale_kernel(size_t n, int P, const float2 *__restrict__ x, const float2 *__restrict__ y,
+                                 const double *s, float2 *__restrict__ out, const int *active) {
+  const size_t total = n * P;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const int p = (int)(e / n);
+    if (active != nullptr && !active[p]) continue;
+    if (s != nullptr) {
+      const float f = (float)s[p];
+      out[e] = make_float2(f * x[e].x, f * x[e].y);
+    } else {
+      out[e] = csub(x[e], y[e]);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ host
+struct PitWork {
+  float2 *V, *Z, *w, *xh, *b, *C, *chirp, *bker, *bhat, *tw;
+  float4 *F;
+  float *gamma;
+  double2 *h;
+  double *nrm, *s;
+  int *active;
+  size_t bytes;
+};
+
+static size_t pit_a256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+static int pit_fft_len(int L) {
+  int M = 4;
+  while (M < 2 * L - 1) M *= 2;
+  return M;
+}
+
+static PitWork pit_layout(char *base, int N, int L, int P, int m) {
+  PitWork w{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char *p = base ? base + off : nullptr;
+    off += pit_a256(bytes);
+    return p;
+  };
+  const size_t n = (size_t)N * L, vec = n * P * sizeof(float2);
+  const int M = pit_fft_len(L);
+  w.V = reinterpret_cast<float2 *>(take(vec * (m + 1)));
+  w.Z = reinterpret_cast<float2 *>(take(vec * m));
+  w.w = reinterpret_cast<float2 *>(take(vec));
+  w.xh = reinterpret_cast<float2 *>(take(vec));
+  w.b = reinterpret_cast<float2 *>(take(vec));
+  w.C = reinterpret_cast<float2 *>(take(n * sizeof(float2)));
+  w.F = reinterpret_cast<float4 *>(take(n * sizeof(float4)));
+  w.gamma = reinterpret_cast<float *>(take((size_t)L * sizeof(float)));
+  w.chirp = reinterpret_cast<float2 *>(take((size_t)L * sizeof(float2)));
+  w.bker = reinterpret_cast<float2 *>(take((size_t)M * sizeof(float2)));
+  w.bhat = reinterpret_cast<float2 *>(take((size_t)M * sizeof(float2)));
+  w.tw = reinterpret_cast<float2 *>(take((size_t)M * sizeof(float2)));
+  w.h = reinterpret_cast<double2 *>(take((size_t)P * (kPitMaxRestart + 1) * sizeof(double2)));
+  w.nrm = reinterpret_cast<double *>(take((size_t)P * sizeof(double)));
+  w.s = reinterpret_cast<double *>(take((size_t)P * sizeof(double)));
+  w.active = reinterpret_cast<int *>(take((size_t)P * sizeof(int)));
+  w.bytes = off;
+  return w;
+}
+
+static PitK pit_k(const tp_cn2d_op *op) {
+  auto f = [](const double v[2]) { return make_float2((float)v[0], (float)v[1]); };
+  return PitK{op->n, f(op->k_off), f(op->k_diag), f(op->k_d0), f(op->k_dn), f(op->k_01), f(op->k_nm)};
+}
+static PitKd pit_kd(const tp_cn2d_op *op) {
+  auto f = [](const double v[2]) { return make_double2(v[0], v[1]); };
+  return PitKd{op->n, f(op->k_off), f(op->k_diag), f(op->k_d0), f(op->k_dn), f(op->k_01), f(op->k_nm)};
+}
+
+static int pit_grid(size_t total) {
+  const size_t g = (total + kPitThreads - 1) / kPitThreads;
+  return (int)(g < 4 * 148 ? (g < 1 ? 1 : g) : 4 * 148);
+}
+
+// Device-side pieces of one solve: the preconditioner, the space-time matvec
+// and the batched Gram-Schmidt kernels, over all probes.
+class PitSolver {
+ public:
+  PitSolver(const tp_cn2d_op *op, int L, int P, const PitWork &w, cudaStream_t st)
+      : K_(pit_k(op)), kd_(pit_kd(op)), N_(op->n), L_(L), P_(P), n_((size_t)op->n * L), w_(w), st_(st) {
+    M_ = pit_fft_len(L);
+    pl_ = make_fft_plan(M_);
+    cpc_ = std::max(1, std::min(16, 4096 / M_));
+    zsmem_ = (size_t)(M_ + 2 * cpc_ * M_) * sizeof(float2);
+  }
+
+  int setup(double alpha) {
+    alpha_root_ = pow(alpha, 1.0 / (double)L_);
+    pit_tables_kernel<<<8, 256, 0, st_>>>(L_, M_, alpha, w_.gamma, w_.chirp, w_.bker, w_.tw);
+    TP_CHECK_CUDA(cudaGetLastError());
+    int rc = tp_fft1d(M_, 1, w_.bker, w_.bhat, 0, reinterpret_cast<tp_stream_t>(st_));
+    if (rc) return rc;
+    pit_factor_kernel<<<(L_ + 127) / 128, 128, 0, st_>>>(kd_, L_, alpha_root_, w_.F);
+    TP_CHECK_CUDA(cudaGetLastError());
+    TP_CHECK_CUDA(cudaFuncSetAttribute(pit_zdft_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem_));
+    TP_CHECK_CUDA(cudaFuncSetAttribute(pit_zdft_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem_));
+    return TP_OK;
+  }
+
+  // out = R in (the preconditioner), active probes only.
+  int precond(const float2 *in, float2 *out) {
+    const dim3 gz((N_ + cpc_ - 1) / cpc_, P_);
+    pit_zdft_kernel<true><<<gz, kPitThreads, zsmem_, st_>>>(pl_, N_, L_, cpc_, in, w_.xh, w_.gamma, w_.chirp,
+                                                            w_.bhat, w_.tw, w_.active);
+    pit_block_solve_kernel<<<(L_ * P_ + 127) / 128, 128, 0, st_>>>(K_, L_, P_, alpha_root_, w_.F, w_.xh, w_.active);
+    pit_zdft_kernel<false><<<gz, kPitThreads, zsmem_, st_>>>(pl_, N_, L_, cpc_, w_.xh, out, w_.gamma, w_.chirp,
+                                                             w_.bhat, w_.tw, w_.active);
+    return check_cuda(cudaGetLastError(), "pit preconditioner launch");
+  }
+  // out = M in
+  int matvec(const float2 *in, float2 *out) {
+    pit_matvec_kernel<<<pit_grid(n_ * P_), kPitThreads, 0, st_>>>(K_, L_, P_, w_.C, in, out, w_.active);
+    return check_cuda(cudaGetLastError(), "pit matvec launch");
+  }
+  // out[p] = ||x[p]||^2 on the host
+  int norms(const float2 *x, std::vector<double> &out) {
+    TP_CHECK_CUDA(cudaMemsetAsync(w_.nrm, 0, P_ * sizeof(double), st_));
+    pit_norm_kernel<<<dim3(red_blocks(), P_), kPitThreads, 0, st_>>>(n_, P_, x, w_.nrm, w_.active);
+    TP_CHECK_CUDA(cudaGetLastError());
+    out.resize(P_);
+    TP_CHECK_CUDA(cudaMemcpyAsync(out.data(), w_.nrm, P_ * sizeof(double), cudaMemcpyDeviceToHost, st_));
+    TP_CHECK_CUDA(cudaStreamSynchronize(st_));
+    return TP_OK;
+  }
+  // h[p][0..nv) = V_{0..nv}^H w (device)
+  int dots(int nv, const float2 *w) {
+    TP_CHECK_CUDA(cudaMemsetAsync(w_.h, 0, (size_t)P_ * (kPitMaxRestart + 1) * sizeof(double2), st_));
+    for (int r0 = 0; r0 < nv; r0 += kPitDotGroup)
+      pit_dots_kernel<<<dim3(red_blocks(), P_), kPitThreads, 0, st_>>>(n_, P_, w_.V, n_ * P_, r0, nv, w, w_.h,
+                                                                      kPitMaxRestart + 1, w_.active);
+    return check_cuda(cudaGetLastError(), "pit dots launch");
+  }
+  // target += sign * sum_r h[p][r] basis_r[p]
+  int combine(const float2 *basis, int nv, float sign, float2 *target) {
+    pit_combine_kernel<<<dim3(red_blocks(), P_), kPitThreads, 0, st_>>>(n_, P_, basis, n_ * P_, nv, w_.h,
+                                                                       kPitMaxRestart + 1, sign, target, w_.active);
+    return check_cuda(cudaGetLastError(), "pit combine launch");
+  }
+  int red_blocks() const {
+    const size_t g = (n_ + kPitThreads - 1) / kPitThreads;
+    return (int)(g < 64 ? g : 64);
+  }
+
+  PitK K_;
+  PitKd kd_;
+  int N_, L_, P_, M_ = 0, cpc_ = 1;
+  size_t n_, zsmem_ = 0;
+  double alpha_root_ = 1.0;
+  FftPlan pl_{};
+  PitWork w_;
+  cudaStream_t st_;
+};
+
+}  // namespace tp
+
+using namespace tp;
+
+extern "C" size_t tp_pit_workspace_bytes(int32_t n, int32_t nz, int32_t num_probes, int32_t restart) {
+  if (n < 2 || nz < 3 || num_probes < 1) return 0;
+  const int m = restart > 0 ? restart : 20;
+  if (m > kPitMaxRestart) return 0;
+  return pit_layout(nullptr, n, nz - 1, num_probes, m).bytes;
+}
+
+extern "C" int tp_pit_solve(const tp_cn2d_op *op, const void *n_field, int32_t n_dtype, const tp_pit_args *a,
+                            void *workspace, size_t workspace_bytes, tp_stream_t stream) {
+  if (op == nullptr || a == nullptr || n_field == nullptr || workspace == nullptr)
+    return set_error(TP_ERR_INVALID, "tp_pit_solve: NULL argument");
+  const int N = op->n, L = op->nz - 1, P = a->num_probes;
+  const int m = a->restart > 0 ? a->restart : 20;
+  if (N < 2 || L < 2 || P < 1) return set_error(TP_ERR_INVALID, "tp_pit_solve: N=%d, nz=%d, P=%d", N, op->nz, P);
+  if (m > kPitMaxRestart) return set_error(TP_ERR_INVALID, "restart=%d > %d", m, kPitMaxRestart);
+  if (2 * L - 1 > kFftMaxN)
+    return set_error(TP_ERR_UNSUPPORTED, "PiT needs nz - 1 <= %d (got %d)", (kFftMaxN + 1) / 2, L);
+  if (a->u == nullptr) return set_error(TP_ERR_INVALID, "tp_pit_solve: u is required");
+  if (op->n_obj + 2 * op->empty_px != N) return set_error(TP_ERR_INVALID, "n_obj + 2 empty_px != n");
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255u) != 0)
+    return set_error(TP_ERR_INVALID, "workspace must be 256-byte aligned");
+  const PitWork w = pit_layout(static_cast<char *>(workspace), N, L, P, m);
+  if (workspace_bytes < w.bytes)
+    return set_error(TP_ERR_WORKSPACE, "PiT workspace %zu B < %zu B", workspace_bytes, w.bytes);
+  const double alpha = a->alpha > 0 ? a->alpha : 1e-2;
+  const double rtol = a->rtol > 0 ? a->rtol : 1e-5, atol = a->atol > 0 ? a->atol : 1e-8;
+  const int max_cycles = a->max_cycles > 0 ? a->max_cycles : 1000;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const size_t n = (size_t)N * L;
+
+  PitSolver S(op, L, P, w, st);
+  // object contribution (slice-major) and right-hand sides
+  PitObj o{N, op->nz, L, op->n_obj, op->empty_px, op->exact_ref_coeff, op->field_is_delta, n_dtype, op->k, op->dz,
+           n_field};
+  pit_object_kernel<<<pit_grid(n), kPitThreads, 0, st>>>(o, w.C);
+  pit_rhs_kernel<<<pit_grid(n * P), kPitThreads, 0, st>>>(S.K_, L, P, static_cast<const float2 *>(a->probes),
+                                                           static_cast<const float2 *>(a->rhs), w.b);
+  TP_CHECK_CUDA(cudaGetLastError());
+  int rc = S.setup(alpha);
+  if (rc) return rc;
+
+  float2 *u = static_cast<float2 *>(a->u);
+  std::vector<int> active(P, 1), iters(P, 0);
+  std::vector<double> tol(P), bn, rn;
+  TP_CHECK_CUDA(cudaMemcpyAsync(w.active, active.data(), P * sizeof(int), cudaMemcpyHostToDevice, st));
+  rc = S.norms(w.b, bn);
+  if (rc) return rc;
+  for (int p = 0; p < P; ++p) tol[p] = std::fmax(atol, rtol * std::sqrt(bn[p]));
+
+  using cd = std::complex<double>;
+  std::vector<cd> H((size_t)P * (m + 1) * m), cs((size_t)P * m), sn((size_t)P * m), g((size_t)P * (m + 1));
+  std::vector<double2> hh((size_t)P * (kPitMaxRestart + 1));
+  std::vector<int> inner(P), kdim(P);
+  auto Hat = [&](int p, int r, int c) -> cd & { return H[((size_t)p * (m + 1) + r) * m + c]; };
+
+  for (int cyc = 0; cyc < max_cycles; ++cyc) {
+    // r = b - M u for every probe still running
+    rc = S.matvec(u, w.w);
+    if (rc) return rc;
+    pit_scale_kernel<<<pit_grid(n * P), kPitThreads, 0, st>>>(n, P, w.b, w.w, nullptr, w.w, w.active);
+    rc = S.norms(w.w, rn);
+    if (rc) return rc;
+    bool any = false;
+    for (int p = 0; p < P; ++p) {
+      if (!active[p]) continue;
+      if (std::sqrt(rn[p]) <= tol[p]) active[p] = 0;
+      else any = true;
+    }
+    if (!any) break;
+    TP_CHECK_CUDA(cudaMemcpyAsync(w.active, active.data(), P * sizeof(int), cudaMemcpyHostToDevice, st));
+    std::vector<double> sc(P, 0.0);
+    for (int p = 0; p < P; ++p) {
+      inner[p] = active[p];
+      kdim[p] = 0;
+      std::fill(g.begin() + (size_t)p * (m + 1), g.begin() + (size_t)(p + 1) * (m + 1), cd(0.0));
+      if (active[p]) {
+        const double beta = std::sqrt(rn[p]);
+        g[(size_t)p * (m + 1)] = beta;
+        sc[p] = 1.0 / beta;
+      }
+    }
+    TP_CHECK_CUDA(cudaMemcpyAsync(w.s, sc.data(), P * sizeof(double), cudaMemcpyHostToDevice, st));
+    pit_scale_kernel<<<pit_grid(n * P), kPitThreads, 0, st>>>(n, P, w.w, nullptr, w.s, w.V, w.active);
+    for (int j = 0; j < m; ++j) {
+      float2 *Vj = w.V + (size_t)j * n * P, *Zj = w.Z + (size_t)j * n * P;
+      rc = S.precond(Vj, Zj);
+      if (rc) return rc;
+      rc = S.matvec(Zj, w.w);
+      if (rc) return rc;
+      // classical Gram-Schmidt, twice
+      std::vector<cd> hsum((size_t)P * (j + 1), cd(0.0));
+      for (int pass = 0; pass < 2; ++pass) {
+        rc = S.dots(j + 1, w.w);
+        if (rc) return rc;
+        rc = S.combine(w.V, j + 1, -1.f, w.w);
+        if (rc) return rc;
+        TP_CHECK_CUDA(cudaMemcpyAsync(hh.data(), w.h, hh.size() * sizeof(double2), cudaMemcpyDeviceToHost, st));
+        TP_CHECK_CUDA(cudaStreamSynchronize(st));
+        for (int p = 0; p < P; ++p)
+          for (int r = 0; r <= j; ++r) {
+            const double2 v = hh[(size_t)p * (kPitMaxRestart + 1) + r];
+            hsum[(size_t)p * (j + 1) + r] += cd(v.x, v.y);
+          }
+      }
+      rc = S.norms(w.w, rn);
+      if (rc) return rc;
+      bool cont = false;
+      for (int p = 0; p < P; ++p) {
+        sc[p] = 0.0;
+        if (!inner[p]) continue;
+        for (int r = 0; r <= j; ++r) Hat(p, r, j) = hsum[(size_t)p * (j + 1) + r];
+        const double eta = std::sqrt(rn[p]);
+        Hat(p, j + 1, j) = eta;
+        cd *csp = &cs[(size_t)p * m], *snp = &sn[(size_t)p * m], *gp = &g[(size_t)p * (m + 1)];
+        for (int r = 0; r < j; ++r) {  // previous rotations
+          const cd h0 = Hat(p, r, j), h1 = Hat(p, r + 1, j);
+          Hat(p, r, j) = std::conj(csp[r]) * h0 + std::conj(snp[r]) * h1;
+          Hat(p, r + 1, j) = -snp[r] * h0 + csp[r] * h1;
+        }
+        const cd a0 = Hat(p, j, j), a1 = Hat(p, j + 1, j);
+        const double den = std::sqrt(std::norm(a0) + std::norm(a1));
+        csp[j] = den > 0 ? a0 / den : cd(1.0);
+        snp[j] = den > 0 ? a1 / den : cd(0.0);
+        Hat(p, j, j) = den;
+        Hat(p, j + 1, j) = 0.0;
+        gp[j + 1] = -snp[j] * gp[j];
+        gp[j] = std::conj(csp[j]) * gp[j];
+        iters[p] += 1;
+        kdim[p] = j + 1;
+        if (std::abs(gp[j + 1]) <= tol[p] || eta == 0.0 || j == m - 1) {
+          inner[p] = 0;
+        } else {
+          sc[p] = 1.0 / eta;
+          cont = true;
+        }
+      }
+      if (!cont) break;
+      // V_{j+1} = w / eta for the probes that continue
+      TP_CHECK_CUDA(cudaMemcpyAsync(w.active, inner.data(), P * sizeof(int), cudaMemcpyHostToDevice, st));
+      TP_CHECK_CUDA(cudaMemcpyAsync(w.s, sc.data(), P * sizeof(double), cudaMemcpyHostToDevice, st));
+      pit_scale_kernel<<<pit_grid(n * P), kPitThreads, 0, st>>>(n, P, w.w, nullptr, w.s, Vj + n * P, w.active);
+    }
+    // u += Z_k s_k, s_k solving the rotated triangular system
+    std::fill(hh.begin(), hh.end(), make_double2(0.0, 0.0));
+    int kmax = 0;
+    for (int p = 0; p < P; ++p) {
+      if (!active[p] || kdim[p] == 0) continue;
+      const int k = kdim[p];
+      std::vector<cd> sv(k);
+      for (int r = k - 1; r >= 0; --r) {
+        cd acc = g[(size_t)p * (m + 1) + r];
+        for (int c = r + 1; c < k; ++c) acc -= Hat(p, r, c) * sv[c];
+        sv[r] = acc / Hat(p, r, r);
+      }
+      for (int r = 0; r < k; ++r) hh[(size_t)p * (kPitMaxRestart + 1) + r] = make_double2(sv[r].real(), sv[r].imag());
+      if (k > kmax) kmax = k;
+    }
+    TP_CHECK_CUDA(cudaMemcpyAsync(w.active, active.data(), P * sizeof(int), cudaMemcpyHostToDevice, st));
+    TP_CHECK_CUDA(cudaMemcpyAsync(w.h, hh.data(), hh.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
+    if (kmax > 0) {
+      rc = S.combine(w.Z, kmax, 1.f, u);
+      if (rc) return rc;
+    }
+  }
+  // final true residuals
+  std::fill(active.begin(), active.end(), 1);
+  TP_CHECK_CUDA(cudaMemcpyAsync(w.active, active.data(), P * sizeof(int), cudaMemcpyHostToDevice, st));
+  if (a->resid != nullptr) {
+    rc = S.matvec(u, w.w);
+    if (rc) return rc;
+    pit_scale_kernel<<<pit_grid(n * P), kPitThreads, 0, st>>>(n, P, w.b, w.w, nullptr, w.w, w.active);
+    rc = S.norms(w.w, rn);
+    if (rc) return rc;
+    for (int p = 0; p < P; ++p) a->resid[p] = std::sqrt(rn[p]);
+  }
+  if (a->iters != nullptr)
+    for (int p = 0; p < P; ++p) a->iters[p] = iters[p];
+  TP_CHECK_CUDA(cudaStreamSynchronize(st));
+  return check_cuda(cudaGetLastError(), "tp_pit_solve");
+}
