@@ -42,6 +42,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "probe·slice solves/s fwd+adj (2D CN, complex64, exact adjoint + fused gradient)"
+# DRAM bytes (read + write) of one exact-adjoint march launch at N = 2048, nz = 1024, 512
+# probes: an ncu capture at nz = 128 measured 1.095 GB for 127 slices (traffic grows with the
+# slices), scaled by 1023/127 (profiles/cn2d_team_2048x1024_p512_launches.md).
+ADJ_TRAFFIC_BYTES_2048x1024_P512 = 1.095e9 * 1023 / 127
 UNIT = "probe·slice/s"
 
 
@@ -468,7 +472,9 @@ def run_ours(a):
                            "step_total": ms_max / a.steps},
             "roofline": {"kernel": "cn2d_march_kernel (" + ("adjoint_exact+grad" if dom == "adj" else "forward") + ")",
                          "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "peak_kind": kind, "traffic": None,
+                         "peak_kind": kind,
+                         "traffic": (ADJ_TRAFFIC_BYTES_2048x1024_P512
+                                     if dom == "adj" and (N, nz, P) == (2048, 1024, 512) else None),
                          "algorithmic_bytes_per_launch": dom_bytes},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             # per step: 2 factorisations, 2 marches, the amplitude residual, the node mapping
