@@ -114,6 +114,6 @@ int team_spike_rows(const tp_cn2d_op *op, int M);
 
 // Team-path launcher (cn2d_team.cu).
 int launch_team_march(const Partition &pt, MarchParams &mp, bool lagged, cudaStream_t st);
-size_t team_smem_bytes(const Partition &pt, int trunc, int Q, int TM, bool grad);
+size_t team_smem_bytes(const Partition &pt, int trunc, int Q, int TM, bool qd);
 
 }  // namespace tp

@@ -65,23 +65,26 @@ __device__ __forceinline__ void load_pairs(float2 (&dst)[M], const float2 *slice
   }
 }
 
-__host__ __device__ inline size_t team_slice_smem(int M, int T) {
-  return (size_t)(3 * M + 2 * T + 3 + 2 * kTeamLevels) * kTeamChunks * sizeof(float2);
+// Shared-memory bytes of one staged factor slice.  The Cayley-form kernels
+// never apply the right-hand-side stencil, so they stage LF|EP without the
+// QD rows (qd = false).
+__host__ __device__ inline size_t team_slice_smem(int M, int T, bool qd = true) {
+  return (size_t)((qd ? 3 : 2) * M + 2 * T + 3 + 2 * kTeamLevels) * kTeamChunks * sizeof(float2);
 }
 
-size_t team_smem_bytes(const Partition &pt, int trunc, int Q, int TM, bool grad) {
-  (void)grad;
-  return 2 * team_slice_smem(pt.M, trunc) + 6 * (size_t)TM * Q * kTeamChunks * sizeof(float2) + 2 * sizeof(uint64_t);
+size_t team_smem_bytes(const Partition &pt, int trunc, int Q, int TM, bool qd) {
+  return 2 * team_slice_smem(pt.M, trunc, qd) + 6 * (size_t)TM * Q * kTeamChunks * sizeof(float2) +
+         2 * sizeof(uint64_t);
 }
 
-// Issue the bulk copies of one slice's factor set (QD|LF|EP, V head, W tail, records).
-__device__ __forceinline__ void team_issue(float2 *dst, const char *slice, int M, int T, uint64_t *bar) {
+// Issue the bulk copies of one slice's factor set ([QD|]LF|EP, V head, W tail, records).
+__device__ __forceinline__ void team_issue(float2 *dst, const char *slice, int M, int T, uint64_t *bar, bool qd) {
   constexpr int C = kTeamChunks;
   const uint32_t row = C * sizeof(float2);
-  const uint32_t b_main = 3 * M * row, b_sp = T * row, b_rec = (3 + 2 * kTeamLevels) * row;
+  const uint32_t b_main = (qd ? 3 : 2) * M * row, b_sp = T * row, b_rec = (3 + 2 * kTeamLevels) * row;
   mbar_arrive_expect_tx(bar, b_main + 2 * b_sp + b_rec);
   char *d = reinterpret_cast<char *>(dst);
-  bulk_g2s(d, slice, b_main, bar);
+  bulk_g2s(d, slice + (qd ? 0 : (size_t)M * row), b_main, bar);
   bulk_g2s(d + b_main, slice + (size_t)3 * M * row, b_sp, bar);
   bulk_g2s(d + b_main + b_sp, slice + (size_t)(4 * M + (M - 1 - T)) * row, b_sp, bar);
   bulk_g2s(d + b_main + 2 * b_sp, slice + (size_t)5 * M * row, b_rec, bar);
@@ -126,14 +129,15 @@ __device__ __forceinline__ void team_rhs(float2 (&U)[Q][M], const float2 *__rest
 }
 
 // U <- M_s^{-1} U with the staged factor slice F (T spike rows staged: a
-// compile-time count, so the spike corrections touch only those rows).
-template <int M, int Q, int T>
+// compile-time count, so the spike corrections touch only those rows; QD:
+// the slice starts with the QD rows).
+template <int M, int Q, int T, bool QD>
 __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__restrict__ F, float2 *Y0,
                                            float2 *R0, float2 *R1, float2 *XS, int c, int team, const Spec &sp,
                                            bool pcr) {
   constexpr int C = kTeamChunks;
   const float2 zero = make_float2(0.f, 0.f);
-  const float2 *LF = F + M * C, *EP = F + 2 * M * C, *VH = F + 3 * M * C, *WT = VH + T * C, *LR = WT + T * C;
+  const float2 *LF = F + (QD ? M * C : 0), *EP = LF + M * C, *VH = EP + M * C, *WT = VH + T * C, *LR = WT + T * C;
 #pragma unroll
   for (int i = 1; i <= M - 2; ++i) {
     const float2 lf = LF[i * C + c];
@@ -159,48 +163,78 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
       U[q][i] = cfma(t, ep, t);
     }
   }
-#pragma unroll
-  for (int q = 0; q < Q; ++q) Y0[q * C + c] = U[q][0];
-  team_sync(team);
-  float2 rho[Q];
-  {
+  float2 x[Q], xp[Q];
+  constexpr int kRd = 2 + 2 * kTeamLevels;  // record row of the reduced diagonal
+  if (!pcr) {
+    // The factorisation found every separator coupling below kPcrSkipBound,
+    // so the reduced system is diagonal to far beneath fp32 round-off:
+    // x_c = rho_c / rd_c with rho_c = z_c - mc_c y0_{c+1}.  One exchange
+    // publishes each chunk's first row y0 and partial residual z; thread c
+    // then forms its own separator and recomputes its left neighbour's from
+    // the neighbour's records (the same operations, so the same bits), which
+    // saves the second exchange and its barrier.
     const float2 ma = LR[0 * C + c], mc = LR[1 * C + c];
+    float2 zc[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      zc[q] = cfnma(ma, U[q][M - 2], U[q][M - 1]);
+      Y0[q * C + c] = U[q][0];
+      R0[q * C + c] = zc[q];
+    }
+    team_sync(team);
+    const float2 rde = LR[kRd * C + c];
+    const float2 mcl = c > 0 ? LR[1 * C + c - 1] : zero, rdel = c > 0 ? LR[kRd * C + c - 1] : zero;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       const float2 y0n = (c < C - 1) ? Y0[q * C + c + 1] : zero;
-      rho[q] = cfnma(mc, y0n, cfnma(ma, U[q][M - 2], U[q][M - 1]));
+      const float2 r = cfnma(mc, y0n, zc[q]);
+      x[q] = cfma(r, rde, r);
+      if (c > 0) {
+        const float2 rl = cfnma(mcl, U[q][0], R0[q * C + c - 1]);
+        xp[q] = cfma(rl, rdel, rl);
+      } else {
+        xp[q] = zero;
+      }
     }
-  }
-  // PCR on the separators; skipped when the factorisation found every
-  // coupling coefficient below kPcrSkipBound (the reduced system is then
-  // diagonal to far beneath fp32 round-off: x = rho / rd)
+  } else {
 #pragma unroll
-  for (int l = 0; l < (pcr ? kTeamLevels : 0); ++l) {
-    const int s = 1 << l;
-    float2 *Rb = (l & 1) ? R1 : R0;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) Rb[q * C + c] = rho[q];
+    for (int q = 0; q < Q; ++q) Y0[q * C + c] = U[q][0];
     team_sync(team);
-    const float2 al = LR[(2 + l) * C + c], ga = LR[(2 + kTeamLevels + l) * C + c];
+    float2 rho[Q];
+    {
+      const float2 ma = LR[0 * C + c], mc = LR[1 * C + c];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const float2 up = (c >= s) ? Rb[q * C + c - s] : zero;
-      const float2 dn = (c + s < C) ? Rb[q * C + c + s] : zero;
-      rho[q] = cfma(ga, dn, cfma(al, up, rho[q]));
+      for (int q = 0; q < Q; ++q) {
+        const float2 y0n = (c < C - 1) ? Y0[q * C + c + 1] : zero;
+        rho[q] = cfnma(mc, y0n, cfnma(ma, U[q][M - 2], U[q][M - 1]));
+      }
     }
-  }
-  float2 x[Q], xp[Q];
-  {
-    const float2 rde = LR[(2 + 2 * kTeamLevels) * C + c];
+    // PCR on the separators (7 levels through shared memory)
+#pragma unroll
+    for (int l = 0; l < kTeamLevels; ++l) {
+      const int s = 1 << l;
+      float2 *Rb = (l & 1) ? R1 : R0;
+#pragma unroll
+      for (int q = 0; q < Q; ++q) Rb[q * C + c] = rho[q];
+      team_sync(team);
+      const float2 al = LR[(2 + l) * C + c], ga = LR[(2 + kTeamLevels + l) * C + c];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const float2 up = (c >= s) ? Rb[q * C + c - s] : zero;
+        const float2 dn = (c + s < C) ? Rb[q * C + c + s] : zero;
+        rho[q] = cfma(ga, dn, cfma(al, up, rho[q]));
+      }
+    }
+    const float2 rde = LR[kRd * C + c];
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       x[q] = cfma(rho[q], rde, rho[q]);
       XS[q * C + c] = x[q];
     }
-  }
-  team_sync(team);
+    team_sync(team);
 #pragma unroll
-  for (int q = 0; q < Q; ++q) xp[q] = (c > 0) ? XS[q * C + c - 1] : zero;
+    for (int q = 0; q < Q; ++q) xp[q] = (c > 0) ? XS[q * C + c - 1] : zero;
+  }
   constexpr int wlo = M - 1 - T;
 #pragma unroll
   for (int i = 0; i <= M - 2; ++i) {
@@ -228,6 +262,7 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
 template <int M, int Q, int TM, bool LAGGED, bool SUMS, int TS>
 __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const MarchParams p) {
   static_assert(LAGGED || !SUMS, "SUMS selects the exact-adjoint Cayley step");
+  constexpr bool QD = LAGGED && !SUMS;  // only the two-slice exact adjoint applies the stencil
   constexpr int C = kTeamChunks;
   constexpr int NT = kTeamThreads * TM;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -252,7 +287,8 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
   }
   __syncthreads();
   auto slice_of = [&](int t) { return p.backward ? (p.L + 1 - t) : t; };
-  if (tid == 0) team_issue(bufs + ssf, p.factors + (size_t)(slice_of(p.t0) - 1) * p.slice_bytes, M, T, &mbar[1]);
+  if (tid == 0)
+    team_issue(bufs + ssf, p.factors + (size_t)(slice_of(p.t0) - 1) * p.slice_bytes, M, T, &mbar[1], QD);
 
   float2 U[Q][M];
 #pragma unroll
@@ -313,7 +349,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
     if (tid == 0 && t < p.t1) {
       fence_proxy_async_smem();
       team_issue(bufs + (cb ^ 1) * ssf, p.factors + (size_t)(slice_of(t + 1) - 1) * p.slice_bytes, M, T,
-                 &mbar[cb ^ 1]);
+                 &mbar[cb ^ 1], QD);
     }
     const float2 *F = bufs + cb * ssf;
     if (do_grad) {
@@ -368,7 +404,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
 #pragma unroll
         for (int i = 0; i < M; ++i) u_old[q][i] = U[q][i];
     }
-    team_solve<M, Q, T>(U, F, Y0, R0, R1, XS, c, team, p.sp, pcr);
+    team_solve<M, Q, T, QD>(U, F, Y0, R0, R1, XS, c, team, p.sp, pcr);
     const int sidx = p.u_store != nullptr ? store_index(p, t) : -1;
     if constexpr (!LAGGED) {
       if (p.store_sums && sidx >= 0) {
@@ -408,8 +444,14 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
           if (p0 + q >= p.P) continue;  // padded probes contribute nothing
-          const float2 wa = SUMS ? u_new[q][2 * j] : cadd(u_prev[q][2 * j], u_new[q][2 * j]);
-          const float2 wb = SUMS ? u_new[q][2 * j + 1] : cadd(u_prev[q][2 * j + 1], u_new[q][2 * j + 1]);
+          float2 wa, wb;
+          if constexpr (SUMS) {
+            wa = u_new[q][2 * j];
+            wb = u_new[q][2 * j + 1];
+          } else {
+            wa = cadd(u_prev[q][2 * j], u_new[q][2 * j]);
+            wb = cadd(u_prev[q][2 * j + 1], u_new[q][2 * j + 1]);
+          }
           const float2 a = cmulc(U[q][2 * j], wa);
           const float2 b = cmulc(U[q][2 * j + 1], wb);
           acc.x += a.x;
@@ -460,8 +502,9 @@ template <int M, int Q, int TM, bool LAGGED, bool SUMS, int TS>
 static int launch_team_t(const Partition &pt, MarchParams &mp, cudaStream_t st) {
   auto kern = cn2d_team_kernel<M, Q, TM, LAGGED, SUMS, TS>;
   if (mp.trunc != TS) return set_error(TP_ERR_INVALID, "team march staged %d spike rows, kernel has %d", mp.trunc, TS);
-  const bool grad = LAGGED && mp.grad_c != nullptr;
-  const size_t smem = team_smem_bytes(pt, mp.trunc, Q, TM, grad);
+  constexpr bool QD = LAGGED && !SUMS;
+  mp.smem_slice_bytes = team_slice_smem(M, TS, QD);
+  const size_t smem = team_smem_bytes(pt, mp.trunc, Q, TM, QD);
   TP_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = (mp.P + Q * TM - 1) / (Q * TM);
   kern<<<grid, kTeamThreads * TM, smem, st>>>(mp);
@@ -482,8 +525,8 @@ static int launch_team_qt(const Partition &pt, MarchParams &mp, int Q, int TM, c
 // Exact adjoint in Cayley form unless a gradient reads plain forward slices
 // (two per step: not enough registers for the Cayley state as well).
 template <int M, int TS>
-static int launch_team_m(const Partition &pt, MarchParams &mp, bool lagged, int Q, int TM, cudaStream_t st) {
-  const bool sums = lagged && (mp.u_fwd == nullptr || mp.store_sums);
+static int launch_team_m(const Partition &pt, MarchParams &mp, bool lagged, bool sums, int Q, int TM,
+                         cudaStream_t st) {
   if (!lagged) return launch_team_qt<M, false, false, TS>(pt, mp, Q, TM, st);
   return sums ? launch_team_qt<M, true, true, TS>(pt, mp, Q, TM, st)
               : launch_team_qt<M, true, false, TS>(pt, mp, Q, TM, st);
@@ -510,7 +553,8 @@ int launch_team_march(const Partition &pt, MarchParams &mp, bool lagged, cudaStr
   TP_CHECK_CUDA(cudaGetDevice(&dev));
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  const bool grad = lagged && mp.grad_c != nullptr;
+  const bool sums = lagged && (mp.u_fwd == nullptr || mp.store_sums);
+  const bool qd = lagged && !sums;
   // Probes per CTA: one CTA per SM (the factor double buffer fills most of
   // an SM's shared memory), so K = ceil(P / SMs) rounded up to 1, 2 or 4.
   int K = 1;
@@ -524,21 +568,21 @@ int launch_team_march(const Partition &pt, MarchParams &mp, bool lagged, cudaStr
   } else {
     team_shape(K, &TM, &Q);
   }
-  while (team_smem_bytes(pt, mp.trunc, Q, TM, grad) > (size_t)max_smem && TM * Q > 1) {
+  while (team_smem_bytes(pt, mp.trunc, Q, TM, qd) > (size_t)max_smem && TM * Q > 1) {
     if (TM > 1) TM /= 2;
     else Q /= 2;
   }
-  if (team_smem_bytes(pt, mp.trunc, Q, TM, grad) > (size_t)max_smem)
+  if (team_smem_bytes(pt, mp.trunc, Q, TM, qd) > (size_t)max_smem)
     return set_error(TP_ERR_UNSUPPORTED, "team march needs %zu B of shared memory (> %d)",
-                     team_smem_bytes(pt, mp.trunc, Q, TM, grad), max_smem);
+                     team_smem_bytes(pt, mp.trunc, Q, TM, qd), max_smem);
   switch (pt.M) {
     case 4:
-      return launch_team_m<4, 3>(pt, mp, lagged, Q, TM, st);
+      return launch_team_m<4, 3>(pt, mp, lagged, sums, Q, TM, st);
     case 8:
-      return launch_team_m<8, 7>(pt, mp, lagged, Q, TM, st);
+      return launch_team_m<8, 7>(pt, mp, lagged, sums, Q, TM, st);
     case 16:
-      return mp.trunc == 8 ? launch_team_m<16, 8>(pt, mp, lagged, Q, TM, st)
-                           : launch_team_m<16, 15>(pt, mp, lagged, Q, TM, st);
+      return mp.trunc == 8 ? launch_team_m<16, 8>(pt, mp, lagged, sums, Q, TM, st)
+                           : launch_team_m<16, 15>(pt, mp, lagged, sums, Q, TM, st);
     default:
       return set_error(TP_ERR_UNSUPPORTED, "no team kernel for %d rows per chunk", pt.M);
   }
