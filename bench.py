@@ -42,6 +42,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "probe·slice solves/s fwd+adj (2D CN, complex64, exact adjoint + fused gradient)"
+REF_BUDGET_S = 150.0  # wall-time target of a whole `--impl reference` run
 # DRAM bytes (read + write) of one exact-adjoint march launch at N = 2048, nz = 1024, 512
 # probes: an ncu capture at nz = 128 measured 1.095 GB for 127 slices (traffic grows with the
 # slices), scaled by 1023/127 (profiles/cn2d_team_2048x1024_p512_launches.md).
@@ -171,20 +172,33 @@ class ClockSampler:
 # --------------------------------------------------------------------------
 # CPU legs (the oracle restatement of the reference's IterativeLU path)
 # --------------------------------------------------------------------------
-def _cpu_sample(args):
-    """Factorisation + per-probe fwd/adj march time of the CPU restatement."""
-    N, nz, probes_idx, seed = args
-    from oracle import pwe_oracle as po
-    from thick_ptycho_b200.workloads import CONFIGS
+_CPU_CASE = {}
 
-    w = [c for c in CONFIGS.values() if c.nx == N and c.nz == nz and c.dimension == 2][0]
-    geo = w.geometry()
-    dn = w.delta_n()
-    probes = w.probes(geo)
-    co = po.bc_coefficients(geo.k, 1.0, 1.0, bc_type="impedance")
-    A, B = po.step_matrices_1d(N, co, "impedance", 1.0)
+
+def _cpu_case(N, nz):
+    """The 2D workload of size (N, nz) with its step matrices (cached per process)."""
+    if (N, nz) not in _CPU_CASE:
+        from oracle import pwe_oracle as po
+        from thick_ptycho_b200.workloads import CONFIGS
+
+        w = [c for c in CONFIGS.values() if c.nx == N and c.nz == nz and c.dimension == 2][0]
+        geo = w.geometry()
+        co = po.bc_coefficients(geo.k, 1.0, 1.0, bc_type="impedance")
+        A, B = po.step_matrices_1d(N, co, "impedance", 1.0)
+        _CPU_CASE[(N, nz)] = (geo, w.delta_n(), w.probes(geo), A, B)
+    return _CPU_CASE[(N, nz)]
+
+
+def _cpu_sample(args):
+    """Factorisation + per-probe fwd/adj march time of the CPU restatement over
+    the first `S` slices (the costs are linear in the slices)."""
+    N, nz, probes_idx, seed, S = args
+    from oracle import pwe_oracle as po
+
+    geo, dn, probes, A, B = _cpu_case(N, nz)
+    S = min(S, nz - 1)
     t0 = time.perf_counter()
-    C = po.object_contribution(1 - dn, geo.k, 1.0)
+    C = po.object_contribution(1 - dn[:, : S + 1], geo.k, 1.0)
     lf, bf = po.build_lu_factors(A, B, C, "forward")
     la, ba = po.build_lu_factors(A, B, C, "adjoint")
     t_fact = time.perf_counter() - t0
@@ -192,28 +206,32 @@ def _cpu_sample(args):
     t1 = time.perf_counter()
     for p in probes_idx:
         u = po.march_with_lu(lf, bf, b0, probes[p])
-        rhs = np.zeros((N, nz - 1), dtype=complex)
+        rhs = np.zeros((N, S), dtype=complex)
         rhs[:, -1] = u[:, -1]
         po.march_with_lu(la, ba, b0, None, "adjoint", rhs)
     t_probe = (time.perf_counter() - t1) / len(probes_idx)
     return t_fact, t_probe
 
 
-def cpu_rate(N, nz, P, cores, probes_per_worker):
-    """probe·slice/s of the CPU path extrapolated to P probes on `cores` workers."""
+def cpu_rate(N, nz, P, cores, probes_per_worker, slices=None, pool=None):
+    """probe·slice/s of the CPU path extrapolated to P probes on `cores` workers
+    (from `slices` of the L slices, default all of them, scaled linearly)."""
     L = nz - 1
-    jobs = [(N, nz, [(c * 7 + i) % P for i in range(probes_per_worker)], c) for c in range(cores)]
+    S = L if slices is None else max(1, min(int(slices), L))
+    jobs = [(N, nz, [(c * 7 + i) % P for i in range(probes_per_worker)], c, S) for c in range(cores)]
     t0 = time.perf_counter()
     if cores == 1:
         res = [_cpu_sample(jobs[0])]
+    elif pool is not None:
+        res = pool.map(_cpu_sample, jobs)
     else:
         import multiprocessing as mp
 
-        with mp.get_context("spawn").Pool(cores) as pool:
-            res = pool.map(_cpu_sample, jobs)
+        with mp.get_context("spawn").Pool(cores) as p:
+            res = p.map(_cpu_sample, jobs)
     wall = time.perf_counter() - t0
-    t_fact = statistics.mean(r[0] for r in res)
-    t_probe = statistics.mean(r[1] for r in res)
+    t_fact = statistics.mean(r[0] for r in res) * L / S
+    t_probe = statistics.mean(r[1] for r in res) * L / S
     per_worker = -(-P // cores)
     total = t_fact + per_worker * t_probe
     return P * L / total, t_fact, t_probe, wall
@@ -225,27 +243,39 @@ def run_reference(a):
         return
     from thick_ptycho_b200.workloads import CONFIGS
 
+    import multiprocessing as mp
+
     w = CONFIGS[a.config]
     cores = os.cpu_count() or 1
+    L = w.nz - 1
+    # Each step times a sample of S of the L slices on every worker, S chosen
+    # from a first small sample so that the whole --steps/--warmup run takes
+    # about REF_BUDGET_S seconds (factorisation and marches are linear in S).
+    budget = REF_BUDGET_S / max(1, a.warmup + a.steps)
     vals = []
     info = None
-    for i in range(a.warmup + a.steps):
-        v, tf, tp, wall = cpu_rate(w.nx, w.nz, w.num_probes, cores, 1)
-        if i >= a.warmup:
-            vals.append(v)
-            info = (tf, tp, wall)
+    with mp.get_context("spawn").Pool(cores) as pool:
+        probe_s = min(L, 32)
+        _, _, _, wall0 = cpu_rate(w.nx, w.nz, w.num_probes, cores, 1, probe_s, pool)  # also warms the workers
+        _, _, _, wall0 = cpu_rate(w.nx, w.nz, w.num_probes, cores, 1, probe_s, pool)
+        S = max(8, min(L, int(probe_s * budget / max(wall0, 1e-3))))
+        for i in range(a.warmup + a.steps):
+            v, tf, tp, wall = cpu_rate(w.nx, w.nz, w.num_probes, cores, 1, S, pool)
+            if i >= a.warmup:
+                vals.append(v)
+                info = (tf, tp, wall)
     value = statistics.median(vals)
-    L = w.nz - 1
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": 1e3 * w.num_probes * L / value, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded)", "impl": "reference",
         "config": {"workload": w.name, "N": w.nx, "nz": w.nz, "probes": w.num_probes},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": (f"per step: {cores} spawn workers each factorise all {L} slices (forward + "
-                                    f"reference adjoint SuperLU) and march 1 probe fwd+adj; rate extrapolated to "
-                                    f"{w.num_probes} probes split over {cores} workers (last: factor {info[0]:.2f} s, "
-                                    f"probe {info[1]:.3f} s)")},
+                         "sample": (f"per step: {cores} spawn workers each factorise the first {S} of {L} slices "
+                                    f"(forward + reference adjoint SuperLU) and march 1 probe fwd+adj over them; "
+                                    f"rate scaled to {L} slices and {w.num_probes} probes split over {cores} workers "
+                                    f"(last, scaled: factor {info[0]:.2f} s, probe {info[1]:.3f} s; step wall "
+                                    f"{info[2]:.2f} s)")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
