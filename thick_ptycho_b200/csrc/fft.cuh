@@ -91,6 +91,51 @@ __device__ __forceinline__ void dft_small<8>(float2 (&v)[8], float sign) {
   }
 }
 
+// 4-point DFT of (a0, a1, a2, a3) in place, X_m = sum_r a_r exp(sign 2 pi i r m / 4).
+__device__ __forceinline__ void dft4_inplace(float2 &a0, float2 &a1, float2 &a2, float2 &a3, float sign) {
+  const float2 s02 = cadd(a0, a2), d02 = csub(a0, a2), s13 = cadd(a1, a3);
+  const float2 jd13 = mul_si(csub(a1, a3), sign);
+  a0 = cadd(s02, s13);
+  a2 = csub(s02, s13);
+  a1 = cadd(d02, jd13);
+  a3 = csub(d02, jd13);
+}
+
+// 16-point DFT as 4 x 4: with n = 4 n1 + n2 and m = k1 + 4 k2,
+// X_m = sum_n2 W16^{n2 k1} W4^{n2 k2} sum_n1 x_{4 n1 + n2} W4^{n1 k1}:
+// DFT-4 over n1 for every n2, twiddles W16^{n2 k1}, DFT-4 over n2 for every
+// k1, then the 4 x 4 transpose of the output order.
+__device__ __forceinline__ void dft16(float2 (&v)[16], float sign) {
+  // cos and sin of 2 pi m / 16, m = 0..9 (the twiddle exponents n2 k1 used)
+  constexpr float kc[10] = {1.f, 0.92387953251128675613f, 0.70710678118654752440f, 0.38268343236508977173f, 0.f,
+                            -0.38268343236508977173f, -0.70710678118654752440f, -0.92387953251128675613f, -1.f,
+                            -0.92387953251128675613f};
+  constexpr float ks[10] = {0.f, 0.38268343236508977173f, 0.70710678118654752440f, 0.92387953251128675613f, 1.f,
+                            0.92387953251128675613f, 0.70710678118654752440f, 0.38268343236508977173f, 0.f,
+                            -0.38268343236508977173f};
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) dft4_inplace(v[n2], v[4 + n2], v[8 + n2], v[12 + n2], sign);
+  // now v[4 k1 + n2] holds the inner DFT for (n2, k1)
+#pragma unroll
+  for (int k1 = 1; k1 < 4; ++k1)
+#pragma unroll
+    for (int n2 = 1; n2 < 4; ++n2) {
+      const int m = n2 * k1;
+      v[4 * k1 + n2] = cmul(v[4 * k1 + n2], make_float2(kc[m], sign * ks[m]));
+    }
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) dft4_inplace(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3], sign);
+  // v[4 k1 + k2] holds X_{k1 + 4 k2}: transpose
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = r + 1; c < 4; ++c) {
+      const float2 t = v[4 * r + c];
+      v[4 * r + c] = v[4 * c + r];
+      v[4 * c + r] = t;
+    }
+}
+
 template <>
 __device__ __forceinline__ void dft_small<3>(float2 (&v)[8], float sign) {
   const float s3 = 0.86602540378443864676f;  // sin(2 pi / 3)
@@ -159,7 +204,7 @@ __device__ __forceinline__ void fft_pass_fixed(const float2 *a, float2 *b, const
     const float2 *src = a + bi * N;
     float2 *dst = b + bi * N;
     const int k = j % Ns;
-    float2 v[8];
+    float2 v[R > 8 ? 16 : 8];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = src[j + r * T];
 #pragma unroll
@@ -167,7 +212,8 @@ __device__ __forceinline__ void fft_pass_fixed(const float2 *a, float2 *b, const
       const float2 t = tw[(r * k * step) % N];
       v[r] = cmul(v[r], make_float2(t.x, sign < 0 ? t.y : -t.y));
     }
-    dft_small<R>(v, sign);
+    if constexpr (R == 16) dft16(v, sign);
+    else dft_small<R>(v, sign);
     const int idx = (j / Ns) * Ns * R + k;
 #pragma unroll
     for (int r = 0; r < R; ++r) dst[idx + r * Ns] = v[r];
@@ -208,7 +254,7 @@ __device__ __forceinline__ void fft_pass_padded(const float2 *a, float2 *b, cons
     const float2 *src = a + bi * S;
     float2 *dst = b + bi * S;
     const int k = j % Ns;
-    float2 v[8];
+    float2 v[R > 8 ? 16 : 8];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = src[fft_pad(j + r * T)];
 #pragma unroll
@@ -216,7 +262,8 @@ __device__ __forceinline__ void fft_pass_padded(const float2 *a, float2 *b, cons
       const float2 t = tw[(r * k * step) % N];
       v[r] = cmul(v[r], make_float2(t.x, sign < 0 ? t.y : -t.y));
     }
-    dft_small<R>(v, sign);
+    if constexpr (R == 16) dft16(v, sign);
+    else dft_small<R>(v, sign);
     const int idx = (j / Ns) * Ns * R + k;
 #pragma unroll
     for (int r = 0; r < R; ++r) dst[fft_pad(idx + r * Ns)] = v[r];
@@ -235,7 +282,8 @@ __device__ __forceinline__ float2 *fft_run_padded(float2 *a, float2 *b, const fl
   }
 }
 
-// Lengths with a compile-time plan (radices 8s first, then 4, 2, 3).
+// Lengths with a compile-time plan (radix 16 for 128 and 256, else 8s first,
+// then 4, 2, 3).
 __host__ __device__ constexpr bool fft_fixed_size(int n) {
   return n == 32 || n == 64 || n == 128 || n == 192 || n == 256 || n == 512;
 }
@@ -246,9 +294,9 @@ __device__ __forceinline__ float2 *fft_block_fixed(float2 *a, float2 *b, const f
   const float sign = inverse ? 1.f : -1.f;
   if constexpr (N == 32) return fft_run_fixed<32, 1, 8, 4>(a, b, tw, sign, nb, tid, nth);
   else if constexpr (N == 64) return fft_run_fixed<64, 1, 8, 8>(a, b, tw, sign, nb, tid, nth);
-  else if constexpr (N == 128) return fft_run_fixed<128, 1, 8, 8, 2>(a, b, tw, sign, nb, tid, nth);
+  else if constexpr (N == 128) return fft_run_fixed<128, 1, 8, 16>(a, b, tw, sign, nb, tid, nth);
   else if constexpr (N == 192) return fft_run_fixed<192, 1, 8, 8, 3>(a, b, tw, sign, nb, tid, nth);
-  else if constexpr (N == 256) return fft_run_fixed<256, 1, 8, 8, 4>(a, b, tw, sign, nb, tid, nth);
+  else if constexpr (N == 256) return fft_run_fixed<256, 1, 16, 16>(a, b, tw, sign, nb, tid, nth);
   else return fft_run_fixed<512, 1, 8, 8, 8>(a, b, tw, sign, nb, tid, nth);
 }
 
@@ -259,9 +307,9 @@ __device__ __forceinline__ float2 *fft_block_padded(float2 *a, float2 *b, const 
   const float sign = inverse ? 1.f : -1.f;
   if constexpr (N == 32) return fft_run_padded<32, 1, 8, 4>(a, b, tw, sign, nb, tid, nth);
   else if constexpr (N == 64) return fft_run_padded<64, 1, 8, 8>(a, b, tw, sign, nb, tid, nth);
-  else if constexpr (N == 128) return fft_run_padded<128, 1, 8, 8, 2>(a, b, tw, sign, nb, tid, nth);
+  else if constexpr (N == 128) return fft_run_padded<128, 1, 8, 16>(a, b, tw, sign, nb, tid, nth);
   else if constexpr (N == 192) return fft_run_padded<192, 1, 8, 8, 3>(a, b, tw, sign, nb, tid, nth);
-  else if constexpr (N == 256) return fft_run_padded<256, 1, 8, 8, 4>(a, b, tw, sign, nb, tid, nth);
+  else if constexpr (N == 256) return fft_run_padded<256, 1, 16, 16>(a, b, tw, sign, nb, tid, nth);
   else return fft_run_padded<512, 1, 8, 8, 8>(a, b, tw, sign, nb, tid, nth);
 }
 
