@@ -72,6 +72,7 @@ class PWEGradient2D:
         self.sums = self.engine.chunks == 128
         self._ff = self.engine.new_factor_buffer()
         self._fa = self.engine.new_factor_buffer()
+        self._copy_stream = None
         self._bufs = {}
         self._grad_c = self.engine.new_grad_buffer()
 
@@ -89,11 +90,16 @@ class PWEGradient2D:
             return P * e.nz * e.npad * 8
         return P * (e.L // self.ckpt + 1 + self.ckpt + 1 + 2) * e.npad * 8
 
-    def forward(self, field: torch.Tensor, probes: torch.Tensor, is_delta=False, exit_out=None):
-        """Forward march keeping the field (every slice, or the checkpoints)."""
+    def forward(self, field: torch.Tensor, probes: torch.Tensor, is_delta=False, exit_out=None, probes_ready=None):
+        """Forward march keeping the field (every slice, or the checkpoints).
+
+        ``probes_ready``: a CUDA event the march waits for (the probes may
+        still be in flight on another stream while the slices factorise)."""
         P = probes.shape[0]
         e = self.engine
         fs = e.factor(field, "forward", is_delta, out=self._ff)
+        if probes_ready is not None:
+            torch.cuda.current_stream(self.device).wait_event(probes_ready)
         ex = exit_out if exit_out is not None else torch.empty((P, e.n), dtype=torch.complex64, device=self.device)
         if not self.ckpt:
             e.march(fs, P, probes=probes, u_store=self._buf("full", P, e.nz), exit_out=ex, store_sums=self.sums)
@@ -151,10 +157,24 @@ class PWEGradient2D:
         Host inputs are copied to the device; if ``grad_out`` is a host tensor
         the gradient is copied back into it.  Returns a float loss.
         """
+        main = torch.cuda.current_stream(self.device)
         field = _as_device(n, self.device, torch.complex128)
-        pr = _as_device(probes, self.device, torch.complex64)
-        amp = _as_device(amplitude, self.device, torch.float64)
-        ex = self.forward(field, pr)
+        # Host probes and amplitudes travel on a side stream after n, so that
+        # their copies overlap the factorisation and the forward march (n is
+        # needed first; the probes at the march, the amplitudes at the residual).
+        if self._copy_stream is None:
+            self._copy_stream = torch.cuda.Stream(self.device)
+        side = self._copy_stream
+        side.wait_stream(main)
+        with torch.cuda.stream(side):
+            pr = _as_device(probes, self.device, torch.complex64)
+            pr_ready = side.record_event()
+            amp = _as_device(amplitude, self.device, torch.float64)
+            amp_ready = side.record_event()
+        pr.record_stream(main)
+        amp.record_stream(main)
+        ex = self.forward(field, pr, probes_ready=pr_ready)
+        main.wait_event(amp_ready)
         loss, ge = amplitude_residual(ex, amp)
         g = self.backward(field, ge)
         if grad_out is not None:
