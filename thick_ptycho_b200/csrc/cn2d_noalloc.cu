@@ -11,7 +11,7 @@
 // The array is kStaticScratchBytes (32 MiB).  Every GPU that loads this
 // library reserves it for the life of the process.  Problems whose factor set
 // is larger (tp_cn2d_factor_bytes(N, nz) > 32 MiB, e.g. N = 2048 with more
-// than 393 slices) are rejected with TP_ERR_WORKSPACE.
+// than 337 slices) are rejected with TP_ERR_WORKSPACE.
 //
 // All calls share the one array, and each call overwrites the part it uses
 // before reading it, so nothing carries over between calls.  Calls that
