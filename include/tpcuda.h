@@ -146,6 +146,24 @@ TP_API size_t tp_cn2d_factor_bytes(int32_t n, int32_t nz);
 TP_API int tp_cn2d_factor(const tp_cn2d_op *op, const void *n_field, int32_t n_dtype, int32_t mode,
                    void *factors, size_t factors_bytes, tp_stream_t stream);
 
+/* The same for slices [slice_begin, slice_end] only (1-based, inclusive;
+ * slice s reads index columns s-1 and s), so that factorisation can follow
+ * the index field onto the device column block by column block.  The range
+ * starting at slice 1 resets the factor set's PCR coupling bound, which later
+ * ranges raise: factorise the ranges in increasing order and march a range
+ * only after it is factorised.  (No reference counterpart: a pipelining
+ * form of tp_cn2d_factor.) */
+TP_API int tp_cn2d_factor_range(const tp_cn2d_op *op, const void *n_field, int32_t n_dtype, int32_t mode,
+                                void *factors, size_t factors_bytes, int32_t slice_begin, int32_t slice_end,
+                                tp_stream_t stream);
+
+/* Asynchronous copy of bytes [byte_begin, byte_begin + byte_count) of each of
+ * `rows` rows of `row_bytes` bytes between equally laid-out arrays (host or
+ * device, pinned host memory for asynchrony): a column block of a row-major
+ * array, e.g. the z nodes of the index field a factorisation range needs. */
+TP_API int tp_copy_columns(void *dst, const void *src, int64_t rows, int64_t row_bytes, int64_t byte_begin,
+                           int64_t byte_count, tp_stream_t stream);
+
 /*
  * March all probes through the slices with a factor set of the same mode
  * (the reference's per-probe loop iterative_lu.py:138-197 and the serial

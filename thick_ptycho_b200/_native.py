@@ -164,6 +164,11 @@ SIGNATURES = [
     ("tp_cn2d_factor_bytes", ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
     ("tp_cn2d_factor", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                       ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    ("tp_cn2d_factor_range", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.c_void_p]),
+    ("tp_copy_columns", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                                       ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p]),
     ("tp_cn2d_march", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_void_p, ctypes.POINTER(TpCn2dMarchArgs),
                                      ctypes.c_void_p]),
     ("tp_cn2d_grad_to_n", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,

@@ -95,6 +95,20 @@ class CN2D:
         _native.check(rc, "tp_cn2d_factor")
         return FactorSet(mode_i, buf)
 
+    def factor_range(self, field: torch.Tensor, mode, slice_begin: int, slice_end: int, out: torch.Tensor,
+                     is_delta=False) -> FactorSet:
+        """Factorise slices ``slice_begin..slice_end`` (1-based, inclusive) of ``mode``
+        into ``out``; slice s reads index columns s−1 and s.  The range that
+        starts at slice 1 resets the PCR coupling bound the later ranges raise."""
+        field = self._check_field(field)
+        mode_i = _native.MODES[mode] if isinstance(mode, str) else int(mode)
+        dtype = _native.C128 if field.dtype == torch.complex128 else _native.C64
+        o = self.op(is_delta)
+        rc = self.lib.tp_cn2d_factor_range(ctypes.byref(o), _ptr(field), dtype, mode_i, _ptr(out), out.numel(),
+                                           int(slice_begin), int(slice_end), _stream(self.device))
+        _native.check(rc, "tp_cn2d_factor_range")
+        return FactorSet(mode_i, out)
+
     # -------------------------------------------------------------- march
     def march(
         self,

@@ -149,7 +149,7 @@ __device__ __forceinline__ double2 p_sup(const FactorParams &f, int g) {  // P[g
 __global__ void __launch_bounds__(128) cn2d_factor_kernel(const FactorParams f) {
   extern __shared__ double2 fsm[];  // [5][C]: ra, rd, rc, v_first, w_first
   const int c = threadIdx.x;
-  const int sl = blockIdx.x;
+  const int sl = f.sl0 + blockIdx.x;
   const int M = f.M, C = f.C;
   float2 *base = reinterpret_cast<float2 *>(f.factors + (size_t)sl * f.slice_bytes);
   float2 *QD = base, *LF = base + M * C, *EP = base + 2 * M * C, *V = base + 3 * M * C, *W = base + 4 * M * C,
@@ -677,8 +677,9 @@ extern "C" size_t tp_cn2d_factor_bytes(int32_t n, int32_t nz) {
   return slice_bytes(pt) * (size_t)(nz - 1) + kFactorTailBytes;
 }
 
-extern "C" int tp_cn2d_factor(const tp_cn2d_op *op, const void *n_field, int32_t n_dtype, int32_t mode,
-                              void *factors, size_t factors_bytes, tp_stream_t stream) {
+// Factorise slices [s_begin, s_end] (1-based, inclusive) of the factor set.
+static int factor_slices(const tp_cn2d_op *op, const void *n_field, int32_t n_dtype, int32_t mode, void *factors,
+                         size_t factors_bytes, int s_begin, int s_end, tp_stream_t stream) {
   int rc = validate_op(op);
   if (rc) return rc;
   if (n_field == nullptr || factors == nullptr) return set_error(TP_ERR_INVALID, "n_field/factors is NULL");
@@ -722,10 +723,41 @@ extern "C" int tp_cn2d_factor(const tp_cn2d_op *op, const void *n_field, int32_t
   f.slice_bytes = slice_bytes(pt);
   f.coupling = reinterpret_cast<unsigned *>(f.factors + (size_t)f.L * f.slice_bytes);
   f.err = err;
-  TP_CHECK_CUDA(cudaMemsetAsync(f.coupling, 0, sizeof(unsigned), reinterpret_cast<cudaStream_t>(stream)));
+  if (s_begin < 1 || s_end > f.L || s_begin > s_end)
+    return set_error(TP_ERR_INVALID, "slice range [%d, %d] outside [1, %d]", s_begin, s_end, f.L);
+  f.sl0 = s_begin - 1;
+  // the PCR coupling bound is a running maximum over the slices factorised
+  // since the last reset, which the range starting at slice 1 performs
+  if (s_begin == 1)
+    TP_CHECK_CUDA(cudaMemsetAsync(f.coupling, 0, sizeof(unsigned), reinterpret_cast<cudaStream_t>(stream)));
   const size_t smem = 5 * (size_t)pt.C * sizeof(double2);
-  cn2d_factor_kernel<<<f.L, pt.C, smem, reinterpret_cast<cudaStream_t>(stream)>>>(f);
+  cn2d_factor_kernel<<<s_end - s_begin + 1, pt.C, smem, reinterpret_cast<cudaStream_t>(stream)>>>(f);
   return check_cuda(cudaGetLastError(), "cn2d_factor_kernel launch");
+}
+
+extern "C" int tp_cn2d_factor(const tp_cn2d_op *op, const void *n_field, int32_t n_dtype, int32_t mode,
+                              void *factors, size_t factors_bytes, tp_stream_t stream) {
+  if (op == nullptr) return set_error(TP_ERR_INVALID, "op is NULL");
+  return factor_slices(op, n_field, n_dtype, mode, factors, factors_bytes, 1, op->nz - 1, stream);
+}
+
+extern "C" int tp_cn2d_factor_range(const tp_cn2d_op *op, const void *n_field, int32_t n_dtype, int32_t mode,
+                                    void *factors, size_t factors_bytes, int32_t slice_begin, int32_t slice_end,
+                                    tp_stream_t stream) {
+  if (op == nullptr) return set_error(TP_ERR_INVALID, "op is NULL");
+  return factor_slices(op, n_field, n_dtype, mode, factors, factors_bytes, slice_begin, slice_end, stream);
+}
+
+extern "C" int tp_copy_columns(void *dst, const void *src, int64_t rows, int64_t row_bytes, int64_t byte_begin,
+                               int64_t byte_count, tp_stream_t stream) {
+  if (dst == nullptr || src == nullptr || rows < 1 || row_bytes < 1 || byte_begin < 0 || byte_count < 1 ||
+      byte_begin + byte_count > row_bytes)
+    return set_error(TP_ERR_INVALID, "bad tp_copy_columns arguments");
+  char *d = static_cast<char *>(dst) + byte_begin;
+  const char *s = static_cast<const char *>(src) + byte_begin;
+  return check_cuda(cudaMemcpy2DAsync(d, (size_t)row_bytes, s, (size_t)row_bytes, (size_t)byte_count, (size_t)rows,
+                                      cudaMemcpyDefault, reinterpret_cast<cudaStream_t>(stream)),
+                    "tp_copy_columns");
 }
 
 extern "C" int tp_cn2d_march(const tp_cn2d_op *op, const void *factors, const tp_cn2d_march_args *a,

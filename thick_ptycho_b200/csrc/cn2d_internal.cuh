@@ -51,6 +51,7 @@ enum DeviceErrorBits : int { kDevSpikeTruncation = 2 };
 
 struct FactorParams {
   int N, L, nz, n_obj, empty_px, exact, is_delta, dtype;
+  int sl0;  // first slice (0-based) of this launch; CTA b factorises slice sl0 + b
   int C, M, levels, nrec;
   int trunc;  // spike rows the march keeps (V rows [0,T), W rows [M-1-T, M-1))
   double sigma;

@@ -12,13 +12,14 @@ Gradients follow torch's complex convention ``∂ℓ/∂Re + i ∂ℓ/∂Im``.
 
 from __future__ import annotations
 
+import ctypes
 import math
 from typing import Optional, Union
 
 import numpy as np
 import torch
 
-from . import heads
+from . import _native, heads
 from .cn2d import CN2D
 
 
@@ -73,6 +74,7 @@ class PWEGradient2D:
         self._ff = self.engine.new_factor_buffer()
         self._fa = self.engine.new_factor_buffer()
         self._copy_stream = None
+        self._n_dev = None
         self._bufs = {}
         self._grad_c = self.engine.new_grad_buffer()
 
@@ -106,6 +108,42 @@ class PWEGradient2D:
         else:
             ck = self._buf("ckpt", P, e.L // self.ckpt + 1)
             e.march(fs, P, probes=probes, u_store=ck, store_every=self.ckpt, exit_out=ex)
+        self._fs_fwd = fs
+        return ex
+
+    def _n_device(self) -> torch.Tensor:
+        """Device buffer for a host index field (complex128, (n_obj, nz))."""
+        e = self.engine
+        if self._n_dev is None:
+            self._n_dev = torch.empty((e.n_obj, e.nz), dtype=torch.complex128, device=self.device)
+        return self._n_dev
+
+    def _slice_ranges(self, parts: int = 4):
+        """`parts` consecutive slice ranges covering 1..L (1-based, inclusive)."""
+        L = self.engine.L
+        b = [round(k * L / parts) for k in range(parts + 1)]
+        return [(b[k] + 1, b[k + 1]) for k in range(parts) if b[k + 1] > b[k]]
+
+    def _forward_ranges(self, field, probes, probes_ready, ranges, ready):
+        """Forward march range by range, each after its index columns arrived
+        (`ready` events) and its slices were factorised; the state passes from
+        range to range, the stored field and the exit wave are those of one
+        march over all slices."""
+        e = self.engine
+        P = probes.shape[0]
+        main = torch.cuda.current_stream(self.device)
+        ex = torch.empty((P, e.n), dtype=torch.complex64, device=self.device)
+        store = self._buf("full", P, e.nz)
+        state = [self._buf("range_state0", P, 1)[:, 0], self._buf("range_state1", P, 1)[:, 0]]
+        last = len(ranges) - 1
+        for k, (s0, s1) in enumerate(ranges):
+            main.wait_event(ready[k])
+            fs = e.factor_range(field, "forward", s0, s1, out=self._ff)
+            if k == 0:
+                main.wait_event(probes_ready)
+            e.march(fs, P, probes=probes if k == 0 else None, u_store=store, exit_out=ex, t_begin=s0, t_end=s1,
+                    state_in=None if k == 0 else state[(k - 1) % 2], state_out=None if k == last else state[k % 2],
+                    store_sums=self.sums)
         self._fs_fwd = fs
         return ex
 
@@ -158,22 +196,49 @@ class PWEGradient2D:
         the gradient is copied back into it.  Returns a float loss.
         """
         main = torch.cuda.current_stream(self.device)
-        field = _as_device(n, self.device, torch.complex128)
-        # Host probes and amplitudes travel on a side stream after n, so that
-        # their copies overlap the factorisation and the forward march (n is
-        # needed first; the probes at the march, the amplitudes at the residual).
         if self._copy_stream is None:
             self._copy_stream = torch.cuda.Stream(self.device)
         side = self._copy_stream
         side.wait_stream(main)
-        with torch.cuda.stream(side):
-            pr = _as_device(probes, self.device, torch.complex64)
-            pr_ready = side.record_event()
-            amp = _as_device(amplitude, self.device, torch.float64)
-            amp_ready = side.record_event()
+        e = self.engine
+        streamed = (isinstance(n, torch.Tensor) and not n.is_cuda and n.dtype == torch.complex128
+                    and n.is_contiguous() and tuple(n.shape) == (e.n_obj, e.nz) and not self.ckpt and e.L >= 64)
+        if streamed:
+            # A host index field goes up in column blocks on the side stream;
+            # each block's slices are factorised and marched while the next
+            # block is in flight (slice s needs index columns s-1 and s).
+            field = self._n_device()
+            ranges = self._slice_ranges()
+            ready = []
+            with torch.cuda.stream(side):
+                for k, (s0, s1) in enumerate(ranges):
+                    c0 = 0 if k == 0 else s0
+                    rc = e.lib.tp_copy_columns(ctypes.c_void_p(field.data_ptr()), ctypes.c_void_p(n.data_ptr()),
+                                               e.n_obj, e.nz * 16, c0 * 16, (s1 - c0 + 1) * 16,
+                                               ctypes.c_void_p(side.cuda_stream))
+                    _native.check(rc, "tp_copy_columns")
+                    ready.append(side.record_event())
+                    if k == 0:
+                        pr = _as_device(probes, self.device, torch.complex64)
+                        pr_ready = side.record_event()
+                amp = _as_device(amplitude, self.device, torch.float64)
+                amp_ready = side.record_event()
+        else:
+            field = _as_device(n, self.device, torch.complex128)
+            # Host probes and amplitudes travel on a side stream after n, so that
+            # their copies overlap the factorisation and the forward march (n is
+            # needed first; the probes at the march, the amplitudes at the residual).
+            with torch.cuda.stream(side):
+                pr = _as_device(probes, self.device, torch.complex64)
+                pr_ready = side.record_event()
+                amp = _as_device(amplitude, self.device, torch.float64)
+                amp_ready = side.record_event()
         pr.record_stream(main)
         amp.record_stream(main)
-        ex = self.forward(field, pr, probes_ready=pr_ready)
+        if streamed:
+            ex = self._forward_ranges(field, pr, pr_ready, ranges, ready)
+        else:
+            ex = self.forward(field, pr, probes_ready=pr_ready)
         main.wait_event(amp_ready)
         loss, ge = amplitude_residual(ex, amp)
         g = self.backward(field, ge)
