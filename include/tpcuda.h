@@ -182,6 +182,12 @@ TP_API int tp_cn2d_march(const tp_cn2d_op *op, const void *factors, const tp_cn2
  */
 TP_API int tp_cn2d_grad_to_n(const tp_cn2d_op *op, const void *grad_c, const void *n_field, int32_t n_dtype,
                       void *grad_n, tp_stream_t stream);
+/* The same for node columns [node_begin, node_end] only (node t reads slices
+ * t and t + 1 of grad_c), so that finished columns can be mapped and copied
+ * off while the adjoint march still runs on the earlier slices.  (No
+ * reference counterpart.) */
+TP_API int tp_cn2d_grad_to_n_range(const tp_cn2d_op *op, const void *grad_c, const void *n_field, int32_t n_dtype,
+                                   void *grad_n, int32_t node_begin, int32_t node_end, tp_stream_t stream);
 
 /* Gather a chunked full field (P, nz, Npad) into the reference layout
  * (P, N, nz) complex64. */

@@ -173,6 +173,9 @@ SIGNATURES = [
                                      ctypes.c_void_p]),
     ("tp_cn2d_grad_to_n", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                          ctypes.c_void_p, ctypes.c_void_p]),
+    ("tp_cn2d_grad_to_n_range", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                               ctypes.c_void_p]),
     ("tp_cn2d_unchunk", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.c_void_p]),
     ("tp_cn2d_march_noalloc", ctypes.c_int, [ctypes.POINTER(TpCn2dOp), ctypes.c_void_p, ctypes.c_int32,

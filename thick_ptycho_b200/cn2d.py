@@ -228,6 +228,19 @@ class CN2D:
         _native.check(rc, "tp_cn2d_grad_to_n")
         return out
 
+    def grad_to_n_range(self, grad_c: torch.Tensor, out: torch.Tensor, node_begin: int, node_end: int,
+                        field: Optional[torch.Tensor] = None, is_delta=False) -> torch.Tensor:
+        """:meth:`grad_to_n` for node columns ``node_begin..node_end`` of ``out`` only."""
+        dtype = _native.C128
+        if field is not None:
+            field = self._check_field(field)
+            dtype = _native.C128 if field.dtype == torch.complex128 else _native.C64
+        o = self.op(is_delta)
+        rc = self.lib.tp_cn2d_grad_to_n_range(ctypes.byref(o), _ptr(grad_c), _ptr(field), dtype, _ptr(out),
+                                              int(node_begin), int(node_end), _stream(self.device))
+        _native.check(rc, "tp_cn2d_grad_to_n_range")
+        return out
+
     def device_status(self):
         code = ctypes.c_int32()
         rc = self.lib.tp_device_status(_stream(self.device), ctypes.byref(code))

@@ -510,6 +510,7 @@ __global__ void cn2d_unchunk_kernel(const float2 *__restrict__ st, float2 *__res
 
 struct GradParams {
   int N, L, nz, n_obj, empty_px, exact, is_delta, dtype;
+  int t0, nt;  // node columns [t0, t0 + nt) are mapped
   int M, C, pair, Npad;
   double k, dz;
   const float2 *gc;
@@ -518,10 +519,11 @@ struct GradParams {
 };
 
 __global__ void cn2d_grad_to_n_kernel(const GradParams q) {
-  const size_t total = (size_t)q.n_obj * q.nz;
-  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
-    const int t = (int)(idx % q.nz);
-    const int x = (int)(idx / q.nz);
+  const size_t total = (size_t)q.n_obj * q.nt;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const int t = q.t0 + (int)(e % q.nt);
+    const int x = (int)(e / q.nt);
+    const size_t idx = (size_t)x * q.nz + t;
     const int g = x + q.empty_px;
     const int i = g % q.M, k = g / q.M;
     const size_t off = q.pair ? ((size_t)(i >> 1) * q.C + k) * 2 + (i & 1) : (size_t)i * q.C + k;
@@ -848,8 +850,8 @@ extern "C" int tp_cn2d_unchunk(const tp_cn2d_op *op, int32_t num_probes, const v
   return check_cuda(cudaGetLastError(), "cn2d_unchunk_kernel launch");
 }
 
-extern "C" int tp_cn2d_grad_to_n(const tp_cn2d_op *op, const void *grad_c, const void *n_field, int32_t n_dtype,
-                                 void *grad_n, tp_stream_t stream) {
+static int grad_to_n_nodes(const tp_cn2d_op *op, const void *grad_c, const void *n_field, int32_t n_dtype,
+                           void *grad_n, int node_begin, int node_end, tp_stream_t stream) {
   int rc = validate_op(op);
   if (rc) return rc;
   if (grad_c == nullptr || grad_n == nullptr) return set_error(TP_ERR_INVALID, "grad_c/grad_n is NULL");
@@ -875,8 +877,25 @@ extern "C" int tp_cn2d_grad_to_n(const tp_cn2d_op *op, const void *grad_c, const
   q.gc = static_cast<const float2 *>(grad_c);
   q.n = n_field;
   q.gn = static_cast<float2 *>(grad_n);
+  if (node_begin < 0 || node_end >= op->nz || node_begin > node_end)
+    return set_error(TP_ERR_INVALID, "node range [%d, %d] outside [0, %d]", node_begin, node_end, op->nz - 1);
+  q.t0 = node_begin;
+  q.nt = node_end - node_begin + 1;
   cn2d_grad_to_n_kernel<<<592, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(q);
   return check_cuda(cudaGetLastError(), "cn2d_grad_to_n_kernel launch");
+}
+
+extern "C" int tp_cn2d_grad_to_n(const tp_cn2d_op *op, const void *grad_c, const void *n_field, int32_t n_dtype,
+                                 void *grad_n, tp_stream_t stream) {
+  if (op == nullptr) return set_error(TP_ERR_INVALID, "op is NULL");
+  return grad_to_n_nodes(op, grad_c, n_field, n_dtype, grad_n, 0, op->nz - 1, stream);
+}
+
+extern "C" int tp_cn2d_grad_to_n_range(const tp_cn2d_op *op, const void *grad_c, const void *n_field,
+                                       int32_t n_dtype, void *grad_n, int32_t node_begin, int32_t node_end,
+                                       tp_stream_t stream) {
+  if (op == nullptr) return set_error(TP_ERR_INVALID, "op is NULL");
+  return grad_to_n_nodes(op, grad_c, n_field, n_dtype, grad_n, node_begin, node_end, stream);
 }
 
 extern "C" int tp_device_status(tp_stream_t stream, int32_t *code) {

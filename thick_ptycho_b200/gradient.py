@@ -118,11 +118,17 @@ class PWEGradient2D:
             self._n_dev = torch.empty((e.n_obj, e.nz), dtype=torch.complex128, device=self.device)
         return self._n_dev
 
-    def _slice_ranges(self, parts: int = 4):
-        """`parts` consecutive slice ranges covering 1..L (1-based, inclusive)."""
+    # Range boundaries as fractions of the slices: a short first range, so
+    # that little of the index field (and, for the adjoint, which runs the
+    # ranges backwards, little of the gradient) is exposed outside the
+    # overlap, then three equal ones.
+    _RANGE_FRACTIONS = (0.0, 1.0 / 32.0, 1.0 / 3.0, 2.0 / 3.0, 1.0)
+
+    def _slice_ranges(self):
+        """Consecutive slice ranges covering 1..L (1-based, inclusive)."""
         L = self.engine.L
-        b = [round(k * L / parts) for k in range(parts + 1)]
-        return [(b[k] + 1, b[k + 1]) for k in range(parts) if b[k + 1] > b[k]]
+        b = sorted({round(f * L) for f in self._RANGE_FRACTIONS})
+        return [(b[k] + 1, b[k + 1]) for k in range(len(b) - 1) if b[k + 1] > b[k]]
 
     def _forward_ranges(self, field, probes, probes_ready, ranges, ready):
         """Forward march range by range, each after its index columns arrived
@@ -146,6 +152,40 @@ class PWEGradient2D:
                     store_sums=self.sums)
         self._fs_fwd = fs
         return ex
+
+    def _backward_ranges(self, field, exit_grad, grad_out, side):
+        """:meth:`backward` (full field kept) with the adjoint run range by range
+        from the last slice down: once slices s0..L are done, index nodes
+        s0..nz-1 are final (node t reads slices t and t+1), so they are mapped
+        and copied into the host tensor `grad_out` on the side stream while the
+        adjoint goes on with the earlier slices.  Returns the device gradient."""
+        e = self.engine
+        P = exit_grad.shape[0]
+        main = torch.cuda.current_stream(self.device)
+        fa = e.factor(field, "adjoint_exact", out=self._fa)
+        self._grad_c.zero_()
+        src = exit_grad.contiguous()
+        gn = torch.empty((e.n_obj, e.nz), dtype=torch.complex64, device=self.device)
+        state = [self._buf("range_state0", P, 1)[:, 0], self._buf("range_state1", P, 1)[:, 0]]
+        ranges = self._slice_ranges()[::-1]  # last slices first
+        hi = e.nz - 1  # highest node not yet mapped
+        for k, (s0, s1) in enumerate(ranges):
+            # slices s1 .. s0 are steps L+1-s1 .. L+1-s0 of the adjoint march
+            e.march(fa, P, src_exit=src if k == 0 else None, u_fwd=self._buf("full", P, e.nz), grad_c=self._grad_c,
+                    t_begin=e.L + 1 - s1, t_end=e.L + 1 - s0,
+                    state_in=None if k == 0 else state[(k - 1) % 2],
+                    state_out=None if k == len(ranges) - 1 else state[k % 2], store_sums=self.sums)
+            lo = 0 if k == len(ranges) - 1 else s0
+            e.grad_to_n_range(self._grad_c, gn, lo, hi, field if e.exact_ref_coeff else None)
+            side.wait_stream(main)
+            with torch.cuda.stream(side):
+                rc = e.lib.tp_copy_columns(ctypes.c_void_p(grad_out.data_ptr()), ctypes.c_void_p(gn.data_ptr()),
+                                           e.n_obj, e.nz * 8, lo * 8, (hi - lo + 1) * 8,
+                                           ctypes.c_void_p(side.cuda_stream))
+                _native.check(rc, "tp_copy_columns")
+            hi = lo - 1
+        gn.record_stream(side)
+        return gn
 
     def backward(self, field: torch.Tensor, exit_grad: torch.Tensor, is_delta=False) -> torch.Tensor:
         """Exact adjoint from the exit-wave gradient; returns ∂ℓ/∂n (n_obj, nz).
@@ -241,9 +281,15 @@ class PWEGradient2D:
             ex = self.forward(field, pr, probes_ready=pr_ready)
         main.wait_event(amp_ready)
         loss, ge = amplitude_residual(ex, amp)
-        g = self.backward(field, ge)
-        if grad_out is not None:
-            grad_out.copy_(g, non_blocking=True)
+        host_out = (grad_out is not None and not grad_out.is_cuda and grad_out.dtype == torch.complex64
+                    and grad_out.is_contiguous() and tuple(grad_out.shape) == (e.n_obj, e.nz))
+        if streamed and host_out:
+            g = self._backward_ranges(field, ge, grad_out, side)
+            main.wait_stream(side)
+        else:
+            g = self.backward(field, ge)
+            if grad_out is not None:
+                grad_out.copy_(g, non_blocking=True)
         return float(loss.item()), g
 
 
