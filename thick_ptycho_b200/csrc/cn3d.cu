@@ -269,9 +269,10 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_cols_kernel(const FftPlan p
   float2 *base = hat + (size_t)pr * q.N;
   load_twiddles(tw, twg, nb);
   for (int e = threadIdx.x; e < cpc * nb; e += blockDim.x) {
-    const int c = e % cpc, bb = e / cpc;  // coalesced over c
-    a[fslot<NB>(c, bb, nb)] = base[(size_t)bb * nf + f0 + c];
+    const int c = e % cpc, bb = e / cpc;  // coalesced over c; asynchronous copies
+    cp_async8(&a[fslot<NB>(c, bb, nb)], &base[(size_t)bb * nf + f0 + c]);
   }
+  cp_async_wait_all();
   __syncthreads();
   float2 *F = fft_rows<NB>(a, b, pl, tw, false, cpc);
   float2 *o = (F == a) ? b : a;
@@ -302,7 +303,8 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_inv_kernel(const FftPl
   const int tot = rpc * n;
   auto slot = [&](int e) { return fslot<NF>(e / n, e % n, n); };
   load_twiddles(tw, twg, n);
-  for (int e = threadIdx.x; e < tot; e += blockDim.x) a[slot(e)] = hat[off + e];
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) cp_async8(&a[slot(e)], &hat[off + e]);
+  cp_async_wait_all();
   __syncthreads();
   const float2 *res = fft_rows<NF>(a, b, pl, tw, true, rpc);
   for (int e = threadIdx.x; e < tot; e += blockDim.x) out[off + e] = res[slot(e)];
