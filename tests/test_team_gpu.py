@@ -100,19 +100,24 @@ def test_team_groups_of_four_with_partial_group_and_gradient():
     assert rel(got, gref) < GRAD_TOL, rel(got, gref)
 
 
-def test_team_pair_sums_store_and_cayley_adjoint():
+@pytest.mark.parametrize("N,k", [(1024, K), (2048, K), (2048, 0.5)])
+def test_team_pair_sums_store_and_cayley_adjoint(N, k):
     """store_sums: the forward store holds (u_t + u_{t-1})/2; the exact adjoint
     reading those sums (one slice per step, Cayley-form step) gives the same
-    lambda and gradient as the two-slice form and as the oracle."""
+    lambda and gradient as the two-slice form and as the oracle.  N = 2048 at
+    k = 4 pi keeps 8 spike rows (the shared-memory staged bulk stores, bulk
+    half-sum loads and CTA gradient accumulator); k = 0.5 couples the chunks
+    strongly (all 15 spike rows, parallel cyclic reduction), where the staging
+    does not fit and the direct per-thread path runs."""
     from thick_ptycho_b200._native import NativeLibraryError
 
-    N, nz, P = 1024, 24, 9
+    nz, P = 24, 9
     n = _field(N, nz, 11)
     probes = _probes(N, P, 12)
-    eng = CN2D(N, nz, K, DX, DZ, "impedance")
-    co = po.bc_coefficients(K, DX, DZ, bc_type="impedance")
+    eng = CN2D(N, nz, k, DX, DZ, "impedance")
+    co = po.bc_coefficients(k, DX, DZ, bc_type="impedance")
     A, B = po.step_matrices_1d(N, co, "impedance", DZ)
-    C = po.object_contribution(n, K, DZ)
+    C = po.object_contribution(n, k, DZ)
     field = torch.from_numpy(n).cuda()
     pr = torch.from_numpy(probes.astype(np.complex64)).cuda()
     ff = eng.factor(field, "forward")
@@ -153,7 +158,7 @@ def test_team_pair_sums_store_and_cayley_adjoint():
     # checkpoint stores keep states; the warp path (N = 256) has no pair sums
     with pytest.raises(NativeLibraryError):
         eng.march(ff, P, probes=pr, u_store=eng.new_store(P, 4), store_every=8, store_sums=True)
-    small = CN2D(256, nz, K, DX, DZ, "impedance")
+    small = CN2D(256, nz, k, DX, DZ, "impedance")
     with pytest.raises(NativeLibraryError):
         small.march(small.factor(torch.from_numpy(n[:256]).cuda(), "forward"), 1, u_store=small.new_store(1),
                     store_sums=True)

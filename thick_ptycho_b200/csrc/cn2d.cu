@@ -832,6 +832,11 @@ extern "C" int tp_cn2d_march(const tp_cn2d_op *op, const void *factors, const tp
       return set_error(TP_ERR_UNSUPPORTED,
                        "N=%d uses the team kernels, which need purely imaginary off-diagonals of K "
                        "(mu = i dz/(4 k dx^2))", op->n);
+    // 16-byte row-pair vectors and whole-slice bulk copies (stores, loads, reductions)
+    const void *vec[] = {a->u_store, a->u_fwd, a->grad_c, a->state_in, a->state_out};
+    for (const void *v : vec)
+      if (v != nullptr && (reinterpret_cast<uintptr_t>(v) & 15u) != 0)
+        return set_error(TP_ERR_INVALID, "the team path needs 16-byte aligned u_store, u_fwd, grad_c, state_in, state_out");
     return launch_team_march(pt, mp, lagged, reinterpret_cast<cudaStream_t>(stream));
   }
   return launch_march(pt.M, mp, op->n == pt.C * pt.M, lagged, reinterpret_cast<cudaStream_t>(stream));

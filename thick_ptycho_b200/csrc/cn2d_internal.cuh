@@ -115,6 +115,6 @@ int team_spike_rows(const tp_cn2d_op *op, int M);
 
 // Team-path launcher (cn2d_team.cu).
 int launch_team_march(const Partition &pt, MarchParams &mp, bool lagged, cudaStream_t st);
-size_t team_smem_bytes(const Partition &pt, int trunc, int Q, int TM, bool qd);
+size_t team_smem_bytes(const Partition &pt, int trunc, int Q, int TM, bool qd, bool stg);
 
 }  // namespace tp

@@ -13,10 +13,13 @@
 // spike vectors are staged (they decay geometrically; T is chosen from the
 // operator and verified when factorising).
 //
-// Exact-adjoint gradient: the Q probes' contributions lambda*conj(u_s+u_{s-1})
-// are summed in registers and added to the chunked gradient buffer with
-// fire-and-forget 16-byte vector reductions (one per row pair), coalesced
-// across the team; no shared-memory accumulator or flush stage is needed.
+// Exact-adjoint gradient: each probe's contribution lambda*conj(u_s+u_{s-1})
+// is added to the chunked gradient buffer.  In the Cayley-form kernel the
+// forward half sums arrive by bulk loads into shared memory, each team
+// writes its contributions over them, and the CTA sums its teams before one
+// 16-byte vector reduction per row pair (a quarter of the global reductions
+// of one per probe); the two-slice kernel adds each probe's contribution
+// with its own vector reductions.
 #include "cn2d_internal.cuh"
 #include <stdio.h>
 #include <stdlib.h>
@@ -72,9 +75,18 @@ __host__ __device__ inline size_t team_slice_smem(int M, int T, bool qd = true) 
   return (size_t)((qd ? 3 : 2) * M + 2 * T + 3 + 2 * kTeamLevels) * kTeamChunks * sizeof(float2);
 }
 
-size_t team_smem_bytes(const Partition &pt, int trunc, int Q, int TM, bool qd) {
-  return 2 * team_slice_smem(pt.M, trunc, qd) + 6 * (size_t)TM * Q * kTeamChunks * sizeof(float2) +
-         2 * sizeof(uint64_t);
+// Exchange rows per probe: Y0, R0, R1, XS, and for the stencil (qd) XL, XF.
+__host__ __device__ constexpr int team_xrows(bool qd) { return qd ? 6 : 4; }
+
+// Shared memory of a team kernel: the factor double buffer, the exchange
+// rows, for the staged kernels (stg; never the two-slice exact adjoint, qd)
+// one staging slice per probe, and the mbarriers (factor double buffer, one
+// per team).
+size_t team_smem_bytes(const Partition &pt, int trunc, int Q, int TM, bool qd, bool stg) {
+  const size_t slice = (size_t)pt.M * kTeamChunks * sizeof(float2);
+  const size_t stage = (qd || !stg) ? 0 : (size_t)TM * Q * slice;
+  return 2 * team_slice_smem(pt.M, trunc, qd) + (size_t)team_xrows(qd) * TM * Q * kTeamChunks * sizeof(float2) +
+         stage + (2 + (size_t)TM) * sizeof(uint64_t);
 }
 
 // Issue the bulk copies of one slice's factor set ([QD|]LF|EP, V head, W tail, records).
@@ -130,8 +142,8 @@ __device__ __forceinline__ void team_rhs(float2 (&U)[Q][M], const float2 *__rest
 
 // U <- M_s^{-1} U with the staged factor slice F (T spike rows staged: a
 // compile-time count, so the spike corrections touch only those rows; QD:
-// the slice starts with the QD rows).
-template <int M, int Q, int T, bool QD>
+// the slice starts with the QD rows; WAITR: the caller stages bulk stores).
+template <int M, int Q, int T, bool QD, bool WAITR>
 __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__restrict__ F, float2 *Y0,
                                            float2 *R0, float2 *R1, float2 *XS, int c, int team, const Spec &sp,
                                            bool pcr) {
@@ -162,6 +174,13 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
       const float2 t = imul_acc(bsup, U[q][i + 1], U[q][i]);
       U[q][i] = cfma(t, ep, t);
     }
+  }
+  // The staging slice that is written after this solve may still be read by
+  // the bulk store issued from it in the previous step: the issuing thread
+  // waits for that read before the exchange barrier below, which every
+  // thread of the team passes before it writes the staging slice again.
+  if constexpr (WAITR) {
+    if (c == 0) bulk_wait_read();
   }
   float2 x[Q], xp[Q];
   constexpr int kRd = 2 + 2 * kTeamLevels;  // record row of the reduced diagonal
@@ -253,18 +272,105 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
   for (int q = 0; q < Q; ++q) U[q][M - 1] = x[q];
 }
 
+// Forward store through the staging slices: thread c writes its row pairs of
+// the Q probes (conflict-free 16-byte shared stores), and after the team
+// barrier thread 0 copies each probe's slice to store slice sidx with one
+// bulk store.  The staging slices are written again only after the next
+// solve's exchange barrier, before which thread 0 waits for the copy's read.
+template <int M, int Q>
+__device__ __forceinline__ void store_staged(const float2 (&U)[Q][M], float4 *stg, const MarchParams &p, int p0,
+                                             int sidx, int c, int team) {
+  constexpr int C = kTeamChunks;
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    if (p0 + q >= p.P) continue;
+#pragma unroll
+    for (int j = 0; j < M / 2; ++j)
+      stg[(q * (M / 2) + j) * C + c] =
+          make_float4(U[q][2 * j].x, U[q][2 * j].y, U[q][2 * j + 1].x, U[q][2 * j + 1].y);
+  }
+  fence_proxy_async_smem();
+  team_sync(team);
+  if (c == 0) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+      if (p0 + q < p.P)
+        bulk_s2g(p.u_store + ((size_t)(p0 + q) * p.store_slices + sidx) * p.Npad, stg + (size_t)q * (M / 2) * C,
+                 M * C * sizeof(float2));
+    bulk_commit();
+  }
+}
+
+// Exact-adjoint gradient of one team and step: the team's staging slice
+// holds this step's forward half pair sums (u_s + u_{s-1})/2, bulk-loaded
+// ahead of the solve; each row pair is replaced in place by its contribution
+// 2 lambda conj(half sum) (zeros for a padded probe), so that after the
+// end-of-step barrier the CTA's teams can be summed before the gradient row
+// is updated (grad_sum_flush).
+template <int M>
+__device__ __forceinline__ void grad_contrib(const float2 (&U)[1][M], float4 *stg, bool valid, int c) {
+  constexpr int C = kTeamChunks;
+#pragma unroll
+  for (int j = 0; j < M / 2; ++j) {
+    float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid) {
+      const float4 v = stg[j * C + c];
+      const float2 a = cmulc(U[0][2 * j], make_float2(v.x, v.y));
+      const float2 b = cmulc(U[0][2 * j + 1], make_float2(v.z, v.w));
+      w = make_float4(2.f * a.x, 2.f * a.y, 2.f * b.x, 2.f * b.y);
+    }
+    stg[j * C + c] = w;
+  }
+}
+
+// Sum the TM teams' contribution slices and add them to gradient row `row`
+// (chunked row pairs) with 16-byte vector reductions: one reduction per row
+// pair and CTA instead of one per probe.  Every thread of the CTA takes its
+// share of the row pairs; the slices are complete after a CTA barrier and
+// free for the next bulk loads after the next one.
+template <int M, int TM>
+__device__ __forceinline__ void grad_sum_flush(const float4 *stage, float2 *row, int tid) {
+  constexpr int E = (M / 2) * kTeamChunks, NT = TM * kTeamThreads;
+  float4 *g = reinterpret_cast<float4 *>(row);
+#pragma unroll
+  for (int e = tid; e < E; e += NT) {
+    float4 v = stage[e];
+#pragma unroll
+    for (int m = 1; m < TM; ++m) {
+      const float4 w = stage[m * E + e];
+      v = make_float4(v.x + w.x, v.y + w.y, v.z + w.z, v.w + w.w);
+    }
+    red_add_v4(g + e, v);
+  }
+  // the slices are next written by bulk loads (async proxy)
+  fence_proxy_async_smem();
+}
+
 // TS: spike rows staged per slice (>= the rows the factorisation found
 // significant).  LAGGED: exact-adjoint order (solve, gradient, then the
 // right-hand side of the same slice).  SUMS (LAGGED only): that step in Cayley form, with u_fwd
 // (when given) holding the half pair sums (u_s + u_{s-1})/2 written by a
 // forward march with store_sums, so one forward slice is read per step and
 // the registers of the second serve the Cayley step.
-template <int M, int Q, int TM, bool LAGGED, bool SUMS, int TS>
+//
+// STG: whole-slice global traffic goes through one staging slice per probe
+// in shared memory (never in the two-slice exact adjoint; the host selects it
+// where it fits beside the factor double buffer, i.e. all but the 15-spike-row
+// factor sets, which keep direct per-thread stores and loads): the forward
+// stores its slices with bulk stores, and the exact adjoint's gradient has
+// its half-sum slice bulk-loaded one step ahead (no registers hold data in
+// flight) and its contribution summed over the CTA's teams before it
+// reaches global memory.
+template <int M, int Q, int TM, bool LAGGED, bool SUMS, int TS, bool STG>
 __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const MarchParams p) {
   static_assert(LAGGED || !SUMS, "SUMS selects the exact-adjoint Cayley step");
-  constexpr bool QD = LAGGED && !SUMS;  // only the two-slice exact adjoint applies the stencil
+  static_assert(!LAGGED || Q == 1, "exact-adjoint kernels march one probe per thread");
+  constexpr bool QD = LAGGED && !SUMS;     // only the two-slice exact adjoint applies the stencil
+  constexpr bool STAGE = !QD && STG;              // staging slices in shared memory
+  constexpr bool GSTAGE = LAGGED && SUMS && STG;  // the gradient goes through them
   constexpr int C = kTeamChunks;
   constexpr int NT = kTeamThreads * TM;
+  constexpr uint32_t NB = M * C * sizeof(float2);  // bytes of one probe's slice
   extern __shared__ __align__(128) unsigned char smem[];
   const int tid = threadIdx.x;
   const int team = tid / kTeamThreads;
@@ -272,10 +378,16 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
   constexpr int T = TS;  // the host sets p.trunc = TS
   const size_t ss = p.smem_slice_bytes;
   float2 *bufs = reinterpret_cast<float2 *>(smem);
-  float2 *XL = reinterpret_cast<float2 *>(smem + 2 * ss) + (size_t)team * 6 * Q * C;
-  float2 *XF = XL + Q * C, *Y0 = XF + Q * C, *R0 = Y0 + Q * C, *R1 = R0 + Q * C, *XS = R1 + Q * C;
+  constexpr int XR = team_xrows(QD);
+  float2 *xb = reinterpret_cast<float2 *>(smem + 2 * ss) + (size_t)team * XR * Q * C;
+  float2 *XL = QD ? xb : nullptr, *XF = QD ? xb + Q * C : nullptr;  // stencil rows (QD only)
+  float2 *Y0 = xb + (QD ? 2 : 0) * Q * C, *R0 = Y0 + Q * C, *R1 = R0 + Q * C, *XS = R1 + Q * C;
+  float4 *stage = reinterpret_cast<float4 *>(smem + 2 * ss + (size_t)TM * XR * Q * C * sizeof(float2));
+  float4 *stg = stage + (size_t)team * Q * (M / 2) * C;  // this team's Q staging slices
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(reinterpret_cast<unsigned char *>(stage) +
+                                                (STAGE ? (size_t)TM * Q * NB : 0));
+  uint64_t *gbar = mbar + 2;  // one per team: its half-sum slice
   const bool do_grad = LAGGED && (p.grad_c != nullptr);
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(reinterpret_cast<float2 *>(smem + 2 * ss) + (size_t)TM * 6 * Q * C);
   const size_t ssf = ss / sizeof(float2);
   const int p0 = (blockIdx.x * TM + team) * Q;
   const bool pcr = p.coupling == nullptr || __uint_as_float(__ldg(p.coupling)) >= kPcrSkipBound;
@@ -283,6 +395,8 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
   if (tid == 0) {
     mbar_init(&mbar[0], 1);
     mbar_init(&mbar[1], 1);
+#pragma unroll
+    for (int m = 0; m < TM; ++m) mbar_init(&gbar[m], 1);
     fence_mbar_init();
   }
   __syncthreads();
@@ -319,16 +433,17 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
     }
   }
 
-  // Gradient: the forward slice u_s of the current step is kept from the
-  // previous step (u_prev); only u_{s-1} is read, issued at the start of the
-  // step so that its latency overlaps the solve.  With SUMS the one slice
-  // read is the pair sum itself.
+  // Two-slice gradient (QD): the forward slice u_s of the current step is
+  // kept from the previous step (u_prev); only u_{s-1} is read, issued at the
+  // start of the step so that its latency overlaps the solve.
   float2 u_prev[Q][M], u_new[Q][M];
-  if (do_grad && !SUMS) {
+  if constexpr (QD) {
+    if (do_grad) {
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const int pq = (p0 + q < p.P) ? p0 + q : p.P - 1;
-      load_pairs<M>(u_prev[q], p.u_fwd + ((size_t)pq * p.ufwd_slices + (slice_of(p.t0) - p.ufwd_base)) * p.Npad, c);
+      for (int q = 0; q < Q; ++q) {
+        const int pq = (p0 + q < p.P) ? p0 + q : p.P - 1;
+        load_pairs<M>(u_prev[q], p.u_fwd + ((size_t)pq * p.ufwd_slices + (slice_of(p.t0) - p.ufwd_base)) * p.Npad, c);
+      }
     }
   }
 
@@ -343,21 +458,59 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
     }
   }
 
+  // Half-sum slices of the staged gradient: thread 0 of the team loads the
+  // slice of step t into the team's staging slice at the start of step t,
+  // once the previous step's contributions have been summed out of it.
+  // g_pending / g_pend_par track a load that thread 0 has not yet seen
+  // complete, so that an early return waits for it.
+  const bool gvalid = p0 < p.P;
+  uint32_t gphase = 0, g_pend_par = 0;
+  bool g_pending = false;
+  auto half_sums = [&](int t) {
+    return p.u_fwd + ((size_t)p0 * p.ufwd_slices + (slice_of(t) - p.ufwd_base)) * p.Npad;
+  };
+  if constexpr (GSTAGE) {
+    if (do_grad && c == 0 && gvalid) {
+      mbar_arrive_expect_tx(&gbar[team], NB);
+      bulk_g2s(stg, half_sums(p.t0), NB, &gbar[team]);
+      g_pending = true;
+      g_pend_par = gphase;
+    }
+  }
+
   for (int t = p.t0; t <= p.t1; ++t) {
     const int cb = (t - p.t0 + 1) & 1;
     const int s = slice_of(t);
+    if constexpr (GSTAGE) {
+      // the previous step's contributions are complete (end-of-step
+      // barrier): sum them into the gradient, then reload the slices
+      if (do_grad && t > p.t0) {
+        grad_sum_flush<M, TM>(stage, p.grad_c + (size_t)(slice_of(t - 1) - 1) * p.Npad, tid);
+        __syncthreads();
+        if (c == 0 && gvalid) {
+          mbar_arrive_expect_tx(&gbar[team], NB);
+          bulk_g2s(stg, half_sums(t), NB, &gbar[team]);
+          g_pending = true;
+          g_pend_par = gphase;
+        }
+      }
+    }
     if (tid == 0 && t < p.t1) {
       fence_proxy_async_smem();
       team_issue(bufs + (cb ^ 1) * ssf, p.factors + (size_t)(slice_of(t + 1) - 1) * p.slice_bytes, M, T,
                  &mbar[cb ^ 1], QD);
     }
     const float2 *F = bufs + cb * ssf;
-    if (do_grad) {
+    if constexpr (!GSTAGE) {
+      // unstaged gradient: this step's forward slice (QD: u_{s-1}; SUMS: the
+      // half sum), issued before the solve so that its latency overlaps it
+      if (do_grad) {
 #pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        const int pq = (p0 + q < p.P) ? p0 + q : p.P - 1;
-        const int ix = SUMS ? s - p.ufwd_base : s - 1 - p.ufwd_base;
-        load_pairs<M>(u_new[q], p.u_fwd + ((size_t)pq * p.ufwd_slices + ix) * p.Npad, c);
+        for (int q = 0; q < Q; ++q) {
+          const int pq = (p0 + q < p.P) ? p0 + q : p.P - 1;
+          const int ix = SUMS ? s - p.ufwd_base : s - 1 - p.ufwd_base;
+          load_pairs<M>(u_new[q], p.u_fwd + ((size_t)pq * p.ufwd_slices + ix) * p.Npad, c);
+        }
       }
     }
     // Forward and reference-adjoint steps use the Cayley form of the step:
@@ -404,28 +557,31 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
 #pragma unroll
         for (int i = 0; i < M; ++i) u_old[q][i] = U[q][i];
     }
-    team_solve<M, Q, T, QD>(U, F, Y0, R0, R1, XS, c, team, p.sp, pcr);
+    team_solve<M, Q, T, QD, STAGE && !LAGGED>(U, F, Y0, R0, R1, XS, c, team, p.sp, pcr);
     const int sidx = p.u_store != nullptr ? store_index(p, t) : -1;
+    auto store_direct = [&]() {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        if (p0 + q >= p.P) continue;
+        store_pairs(p.u_store + ((size_t)(p0 + q) * p.store_slices + sidx) * p.Npad, U[q], M, c);
+      }
+    };
     if constexpr (!LAGGED) {
       if (p.store_sums && sidx >= 0) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-          if (p0 + q >= p.P) continue;
-          store_pairs(p.u_store + ((size_t)(p0 + q) * p.store_slices + sidx) * p.Npad, U[q], M, c);
-        }
+        if constexpr (STAGE) store_staged<M, Q>(U, stg, p, p0, sidx, c, team);
+        else store_direct();
       }
 #pragma unroll
       for (int q = 0; q < Q; ++q)
 #pragma unroll
         for (int i = 0; i < M; ++i)
           U[q][i] = make_float2(fmaf(2.f, U[q][i].x, -u_old[q][i].x), fmaf(2.f, U[q][i].y, -u_old[q][i].y));
-    }
-    if (sidx >= 0 && (LAGGED || !p.store_sums)) {
-#pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        if (p0 + q >= p.P) continue;
-        store_pairs(p.u_store + ((size_t)(p0 + q) * p.store_slices + sidx) * p.Npad, U[q], M, c);
+      if (!p.store_sums && sidx >= 0) {
+        if constexpr (STAGE) store_staged<M, Q>(U, stg, p, p0, sidx, c, team);
+        else store_direct();
       }
+    } else {
+      if (sidx >= 0) store_direct();
     }
     if (t == p.L && p.exit_out != nullptr) {
 #pragma unroll
@@ -436,37 +592,47 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
         for (int i = 0; i < M; ++i) dst[i] = U[q][i];
       }
     }
+    bool good = true;
     if (do_grad) {
-      float4 *gdst = reinterpret_cast<float4 *>(p.grad_c + (size_t)(s - 1) * p.Npad) + c;
+      if constexpr (GSTAGE) {
+        bool okg = true;
+        if (gvalid) okg = mbar_wait_bounded(&gbar[team], gphase, p.err);
+        if (okg) g_pending = false;
+        gphase ^= 1u;
+        good = okg;
+        grad_contrib<M>(U, stg, gvalid, c);
+      } else {
+        float4 *gdst = reinterpret_cast<float4 *>(p.grad_c + (size_t)(s - 1) * p.Npad) + c;
 #pragma unroll
-      for (int j = 0; j < M / 2; ++j) {
-        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int j = 0; j < M / 2; ++j) {
+          float4 ga = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-          if (p0 + q >= p.P) continue;  // padded probes contribute nothing
-          float2 wa, wb;
-          if constexpr (SUMS) {
-            wa = u_new[q][2 * j];
-            wb = u_new[q][2 * j + 1];
-          } else {
-            wa = cadd(u_prev[q][2 * j], u_new[q][2 * j]);
-            wb = cadd(u_prev[q][2 * j + 1], u_new[q][2 * j + 1]);
+          for (int q = 0; q < Q; ++q) {
+            if (p0 + q >= p.P) continue;  // padded probes contribute nothing
+            float2 wa, wb;
+            if constexpr (SUMS) {
+              wa = u_new[q][2 * j];
+              wb = u_new[q][2 * j + 1];
+            } else {
+              wa = cadd(u_prev[q][2 * j], u_new[q][2 * j]);
+              wb = cadd(u_prev[q][2 * j + 1], u_new[q][2 * j + 1]);
+            }
+            const float2 a = cmulc(U[q][2 * j], wa);
+            const float2 b = cmulc(U[q][2 * j + 1], wb);
+            ga.x += a.x;
+            ga.y += a.y;
+            ga.z += b.x;
+            ga.w += b.y;
           }
-          const float2 a = cmulc(U[q][2 * j], wa);
-          const float2 b = cmulc(U[q][2 * j + 1], wb);
-          acc.x += a.x;
-          acc.y += a.y;
-          acc.z += b.x;
-          acc.w += b.y;
+          if constexpr (SUMS) ga = make_float4(2.f * ga.x, 2.f * ga.y, 2.f * ga.z, 2.f * ga.w);  // half sums
+          red_add_v4(gdst + j * C, ga);
         }
-        if constexpr (SUMS) acc = make_float4(2.f * acc.x, 2.f * acc.y, 2.f * acc.z, 2.f * acc.w);  // half sums
-        red_add_v4(gdst + j * C, acc);
-      }
-      if constexpr (!SUMS) {
+        if constexpr (!SUMS) {
 #pragma unroll
-        for (int q = 0; q < Q; ++q)
+          for (int q = 0; q < Q; ++q)
 #pragma unroll
-          for (int i = 0; i < M; ++i) u_prev[q][i] = u_new[q][i];
+            for (int i = 0; i < M; ++i) u_prev[q][i] = u_new[q][i];
+        }
       }
     }
     if constexpr (SUMS) {
@@ -478,16 +644,25 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
     } else if constexpr (LAGGED) {
       team_rhs<M, Q>(U, F, XL, XF, c, team, p.sp);
     }
-    bool good = true;
     if (t < p.t1) {
-      good = mbar_wait_bounded(&mbar[cb ^ 1], (phase >> (cb ^ 1)) & 1u, p.err);
+      const bool okf = mbar_wait_bounded(&mbar[cb ^ 1], (phase >> (cb ^ 1)) & 1u, p.err);
+      good = good && okf;
       phase ^= (1u << (cb ^ 1));
     }
     if (__syncthreads_or(!good)) {
       if (tid == 0) mbar_wait_bounded(&mbar[cb ^ 1], ((phase >> (cb ^ 1)) & 1u) ^ 1u, nullptr);
+      if constexpr (STAGE) {
+        if (c == 0) {
+          if (g_pending) mbar_wait_bounded(&gbar[team], g_pend_par, nullptr);
+          bulk_wait();
+        }
+      }
       __syncthreads();
       return;
     }
+  }
+  if constexpr (GSTAGE) {
+    if (do_grad) grad_sum_flush<M, TM>(stage, p.grad_c + (size_t)(slice_of(p.t1) - 1) * p.Npad, tid);
   }
   if (p.state_out != nullptr) {
 #pragma unroll
@@ -496,40 +671,48 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
       store_pairs(p.state_out + (size_t)(p0 + q) * p.Npad, U[q], M, c);
     }
   }
+  if constexpr (STAGE) {
+    if (c == 0) bulk_wait();
+  }
 }
 
-template <int M, int Q, int TM, bool LAGGED, bool SUMS, int TS>
+template <int M, int Q, int TM, bool LAGGED, bool SUMS, int TS, bool STG>
 static int launch_team_t(const Partition &pt, MarchParams &mp, cudaStream_t st) {
-  auto kern = cn2d_team_kernel<M, Q, TM, LAGGED, SUMS, TS>;
+  auto kern = cn2d_team_kernel<M, Q, TM, LAGGED, SUMS, TS, STG>;
   if (mp.trunc != TS) return set_error(TP_ERR_INVALID, "team march staged %d spike rows, kernel has %d", mp.trunc, TS);
   constexpr bool QD = LAGGED && !SUMS;
   mp.smem_slice_bytes = team_slice_smem(M, TS, QD);
-  const size_t smem = team_smem_bytes(pt, mp.trunc, Q, TM, QD);
+  const size_t smem = team_smem_bytes(pt, mp.trunc, Q, TM, QD, STG);
   TP_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = (mp.P + Q * TM - 1) / (Q * TM);
   kern<<<grid, kTeamThreads * TM, smem, st>>>(mp);
   return check_cuda(cudaGetLastError(), "cn2d_team_kernel launch");
 }
 
-template <int M, bool LAGGED, bool SUMS, int TS>
+template <int M, bool LAGGED, bool SUMS, int TS, bool STG>
 static int launch_team_qt(const Partition &pt, MarchParams &mp, int Q, int TM, cudaStream_t st) {
-  if (TM == 1 && Q == 1) return launch_team_t<M, 1, 1, LAGGED, SUMS, TS>(pt, mp, st);
-  if (TM == 2 && Q == 1) return launch_team_t<M, 1, 2, LAGGED, SUMS, TS>(pt, mp, st);
-  if (TM == 4 && Q == 1) return launch_team_t<M, 1, 4, LAGGED, SUMS, TS>(pt, mp, st);
+  if (TM == 1 && Q == 1) return launch_team_t<M, 1, 1, LAGGED, SUMS, TS, STG>(pt, mp, st);
+  if (TM == 2 && Q == 1) return launch_team_t<M, 1, 2, LAGGED, SUMS, TS, STG>(pt, mp, st);
+  if (TM == 4 && Q == 1) return launch_team_t<M, 1, 4, LAGGED, SUMS, TS, STG>(pt, mp, st);
   if constexpr (!LAGGED) {
-    if (TM == 2 && Q == 2) return launch_team_t<M, 2, 2, LAGGED, SUMS, TS>(pt, mp, st);
+    if (TM == 2 && Q == 2) return launch_team_t<M, 2, 2, LAGGED, SUMS, TS, STG>(pt, mp, st);
   }
   return set_error(TP_ERR_UNSUPPORTED, "no team kernel for Q=%d, TM=%d", Q, TM);
 }
 
 // Exact adjoint in Cayley form unless a gradient reads plain forward slices
-// (two per step: not enough registers for the Cayley state as well).
+// (two per step: not enough registers for the Cayley state as well).  The
+// staged variants exist for the Cayley-form kernels only.
 template <int M, int TS>
-static int launch_team_m(const Partition &pt, MarchParams &mp, bool lagged, bool sums, int Q, int TM,
+static int launch_team_m(const Partition &pt, MarchParams &mp, bool lagged, bool sums, bool stg, int Q, int TM,
                          cudaStream_t st) {
-  if (!lagged) return launch_team_qt<M, false, false, TS>(pt, mp, Q, TM, st);
-  return sums ? launch_team_qt<M, true, true, TS>(pt, mp, Q, TM, st)
-              : launch_team_qt<M, true, false, TS>(pt, mp, Q, TM, st);
+  if (!lagged)
+    return stg ? launch_team_qt<M, false, false, TS, true>(pt, mp, Q, TM, st)
+               : launch_team_qt<M, false, false, TS, false>(pt, mp, Q, TM, st);
+  if (sums)
+    return stg ? launch_team_qt<M, true, true, TS, true>(pt, mp, Q, TM, st)
+               : launch_team_qt<M, true, true, TS, false>(pt, mp, Q, TM, st);
+  return launch_team_qt<M, true, false, TS, false>(pt, mp, Q, TM, st);
 }
 
 // (teams per CTA, probes per thread) for K probes per CTA: one probe per
@@ -568,21 +751,25 @@ int launch_team_march(const Partition &pt, MarchParams &mp, bool lagged, cudaStr
   } else {
     team_shape(K, &TM, &Q);
   }
-  while (team_smem_bytes(pt, mp.trunc, Q, TM, qd) > (size_t)max_smem && TM * Q > 1) {
+  // Staged global traffic where the staging slices fit beside the factor
+  // double buffer at this shape; otherwise the direct path at this shape
+  // (fewer teams per CTA would mean more CTAs than SMs).
+  const bool stg = !qd && team_smem_bytes(pt, mp.trunc, Q, TM, qd, true) <= (size_t)max_smem;
+  while (team_smem_bytes(pt, mp.trunc, Q, TM, qd, stg) > (size_t)max_smem && TM * Q > 1) {
     if (TM > 1) TM /= 2;
     else Q /= 2;
   }
-  if (team_smem_bytes(pt, mp.trunc, Q, TM, qd) > (size_t)max_smem)
+  if (team_smem_bytes(pt, mp.trunc, Q, TM, qd, stg) > (size_t)max_smem)
     return set_error(TP_ERR_UNSUPPORTED, "team march needs %zu B of shared memory (> %d)",
-                     team_smem_bytes(pt, mp.trunc, Q, TM, qd), max_smem);
+                     team_smem_bytes(pt, mp.trunc, Q, TM, qd, stg), max_smem);
   switch (pt.M) {
     case 4:
-      return launch_team_m<4, 3>(pt, mp, lagged, sums, Q, TM, st);
+      return launch_team_m<4, 3>(pt, mp, lagged, sums, stg, Q, TM, st);
     case 8:
-      return launch_team_m<8, 7>(pt, mp, lagged, sums, Q, TM, st);
+      return launch_team_m<8, 7>(pt, mp, lagged, sums, stg, Q, TM, st);
     case 16:
-      return mp.trunc == 8 ? launch_team_m<16, 8>(pt, mp, lagged, sums, Q, TM, st)
-                           : launch_team_m<16, 15>(pt, mp, lagged, sums, Q, TM, st);
+      return mp.trunc == 8 ? launch_team_m<16, 8>(pt, mp, lagged, sums, stg, Q, TM, st)
+                           : launch_team_m<16, 15>(pt, mp, lagged, sums, stg, Q, TM, st);
     default:
       return set_error(TP_ERR_UNSUPPORTED, "no team kernel for %d rows per chunk", pt.M);
   }

@@ -1,5 +1,5 @@
 // Shared device helpers for libtpcuda: complex arithmetic, bulk-copy (TMA)
-// staging with bounded mbarrier waits, and the error channel.
+// staging with bounded mbarrier waits, bulk stores, and the error channel.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -94,6 +94,22 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       "l"(src), "r"(bytes), "r"(smem_addr(bar))
       : "memory");
 }
+// Shared -> global bulk copy, tracked by the issuing thread's bulk groups
+// (commit with bulk_commit; the source may be rewritten after
+// bulk_wait_read, the global result is complete after bulk_wait).  Addresses
+// 16-byte aligned, bytes a multiple of 16.  The generic-proxy writes of the
+// source must be followed by fence_proxy_async_smem and a barrier before the
+// issuing thread copies.
+__device__ __forceinline__ void bulk_s2g(void *gdst, const void *ssrc, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_addr(ssrc)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Every committed bulk group of this thread has finished reading shared memory.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// Every committed bulk group of this thread has completed.
+__device__ __forceinline__ void bulk_wait() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 // 8-byte global -> shared asynchronous copy (no registers; completes at
 // cp_async_wait_all).  Both addresses 8-byte aligned.
 __device__ __forceinline__ void cp_async8(void *dst, const void *src) {
