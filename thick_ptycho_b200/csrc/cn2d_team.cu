@@ -176,12 +176,12 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
     }
   }
   // The staging slice that is written after this solve may still be read by
-  // the bulk store issued from it in the previous step: the issuing thread
+  // the bulk store issued from it in the previous step: its issuing thread
   // waits for that read before the exchange barrier below, which every
-  // thread of the team passes before it writes the staging slice again.
-  if constexpr (WAITR) {
-    if (c == 0) bulk_wait_read();
-  }
+  // thread of the team passes before it writes the staging slice again (the
+  // wait is executed by all threads, without a branch; it returns at once
+  // in threads with no bulk copies in flight).
+  if constexpr (WAITR) bulk_wait_read();
   float2 x[Q], xp[Q];
   constexpr int kRd = 2 + 2 * kTeamLevels;  // record row of the reduced diagonal
   if (!pcr) {
