@@ -136,9 +136,10 @@ def test_reference_gradient_agreement(golden):
 
 def test_streamed_host_index_field_equals_device_field():
     """A host (pinned) index field is uploaded in column blocks with the
-    forward march following range by range; loss and gradient must equal
-    those of a device-resident field (the same kernels on the same data),
-    on two calls in a row."""
+    forward march following range by range (the later ranges and the adjoint
+    factorised on a second stream beside the marches); loss and gradient must
+    equal those of a device-resident field (the same kernels on the same
+    data), on two calls in a row, and with the gradient kept on the device."""
     geo, n, probes, amp = _problem(1024, 200, 40, 3)
     pg = PWEGradient2D(geo)
     n_h = torch.from_numpy(n).pin_memory()
@@ -155,3 +156,13 @@ def test_streamed_host_index_field_equals_device_field():
         assert abs(l_h - l_dev) <= 1e-12 * abs(l_dev)
         assert rel(g_h.numpy(), g_dev) < 1e-7
         assert rel(g.cpu().numpy(), g_dev) < 1e-7
+    # streamed index field with the gradient left on the device, or copied
+    # into a device tensor (factorisations on the factor stream, one adjoint)
+    l_h2, g2 = pg.loss_and_grad(n_h, p_h, a_h)
+    g_d = torch.empty_like(g2)
+    pg.loss_and_grad(n_h, p_h, a_h, grad_out=g_d)
+    torch.cuda.synchronize()
+    pg.engine.device_status()
+    assert abs(l_h2 - l_dev) <= 1e-12 * abs(l_dev)
+    assert rel(g2.cpu().numpy(), g_dev) < 1e-7
+    assert rel(g_d.cpu().numpy(), g_dev) < 1e-7

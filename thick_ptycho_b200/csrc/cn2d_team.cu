@@ -301,34 +301,38 @@ __device__ __forceinline__ void store_staged(const float2 (&U)[Q][M], float4 *st
   }
 }
 
-// Exact-adjoint gradient of one team and step: the team's staging slice
-// holds this step's forward half pair sums (u_s + u_{s-1})/2, bulk-loaded
-// ahead of the solve; each row pair is replaced in place by its contribution
-// 2 lambda conj(half sum) (zeros for a padded probe), so that after the
+// Exact-adjoint gradient of one team and step: the team's Q staging slices
+// hold this step's forward half pair sums (u_s + u_{s-1})/2 of its probes,
+// bulk-loaded ahead of the solve; each row pair's contributions
+// 2 lambda conj(half sum), summed over the Q probes in registers (zero for
+// padded probes), replace the first slice in place, so that after the
 // end-of-step barrier the CTA's teams can be summed before the gradient row
 // is updated (grad_sum_flush).
-template <int M>
-__device__ __forceinline__ void grad_contrib(const float2 (&U)[1][M], float4 *stg, bool valid, int c) {
+template <int M, int Q>
+__device__ __forceinline__ void grad_contrib(const float2 (&U)[Q][M], float4 *stg, int nvalid, int c) {
   constexpr int C = kTeamChunks;
 #pragma unroll
   for (int j = 0; j < M / 2; ++j) {
     float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (valid) {
-      const float4 v = stg[j * C + c];
-      const float2 a = cmulc(U[0][2 * j], make_float2(v.x, v.y));
-      const float2 b = cmulc(U[0][2 * j + 1], make_float2(v.z, v.w));
-      w = make_float4(2.f * a.x, 2.f * a.y, 2.f * b.x, 2.f * b.y);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      if (q >= nvalid) continue;
+      const float4 v = stg[(q * (M / 2) + j) * C + c];
+      const float2 a = cmulc(U[q][2 * j], make_float2(v.x, v.y));
+      const float2 b = cmulc(U[q][2 * j + 1], make_float2(v.z, v.w));
+      w = make_float4(w.x + a.x, w.y + a.y, w.z + b.x, w.w + b.y);
     }
-    stg[j * C + c] = w;
+    stg[j * C + c] = make_float4(2.f * w.x, 2.f * w.y, 2.f * w.z, 2.f * w.w);
   }
 }
 
-// Sum the TM teams' contribution slices and add them to gradient row `row`
+// Sum the TM teams' contribution slices (each team's first staging slice)
+// and add them to gradient row `row`
 // (chunked row pairs) with 16-byte vector reductions: one reduction per row
 // pair and CTA instead of one per probe.  Every thread of the CTA takes its
 // share of the row pairs; the slices are complete after a CTA barrier and
 // free for the next bulk loads after the next one.
-template <int M, int TM>
+template <int M, int Q, int TM>
 __device__ __forceinline__ void grad_sum_flush(const float4 *stage, float2 *row, int tid) {
   constexpr int E = (M / 2) * kTeamChunks, NT = TM * kTeamThreads;
   float4 *g = reinterpret_cast<float4 *>(row);
@@ -337,7 +341,7 @@ __device__ __forceinline__ void grad_sum_flush(const float4 *stage, float2 *row,
     float4 v = stage[e];
 #pragma unroll
     for (int m = 1; m < TM; ++m) {
-      const float4 w = stage[m * E + e];
+      const float4 w = stage[m * Q * E + e];  // team m's first slice
       v = make_float4(v.x + w.x, v.y + w.y, v.z + w.z, v.w + w.w);
     }
     red_add_v4(g + e, v);
@@ -364,12 +368,11 @@ __device__ __forceinline__ void grad_sum_flush(const float4 *stage, float2 *row,
 template <int M, int Q, int TM, bool LAGGED, bool SUMS, int TS, bool STG>
 __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const MarchParams p) {
   static_assert(LAGGED || !SUMS, "SUMS selects the exact-adjoint Cayley step");
-  static_assert(!LAGGED || Q == 1, "exact-adjoint kernels march one probe per thread");
+  static_assert(!LAGGED || Q == 1 || (SUMS && STG), "exact adjoint: several probes per thread only staged");
   constexpr bool QD = LAGGED && !SUMS;     // only the two-slice exact adjoint applies the stencil
   constexpr bool STAGE = !QD && STG;              // staging slices in shared memory
   constexpr bool GSTAGE = LAGGED && SUMS && STG;  // the gradient goes through them
   constexpr int C = kTeamChunks;
-  constexpr int NT = kTeamThreads * TM;
   constexpr uint32_t NB = M * C * sizeof(float2);  // bytes of one probe's slice
   extern __shared__ __align__(128) unsigned char smem[];
   const int tid = threadIdx.x;
@@ -463,19 +466,23 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
   // once the previous step's contributions have been summed out of it.
   // g_pending / g_pend_par track a load that thread 0 has not yet seen
   // complete, so that an early return waits for it.
-  const bool gvalid = p0 < p.P;
+  const int nvalid = p.P - p0 < Q ? p.P - p0 : Q;  // probes of this team (<= 0: padding)
+  const bool gvalid = nvalid > 0;
   uint32_t gphase = 0, g_pend_par = 0;
   bool g_pending = false;
-  auto half_sums = [&](int t) {
-    return p.u_fwd + ((size_t)p0 * p.ufwd_slices + (slice_of(t) - p.ufwd_base)) * p.Npad;
+  auto load_half_sums = [&](int t) {  // thread 0 of the team: step t's slices of its probes
+    mbar_arrive_expect_tx(&gbar[team], (uint32_t)nvalid * NB);
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+      if (q < nvalid)
+        bulk_g2s(stg + (size_t)q * (M / 2) * C,
+                 p.u_fwd + ((size_t)(p0 + q) * p.ufwd_slices + (slice_of(t) - p.ufwd_base)) * p.Npad, NB,
+                 &gbar[team]);
+    g_pending = true;
+    g_pend_par = gphase;
   };
   if constexpr (GSTAGE) {
-    if (do_grad && c == 0 && gvalid) {
-      mbar_arrive_expect_tx(&gbar[team], NB);
-      bulk_g2s(stg, half_sums(p.t0), NB, &gbar[team]);
-      g_pending = true;
-      g_pend_par = gphase;
-    }
+    if (do_grad && c == 0 && gvalid) load_half_sums(p.t0);
   }
 
   for (int t = p.t0; t <= p.t1; ++t) {
@@ -485,14 +492,9 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
       // the previous step's contributions are complete (end-of-step
       // barrier): sum them into the gradient, then reload the slices
       if (do_grad && t > p.t0) {
-        grad_sum_flush<M, TM>(stage, p.grad_c + (size_t)(slice_of(t - 1) - 1) * p.Npad, tid);
+        grad_sum_flush<M, Q, TM>(stage, p.grad_c + (size_t)(slice_of(t - 1) - 1) * p.Npad, tid);
         __syncthreads();
-        if (c == 0 && gvalid) {
-          mbar_arrive_expect_tx(&gbar[team], NB);
-          bulk_g2s(stg, half_sums(t), NB, &gbar[team]);
-          g_pending = true;
-          g_pend_par = gphase;
-        }
+        if (c == 0 && gvalid) load_half_sums(t);
       }
     }
     if (tid == 0 && t < p.t1) {
@@ -600,7 +602,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
         if (okg) g_pending = false;
         gphase ^= 1u;
         good = okg;
-        grad_contrib<M>(U, stg, gvalid, c);
+        grad_contrib<M, Q>(U, stg, nvalid, c);
       } else {
         float4 *gdst = reinterpret_cast<float4 *>(p.grad_c + (size_t)(s - 1) * p.Npad) + c;
 #pragma unroll
@@ -662,7 +664,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
     }
   }
   if constexpr (GSTAGE) {
-    if (do_grad) grad_sum_flush<M, TM>(stage, p.grad_c + (size_t)(slice_of(p.t1) - 1) * p.Npad, tid);
+    if (do_grad) grad_sum_flush<M, Q, TM>(stage, p.grad_c + (size_t)(slice_of(p.t1) - 1) * p.Npad, tid);
   }
   if (p.state_out != nullptr) {
 #pragma unroll
@@ -694,7 +696,7 @@ static int launch_team_qt(const Partition &pt, MarchParams &mp, int Q, int TM, c
   if (TM == 1 && Q == 1) return launch_team_t<M, 1, 1, LAGGED, SUMS, TS, STG>(pt, mp, st);
   if (TM == 2 && Q == 1) return launch_team_t<M, 1, 2, LAGGED, SUMS, TS, STG>(pt, mp, st);
   if (TM == 4 && Q == 1) return launch_team_t<M, 1, 4, LAGGED, SUMS, TS, STG>(pt, mp, st);
-  if constexpr (!LAGGED) {
+  if constexpr (!LAGGED || (SUMS && STG)) {
     if (TM == 2 && Q == 2) return launch_team_t<M, 2, 2, LAGGED, SUMS, TS, STG>(pt, mp, st);
   }
   return set_error(TP_ERR_UNSUPPORTED, "no team kernel for Q=%d, TM=%d", Q, TM);
@@ -719,8 +721,8 @@ static int launch_team_m(const Partition &pt, MarchParams &mp, bool lagged, bool
 // thread (K teams) unless overridden.  With the Cayley step 4 teams x 1 probe
 // time 2.75 ms per forward march at N = 2048 x 1023 slices x 512 probes
 // against 2.84 ms for 2 x 2.
-static void team_shape(int K, int *TM, int *Q) {
-  const char *env = getenv("TPCUDA_TEAM_SHAPE");  // "TM,Q" override for tuning sweeps
+static void team_shape(int K, int *TM, int *Q, const char *var = "TPCUDA_TEAM_SHAPE") {
+  const char *env = getenv(var);  // "TM,Q" override for tuning sweeps
   if (env != nullptr && sscanf(env, "%d,%d", TM, Q) == 2 && *TM * *Q == K) return;
   *TM = K;
   *Q = 1;
@@ -745,16 +747,23 @@ int launch_team_march(const Partition &pt, MarchParams &mp, bool lagged, cudaStr
   int TM, Q;
   if (lagged) {
     // one probe per thread: the kept and prefetched forward slices need 2M
-    // complex registers per probe on top of the state
+    // complex registers per probe on top of the state; the staged Cayley
+    // form keeps none and may take a tuning override
     TM = K;
     Q = 1;
+    if (sums) team_shape(K, &TM, &Q, "TPCUDA_ADJ_SHAPE");
   } else {
     team_shape(K, &TM, &Q);
   }
   // Staged global traffic where the staging slices fit beside the factor
   // double buffer at this shape; otherwise the direct path at this shape
   // (fewer teams per CTA would mean more CTAs than SMs).
-  const bool stg = !qd && team_smem_bytes(pt, mp.trunc, Q, TM, qd, true) <= (size_t)max_smem;
+  bool stg = !qd && team_smem_bytes(pt, mp.trunc, Q, TM, qd, true) <= (size_t)max_smem;
+  if (lagged && Q > 1 && !stg) {  // several probes per thread need the staged gradient
+    TM = K;
+    Q = 1;
+    stg = !qd && team_smem_bytes(pt, mp.trunc, Q, TM, qd, true) <= (size_t)max_smem;
+  }
   while (team_smem_bytes(pt, mp.trunc, Q, TM, qd, stg) > (size_t)max_smem && TM * Q > 1) {
     if (TM > 1) TM /= 2;
     else Q /= 2;

@@ -74,6 +74,7 @@ class PWEGradient2D:
         self._ff = self.engine.new_factor_buffer()
         self._fa = self.engine.new_factor_buffer()
         self._copy_stream = None
+        self._factor_stream = None
         self._n_dev = None
         self._bufs = {}
         self._grad_c = self.engine.new_grad_buffer()
@@ -121,8 +122,10 @@ class PWEGradient2D:
     # Range boundaries as fractions of the slices: a short first range, so
     # that little of the index field (and, for the adjoint, which runs the
     # ranges backwards, little of the gradient) is exposed outside the
-    # overlap, then three equal ones.
-    _RANGE_FRACTIONS = (0.0, 1.0 / 32.0, 1.0 / 3.0, 2.0 / 3.0, 1.0)
+    # overlap, then ranges doubling in length, so that each range's index
+    # columns arrive and its slices are factorised while the one before it
+    # marches.
+    _RANGE_FRACTIONS = (0.0, 1.0 / 32.0, 1.0 / 16.0, 1.0 / 8.0, 1.0 / 4.0, 1.0 / 2.0, 1.0)
 
     def _slice_ranges(self):
         """Consecutive slice ranges covering 1..L (1-based, inclusive)."""
@@ -130,11 +133,13 @@ class PWEGradient2D:
         b = sorted({round(f * L) for f in self._RANGE_FRACTIONS})
         return [(b[k] + 1, b[k + 1]) for k in range(len(b) - 1) if b[k + 1] > b[k]]
 
-    def _forward_ranges(self, field, probes, probes_ready, ranges, ready):
-        """Forward march range by range, each after its index columns arrived
-        (`ready` events) and its slices were factorised; the state passes from
-        range to range, the stored field and the exit wave are those of one
-        march over all slices."""
+    def _forward_ranges(self, fs, probes, probes_ready, ranges, prepare):
+        """Forward march range by range, each after its slices were factorised
+        into ``fs``: the first range's already on this stream; ``prepare(k)``
+        enqueues what range k > 0 needs and returns the event its march waits
+        for, so that the host enqueues each range right after the one before.
+        The state passes from range to range; the stored field and the exit
+        wave are those of one march over all slices."""
         e = self.engine
         P = probes.shape[0]
         main = torch.cuda.current_stream(self.device)
@@ -143,26 +148,23 @@ class PWEGradient2D:
         state = [self._buf("range_state0", P, 1)[:, 0], self._buf("range_state1", P, 1)[:, 0]]
         last = len(ranges) - 1
         for k, (s0, s1) in enumerate(ranges):
-            main.wait_event(ready[k])
-            fs = e.factor_range(field, "forward", s0, s1, out=self._ff)
-            if k == 0:
-                main.wait_event(probes_ready)
+            main.wait_event(probes_ready if k == 0 else prepare(k))
             e.march(fs, P, probes=probes if k == 0 else None, u_store=store, exit_out=ex, t_begin=s0, t_end=s1,
                     state_in=None if k == 0 else state[(k - 1) % 2], state_out=None if k == last else state[k % 2],
                     store_sums=self.sums)
         self._fs_fwd = fs
         return ex
 
-    def _backward_ranges(self, field, exit_grad, grad_out, side):
-        """:meth:`backward` (full field kept) with the adjoint run range by range
-        from the last slice down: once slices s0..L are done, index nodes
-        s0..nz-1 are final (node t reads slices t and t+1), so they are mapped
-        and copied into the host tensor `grad_out` on the side stream while the
-        adjoint goes on with the earlier slices.  Returns the device gradient."""
+    def _backward_ranges(self, field, exit_grad, grad_out, side, fa):
+        """:meth:`backward` (full field kept, exact-adjoint factor set ``fa``
+        ready on this stream) with the adjoint run range by range from the last
+        slice down: once slices s0..L are done, index nodes s0..nz-1 are final
+        (node t reads slices t and t+1), so they are mapped and copied into the
+        host tensor `grad_out` on the side stream while the adjoint goes on with
+        the earlier slices.  Returns the device gradient."""
         e = self.engine
         P = exit_grad.shape[0]
         main = torch.cuda.current_stream(self.device)
-        fa = e.factor(field, "adjoint_exact", out=self._fa)
         self._grad_c.zero_()
         src = exit_grad.contiguous()
         gn = torch.empty((e.n_obj, e.nz), dtype=torch.complex64, device=self.device)
@@ -187,15 +189,17 @@ class PWEGradient2D:
         gn.record_stream(side)
         return gn
 
-    def backward(self, field: torch.Tensor, exit_grad: torch.Tensor, is_delta=False) -> torch.Tensor:
+    def backward(self, field: torch.Tensor, exit_grad: torch.Tensor, is_delta=False, fa=None) -> torch.Tensor:
         """Exact adjoint from the exit-wave gradient; returns ∂ℓ/∂n (n_obj, nz).
 
         Must follow :meth:`forward` with the same field (it reuses the kept
-        field and, when checkpointing, the forward factor set).
+        field and, when checkpointing, the forward factor set).  ``fa``: the
+        field's exact-adjoint factor set when already computed.
         """
         P = exit_grad.shape[0]
         e = self.engine
-        fa = e.factor(field, "adjoint_exact", is_delta, out=self._fa)
+        if fa is None:
+            fa = e.factor(field, "adjoint_exact", is_delta, out=self._fa)
         self._grad_c.zero_()
         src = exit_grad.contiguous()
         if not self.ckpt:
@@ -244,25 +248,45 @@ class PWEGradient2D:
         streamed = (isinstance(n, torch.Tensor) and not n.is_cuda and n.dtype == torch.complex128
                     and n.is_contiguous() and tuple(n.shape) == (e.n_obj, e.nz) and not self.ckpt and e.L >= 64)
         if streamed:
-            # A host index field goes up in column blocks on the side stream;
-            # each block's slices are factorised and marched while the next
-            # block is in flight (slice s needs index columns s-1 and s).
+            # A host index field goes up in column blocks on the side stream
+            # (slice s needs index columns s-1 and s).  The first block's
+            # slices are factorised on this stream as soon as it lands (while
+            # the probes follow it up); every later block's slices, and then
+            # the exact-adjoint factor set, on the factor stream, beside the
+            # marches (which leave SMs free); each range marches once its
+            # slices are factorised, and the amplitudes go up last.
             field = self._n_device()
             ranges = self._slice_ranges()
-            ready = []
+            if self._factor_stream is None:
+                self._factor_stream = torch.cuda.Stream(self.device)
+            fstream = self._factor_stream
+            fstream.wait_stream(main)
+
+            def columns(c0, c1):
+                rc = e.lib.tp_copy_columns(ctypes.c_void_p(field.data_ptr()), ctypes.c_void_p(n.data_ptr()),
+                                           e.n_obj, e.nz * 16, c0 * 16, (c1 - c0 + 1) * 16,
+                                           ctypes.c_void_p(side.cuda_stream))
+                _native.check(rc, "tp_copy_columns")
+                return side.record_event()
+
             with torch.cuda.stream(side):
-                for k, (s0, s1) in enumerate(ranges):
-                    c0 = 0 if k == 0 else s0
-                    rc = e.lib.tp_copy_columns(ctypes.c_void_p(field.data_ptr()), ctypes.c_void_p(n.data_ptr()),
-                                               e.n_obj, e.nz * 16, c0 * 16, (s1 - c0 + 1) * 16,
-                                               ctypes.c_void_p(side.cuda_stream))
-                    _native.check(rc, "tp_copy_columns")
-                    ready.append(side.record_event())
-                    if k == 0:
-                        pr = _as_device(probes, self.device, torch.complex64)
-                        pr_ready = side.record_event()
-                amp = _as_device(amplitude, self.device, torch.float64)
-                amp_ready = side.record_event()
+                arrived = columns(0, ranges[0][1])
+            main.wait_event(arrived)
+            fs = e.factor_range(field, "forward", ranges[0][0], ranges[0][1], out=self._ff)
+            first_done = main.record_event()  # the first range also resets the PCR coupling bound
+            with torch.cuda.stream(side):
+                pr = _as_device(probes, self.device, torch.complex64)
+                pr_ready = side.record_event()
+            fstream.wait_event(first_done)
+
+            def prepare(k):
+                s0, s1 = ranges[k]
+                with torch.cuda.stream(side):
+                    arrived = columns(s0, s1)
+                with torch.cuda.stream(fstream):
+                    fstream.wait_event(arrived)
+                    e.factor_range(field, "forward", s0, s1, out=self._ff)
+                    return fstream.record_event()
         else:
             field = _as_device(n, self.device, torch.complex128)
             # Host probes and amplitudes travel on a side stream after n, so that
@@ -274,20 +298,28 @@ class PWEGradient2D:
                 amp = _as_device(amplitude, self.device, torch.float64)
                 amp_ready = side.record_event()
         pr.record_stream(main)
-        amp.record_stream(main)
         if streamed:
-            ex = self._forward_ranges(field, pr, pr_ready, ranges, ready)
+            ex = self._forward_ranges(fs, pr, pr_ready, ranges, prepare)
+            with torch.cuda.stream(side):
+                amp = _as_device(amplitude, self.device, torch.float64)
+                amp_ready = side.record_event()
+            with torch.cuda.stream(fstream):  # all index columns have arrived
+                fa = e.factor(field, "adjoint_exact", out=self._fa)
+                fa_ready = fstream.record_event()
         else:
             ex = self.forward(field, pr, probes_ready=pr_ready)
+        amp.record_stream(main)
         main.wait_event(amp_ready)
         loss, ge = amplitude_residual(ex, amp)
         host_out = (grad_out is not None and not grad_out.is_cuda and grad_out.dtype == torch.complex64
                     and grad_out.is_contiguous() and tuple(grad_out.shape) == (e.n_obj, e.nz))
+        if streamed:
+            main.wait_event(fa_ready)
         if streamed and host_out:
-            g = self._backward_ranges(field, ge, grad_out, side)
+            g = self._backward_ranges(field, ge, grad_out, side, fa)
             main.wait_stream(side)
         else:
-            g = self.backward(field, ge)
+            g = self.backward(field, ge, fa=fa if streamed else None)
             if grad_out is not None:
                 grad_out.copy_(g, non_blocking=True)
         return float(loss.item()), g
