@@ -44,9 +44,9 @@ sys.path.insert(0, ROOT)
 METRIC = "probe·slice solves/s fwd+adj (2D CN, complex64, exact adjoint + fused gradient)"
 REF_BUDGET_S = 150.0  # wall-time target of a whole `--impl reference` run
 # DRAM bytes (read + write) of one exact-adjoint march launch at N = 2048, nz = 1024, 512
-# probes: an ncu capture at nz = 128 measured 1.095 GB for 127 slices (traffic grows with the
-# slices), scaled by 1023/127 (profiles/cn2d_team_2048x1024_p512_launches.md).
-ADJ_TRAFFIC_BYTES_2048x1024_P512 = 1.095e9 * 1023 / 127
+# probes: an ncu capture at nz = 128 measured 1.0914 GB for 127 slices (traffic grows with the
+# slices), scaled by 1023/127 (profiles/cn2d_team_2048x128_p512_full.md).
+ADJ_TRAFFIC_BYTES_2048x1024_P512 = 1.09139e9 * 1023 / 127
 UNIT = "probe·slice/s"
 
 
