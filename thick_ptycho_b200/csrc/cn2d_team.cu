@@ -304,10 +304,11 @@ __device__ __forceinline__ void store_staged(const float2 (&U)[Q][M], float4 *st
 // Exact-adjoint gradient of one team and step: the team's Q staging slices
 // hold this step's forward half pair sums (u_s + u_{s-1})/2 of its probes,
 // bulk-loaded ahead of the solve; each row pair's contributions
-// 2 lambda conj(half sum), summed over the Q probes in registers (zero for
+// lambda conj(half sum), summed over the Q probes in registers (zero for
 // padded probes), replace the first slice in place, so that after the
-// end-of-step barrier the CTA's teams can be summed before the gradient row
-// is updated (grad_sum_flush).
+// end-of-step barrier the CTA's teams can be summed (and doubled: the pair
+// sum is twice the half sum) before the gradient row is updated
+// (grad_sum_flush).
 template <int M, int Q>
 __device__ __forceinline__ void grad_contrib(const float2 (&U)[Q][M], float4 *stg, int nvalid, int c) {
   constexpr int C = kTeamChunks;
@@ -322,12 +323,12 @@ __device__ __forceinline__ void grad_contrib(const float2 (&U)[Q][M], float4 *st
       const float2 b = cmulc(U[q][2 * j + 1], make_float2(v.z, v.w));
       w = make_float4(w.x + a.x, w.y + a.y, w.z + b.x, w.w + b.y);
     }
-    stg[j * C + c] = make_float4(2.f * w.x, 2.f * w.y, 2.f * w.z, 2.f * w.w);
+    stg[j * C + c] = w;
   }
 }
 
-// Sum the TM teams' contribution slices (each team's first staging slice)
-// and add them to gradient row `row`
+// Sum the TM teams' contribution slices (each team's first staging slice),
+// double the sum (half sums to pair sums) and add it to gradient row `row`
 // (chunked row pairs) with 16-byte vector reductions: one reduction per row
 // pair and CTA instead of one per probe.  Every thread of the CTA takes its
 // share of the row pairs; the slices are complete after a CTA barrier and
@@ -344,7 +345,7 @@ __device__ __forceinline__ void grad_sum_flush(const float4 *stage, float2 *row,
       const float4 w = stage[m * Q * E + e];  // team m's first slice
       v = make_float4(v.x + w.x, v.y + w.y, v.z + w.z, v.w + w.w);
     }
-    red_add_v4(g + e, v);
+    red_add_v4(g + e, make_float4(2.f * v.x, 2.f * v.y, 2.f * v.z, 2.f * v.w));
   }
   // the slices are next written by bulk loads (async proxy)
   fence_proxy_async_smem();
