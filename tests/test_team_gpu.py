@@ -98,13 +98,24 @@ def test_team_groups_of_four_with_partial_group_and_gradient():
     gref = sum(po.grad_c_from_adjoint(u_ref[p], lam[p]) for p in range(P))
     got = eng.unchunk_rows(gc).cpu().numpy().T
     assert rel(got, gref) < GRAD_TOL, rel(got, gref)
+    # the same with stored half pair sums and the Cayley-form adjoint: staged
+    # half-sum loads and the CTA sum of the teams' contributions, the last
+    # CTA holding one probe and three padded teams
+    sums, gs = eng.new_store(P), eng.new_grad_buffer()
+    eng.march(eng.factor(field, "forward"), P, probes=pr, u_store=sums, store_sums=True)
+    eng.march(eng.factor(field, "adjoint_exact"), P, src_exit=torch.from_numpy(e).cuda(), u_fwd=sums, grad_c=gs,
+              store_sums=True)
+    eng.device_status()
+    got_s = eng.unchunk_rows(gs).cpu().numpy().T
+    assert rel(got_s, gref) < GRAD_TOL, rel(got_s, gref)
 
 
-@pytest.mark.parametrize("N,k", [(1024, K), (2048, K), (2048, 0.5)])
+@pytest.mark.parametrize("N,k", [(512, K), (1024, K), (2048, K), (2048, 0.5)])
 def test_team_pair_sums_store_and_cayley_adjoint(N, k):
     """store_sums: the forward store holds (u_t + u_{t-1})/2; the exact adjoint
     reading those sums (one slice per step, Cayley-form step) gives the same
-    lambda and gradient as the two-slice form and as the oracle.  N = 2048 at
+    lambda and gradient as the two-slice form and as the oracle.  N = 512
+    (4-row chunks) keeps parallel cyclic reduction; N = 2048 at
     k = 4 pi keeps 8 spike rows (the shared-memory staged bulk stores, bulk
     half-sum loads and CTA gradient accumulator); k = 0.5 couples the chunks
     strongly (all 15 spike rows, parallel cyclic reduction), where the staging
