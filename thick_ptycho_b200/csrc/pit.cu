@@ -261,6 +261,7 @@ __global__ void pit_factor_kernel(const PitKd K, int L, double alpha_root, float
 }
 
 // Block solves in place on Xh (P, N, L): thread (p, k) solves along i.
+constexpr int kPitRows = 16;  // rows loaded together per pass of the recurrences
 __global__ void pit_block_solve_kernel(const PitK K, int L, int P, double alpha_root, const float4 *__restrict__ F,
                                        float2 *__restrict__ Xh, const int *active) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -272,22 +273,56 @@ __global__ void pit_block_solve_kernel(const PitK K, int L, int P, double alpha_
   sincospi(2.0 * (double)k / (double)L, &s, &c);
   const float2 opw = make_float2((float)(1.0 + alpha_root * c), (float)(alpha_root * s));
   float2 *x = Xh + (size_t)p * N * L + k;
+  // The recurrences are serial along i, but their inputs are not: each pass
+  // loads kPitRows rows of x and of the factors at once (independent loads in
+  // flight together) before running the recurrence over them.
   float2 y = x[0];
-  for (int i = 1; i < N; ++i) {
-    const float4 f = F[(size_t)i * L + k];
-    y = cfnma(make_float2(f.x, f.y), y, x[(size_t)i * L]);
-    x[(size_t)i * L] = y;
+  for (int i0 = 1; i0 < N; i0 += kPitRows) {
+    float2 xv[kPitRows], mv[kPitRows];
+#pragma unroll
+    for (int j = 0; j < kPitRows; ++j) {
+      const int i = i0 + j;
+      if (i < N) {
+        const float4 f = F[(size_t)i * L + k];
+        xv[j] = x[(size_t)i * L];
+        mv[j] = make_float2(f.x, f.y);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kPitRows; ++j) {
+      const int i = i0 + j;
+      if (i < N) {
+        y = cfnma(mv[j], y, xv[j]);
+        x[(size_t)i * L] = y;
+      }
+    }
   }
   {
     const float4 f = F[(size_t)(N - 1) * L + k];
     y = cmul(y, make_float2(f.z, f.w));
     x[(size_t)(N - 1) * L] = y;
   }
-  for (int i = N - 2; i >= 0; --i) {
-    const float4 f = F[(size_t)i * L + k];
-    const float2 ci = cmul(make_float2(-opw.x, -opw.y), K.sup(i));  // row i, column i+1
-    y = cmul(cfnma(ci, y, x[(size_t)i * L]), make_float2(f.z, f.w));
-    x[(size_t)i * L] = y;
+  const float2 mopw = make_float2(-opw.x, -opw.y);
+  for (int i1 = N - 2; i1 >= 0; i1 -= kPitRows) {
+    float2 xv[kPitRows], dv[kPitRows];
+#pragma unroll
+    for (int j = 0; j < kPitRows; ++j) {
+      const int i = i1 - j;
+      if (i >= 0) {
+        const float4 f = F[(size_t)i * L + k];
+        xv[j] = x[(size_t)i * L];
+        dv[j] = make_float2(f.z, f.w);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kPitRows; ++j) {
+      const int i = i1 - j;
+      if (i >= 0) {
+        const float2 ci = cmul(mopw, K.sup(i));  // row i, column i+1
+        y = cmul(cfnma(ci, y, xv[j]), dv[j]);
+        x[(size_t)i * L] = y;
+      }
+    }
   }
 }
 
