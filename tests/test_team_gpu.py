@@ -173,3 +173,24 @@ def test_team_pair_sums_store_and_cayley_adjoint(N, k):
     with pytest.raises(NativeLibraryError):
         small.march(small.factor(torch.from_numpy(n[:256]).cuda(), "forward"), 1, u_store=small.new_store(1),
                     store_sums=True)
+
+
+def test_team_rejects_misaligned_slice_buffers():
+    """The team kernels move whole slices with 16-byte vectors and bulk copies:
+    a store buffer 8 bytes off a 16-byte boundary is refused on the host
+    (nothing is launched), and the aligned buffer works."""
+    from thick_ptycho_b200._native import NativeLibraryError
+
+    N, nz, P = 512, 12, 3
+    eng = CN2D(N, nz, K, DX, DZ, "impedance")
+    field = torch.from_numpy(_field(N, nz, 21)).cuda()
+    pr = torch.from_numpy(_probes(N, P, 22).astype(np.complex64)).cuda()
+    fs = eng.factor(field, "forward")
+    st = eng.new_store(P)
+    flat = torch.empty(st.numel() + 1, dtype=torch.complex64, device="cuda")
+    off = flat[1:].view(st.shape)  # 8 bytes past the allocation's 256-byte boundary
+    assert off.data_ptr() % 16 == 8
+    with pytest.raises(NativeLibraryError, match="16-byte aligned"):
+        eng.march(fs, P, probes=pr, u_store=off)
+    eng.march(fs, P, probes=pr, u_store=st)
+    eng.device_status()
