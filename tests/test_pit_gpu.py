@@ -91,3 +91,25 @@ def test_pit_rhs_block_and_warm_start(golden):
     assert rel(u2, u1) < TOL and max(s.gmres_iterations) <= max(it1)
     with pytest.raises(NotImplementedError):
         s.solve(n=n, mode="adjoint")
+
+
+@pytest.mark.parametrize("nz", [50, 160])
+def test_pit_bluestein_lengths_against_oracle(nz):
+    """L = 49 and 159 give Bluestein lengths 128 and 512 (compile-time FFT
+    plans of the z-DFT; config 0's 256 and the runtime plan of the golden
+    case are covered above): the solve against the oracle's direct one."""
+    k = CONFIG0.geometry().k
+    N, P, L = 128, 2, nz - 1
+    rng = np.random.default_rng(nz)
+    n = 1 - 1e-3 * (rng.standard_normal((N, nz)) + 0.1j * rng.standard_normal((N, nz)))
+    x = np.arange(N)[None]
+    probes = np.exp(-((x - np.array([[40.0], [90.0]])) ** 2) / 50.0).astype(complex)
+    geo = SimulationGeometry(dimension=2, nx=N, nz=nz, dx=1.0, dz=1.0, k=float(k), num_probes=P)
+    s = PWEGpuPiTSolver(geo, probes[None], bc_type="impedance")
+    u = s.solve(n=n)[0, 0]
+    co = po.bc_coefficients(float(k), 1.0, 1.0, bc_type="impedance")
+    A, B = po.step_matrices_1d(N, co, "impedance", 1.0)
+    C = po.object_contribution(n, float(k), 1.0)
+    for p in range(P):
+        ref = po.full_system_solve(A, B, C, po.pit_rhs(B, probes[p], L)).reshape(L, N).T
+        assert rel(u[p][:, 1:], ref) < TOL, (p, rel(u[p][:, 1:], ref))

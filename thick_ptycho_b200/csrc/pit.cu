@@ -181,8 +181,10 @@ __global__ void pit_tables_kernel(int L, int M, double alpha, float *gamma, floa
 //     out Xh[p][i][k] = (1/sqrt L) sum_j x_j e^{+2 pi i jk/L}   (i-major out)
 //   !INV (back):  x_k = Xh[p][i][k],
 //     out[p][j][i] = (1/sqrt L) sum_k x_k e^{-2 pi i jk/L} / gamma_j
-// The inverse direction is conj(DFT(conj x)).  Grid (ceil(N/cpc), P).
-template <bool INV>
+// The inverse direction is conj(DFT(conj x)).  Grid (ceil(N/cpc), P).  MF:
+// the transform length when it has a compile-time plan (radix-16 passes for
+// 256), else 0 and the runtime plan `pl`.
+template <bool INV, int MF>
 __global__ void __launch_bounds__(kPitThreads) pit_zdft_kernel(const FftPlan pl, int N, int L, int cpc,
                                                                const float2 *__restrict__ in, float2 *__restrict__ out,
                                                                const float *__restrict__ gamma,
@@ -213,11 +215,13 @@ __global__ void __launch_bounds__(kPitThreads) pit_zdft_kernel(const FftPlan pl,
     }
   }
   __syncthreads();
-  float2 *F = fft_block(a, b, pl, tw, false, cpc, threadIdx.x, blockDim.x);
+  float2 *F = MF > 0 ? fft_block_fixed<MF>(a, b, tw, false, cpc, threadIdx.x, blockDim.x)
+                     : fft_block(a, b, pl, tw, false, cpc, threadIdx.x, blockDim.x);
   float2 *o = (F == a) ? b : a;
   for (int e = threadIdx.x; e < cpc * M; e += blockDim.x) F[e] = cmul(F[e], bhat[e % M]);
   __syncthreads();
-  const float2 *R = fft_block(F, o, pl, tw, true, cpc, threadIdx.x, blockDim.x);
+  const float2 *R = MF > 0 ? fft_block_fixed<MF>(F, o, tw, true, cpc, threadIdx.x, blockDim.x)
+                           : fft_block(F, o, pl, tw, true, cpc, threadIdx.x, blockDim.x);
   const float sc = 1.f / ((float)M * sqrtf((float)L));
   if (INV) {
     for (int e = threadIdx.x; e < cpc * L; e += blockDim.x) {
@@ -510,19 +514,45 @@ class PitSolver {
     if (rc) return rc;
     pit_factor_kernel<<<(L_ + 127) / 128, 128, 0, st_>>>(kd_, L_, alpha_root_, w_.F);
     TP_CHECK_CUDA(cudaGetLastError());
-    TP_CHECK_CUDA(cudaFuncSetAttribute(pit_zdft_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem_));
-    TP_CHECK_CUDA(cudaFuncSetAttribute(pit_zdft_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem_));
+    switch (M_) {
+      case 128: return zdft_attributes<128>();
+      case 256: return zdft_attributes<256>();
+      case 512: return zdft_attributes<512>();
+      default: return zdft_attributes<0>();
+    }
+  }
+  template <int MF>
+  int zdft_attributes() {
+    TP_CHECK_CUDA(cudaFuncSetAttribute(pit_zdft_kernel<true, MF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)zsmem_));
+    TP_CHECK_CUDA(cudaFuncSetAttribute(pit_zdft_kernel<false, MF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)zsmem_));
     return TP_OK;
+  }
+  template <int MF>
+  void zdft(bool inv, const float2 *in, float2 *out) {
+    const dim3 gz((N_ + cpc_ - 1) / cpc_, P_);
+    if (inv)
+      pit_zdft_kernel<true, MF><<<gz, kPitThreads, zsmem_, st_>>>(pl_, N_, L_, cpc_, in, out, w_.gamma, w_.chirp,
+                                                                  w_.bhat, w_.tw, w_.active);
+    else
+      pit_zdft_kernel<false, MF><<<gz, kPitThreads, zsmem_, st_>>>(pl_, N_, L_, cpc_, in, out, w_.gamma, w_.chirp,
+                                                                   w_.bhat, w_.tw, w_.active);
+  }
+  void zdft_any(bool inv, const float2 *in, float2 *out) {
+    switch (M_) {
+      case 128: return zdft<128>(inv, in, out);
+      case 256: return zdft<256>(inv, in, out);
+      case 512: return zdft<512>(inv, in, out);
+      default: return zdft<0>(inv, in, out);
+    }
   }
 
   // out = R in (the preconditioner), active probes only.
   int precond(const float2 *in, float2 *out) {
-    const dim3 gz((N_ + cpc_ - 1) / cpc_, P_);
-    pit_zdft_kernel<true><<<gz, kPitThreads, zsmem_, st_>>>(pl_, N_, L_, cpc_, in, w_.xh, w_.gamma, w_.chirp,
-                                                            w_.bhat, w_.tw, w_.active);
+    zdft_any(true, in, w_.xh);
     pit_block_solve_kernel<<<(L_ * P_ + 127) / 128, 128, 0, st_>>>(K_, L_, P_, alpha_root_, w_.F, w_.xh, w_.active);
-    pit_zdft_kernel<false><<<gz, kPitThreads, zsmem_, st_>>>(pl_, N_, L_, cpc_, w_.xh, out, w_.gamma, w_.chirp,
-                                                             w_.bhat, w_.tw, w_.active);
+    zdft_any(false, w_.xh, out);
     return check_cuda(cudaGetLastError(), "pit preconditioner launch");
   }
   // out = M in
