@@ -363,9 +363,9 @@ __device__ __forceinline__ void grad_sum_flush(const float4 *stage, float2 *row,
 // where it fits beside the factor double buffer, i.e. all but the 15-spike-row
 // factor sets, which keep direct per-thread stores and loads): the forward
 // stores its slices with bulk stores, and the exact adjoint's gradient has
-// its half-sum slice bulk-loaded one step ahead (no registers hold data in
-// flight) and its contribution summed over the CTA's teams before it
-// reaches global memory.
+// its half-sum slice bulk-loaded at the start of the step, ahead of the
+// solve (no registers hold data in flight), and its contribution summed
+// over the CTA's teams before it reaches global memory.
 template <int M, int Q, int TM, bool LAGGED, bool SUMS, int TS, bool STG>
 __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const MarchParams p) {
   static_assert(LAGGED || !SUMS, "SUMS selects the exact-adjoint Cayley step");
