@@ -500,7 +500,8 @@ def run_ours(a):
                        "l2": "working set 8.6 GB > L2 (no flush needed)", "parallelism": f"probe-shard x{world}"},
             "kernels_ms": {"cn2d_march_forward": fwd_ms, "cn2d_march_adjoint_exact_grad": adj_ms,
                            "step_total": ms_max / a.steps},
-            "roofline": {"kernel": "cn2d_march_kernel (" + ("adjoint_exact+grad" if dom == "adj" else "forward") + ")",
+            "roofline": {"kernel": ("cn2d_team_kernel (" if eng.chunks == 128 else "cn2d_march_kernel (")
+                         + ("adjoint_exact+grad" if dom == "adj" else "forward") + ")",
                          "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_kind": kind,
                          "traffic": (ADJ_TRAFFIC_BYTES_2048x1024_P512
