@@ -93,11 +93,12 @@ def test_pit_rhs_block_and_warm_start(golden):
         s.solve(n=n, mode="adjoint")
 
 
-@pytest.mark.parametrize("nz", [50, 160])
+@pytest.mark.parametrize("nz", [50, 160, 1025])
 def test_pit_bluestein_lengths_against_oracle(nz):
-    """L = 49 and 159 give Bluestein lengths 128 and 512 (compile-time FFT
-    plans of the z-DFT; config 0's 256 and the runtime plan of the golden
-    case are covered above): the solve against the oracle's direct one."""
+    """L = 49, 159 and 1024 give Bluestein lengths 128, 512 and 2048
+    (compile-time FFT plans of the z-DFT; config 0's 256 and the runtime plan
+    of the golden case are covered above): the solve against the oracle's
+    direct one."""
     k = CONFIG0.geometry().k
     N, P, L = 128, 2, nz - 1
     rng = np.random.default_rng(nz)

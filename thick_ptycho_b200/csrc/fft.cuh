@@ -284,6 +284,8 @@ __device__ __forceinline__ float2 *fft_run_padded(float2 *a, float2 *b, const fl
 
 // Lengths with a compile-time plan (radix 16 for 128 and 256, else 8s first,
 // then 4, 2, 3).
+// (fft_block_fixed also has a 2048 plan, 16 * 16 * 8, for callers that select
+// it themselves; the padded layout and the callers of fft_fixed_size do not.)
 __host__ __device__ constexpr bool fft_fixed_size(int n) {
   return n == 32 || n == 64 || n == 128 || n == 192 || n == 256 || n == 512;
 }
@@ -297,6 +299,7 @@ __device__ __forceinline__ float2 *fft_block_fixed(float2 *a, float2 *b, const f
   else if constexpr (N == 128) return fft_run_fixed<128, 1, 8, 16>(a, b, tw, sign, nb, tid, nth);
   else if constexpr (N == 192) return fft_run_fixed<192, 1, 8, 8, 3>(a, b, tw, sign, nb, tid, nth);
   else if constexpr (N == 256) return fft_run_fixed<256, 1, 16, 16>(a, b, tw, sign, nb, tid, nth);
+  else if constexpr (N == 2048) return fft_run_fixed<2048, 1, 16, 16, 8>(a, b, tw, sign, nb, tid, nth);
   else return fft_run_fixed<512, 1, 8, 8, 8>(a, b, tw, sign, nb, tid, nth);
 }
 

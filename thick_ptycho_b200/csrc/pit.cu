@@ -182,8 +182,8 @@ __global__ void pit_tables_kernel(int L, int M, double alpha, float *gamma, floa
 //   !INV (back):  x_k = Xh[p][i][k],
 //     out[p][j][i] = (1/sqrt L) sum_k x_k e^{-2 pi i jk/L} / gamma_j
 // The inverse direction is conj(DFT(conj x)).  Grid (ceil(N/cpc), P).  MF:
-// the transform length when it has a compile-time plan (radix-16 passes for
-// 256), else 0 and the runtime plan `pl`.
+// the transform length when it has a compile-time plan (128, 256, 512,
+// 2048; radix-16 passes for 256 and 2048), else 0 and the runtime plan `pl`.
 template <bool INV, int MF>
 __global__ void __launch_bounds__(kPitThreads) pit_zdft_kernel(const FftPlan pl, int N, int L, int cpc,
                                                                const float2 *__restrict__ in, float2 *__restrict__ out,
@@ -518,6 +518,7 @@ class PitSolver {
       case 128: return zdft_attributes<128>();
       case 256: return zdft_attributes<256>();
       case 512: return zdft_attributes<512>();
+      case 2048: return zdft_attributes<2048>();
       default: return zdft_attributes<0>();
     }
   }
@@ -544,6 +545,7 @@ class PitSolver {
       case 128: return zdft<128>(inv, in, out);
       case 256: return zdft<256>(inv, in, out);
       case 512: return zdft<512>(inv, in, out);
+      case 2048: return zdft<2048>(inv, in, out);
       default: return zdft<0>(inv, in, out);
     }
   }
