@@ -42,10 +42,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "probe·slice solves/s fwd+adj (2D CN, complex64, exact adjoint + fused gradient)"
-REF_BUDGET_S = 150.0  # wall-time target of a whole `--impl reference` run
+REF_BUDGET_S = 150.0    # wall-time target of a whole `--impl reference` run
+REF_DEADLINE_S = 240.0  # hard limit: the arm prints its line from the steps finished by then
+REF_MAX_WORKERS = 32    # worker processes of the reference arm (one thread each)
 # DRAM bytes (read + write) of one exact-adjoint march launch at N = 2048, nz = 1024, 512
-# probes: an ncu capture at nz = 128 measured 1.0914 GB for 127 slices (traffic grows with the
-# slices), scaled by 1023/127 (profiles/cn2d_team_2048x128_p512_full.md).
+# probes: an ncu capture of the same kernel at nz = 128 (127 slices, 512 probes) measured
+# 1.0914 GB; the traffic grows in proportion to the slices, so it is scaled by 1023/127.
 ADJ_TRAFFIC_BYTES_2048x1024_P512 = 1.09139e9 * 1023 / 127
 UNIT = "probe·slice/s"
 
@@ -237,46 +239,91 @@ def cpu_rate(N, nz, P, cores, probes_per_worker, slices=None, pool=None):
     return P * L / total, t_fact, t_probe, wall
 
 
+def ref_workers():
+    """Worker processes of the reference arm: the host threads this process may
+    run on (its affinity mask, not the machine's core count), at most
+    REF_MAX_WORKERS."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        n = os.cpu_count() or 1
+    return max(1, min(n, REF_MAX_WORKERS))
+
+
 def run_reference(a):
+    """The reference's CPU path (the oracle's restatement of its IterativeLU
+    solver: per-slice SuperLU, serial per-probe march, its adjoint) on the host
+    cores.  Each step times a sample of S of the L slices on every worker (the
+    cost is linear in S; S is sized from a calibration sample so that the run
+    takes about REF_BUDGET_S seconds), and the run stops at REF_DEADLINE_S
+    whatever `--steps` asks, reporting the steps it finished."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from thick_ptycho_b200.workloads import CONFIGS
-
     import multiprocessing as mp
 
+    from thick_ptycho_b200.workloads import CONFIGS
+
+    t_start = time.perf_counter()
     w = CONFIGS[a.config]
-    cores = os.cpu_count() or 1
+    cores = ref_workers()
     L = w.nz - 1
-    # Each step times a sample of S of the L slices on every worker, S chosen
-    # from a first small sample so that the whole --steps/--warmup run takes
-    # about REF_BUDGET_S seconds (factorisation and marches are linear in S).
+    # one thread per worker process: the reference's SuperLU and sparse products
+    # are single-threaded, and BLAS/OpenMP pools in every worker oversubscribe
+    for v in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS", "NUMEXPR_NUM_THREADS"):
+        os.environ[v] = "1"
     budget = REF_BUDGET_S / max(1, a.warmup + a.steps)
     vals = []
     info = None
+    S = probe_s = min(L, 16)
     with mp.get_context("spawn").Pool(cores) as pool:
-        probe_s = min(L, 32)
-        _, _, _, wall0 = cpu_rate(w.nx, w.nz, w.num_probes, cores, 1, probe_s, pool)  # also warms the workers
-        _, _, _, wall0 = cpu_rate(w.nx, w.nz, w.num_probes, cores, 1, probe_s, pool)
-        S = max(8, min(L, int(probe_s * budget / max(wall0, 1e-3))))
+
+        def rate(S, limit):
+            jobs = [(w.nx, w.nz, [(c * 7) % w.num_probes], c, S) for c in range(cores)]
+            t0 = time.perf_counter()
+            res = pool.map_async(_cpu_sample, jobs).get(timeout=max(1.0, limit))
+            wall = time.perf_counter() - t0
+            t_fact = statistics.mean(r[0] for r in res) * L / S
+            t_probe = statistics.mean(r[1] for r in res) * L / S
+            total = t_fact + (-(-w.num_probes // cores)) * t_probe
+            return w.num_probes * L / total, t_fact, t_probe, wall
+
+        def left():
+            return REF_DEADLINE_S - (time.perf_counter() - t_start)
+
+        calib = rate(probe_s, left())  # also starts the workers
+        calib = rate(probe_s, left())
+        S = max(8, min(L, int(probe_s * budget / max(calib[3], 1e-3))))
+        done = 0
         for i in range(a.warmup + a.steps):
-            v, tf, tp, wall = cpu_rate(w.nx, w.nz, w.num_probes, cores, 1, S, pool)
+            # stop when the next step would not finish before the deadline
+            if left() < 1.5 * (calib[3] * S / probe_s) + 5.0:
+                break
+            try:
+                v, tf, tp, wall = rate(S, left())
+            except mp.TimeoutError:
+                break
             if i >= a.warmup:
                 vals.append(v)
                 info = (tf, tp, wall)
+                done += 1
+        pool.terminate()
+    if not vals:  # deadline reached during the warm-up: report the calibration sample
+        S, info, vals = probe_s, calib[1:], [calib[0]]
     value = statistics.median(vals)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-        "ms_per_step": 1e3 * w.num_probes * L / value, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded)", "impl": "reference",
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": max(done, 1), "warmup": a.warmup,
+        "steps_requested": a.steps, "ms_per_step": 1e3 * w.num_probes * L / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded)", "impl": "reference",
         "config": {"workload": w.name, "N": w.nx, "nz": w.nz, "probes": w.num_probes},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": (f"per step: {cores} spawn workers each factorise the first {S} of {L} slices "
-                                    f"(forward + reference adjoint SuperLU) and march 1 probe fwd+adj over them; "
-                                    f"rate scaled to {L} slices and {w.num_probes} probes split over {cores} workers "
-                                    f"(last, scaled: factor {info[0]:.2f} s, probe {info[1]:.3f} s; step wall "
-                                    f"{info[2]:.2f} s)")},
+                         "sample": (f"per step: {cores} spawn workers (one thread each) each factorise the first {S} "
+                                    f"of {L} slices (forward + reference adjoint SuperLU) and march 1 probe fwd+adj "
+                                    f"over them; rate scaled to {L} slices and {w.num_probes} probes split over "
+                                    f"{cores} workers (last, scaled: factor {info[0]:.2f} s, probe {info[1]:.3f} s; "
+                                    f"step wall {info[2]:.2f} s)")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": time.perf_counter() - t_start,
     }
     print(json.dumps(line), flush=True)
 

@@ -420,7 +420,8 @@ TP_API int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t n_dt
 
 /* ------------------------------------------------ learned 3D preconditioner
  * The reference has no learned component; these entry points are this
- * library's own addition to the 3D path (the north-star "learned" form).
+ * library's own addition to the 3D path (a learned correction of the FFT
+ * preconditioner).
  * A four-layer 3x3 CNN (bf16 weights, fp32 accumulation on the tcgen05
  * tensor cores) maps the object diagonal d of one slice to a 13-tap complex
  * filter per pixel; the learned preconditioner is y = z + sum_t F_t(x) z(x + o_t)

@@ -2,7 +2,7 @@
 
 TEST INFRASTRUCTURE ONLY: imported by ``tests/``, never by the product package.
 
-The reference has no learned component (the north-star "learned" form is this
+The reference has no learned component (the learned preconditioner is this
 project's own addition), so there is no reference file to cite or golden vector
 to pin against: this module restates the network's defining equations so the
 GPU kernels (forward, backward data, weight gradients, filter gradient) can be

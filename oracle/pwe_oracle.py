@@ -237,6 +237,33 @@ def march(A, B, C2d, probe, mode="forward", b=None, rhs_block=None, test_rhs=Non
     return march_with_lu(lus, Bs, b, probe, mode, rhs_block, test_rhs)
 
 
+def march_streamed(A, B, C2d, probes, keep=None):
+    """Forward march of several probes, one slice factorised at a time.
+
+    The same arithmetic as ``build_lu_factors(…, "forward")`` followed by
+    ``march_with_lu`` (``iterative_lu.py:116-122,185-193``: ``u_j =
+    splu(A − C_j)⁻¹ (B + C_j) u_{j−1}``, b = 0), but only the current slice's
+    factor is held, so the 3D operators of large grids (one SuperLU of a
+    65 536-unknown 5-point matrix is ~100 MB) fit in memory.  ``probes`` is
+    (K, N).  Returns the exit waves (K, N) and, for the node indices in
+    ``keep``, ``{t: u_t (K, N)}``.
+    """
+    probes = np.asarray(probes, dtype=complex)
+    L = C2d.shape[1]
+    u = probes.T.copy()
+    kept = {}
+    keep = set(keep or ())
+    if 0 in keep:
+        kept[0] = u.T.copy()
+    for j in range(1, L + 1):
+        C = sp.diags(C2d[:, j - 1])
+        lu = spla.splu((A - C).tocsc())
+        u = lu.solve((B + C) @ u)
+        if j in keep:
+            kept[j] = u.T.copy()
+    return u.T.copy(), kept
+
+
 # ---------------------------------------------------------------------------
 # Space-time (parallel-in-time) solve: the reference's PWEFullPinTSolver
 # ---------------------------------------------------------------------------

@@ -1,10 +1,10 @@
 """GPU exact adjoint + fused gradient against the complex128 oracle and
 central finite differences.
 
-Tolerance: relative L2 ≤ 1e-5 for adjoint fields; the fused gradient sums
-probe contributions in fp32, so it is checked at ≤ 1e-4 relative L2 (the
-bound stated in the test), and against finite differences of the complex128
-oracle loss at ≤ 1e-3 relative per sampled voxel.
+Tolerance: relative L2 ≤ 1e-5 for adjoint fields and for the fused gradient
+(which sums the probe contributions in fp32), and against finite differences
+of the complex128 oracle loss at ≤ 1e-3 relative per sampled voxel (the
+finite differences themselves carry ~1e-4 truncation and round-off error).
 """
 
 import numpy as np
@@ -20,7 +20,7 @@ if not torch.cuda.is_available():  # pragma: no cover
 
 from thick_ptycho_b200.cn2d import CN2D  # noqa: E402
 
-GRAD_TOL = 1e-4
+GRAD_TOL = 1e-5
 
 
 def rel(a, b):

@@ -3,10 +3,12 @@ central finite differences of the complex128 oracle, and agreement with the
 reference's own (inexact) least-squares gradient.
 
 Tolerances: checkpointed vs full-store gradients ≤ 1e-5 relative L2 (same
-arithmetic, only the fp32 accumulation order differs); GPU vs oracle ≤ 1e-4
+arithmetic, only the fp32 accumulation order differs); GPU vs oracle ≤ 1e-5
 relative L2; finite differences (h = 1e-7, complex128) within 1e-3 relative
 per sampled voxel; reference gradient: cosine similarity ≥ 0.98 (its adjoint
-is not the exact transpose of its forward, SURVEY B1–B3; measured 0.992).
+is not the exact transpose of its forward: it pairs (A − C_s)ᴴ with
+(B + C_s)ᴴ of the same slice, iterative_lu.py:114-128, and its grad_A drops
+C₀u₀, forward_model.py:151-153; measured 0.992).
 """
 
 import numpy as np
@@ -72,7 +74,7 @@ def test_gradient_matches_oracle_and_autograd():
         gc += po.grad_c_from_adjoint(u, po.exact_adjoint(A, B, C, src))
     gref = po.chain_grad_to_n(gc, geo.k, 1.0)
     assert abs(loss - lref) < 1e-5 * abs(lref)
-    assert rel(g.cpu().numpy(), gref) < 1e-4
+    assert rel(g.cpu().numpy(), gref) < 1e-5
     # the same gradient through torch.autograd
     field = torch.from_numpy(n).cuda().requires_grad_(True)
     pr = torch.from_numpy(probes.astype(np.complex64)).cuda()
@@ -81,7 +83,7 @@ def test_gradient_matches_oracle_and_autograd():
     lt = torch.sum((U.abs() - torch.from_numpy(amp).cuda()) ** 2)
     lt.backward()
     assert field.grad.dtype == torch.complex128
-    assert rel(field.grad.cpu().numpy(), gref) < 1e-4
+    assert rel(field.grad.cpu().numpy(), gref) < 1e-5
 
 
 def test_gradient_matches_central_differences_config3_geometry():

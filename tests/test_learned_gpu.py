@@ -2,9 +2,9 @@
 GPU with the project's own kernels, and what the trained network gains over
 the plain FFT preconditioner on a held-out index field.
 
-Tolerances: exit waves of the learned march ≤ 2e-5 relative L2 against the
-complex128 oracle (the same bound as the plain BiCGStab march, both stopped at
-a 1e-6 relative residual); the trained correction must at least halve the
+Tolerances: exit waves of the learned march ≤ 1e-5 relative L2 against the
+complex128 oracle (the same bound as the plain BiCGStab march, both at the
+default stopping residual); the trained correction must at least halve the
 plain preconditioner's error on the held-out field and must not need more
 Krylov iterations than the plain form.
 """
@@ -104,7 +104,7 @@ def test_learned_march_against_oracle_and_iterations(trained, mode):
                 srcm = np.zeros((NF * NB, NZ - 1), dtype=complex)
                 srcm[:, -1] = probes[p]
                 ref = po.exact_adjoint(A, B, C, srcm)[:, 0]
-            assert np.linalg.norm(got[p] - ref) <= 2e-5 * np.linalg.norm(ref), (pc, p)
+            assert np.linalg.norm(got[p] - ref) <= 1e-5 * np.linalg.norm(ref), (pc, p, np.linalg.norm(got[p] - ref) / np.linalg.norm(ref))
     assert eng.fallbacks == 0
     assert its["learned"] <= its[True], its
 

@@ -556,17 +556,12 @@ __global__ void cn2d_grad_to_n_kernel(const GradParams q) {
 // Device error word (timeouts of bounded waits); read by tp_device_status.
 __device__ int g_device_error;
 
+static SymbolCache g_device_error_addr;
+
 int *device_error_ptr() {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
-  static int *ptrs[64] = {nullptr};
-  if (dev < 0 || dev >= 64) return nullptr;
-  if (ptrs[dev] == nullptr) {
-    void *p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_device_error) != cudaSuccess) return nullptr;
-    ptrs[dev] = static_cast<int *>(p);
-  }
-  return ptrs[dev];
+  void *p = nullptr;
+  if (symbol_address(&g_device_error, g_device_error_addr, &p) != TP_OK) return nullptr;
+  return static_cast<int *>(p);
 }
 
 // --------------------------------------------------------------------------

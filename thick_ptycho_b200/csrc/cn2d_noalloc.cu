@@ -19,10 +19,10 @@
 // without ordering) race on the array and corrupt each other's results.
 //
 // Set-up: the first call on each device resolves the array's device address
-// with cudaGetSymbolAddress while that device is current.  This call should
-// come before any stream capture on that device.
-#include <mutex>
-
+// with cudaGetSymbolAddress while that device is current, and caches it for
+// that device's context; a call in a new context (after cudaDeviceReset)
+// resolves it again.  The first call on a device should come before any
+// stream capture on that device.
 #include "tp_errors.h"
 #include "tpcuda.h"
 
@@ -32,25 +32,11 @@ constexpr size_t kStaticScratchBytes = size_t(32) << 20;
 
 static __device__ __align__(256) unsigned char g_cn2d_static_scratch[kStaticScratchBytes];
 
-constexpr int kMaxDevices = 64;
-static std::mutex g_scratch_mu;
-static void *g_scratch_addr[kMaxDevices] = {nullptr};
+static SymbolCache g_scratch_addr;
 
 // Device address of g_cn2d_static_scratch on the current device.  The host
 // symbol is only a stand-in; kernels must be given this address instead.
-static int static_scratch(void **out) {
-  int dev = 0;
-  TP_CHECK_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) return set_error(TP_ERR_UNSUPPORTED, "device ordinal %d out of range", dev);
-  std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (g_scratch_addr[dev] == nullptr) {
-    void *p = nullptr;
-    TP_CHECK_CUDA(cudaGetSymbolAddress(&p, g_cn2d_static_scratch));
-    g_scratch_addr[dev] = p;
-  }
-  *out = g_scratch_addr[dev];
-  return TP_OK;
-}
+static int static_scratch(void **out) { return symbol_address(g_cn2d_static_scratch, g_scratch_addr, out); }
 
 }  // namespace tp
 

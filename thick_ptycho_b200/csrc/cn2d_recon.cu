@@ -5,7 +5,7 @@
 // operator grad_A = -(diag(G) + subdiag(G)), G = (dz/2)(k/i)
 // (forward_model.py:128-153), which pairs block b of the vector form (slice
 // b+1) with u_{b+1} + u_b for b >= 1 and with u_1 alone for b = 0 (the
-// reference drops C_0 u_0).
+// reference's full-system gradient drops C_0 u_0, forward_model.py:151-153).
 //
 //   cn2d_refgrad_kernel: the reference's compute_grad_least_squares
 //     (pwe_reconstructor.py:100-164): with the reference adjoint lambda
