@@ -298,7 +298,12 @@ typedef struct tp_pit_args {
   int32_t restart;         /* Krylov vectors per cycle (0 = 20, scipy's
                               default), <= 64                                  */
   int32_t max_cycles;      /* restart cycles (0 = 1000)                        */
-  int32_t reserved;
+  int32_t mode;            /* TP_MODE_FORWARD, or TP_MODE_ADJOINT: the
+                              reference's adjoint system (full_pint.py:140-166)
+                              - blocks A^H - C'_j, -(B^H + C'_j) with
+                              C' = conj(C) flipped along z, the forward
+                              preconditioner, b = rhs (+ B u_0 with the forward
+                              B), u not flipped                               */
   double alpha;            /* circulant parameter (0 = 1e-2, the reference's)  */
   double rtol, atol;       /* stop at ||b - M u|| <= max(atol, rtol ||b||)
                               (0 = 1e-5 / 1e-8, the reference's gmres call)    */
@@ -380,9 +385,15 @@ typedef struct tp_cn3d_march_args {
                                 2^a 3^b 5^c and tile), 0: none, 2: the FFT
                                 preconditioner with the learned per-pixel
                                 correction of `model` (not REVERSE)             */
-  int32_t host_check;        /* 1: stop launching iterations once all probes of
-                                a slice converged (synchronises the stream)     */
-  int32_t reserved;
+  int32_t host_check;        /* 1: stop iterating a step once all its probes
+                                converged (on the device when the march runs as
+                                a graph, else by a stream synchronisation per
+                                iteration); 0: always max_iter iterations, step
+                                by step                                          */
+  int32_t launch;            /* 0: one CUDA graph per march, whose step and
+                                iteration loops are conditional WHILE nodes (no
+                                host round trip), except on a capturing stream
+                                or with training pairs; 1: step by step          */
   double tol;                /* relative residual per solve (0 = 1e-6)           */
   const void *probes;        /* float2 (P, N) initial fields, or NULL            */
   const void *src_shared;    /* float2 (L, N) probe-independent source by step   */
@@ -392,11 +403,13 @@ typedef struct tp_cn3d_march_args {
   const void *u_fwd;         /* ADJOINT_EXACT gradient: forward field (P, nz, N) */
   void *grad_c;              /* ADJOINT_EXACT: float2 (L, N) accumulator of
                                 sum_p lambda_s conj(u_s + u_{s-1}); caller zeroes */
-  int32_t *stats;            /* device int32[4]: total iterations, solves, solves
+  int32_t *stats;            /* device int32[5]: total iterations, solves, solves
                                 whose true residual exceeded 10 tol, largest
-                                iteration count; accumulated; or NULL.  A
-                                caller of the learned form re-runs the march
-                                with precond = 1 when stats[2] grew (fallback) */
+                                iteration count (accumulated), and [4] = 1 when
+                                the march ran as one graph (0 step by step);
+                                or NULL.  A caller of the learned form re-runs
+                                the march with precond = 1 when stats[2] grew
+                                (fallback) */
   const struct tp_cnn_model *model;  /* precond == 2: the network            */
   void *learned_ws;          /* precond == 2: tp_cn3d_learned_ws_bytes, 256-B aligned */
   size_t learned_ws_bytes;
@@ -414,7 +427,10 @@ typedef struct tp_cn3d_march_args {
 } tp_cn3d_march_args;
 
 TP_API size_t tp_cn3d_workspace_bytes(int32_t n_total, int32_t num_probes);
-TP_API size_t tp_cn3d_learned_ws_bytes(int32_t nf, int32_t nb, int32_t num_probes);
+/* Learned-form workspace: the CNN activations of 64 slices, the filters of
+ * all nz - 1 slices (13 complex64 taps per pixel) and P plain-preconditioned
+ * vectors. */
+TP_API size_t tp_cn3d_learned_ws_bytes(int32_t nf, int32_t nb, int32_t nz, int32_t num_probes);
 TP_API int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t n_dtype, const tp_cn3d_march_args *args,
                          void *workspace, size_t workspace_bytes, tp_stream_t stream);
 

@@ -365,6 +365,37 @@ def pit_solve(A, B, C2d, probes, alpha=1e-2, atol=1e-8, rtol=1e-5, restart=20, w
     return out, its
 
 
+def pit_solve_adjoint(A, B, C2d, probe=None, rhs=None, alpha=1e-2, atol=1e-8, rtol=1e-5, restart=20):
+    """``PWEFullPinTSolver`` in mode "adjoint" for one probe (``full_pint.py:
+    140-166`` with ``_pintobj_matvec_exact`` in its forward form,
+    ``_pint_utils.py:27-54``): the system keeps the forward block structure —
+    diagonal ``Aᴴ − C'_j``, subdiagonal ``−(Bᴴ + C'_j)`` of row j — with
+    ``C' = conj(C)`` flipped along z, right-preconditioned by the *forward*
+    α-circulant preconditioner of A, B (the solver builds one, in mode
+    "forward").  The right-hand side is ``rhs`` (the flat column-major (N, L)
+    vector, used as given) or ``[B u_0, 0, …]`` with the forward B.  Returns
+    ``u`` (N, L+1) with the probe (or zeros) as column 0 — no flip along z —
+    and the GMRES iteration count."""
+    N, L = C2d.shape
+    Ah, Bh = A.conj().T.tocsr(), B.conj().T.tocsr()
+    Cf = np.flip(np.conj(C2d), axis=1)
+    R = PiTPreconditionerOracle(A, B, L, alpha)
+    M = spla.LinearOperator((N * L, N * L), dtype=np.complex128,
+                            matvec=lambda y: pit_matvec(Ah, Bh, Cf, R.apply(y)))
+    p0 = np.zeros(N, dtype=complex) if probe is None else np.asarray(probe, dtype=complex).ravel()
+    b = np.asarray(rhs, dtype=complex).ravel() if rhs is not None else pit_rhs(B, p0, L)
+    count = [0]
+
+    def cb(_r):
+        count[0] += 1
+
+    y, info = spla.gmres(M, b, atol=atol, rtol=rtol, restart=restart, callback=cb, callback_type="pr_norm")
+    u = np.zeros((N, L + 1), dtype=complex)
+    u[:, 0] = p0
+    u[:, 1:] = R.apply(y).reshape(L, N).T
+    return u, count[0]
+
+
 # ---------------------------------------------------------------------------
 # Exact discrete adjoint and gradient (no reference counterpart; the
 # reference's adjoint differs, see ``reference_grad_least_squares``)

@@ -309,6 +309,29 @@ def pit_reference():
     save("pit2d", **out)
 
 
+def pit_adjoint_reference():
+    """PWEFullPinTSolver in mode "adjoint" (full_pint.py:140-166, _pint_utils.py:
+    27-54): GMRES on the block-bidiagonal system with conjugate-transposed A, B
+    and the z-flipped conjugate C, right-preconditioned by the forward
+    α-circulant preconditioner, for a given right-hand side (the flat
+    column-major (N, L) space-time vector) and for the probe right-hand side."""
+    from thick_ptycho.forward_model import PWEFullPinTSolver
+
+    g = np.load(os.path.join(HERE, "random2d.npz"))
+    ss = small_space_2d()
+    probes = create_ptycho_probes(ss)
+    n = g["n"]
+    rhs = g["rhs_block"]
+    out = {"n": n, "probes": probes[0], "rhs_block": rhs, **sim_params(ss)}
+    for bc in ("neumann", "impedance", "dirichlet"):
+        s = PWEFullPinTSolver(ss, probes, bc_type=bc)
+        out[f"adj_rhs_{bc}"] = s._solve_single_probe(scan_idx=1, n=n, mode="adjoint",
+                                                     rhs_block=rhs.ravel(order="F"), probe=probes[0, 1])
+        s = PWEFullPinTSolver(ss, probes, bc_type=bc)
+        out[f"adj_probe_{bc}"] = s._solve_single_probe(scan_idx=2, n=n, mode="adjoint", probe=probes[0, 2])
+    save("pit2d_adjoint", **out)
+
+
 def random_3d():
     rng = np.random.default_rng(77)
     cfg = SimulationConfig(
@@ -356,7 +379,7 @@ def geometry():
 
 if __name__ == "__main__":
     sections = [geometry, kat_2d, random_2d, config0_reference, gradient_reference, farfield_reference,
-                nlcg_reference, ms3pie_reference, kat_3d, random_3d, pit_reference]
+                nlcg_reference, ms3pie_reference, kat_3d, random_3d, pit_reference, pit_adjoint_reference]
     wanted = set(sys.argv[2:])
     for fn in sections:
         if not wanted or fn.__name__ in wanted:

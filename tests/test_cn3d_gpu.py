@@ -214,3 +214,46 @@ def test_rejects_bad_arguments():
     with pytest.raises(Exception, match="gradient"):
         eng.march(f, 1, "forward", u_fwd=eng.new_store(1),
                   grad_c=torch.zeros((3, 64), dtype=torch.complex64, device="cuda"))
+
+
+@pytest.mark.parametrize("mode", ["forward", "adjoint_exact", "adjoint", "reverse"])
+def test_graph_march_matches_step_by_step(mode):
+    """The march recorded as one CUDA graph (conditional WHILE nodes for the
+    step and BiCGStab loops, no host round trip) against the same kernels
+    launched step by step with a host check per iteration: the same iteration
+    counts (up to a convergence decision that round-off may tip), fields equal
+    to fp32 round-off (the fp64 dot products are summed with atomics in
+    varying order), and the gradient likewise."""
+    rng = np.random.default_rng(31)
+    nf = nb = 32
+    nz, k, P = 12, 4 * np.pi, 3
+    N = nf * nb
+    n = _field(rng, N, nz)
+    field = torch.from_numpy(n).cuda()
+    dz = 0.5 if mode == "reverse" else 1.0
+    probes = c64(_gauss(nf, nb, rng.uniform(10, 22, (P, 2)), 5.0))
+    eng = CN3D(nf, nb, nz, k, 1.0, 1.0, dz, "impedance")
+    fwd = eng.new_store(P)
+    eng.march(field, P, "forward", probes=probes, u_store=fwd, tol=1e-7)
+    src = c64(rng.standard_normal((P, N)) + 1j * rng.standard_normal((P, N)))
+    out = {}
+    for launch in (0, 1):
+        eng.launch = launch
+        eng.read_stats()
+        store = eng.new_store(P)
+        gc = torch.zeros((nz - 1, N), dtype=torch.complex64, device="cuda")
+        if mode == "adjoint_exact":
+            eng.march(field, P, mode, src_exit=src, u_fwd=fwd, grad_c=gc, u_store=store, tol=1e-7)
+        elif mode == "adjoint":
+            eng.march(field, P, mode, src_exit=src, u_store=store, tol=1e-7)
+        else:
+            eng.march(field, P, mode, probes=probes, u_store=store, tol=1e-7)
+        st = eng.read_stats()
+        assert st["graph"] == (launch == 0), st
+        out[launch] = (store.cpu().numpy(), gc.cpu().numpy(), st)
+    eng.launch = 0
+    assert abs(out[0][2]["iterations"] - out[1][2]["iterations"]) <= 2
+    assert out[0][2]["solves"] == out[1][2]["solves"] == P * (nz - 1)
+    assert rel(out[0][0], out[1][0]) < 1e-6
+    if mode == "adjoint_exact":
+        assert rel(out[0][1], out[1][1]) < 1e-6

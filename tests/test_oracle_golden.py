@@ -260,3 +260,25 @@ def test_pit_gmres_matches_reference(golden, bc):
     for p in range(g["probes"].shape[0]):
         x = po.full_system_solve(A, B, C, po.pit_rhs(B, g["probes"][p], L))
         assert rel(x.reshape(L, N).T, g[f"fulllu_{bc}"][p][:, 1:]) < RTOL
+
+
+@pytest.mark.parametrize("bc", ["neumann", "impedance", "dirichlet"])
+def test_pit_adjoint_matches_reference(golden, bc):
+    """The restated adjoint-mode PiT solve (conjugate-transposed blocks, z-flipped
+    conjugate C, forward preconditioner) against PWEFullPinTSolver's mode
+    "adjoint", for a given right-hand side and for the probe right-hand side,
+    and against the direct solve of the same space-time system."""
+    g = golden("pit2d_adjoint")
+    N, dz, dx, k = int(g["nx"]), float(g["dz"]), float(g["dx"]), float(g["k"])
+    co = po.bc_coefficients(k, dx, dz, bc_type=bc)
+    A, B = po.step_matrices_1d(N, co, bc, dz)
+    C = po.object_contribution(g["n"], k, dz)
+    L = C.shape[1]
+    rhs = g["rhs_block"]
+    u, its = po.pit_solve_adjoint(A, B, C, probe=g["probes"][1], rhs=rhs.ravel(order="F"))
+    assert rel(u, g[f"adj_rhs_{bc}"]) < RTOL, rel(u, g[f"adj_rhs_{bc}"])
+    u2, _ = po.pit_solve_adjoint(A, B, C, probe=g["probes"][2])
+    assert rel(u2, g[f"adj_probe_{bc}"]) < RTOL, rel(u2, g[f"adj_probe_{bc}"])
+    # the system it solves: forward structure on (A^H, B^H, flipped conj C)
+    x = po.full_system_solve(A.conj().T.tocsr(), B.conj().T.tocsr(), np.flip(np.conj(C), axis=1), rhs.T.ravel())
+    assert rel(x.reshape(L, N).T, g[f"adj_rhs_{bc}"][:, 1:]) < 2e-5

@@ -1,5 +1,6 @@
 """GPU parity of the PiT space-time solve (the reference's PWEFullPinTSolver):
-against golden vectors of the unmodified reference (both α), the FullLU
+against golden vectors of the unmodified reference (both α, and its adjoint
+mode for a given right-hand side and for the probe right-hand side), the FullLU
 solution of the same system, the oracle's direct solve at N = 256 with a
 prime L = 127 (Bluestein z-DFT), a replaced right-hand side, and the warm
 start.
@@ -91,7 +92,7 @@ def test_pit_rhs_block_and_warm_start(golden):
     u2 = s.solve(n=n)[0, 0]
     assert rel(u2, u1) < TOL and max(s.gmres_iterations) <= max(it1)
     with pytest.raises(NotImplementedError):
-        s.solve(n=n, mode="adjoint")
+        s.solve(n=n, mode="reverse")
 
 
 @pytest.mark.parametrize("nz", [50, 160, 1025])
@@ -115,3 +116,31 @@ def test_pit_bluestein_lengths_against_oracle(nz):
     for p in range(P):
         ref = po.full_system_solve(A, B, C, po.pit_rhs(B, probes[p], L)).reshape(L, N).T
         assert rel(u[p][:, 1:], ref) < TOL, (p, rel(u[p][:, 1:], ref))
+
+
+@pytest.mark.parametrize("bc", ["neumann", "impedance", "dirichlet"])
+def test_pit_adjoint_against_reference_golden(golden, bc):
+    """mode "adjoint" (full_pint.py:140-166): the reference's system with
+    conjugate-transposed blocks and the z-flipped conjugate object term,
+    right-preconditioned by the forward preconditioner, against its own solve
+    for a flat column-major right-hand side and for a probe (B u_0 with the
+    forward B), and against the direct solve of that system."""
+    g = golden("pit2d_adjoint")
+    N, nz = int(g["nx"]), int(g["nz"])
+    L = nz - 1
+    s = PWEGpuPiTSolver(_geo(g, 4), g["probes"][None], bc_type=bc)
+    rhs = g["rhs_block"]
+    n = g["n"]
+    u = s._solve_single_probe(n=n, mode="adjoint", rhs_block=rhs.ravel(order="F"), probe=g["probes"][1])
+    assert rel(u, g[f"adj_rhs_{bc}"]) < TOL, rel(u, g[f"adj_rhs_{bc}"])
+    co = po.bc_coefficients(float(g["k"]), float(g["dx"]), float(g["dz"]), bc_type=bc)
+    A, B = po.step_matrices_1d(N, co, bc, float(g["dz"]))
+    C = po.object_contribution(n, float(g["k"]), float(g["dz"]))
+    x = po.full_system_solve(A.conj().T.tocsr(), B.conj().T.tocsr(), np.flip(np.conj(C), axis=1), rhs.T.ravel())
+    assert rel(u[:, 1:], x.reshape(L, N).T) < TOL
+    s2 = PWEGpuPiTSolver(_geo(g, 4), g["probes"][None], bc_type=bc)
+    u2 = s2._solve_single_probe(n=n, mode="adjoint", probe=g["probes"][2])
+    assert rel(u2, g[f"adj_probe_{bc}"]) < TOL, rel(u2, g[f"adj_probe_{bc}"])
+    # the batched solve over every probe in adjoint mode equals the per-probe one
+    ub = s2.solve(n=n, mode="adjoint")[0, 0]
+    assert rel(ub[2], u2) < TOL

@@ -93,7 +93,7 @@ class TpPitArgs(ctypes.Structure):
         ("num_probes", ctypes.c_int32),
         ("restart", ctypes.c_int32),
         ("max_cycles", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("mode", ctypes.c_int32),
         ("alpha", ctypes.c_double),
         ("rtol", ctypes.c_double),
         ("atol", ctypes.c_double),
@@ -133,7 +133,7 @@ class TpCn3dOp(ctypes.Structure):
 class TpCn3dMarchArgs(ctypes.Structure):
     _fields_ = [
         ("num_probes", ctypes.c_int32), ("mode", ctypes.c_int32), ("max_iter", ctypes.c_int32),
-        ("precond", ctypes.c_int32), ("host_check", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("precond", ctypes.c_int32), ("host_check", ctypes.c_int32), ("launch", ctypes.c_int32),
         ("tol", ctypes.c_double),
         ("probes", ctypes.c_void_p), ("src_shared", ctypes.c_void_p), ("src_exit", ctypes.c_void_p),
         ("u_store", ctypes.c_void_p), ("exit_out", ctypes.c_void_p), ("u_fwd", ctypes.c_void_p),
@@ -213,7 +213,7 @@ SIGNATURES = [
                                         ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
                                         ctypes.c_void_p]),
     ("tp_cn3d_workspace_bytes", ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
-    ("tp_cn3d_learned_ws_bytes", ctypes.c_size_t, [ctypes.c_int32] * 3),
+    ("tp_cn3d_learned_ws_bytes", ctypes.c_size_t, [ctypes.c_int32] * 4),
     ("tp_cn3d_march", ctypes.c_int, [ctypes.POINTER(TpCn3dOp), ctypes.c_void_p, ctypes.c_int32,
                                      ctypes.POINTER(TpCn3dMarchArgs), ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
     ("tp_cnn_act_bytes", ctypes.c_size_t, [ctypes.c_int32] * 4),

@@ -48,8 +48,11 @@ class CN3D:
         self._ws_P = None
         self._lws = None
         self._lws_P = None
-        self.stats = torch.zeros(4, dtype=torch.int32, device=self.device)
+        self.stats = torch.zeros(5, dtype=torch.int32, device=self.device)
         self.fallbacks = 0
+        # 0: each march runs as one CUDA graph with device-side step and
+        # iteration loops; 1: step by step (host loop)
+        self.launch = 0
 
     def op(self, is_delta=False) -> _native.TpCn3dOp:
         o = _native.TpCn3dOp()
@@ -69,7 +72,7 @@ class CN3D:
 
     def learned_workspace(self, P):
         if self._lws is None or self._lws_P != P:
-            nbytes = int(self.lib.tp_cn3d_learned_ws_bytes(self.nx, self.ny, P))
+            nbytes = int(self.lib.tp_cn3d_learned_ws_bytes(self.nx, self.ny, self.nz, P))
             self._lws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
             self._lws_P = P
         return self._lws
@@ -128,6 +131,7 @@ class CN3D:
         a = _native.TpCn3dMarchArgs()
         a.num_probes, a.mode, a.max_iter, a.precond, a.host_check = P, mode_i, int(max_iter), int(precond), int(host_check)
         a.tol = float(tol)
+        a.launch = int(self.launch)
         a.probes, a.src_shared, a.src_exit = _ptr(probes), _ptr(src_shared), _ptr(src_exit)
         a.u_store, a.exit_out, a.u_fwd, a.grad_c = _ptr(u_store), _ptr(exit_out), _ptr(u_fwd), _ptr(grad_c)
         a.stats = ctypes.c_void_p(self.stats.data_ptr())
@@ -152,11 +156,12 @@ class CN3D:
         _native.check(rc, "tp_cn3d_march")
 
     def read_stats(self, reset=True):
-        """(total iterations, solves, failed solves, max iterations per solve)."""
+        """(total iterations, solves, failed solves, max iterations per solve,
+        whether the last march ran as one CUDA graph)."""
         s = self.stats.cpu().tolist()
         if reset:
             self.stats.zero_()
-        return {"iterations": s[0], "solves": s[1], "failed": s[2], "max_iterations": s[3]}
+        return {"iterations": s[0], "solves": s[1], "failed": s[2], "max_iterations": s[3], "graph": bool(s[4])}
 
     def grad_to_n(self, grad_c: torch.Tensor, field=None, is_delta=False) -> torch.Tensor:
         """Σ_p λ conj(u_s + u_{s−1}) (L, N) → torch-convention ∂/∂n (N, nz)."""

@@ -51,6 +51,30 @@ struct __align__(16) Krylov {
 // exceeded the tolerance, [3] largest iteration count of one solve.
 enum { kStatIters = 0, kStatSolves = 1, kStatFailed = 2, kStatMaxIters = 3 };
 
+// Step state of a march, kept on the device so that one launch sequence (or
+// one CUDA graph with device-side loops) serves every step: t is the current
+// step (1..L; 0 before the first), s its slice, it the BiCGStab iterations
+// of this step, pending = 1 while a probe of the step is still iterating.
+struct __align__(16) C3State {
+  int t, s, it, pending;
+};
+
+// Start step t = state.t + 1.  In a graph, `outer` is the condition of the
+// step loop (set to 0 at the last step, so the loop ends after L bodies) and
+// `inner` that of the iteration loop (re-armed for the new step).
+__global__ void c3_advance_kernel(C3State *st, int L, int backward, int use_cond, cudaGraphConditionalHandle outer,
+                                  cudaGraphConditionalHandle inner) {
+  const int t = st->t + 1;
+  st->t = t;
+  st->s = backward ? (L + 1 - t) : t;
+  st->it = 0;
+  st->pending = 1;
+  if (use_cond) {
+    cudaGraphSetConditional(outer, t < L ? 1u : 0u);
+    cudaGraphSetConditional(inner, 1u);
+  }
+}
+
 __device__ __forceinline__ double2 load_field(const C3Params &q, size_t idx) {
   if (q.dtype == TP_C128) return static_cast<const double2 *>(q.field)[idx];
   const float2 v = static_cast<const float2 *>(q.field)[idx];
@@ -88,14 +112,33 @@ __global__ void c3_diag_kernel(int N, int nf, double sigma, int conj_t, const fl
   }
 }
 
-// cd[i] = sigma*T(K)_c[i] + sigma*T(c_s(i)) for slice s (1-based), fp64 -> fp32.
-__global__ void c3_center_kernel(const C3Params q, int s, float2 *__restrict__ cd) {
+// cd[i] = sigma*T(K)_c[i] + sigma*T(c_s(i)) for slice s (1-based), fp64 -> fp32,
+// s = the current step's slice + next (next = 1: the slice after it, used by
+// the exact adjoint from its second step on).
+__global__ void c3_center_kernel(const C3Params q, const C3State *st, int next, float2 *__restrict__ cd) {
+  if (next && st->t == 1) return;
+  const int s = st->s + next;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
     const size_t base = (size_t)i * q.nz;
     const double2 c = zscale(zadd(coef3(q, load_field(q, base + s - 1)), coef3(q, load_field(q, base + s))), 0.25 * q.dz);
     const double2 v = zscale(q.conj_t ? zconj(c) : c, q.sigma);
     const float2 k = q.kc[i];
     cd[i] = make_float2((float)(k.x + v.x), (float)(k.y + v.y));
+  }
+}
+
+// Object diagonals of slices s0+1 .. s0+count in the forward orientation,
+// out[(s - s0 - 1) * N + i] = c_s(i) (sigma = 1, no transpose): the learned
+// filters' inputs.  The adjoint modes apply the conjugate of the forward
+// slice's filter (the transposed operator of a complex-symmetric K is its
+// elementwise conjugate, so its corrected inverse is the conjugate one).
+__global__ void c3_obj_diag_kernel(const C3Params q, int s0, int count, float2 *__restrict__ out) {
+  const size_t total = (size_t)count * q.N;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const int s = s0 + 1 + (int)(e / q.N), i = (int)(e % q.N);
+    const size_t base = (size_t)i * q.nz;
+    const double2 c = zscale(zadd(coef3(q, load_field(q, base + s - 1)), coef3(q, load_field(q, base + s))), 0.25 * q.dz);
+    out[e] = to_f2(c);
   }
 }
 
@@ -123,15 +166,23 @@ __device__ __forceinline__ void block_reduce_add(double v, double *dst, double *
   __syncthreads();
 }
 
-// Grid (chunks, P).  r = r0 = rhs = (P_l + P_r) u + src; x = p = v = 0.
-__global__ void __launch_bounds__(k3Threads) c3_init_kernel(const C3Params q, const float2 *__restrict__ cdl,
-                                                            const float2 *__restrict__ cdr, const float2 *__restrict__ u,
-                                                            int use_u, const float2 *__restrict__ src,
-                                                            const float2 *__restrict__ shared, float2 *x, float2 *r,
+// Grid (chunks, P).  r = r0 = rhs = (P_l + P_r) u + src; x = p = v = 0.  The
+// step t decides the terms: the exact adjoint's right-hand side uses the next
+// slice's operator (cdr) and has no u term at t = 1 (lambda_{L+1} = 0); the
+// per-probe source enters at t = 1; src_shared is (L, N) by step.
+__global__ void __launch_bounds__(k3Threads) c3_init_kernel(const C3Params q, const C3State *st, int adj_exact,
+                                                            const float2 *__restrict__ cdl, const float2 *__restrict__ cdn,
+                                                            const float2 *__restrict__ u, const float2 *__restrict__ src_exit,
+                                                            const float2 *__restrict__ src_shared, float2 *x, float2 *r,
                                                             float2 *r0, float2 *p, float2 *v, Krylov *K) {
   __shared__ double red[k3Threads / 32];
   const int pr = blockIdx.y;
   const size_t off = (size_t)pr * q.N;
+  const int t = st->t;
+  const int use_u = !(adj_exact && t == 1);
+  const float2 *cdr = (adj_exact && t > 1) ? cdn : cdl;
+  const float2 *src = (t == 1) ? src_exit : nullptr;
+  const float2 *shared = src_shared ? src_shared + (size_t)(t - 1) * q.N : nullptr;
   double acc = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
     float2 b = use_u ? cadd(apply_P(q, cdl, u + off, i), apply_P(q, cdr, u + off, i)) : make_float2(0.f, 0.f);
@@ -148,33 +199,54 @@ __global__ void __launch_bounds__(k3Threads) c3_init_kernel(const C3Params q, co
   block_reduce_add(acc, &K[pr].bnorm2, red);
 }
 
-// Per probe: start (first = 1) or commit an iteration.
-__global__ void c3_scalar_kernel(Krylov *K, int P, double tol2, int first, int *stats) {
+// Per probe: start a solve (rho = <r0, r0>, done when the right-hand side is zero).
+__global__ void c3_start_kernel(Krylov *K, int P) {
   const int pr = blockIdx.x * blockDim.x + threadIdx.x;
   if (pr >= P) return;
   Krylov &k = K[pr];
-  if (first) {
-    k.rho_prev = z2(1, 0);
-    k.rho_cur = z2(k.bnorm2, 0.0);  // <r0, r0>
-    k.alpha = z2(1, 0);
-    k.omega = z2(1, 0);
-    k.iters = 0;
-    k.done = (k.bnorm2 == 0.0) ? 1 : 0;
-  } else if (!k.done) {
-    const double den = k.acc_r0v.x * k.acc_r0v.x + k.acc_r0v.y * k.acc_r0v.y;
-    k.alpha = den > 0.0 ? zdiv(k.rho_cur, k.acc_r0v) : z2(0, 0);
-    k.omega = (k.acc_tt > 0.0) ? zscale(k.acc_ts, 1.0 / k.acc_tt) : z2(0, 0);
-    k.rho_prev = k.rho_cur;
-    k.rho_cur = k.acc_r0r;
-    k.iters += 1;
-    const double om2 = k.omega.x * k.omega.x + k.omega.y * k.omega.y;
-    const double rp2 = k.rho_prev.x * k.rho_prev.x + k.rho_prev.y * k.rho_prev.y;
-    if (k.acc_rr <= tol2 * k.bnorm2 || om2 == 0.0 || rp2 == 0.0) k.done = 1;
-  }
+  k.rho_prev = z2(1, 0);
+  k.rho_cur = z2(k.bnorm2, 0.0);
+  k.alpha = z2(1, 0);
+  k.omega = z2(1, 0);
+  k.iters = 0;
+  k.done = (k.bnorm2 == 0.0) ? 1 : 0;
   k.acc_r0v = k.acc_ts = k.acc_r0r = z2(0, 0);
   k.acc_tt = 0.0;
   k.acc_rr = 0.0;
-  (void)stats;
+}
+
+// Commit an iteration of every probe (one CTA loops over the probes), count
+// it in the step state and record whether a probe is still iterating.  In a
+// graph, `inner` (the iteration loop's condition) stays 1 only while a probe
+// is pending and fewer than max_iter iterations ran, so the loop is bounded.
+__global__ void c3_commit_kernel(Krylov *K, int P, double tol2, C3State *st, int max_iter, int use_cond,
+                                 cudaGraphConditionalHandle inner) {
+  int pend = 0;
+  for (int pr = threadIdx.x; pr < P; pr += blockDim.x) {
+    Krylov &k = K[pr];
+    if (!k.done) {
+      const double den = k.acc_r0v.x * k.acc_r0v.x + k.acc_r0v.y * k.acc_r0v.y;
+      k.alpha = den > 0.0 ? zdiv(k.rho_cur, k.acc_r0v) : z2(0, 0);
+      k.omega = (k.acc_tt > 0.0) ? zscale(k.acc_ts, 1.0 / k.acc_tt) : z2(0, 0);
+      k.rho_prev = k.rho_cur;
+      k.rho_cur = k.acc_r0r;
+      k.iters += 1;
+      const double om2 = k.omega.x * k.omega.x + k.omega.y * k.omega.y;
+      const double rp2 = k.rho_prev.x * k.rho_prev.x + k.rho_prev.y * k.rho_prev.y;
+      if (k.acc_rr <= tol2 * k.bnorm2 || om2 == 0.0 || rp2 == 0.0) k.done = 1;
+    }
+    pend |= !k.done;
+    k.acc_r0v = k.acc_ts = k.acc_r0r = z2(0, 0);
+    k.acc_tt = 0.0;
+    k.acc_rr = 0.0;
+  }
+  pend = __syncthreads_or(pend);
+  if (threadIdx.x == 0) {
+    const int it = st->it + 1;
+    st->it = it;
+    st->pending = pend;
+    if (use_cond) cudaGraphSetConditional(inner, (pend && it < max_iter) ? 1u : 0u);
+  }
 }
 
 // Twiddle table W_n^t = exp(-2 pi i t / n) (fp64 sincospi, rounded once).
@@ -376,40 +448,49 @@ __global__ void __launch_bounds__(k3Threads) c3_update_kernel(const C3Params q, 
 }
 
 // True residual of each solve: res2 = ||rhs - (I - P) d||^2 (rhs = r0, d = x),
-// then u += d.  Grid (chunks, P).
-__global__ void __launch_bounds__(k3Threads) c3_finish_kernel(const C3Params q, const float2 *__restrict__ cd,
+// then u += d, stored into node `to` of u_store (to = t, or L - t for the
+// flipped reference adjoint) and, at the last step, into exit_out.
+// Grid (chunks, P).
+__global__ void __launch_bounds__(k3Threads) c3_finish_kernel(const C3Params q, const C3State *st,
+                                                              const float2 *__restrict__ cd,
                                                               const float2 *__restrict__ x, const float2 *__restrict__ r0,
-                                                              float2 *u, Krylov *K) {
+                                                              float2 *u, Krylov *K, float2 *u_store, int flip,
+                                                              float2 *exit_out) {
   __shared__ double red[k3Threads / 32];
   const int pr = blockIdx.y;
   const size_t off = (size_t)pr * q.N;
+  const int t = st->t;
+  float2 *dst = u_store ? u_store + ((size_t)pr * q.nz + (flip ? q.L - t : t)) * q.N : nullptr;
+  float2 *ex = (exit_out && t == q.L) ? exit_out + off : nullptr;
   double acc = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
-    const float2 mx = csub(x[off + i], apply_P(q, cd, x + off, i));
+    const float2 xi = x[off + i];
+    const float2 mx = csub(xi, apply_P(q, cd, x + off, i));
     const float2 d = csub(r0[off + i], mx);
     acc += (double)d.x * d.x + (double)d.y * d.y;
-    u[off + i] = cadd(u[off + i], x[off + i]);
+    const float2 un = cadd(u[off + i], xi);
+    u[off + i] = un;
+    if (dst) dst[i] = un;
+    if (ex) ex[i] = un;
   }
   block_reduce_add(acc, &K[pr].res2, red);
 }
 
-// pending[0] += number of probes still iterating (the caller zeroes it).
-__global__ void c3_pending_kernel(const Krylov *K, int P, int *pending) {
-  const int pr = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pr < P && !K[pr].done) atomicAdd(pending, 1);
-}
-
+// After a step (one CTA loops over the probes): accumulate the statistics
+// (when `stats` is given) and clear the per-probe sums of the next step.
 __global__ void c3_stats_kernel(Krylov *K, int P, double tol2, int *stats) {
-  const int pr = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pr >= P) return;
-  Krylov &k = K[pr];
-  atomicAdd(&stats[kStatIters], k.iters);
-  atomicAdd(&stats[kStatSolves], 1);
-  atomicMax(&stats[kStatMaxIters], k.iters);
-  // the true residual may exceed the recursive one by round-off; allow 10x
-  if (k.res2 > 100.0 * tol2 * k.bnorm2) atomicAdd(&stats[kStatFailed], 1);
-  k.res2 = 0.0;
-  k.bnorm2 = 0.0;
+  for (int pr = threadIdx.x; pr < P; pr += blockDim.x) {
+    Krylov &k = K[pr];
+    if (stats != nullptr) {
+      atomicAdd(&stats[kStatIters], k.iters);
+      atomicAdd(&stats[kStatSolves], 1);
+      atomicMax(&stats[kStatMaxIters], k.iters);
+      // the true residual may exceed the recursive one by round-off; allow 10x
+      if (k.res2 > 100.0 * tol2 * k.bnorm2) atomicAdd(&stats[kStatFailed], 1);
+    }
+    k.res2 = 0.0;
+    k.bnorm2 = 0.0;
+  }
 }
 
 // Store the state (P, N) into slice `t` of u_store (P, nz, N) and/or exit.
@@ -423,10 +504,12 @@ __global__ void c3_store_kernel(int N, int P, int nz, int t, const float2 *__res
   }
 }
 
-// grad_c[s-1][i] += sum_p lambda_p[i] conj(u_p,s[i] + u_p,s-1[i])  (no atomics:
-// one thread owns element i and loops over the probes).
-__global__ void c3_grad_kernel(int N, int P, int nz, int s, const float2 *__restrict__ lam,
+// grad_c[s-1][i] += sum_p lambda_p[i] conj(u_p,s[i] + u_p,s-1[i]) for the
+// current step's slice s (no atomics: one thread owns element i and loops
+// over the probes).
+__global__ void c3_grad_kernel(int N, int P, int nz, const C3State *st, const float2 *__restrict__ lam,
                                const float2 *__restrict__ u_fwd, float2 *grad_c) {
+  const int s = st->s;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
     float2 acc = make_float2(0.f, 0.f);
     for (int pr = 0; pr < P; ++pr) {
@@ -439,15 +522,22 @@ __global__ void c3_grad_kernel(int N, int P, int nz, int s, const float2 *__rest
 }
 
 // Learned correction of the preconditioned vector: out = z + sum_t F_t z(x + o_t)
-// (conj(F) in the adjoint modes).  A thread owns one pixel for
-// kFilterProbes probes, so each filter value is read once per pixel group.
-// Grid (N / 256, P / kFilterProbes).
+// with the filter of the current step's slice s (conj(F) in the adjoint
+// modes).  The filters of all slices are computed before the march, in
+// chunks of `chunk` slices: slice s uses image (s-1) % chunk of chunk
+// (s-1) / chunk, tap-major within the chunk (13, chunk * N).  A thread owns
+// one pixel for kFilterProbes probes, so each filter value is read once per
+// pixel group.  Grid (N / 256, P / kFilterProbes).
 constexpr int kFilterProbes = 8;
-__global__ void __launch_bounds__(k3Threads) c3_filter_kernel(const C3Params q, const float2 *__restrict__ F,
+__global__ void __launch_bounds__(k3Threads) c3_filter_kernel(const C3Params q, const C3State *st, int chunk,
+                                                              const float2 *__restrict__ Fall,
                                                               const float2 *__restrict__ z, float2 *out,
                                                               const Krylov *K) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= q.N) return;
+  const int sl = st->s - 1;
+  const size_t np = (size_t)chunk * q.N;
+  const float2 *F = Fall + (size_t)(sl / chunk) * kFilterTaps * np + (size_t)(sl % chunk) * q.N;
   const int b = i / q.nf, f = i - b * q.nf;
   float2 w[kFilterTaps];
   int o[kFilterTaps];
@@ -455,7 +545,7 @@ __global__ void __launch_bounds__(k3Threads) c3_filter_kernel(const C3Params q, 
   for (int t = 0; t < kFilterTaps; ++t) {
     const int bb = b + filter_tap_dy(t), ff = f + filter_tap_dx(t);
     const bool in = bb >= 0 && bb < q.nb && ff >= 0 && ff < q.nf;
-    float2 v = in ? F[(size_t)t * q.N + i] : make_float2(0.f, 0.f);
+    float2 v = in ? F[(size_t)t * np + i] : make_float2(0.f, 0.f);
     if (q.conj_t) v.y = -v.y;
     w[t] = v;
     o[t] = in ? (bb * q.nf + ff) : i;
@@ -498,6 +588,9 @@ __global__ void c3_noise_kernel(int N, int P, int step, float2 *x) {
   }
 }
 
+// stats[4] = how the march ran: 1 as one CUDA graph with device-side loops, 0 step by step.
+__global__ void c3_flag_kernel(int *stats, int graph) { stats[4] = graph; }
+
 // out[i] = cd[i] - kc[i]: the object part sigma*T(c_s) of the slice's diagonal.
 __global__ void c3_diag_diff_kernel(int N, const float2 *__restrict__ cd, const float2 *__restrict__ kc, float2 *out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
@@ -511,7 +604,7 @@ struct C3Work {
   float2 *dc, *dw, *de, *ds, *dn;
   float2 *sym, *twf, *twb;  // preconditioner symbol (N) and twiddle tables
   Krylov *K;
-  int *pending;
+  C3State *st;
   size_t bytes;
 };
 
@@ -533,7 +626,7 @@ static C3Work c3_layout(char *base, int N, int P) {
   w.twf = reinterpret_cast<float2 *>(take((size_t)kFftMaxN * sizeof(float2)));
   w.twb = reinterpret_cast<float2 *>(take((size_t)kFftMaxN * sizeof(float2)));
   w.K = reinterpret_cast<Krylov *>(take((size_t)P * sizeof(Krylov)));
-  w.pending = reinterpret_cast<int *>(take(sizeof(int)));
+  w.st = reinterpret_cast<C3State *>(take(sizeof(C3State)));
   w.bytes = off;
   return w;
 }
@@ -580,15 +673,21 @@ static int fft_rows_of(int n, int rows) {
   return r;
 }
 
-// Learned-preconditioner workspace: the CNN activations of one slice, the
-// slice's filter (13, N) and the plain-preconditioned vectors (P, N).
+// Learned-preconditioner workspace: the CNN activations of one chunk of
+// slices, the per-pixel filters of every slice (chunked, see c3_filter_kernel),
+// the object diagonals of one chunk and the plain-preconditioned vectors (P, N).
+constexpr int kCnnChunk = 64;
+
+static int cnn_chunk(int L) { return L < kCnnChunk ? L : kCnnChunk; }
+
 struct C3Learned {
   char *cnn;
-  float2 *F, *zt;
+  float2 *F, *dg, *zt;
+  int chunk, nchunks;
   size_t cnn_bytes, bytes;
 };
 
-static C3Learned c3_learned_layout(char *base, int nf, int nb, int P) {
+static C3Learned c3_learned_layout(char *base, int nf, int nb, int nz, int P) {
   C3Learned l{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -597,21 +696,74 @@ static C3Learned c3_learned_layout(char *base, int nf, int nb, int P) {
     return ptr;
   };
   const size_t N = (size_t)nf * nb;
-  l.cnn_bytes = cnn_forward_ws_bytes(conv_geom(nb, nf, 1));
+  const int L = nz - 1;
+  l.chunk = cnn_chunk(L);
+  l.nchunks = (L + l.chunk - 1) / l.chunk;
+  l.cnn_bytes = cnn_forward_ws_bytes(conv_geom(nb, nf, l.chunk));
   l.cnn = take(l.cnn_bytes);
-  l.F = reinterpret_cast<float2 *>(take((size_t)kFilterTaps * N * sizeof(float2)));
+  l.F = reinterpret_cast<float2 *>(take((size_t)l.nchunks * kFilterTaps * l.chunk * N * sizeof(float2)));
+  l.dg = reinterpret_cast<float2 *>(take((size_t)l.chunk * N * sizeof(float2)));
   l.zt = reinterpret_cast<float2 *>(take((size_t)P * N * sizeof(float2)));
   l.bytes = off;
   return l;
+}
+
+// Streams used only to record graphs (never to run work), one set per host thread.
+struct CaptureStreams {
+  cudaStream_t s[3] = {nullptr, nullptr, nullptr};
+  int dev = -1;
+  ~CaptureStreams() {
+    for (cudaStream_t &x : s)
+      if (x) cudaStreamDestroy(x);
+  }
+};
+
+static int capture_streams(cudaStream_t **out) {
+  static thread_local CaptureStreams cs;
+  int dev = 0;
+  TP_CHECK_CUDA(cudaGetDevice(&dev));
+  if (cs.dev != dev) {
+    for (cudaStream_t &x : cs.s) {
+      if (x) cudaStreamDestroy(x);
+      x = nullptr;
+    }
+    for (cudaStream_t &x : cs.s) TP_CHECK_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+    cs.dev = dev;
+  }
+  *out = cs.s;
+  return TP_OK;
+}
+
+// Append a WHILE node (condition `h`, created on the graph being recorded by
+// `rec`, default value `dflt` at every launch) after the nodes recorded so
+// far on `rec`; returns its body graph.
+static int add_while(cudaStream_t rec, unsigned dflt, cudaGraphConditionalHandle *h, cudaGraph_t *body) {
+  cudaStreamCaptureStatus status;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  TP_CHECK_CUDA(cudaStreamGetCaptureInfo(rec, &status, nullptr, &g, &deps, &nd));
+  if (status != cudaStreamCaptureStatusActive) return set_error(TP_ERR_CUDA, "add_while: stream is not recording");
+  TP_CHECK_CUDA(cudaGraphConditionalHandleCreate(h, g, dflt, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = *h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  TP_CHECK_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p));
+  *body = p.conditional.phGraph_out[0];
+  TP_CHECK_CUDA(cudaStreamUpdateCaptureDependencies(rec, &node, 1, cudaStreamSetCaptureDependencies));
+  return TP_OK;
 }
 
 }  // namespace tp
 
 using namespace tp;
 
-extern "C" size_t tp_cn3d_learned_ws_bytes(int32_t nf, int32_t nb, int32_t num_probes) {
-  if (nf < 1 || nb < 1 || num_probes < 1) return 0;
-  return c3_learned_layout(nullptr, nf, nb, num_probes).bytes;
+extern "C" size_t tp_cn3d_learned_ws_bytes(int32_t nf, int32_t nb, int32_t nz, int32_t num_probes) {
+  if (nf < 1 || nb < 1 || nz < 2 || num_probes < 1) return 0;
+  return c3_learned_layout(nullptr, nf, nb, nz, num_probes).bytes;
 }
 
 extern "C" size_t tp_cn3d_workspace_bytes(int32_t n_total, int32_t num_probes) {
@@ -670,11 +822,12 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     if (a->mode == TP_MODE_REVERSE) return set_error(TP_ERR_UNSUPPORTED, "learned preconditioner: REVERSE mode is not supported");
     if ((reinterpret_cast<uintptr_t>(a->learned_ws) & 255u) != 0)
       return set_error(TP_ERR_INVALID, "learned workspace must be 256-byte aligned");
-    lw = c3_learned_layout(static_cast<char *>(a->learned_ws), nf, nb, P);
+    lw = c3_learned_layout(static_cast<char *>(a->learned_ws), nf, nb, nz, P);
     if (a->learned_ws_bytes < lw.bytes)
       return set_error(TP_ERR_WORKSPACE, "learned workspace %zu B < %zu B", a->learned_ws_bytes, lw.bytes);
   }
-  if (a->train_every > 0 && (a->train_z0 == nullptr || a->train_sol == nullptr || a->train_diag == nullptr))
+  const bool train = a->train_every > 0;
+  if (train && (a->train_z0 == nullptr || a->train_sol == nullptr || a->train_diag == nullptr))
     return set_error(TP_ERR_INVALID, "train_every needs train_z0, train_sol and train_diag");
   const int rpc = fft_rows_of(nf, nb), cpc = fft_rows_of(nb, nf);
   const int use_fft = fft_on;
@@ -692,84 +845,199 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   const int max_iter = a->max_iter > 0 ? a->max_iter : 20;
   const double tol2 = (a->tol > 0 ? a->tol : 1e-6) * (a->tol > 0 ? a->tol : 1e-6);
   int *stats = a->stats;
-
-  const int eb = 296;
-  if (use_fft) {
-    c3_twiddle_kernel<<<(nf + 255) / 256, 256, 0, st>>>(nf, w.twf);
-    c3_twiddle_kernel<<<(nb + 255) / 256, 256, 0, st>>>(nb, w.twb);
-    c3_symbol_kernel<<<eb, 256, 0, st>>>(q, w.sym);
-  }
-  // M0^{-1} in -> out (mode 0/1/2 input of the row kernel; Kp NULL = all probes)
-  auto precondition = [&](int mode, const float2 *rin, float2 *out, const Krylov *Kp) {
-    pk.rows<<<dim3(nb / rows_cta, P), k3Threads, use_fft ? smem_rows : 0, st>>>(
-        pf, q, mode, rin, w.p, w.v, w.s, use_fft ? w.hat : out, Kp, rows_cta, use_fft, w.twf);
-    if (use_fft) {
-      pk.cols<<<dim3(nf / cpc, P), k3Threads, smem_cols, st>>>(pb, q, w.hat, Kp, cpc, w.twb, w.sym);
-      pk.inv<<<dim3(nb / rpc, P), k3Threads, smem_rows, st>>>(pf, q, w.hat, out, Kp, rpc, w.twf);
-    }
-  };
-  const dim3 fgrid((N + k3Threads - 1) / k3Threads, (P + kFilterProbes - 1) / kFilterProbes);
-  c3_diag_kernel<<<eb, 256, 0, st>>>(N, nf, q.sigma, q.conj_t, static_cast<const float2 *>(op->kc),
-                                     static_cast<const float2 *>(op->kw), static_cast<const float2 *>(op->ke),
-                                     static_cast<const float2 *>(op->ks), static_cast<const float2 *>(op->kn), w.dc, w.dw,
-                                     w.de, w.ds, w.dn);
-  // the CNN activations' zero borders are never written by the kernels
-  if (learned) TP_CHECK_CUDA(cudaMemsetAsync(lw.cnn, 0, lw.cnn_bytes, st));
-  const ConvGeom g1 = conv_geom(nb, nf, 1);
-  // initial state
-  TP_CHECK_CUDA(cudaMemsetAsync(w.u, 0, (size_t)P * N * sizeof(float2), st));
-  if (a->probes != nullptr)
-    TP_CHECK_CUDA(cudaMemcpyAsync(w.u, a->probes, (size_t)P * N * sizeof(float2), cudaMemcpyDeviceToDevice, st));
-  TP_CHECK_CUDA(cudaMemsetAsync(w.K, 0, (size_t)P * sizeof(Krylov), st));
   const bool backward = a->mode != TP_MODE_FORWARD;
   const bool flip = a->mode == TP_MODE_ADJOINT;
+  const int adj_exact = a->mode == TP_MODE_ADJOINT_EXACT ? 1 : 0;
   float2 *ust = static_cast<float2 *>(a->u_store);
-  if (ust) c3_store_kernel<<<eb, 256, 0, st>>>(N, P, nz, flip ? L : 0, w.u, ust, nullptr);
+  float2 *exit_out = static_cast<float2 *>(a->exit_out);
+  const dim3 fgrid((N + k3Threads - 1) / k3Threads, (P + kFilterProbes - 1) / kFilterProbes);
   const dim3 vgrid((N + 256 * 8 - 1) / (256 * 8), P);
   const int pgrid = (P + 127) / 128;
-  for (int t = 1; t <= L; ++t) {
-    const int s = backward ? (L + 1 - t) : t;
-    c3_center_kernel<<<eb, 256, 0, st>>>(q, s, w.cdl);
-    const float2 *cdr = w.cdl;
-    int use_u = 1;
-    if (a->mode == TP_MODE_ADJOINT_EXACT) {
-      if (t == 1) use_u = 0;  // lambda_{L+1} = 0
-      else {
-        c3_center_kernel<<<eb, 256, 0, st>>>(q, s + 1, w.cdr);
-        cdr = w.cdr;
+  const int one_cta = P >= 1024 ? 1024 : ((P + 31) / 32) * 32;
+  const int eb = 296;
+  const ConvGeom gch = learned ? conv_geom(nb, nf, lw.chunk) : ConvGeom{};
+
+  // ---- launch sequences (recorded into a graph, or issued step by step)
+  // M0^{-1} in -> out (mode 0/1/2 input of the row kernel; Kp NULL = all probes)
+  auto precondition = [&](cudaStream_t s, int mode, const float2 *rin, float2 *out, const Krylov *Kp) {
+    pk.rows<<<dim3(nb / rows_cta, P), k3Threads, use_fft ? smem_rows : 0, s>>>(
+        pf, q, mode, rin, w.p, w.v, w.s, use_fft ? w.hat : out, Kp, rows_cta, use_fft, w.twf);
+    if (use_fft) {
+      pk.cols<<<dim3(nf / cpc, P), k3Threads, smem_cols, s>>>(pb, q, w.hat, Kp, cpc, w.twb, w.sym);
+      pk.inv<<<dim3(nb / rpc, P), k3Threads, smem_rows, s>>>(pf, q, w.hat, out, Kp, rpc, w.twf);
+    }
+  };
+  auto prologue = [&](cudaStream_t s) -> int {
+    if (use_fft) {
+      c3_twiddle_kernel<<<(nf + 255) / 256, 256, 0, s>>>(nf, w.twf);
+      c3_twiddle_kernel<<<(nb + 255) / 256, 256, 0, s>>>(nb, w.twb);
+      c3_symbol_kernel<<<eb, 256, 0, s>>>(q, w.sym);
+    }
+    c3_diag_kernel<<<eb, 256, 0, s>>>(N, nf, q.sigma, q.conj_t, static_cast<const float2 *>(op->kc),
+                                      static_cast<const float2 *>(op->kw), static_cast<const float2 *>(op->ke),
+                                      static_cast<const float2 *>(op->ks), static_cast<const float2 *>(op->kn), w.dc,
+                                      w.dw, w.de, w.ds, w.dn);
+    if (learned) {
+      // the filters of every slice, chunk by chunk (the CNN activations' zero
+      // borders are never written by the kernels)
+      TP_CHECK_CUDA(cudaMemsetAsync(lw.cnn, 0, lw.cnn_bytes, s));
+      C3Params qf = q;  // forward orientation
+      qf.sigma = 1.0;
+      qf.conj_t = 0;
+      for (int c = 0; c < lw.nchunks; ++c) {
+        const int s0 = c * lw.chunk, cnt = (L - s0) < lw.chunk ? (L - s0) : lw.chunk;
+        if (cnt < lw.chunk) TP_CHECK_CUDA(cudaMemsetAsync(lw.dg, 0, (size_t)lw.chunk * N * sizeof(float2), s));
+        c3_obj_diag_kernel<<<eb * 2, 256, 0, s>>>(qf, s0, cnt, lw.dg);
+        const int rc = cnn_forward(gch, *a->model, lw.dg, N, nullptr, lw.cnn,
+                                   lw.F + (size_t)c * kFilterTaps * lw.chunk * N, s);
+        if (rc != TP_OK) return rc;
       }
     }
-    const float2 *src = (t == 1) ? static_cast<const float2 *>(a->src_exit) : nullptr;
-    const float2 *shared = a->src_shared ? static_cast<const float2 *>(a->src_shared) + (size_t)(t - 1) * N : nullptr;
-    if (learned) {
-      const int rc = cnn_forward(g1, *a->model, w.cdl, 0, w.dc, lw.cnn, lw.F, st);
-      if (rc != TP_OK) return rc;
-    }
-    c3_init_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, cdr, w.u, use_u, src, shared, w.x, w.r, w.r0, w.p, w.v, w.K);
-    c3_scalar_kernel<<<pgrid, 128, 0, st>>>(w.K, P, tol2, 1, stats);
+    TP_CHECK_CUDA(cudaMemsetAsync(w.u, 0, (size_t)P * N * sizeof(float2), s));
+    if (a->probes != nullptr)
+      TP_CHECK_CUDA(cudaMemcpyAsync(w.u, a->probes, (size_t)P * N * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+    TP_CHECK_CUDA(cudaMemsetAsync(w.K, 0, (size_t)P * sizeof(Krylov), s));
+    TP_CHECK_CUDA(cudaMemsetAsync(w.st, 0, sizeof(C3State), s));
+    if (ust) c3_store_kernel<<<eb, 256, 0, s>>>(N, P, nz, flip ? L : 0, w.u, ust, nullptr);
+    return TP_OK;
+  };
+  // step head: slice state, operators, right-hand side, Krylov start
+  auto step_head = [&](cudaStream_t s, int use_cond, cudaGraphConditionalHandle outer, cudaGraphConditionalHandle inner) {
+    c3_advance_kernel<<<1, 1, 0, s>>>(w.st, L, backward ? 1 : 0, use_cond, outer, inner);
+    c3_center_kernel<<<eb, 256, 0, s>>>(q, w.st, 0, w.cdl);
+    if (adj_exact) c3_center_kernel<<<eb, 256, 0, s>>>(q, w.st, 1, w.cdr);
+    c3_init_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.st, adj_exact, w.cdl, w.cdr, w.u,
+                                                static_cast<const float2 *>(a->src_exit),
+                                                static_cast<const float2 *>(a->src_shared), w.x, w.r, w.r0, w.p, w.v,
+                                                w.K);
+    c3_start_kernel<<<pgrid, 128, 0, s>>>(w.K, P);
+  };
+  // one BiCGStab iteration of every pending probe
+  auto iteration = [&](cudaStream_t s, int use_cond, cudaGraphConditionalHandle inner) {
+    // p = r + beta (p - omega v); y = Prec(p); v = M y
+    precondition(s, 0, w.r, learned ? lw.zt : w.y, w.K);
+    if (learned) c3_filter_kernel<<<fgrid, k3Threads, 0, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.y, w.K);
+    c3_matvec_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.cdl, w.y, w.v, w.r0, w.s, w.K, 0);
+    // s = r - alpha v; z = Prec(s); t = M z
+    precondition(s, 1, w.r, learned ? lw.zt : w.z, w.K);
+    if (learned) c3_filter_kernel<<<fgrid, k3Threads, 0, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.z, w.K);
+    c3_matvec_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K, 1);
+    c3_update_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.x, w.r, w.r0, w.y, w.z, w.s, w.t, w.K);
+    c3_commit_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, w.st, max_iter, use_cond, inner);
+  };
+  // step tail: u += x (true residual, store), statistics, gradient
+  auto step_tail = [&](cudaStream_t s) {
+    c3_finish_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.st, w.cdl, w.x, w.r0, w.u, w.K, ust, flip ? 1 : 0, exit_out);
+    c3_stats_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, stats);
+    if (a->grad_c)
+      c3_grad_kernel<<<eb, 256, 0, s>>>(N, P, nz, w.st, w.u, static_cast<const float2 *>(a->u_fwd),
+                                        static_cast<float2 *>(a->grad_c));
+  };
+
+  // ---- one graph: prologue, then WHILE(step) { head; WHILE(iteration) {..}; tail }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  TP_CHECK_CUDA(cudaStreamIsCapturing(st, &cap));
+  const bool use_graph = !train && cap == cudaStreamCaptureStatusNone && a->launch == 0 && a->host_check != 0;
+  if (use_graph) {
+    cudaStream_t *rs = nullptr;
+    int rc = capture_streams(&rs);
+    if (rc != TP_OK) return rc;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    TP_CHECK_CUDA(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h_step = 0, h_iter = 0;
+    cudaGraph_t body_step = nullptr, body_iter = nullptr;
+    auto record = [&]() -> int {
+      TP_CHECK_CUDA(cudaStreamBeginCaptureToGraph(rs[0], g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+      int r = prologue(rs[0]);
+      if (r == TP_OK) r = add_while(rs[0], 1u, &h_step, &body_step);
+      cudaGraph_t g_end = nullptr;
+      const cudaError_t e0 = cudaStreamEndCapture(rs[0], &g_end);
+      if (r != TP_OK) return r;
+      TP_CHECK_CUDA(e0);
+      // step body
+      TP_CHECK_CUDA(cudaStreamBeginCaptureToGraph(rs[1], body_step, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+      // h_iter is created on the step body (it is re-armed by the advance kernel)
+      {
+        cudaStreamCaptureStatus status;
+        cudaGraph_t gb = nullptr;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t nd = 0;
+        r = check_cuda(cudaStreamGetCaptureInfo(rs[1], &status, nullptr, &gb, &deps, &nd), "cudaStreamGetCaptureInfo");
+        if (r == TP_OK) r = check_cuda(cudaGraphConditionalHandleCreate(&h_iter, gb, 1u, 0), "cudaGraphConditionalHandleCreate");
+      }
+      if (r == TP_OK) {
+        step_head(rs[1], 1, h_step, h_iter);
+        r = check_cuda(cudaGetLastError(), "step head launches");
+      }
+      if (r == TP_OK) {
+        // the iteration loop, on a node whose handle already exists
+        cudaStreamCaptureStatus status;
+        cudaGraph_t gb = nullptr;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t nd = 0;
+        r = check_cuda(cudaStreamGetCaptureInfo(rs[1], &status, nullptr, &gb, &deps, &nd), "cudaStreamGetCaptureInfo");
+        if (r == TP_OK) {
+          cudaGraphNodeParams p = {};
+          p.type = cudaGraphNodeTypeConditional;
+          p.conditional.handle = h_iter;
+          p.conditional.type = cudaGraphCondTypeWhile;
+          p.conditional.size = 1;
+          cudaGraphNode_t node;
+          r = check_cuda(cudaGraphAddNode(&node, gb, deps, nd, &p), "cudaGraphAddNode (iteration loop)");
+          if (r == TP_OK) {
+            body_iter = p.conditional.phGraph_out[0];
+            r = check_cuda(cudaStreamUpdateCaptureDependencies(rs[1], &node, 1, cudaStreamSetCaptureDependencies),
+                           "cudaStreamUpdateCaptureDependencies");
+          }
+        }
+      }
+      if (r == TP_OK) {
+        step_tail(rs[1]);
+        r = check_cuda(cudaGetLastError(), "step tail launches");
+      }
+      cudaGraph_t b_end = nullptr;
+      const cudaError_t e1 = cudaStreamEndCapture(rs[1], &b_end);
+      if (r != TP_OK) return r;
+      TP_CHECK_CUDA(e1);
+      // iteration body
+      TP_CHECK_CUDA(cudaStreamBeginCaptureToGraph(rs[2], body_iter, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+      iteration(rs[2], 1, h_iter);
+      r = check_cuda(cudaGetLastError(), "iteration launches");
+      cudaGraph_t i_end = nullptr;
+      const cudaError_t e2 = cudaStreamEndCapture(rs[2], &i_end);
+      if (r != TP_OK) return r;
+      TP_CHECK_CUDA(e2);
+      TP_CHECK_CUDA(cudaGraphInstantiate(&ge, g, 0));
+      return TP_OK;
+    };
+    rc = record();
+    if (rc == TP_OK) rc = check_cuda(cudaGraphLaunch(ge, st), "cudaGraphLaunch (3D march)");
+    // an executable graph still running is freed when it completes
+    if (ge) cudaGraphExecDestroy(ge);
+    cudaGraphDestroy(g);
+    if (rc != TP_OK) return rc;
+    if (stats) c3_flag_kernel<<<1, 1, 0, st>>>(stats, 1);
+    return check_cuda(cudaGetLastError(), "tp_cn3d_march graph");
+  }
+
+  // ---- step by step on the caller's stream
+  int rc = prologue(st);
+  if (rc != TP_OK) return rc;
+  for (int t = 1; t <= L; ++t) {
+    step_head(st, 0, 0, 0);
     for (int it = 0; it < max_iter; ++it) {
-      // p = r + beta (p - omega v); y = Prec(p); v = M y
-      precondition(0, w.r, learned ? lw.zt : w.y, w.K);
-      if (learned) c3_filter_kernel<<<fgrid, k3Threads, 0, st>>>(q, lw.F, lw.zt, w.y, w.K);
-      c3_matvec_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, w.y, w.v, w.r0, w.s, w.K, 0);
-      // s = r - alpha v; z = Prec(s); t = M z
-      precondition(1, w.r, learned ? lw.zt : w.z, w.K);
-      if (learned) c3_filter_kernel<<<fgrid, k3Threads, 0, st>>>(q, lw.F, lw.zt, w.z, w.K);
-      c3_matvec_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K, 1);
-      c3_update_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.x, w.r, w.r0, w.y, w.z, w.s, w.t, w.K);
-      c3_scalar_kernel<<<pgrid, 128, 0, st>>>(w.K, P, tol2, 0, stats);
+      iteration(st, 0, 0);
       if (a->host_check && it + 1 < max_iter) {
         // stop launching iterations once every probe has converged
-        TP_CHECK_CUDA(cudaMemsetAsync(w.pending, 0, sizeof(int), st));
-        c3_pending_kernel<<<pgrid, 128, 0, st>>>(w.K, P, w.pending);
-        int pending = 0;
-        TP_CHECK_CUDA(cudaMemcpyAsync(&pending, w.pending, sizeof(int), cudaMemcpyDeviceToHost, st));
+        C3State hs{};
+        TP_CHECK_CUDA(cudaMemcpyAsync(&hs, w.st, sizeof(C3State), cudaMemcpyDeviceToHost, st));
         TP_CHECK_CUDA(cudaStreamSynchronize(st));
-        if (pending == 0) break;
+        if (hs.pending == 0) break;
       }
     }
-    c3_finish_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, w.x, w.r0, w.u, w.K);
-    if (a->train_every > 0 && t % a->train_every == 0) {
+    c3_finish_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.st, w.cdl, w.x, w.r0, w.u, w.K, ust, flip ? 1 : 0, exit_out);
+    if (train && t % a->train_every == 0) {
       // training pair of this step: z0 = M0^{-1} v and x with (I - P_s) x = v,
       // v the step's right-hand side r0 and x its converged update
       // (train_kind 0), or x white noise and v = (I - P_s) x (train_kind 1);
@@ -785,17 +1053,14 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
       } else {
         TP_CHECK_CUDA(cudaMemcpyAsync(tx, w.x, (size_t)P * N * sizeof(float2), cudaMemcpyDeviceToDevice, st));
       }
-      precondition(2, v, tz, nullptr);
+      precondition(st, 2, v, tz, nullptr);
       c3_diag_diff_kernel<<<eb, 256, 0, st>>>(N, w.cdl, w.dc, static_cast<float2 *>(a->train_diag) + k * N);
     }
-    if (stats) c3_stats_kernel<<<pgrid, 128, 0, st>>>(w.K, P, tol2, stats);
-    else TP_CHECK_CUDA(cudaMemsetAsync(w.K, 0, (size_t)P * sizeof(Krylov), st));
-    const int to = flip ? (L - t) : t;
-    if (ust || (t == L && a->exit_out))
-      c3_store_kernel<<<eb, 256, 0, st>>>(N, P, nz, to, w.u, ust, (t == L) ? static_cast<float2 *>(a->exit_out) : nullptr);
+    c3_stats_kernel<<<1, one_cta, 0, st>>>(w.K, P, tol2, stats);
     if (a->grad_c)
-      c3_grad_kernel<<<eb, 256, 0, st>>>(N, P, nz, s, w.u, static_cast<const float2 *>(a->u_fwd),
+      c3_grad_kernel<<<eb, 256, 0, st>>>(N, P, nz, w.st, w.u, static_cast<const float2 *>(a->u_fwd),
                                          static_cast<float2 *>(a->grad_c));
   }
+  if (stats) c3_flag_kernel<<<1, 1, 0, st>>>(stats, 0);
   return check_cuda(cudaGetLastError(), "tp_cn3d_march launches");
 }

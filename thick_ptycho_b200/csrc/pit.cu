@@ -43,12 +43,17 @@ constexpr int kPitThreads = 256;
 constexpr int kPitMaxRestart = 64;
 constexpr int kPitDotGroup = 8;  // basis vectors per inner-product launch
 
-// K's tridiagonal from the 2D operator (fp32 copies for the stencils).
+// A tridiagonal K (fp32 copies for the stencils): interior values, the two
+// corner diagonals, and one special entry on each off-diagonal (K's at
+// K[N-1, N-2] and K[0, 1]; its conjugate transpose's at K^H[1, 0] and
+// K^H[N-2, N-1]).
 struct PitK {
   int N;
-  float2 off, diag, d0, dn, k01, knm;
-  __device__ __forceinline__ float2 sub(int i) const { return i == N - 1 ? knm : off; }  // K[i, i-1]
-  __device__ __forceinline__ float2 sup(int i) const { return i == 0 ? k01 : off; }      // K[i, i+1]
+  float2 off, diag, d0, dn;
+  int sub_i, sup_i;
+  float2 sub_v, sup_v;
+  __device__ __forceinline__ float2 sub(int i) const { return i == sub_i ? sub_v : off; }  // K[i, i-1]
+  __device__ __forceinline__ float2 sup(int i) const { return i == sup_i ? sup_v : off; }  // K[i, i+1]
   __device__ __forceinline__ float2 dia(int i) const { return i == 0 ? d0 : (i == N - 1 ? dn : diag); }
 };
 struct PitKd {  // the same in fp64 (block factorisation)
@@ -70,6 +75,7 @@ __device__ __forceinline__ float2 pit_kv(const PitK &K, const float2 *v, int i) 
 // ------------------------------------------------------------------ object
 struct PitObj {
   int N, nz, L, n_obj, empty_px, exact, is_delta, dtype;
+  int flip_conj;  // 1: C'[j] = conj(C[L-1-j]) (the reference's adjoint system)
   double k, dz;
   const void *n;
 };
@@ -82,11 +88,13 @@ __device__ __forceinline__ double2 pit_coef(const PitObj &o, double2 v) {
 }
 
 // C[j][i] = (dz/2) * (coef(n[r, j]) + coef(n[r, j+1])) / 2, r = i - empty_px
-// (base_simulation_space.py:315-383), slice-major (L, N).
+// (base_simulation_space.py:315-383), slice-major (L, N); with flip_conj the
+// z-flipped conjugate the reference's adjoint mode builds (full_pint.py:154-157).
 __global__ void pit_object_kernel(const PitObj o, float2 *__restrict__ C) {
   const size_t total = (size_t)o.L * o.N;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-    const int j = (int)(e / o.N), i = (int)(e % o.N);
+    const int jo = (int)(e / o.N), i = (int)(e % o.N);
+    const int j = o.flip_conj ? o.L - 1 - jo : jo;
     const int r = i - o.empty_px;
     double2 c = z2(0.0, 0.0);
     if (r >= 0 && r < o.n_obj) {
@@ -98,13 +106,14 @@ __global__ void pit_object_kernel(const PitObj o, float2 *__restrict__ C) {
       };
       c = zscale(zadd(pit_coef(o, ld(j)), pit_coef(o, ld(j + 1))), 0.25 * o.dz);
     }
-    C[e] = to_f2(c);
+    C[e] = to_f2(o.flip_conj ? zconj(c) : c);
   }
 }
 
 // ------------------------------------------------------------------ matvec
 // out = M v for the active probes: slice j gets
-// (A - C_j) v_j - (B + C_j) v_{j-1}, A = I - K, B = I + K (_pint_utils.py:27-54).
+// (A - C_j) v_j - (B + C_j) v_{j-1}, A = I - K, B = I + K (_pint_utils.py:27-54;
+// the adjoint system passes K^H and the flipped conjugate C).
 __global__ void pit_matvec_kernel(const PitK K, int L, int P, const float2 *__restrict__ C,
                                   const float2 *__restrict__ v, float2 *__restrict__ out, const int *active) {
   const int N = K.N;
@@ -480,9 +489,13 @@ static PitWork pit_layout(char *base, int N, int L, int P, int m) {
   return w;
 }
 
-static PitK pit_k(const tp_cn2d_op *op) {
-  auto f = [](const double v[2]) { return make_float2((float)v[0], (float)v[1]); };
-  return PitK{op->n, f(op->k_off), f(op->k_diag), f(op->k_d0), f(op->k_dn), f(op->k_01), f(op->k_nm)};
+// K of the operator, or its conjugate transpose (conj_t): K^H[i, i-1] =
+// conj(K[i-1, i]) and K^H[i, i+1] = conj(K[i+1, i]).
+static PitK pit_k(const tp_cn2d_op *op, bool conj_t = false) {
+  auto f = [&](const double v[2]) { return make_float2((float)v[0], (float)(conj_t ? -v[1] : v[1])); };
+  const int N = op->n;
+  if (!conj_t) return PitK{N, f(op->k_off), f(op->k_diag), f(op->k_d0), f(op->k_dn), N - 1, 0, f(op->k_nm), f(op->k_01)};
+  return PitK{N, f(op->k_off), f(op->k_diag), f(op->k_d0), f(op->k_dn), 1, N - 2, f(op->k_01), f(op->k_nm)};
 }
 static PitKd pit_kd(const tp_cn2d_op *op) {
   auto f = [](const double v[2]) { return make_double2(v[0], v[1]); };
@@ -498,8 +511,9 @@ static int pit_grid(size_t total) {
 // and the batched Gram-Schmidt kernels, over all probes.
 class PitSolver {
  public:
-  PitSolver(const tp_cn2d_op *op, int L, int P, const PitWork &w, cudaStream_t st)
-      : K_(pit_k(op)), kd_(pit_kd(op)), N_(op->n), L_(L), P_(P), n_((size_t)op->n * L), w_(w), st_(st) {
+  PitSolver(const tp_cn2d_op *op, int L, int P, const PitWork &w, cudaStream_t st, bool adjoint = false)
+      : K_(pit_k(op)), KM_(pit_k(op, adjoint)), kd_(pit_kd(op)), N_(op->n), L_(L), P_(P), n_((size_t)op->n * L),
+        w_(w), st_(st) {
     M_ = pit_fft_len(L);
     pl_ = make_fft_plan(M_);
     cpc_ = std::max(1, std::min(16, 4096 / M_));
@@ -557,9 +571,9 @@ class PitSolver {
     zdft_any(false, w_.xh, out);
     return check_cuda(cudaGetLastError(), "pit preconditioner launch");
   }
-  // out = M in
+  // out = M in (M of the forward or the reference's adjoint system)
   int matvec(const float2 *in, float2 *out) {
-    pit_matvec_kernel<<<pit_grid(n_ * P_), kPitThreads, 0, st_>>>(K_, L_, P_, w_.C, in, out, w_.active);
+    pit_matvec_kernel<<<pit_grid(n_ * P_), kPitThreads, 0, st_>>>(KM_, L_, P_, w_.C, in, out, w_.active);
     return check_cuda(cudaGetLastError(), "pit matvec launch");
   }
   // out[p] = ||x[p]||^2 on the host
@@ -591,7 +605,8 @@ class PitSolver {
     return (int)(g < 64 ? g : 64);
   }
 
-  PitK K_;
+  PitK K_;   // the operator's K: right-hand side, preconditioner blocks
+  PitK KM_;  // K of the system matrix: K, or K^H in the adjoint mode
   PitKd kd_;
   int N_, L_, P_, M_ = 0, cpc_ = 1;
   size_t n_, zsmem_ = 0;
@@ -635,10 +650,13 @@ extern "C" int tp_pit_solve(const tp_cn2d_op *op, const void *n_field, int32_t n
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const size_t n = (size_t)N * L;
 
-  PitSolver S(op, L, P, w, st);
+  if (a->mode != TP_MODE_FORWARD && a->mode != TP_MODE_ADJOINT)
+    return set_error(TP_ERR_UNSUPPORTED, "tp_pit_solve: mode %d (FORWARD or ADJOINT)", a->mode);
+  const bool adjoint = a->mode == TP_MODE_ADJOINT;
+  PitSolver S(op, L, P, w, st, adjoint);
   // object contribution (slice-major) and right-hand sides
-  PitObj o{N, op->nz, L, op->n_obj, op->empty_px, op->exact_ref_coeff, op->field_is_delta, n_dtype, op->k, op->dz,
-           n_field};
+  PitObj o{N, op->nz, L, op->n_obj, op->empty_px, op->exact_ref_coeff, op->field_is_delta, n_dtype, adjoint ? 1 : 0,
+           op->k, op->dz, n_field};
   pit_object_kernel<<<pit_grid(n), kPitThreads, 0, st>>>(o, w.C);
   pit_rhs_kernel<<<pit_grid(n * P), kPitThreads, 0, st>>>(S.K_, L, P, static_cast<const float2 *>(a->probes),
                                                            static_cast<const float2 *>(a->rhs), w.b);

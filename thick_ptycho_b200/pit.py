@@ -58,9 +58,13 @@ class PiT2D:
         return self._ws
 
     def solve(self, field: torch.Tensor, probes: Optional[torch.Tensor] = None, rhs: Optional[torch.Tensor] = None,
-              u0: Optional[torch.Tensor] = None, num_probes: Optional[int] = None) -> torch.Tensor:
+              u0: Optional[torch.Tensor] = None, num_probes: Optional[int] = None, mode="forward") -> torch.Tensor:
         """The field at steps 1..L, (P, L, N) complex64; ``u0`` is the initial
-        guess (a warm start, e.g. an earlier solution)."""
+        guess (a warm start, e.g. an earlier solution).  ``mode`` "adjoint"
+        solves the reference's adjoint system (conjugate-transposed blocks,
+        z-flipped conjugate object term, the forward preconditioner)."""
+        if mode not in ("forward", "adjoint"):
+            raise ValueError(f"PiT mode must be 'forward' or 'adjoint' (got {mode!r})")
         field = self.engine._check_field(field)
         P = int(num_probes if num_probes is not None else (probes.shape[0] if probes is not None else rhs.shape[0]))
         for name, t, shp in (("probes", probes, (P, self.N)), ("rhs", rhs, (P, self.L, self.N)),
@@ -73,6 +77,7 @@ class PiT2D:
         resid = (ctypes.c_double * P)()
         a = _native.TpPitArgs()
         a.num_probes, a.restart, a.max_cycles = P, self.restart, self.max_cycles
+        a.mode = _native.MODES[mode]
         a.alpha, a.rtol, a.atol = self.alpha, self.rtol, self.atol
         a.probes, a.rhs, a.u = _ptr(probes), _ptr(rhs), _ptr(u)
         a.iters = ctypes.cast(iters, ctypes.POINTER(ctypes.c_int32))
@@ -89,7 +94,7 @@ class PiT2D:
 
 
 class PWEGpuPiTSolver(PWEGpuSolver):
-    """Drop-in for ``PWEFullPinTSolver`` (forward mode, 2D) on one B200.
+    """Drop-in for ``PWEFullPinTSolver`` (2D; modes "forward" and "adjoint") on one B200.
 
     Same constructor arguments (``alpha``, ``atol``) and ``solve`` /
     ``_solve_single_probe`` results; ``gmres_iterations`` holds the Arnoldi
@@ -98,8 +103,8 @@ class PWEGpuPiTSolver(PWEGpuSolver):
     complex128 (``full_pint.py:250``), whose solution then sits ~1e-6 from the
     exact one; stopping ten times tighter keeps this complex64 solve within
     1e-5 of both.  Like the reference's per-mode
-    ``u0_cache``, the last solution warm-starts the next solve for the same
-    ``n`` object (per probe here: the probes are solved together; the
+    ``u0_cache``, the last solution of a mode warm-starts that mode's next
+    solve for the same ``n`` object (per probe here: the probes are solved together; the
     reference keeps the preconditioned unknown, this keeps u itself).
     """
 
@@ -113,7 +118,7 @@ class PWEGpuPiTSolver(PWEGpuSolver):
             raise NotImplementedError("the GPU PiT solver does not take exact test boundary data")
         self.alpha, self.atol = float(alpha), float(atol)
         self.pit = PiT2D(self.engine, alpha=alpha, atol=atol, rtol=rtol, restart=restart)
-        self._warm = None  # (n object, u)
+        self._warm = {}  # mode -> (n object, u)
         self.gmres_iterations = None
 
     def _rhs_rows(self, rhs_block) -> np.ndarray:
@@ -124,23 +129,29 @@ class PWEGpuPiTSolver(PWEGpuSolver):
             rb = rb.reshape(self.block_size, self.nz - 1, order="F")
         return np.ascontiguousarray(rb.reshape(self.block_size, self.nz - 1).T)
 
-    def _pit(self, n, probes_dev, rhs=None):
+    def _pit(self, n, probes_dev, rhs=None, mode="forward"):
         if n is None:
             n = self.simulation_space.refractive_index_empty
         field = self._field_device(n)
         P = probes_dev.shape[0] if probes_dev is not None else rhs.shape[0]
         u0 = None
-        if self._warm is not None and self._warm[0] is n and tuple(self._warm[1].shape)[0] == P:
-            u0 = self._warm[1]
-        u = self.pit.solve(field, probes=probes_dev, rhs=rhs, u0=u0, num_probes=P)
-        self._warm = (n, u)
+        warm = self._warm.get(mode)
+        if warm is not None and warm[0] is n and tuple(warm[1].shape)[0] == P:
+            u0 = warm[1]
+        u = self.pit.solve(field, probes=probes_dev, rhs=rhs, u0=u0, num_probes=P, mode=mode)
+        self._warm[mode] = (n, u)
         self.gmres_iterations = self.pit.iters
         return u
 
+    @staticmethod
+    def _check_mode(mode):
+        if mode not in ("forward", "adjoint"):
+            raise NotImplementedError(f"the PiT solver supports modes 'forward' and 'adjoint' (got {mode!r})")
+
     def solve(self, n=None, mode="forward", rhs_block=None, probes=None, **kwargs) -> np.ndarray:
-        """All probes, shape (proj, angle, probes, N, nz) complex128 (``full_pint.py:179-275``)."""
-        if mode != "forward":
-            raise NotImplementedError("the GPU PiT solver covers the forward mode")
+        """All probes, shape (proj, angle, probes, N, nz) complex128 (``full_pint.py:179-275``);
+        in mode "adjoint" the reference's adjoint system (``full_pint.py:140-166``)."""
+        self._check_mode(mode)
         if self.num_projections != 1:
             raise NotImplementedError("the GPU PiT solver covers one projection")
         count = self.num_angles * self.num_probes
@@ -152,7 +163,7 @@ class PWEGpuPiTSolver(PWEGpuSolver):
             rhs = torch.from_numpy(np.ascontiguousarray(np.broadcast_to(rows, (count, self.nz - 1, self.block_size)))
                                    .astype(np.complex64)).to(self.device)
             pr_in = None
-        u = self._pit(n, pr_in, rhs)
+        u = self._pit(n, pr_in, rhs, mode)
         full = torch.cat([pr[:, None, :], u], dim=1).permute(0, 2, 1)
         out = np.zeros((self.num_projections, self.num_angles, self.num_probes, *self.effective_shape), dtype=complex)
         out[0] = full.cpu().numpy().astype(np.complex128).reshape(self.num_angles, self.num_probes,
@@ -161,13 +172,13 @@ class PWEGpuPiTSolver(PWEGpuSolver):
 
     def _solve_single_probe(self, scan_idx=0, proj_idx=0, probe=None, n=None, mode="forward", rhs_block=None):
         """One probe, shape (N, nz) (``full_pint.py:179-275``): with ``rhs_block``
-        it replaces b (the reference's behaviour), else b = [B u_0, 0, …]."""
-        if mode != "forward":
-            raise NotImplementedError("the GPU PiT solver covers the forward mode")
+        it replaces b (the reference's behaviour), else b = [B u_0, 0, …] (the
+        forward B in both modes, as the reference's ``probe_contribution``)."""
+        self._check_mode(mode)
         pr = self._probes_device(probe if probe is not None else np.zeros(self.block_size), 1)
         rhs = None
         if rhs_block is not None:
             rhs = torch.from_numpy(self._rhs_rows(rhs_block)[None].astype(np.complex64)).to(self.device)
-        u = self._pit(n, None if rhs is not None else pr, rhs)
+        u = self._pit(n, None if rhs is not None else pr, rhs, mode)
         full = torch.cat([pr[:, None, :], u], dim=1)[0].T
         return full.cpu().numpy().astype(np.complex128)
