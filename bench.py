@@ -42,8 +42,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "probe·slice solves/s fwd+adj (2D CN, complex64, exact adjoint + fused gradient)"
-REF_BUDGET_S = 150.0    # wall-time target of a whole `--impl reference` run
-REF_DEADLINE_S = 240.0  # hard limit: the arm prints its line from the steps finished by then
+REF_BUDGET_S = 120.0    # wall-time target of a whole `--impl reference` run
+REF_DEADLINE_S = 200.0  # hard limit: the arm prints its line from the steps finished by then
 REF_MAX_WORKERS = 32    # worker processes of the reference arm (one thread each)
 # DRAM bytes (read + write) of one exact-adjoint march launch at N = 2048, nz = 1024, 512
 # probes: an ncu capture of the same kernel at nz = 128 (127 slices, 512 probes) measured
@@ -291,10 +291,12 @@ def run_reference(a):
         def left():
             return REF_DEADLINE_S - (time.perf_counter() - t_start)
 
-        calib = rate(probe_s, left())  # also starts the workers
+        t_pool = time.perf_counter() - t_start
+        calib0 = rate(probe_s, left())  # also starts the workers
         calib = rate(probe_s, left())
         S = max(8, min(L, int(probe_s * budget / max(calib[3], 1e-3))))
         done = 0
+        walls = []
         for i in range(a.warmup + a.steps):
             # stop when the next step would not finish before the deadline
             if left() < 1.5 * (calib[3] * S / probe_s) + 5.0:
@@ -303,6 +305,7 @@ def run_reference(a):
                 v, tf, tp, wall = rate(S, left())
             except mp.TimeoutError:
                 break
+            walls.append(round(wall, 2))
             if i >= a.warmup:
                 vals.append(v)
                 info = (tf, tp, wall)
@@ -324,6 +327,8 @@ def run_reference(a):
                                     f"step wall {info[2]:.2f} s)")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": time.perf_counter() - t_start,
+        "timing_s": {"pool_start": round(t_pool, 2), "calibration": [round(calib0[3], 2), round(calib[3], 2)],
+                     "slices_per_step": S, "step_walls": walls},
     }
     print(json.dumps(line), flush=True)
 

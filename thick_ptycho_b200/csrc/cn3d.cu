@@ -1012,13 +1012,20 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
       return TP_OK;
     };
     rc = record();
-    if (rc == TP_OK) rc = check_cuda(cudaGraphLaunch(ge, st), "cudaGraphLaunch (3D march)");
-    // an executable graph still running is freed when it completes
+    if (rc == TP_OK) {
+      rc = check_cuda(cudaGraphLaunch(ge, st), "cudaGraphLaunch (3D march)");
+      // an executable graph still running is freed when it completes
+      cudaGraphExecDestroy(ge);
+      cudaGraphDestroy(g);
+      if (rc != TP_OK) return rc;
+      if (stats) c3_flag_kernel<<<1, 1, 0, st>>>(stats, 1);
+      return check_cuda(cudaGetLastError(), "tp_cn3d_march graph");
+    }
+    // the graph could not be recorded (nothing of it ran): run step by step
+    // below; stats[4] = 0 reports it
     if (ge) cudaGraphExecDestroy(ge);
     cudaGraphDestroy(g);
-    if (rc != TP_OK) return rc;
-    if (stats) c3_flag_kernel<<<1, 1, 0, st>>>(stats, 1);
-    return check_cuda(cudaGetLastError(), "tp_cn3d_march graph");
+    (void)cudaGetLastError();
   }
 
   // ---- step by step on the caller's stream
