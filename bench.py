@@ -239,6 +239,17 @@ def cpu_rate(N, nz, P, cores, probes_per_worker, slices=None, pool=None):
     return P * L / total, t_fact, t_probe, wall
 
 
+def _cpu_quota():
+    """The cgroup CPU limit of this process ("quota period"), if readable."""
+    for path in ("/sys/fs/cgroup/cpu.max", "/sys/fs/cgroup/cpu/cpu.cfs_quota_us"):
+        try:
+            with open(path) as f:
+                return f.read().strip()
+        except OSError:
+            continue
+    return None
+
+
 def ref_workers():
     """Worker processes of the reference arm: the host threads this process may
     run on (its affinity mask, not the machine's core count), at most
@@ -305,12 +316,14 @@ def run_reference(a):
                 v, tf, tp, wall = rate(S, left())
             except mp.TimeoutError:
                 break
-            walls.append(round(wall, 2))
+            walls.append((round(time.perf_counter() - t_start - wall, 2), round(wall, 2)))
             if i >= a.warmup:
                 vals.append(v)
                 info = (tf, tp, wall)
                 done += 1
+        t_loop = time.perf_counter() - t_start
         pool.terminate()
+    t_term = time.perf_counter() - t_start
     if not vals:  # deadline reached during the warm-up: report the calibration sample
         S, info, vals = probe_s, calib[1:], [calib[0]]
     value = statistics.median(vals)
@@ -328,7 +341,8 @@ def run_reference(a):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": time.perf_counter() - t_start,
         "timing_s": {"pool_start": round(t_pool, 2), "calibration": [round(calib0[3], 2), round(calib[3], 2)],
-                     "slices_per_step": S, "step_walls": walls},
+                     "slices_per_step": S, "step_start_and_wall": walls, "loop_end": round(t_loop, 2),
+                     "pool_closed": round(t_term, 2), "cpu_quota": _cpu_quota()},
     }
     print(json.dumps(line), flush=True)
 

@@ -122,9 +122,10 @@ def test_pit_bluestein_lengths_against_oracle(nz):
 def test_pit_adjoint_against_reference_golden(golden, bc):
     """mode "adjoint" (full_pint.py:140-166): the reference's system with
     conjugate-transposed blocks and the z-flipped conjugate object term,
-    right-preconditioned by the forward preconditioner, against its own solve
-    for a flat column-major right-hand side and for a probe (B u_0 with the
-    forward B), and against the direct solve of that system."""
+    right-preconditioned by the forward preconditioner, for a flat
+    column-major right-hand side and for a probe (B u_0 with the forward B):
+    against the direct solve of that system (1e-5) and against the
+    reference's own GMRES output (within its stopping error, 2e-5)."""
     g = golden("pit2d_adjoint")
     N, nz = int(g["nx"]), int(g["nz"])
     L = nz - 1
@@ -132,15 +133,21 @@ def test_pit_adjoint_against_reference_golden(golden, bc):
     rhs = g["rhs_block"]
     n = g["n"]
     u = s._solve_single_probe(n=n, mode="adjoint", rhs_block=rhs.ravel(order="F"), probe=g["probes"][1])
-    assert rel(u, g[f"adj_rhs_{bc}"]) < TOL, rel(u, g[f"adj_rhs_{bc}"])
     co = po.bc_coefficients(float(g["k"]), float(g["dx"]), float(g["dz"]), bc_type=bc)
     A, B = po.step_matrices_1d(N, co, bc, float(g["dz"]))
     C = po.object_contribution(n, float(g["k"]), float(g["dz"]))
     x = po.full_system_solve(A.conj().T.tocsr(), B.conj().T.tocsr(), np.flip(np.conj(C), axis=1), rhs.T.ravel())
-    assert rel(u[:, 1:], x.reshape(L, N).T) < TOL
+    assert rel(u[:, 1:], x.reshape(L, N).T) < TOL, rel(u[:, 1:], x.reshape(L, N).T)
+    # The reference's own adjoint solve stops at a 1e-5 relative residual and
+    # sits 1.15e-5 to 1.3e-5 from the exact solution (measured on these
+    # vectors), so against its output the bound is that error plus this one's.
+    assert rel(u, g[f"adj_rhs_{bc}"]) < 2 * TOL, rel(u, g[f"adj_rhs_{bc}"])
     s2 = PWEGpuPiTSolver(_geo(g, 4), g["probes"][None], bc_type=bc)
     u2 = s2._solve_single_probe(n=n, mode="adjoint", probe=g["probes"][2])
-    assert rel(u2, g[f"adj_probe_{bc}"]) < TOL, rel(u2, g[f"adj_probe_{bc}"])
+    x2 = po.full_system_solve(A.conj().T.tocsr(), B.conj().T.tocsr(), np.flip(np.conj(C), axis=1),
+                              po.pit_rhs(B, g["probes"][2], L))
+    assert rel(u2[:, 1:], x2.reshape(L, N).T) < TOL, rel(u2[:, 1:], x2.reshape(L, N).T)
+    assert rel(u2, g[f"adj_probe_{bc}"]) < 2 * TOL, rel(u2, g[f"adj_probe_{bc}"])
     # the batched solve over every probe in adjoint mode equals the per-probe one
     ub = s2.solve(n=n, mode="adjoint")[0, 0]
     assert rel(ub[2], u2) < TOL

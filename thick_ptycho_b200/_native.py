@@ -11,10 +11,11 @@ import ctypes
 import os
 import threading
 
-from .build_native import LIB
+from .build_native import LIB, LIB_C128
 
 _lock = threading.Lock()
 _lib = None
+_lib_c128 = None
 
 TP_OK = 0
 TP_ERR_TIMEOUT = 4
@@ -264,7 +265,31 @@ def load() -> ctypes.CDLL:
         return lib
 
 
-def check(rc: int, what: str):
+def load_check() -> ctypes.CDLL:
+    """Load libtpcuda_c128.so, the complex128 check build of the 2D
+    Crank–Nicolson entry points (tp_cn2d_*: every complex buffer complex128)."""
+    global _lib_c128
+    if _lib_c128 is not None:
+        return _lib_c128
+    with _lock:
+        if _lib_c128 is not None:
+            return _lib_c128
+        if not os.path.exists(LIB_C128):
+            raise NativeLibraryError(f"{LIB_C128} not found: build it with `python -m thick_ptycho_b200.build_native`")
+        try:
+            lib = ctypes.CDLL(LIB_C128)
+        except OSError as e:  # pragma: no cover - depends on the machine
+            raise NativeLibraryError(f"failed to load {LIB_C128}: {e}") from e
+        for name, res, args in SIGNATURES:
+            fn = getattr(lib, name, None)
+            if fn is not None:
+                fn.restype = res
+                fn.argtypes = args
+        _lib_c128 = lib
+        return lib
+
+
+def check(rc: int, what: str, lib=None):
     if rc != TP_OK:
-        msg = load().tp_last_error_string().decode(errors="replace")
+        msg = (lib or load()).tp_last_error_string().decode(errors="replace")
         raise NativeLibraryError(f"{what} failed (status {rc}): {msg}")

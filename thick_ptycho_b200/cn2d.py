@@ -4,6 +4,9 @@
 of libtpcuda.so (``include/tpcuda.h``) on the current torch CUDA stream.
 Tensors are complex64 on the device except the refractive index, which may
 be complex128 (``n``) or complex64 holding ``n − 1`` (``is_delta=True``).
+With ``check=True`` the geometry runs on the complex128 check build
+(``libtpcuda_c128.so``): the same algorithms with complex128 state, factor
+sets and fields, and every complex tensor complex128.
 """
 
 from __future__ import annotations
@@ -39,10 +42,14 @@ class FactorSet:
 class CN2D:
     """One 2D geometry: N transverse rows, nz nodes (L = nz − 1 steps)."""
 
-    def __init__(self, n, nz, k, dx, dz, bc_type="impedance", empty_px=0, exact_ref_coeff=False, device=None):
+    def __init__(self, n, nz, k, dx, dz, bc_type="impedance", empty_px=0, exact_ref_coeff=False, device=None,
+                 check=False):
         if not torch.cuda.is_available():
             raise _native.NativeLibraryError("CN2D needs a CUDA device (there is no CPU fallback)")
-        self.lib = _native.load()
+        self.check = bool(check)
+        self.lib = _native.load_check() if self.check else _native.load()
+        # complex type of fields, sources, exit waves and gradients
+        self.cdtype = torch.complex128 if self.check else torch.complex64
         self.device = torch.device(device if device is not None else "cuda")
         self.n, self.nz, self.L = int(n), int(nz), int(nz) - 1
         self.k, self.dx, self.dz = float(k), float(dx), float(dz)
@@ -54,7 +61,7 @@ class CN2D:
         self.kop = operator_1d(self.n, co, self.bc_type, self.dz)
         c, m, npad = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
         rc = self.lib.tp_cn2d_layout(self.n, ctypes.byref(c), ctypes.byref(m), ctypes.byref(npad))
-        _native.check(rc, "tp_cn2d_layout")
+        _native.check(rc, "tp_cn2d_layout", self.lib)
         self.chunks, self.rows_per_chunk, self.npad = c.value, m.value, npad.value
         self.factor_bytes = int(self.lib.tp_cn2d_factor_bytes(self.n, self.nz))
 
@@ -92,7 +99,7 @@ class CN2D:
         o = self.op(is_delta)
         rc = self.lib.tp_cn2d_factor(ctypes.byref(o), _ptr(field), dtype, mode_i, _ptr(buf), buf.numel(),
                                      _stream(self.device))
-        _native.check(rc, "tp_cn2d_factor")
+        _native.check(rc, "tp_cn2d_factor", self.lib)
         return FactorSet(mode_i, buf)
 
     def factor_range(self, field: torch.Tensor, mode, slice_begin: int, slice_end: int, out: torch.Tensor,
@@ -106,7 +113,7 @@ class CN2D:
         o = self.op(is_delta)
         rc = self.lib.tp_cn2d_factor_range(ctypes.byref(o), _ptr(field), dtype, mode_i, _ptr(out), out.numel(),
                                            int(slice_begin), int(slice_end), _stream(self.device))
-        _native.check(rc, "tp_cn2d_factor_range")
+        _native.check(rc, "tp_cn2d_factor_range", self.lib)
         return FactorSet(mode_i, out)
 
     # -------------------------------------------------------------- march
@@ -131,7 +138,8 @@ class CN2D:
         ufwd_base: int = 0,
         store_sums: bool = False,
     ):
-        """One batched march; every tensor is complex64, contiguous, on device.
+        """One batched march; every tensor is complex64 (complex128 in the
+        check build), contiguous, on device.
 
         ``u_store`` is (P, S, Npad) with S slices per probe: the state after
         step t goes to index ``t − store_base`` (or ``t / store_every`` when
@@ -160,8 +168,8 @@ class CN2D:
         for name, (t, shp) in shapes.items():
             if t is None:
                 continue
-            if t.dtype != torch.complex64 or not t.is_contiguous() or not t.is_cuda:
-                raise TypeError(f"{name} must be a contiguous complex64 CUDA tensor")
+            if t.dtype != self.cdtype or not t.is_contiguous() or not t.is_cuda:
+                raise TypeError(f"{name} must be a contiguous {self.cdtype} CUDA tensor")
             if shp is not None and tuple(t.shape) != shp:
                 raise ValueError(f"{name} has shape {tuple(t.shape)}, expected {shp}")
         if u_fwd is not None and (u_fwd.dim() != 3 or u_fwd.shape[2] != self.npad or u_fwd.shape[0] < P):
@@ -181,20 +189,20 @@ class CN2D:
         a.store_sums = 1 if store_sums else 0
         o = self.op()
         rc = self.lib.tp_cn2d_march(ctypes.byref(o), _ptr(fs.buf), ctypes.byref(a), _stream(self.device))
-        _native.check(rc, "tp_cn2d_march")
+        _native.check(rc, "tp_cn2d_march", self.lib)
 
     # ------------------------------------------------------------ helpers
     def new_store(self, num_probes: int, slices: Optional[int] = None) -> torch.Tensor:
         s = self.nz if slices is None else int(slices)
-        return torch.empty((num_probes, s, self.npad), dtype=torch.complex64, device=self.device)
+        return torch.empty((num_probes, s, self.npad), dtype=self.cdtype, device=self.device)
 
     def unchunk(self, u_store: torch.Tensor) -> torch.Tensor:
         """Chunked (P, nz, Npad) → reference layout (P, N, nz)."""
         P = u_store.shape[0]
-        out = torch.empty((P, self.n, self.nz), dtype=torch.complex64, device=self.device)
+        out = torch.empty((P, self.n, self.nz), dtype=self.cdtype, device=self.device)
         o = self.op()
         rc = self.lib.tp_cn2d_unchunk(ctypes.byref(o), P, _ptr(u_store), _ptr(out), _stream(self.device))
-        _native.check(rc, "tp_cn2d_unchunk")
+        _native.check(rc, "tp_cn2d_unchunk", self.lib)
         return out
 
     def chunk_index(self) -> torch.Tensor:
@@ -214,18 +222,18 @@ class CN2D:
         return x.index_select(-1, self.chunk_index())
 
     def new_grad_buffer(self) -> torch.Tensor:
-        return torch.zeros((self.L, self.npad), dtype=torch.complex64, device=self.device)
+        return torch.zeros((self.L, self.npad), dtype=self.cdtype, device=self.device)
 
     def grad_to_n(self, grad_c: torch.Tensor, field: Optional[torch.Tensor] = None, is_delta=False) -> torch.Tensor:
         """Σ_p λ conj(u_s + u_{s−1}) (L, Npad chunked) → torch-convention gradient on n (n_obj, nz)."""
-        out = torch.empty((self.n_obj, self.nz), dtype=torch.complex64, device=self.device)
+        out = torch.empty((self.n_obj, self.nz), dtype=self.cdtype, device=self.device)
         dtype = _native.C128
         if field is not None:
             field = self._check_field(field)
             dtype = _native.C128 if field.dtype == torch.complex128 else _native.C64
         o = self.op(is_delta)
         rc = self.lib.tp_cn2d_grad_to_n(ctypes.byref(o), _ptr(grad_c), _ptr(field), dtype, _ptr(out), _stream(self.device))
-        _native.check(rc, "tp_cn2d_grad_to_n")
+        _native.check(rc, "tp_cn2d_grad_to_n", self.lib)
         return out
 
     def grad_to_n_range(self, grad_c: torch.Tensor, out: torch.Tensor, node_begin: int, node_end: int,
@@ -238,10 +246,10 @@ class CN2D:
         o = self.op(is_delta)
         rc = self.lib.tp_cn2d_grad_to_n_range(ctypes.byref(o), _ptr(grad_c), _ptr(field), dtype, _ptr(out),
                                               int(node_begin), int(node_end), _stream(self.device))
-        _native.check(rc, "tp_cn2d_grad_to_n_range")
+        _native.check(rc, "tp_cn2d_grad_to_n_range", self.lib)
         return out
 
     def device_status(self):
         code = ctypes.c_int32()
         rc = self.lib.tp_device_status(_stream(self.device), ctypes.byref(code))
-        _native.check(rc, "tp_device_status")
+        _native.check(rc, "tp_device_status", self.lib)

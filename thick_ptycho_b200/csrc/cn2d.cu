@@ -25,7 +25,7 @@
 // factors, the two spike vectors, the PCR multipliers) is probe-independent;
 // it is computed once per slice in fp64 by cn2d_factor_kernel and streamed
 // into shared memory with bulk (TMA) copies, so each probe pays only for
-// right-hand-side work.  Data layout of one slice of the factor set (float2
+// right-hand-side work.  Data layout of one slice of the factor set (cx
 // [rows][32 lanes], row i of lane k is matrix row k*M + i):
 //   QD  [M][32]  diagonal of P_s
 //   LF  [M][32]  interior forward multipliers (row 0 unused)
@@ -88,7 +88,7 @@ int team_spike_rows(const tp_cn2d_op *op, int M) {
   if (disc <= 0.0) return M - 1;
   const double rho = (d0 - sqrt(disc)) / (2.0 * b);
   if (!(rho > 0.0) || rho >= 0.5) return M - 1;
-  int t = (int)ceil(log(1e-9) / log(rho)) + 1;
+  int t = (int)ceil(log(kSpikeDrop) / log(rho)) + 1;
   if (t < 1) t = 1;
   if (t > M - 1) t = M - 1;
   return t;
@@ -151,8 +151,8 @@ __global__ void __launch_bounds__(128) cn2d_factor_kernel(const FactorParams f) 
   const int c = threadIdx.x;
   const int sl = f.sl0 + blockIdx.x;
   const int M = f.M, C = f.C;
-  float2 *base = reinterpret_cast<float2 *>(f.factors + (size_t)sl * f.slice_bytes);
-  float2 *QD = base, *LF = base + M * C, *EP = base + 2 * M * C, *V = base + 3 * M * C, *W = base + 4 * M * C,
+  cx *base = reinterpret_cast<cx *>(f.factors + (size_t)sl * f.slice_bytes);
+  cx *QD = base, *LF = base + M * C, *EP = base + 2 * M * C, *V = base + 3 * M * C, *W = base + 4 * M * C,
          *LR = base + 5 * M * C;
 
   double2 pl[kMaxRowsPerLane], msl[kMaxRowsPerLane], fv[kMaxRowsPerLane];
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(128) cn2d_factor_kernel(const FactorParams f) 
   for (int i = 0; i < M; ++i) {
     const int g = g0 + i;
     const double2 pd = p_diag(f, g, sl);
-    QD[i * C + c] = to_f2(pd);
+    QD[i * C + c] = to_cx(pd);
     const double2 md = z2(1.0 - pd.x, -pd.y);
     const double2 msub = zneg(p_sub(f, g));
     const double2 msup = zneg(p_sup(f, g));
@@ -177,8 +177,8 @@ __global__ void __launch_bounds__(128) cn2d_factor_kernel(const FactorParams f) 
         p = zsub(md, zmul(l, msup_prev));
         fvv = zneg(zmul(l, fvv));
       }
-      LF[i * C + c] = to_f2(l);
-      EP[i * C + c] = to_f2(zdiv(z2(1.0 - p.x, -p.y), p));  // 1/p - 1
+      LF[i * C + c] = to_cx(l);
+      EP[i * C + c] = to_cx(zdiv(z2(1.0 - p.x, -p.y), p));  // 1/p - 1
       pl[i] = p;
       msl[i] = msup;
       fv[i] = fvv;
@@ -188,28 +188,28 @@ __global__ void __launch_bounds__(128) cn2d_factor_kernel(const FactorParams f) 
       me_d = md;
       me_a = msub;
       me_c = msup;
-      LF[i * C + c] = make_float2(0.f, 0.f);
-      EP[i * C + c] = make_float2(0.f, 0.f);
-      V[i * C + c] = make_float2(0.f, 0.f);
-      W[i * C + c] = make_float2(0.f, 0.f);
+      LF[i * C + c] = czero();
+      EP[i * C + c] = czero();
+      V[i * C + c] = czero();
+      W[i * C + c] = czero();
     }
   }
   double2 v_last, w_last, v_first, w_first;
   bool trunc_bad = false;
-  const double thr = 1e-9;
+  const double thr = kSpikeDrop;
   if (M >= 2) {
     double2 v = zdiv(fv[M - 2], pl[M - 2]);
     double2 w = zdiv(zneg(msl[M - 2]), pl[M - 2]);
-    V[(M - 2) * C + c] = to_f2(v);
-    W[(M - 2) * C + c] = to_f2(w);
+    V[(M - 2) * C + c] = to_cx(v);
+    W[(M - 2) * C + c] = to_cx(w);
     if (M - 2 >= f.trunc && hypot(v.x, v.y) > thr) trunc_bad = true;
     v_last = v;
     w_last = w;
     for (int i = M - 3; i >= 0; --i) {
       v = zdiv(zsub(fv[i], zmul(msl[i], v)), pl[i]);
       w = zdiv(zneg(zmul(msl[i], w)), pl[i]);
-      V[i * C + c] = to_f2(v);
-      W[i * C + c] = to_f2(w);
+      V[i * C + c] = to_cx(v);
+      W[i * C + c] = to_cx(w);
       if (i >= f.trunc && hypot(v.x, v.y) > thr) trunc_bad = true;
       if (i < M - 1 - f.trunc && hypot(w.x, w.y) > thr) trunc_bad = true;
     }
@@ -231,8 +231,8 @@ __global__ void __launch_bounds__(128) cn2d_factor_kernel(const FactorParams f) 
   double2 ra = zmul(me_a, v_last);
   double2 rd = zadd(me_d, zadd(zmul(me_a, w_last), c < C - 1 ? zmul(me_c, vf_n) : z2(0, 0)));
   double2 rc = c < C - 1 ? zmul(me_c, wf_n) : z2(0, 0);
-  LR[0 * C + c] = to_f2(me_a);
-  LR[1 * C + c] = to_f2(c < C - 1 ? me_c : z2(0, 0));
+  LR[0 * C + c] = to_cx(me_a);
+  LR[1 * C + c] = to_cx(c < C - 1 ? me_c : z2(0, 0));
   double amax = 0.0;  // largest PCR coefficient of this chunk
   for (int l = 0; l < f.levels; ++l) {
     const int s = 1 << l;
@@ -252,13 +252,13 @@ __global__ void __launch_bounds__(128) cn2d_factor_kernel(const FactorParams f) 
     rd = zadd(rd, zadd(zmul(al, rc_m), zmul(ga, ra_p)));
     ra = nra;
     rc = nrc;
-    LR[rec_alpha(f.levels, l) * C + c] = to_f2(al);
-    LR[rec_gamma(f.levels, l) * C + c] = to_f2(ga);
+    LR[rec_alpha(f.levels, l) * C + c] = to_cx(al);
+    LR[rec_gamma(f.levels, l) * C + c] = to_cx(ga);
     amax = fmax(amax, fmax(hypot(al.x, al.y), hypot(ga.x, ga.y)));
   }
   // non-negative floats order like their bit patterns
   if (f.coupling != nullptr) atomicMax(f.coupling, __float_as_uint((float)fmin(amax, 3.0e38)));
-  LR[rec_rde(f.levels) * C + c] = to_f2(zdiv(z2(1.0 - rd.x, -rd.y), rd));
+  LR[rec_rde(f.levels) * C + c] = to_cx(zdiv(z2(1.0 - rd.x, -rd.y), rd));
 }
 
 // --------------------------------------------------------------------------
@@ -270,18 +270,18 @@ __global__ void __launch_bounds__(128) cn2d_factor_kernel(const FactorParams f) 
 
 // U <- (I + P_s) U with P's boundary-row specials.
 template <int M, bool ALIGNED>
-__device__ __forceinline__ void cn2d_rhs(float2 (&U)[M], const float2 *__restrict__ QD, int lane,
+__device__ __forceinline__ void cn2d_rhs(cx (&U)[M], const cx *__restrict__ QD, int lane,
                                          const MarchParams &p) {
-  const float2 zero = make_float2(0.f, 0.f);
-  const float2 left = shfl_up2(U[M - 1], 1);
-  const float2 right = shfl_down2(U[0], 1);
-  float2 prev = (lane == 0) ? zero : left;
-  const float2 rlast = (lane == 31) ? zero : right;
+  const cx zero = czero();
+  const cx left = shfl_up2(U[M - 1], 1);
+  const cx right = shfl_down2(U[0], 1);
+  cx prev = (lane == 0) ? zero : left;
+  const cx rlast = (lane == 31) ? zero : right;
 #pragma unroll
   for (int i = 0; i < M; ++i) {
-    const float2 cur = U[i];
-    const float2 nxt = (i < M - 1) ? U[(i + 1) < M ? i + 1 : i] : rlast;
-    float2 r = cfma(QD[i * 32 + lane], cur, cur);
+    const cx cur = U[i];
+    const cx nxt = (i < M - 1) ? U[(i + 1) < M ? i + 1 : i] : rlast;
+    cx r = cfma(QD[i * 32 + lane], cur, cur);
     if constexpr (ALIGNED) {
       r = cfma(p.sp.p_o, cadd(prev, nxt), r);
       if (i == 0 && lane == 0) r = cfma(p.sp.d_sup0, nxt, r);
@@ -290,8 +290,8 @@ __device__ __forceinline__ void cn2d_rhs(float2 (&U)[M], const float2 *__restric
       if (i == M - 1 && lane == 31) r = cfma(p.sp.d_subN1, prev, r);
     } else {
       const int g = lane * M + i;
-      const float2 psub = (g == p.N - 1) ? p.sp.subN1 : ((g == 1) ? p.sp.sub1 : p.sp.p_o);
-      const float2 psup = (g == 0) ? p.sp.sup0 : ((g == p.N - 2) ? p.sp.supN2 : p.sp.p_o);
+      const cx psub = (g == p.N - 1) ? p.sp.subN1 : ((g == 1) ? p.sp.sub1 : p.sp.p_o);
+      const cx psup = (g == 0) ? p.sp.sup0 : ((g == p.N - 2) ? p.sp.supN2 : p.sp.p_o);
       r = cfma(psub, prev, r);
       r = cfma(psup, nxt, r);
       if (g >= p.N) r = zero;
@@ -303,32 +303,32 @@ __device__ __forceinline__ void cn2d_rhs(float2 (&U)[M], const float2 *__restric
 
 // U <- M_s^{-1} U (partitioned solve with the slice's factor set F).
 template <int M, bool ALIGNED>
-__device__ __forceinline__ void cn2d_solve(float2 (&U)[M], const float2 *__restrict__ F, int lane,
+__device__ __forceinline__ void cn2d_solve(cx (&U)[M], const cx *__restrict__ F, int lane,
                                            const MarchParams &p) {
-  const float2 *LF = F + M * 32, *EP = F + 2 * M * 32, *V = F + 3 * M * 32, *W = F + 4 * M * 32,
+  const cx *LF = F + M * 32, *EP = F + 2 * M * 32, *V = F + 3 * M * 32, *W = F + 4 * M * 32,
                *LR = F + 5 * M * 32;
   if constexpr (M >= 2) {
 #pragma unroll
     for (int i = 1; i <= M - 2; ++i) U[i] = cfnma(LF[i * 32 + lane], U[i - 1], U[i]);
     {
-      const float2 t = U[M - 2];
+      const cx t = U[M - 2];
       U[M - 2] = cfma(t, EP[(M - 2) * 32 + lane], t);
     }
-    const float2 m_o = make_float2(-p.sp.p_o.x, -p.sp.p_o.y);
+    const cx m_o = mkcx(-p.sp.p_o.x, -p.sp.p_o.y);
 #pragma unroll
     for (int i = M - 3; i >= 0; --i) {
-      float2 msup = m_o;
-      if (i == 0 && lane == 0) msup = make_float2(-p.sp.sup0.x, -p.sp.sup0.y);
+      cx msup = m_o;
+      if (i == 0 && lane == 0) msup = mkcx(-p.sp.sup0.x, -p.sp.sup0.y);
       if constexpr (!ALIGNED) {
-        if (lane * M + i == p.N - 2) msup = make_float2(-p.sp.supN2.x, -p.sp.supN2.y);
+        if (lane * M + i == p.N - 2) msup = mkcx(-p.sp.supN2.x, -p.sp.supN2.y);
       }
-      const float2 t = cfnma(msup, U[i + 1], U[i]);
+      const cx t = cfnma(msup, U[i + 1], U[i]);
       U[i] = cfma(t, EP[i * 32 + lane], t);
     }
   }
-  float2 rho;
+  cx rho;
   if constexpr (M >= 2) {
-    const float2 y0n = shfl_down2(U[0], 1);
+    const cx y0n = shfl_down2(U[0], 1);
     rho = cfnma(LR[kRecMA * 32 + lane], U[M - 2], U[M - 1]);
     rho = cfnma(LR[kRecMC * 32 + lane], y0n, rho);
   } else {
@@ -337,12 +337,12 @@ __device__ __forceinline__ void cn2d_solve(float2 (&U)[M], const float2 *__restr
 #pragma unroll
   for (int l = 0; l < 5; ++l) {
     const int s = 1 << l;
-    const float2 up = shfl_up2(rho, s), dn = shfl_down2(rho, s);
-    const float2 r2 = cfma(LR[(kRecAlpha + l) * 32 + lane], up, rho);
+    const cx up = shfl_up2(rho, s), dn = shfl_down2(rho, s);
+    const cx r2 = cfma(LR[(kRecAlpha + l) * 32 + lane], up, rho);
     rho = cfma(LR[(kRecGamma + l) * 32 + lane], dn, r2);
   }
-  const float2 x = cfma(rho, LR[kRecRDE * 32 + lane], rho);
-  const float2 xp = shfl_up2(x, 1);
+  const cx x = cfma(rho, LR[kRecRDE * 32 + lane], rho);
+  const cx xp = shfl_up2(x, 1);
   if constexpr (M >= 2) {
 #pragma unroll
     for (int i = 0; i <= M - 2; ++i) U[i] = cfma(W[i * 32 + lane], x, cfma(V[i * 32 + lane], xp, U[i]));
@@ -351,7 +351,7 @@ __device__ __forceinline__ void cn2d_solve(float2 (&U)[M], const float2 *__restr
 }
 
 template <int M>
-__device__ __forceinline__ void add_natural(float2 (&U)[M], const float2 *__restrict__ src, int lane, int N) {
+__device__ __forceinline__ void add_natural(cx (&U)[M], const cx *__restrict__ src, int lane, int N) {
 #pragma unroll
   for (int i = 0; i < M; ++i) {
     const int g = lane * M + i;
@@ -366,11 +366,11 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
   const int probe = blockIdx.x * kMarchWarps + warp;
   const bool active = probe < p.P;
   const size_t sb = p.slice_bytes;
-  float2 *bufs = reinterpret_cast<float2 *>(smem);
-  float2 *gacc = reinterpret_cast<float2 *>(smem + 2 * sb);  // [2][M][33]
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + 2 * sb + 2 * M * 33 * sizeof(float2));
+  cx *bufs = reinterpret_cast<cx *>(smem);
+  cx *gacc = reinterpret_cast<cx *>(smem + 2 * sb);  // [2][M][33]
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + 2 * sb + 2 * M * 33 * sizeof(cx));
   const bool do_grad = LAGGED && (p.grad_c != nullptr);
-  const size_t slice_f2 = sb / sizeof(float2);
+  const size_t slice_f2 = sb / sizeof(cx);
 
   if (tid == 0) {
     mbar_init(&mbar[0], 1);
@@ -378,7 +378,7 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
     fence_mbar_init();
   }
   if (do_grad)
-    for (int e = tid; e < 2 * M * 33; e += blockDim.x) gacc[e] = make_float2(0.f, 0.f);
+    for (int e = tid; e < 2 * M * 33; e += blockDim.x) gacc[e] = czero();
   __syncthreads();
 
   auto slice_of = [&](int t) { return p.backward ? (p.L + 1 - t) : t; };
@@ -387,18 +387,18 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
     bulk_g2s(bufs + slice_f2, p.factors + (size_t)(slice_of(p.t0) - 1) * sb, (uint32_t)sb, &mbar[1]);
   }
 
-  float2 U[M];
+  cx U[M];
 #pragma unroll
-  for (int i = 0; i < M; ++i) U[i] = make_float2(0.f, 0.f);
+  for (int i = 0; i < M; ++i) U[i] = czero();
   if (active && p.state_in != nullptr) {
-    const float2 *src = p.state_in + (size_t)probe * p.Npad;
+    const cx *src = p.state_in + (size_t)probe * p.Npad;
 #pragma unroll
     for (int i = 0; i < M; ++i) U[i] = src[i * 32 + lane];
   } else if (active && p.probes != nullptr && p.t0 == 1) {
     add_natural<M>(U, p.probes + (size_t)probe * p.N, lane, p.N);
   }
   if (active && p.u_store != nullptr && store_index(p, p.t0 - 1) >= 0) {
-    float2 *dst = p.u_store + ((size_t)probe * p.store_slices + store_index(p, p.t0 - 1)) * p.Npad;
+    cx *dst = p.u_store + ((size_t)probe * p.store_slices + store_index(p, p.t0 - 1)) * p.Npad;
 #pragma unroll
     for (int i = 0; i < M; ++i) dst[i * 32 + lane] = U[i];
   }
@@ -423,7 +423,7 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
       bulk_g2s(bufs + (cb ^ 1) * slice_f2, p.factors + (size_t)(slice_of(t + 1) - 1) * sb, (uint32_t)sb,
                &mbar[cb ^ 1]);
     }
-    const float2 *F = bufs + cb * slice_f2;
+    const cx *F = bufs + cb * slice_f2;
     if (active) {
       if constexpr (!LAGGED) cn2d_rhs<M, ALIGNED>(U, F, lane, p);
       if (p.src_shared != nullptr) add_natural<M>(U, p.src_shared + (size_t)(t - 1) * p.N, lane, p.N);
@@ -434,12 +434,12 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
       if (t == 1 && p.src_exit != nullptr) add_natural<M>(U, p.src_exit + (size_t)probe * p.N, lane, p.N);
       cn2d_solve<M, ALIGNED>(U, F, lane, p);
       if (p.u_store != nullptr && store_index(p, t) >= 0) {
-        float2 *dst = p.u_store + ((size_t)probe * p.store_slices + store_index(p, t)) * p.Npad;
+        cx *dst = p.u_store + ((size_t)probe * p.store_slices + store_index(p, t)) * p.Npad;
 #pragma unroll
         for (int i = 0; i < M; ++i) dst[i * 32 + lane] = U[i];
       }
       if (t == p.L && p.exit_out != nullptr) {
-        float2 *dst = p.exit_out + (size_t)probe * p.N;
+        cx *dst = p.exit_out + (size_t)probe * p.N;
 #pragma unroll
         for (int i = 0; i < M; ++i) {
           const int g = lane * M + i;
@@ -447,13 +447,13 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
         }
       }
       if (do_grad) {
-        const float2 *ua = p.u_fwd + ((size_t)probe * p.ufwd_slices + (s - p.ufwd_base)) * p.Npad;
-        const float2 *ub = ua - p.Npad;
-        float2 *ga = gacc + cb * M * 33;
+        const cx *ua = p.u_fwd + ((size_t)probe * p.ufwd_slices + (s - p.ufwd_base)) * p.Npad;
+        const cx *ub = ua - p.Npad;
+        cx *ga = gacc + cb * M * 33;
 #pragma unroll
         for (int i = 0; i < M; ++i) {
-          const float2 w = cadd(ua[i * 32 + lane], ub[i * 32 + lane]);
-          const float2 v = cmulc(U[i], w);
+          const cx w = cadd(ua[i * 32 + lane], ub[i * 32 + lane]);
+          const cx v = cmulc(U[i], w);
           atomicAdd(&ga[i * 33 + lane].x, v.x);
           atomicAdd(&ga[i * 33 + lane].y, v.y);
         }
@@ -473,18 +473,18 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
     }
     if (do_grad) {
       // gradient buffer in the chunked layout: row k*M + i at offset i*32 + k
-      float2 *ga = gacc + cb * M * 33;
-      float2 *dst = p.grad_c + (size_t)(s - 1) * p.Npad;
+      cx *ga = gacc + cb * M * 33;
+      cx *dst = p.grad_c + (size_t)(s - 1) * p.Npad;
       for (int e = tid; e < p.Npad; e += blockDim.x) {
         const int i = e / 32, k = e % 32;
-        const float2 v = ga[i * 33 + k];
-        asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(&dst[e]), "f"(v.x), "f"(v.y) : "memory");
-        ga[i * 33 + k] = make_float2(0.f, 0.f);
+        const cx v = ga[i * 33 + k];
+        red_add_cx(&dst[e], v);
+        ga[i * 33 + k] = czero();
       }
     }
   }
   if (active && p.state_out != nullptr) {
-    float2 *dst = p.state_out + (size_t)probe * p.Npad;
+    cx *dst = p.state_out + (size_t)probe * p.Npad;
 #pragma unroll
     for (int i = 0; i < M; ++i) dst[i * 32 + lane] = U[i];
   }
@@ -493,7 +493,7 @@ __global__ void __launch_bounds__(kMarchWarps * 32, 1) cn2d_march_kernel(const M
 // --------------------------------------------------------------------------
 // Layout and gradient helpers
 // --------------------------------------------------------------------------
-__global__ void cn2d_unchunk_kernel(const float2 *__restrict__ st, float2 *__restrict__ out, int P, int N, int nz,
+__global__ void cn2d_unchunk_kernel(const cx *__restrict__ st, cx *__restrict__ out, int P, int N, int nz,
                                     int M, int C, int pair) {
   const size_t Npad = (size_t)C * M;
   const size_t total = (size_t)P * N * nz;
@@ -513,9 +513,9 @@ struct GradParams {
   int t0, nt;  // node columns [t0, t0 + nt) are mapped
   int M, C, pair, Npad;
   double k, dz;
-  const float2 *gc;
+  const cx *gc;
   const void *n;
-  float2 *gn;
+  cx *gn;
 };
 
 __global__ void cn2d_grad_to_n_kernel(const GradParams q) {
@@ -529,11 +529,11 @@ __global__ void cn2d_grad_to_n_kernel(const GradParams q) {
     const size_t off = q.pair ? ((size_t)(i >> 1) * q.C + k) * 2 + (i & 1) : (size_t)i * q.C + k;
     double2 acc = z2(0, 0);
     if (t >= 1) {
-      const float2 a = q.gc[(size_t)(t - 1) * q.Npad + off];
+      const cx a = q.gc[(size_t)(t - 1) * q.Npad + off];
       acc = zadd(acc, z2(a.x, a.y));
     }
     if (t <= q.L - 1) {
-      const float2 b = q.gc[(size_t)t * q.Npad + off];
+      const cx b = q.gc[(size_t)t * q.Npad + off];
       acc = zadd(acc, z2(b.x, b.y));
     }
     // dc/dn = (dz/4) coef'(n); coef' = k/i  or (k/i) n
@@ -549,7 +549,7 @@ __global__ void cn2d_grad_to_n_kernel(const GradParams q) {
       d = zmul(d, nv);
     }
     const double2 r = zmul(zconj(d), acc);
-    q.gn[idx] = make_float2((float)r.x, (float)r.y);
+    q.gn[idx] = to_cx(r);
   }
 }
 
@@ -592,7 +592,7 @@ static Spec make_spec(const tp_cn2d_op *op, int mode) {
   int ct;
   mode_transform(mode, &sigma, &ct);
   auto f = [&](const double v[2], bool conj) {
-    return make_float2((float)(sigma * v[0]), (float)(sigma * (conj ? -v[1] : v[1])));
+    return mkcx((rx)(sigma * v[0]), (rx)(sigma * (conj ? -v[1] : v[1])));
   };
   Spec s;
   s.p_o = f(op->k_off, ct);
@@ -607,7 +607,7 @@ static Spec make_spec(const tp_cn2d_op *op, int mode) {
     s.sup0 = s.p_o;
     s.subN1 = s.p_o;
   }
-  auto d = [&](float2 a) { return make_float2(a.x - s.p_o.x, a.y - s.p_o.y); };
+  auto d = [&](cx a) { return mkcx(a.x - s.p_o.x, a.y - s.p_o.y); };
   s.d_sup0 = d(s.sup0);
   s.d_sub1 = d(s.sub1);
   s.d_supN2 = d(s.supN2);
@@ -618,7 +618,7 @@ static Spec make_spec(const tp_cn2d_op *op, int mode) {
 template <int M, bool ALIGNED, bool LAGGED>
 static int launch_march_t(const MarchParams &mp, cudaStream_t st) {
   auto kern = cn2d_march_kernel<M, ALIGNED, LAGGED>;
-  const size_t smem = 2 * mp.slice_bytes + 2 * (size_t)M * 33 * sizeof(float2) + 2 * sizeof(uint64_t);
+  const size_t smem = 2 * mp.slice_bytes + 2 * (size_t)M * 33 * sizeof(cx) + 2 * sizeof(uint64_t);
   TP_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = (mp.P + kMarchWarps - 1) / kMarchWarps;
   kern<<<grid, kMarchWarps * 32, smem, st>>>(mp);
@@ -790,14 +790,14 @@ extern "C" int tp_cn2d_march(const tp_cn2d_op *op, const void *factors, const tp
   mp.slice_bytes = slice_bytes(pt);
   mp.factors = static_cast<const char *>(factors);
   mp.sp = make_spec(op, a->mode);
-  mp.probes = static_cast<const float2 *>(a->probes);
-  mp.src_shared = static_cast<const float2 *>(a->src_shared);
-  mp.src_probe = static_cast<const float2 *>(a->src_probe);
-  mp.src_exit = static_cast<const float2 *>(a->src_exit);
-  mp.u_store = static_cast<float2 *>(a->u_store);
-  mp.exit_out = static_cast<float2 *>(a->exit_out);
-  mp.u_fwd = static_cast<const float2 *>(a->u_fwd);
-  mp.grad_c = static_cast<float2 *>(a->grad_c);
+  mp.probes = static_cast<const cx *>(a->probes);
+  mp.src_shared = static_cast<const cx *>(a->src_shared);
+  mp.src_probe = static_cast<const cx *>(a->src_probe);
+  mp.src_exit = static_cast<const cx *>(a->src_exit);
+  mp.u_store = static_cast<cx *>(a->u_store);
+  mp.exit_out = static_cast<cx *>(a->exit_out);
+  mp.u_fwd = static_cast<const cx *>(a->u_fwd);
+  mp.grad_c = static_cast<cx *>(a->grad_c);
   mp.coupling = reinterpret_cast<const unsigned *>(mp.factors + (size_t)mp.L * mp.slice_bytes);
   mp.err = err;
   mp.t0 = a->t_begin > 0 ? a->t_begin : 1;
@@ -805,8 +805,8 @@ extern "C" int tp_cn2d_march(const tp_cn2d_op *op, const void *factors, const tp
   if (mp.t0 > mp.t1 || mp.t1 > mp.L) return set_error(TP_ERR_INVALID, "bad step range [%d, %d] (L=%d)", mp.t0, mp.t1, mp.L);
   if (mp.flip_out && (mp.t0 != 1 || mp.t1 != mp.L) && a->u_store != nullptr)
     return set_error(TP_ERR_INVALID, "the flipped ADJOINT store needs the full step range");
-  mp.state_in = static_cast<const float2 *>(a->state_in);
-  mp.state_out = static_cast<float2 *>(a->state_out);
+  mp.state_in = static_cast<const cx *>(a->state_in);
+  mp.state_out = static_cast<cx *>(a->state_out);
   mp.store_slices = a->store_slices > 0 ? a->store_slices : op->nz;
   mp.store_every = a->store_every;
   mp.store_base = a->store_base;
@@ -846,7 +846,7 @@ extern "C" int tp_cn2d_unchunk(const tp_cn2d_op *op, int32_t num_probes, const v
   rc = partition_for(op->n, &pt);
   if (rc) return rc;
   cn2d_unchunk_kernel<<<1184, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-      static_cast<const float2 *>(u_store), static_cast<float2 *>(u_out), num_probes, op->n, op->nz, pt.M, pt.C, pt.team);
+      static_cast<const cx *>(u_store), static_cast<cx *>(u_out), num_probes, op->n, op->nz, pt.M, pt.C, pt.team);
   return check_cuda(cudaGetLastError(), "cn2d_unchunk_kernel launch");
 }
 
@@ -874,9 +874,9 @@ static int grad_to_n_nodes(const tp_cn2d_op *op, const void *grad_c, const void 
   q.dtype = n_dtype;
   q.k = op->k;
   q.dz = op->dz;
-  q.gc = static_cast<const float2 *>(grad_c);
+  q.gc = static_cast<const cx *>(grad_c);
   q.n = n_field;
-  q.gn = static_cast<float2 *>(grad_n);
+  q.gn = static_cast<cx *>(grad_n);
   if (node_begin < 0 || node_end >= op->nz || node_begin > node_end)
     return set_error(TP_ERR_INVALID, "node range [%d, %d] outside [0, %d]", node_begin, node_end, op->nz - 1);
   q.t0 = node_begin;

@@ -30,19 +30,28 @@ __host__ __device__ inline int rec_alpha(int levels, int l) { return 2 + l; }
 __host__ __device__ inline int rec_gamma(int levels, int l) { return 2 + levels + l; }
 __host__ __device__ inline int rec_rde(int levels) { return 2 + 2 * levels; }
 
-// Global factor set of one slice: QD, LF, EP, V, W ([M][C] float2 each) then
-// the records ([nrec][C] float2), padded to 256 bytes.  The workspace of a
+// Global factor set of one slice: QD, LF, EP, V, W ([M][C] complex values
+// each) then the records ([nrec][C]), padded to 256 bytes.  The workspace of a
 // factorisation holds L slices and then kFactorTailBytes: the largest PCR
 // coefficient of all slices (float bits), which the team march reads.
 __host__ __device__ inline size_t slice_bytes(const Partition &pt) {
-  size_t b = (size_t)(5 * pt.M + pt.nrec) * pt.C * sizeof(float2);
+  size_t b = (size_t)(5 * pt.M + pt.nrec) * pt.C * sizeof(cx);
   return (b + 255) & ~size_t(255);
 }
 
 constexpr size_t kFactorTailBytes = 256;
 // Below this bound the reduced (separator) system is diagonal to far beneath
-// fp32 round-off and the team march skips its PCR levels.
+// the state's round-off and the team march skips its PCR levels; spike
+// entries below kSpikeDrop are not staged.  Both scale with the precision of
+// the build, so that in the complex128 check build the approximations stay
+// beneath fp64 round-off too.
+#ifdef TP_C128_CHECK
+constexpr float kPcrSkipBound = 1e-17f;
+constexpr double kSpikeDrop = 1e-17;
+#else
 constexpr float kPcrSkipBound = 1e-12f;
+constexpr double kSpikeDrop = 1e-9;
+#endif
 
 int partition_for(int n, Partition *pt);  // TP_OK or an error code
 
@@ -67,9 +76,9 @@ struct FactorParams {
 
 // P's off-diagonals: interior value and the four boundary entries (+ deltas).
 struct Spec {
-  float2 p_o;
-  float2 sup0, sub1, supN2, subN1;
-  float2 d_sup0, d_sub1, d_supN2, d_subN1;
+  cx p_o;
+  cx sup0, sub1, supN2, subN1;
+  cx d_sup0, d_sub1, d_supN2, d_subN1;
 };
 
 struct MarchParams {
@@ -80,15 +89,15 @@ struct MarchParams {
   size_t smem_slice_bytes;   // team path: shared-memory slice size
   const char *factors;
   Spec sp;
-  const float2 *probes, *src_shared, *src_probe, *src_exit;
-  float2 *u_store, *exit_out;
-  const float2 *u_fwd;
-  float2 *grad_c;
+  const cx *probes, *src_shared, *src_probe, *src_exit;
+  cx *u_store, *exit_out;
+  const cx *u_fwd;
+  cx *grad_c;
   const unsigned *coupling;     // the factor set's PCR coupling bound (float bits), or NULL
   int *err;
   int t0, t1;                   // step range
-  const float2 *state_in;       // chunked (P, Npad) or null
-  float2 *state_out;
+  const cx *state_in;           // chunked (P, Npad) or null
+  cx *state_out;
   int store_slices, store_every, store_base;
   int ufwd_slices, ufwd_base;
   int store_sums;               // FORWARD: u_store gets u_t + u_{t-1}; ADJOINT_EXACT: u_fwd holds them
@@ -109,8 +118,8 @@ __host__ __device__ inline int store_index(const MarchParams &p, int t) {
 // Spike rows kept by the team path for operator `op` with M rows per chunk:
 // the inverse of a diagonally dominant tridiagonal matrix decays like rho^d,
 // rho = (d0 - sqrt(d0^2 - 4 b^2)) / (2 b) with b the off-diagonal and d0 the
-// diagonal magnitude of the free-space matrix; keep rows until rho^T < 1e-10
-// (plus two).  The factor kernel verifies the choice on the actual matrices.
+// diagonal magnitude of the free-space matrix; keep rows until rho^T is
+// below kSpikeDrop (plus one).  The factor kernel verifies the choice on the actual matrices.
 int team_spike_rows(const tp_cn2d_op *op, int M);
 
 // Team-path launcher (cn2d_team.cu).

@@ -35,33 +35,32 @@ constexpr int kTeamLevels = 7;
 __device__ __forceinline__ void team_sync(int team) {
   asm volatile("bar.sync %0, %1;" ::"r"(1 + team), "r"(kTeamThreads) : "memory");
 }
-__device__ __forceinline__ void red_add_v4(float4 *addr, float4 v) {
-  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
-               : "memory");
-}
+// fused a*b + c in the march's real type
+__device__ __forceinline__ float rfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double rfma(double a, double b, double c) { return fma(a, b, c); }
 
 // b * i * z for real b (the off-diagonal of P is purely imaginary: i*dz/(4k dx^2)).
-__device__ __forceinline__ float2 imul_acc(float b, float2 z, float2 acc) {
-  return make_float2(fmaf(-b, z.y, acc.x), fmaf(b, z.x, acc.y));
+__device__ __forceinline__ cx imul_acc(rx b, cx z, cx acc) {
+  return mkcx(rfma(-b, z.y, acc.x), rfma(b, z.x, acc.y));
 }
 
 // Chunked team layout: rows are stored in pairs, so thread c's rows 2j, 2j+1
 // are one 16-byte vector at offset (j*C + c)*2 of a slice.
-__device__ __forceinline__ void store_pairs(float2 *dst, const float2 *U, int M, int c) {
+__device__ __forceinline__ void store_pairs(cx *dst, const cx *U, int M, int c) {
 #pragma unroll 8
   for (int j = 0; j < M / 2; ++j)
-    reinterpret_cast<float4 *>(dst)[j * kTeamChunks + c] = make_float4(U[2 * j].x, U[2 * j].y, U[2 * j + 1].x, U[2 * j + 1].y);
+    reinterpret_cast<cx2 *>(dst)[j * kTeamChunks + c] = mkcx2(U[2 * j], U[2 * j + 1]);
 }
 
 // Load thread c's M rows of one stored slice (row pairs).
 template <int M>
-__device__ __forceinline__ void load_pairs(float2 (&dst)[M], const float2 *slice, int c) {
-  const float4 *src = reinterpret_cast<const float4 *>(slice) + c;
+__device__ __forceinline__ void load_pairs(cx (&dst)[M], const cx *slice, int c) {
+  const cx2 *src = reinterpret_cast<const cx2 *>(slice) + c;
 #pragma unroll
   for (int j = 0; j < M / 2; ++j) {
-    const float4 v = src[j * kTeamChunks];
-    dst[2 * j] = make_float2(v.x, v.y);
-    dst[2 * j + 1] = make_float2(v.z, v.w);
+    const cx2 v = src[j * kTeamChunks];
+    dst[2 * j] = mkcx(v.x, v.y);
+    dst[2 * j + 1] = mkcx(v.z, v.w);
   }
 }
 
@@ -69,7 +68,7 @@ __device__ __forceinline__ void load_pairs(float2 (&dst)[M], const float2 *slice
 // never apply the right-hand-side stencil, so they stage LF|EP without the
 // QD rows (qd = false).
 __host__ __device__ inline size_t team_slice_smem(int M, int T, bool qd = true) {
-  return (size_t)((qd ? 3 : 2) * M + 2 * T + 3 + 2 * kTeamLevels) * kTeamChunks * sizeof(float2);
+  return (size_t)((qd ? 3 : 2) * M + 2 * T + 3 + 2 * kTeamLevels) * kTeamChunks * sizeof(cx);
 }
 
 // Exchange rows per probe: Y0, R0, R1, XS, and for the stencil (qd) XL, XF.
@@ -80,16 +79,16 @@ __host__ __device__ constexpr int team_xrows(bool qd) { return qd ? 6 : 4; }
 // one staging slice per probe, and the mbarriers (factor double buffer, one
 // per team).
 size_t team_smem_bytes(const Partition &pt, int trunc, int Q, int TM, bool qd, bool stg) {
-  const size_t slice = (size_t)pt.M * kTeamChunks * sizeof(float2);
+  const size_t slice = (size_t)pt.M * kTeamChunks * sizeof(cx);
   const size_t stage = (qd || !stg) ? 0 : (size_t)TM * Q * slice;
-  return 2 * team_slice_smem(pt.M, trunc, qd) + (size_t)team_xrows(qd) * TM * Q * kTeamChunks * sizeof(float2) +
+  return 2 * team_slice_smem(pt.M, trunc, qd) + (size_t)team_xrows(qd) * TM * Q * kTeamChunks * sizeof(cx) +
          stage + (2 + (size_t)TM) * sizeof(uint64_t);
 }
 
 // Issue the bulk copies of one slice's factor set ([QD|]LF|EP, V head, W tail, records).
-__device__ __forceinline__ void team_issue(float2 *dst, const char *slice, int M, int T, uint64_t *bar, bool qd) {
+__device__ __forceinline__ void team_issue(cx *dst, const char *slice, int M, int T, uint64_t *bar, bool qd) {
   constexpr int C = kTeamChunks;
-  const uint32_t row = C * sizeof(float2);
+  const uint32_t row = C * sizeof(cx);
   const uint32_t b_main = (qd ? 3 : 2) * M * row, b_sp = T * row, b_rec = (3 + 2 * kTeamLevels) * row;
   mbar_arrive_expect_tx(bar, b_main + 2 * b_sp + b_rec);
   char *d = reinterpret_cast<char *>(dst);
@@ -102,17 +101,17 @@ __device__ __forceinline__ void team_issue(float2 *dst, const char *slice, int M
 // U <- (I + P_s) U for the Q probes (boundary rows: chunk 0 rows 0,1 and
 // chunk C-1 rows M-2, M-1).
 template <int M, int Q>
-__device__ __forceinline__ void team_rhs(float2 (&U)[Q][M], const float2 *__restrict__ QD, float2 *XL, float2 *XF,
+__device__ __forceinline__ void team_rhs(cx (&U)[Q][M], const cx *__restrict__ QD, cx *XL, cx *XF,
                                          int c, int team, const Spec &sp) {
   constexpr int C = kTeamChunks;
-  const float2 zero = make_float2(0.f, 0.f);
+  const cx zero = czero();
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     XL[q * C + c] = U[q][M - 1];
     XF[q * C + c] = U[q][0];
   }
   team_sync(team);
-  float2 prev[Q], right[Q];
+  cx prev[Q], right[Q];
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     prev[q] = (c > 0) ? XL[q * C + c - 1] : zero;
@@ -120,12 +119,12 @@ __device__ __forceinline__ void team_rhs(float2 (&U)[Q][M], const float2 *__rest
   }
 #pragma unroll
   for (int i = 0; i < M; ++i) {
-    const float2 qd = QD[i * C + c];
+    const cx qd = QD[i * C + c];
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-      const float2 cur = U[q][i];
-      const float2 nxt = (i < M - 1) ? U[q][(i + 1) < M ? i + 1 : i] : right[q];
-      float2 r = cfma(qd, cur, cur);
+      const cx cur = U[q][i];
+      const cx nxt = (i < M - 1) ? U[q][(i + 1) < M ? i + 1 : i] : right[q];
+      cx r = cfma(qd, cur, cur);
       r = imul_acc(sp.p_o.y, cadd(prev[q], nxt), r);
       if (i == 0 && c == 0) r = cfma(sp.d_sup0, nxt, r);
       if (i == 1 && c == 0) r = cfma(sp.d_sub1, prev[q], r);
@@ -141,34 +140,34 @@ __device__ __forceinline__ void team_rhs(float2 (&U)[Q][M], const float2 *__rest
 // compile-time count, so the spike corrections touch only those rows; QD:
 // the slice starts with the QD rows; WAITR: the caller stages bulk stores).
 template <int M, int Q, int T, bool QD, bool WAITR>
-__device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__restrict__ F, float2 *Y0,
-                                           float2 *R0, float2 *R1, float2 *XS, int c, int team, const Spec &sp,
+__device__ __forceinline__ void team_solve(cx (&U)[Q][M], const cx *__restrict__ F, cx *Y0,
+                                           cx *R0, cx *R1, cx *XS, int c, int team, const Spec &sp,
                                            bool pcr) {
   constexpr int C = kTeamChunks;
-  const float2 zero = make_float2(0.f, 0.f);
-  const float2 *LF = F + (QD ? M * C : 0), *EP = LF + M * C, *VH = EP + M * C, *WT = VH + T * C, *LR = WT + T * C;
+  const cx zero = czero();
+  const cx *LF = F + (QD ? M * C : 0), *EP = LF + M * C, *VH = EP + M * C, *WT = VH + T * C, *LR = WT + T * C;
 #pragma unroll
   for (int i = 1; i <= M - 2; ++i) {
-    const float2 lf = LF[i * C + c];
+    const cx lf = LF[i * C + c];
 #pragma unroll
     for (int q = 0; q < Q; ++q) U[q][i] = cfnma(lf, U[q][i - 1], U[q][i]);
   }
   {
-    const float2 ep = EP[(M - 2) * C + c];
+    const cx ep = EP[(M - 2) * C + c];
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-      const float2 t = U[q][M - 2];
+      const cx t = U[q][M - 2];
       U[q][M - 2] = cfma(t, ep, t);
     }
   }
 #pragma unroll
   for (int i = M - 3; i >= 0; --i) {
-    const float2 ep = EP[i * C + c];
+    const cx ep = EP[i * C + c];
     // t = U[i] - M[i,i+1] U[i+1] = U[i] + P[i,i+1] U[i+1]; P[0,1] is the only special entry here.
-    const float bsup = (i == 0 && c == 0) ? sp.sup0.y : sp.p_o.y;
+    const rx bsup = (i == 0 && c == 0) ? sp.sup0.y : sp.p_o.y;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-      const float2 t = imul_acc(bsup, U[q][i + 1], U[q][i]);
+      const cx t = imul_acc(bsup, U[q][i + 1], U[q][i]);
       U[q][i] = cfma(t, ep, t);
     }
   }
@@ -179,7 +178,7 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
   // wait is executed by all threads, without a branch; it returns at once
   // in threads with no bulk copies in flight).
   if constexpr (WAITR) bulk_wait_read();
-  float2 x[Q], xp[Q];
+  cx x[Q], xp[Q];
   constexpr int kRd = 2 + 2 * kTeamLevels;  // record row of the reduced diagonal
   if (!pcr) {
     // The factorisation found every separator coupling below kPcrSkipBound,
@@ -189,8 +188,8 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
     // then forms its own separator and recomputes its left neighbour's from
     // the neighbour's records (the same operations, so the same bits), which
     // saves the second exchange and its barrier.
-    const float2 ma = LR[0 * C + c], mc = LR[1 * C + c];
-    float2 zc[Q];
+    const cx ma = LR[0 * C + c], mc = LR[1 * C + c];
+    cx zc[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       zc[q] = cfnma(ma, U[q][M - 2], U[q][M - 1]);
@@ -198,15 +197,15 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
       R0[q * C + c] = zc[q];
     }
     team_sync(team);
-    const float2 rde = LR[kRd * C + c];
-    const float2 mcl = c > 0 ? LR[1 * C + c - 1] : zero, rdel = c > 0 ? LR[kRd * C + c - 1] : zero;
+    const cx rde = LR[kRd * C + c];
+    const cx mcl = c > 0 ? LR[1 * C + c - 1] : zero, rdel = c > 0 ? LR[kRd * C + c - 1] : zero;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-      const float2 y0n = (c < C - 1) ? Y0[q * C + c + 1] : zero;
-      const float2 r = cfnma(mc, y0n, zc[q]);
+      const cx y0n = (c < C - 1) ? Y0[q * C + c + 1] : zero;
+      const cx r = cfnma(mc, y0n, zc[q]);
       x[q] = cfma(r, rde, r);
       if (c > 0) {
-        const float2 rl = cfnma(mcl, U[q][0], R0[q * C + c - 1]);
+        const cx rl = cfnma(mcl, U[q][0], R0[q * C + c - 1]);
         xp[q] = cfma(rl, rdel, rl);
       } else {
         xp[q] = zero;
@@ -216,12 +215,12 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
 #pragma unroll
     for (int q = 0; q < Q; ++q) Y0[q * C + c] = U[q][0];
     team_sync(team);
-    float2 rho[Q];
+    cx rho[Q];
     {
-      const float2 ma = LR[0 * C + c], mc = LR[1 * C + c];
+      const cx ma = LR[0 * C + c], mc = LR[1 * C + c];
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
-        const float2 y0n = (c < C - 1) ? Y0[q * C + c + 1] : zero;
+        const cx y0n = (c < C - 1) ? Y0[q * C + c + 1] : zero;
         rho[q] = cfnma(mc, y0n, cfnma(ma, U[q][M - 2], U[q][M - 1]));
       }
     }
@@ -229,19 +228,19 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
 #pragma unroll
     for (int l = 0; l < kTeamLevels; ++l) {
       const int s = 1 << l;
-      float2 *Rb = (l & 1) ? R1 : R0;
+      cx *Rb = (l & 1) ? R1 : R0;
 #pragma unroll
       for (int q = 0; q < Q; ++q) Rb[q * C + c] = rho[q];
       team_sync(team);
-      const float2 al = LR[(2 + l) * C + c], ga = LR[(2 + kTeamLevels + l) * C + c];
+      const cx al = LR[(2 + l) * C + c], ga = LR[(2 + kTeamLevels + l) * C + c];
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
-        const float2 up = (c >= s) ? Rb[q * C + c - s] : zero;
-        const float2 dn = (c + s < C) ? Rb[q * C + c + s] : zero;
+        const cx up = (c >= s) ? Rb[q * C + c - s] : zero;
+        const cx dn = (c + s < C) ? Rb[q * C + c + s] : zero;
         rho[q] = cfma(ga, dn, cfma(al, up, rho[q]));
       }
     }
-    const float2 rde = LR[kRd * C + c];
+    const cx rde = LR[kRd * C + c];
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       x[q] = cfma(rho[q], rde, rho[q]);
@@ -255,12 +254,12 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
 #pragma unroll
   for (int i = 0; i <= M - 2; ++i) {
     if (i < T) {
-      const float2 v = VH[i * C + c];
+      const cx v = VH[i * C + c];
 #pragma unroll
       for (int q = 0; q < Q; ++q) U[q][i] = cfma(v, xp[q], U[q][i]);
     }
     if (i >= wlo) {
-      const float2 w = WT[(i - wlo) * C + c];
+      const cx w = WT[(i - wlo) * C + c];
 #pragma unroll
       for (int q = 0; q < Q; ++q) U[q][i] = cfma(w, x[q], U[q][i]);
     }
@@ -275,7 +274,7 @@ __device__ __forceinline__ void team_solve(float2 (&U)[Q][M], const float2 *__re
 // bulk store.  The staging slices are written again only after the next
 // solve's exchange barrier, before which thread 0 waits for the copy's read.
 template <int M, int Q>
-__device__ __forceinline__ void store_staged(const float2 (&U)[Q][M], float4 *stg, const MarchParams &p, int p0,
+__device__ __forceinline__ void store_staged(const cx (&U)[Q][M], cx2 *stg, const MarchParams &p, int p0,
                                              int sidx, int c, int team) {
   constexpr int C = kTeamChunks;
 #pragma unroll
@@ -284,7 +283,7 @@ __device__ __forceinline__ void store_staged(const float2 (&U)[Q][M], float4 *st
 #pragma unroll
     for (int j = 0; j < M / 2; ++j)
       stg[(q * (M / 2) + j) * C + c] =
-          make_float4(U[q][2 * j].x, U[q][2 * j].y, U[q][2 * j + 1].x, U[q][2 * j + 1].y);
+          mkcx2(U[q][2 * j], U[q][2 * j + 1]);
   }
   fence_proxy_async_smem();
   team_sync(team);
@@ -293,7 +292,7 @@ __device__ __forceinline__ void store_staged(const float2 (&U)[Q][M], float4 *st
     for (int q = 0; q < Q; ++q)
       if (p0 + q < p.P)
         bulk_s2g(p.u_store + ((size_t)(p0 + q) * p.store_slices + sidx) * p.Npad, stg + (size_t)q * (M / 2) * C,
-                 M * C * sizeof(float2));
+                 M * C * sizeof(cx));
     bulk_commit();
   }
 }
@@ -307,18 +306,18 @@ __device__ __forceinline__ void store_staged(const float2 (&U)[Q][M], float4 *st
 // sum is twice the half sum) before the gradient row is updated
 // (grad_sum_flush).
 template <int M, int Q>
-__device__ __forceinline__ void grad_contrib(const float2 (&U)[Q][M], float4 *stg, int nvalid, int c) {
+__device__ __forceinline__ void grad_contrib(const cx (&U)[Q][M], cx2 *stg, int nvalid, int c) {
   constexpr int C = kTeamChunks;
 #pragma unroll
   for (int j = 0; j < M / 2; ++j) {
-    float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+    cx2 w = mkcx2(czero(), czero());
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       if (q >= nvalid) continue;
-      const float4 v = stg[(q * (M / 2) + j) * C + c];
-      const float2 a = cmulc(U[q][2 * j], make_float2(v.x, v.y));
-      const float2 b = cmulc(U[q][2 * j + 1], make_float2(v.z, v.w));
-      w = make_float4(w.x + a.x, w.y + a.y, w.z + b.x, w.w + b.y);
+      const cx2 v = stg[(q * (M / 2) + j) * C + c];
+      const cx a = cmulc(U[q][2 * j], mkcx(v.x, v.y));
+      const cx b = cmulc(U[q][2 * j + 1], mkcx(v.z, v.w));
+      w = mkcx2(mkcx(w.x + a.x, w.y + a.y), mkcx(w.z + b.x, w.w + b.y));
     }
     stg[j * C + c] = w;
   }
@@ -331,18 +330,18 @@ __device__ __forceinline__ void grad_contrib(const float2 (&U)[Q][M], float4 *st
 // share of the row pairs; the slices are complete after a CTA barrier and
 // free for the next bulk loads after the next one.
 template <int M, int Q, int TM>
-__device__ __forceinline__ void grad_sum_flush(const float4 *stage, float2 *row, int tid) {
+__device__ __forceinline__ void grad_sum_flush(const cx2 *stage, cx *row, int tid) {
   constexpr int E = (M / 2) * kTeamChunks, NT = TM * kTeamThreads;
-  float4 *g = reinterpret_cast<float4 *>(row);
+  cx2 *g = reinterpret_cast<cx2 *>(row);
 #pragma unroll
   for (int e = tid; e < E; e += NT) {
-    float4 v = stage[e];
+    cx2 v = stage[e];
 #pragma unroll
     for (int m = 1; m < TM; ++m) {
-      const float4 w = stage[m * Q * E + e];  // team m's first slice
-      v = make_float4(v.x + w.x, v.y + w.y, v.z + w.z, v.w + w.w);
+      const cx2 w = stage[m * Q * E + e];  // team m's first slice
+      v = mkcx2(mkcx(v.x + w.x, v.y + w.y), mkcx(v.z + w.z, v.w + w.w));
     }
-    red_add_v4(g + e, make_float4(2.f * v.x, 2.f * v.y, 2.f * v.z, 2.f * v.w));
+    red_add_cx2(g + e, mkcx2(mkcx(2 * v.x, 2 * v.y), mkcx(2 * v.z, 2 * v.w)));
   }
   // the slices are next written by bulk loads (async proxy)
   fence_proxy_async_smem();
@@ -371,25 +370,25 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
   constexpr bool STAGE = !QD && STG;              // staging slices in shared memory
   constexpr bool GSTAGE = LAGGED && SUMS && STG;  // the gradient goes through them
   constexpr int C = kTeamChunks;
-  constexpr uint32_t NB = M * C * sizeof(float2);  // bytes of one probe's slice
+  constexpr uint32_t NB = M * C * sizeof(cx);  // bytes of one probe's slice
   extern __shared__ __align__(128) unsigned char smem[];
   const int tid = threadIdx.x;
   const int team = tid / kTeamThreads;
   const int c = tid % kTeamThreads;
   constexpr int T = TS;  // the host sets p.trunc = TS
   const size_t ss = p.smem_slice_bytes;
-  float2 *bufs = reinterpret_cast<float2 *>(smem);
+  cx *bufs = reinterpret_cast<cx *>(smem);
   constexpr int XR = team_xrows(QD);
-  float2 *xb = reinterpret_cast<float2 *>(smem + 2 * ss) + (size_t)team * XR * Q * C;
-  float2 *XL = QD ? xb : nullptr, *XF = QD ? xb + Q * C : nullptr;  // stencil rows (QD only)
-  float2 *Y0 = xb + (QD ? 2 : 0) * Q * C, *R0 = Y0 + Q * C, *R1 = R0 + Q * C, *XS = R1 + Q * C;
-  float4 *stage = reinterpret_cast<float4 *>(smem + 2 * ss + (size_t)TM * XR * Q * C * sizeof(float2));
-  float4 *stg = stage + (size_t)team * Q * (M / 2) * C;  // this team's Q staging slices
+  cx *xb = reinterpret_cast<cx *>(smem + 2 * ss) + (size_t)team * XR * Q * C;
+  cx *XL = QD ? xb : nullptr, *XF = QD ? xb + Q * C : nullptr;  // stencil rows (QD only)
+  cx *Y0 = xb + (QD ? 2 : 0) * Q * C, *R0 = Y0 + Q * C, *R1 = R0 + Q * C, *XS = R1 + Q * C;
+  cx2 *stage = reinterpret_cast<cx2 *>(smem + 2 * ss + (size_t)TM * XR * Q * C * sizeof(cx));
+  cx2 *stg = stage + (size_t)team * Q * (M / 2) * C;  // this team's Q staging slices
   uint64_t *mbar = reinterpret_cast<uint64_t *>(reinterpret_cast<unsigned char *>(stage) +
                                                 (STAGE ? (size_t)TM * Q * NB : 0));
   uint64_t *gbar = mbar + 2;  // one per team: its half-sum slice
   const bool do_grad = LAGGED && (p.grad_c != nullptr);
-  const size_t ssf = ss / sizeof(float2);
+  const size_t ssf = ss / sizeof(cx);
   const int p0 = (blockIdx.x * TM + team) * Q;
   const bool pcr = p.coupling == nullptr || __uint_as_float(__ldg(p.coupling)) >= kPcrSkipBound;
 
@@ -405,22 +404,22 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
   if (tid == 0)
     team_issue(bufs + ssf, p.factors + (size_t)(slice_of(p.t0) - 1) * p.slice_bytes, M, T, &mbar[1], QD);
 
-  float2 U[Q][M];
+  cx U[Q][M];
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
 #pragma unroll
-    for (int i = 0; i < M; ++i) U[q][i] = make_float2(0.f, 0.f);
+    for (int i = 0; i < M; ++i) U[q][i] = czero();
     if (p0 + q >= p.P) continue;
     if (p.state_in != nullptr) {
-      const float4 *src = reinterpret_cast<const float4 *>(p.state_in + (size_t)(p0 + q) * p.Npad) + c;
+      const cx2 *src = reinterpret_cast<const cx2 *>(p.state_in + (size_t)(p0 + q) * p.Npad) + c;
 #pragma unroll
       for (int j = 0; j < M / 2; ++j) {
-        const float4 v = src[j * C];
-        U[q][2 * j] = make_float2(v.x, v.y);
-        U[q][2 * j + 1] = make_float2(v.z, v.w);
+        const cx2 v = src[j * C];
+        U[q][2 * j] = mkcx(v.x, v.y);
+        U[q][2 * j + 1] = mkcx(v.z, v.w);
       }
     } else if (p.probes != nullptr && p.t0 == 1) {
-      const float2 *src = p.probes + (size_t)(p0 + q) * p.N + c * M;
+      const cx *src = p.probes + (size_t)(p0 + q) * p.N + c * M;
 #pragma unroll
       for (int i = 0; i < M; ++i) U[q][i] = src[i];
     }
@@ -437,7 +436,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
   // Two-slice gradient (QD): the forward slice u_s of the current step is
   // kept from the previous step (u_prev); only u_{s-1} is read, issued at the
   // start of the step so that its latency overlaps the solve.
-  float2 u_prev[Q][M], u_new[Q][M];
+  cx u_prev[Q][M], u_new[Q][M];
   if constexpr (QD) {
     if (do_grad) {
 #pragma unroll
@@ -500,7 +499,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
       team_issue(bufs + (cb ^ 1) * ssf, p.factors + (size_t)(slice_of(t + 1) - 1) * p.slice_bytes, M, T,
                  &mbar[cb ^ 1], QD);
     }
-    const float2 *F = bufs + cb * ssf;
+    const cx *F = bufs + cb * ssf;
     if constexpr (!GSTAGE) {
       // unstaged gradient: this step's forward slice (QD: u_{s-1}; SUMS: the
       // half sum), issued before the solve so that its latency overlaps it
@@ -522,31 +521,31 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
     // solve's input v = u + b instead.  In the forward step the solve result
     // x = M^{-1}(u_{t-1} + b/2) is exactly (u_t + u_{t-1})/2, the half pair
     // sum the gradient contracts with: store_sums stores x itself.
-    float2 u_old[Q][M];
+    cx u_old[Q][M];
     if constexpr (!LAGGED) {
 #pragma unroll
       for (int q = 0; q < Q; ++q)
 #pragma unroll
         for (int i = 0; i < M; ++i) u_old[q][i] = U[q][i];
     }
-    const float sw = LAGGED ? 1.f : 0.5f;  // source weight
+    const rx sw = LAGGED ? rx(1) : rx(0.5);  // source weight
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       if (p0 + q >= p.P) continue;
       const int g0 = c * M;
       if (p.src_shared != nullptr) {
-        const float2 *src = p.src_shared + (size_t)(t - 1) * p.N + g0;
+        const cx *src = p.src_shared + (size_t)(t - 1) * p.N + g0;
 #pragma unroll
         for (int i = 0; i < M; ++i) U[q][i] = caxpy(sw, src[i], U[q][i]);
       }
       if (p.src_probe != nullptr) {
         const int col = p.src_rev ? (p.L - t) : (t - 1);
-        const float2 *src = p.src_probe + ((size_t)(p0 + q) * p.L + col) * p.N + g0;
+        const cx *src = p.src_probe + ((size_t)(p0 + q) * p.L + col) * p.N + g0;
 #pragma unroll
         for (int i = 0; i < M; ++i) U[q][i] = caxpy(sw, src[i], U[q][i]);
       }
       if (t == 1 && p.src_exit != nullptr) {
-        const float2 *src = p.src_exit + (size_t)(p0 + q) * p.N + g0;
+        const cx *src = p.src_exit + (size_t)(p0 + q) * p.N + g0;
 #pragma unroll
         for (int i = 0; i < M; ++i) U[q][i] = caxpy(sw, src[i], U[q][i]);
       }
@@ -575,7 +574,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
       for (int q = 0; q < Q; ++q)
 #pragma unroll
         for (int i = 0; i < M; ++i)
-          U[q][i] = make_float2(fmaf(2.f, U[q][i].x, -u_old[q][i].x), fmaf(2.f, U[q][i].y, -u_old[q][i].y));
+          U[q][i] = mkcx(rfma(rx(2), U[q][i].x, -u_old[q][i].x), rfma(rx(2), U[q][i].y, -u_old[q][i].y));
       if (!p.store_sums && sidx >= 0) {
         if constexpr (STAGE) store_staged<M, Q>(U, stg, p, p0, sidx, c, team);
         else store_direct();
@@ -587,7 +586,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         if (p0 + q >= p.P) continue;
-        float2 *dst = p.exit_out + (size_t)(p0 + q) * p.N + c * M;
+        cx *dst = p.exit_out + (size_t)(p0 + q) * p.N + c * M;
 #pragma unroll
         for (int i = 0; i < M; ++i) dst[i] = U[q][i];
       }
@@ -602,14 +601,14 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
         good = okg;
         grad_contrib<M, Q>(U, stg, nvalid, c);
       } else {
-        float4 *gdst = reinterpret_cast<float4 *>(p.grad_c + (size_t)(s - 1) * p.Npad) + c;
+        cx2 *gdst = reinterpret_cast<cx2 *>(p.grad_c + (size_t)(s - 1) * p.Npad) + c;
 #pragma unroll
         for (int j = 0; j < M / 2; ++j) {
-          float4 ga = make_float4(0.f, 0.f, 0.f, 0.f);
+          cx2 ga = mkcx2(czero(), czero());
 #pragma unroll
           for (int q = 0; q < Q; ++q) {
             if (p0 + q >= p.P) continue;  // padded probes contribute nothing
-            float2 wa, wb;
+            cx wa, wb;
             if constexpr (SUMS) {
               wa = u_new[q][2 * j];
               wb = u_new[q][2 * j + 1];
@@ -617,15 +616,15 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
               wa = cadd(u_prev[q][2 * j], u_new[q][2 * j]);
               wb = cadd(u_prev[q][2 * j + 1], u_new[q][2 * j + 1]);
             }
-            const float2 a = cmulc(U[q][2 * j], wa);
-            const float2 b = cmulc(U[q][2 * j + 1], wb);
+            const cx a = cmulc(U[q][2 * j], wa);
+            const cx b = cmulc(U[q][2 * j + 1], wb);
             ga.x += a.x;
             ga.y += a.y;
             ga.z += b.x;
             ga.w += b.y;
           }
-          if constexpr (SUMS) ga = make_float4(2.f * ga.x, 2.f * ga.y, 2.f * ga.z, 2.f * ga.w);  // half sums
-          red_add_v4(gdst + j * C, ga);
+          if constexpr (SUMS) ga = mkcx2(mkcx(2 * ga.x, 2 * ga.y), mkcx(2 * ga.z, 2 * ga.w));  // half sums
+          red_add_cx2(gdst + j * C, ga);
         }
         if constexpr (!SUMS) {
 #pragma unroll
@@ -640,7 +639,7 @@ __global__ void __launch_bounds__(kTeamThreads *TM, 1) cn2d_team_kernel(const Ma
       for (int q = 0; q < Q; ++q)
 #pragma unroll
         for (int i = 0; i < M; ++i)
-          U[q][i] = make_float2(fmaf(2.f, U[q][i].x, -u_old[q][i].x), fmaf(2.f, U[q][i].y, -u_old[q][i].y));
+          U[q][i] = mkcx(rfma(rx(2), U[q][i].x, -u_old[q][i].x), rfma(rx(2), U[q][i].y, -u_old[q][i].y));
     } else if constexpr (LAGGED) {
       team_rhs<M, Q>(U, F, XL, XF, c, team, p.sp);
     }

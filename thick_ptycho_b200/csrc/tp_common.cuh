@@ -41,6 +41,91 @@ __device__ __forceinline__ float2 shfl_down2(float2 v, int d) {
   return c2(__shfl_down_sync(0xffffffffu, v.x, d), __shfl_down_sync(0xffffffffu, v.y, d));
 }
 
+// The same operations on complex128 (the check build's march state).
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {
+  return make_double2(fma(a.x, b.x, fma(-a.y, b.y, c.x)), fma(a.x, b.y, fma(a.y, b.x, c.y)));
+}
+__device__ __forceinline__ double2 cfnma(double2 a, double2 b, double2 c) {
+  return make_double2(fma(-a.x, b.x, fma(a.y, b.y, c.x)), fma(-a.x, b.y, fma(-a.y, b.x, c.y)));
+}
+__device__ __forceinline__ double2 caxpy(double s, double2 a, double2 c) {
+  return make_double2(fma(s, a.x, c.x), fma(s, a.y, c.y));
+}
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, a.y * b.y), fma(a.y, b.x, -a.x * b.y));
+}
+__device__ __forceinline__ double2 shfl_up2(double2 v, int d) {
+  return make_double2(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d));
+}
+__device__ __forceinline__ double2 shfl_down2(double2 v, int d) {
+  return make_double2(__shfl_down_sync(0xffffffffu, v.x, d), __shfl_down_sync(0xffffffffu, v.y, d));
+}
+
+// A pair of complex128 values (two rows of a stored field in one 32-byte unit).
+struct __align__(32) zpair {
+  double x, y, z, w;
+};
+
+// ------------------------------------------------- state type of the 2D march
+// cx is the complex type of the 2D march's state, factor sets and stored
+// fields: complex64, or complex128 in the check build (compiled with
+// TP_C128_CHECK), which runs the same algorithms -- partitioned solve,
+// truncated spikes, PCR skip, Cayley step, pair-sum store -- with every
+// stored value and all arithmetic in fp64, so that they can be compared with
+// the complex128 oracle far below complex64 round-off.  rx is its real type
+// and cx2 a pair of cx (two rows in one vector access).
+#ifdef TP_C128_CHECK
+using cx = double2;
+using rx = double;
+using cx2 = zpair;
+#else
+using cx = float2;
+using rx = float;
+using cx2 = float4;
+#endif
+__host__ __device__ __forceinline__ cx mkcx(rx x, rx y) {
+  cx v;
+  v.x = x;
+  v.y = y;
+  return v;
+}
+__host__ __device__ __forceinline__ cx czero() { return mkcx(rx(0), rx(0)); }
+__host__ __device__ __forceinline__ cx2 mkcx2(cx a, cx b) {
+  cx2 v;
+  v.x = a.x;
+  v.y = a.y;
+  v.z = b.x;
+  v.w = b.y;
+  return v;
+}
+__host__ __device__ __forceinline__ cx cx2_lo(cx2 v) { return mkcx(v.x, v.y); }
+__host__ __device__ __forceinline__ cx cx2_hi(cx2 v) { return mkcx(v.z, v.w); }
+// global dst += v without a return value (vector reductions in the normal build)
+__device__ __forceinline__ void red_add_cx(cx *dst, cx v) {
+#ifdef TP_C128_CHECK
+  atomicAdd(&dst->x, v.x);
+  atomicAdd(&dst->y, v.y);
+#else
+  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(dst), "f"(v.x), "f"(v.y) : "memory");
+#endif
+}
+__device__ __forceinline__ void red_add_cx2(cx2 *dst, cx2 v) {
+#ifdef TP_C128_CHECK
+  atomicAdd(&dst->x, v.x);
+  atomicAdd(&dst->y, v.y);
+  atomicAdd(&dst->z, v.z);
+  atomicAdd(&dst->w, v.w);
+#else
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(dst), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+               : "memory");
+#endif
+}
+
 // ---------------------------------------------------------------- complex128
 __host__ __device__ __forceinline__ double2 z2(double x, double y) { return make_double2(x, y); }
 __host__ __device__ __forceinline__ double2 zadd(double2 a, double2 b) { return z2(a.x + b.x, a.y + b.y); }
@@ -61,6 +146,8 @@ __host__ __device__ __forceinline__ double2 zdiv(double2 a, double2 b) {
   return z2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
 }
 __device__ __forceinline__ float2 to_f2(double2 a) { return make_float2((float)a.x, (float)a.y); }
+// fp64 value to the march's complex type (rounded to complex64 in the normal build)
+__host__ __device__ __forceinline__ cx to_cx(double2 a) { return mkcx((rx)a.x, (rx)a.y); }
 __device__ __forceinline__ double2 shfl_up_z(double2 v, int d) {
   return z2(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d));
 }
