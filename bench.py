@@ -28,6 +28,7 @@ Multi-GPU (weak scaling: 512 probes per rank, gradient all-reduced over NCCL):
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -62,7 +63,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-3d", action="store_true", help="skip the 3D learned-vs-plain section")
     ap.add_argument("--ms-nz", type=int, default=0, help="3d-ms case: use the first N z nodes only")
-    ap.add_argument("--case", choices=("headline", "3d-march-small", "3d-recon", "3d-ms", "pit"), default="headline",
+    ap.add_argument("--step-by-step", action="store_true",
+                    help="3D cases: launch the march's kernels step by step instead of as one CUDA graph with "
+                         "conditional loops (the same kernels; profilers list the kernels of such graphs only "
+                         "as one workload)")
+    ap.add_argument("--case", choices=("headline", "3d-march-small", "3d-recon", "3d-ms", "pit", "kernels"),
+                    default="headline",
                     help="3d-march-small: a few learned 3D forward marches (256 x 256 x 5 nodes, 64 probes), "
                          "a small profiler target for the conv and FFT kernels; 3d-recon: `steps` gradient-descent "
                          "iterations of the 3D reconstruction (192 x 192 x 192, 256 probes), plain vs learned")
@@ -193,26 +199,39 @@ def _cpu_case(N, nz):
 
 def _cpu_sample(args):
     """Factorisation + per-probe fwd/adj march time of the CPU restatement over
-    the first `S` slices (the costs are linear in the slices)."""
+    the first `S` slices (the costs are linear in the slices).
+
+    The same per-slice arithmetic as the reference's IterativeLU path
+    (``build_lu_factors`` then ``march_with_lu``: one SuperLU of A − C_j and
+    B + C_j per slice and mode, u_j = LU_j⁻¹(B_j u_{j−1}), the adjoint from
+    the exit), but one slice's factor is held at a time: every SuperLU object
+    keeps its work memory, and holding all 2 × 1023 of them takes ~7 GB per
+    process.  Factorisation and march times are accumulated separately."""
     N, nz, probes_idx, seed, S = args
     from oracle import pwe_oracle as po
 
     geo, dn, probes, A, B = _cpu_case(N, nz)
     S = min(S, nz - 1)
-    t0 = time.perf_counter()
     C = po.object_contribution(1 - dn[:, : S + 1], geo.k, 1.0)
-    lf, bf = po.build_lu_factors(A, B, C, "forward")
-    la, ba = po.build_lu_factors(A, B, C, "adjoint")
-    t_fact = time.perf_counter() - t0
-    b0 = np.zeros(N, dtype=complex)
-    t1 = time.perf_counter()
-    for p in probes_idx:
-        u = po.march_with_lu(lf, bf, b0, probes[p])
-        rhs = np.zeros((N, S), dtype=complex)
-        rhs[:, -1] = u[:, -1]
-        po.march_with_lu(la, ba, b0, None, "adjoint", rhs)
-    t_probe = (time.perf_counter() - t1) / len(probes_idx)
-    return t_fact, t_probe
+    t_fact = 0.0
+    t_march = 0.0
+    exits = []
+    for mode in ("forward", "adjoint"):
+        states = [probes[p].astype(complex) for p in probes_idx] if mode == "forward" else \
+            [np.zeros(N, dtype=complex) for _ in probes_idx]
+        for j in range(1, S + 1):
+            col = j - 1 if mode == "forward" else S - j  # the slice of step j (adjoint: C[:, -j])
+            t0 = time.perf_counter()
+            (lu,), (Bw,) = po.build_lu_factors(A, B, C[:, col:col + 1], mode)
+            t1 = time.perf_counter()
+            for i in range(len(states)):
+                b = exits[i] if (mode == "adjoint" and j == 1) else 0.0  # rhs[:, -1] = the exit
+                states[i] = lu.solve(Bw @ states[i] + b)
+            t_fact += t1 - t0
+            t_march += time.perf_counter() - t1
+        if mode == "forward":
+            exits = list(states)
+    return t_fact, t_march / len(probes_idx)
 
 
 def cpu_rate(N, nz, P, cores, probes_per_worker, slices=None, pool=None):
@@ -611,6 +630,7 @@ def run_case_3d_small(a):
     field = torch.from_numpy((1 - ellipsoid_field_3d(w.nx, w.nx, nz, 10, w.seed)).reshape(-1, nz)).to(dev)
     model = LearnedPreconditioner(w.nx, w.nx, default_kappa(geo.k, 1.0, 5e-4), device=dev, seed=0)
     ex = torch.empty((P, eng.N), dtype=torch.complex64, device=dev)
+    eng.launch = 1 if a.step_by_step else 0
     ms = []
     for i in range(a.warmup + a.steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -793,6 +813,139 @@ def run_case_3d_recon(a):
           flush=True)
 
 
+def run_case_kernels(a):
+    """The kernels around the marches, each on a workload larger than L2 where
+    its data allows, timed with CUDA events (median of `steps` launches after
+    `warmup`) against its algorithmic bytes (or, for the network's weight
+    gradients, FLOPs): the target workload of their profiler captures.
+
+    * cn2d_factor_kernel: forward factor set of the 2048 x 1024 geometry
+      (reads two index columns per slice, complex128; writes 1023 slices);
+    * cn2d_grad_to_n_kernel: its gradient buffer mapped onto the index nodes;
+    * cn2d_refgrad_kernel / cn2d_alpha_source_kernel: the reference NLCG's
+      gradient contraction and step-size source on the 1024 x 512 geometry,
+      256 probes (reading stored forward and adjoint fields of 1.07 GB each);
+    * ms_march_kernel / ms_backward_kernel: 2D multislice, 2048 x 1024, 64
+      probes, forward keeping the field (1.07 GB) and the adjoint with the
+      gradient;
+    * ms_3pie_kernel: one 3PIE epoch of the 256 x 128 geometry, 32 probes (one
+      persistent CTA: sequential over probes, latency-bound);
+    * conv3x3_wgrad_kernel: weight gradients of the learned preconditioner's
+      four layers on 8 images of 256 x 256.
+    """
+    import torch
+
+    from thick_ptycho_b200.cn2d import CN2D
+    from thick_ptycho_b200.learned import LearnedPreconditioner, default_kappa
+    from thick_ptycho_b200.ms2d import MS2D, ReconstructorMSGpu
+    from thick_ptycho_b200.reconstruct import ReconstructorPWEGpu
+    from thick_ptycho_b200.workloads import CONFIG0, CONFIG1, CONFIG3
+
+    dev = torch.device("cuda", 0)
+    hbm, kind = peaks()
+    out = {"case": "kernels", "peak_gbs": hbm, "peak_kind": kind}
+
+    def timed(fn):
+        for _ in range(max(1, a.warmup)):
+            fn()
+        ms = []
+        for _ in range(max(1, a.steps)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms)
+
+    def report(name, ms, nbytes, note):
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        out[name] = {"ms": ms, "algorithmic_bytes": nbytes, "achieved_gbs": gbs, "frac": gbs / hbm, "note": note}
+
+    # 2D factorisation and node mapping, 2048 x 1024
+    w = CONFIG1
+    geo = w.geometry()
+    eng = CN2D(w.nx, w.nz, geo.k, 1.0, 1.0, "impedance", device=dev)
+    field = torch.from_numpy(1 - w.delta_n()).to(dev)
+    fbuf = eng.new_factor_buffer()
+    ms = timed(lambda: eng.factor(field, "forward", out=fbuf))
+    report("cn2d_factor_kernel", ms, 2 * w.nx * (w.nz - 1) * 16 + eng.factor_bytes,
+           "1023 slices of 2048 rows: fp64 elimination per chunk, PCR records; writes the factor set")
+    gc = eng.new_grad_buffer()
+    gc.copy_(torch.randn_like(gc))
+    gn = torch.empty((w.nx, w.nz), dtype=torch.complex64, device=dev)
+    ms = timed(lambda: eng.grad_to_n(gc))
+    report("cn2d_grad_to_n_kernel", ms, gc.numel() * 8 + gn.numel() * 8, "reads grad_c (L, Npad), writes (N, nz)")
+    del fbuf, gc, gn, field, eng
+    # reference NLCG pieces, 1024 x 512, 256 probes
+    w = CONFIG3
+    geo = w.geometry()
+    probes = w.probes(geo)
+    rec = ReconstructorPWEGpu(geo, np.abs(np.fft.fft(probes, axis=-1)) ** 2, probes, device=dev)
+    nk = torch.from_numpy(1 - w.delta_n()).to(dev)
+    ff = rec.forward_model(nk)
+    err = rec.exit_error()
+    rec.gradient(nk, err)
+    e = rec.engine
+    P = rec.P
+    u_bytes = rec._u.numel() * 8
+    ms = timed(lambda: e.lib.tp_cn2d_ref_gradient(e.op(), P, ctypes.c_void_p(rec._u.data_ptr()),
+                                                  ctypes.c_void_p(rec._lam.data_ptr()),
+                                                  ctypes.c_void_p(rec._gre.data_ptr()),
+                                                  ctypes.c_void_p(rec._gim.data_ptr()),
+                                                  ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    report("cn2d_refgrad_kernel", ms, 2 * u_bytes + 2 * rec._gre.numel() * 4,
+           "reads the stored forward and adjoint fields (256 probes), writes grad_re, grad_im")
+    ms = timed(lambda: e.lib.tp_cn2d_alpha_source(e.op(), P, ctypes.c_void_p(rec._u.data_ptr()),
+                                                  ctypes.c_void_p(rec._src.data_ptr()),
+                                                  ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    report("cn2d_alpha_source_kernel", ms, u_bytes + rec._src.numel() * 8,
+           "reads the stored forward field, writes the per-probe source (P, L, N)")
+    del rec, nk, ff, err
+    torch.cuda.empty_cache()
+    # 2D multislice, 2048 x 1024, 64 probes
+    w = CONFIG1
+    geo = w.geometry()
+    P = 64
+    ms2 = MS2D(w.nx, w.nz, geo.k, 1.0, 1.0, device=dev)
+    T = ms2.transmission(torch.from_numpy(1 + w.delta_n()).to(dev))
+    pr = torch.from_numpy(w.probes(geo)[:P].astype(np.complex64)).to(dev)
+    st = torch.empty((P, w.nz, w.nx), dtype=torch.complex64, device=dev)
+    ex = torch.empty((P, w.nx), dtype=torch.complex64, device=dev)
+    ms = timed(lambda: ms2.march(T, pr, u_store=st, exit_out=ex))
+    report("ms_march_kernel", ms, st.numel() * 8 + T.numel() * 8,
+           "64 probes x 1023 slices: two shared-memory FFTs per slice, writes the field")
+    gt = torch.zeros((w.nz - 1, w.nx), dtype=torch.complex64, device=dev)
+    ms = timed(lambda: ms2.backward(T, st, ex, gt))
+    report("ms_backward_kernel", ms, st.numel() * 8 + T.numel() * 8 + gt.numel() * 8,
+           "reads the forward field, accumulates the transmission gradient")
+    del st, gt, T, ms2
+    torch.cuda.empty_cache()
+    # 3PIE, 256 x 128, 32 probes (sequential)
+    w = CONFIG0
+    geo = w.geometry()
+    probes = w.probes(geo)
+    data = np.abs(np.fft.fft(probes, axis=-1)) ** 2
+    pie = ReconstructorMSGpu(w.nx, w.nz, geo.k, 1.0, 1.0, data, probes, device=dev)
+    ms = timed(lambda: pie.reconstruct(max_iters=1, alpha_obj=0.1))
+    out["ms_3pie_kernel"] = {"ms": ms, "probe_slices_per_s": w.num_probes * (w.nz - 1) / (ms * 1e-3),
+                             "note": "one CTA, 32 probes in sequence, forward + modulus + backward per probe"}
+    # learned-preconditioner weight gradients, 8 images of 256 x 256
+    nf = 256
+    model = LearnedPreconditioner(nf, nf, default_kappa(4 * np.pi, 1.0, 5e-4), device=dev, seed=0)
+    B = 8
+    g = torch.Generator(device=dev).manual_seed(0)
+    diag = (1e-3 * torch.randn((B, nf * nf), dtype=torch.complex64, device=dev, generator=g)).contiguous()
+    z = torch.randn((B, nf * nf), dtype=torch.complex64, device=dev, generator=g)
+    tgt = torch.randn((B, nf * nf), dtype=torch.complex64, device=dev, generator=g)
+    scale = torch.ones(B, dtype=torch.float32, device=dev)
+    ms = timed(lambda: model.loss_and_grads(diag, z, tgt, scale, 1))
+    flops = 2 * B * nf * nf * 9 * (16 * 32 + 3 * 32 * 32)
+    out["cnn_loss_and_grads"] = {"ms": ms, "wgrad_flops": flops,
+                                 "note": "filter, filter gradient, 3 masked data-gradient convs, 4 weight gradients"}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -805,6 +958,8 @@ def main():
         run_case_3d_ms(a)
     elif a.case == "pit":
         run_case_pit(a)
+    elif a.case == "kernels":
+        run_case_kernels(a)
     else:
         run_ours(a)
 
