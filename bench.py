@@ -63,6 +63,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-3d", action="store_true", help="skip the 3D learned-vs-plain section")
     ap.add_argument("--ms-nz", type=int, default=0, help="3d-ms case: use the first N z nodes only")
+    ap.add_argument("--pairs", choices=("mixed", "noise", "noise20k"), default="mixed",
+                    help="training pairs of the learned preconditioner (3D cases)")
+    ap.add_argument("--small", action="store_true",
+                    help="kernels case: 64 probes for the NLCG pieces and 16 for the multislice (~1 GB on the "
+                         "device; the size of the profiler captures)")
     ap.add_argument("--step-by-step", action="store_true",
                     help="3D cases: launch the march's kernels step by step instead of as one CUDA graph with "
                          "conditional loops (the same kernels; profilers list the kernels of such graphs only "
@@ -369,7 +374,57 @@ def run_reference(a):
 # --------------------------------------------------------------------------
 # 3D: learned vs plain FFT-preconditioned BiCGStab (fwd + exact adjoint)
 # --------------------------------------------------------------------------
-def bench_learned_3d(dev, reps=2, train_probes=40, train_steps=1500):
+PAIR_KINDS = {
+    "mixed": "10 200 white-noise pairs (x, (I - P_s) x) and 10 200 step pairs (the step's right-hand side, its "
+             "converged update), 40 probes x 255 slices each, of a different seeded field",
+    "noise": "10 200 white-noise pairs (x, (I - P_s) x), 40 probes x 255 slices, of a different seeded field",
+    "noise20k": "20 400 white-noise pairs (x, (I - P_s) x), 80 probe slots x 255 slices, of a different seeded "
+                "field",
+}
+
+
+def train_learned(eng, geo, w, probes, kind, steps, dev):
+    """The learned preconditioner trained on solver-generated pairs of another
+    seeded field (`kind`, see PAIR_KINDS); returns the model and what it was
+    trained on.  Not timed."""
+    import torch
+
+    from thick_ptycho_b200.cn3d import generate_pairs
+    from thick_ptycho_b200.learned import LearnedPreconditioner, default_kappa
+    from thick_ptycho_b200.workloads import ellipsoid_field_3d
+
+    n, nz = w.nx, w.nz
+    t0 = time.perf_counter()
+    ftrain = torch.from_numpy((1 - ellipsoid_field_3d(n, n, nz, w.n_shapes, 1001)).reshape(n * n, nz)).to(dev)
+    sets = []
+    if kind in ("noise", "mixed"):
+        sets.append(generate_pairs(eng, ftrain, probes[:40].contiguous(), every=1, kind="noise"))
+    if kind == "mixed":
+        sets.append(generate_pairs(eng, ftrain, probes[-40:].contiguous(), every=1, kind="rhs"))
+    if kind == "noise20k":
+        slots = torch.cat([probes, probes])[:80].contiguous()
+        sets.append(generate_pairs(eng, ftrain, slots, every=1, kind="noise"))
+    del ftrain
+    model = LearnedPreconditioner(n, n, default_kappa(geo.k, 1.0, 5e-4), device=dev, seed=0)
+    model.train(sets, steps=steps * len(sets), slices_per_batch=2, lr=1e-3)
+    torch.cuda.synchronize(dev)
+    info = {"pairs": sum(ps.count for ps in sets), "kind": PAIR_KINDS[kind], "steps": steps * len(sets),
+            "seconds": time.perf_counter() - t0, "not_timed": True}
+    del sets
+    torch.cuda.empty_cache()
+    return model, info
+
+
+def fixture_exit_error(name, ex):
+    """Relative L2 error of the exit waves `ex` (P, N) against the complex128
+    oracle fixture of the geometry (its three checked probes)."""
+    with np.load(os.path.join(ROOT, "tests", "golden", f"{name}_3d_full.npz")) as g:
+        idx, ref = [int(i) for i in g["probe_idx"]], g["exit"].astype(np.complex128)
+    got = ex[idx].cpu().numpy().astype(np.complex128)
+    return float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+
+
+def bench_learned_3d(dev, reps=2, train_steps=1500, pairs="mixed"):
     """fwd + adj probe·slice solves/s of the plain and the learned 3D forms.
 
     Workload: 256 x 256 transverse x 256 nodes, 64 probes (8 x 8 raster,
@@ -377,14 +432,14 @@ def bench_learned_3d(dev, reps=2, train_probes=40, train_steps=1500):
     edges, BiCGStab to a 1e-6 relative residual per solve.  One step = a
     forward march storing the full field + an exact-adjoint march with the
     fused gradient, all 64 probes batched.  The network is trained first on
-    solver-generated white-noise pairs (every slice of a different seeded
-    field, `train_probes` probes); training time is reported, not timed.
+    solver-generated pairs of a different seeded field (`pairs`, see
+    PAIR_KINDS); training time is reported, not timed.  Each form's exit
+    waves are compared with the complex128 oracle fixture of the geometry.
     """
     import torch
 
-    from thick_ptycho_b200.cn3d import CN3D, generate_pairs
-    from thick_ptycho_b200.learned import LearnedPreconditioner, default_kappa
-    from thick_ptycho_b200.workloads import CONFIG2, ellipsoid_field_3d
+    from thick_ptycho_b200.cn3d import CN3D
+    from thick_ptycho_b200.workloads import CONFIG2
 
     w = CONFIG2
     geo = w.geometry()
@@ -395,17 +450,7 @@ def bench_learned_3d(dev, reps=2, train_probes=40, train_steps=1500):
     probes = torch.from_numpy(w.probes(geo).reshape(P, N).astype(np.complex64)).to(dev)
     stream = torch.cuda.current_stream(dev)
 
-    t0 = time.perf_counter()
-    ftrain = torch.from_numpy((1 - ellipsoid_field_3d(n, n, nz, w.n_shapes, 1001)).reshape(N, nz)).to(dev)
-    pairs = generate_pairs(eng, ftrain, probes[:train_probes].contiguous(), every=1, kind="noise")
-    del ftrain
-    model = LearnedPreconditioner(n, n, default_kappa(geo.k, 1.0, 5e-4), device=dev, seed=0)
-    model.train(pairs, steps=train_steps, slices_per_batch=2, lr=1e-3)
-    torch.cuda.synchronize(dev)
-    train_s = time.perf_counter() - t0
-    npairs = pairs.count
-    del pairs
-    torch.cuda.empty_cache()
+    model, training = train_learned(eng, geo, w, probes, pairs, train_steps, dev)
 
     store = eng.new_store(P)
     ex = torch.empty((P, N), dtype=torch.complex64, device=dev)
@@ -433,15 +478,14 @@ def bench_learned_3d(dev, reps=2, train_probes=40, train_steps=1500):
         exits[name] = ex.clone()
         out[name] = {"value": P * L / (t / 1e3), "ms_per_step": t,
                      "krylov_iterations_per_solve": st["iterations"] / max(st["solves"], 1),
-                     "failed_solves": st["failed"]}
+                     "failed_solves": st["failed"], "graph": st["graph"],
+                     "exit_rel_error_vs_fp64_fixture": fixture_exit_error("config2", ex)}
     diff = float(torch.linalg.vector_norm(exits["learned"] - exits["plain"]) / torch.linalg.vector_norm(exits["plain"]))
     return {
         "workload": w.name, "metric": "probe·slice solves/s fwd+adj (3D BiCGStab, exact adjoint + gradient)",
         "unit": UNIT, "plain": out["plain"], "learned": out["learned"],
         "learned_over_plain": out["learned"]["value"] / out["plain"]["value"],
-        "exit_rel_diff_learned_vs_plain": diff, "fallbacks": eng.fallbacks,
-        "training": {"pairs": npairs, "kind": "white-noise pairs (x, (I - P_s) x) of a different seeded field",
-                     "steps": train_steps, "seconds": train_s, "not_timed": True},
+        "exit_rel_diff_learned_vs_plain": diff, "fallbacks": eng.fallbacks, "training": training,
     }
 
 
@@ -598,7 +642,7 @@ def run_ours(a):
             "clocks": clk.summary(),
         }
         if world == 1 and not a.no_3d:
-            line["learned_vs_plain_3d"] = bench_learned_3d(dev)
+            line["learned_vs_plain_3d"] = bench_learned_3d(dev, pairs=a.pairs)
         if world == 1 and not a.no_cpu_baseline:
             v, tf, tp, wall = cpu_rate(N, nz, P, 1, 2)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
@@ -773,17 +817,15 @@ def run_case_3d_recon(a):
     truth = PWEGradient3D(geo, device=dev)
     ex = truth.forward(torch.from_numpy(1 - dn_true).to(dev), probes)
     amp = heads.fft2_last(ex.reshape(P, n, n).contiguous()).abs().to(torch.float64)
+    fixture_err = {"plain": fixture_exit_error("config4", ex)}
     del truth, ex
-    t0 = time.perf_counter()
     eng = CN3D(n, n, nz, geo.k, 1.0, 1.0, 1.0, "impedance", device=dev)
-    pairs = generate_pairs(eng, torch.from_numpy((1 - ellipsoid_field_3d(n, n, nz, w.n_shapes, 1001)).reshape(N, nz)).to(dev),
-                           probes[:40].contiguous(), every=1, kind="noise")
-    model = LearnedPreconditioner(n, n, default_kappa(geo.k, 1.0, 5e-4), device=dev, seed=0)
-    model.train(pairs, steps=1500, slices_per_batch=2, lr=1e-3)
-    torch.cuda.synchronize(dev)
-    train_s = time.perf_counter() - t0
-    del pairs, eng
-    torch.cuda.empty_cache()
+    model, training = train_learned(eng, geo, w, probes, a.pairs, 1500, dev)
+    del eng
+    # the learned form's exit waves of the ground truth against the same fixture
+    lt = PWEGradient3D(geo, device=dev, precond="learned", model=model)
+    fixture_err["learned"] = fixture_exit_error("config4", lt.forward(torch.from_numpy(1 - dn_true).to(dev), probes))
+    del lt
     n0 = np.ones((N, nz), dtype=complex)
     res = {}
     for name, pc in (("plain", True), ("learned", "learned")):
@@ -809,7 +851,7 @@ def run_case_3d_recon(a):
                       "metric": "probe·slice solves/s fwd+adj (3D gradient descent)", "plain": res["plain"],
                       "learned": res["learned"], "learned_over_plain": res["learned"]["value"] / res["plain"]["value"],
                       "n_diff_learned_vs_plain_rel_update": diff,
-                      "training": {"seconds": train_s, "pairs": 191 * 40, "steps": 1500, "not_timed": True}}),
+                      "truth_exit_rel_error_vs_fp64_fixture": fixture_err, "training": training}),
           flush=True)
 
 
@@ -832,6 +874,9 @@ def run_case_kernels(a):
       persistent CTA: sequential over probes, latency-bound);
     * conv3x3_wgrad_kernel: weight gradients of the learned preconditioner's
       four layers on 8 images of 256 x 256.
+
+    ``--small``: 64 of the NLCG probes and 16 multislice probes (stored fields
+    of 268 MB, still larger than L2).
     """
     import torch
 
@@ -880,7 +925,7 @@ def run_case_kernels(a):
     # reference NLCG pieces, 1024 x 512, 256 probes
     w = CONFIG3
     geo = w.geometry()
-    probes = w.probes(geo)
+    probes = w.probes(geo)[: 64 if a.small else w.num_probes]
     rec = ReconstructorPWEGpu(geo, np.abs(np.fft.fft(probes, axis=-1)) ** 2, probes, device=dev)
     nk = torch.from_numpy(1 - w.delta_n()).to(dev)
     ff = rec.forward_model(nk)
@@ -895,7 +940,7 @@ def run_case_kernels(a):
                                                   ctypes.c_void_p(rec._gim.data_ptr()),
                                                   ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
     report("cn2d_refgrad_kernel", ms, 2 * u_bytes + 2 * rec._gre.numel() * 4,
-           "reads the stored forward and adjoint fields (256 probes), writes grad_re, grad_im")
+           f"reads the stored forward and adjoint fields ({P} probes), writes grad_re, grad_im")
     ms = timed(lambda: e.lib.tp_cn2d_alpha_source(e.op(), P, ctypes.c_void_p(rec._u.data_ptr()),
                                                   ctypes.c_void_p(rec._src.data_ptr()),
                                                   ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
@@ -906,7 +951,7 @@ def run_case_kernels(a):
     # 2D multislice, 2048 x 1024, 64 probes
     w = CONFIG1
     geo = w.geometry()
-    P = 64
+    P = 16 if a.small else 64
     ms2 = MS2D(w.nx, w.nz, geo.k, 1.0, 1.0, device=dev)
     T = ms2.transmission(torch.from_numpy(1 + w.delta_n()).to(dev))
     pr = torch.from_numpy(w.probes(geo)[:P].astype(np.complex64)).to(dev)
@@ -914,7 +959,7 @@ def run_case_kernels(a):
     ex = torch.empty((P, w.nx), dtype=torch.complex64, device=dev)
     ms = timed(lambda: ms2.march(T, pr, u_store=st, exit_out=ex))
     report("ms_march_kernel", ms, st.numel() * 8 + T.numel() * 8,
-           "64 probes x 1023 slices: two shared-memory FFTs per slice, writes the field")
+           f"{P} probes x 1023 slices: two shared-memory FFTs per slice, writes the field")
     gt = torch.zeros((w.nz - 1, w.nx), dtype=torch.complex64, device=dev)
     ms = timed(lambda: ms2.backward(T, st, ex, gt))
     report("ms_backward_kernel", ms, st.numel() * 8 + T.numel() * 8 + gt.numel() * 8,
