@@ -166,15 +166,16 @@ __device__ __forceinline__ void block_reduce_add(double v, double *dst, double *
   __syncthreads();
 }
 
-// Grid (chunks, P).  r = r0 = rhs = (P_l + P_r) u + src; x = p = v = 0.  The
+// Grid (chunks, P).  r0 = rhs = (P_l + P_r) u + src and its norm; the first
+// iteration reads r0 as r and takes x = p = v = 0 without reading them.  The
 // step t decides the terms: the exact adjoint's right-hand side uses the next
 // slice's operator (cdr) and has no u term at t = 1 (lambda_{L+1} = 0); the
 // per-probe source enters at t = 1; src_shared is (L, N) by step.
 __global__ void __launch_bounds__(k3Threads) c3_init_kernel(const C3Params q, const C3State *st, int adj_exact,
                                                             const float2 *__restrict__ cdl, const float2 *__restrict__ cdn,
                                                             const float2 *__restrict__ u, const float2 *__restrict__ src_exit,
-                                                            const float2 *__restrict__ src_shared, float2 *x, float2 *r,
-                                                            float2 *r0, float2 *p, float2 *v, Krylov *K) {
+                                                            const float2 *__restrict__ src_shared, float2 *r0,
+                                                            Krylov *K) {
   __shared__ double red[k3Threads / 32];
   const int pr = blockIdx.y;
   const size_t off = (size_t)pr * q.N;
@@ -188,12 +189,7 @@ __global__ void __launch_bounds__(k3Threads) c3_init_kernel(const C3Params q, co
     float2 b = use_u ? cadd(apply_P(q, cdl, u + off, i), apply_P(q, cdr, u + off, i)) : make_float2(0.f, 0.f);
     if (src != nullptr) b = cadd(b, src[off + i]);
     if (shared != nullptr) b = cadd(b, shared[i]);
-    r[off + i] = b;
     r0[off + i] = b;
-    const float2 z = make_float2(0.f, 0.f);
-    x[off + i] = z;
-    p[off + i] = z;
-    v[off + i] = z;
     acc += (double)b.x * b.x + (double)b.y * b.y;
   }
   block_reduce_add(acc, &K[pr].bnorm2, red);
@@ -278,12 +274,16 @@ __global__ void c3_symbol_kernel(const C3Params q, float2 *sym) {
 //   mode 0: p := r + beta (p - omega v)  (p updated in place), input p
 //   mode 1: s := r - alpha v             (s written),          input s
 //   mode 2: input r as is (K may be NULL: every probe is transformed)
+// The first iteration of a step (st->it == 0) starts from x = p = v = 0 and
+// r = r0, which the step head does not write: mode 0 takes p = r0 (and does
+// not store it: the second iteration reads r0 as its p), mode 1 reads r0 as r.
 // Grid (nb / rpc, P).
 template <int NF>
 __global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan pl, const C3Params q, int mode,
                                                                  const float2 *r, float2 *p, const float2 *v, float2 *s,
                                                                  float2 *hat, const Krylov *K, int rpc, int fft_on,
-                                                                 const float2 *twg) {
+                                                                 const float2 *twg, const float2 *r0,
+                                                                 const C3State *st) {
   extern __shared__ __align__(16) float2 fsm[];
   const int n = NF > 0 ? NF : q.nf, pr = blockIdx.y;
   if (K != nullptr && K[pr].done) return;
@@ -298,23 +298,34 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan p
       else hat[off + e] = r[off + e];
     }
   } else if (mode == 0) {
-    const Krylov &k = K[pr];
-    const double den = k.rho_prev.x * k.rho_prev.x + k.rho_prev.y * k.rho_prev.y;
-    const double2 beta = den > 0.0 ? zmul(zdiv(k.rho_cur, k.rho_prev), zdiv(k.alpha, k.omega)) : z2(0, 0);
-    const float2 bt = to_f2(beta), om = to_f2(k.omega);
-    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
-      const float2 pv = cfma(bt, cfnma(om, v[off + e], p[off + e]), r[off + e]);
-      p[off + e] = pv;
-      if (fft_on) a[slot(e)] = pv;
-      else hat[off + e] = pv;
+    const int it = st->it;
+    if (it == 0) {
+      for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+        const float2 pv = r0[off + e];
+        if (fft_on) a[slot(e)] = pv;
+        else hat[off + e] = pv;
+      }
+    } else {
+      const Krylov &k = K[pr];
+      const double den = k.rho_prev.x * k.rho_prev.x + k.rho_prev.y * k.rho_prev.y;
+      const double2 beta = den > 0.0 ? zmul(zdiv(k.rho_cur, k.rho_prev), zdiv(k.alpha, k.omega)) : z2(0, 0);
+      const float2 bt = to_f2(beta), om = to_f2(k.omega);
+      const float2 *pin = (it == 1) ? r0 : p;
+      for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+        const float2 pv = cfma(bt, cfnma(om, v[off + e], pin[off + e]), r[off + e]);
+        p[off + e] = pv;
+        if (fft_on) a[slot(e)] = pv;
+        else hat[off + e] = pv;
+      }
     }
   } else {
     const Krylov &k = K[pr];
     const double den = k.acc_r0v.x * k.acc_r0v.x + k.acc_r0v.y * k.acc_r0v.y;
     const double2 alpha = den > 0.0 ? zdiv(k.rho_cur, k.acc_r0v) : z2(0, 0);
     const float2 al = to_f2(alpha);
+    const float2 *rin = (st->it == 0) ? r0 : r;
     for (int e = threadIdx.x; e < tot; e += blockDim.x) {
-      const float2 sv = cfnma(al, v[off + e], r[off + e]);
+      const float2 sv = cfnma(al, v[off + e], rin[off + e]);
       s[off + e] = sv;
       if (fft_on) a[slot(e)] = sv;
       else hat[off + e] = sv;
@@ -382,101 +393,6 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_inv_kernel(const FftPl
   for (int e = threadIdx.x; e < tot; e += blockDim.x) out[off + e] = res[slot(e)];
 }
 
-// Inverse row FFTs, the learned correction and the matvec in one pass.  A CTA
-// owns rows [b0, b0 + rpc) of one probe's nb x nf plane.  It transforms the
-// rows [b0 - H, b0 + rpc + H) of hat (H = 1; 3 with the learned filter,
-// whose taps reach 2 rows and feed a matvec that reaches 1 more), so that
-// every operand it needs is in shared memory: z = the plain preconditioned
-// rows; LEARNED: y = z + sum_t F_t z(x + o_t) (conj(F) in the adjoint modes)
-// on rows [b0 - 1, b0 + rpc + 1), built in the FFT's free ping-pong buffer;
-// else y = z.  For its own rows it writes y and mv = (I - P) y and adds the
-// fp64 dots of c3_matvec_kernel (which 0: <r0, mv>; 1: <mv, s>, <mv, mv>).
-// Halo rows are transformed by both neighbouring CTAs with the same
-// operations, so every CTA sees the same values.  Grid (nb / rpc, P).
-template <int NF, bool LEARNED>
-__global__ void __launch_bounds__(k3Threads) c3_inv_apply_kernel(const FftPlan pl, const C3Params q,
-                                                                 const float2 *__restrict__ hat, float2 *out,
-                                                                 float2 *mv, const float2 *__restrict__ cd,
-                                                                 const float2 *__restrict__ r0,
-                                                                 const float2 *__restrict__ s, Krylov *K, int which,
-                                                                 int rpc, const float2 *__restrict__ twg,
-                                                                 const C3State *st, int chunk,
-                                                                 const float2 *__restrict__ Fall) {
-  extern __shared__ __align__(16) float2 fsm[];
-  __shared__ double red[k3Threads / 32];
-  const int n = NF > 0 ? NF : q.nf, pr = blockIdx.y;
-  if (K[pr].done) return;
-  constexpr int H = LEARNED ? 3 : 1;
-  const int b0 = blockIdx.x * rpc;
-  const int rlo = b0 - H < 0 ? 0 : b0 - H, rhi = b0 + rpc + H > q.nb ? q.nb : b0 + rpc + H, R = rhi - rlo;
-  const int sr = fstride<NF>(n);
-  float2 *tw = fsm, *a = tw + n, *b = a + (rpc + 2 * H) * sr;
-  const size_t poff = (size_t)pr * q.N;
-  load_twiddles(tw, twg, n);
-  for (int e = threadIdx.x; e < R * n; e += blockDim.x)
-    cp_async8(&a[fslot<NF>(e / n, e % n, n)], &hat[poff + (size_t)rlo * n + e]);
-  cp_async_wait_all();
-  __syncthreads();
-  const float2 *zr = fft_rows<NF>(a, b, pl, tw, true, R);  // ends with a barrier
-  auto zat = [&](int row, int f) { return zr[fslot<NF>(row - rlo, f, n)]; };
-  // y on rows [ylo, yhi): in the free buffer (learned) or read from z
-  const int ylo = b0 - 1 < 0 ? 0 : b0 - 1, yhi = b0 + rpc + 1 > q.nb ? q.nb : b0 + rpc + 1;
-  float2 *Y = (zr == a) ? b : a;
-  if constexpr (LEARNED) {
-    const int sl = st->s - 1;
-    const size_t np = (size_t)chunk * q.N;
-    const float2 *F = Fall + (size_t)(sl / chunk) * kFilterTaps * np + (size_t)(sl % chunk) * q.N;
-    for (int e = threadIdx.x; e < (yhi - ylo) * n; e += blockDim.x) {
-      const int row = ylo + e / n, f = e % n;
-      const size_t i = (size_t)row * n + f;
-      float2 acc = zat(row, f);
-#pragma unroll
-      for (int t = 0; t < kFilterTaps; ++t) {
-        const int rr = row + filter_tap_dy(t), ff = f + filter_tap_dx(t);
-        if (rr < 0 || rr >= q.nb || ff < 0 || ff >= n) continue;
-        float2 w = F[(size_t)t * np + i];
-        if (q.conj_t) w.y = -w.y;
-        acc = cfma(w, zat(rr, ff), acc);
-      }
-      Y[(row - ylo) * n + f] = acc;
-    }
-    __syncthreads();
-  }
-  auto yat = [&](int row, int f) { return LEARNED ? Y[(row - ylo) * n + f] : zat(row, f); };
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-  for (int e = threadIdx.x; e < rpc * n; e += blockDim.x) {
-    const int row = b0 + e / n, f = e % n;
-    const int i = row * n + f;
-    const float2 y = yat(row, f);
-    float2 p = cmul(cd[i], y);
-    if (f > 0) p = cfma(q.kw[i], yat(row, f - 1), p);
-    if (f < n - 1) p = cfma(q.ke[i], yat(row, f + 1), p);
-    if (row > 0) p = cfma(q.ks[i], yat(row - 1, f), p);
-    if (row < q.nb - 1) p = cfma(q.kn[i], yat(row + 1, f), p);
-    const float2 t = csub(y, p);
-    out[poff + i] = y;
-    mv[poff + i] = t;
-    const float2 c = (which == 0) ? r0[poff + i] : s[poff + i];
-    if (which == 0) {  // conj(r0) t
-      a0 += (double)c.x * t.x + (double)c.y * t.y;
-      a1 += (double)c.x * t.y - (double)c.y * t.x;
-    } else {  // conj(t) s, |t|^2
-      a0 += (double)t.x * c.x + (double)t.y * c.y;
-      a1 += (double)t.x * c.y - (double)t.y * c.x;
-      a2 += (double)t.x * t.x + (double)t.y * t.y;
-    }
-  }
-  Krylov &k = K[pr];
-  if (which == 0) {
-    block_reduce_add(a0, &k.acc_r0v.x, red);
-    block_reduce_add(a1, &k.acc_r0v.y, red);
-  } else {
-    block_reduce_add(a0, &k.acc_ts.x, red);
-    block_reduce_add(a1, &k.acc_ts.y, red);
-    block_reduce_add(a2, &k.acc_tt, red);
-  }
-}
-
 // out = (I - P) y with fused fp64 dots: which 0: acc_r0v += <r0, out>;
 // which 1: acc_ts += <out, s>, acc_tt += <out, out>.
 __global__ void __launch_bounds__(k3Threads) c3_matvec_kernel(const C3Params q, const float2 *__restrict__ cd,
@@ -512,12 +428,14 @@ __global__ void __launch_bounds__(k3Threads) c3_matvec_kernel(const C3Params q, 
   }
 }
 
-// omega = <t,s>/<t,t>; x += alpha y + omega z; r = s - omega t; accumulate
-// <r0, r> and ||r||^2 for the next iteration.
+// omega = <t,s>/<t,t>; x += alpha y + omega z (x = 0 before the first
+// iteration of a step: not read then); r = s - omega t; accumulate <r0, r>
+// and ||r||^2 for the next iteration.
 __global__ void __launch_bounds__(k3Threads) c3_update_kernel(const C3Params q, float2 *x, float2 *r,
                                                               const float2 *__restrict__ r0, const float2 *__restrict__ y,
                                                               const float2 *__restrict__ z, const float2 *__restrict__ s,
-                                                              const float2 *__restrict__ t, Krylov *K) {
+                                                              const float2 *__restrict__ t, Krylov *K,
+                                                              const C3State *st) {
   __shared__ double red[k3Threads / 32];
   const int pr = blockIdx.y;
   Krylov &k = K[pr];
@@ -527,9 +445,11 @@ __global__ void __launch_bounds__(k3Threads) c3_update_kernel(const C3Params q, 
   const double2 alpha = den > 0.0 ? zdiv(k.rho_cur, k.acc_r0v) : z2(0, 0);
   const double2 omega = (k.acc_tt > 0.0) ? zscale(k.acc_ts, 1.0 / k.acc_tt) : z2(0, 0);
   const float2 al = to_f2(alpha), om = to_f2(omega);
+  const bool first = st->it == 0;
   double a0 = 0.0, a1 = 0.0, a2 = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
-    x[off + i] = cfma(om, z[off + i], cfma(al, y[off + i], x[off + i]));
+    const float2 x0 = first ? make_float2(0.f, 0.f) : x[off + i];
+    x[off + i] = cfma(om, z[off + i], cfma(al, y[off + i], x0));
     const float2 rv = cfnma(om, t[off + i], s[off + i]);
     r[off + i] = rv;
     const float2 c = r0[off + i];
@@ -557,10 +477,13 @@ __global__ void __launch_bounds__(k3Threads) c3_finish_kernel(const C3Params q, 
   const int t = st->t;
   float2 *dst = u_store ? u_store + ((size_t)pr * q.nz + (flip ? q.L - t : t)) * q.N : nullptr;
   float2 *ex = (exit_out && t == q.L) ? exit_out + off : nullptr;
+  // a probe whose right-hand side was zero did not iterate: its update is 0
+  // (x then holds an earlier step's values)
+  const bool iterated = K[pr].iters > 0;
   double acc = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
-    const float2 xi = x[off + i];
-    const float2 mx = csub(xi, apply_P(q, cd, x + off, i));
+    const float2 xi = iterated ? x[off + i] : make_float2(0.f, 0.f);
+    const float2 mx = iterated ? csub(xi, apply_P(q, cd, x + off, i)) : xi;
     const float2 d = csub(r0[off + i], mx);
     acc += (double)d.x * d.x + (double)d.y * d.y;
     const float2 un = cadd(u[off + i], xi);
@@ -727,25 +650,20 @@ static C3Work c3_layout(char *base, int N, int P) {
 }
 
 using RowsKernel = void (*)(const FftPlan, const C3Params, int, const float2 *, float2 *, const float2 *, float2 *,
-                           float2 *, const Krylov *, int, int, const float2 *);
+                           float2 *, const Krylov *, int, int, const float2 *, const float2 *, const C3State *);
 using ColsKernel = void (*)(const FftPlan, const C3Params, float2 *, const Krylov *, int, const float2 *,
                            const float2 *);
 using InvKernel = void (*)(const FftPlan, const C3Params, const float2 *, float2 *, const Krylov *, int, const float2 *);
-using ApplyKernel = void (*)(const FftPlan, const C3Params, const float2 *, float2 *, float2 *, const float2 *,
-                             const float2 *, const float2 *, Krylov *, int, int, const float2 *, const C3State *, int,
-                             const float2 *);
 struct PrecKernels {
   RowsKernel rows;
   ColsKernel cols;
   InvKernel inv;
-  ApplyKernel apply, apply_learned;  // inverse rows + matvec (+ the learned filter)
   int fixed;  // compile-time plans in the padded shared-memory layout
 };
 
 template <int NF, int NB>
 static PrecKernels prec_kernels_t() {
-  return {c3_prec_rows_kernel<NF>, c3_prec_cols_kernel<NB>, c3_prec_rows_inv_kernel<NF>,
-          c3_inv_apply_kernel<NF, false>, c3_inv_apply_kernel<NF, true>, NF > 0 ? 1 : 0};
+  return {c3_prec_rows_kernel<NF>, c3_prec_cols_kernel<NB>, c3_prec_rows_inv_kernel<NF>, NF > 0 ? 1 : 0};
 }
 
 // Square transverse grids of the common sizes get compile-time FFT plans.
@@ -936,15 +854,10 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   const int srow_f = pk.fixed ? nf + nf / 8 + 1 : nf, srow_b = pk.fixed ? nb + nb / 8 + 1 : nb;
   const size_t smem_rows = (size_t)(nf + 2 * rpc * srow_f) * sizeof(float2);
   const size_t smem_cols = (size_t)(nb + 2 * cpc * srow_b) * sizeof(float2);
-  // the fused inverse-rows + matvec kernel transforms H halo rows on each side
-  const int halo = learned ? 3 : 1;
-  const size_t smem_apply = (size_t)(nf + 2 * (rpc + 2 * halo) * srow_f) * sizeof(float2);
-  const ApplyKernel apply_k = learned ? pk.apply_learned : pk.apply;
   if (use_fft) {
     TP_CHECK_CUDA(cudaFuncSetAttribute(pk.rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
     TP_CHECK_CUDA(cudaFuncSetAttribute(pk.inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
     TP_CHECK_CUDA(cudaFuncSetAttribute(pk.cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cols));
-    TP_CHECK_CUDA(cudaFuncSetAttribute(apply_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_apply));
   }
   const int rows_cta = use_fft ? rpc : 1;
   const int max_iter = a->max_iter > 0 ? a->max_iter : 20;
@@ -966,7 +879,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   // M0^{-1} in -> out (mode 0/1/2 input of the row kernel; Kp NULL = all probes)
   auto precondition = [&](cudaStream_t s, int mode, const float2 *rin, float2 *out, const Krylov *Kp) {
     pk.rows<<<dim3(nb / rows_cta, P), k3Threads, use_fft ? smem_rows : 0, s>>>(
-        pf, q, mode, rin, w.p, w.v, w.s, use_fft ? w.hat : out, Kp, rows_cta, use_fft, w.twf);
+        pf, q, mode, rin, w.p, w.v, w.s, use_fft ? w.hat : out, Kp, rows_cta, use_fft, w.twf, w.r0, w.st);
     if (use_fft) {
       pk.cols<<<dim3(nf / cpc, P), k3Threads, smem_cols, s>>>(pb, q, w.hat, Kp, cpc, w.twb, w.sym);
       pk.inv<<<dim3(nb / rpc, P), k3Threads, smem_rows, s>>>(pf, q, w.hat, out, Kp, rpc, w.twf);
@@ -1013,29 +926,11 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     if (adj_exact) c3_center_kernel<<<eb, 256, 0, s>>>(q, w.st, 1, w.cdr);
     c3_init_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.st, adj_exact, w.cdl, w.cdr, w.u,
                                                 static_cast<const float2 *>(a->src_exit),
-                                                static_cast<const float2 *>(a->src_shared), w.x, w.r, w.r0, w.p, w.v,
-                                                w.K);
+                                                static_cast<const float2 *>(a->src_shared), w.r0, w.K);
     c3_start_kernel<<<pgrid, 128, 0, s>>>(w.K, P);
   };
   // one BiCGStab iteration of every pending probe
   auto iteration = [&](cudaStream_t s, int use_cond, cudaGraphConditionalHandle inner) {
-    if (use_fft) {
-      // p = r + beta (p - omega v); forward row and column passes of Prec(p);
-      // then y = Prec(p) (learned: with the filter) and v = M y in one kernel
-      const dim3 rg(nb / rpc, P);
-      pk.rows<<<rg, k3Threads, smem_rows, s>>>(pf, q, 0, w.r, w.p, w.v, w.s, w.hat, w.K, rpc, 1, w.twf);
-      pk.cols<<<dim3(nf / cpc, P), k3Threads, smem_cols, s>>>(pb, q, w.hat, w.K, cpc, w.twb, w.sym);
-      apply_k<<<rg, k3Threads, smem_apply, s>>>(pf, q, w.hat, w.y, w.v, w.cdl, w.r0, w.s, w.K, 0, rpc, w.twf, w.st,
-                                               lw.chunk, lw.F);
-      // s = r - alpha v; z = Prec(s); t = M z
-      pk.rows<<<rg, k3Threads, smem_rows, s>>>(pf, q, 1, w.r, w.p, w.v, w.s, w.hat, w.K, rpc, 1, w.twf);
-      pk.cols<<<dim3(nf / cpc, P), k3Threads, smem_cols, s>>>(pb, q, w.hat, w.K, cpc, w.twb, w.sym);
-      apply_k<<<rg, k3Threads, smem_apply, s>>>(pf, q, w.hat, w.z, w.t, w.cdl, w.r0, w.s, w.K, 1, rpc, w.twf, w.st,
-                                               lw.chunk, lw.F);
-      c3_update_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.x, w.r, w.r0, w.y, w.z, w.s, w.t, w.K);
-      c3_commit_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, w.st, max_iter, use_cond, inner);
-      return;
-    }
     // p = r + beta (p - omega v); y = Prec(p); v = M y
     precondition(s, 0, w.r, learned ? lw.zt : w.y, w.K);
     if (learned) c3_filter_kernel<<<fgrid, k3Threads, 0, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.y, w.K);
@@ -1044,7 +939,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     precondition(s, 1, w.r, learned ? lw.zt : w.z, w.K);
     if (learned) c3_filter_kernel<<<fgrid, k3Threads, 0, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.z, w.K);
     c3_matvec_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K, 1);
-    c3_update_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.x, w.r, w.r0, w.y, w.z, w.s, w.t, w.K);
+    c3_update_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.x, w.r, w.r0, w.y, w.z, w.s, w.t, w.K, w.st);
     c3_commit_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, w.st, max_iter, use_cond, inner);
   };
   // step tail: u += x (true residual, store), statistics, gradient
@@ -1154,6 +1049,9 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   int rc = prologue(st);
   if (rc != TP_OK) return rc;
   for (int t = 1; t <= L; ++t) {
+    // a training pair copies x, which a probe with a zero right-hand side
+    // never writes in its step
+    if (train) TP_CHECK_CUDA(cudaMemsetAsync(w.x, 0, (size_t)P * N * sizeof(float2), st));
     step_head(st, 0, 0, 0);
     for (int it = 0; it < max_iter; ++it) {
       iteration(st, 0, 0);

@@ -161,9 +161,11 @@ __device__ __forceinline__ void ms_kernel_H(float2 *H, const MsParams &q, int ti
 //   X = psi + (T_z - 1) psi,   psi' = X + IFFT((H - 1) . FFT(X)),
 // so the FFT round-off scales with the small update instead of the field
 // (the same reason the CN march keeps "1 + eps" coefficients).  X stays in
-// registers: a thread owns elements tid + j*nth, j < kMsElems.
-constexpr int kMsElems = 32;  // rows * n <= kMsElems * kFftThreads
+// registers: a thread owns elements tid + j*nth, j < E (E = 8, 16 or 32:
+// rows * n <= E * kFftThreads).
+constexpr int kMsElems = 32;  // the largest E
 
+template <int E>
 __global__ void __launch_bounds__(kFftThreads) ms_march_kernel(const FftPlan pl, const MsParams q, int rows) {
   extern __shared__ __align__(16) float2 fsm[];
   const int n = q.n, tid = threadIdx.x, nth = blockDim.x;
@@ -173,9 +175,9 @@ __global__ void __launch_bounds__(kFftThreads) ms_march_kernel(const FftPlan pl,
   const int tot = nb * n;
   fft_twiddles(tw, n, tid, nth);
   ms_kernel_H(H, q, tid, nth);
-  float2 X[kMsElems];
+  float2 X[E];
 #pragma unroll
-  for (int j = 0; j < kMsElems; ++j) {
+  for (int j = 0; j < E; ++j) {
     const int e = tid + j * nth;
     if (e < tot) {
       X[j] = q.probes[(size_t)p0 * n + e];
@@ -187,7 +189,7 @@ __global__ void __launch_bounds__(kFftThreads) ms_march_kernel(const FftPlan pl,
   for (int z = 0; z < q.L; ++z) {
     const float2 *Tz = q.trans + (size_t)z * n;
 #pragma unroll
-    for (int j = 0; j < kMsElems; ++j) {
+    for (int j = 0; j < E; ++j) {
       const int e = tid + j * nth;
       if (e < tot) {
         X[j] = cfma(Tz[e % n], X[j], X[j]);
@@ -201,7 +203,7 @@ __global__ void __launch_bounds__(kFftThreads) ms_march_kernel(const FftPlan pl,
     __syncthreads();
     float2 *R = fft_block(F, o, pl, tw, true, nb, tid, nth);
 #pragma unroll
-    for (int j = 0; j < kMsElems; ++j) {
+    for (int j = 0; j < E; ++j) {
       const int e = tid + j * nth;
       if (e < tot) {
         X[j] = make_float2(fmaf(R[e].x, s, X[j].x), fmaf(R[e].y, s, X[j].y));
@@ -216,6 +218,7 @@ __global__ void __launch_bounds__(kFftThreads) ms_march_kernel(const FftPlan pl,
 // Adjoint march (delta form as the forward): g = lambda + IFFT(conj(H - 1) .
 // FFT(lambda)); grad_t[z] += sum_p g conj(T_z u_z); lambda <- conj(T_z) g,
 // from lambda = src_exit at the exit plane.
+template <int E>
 __global__ void __launch_bounds__(kFftThreads) ms_backward_kernel(const FftPlan pl, const MsParams q, int rows) {
   extern __shared__ __align__(16) float2 fsm[];
   const int n = q.n, tid = threadIdx.x, nth = blockDim.x;
@@ -225,9 +228,9 @@ __global__ void __launch_bounds__(kFftThreads) ms_backward_kernel(const FftPlan 
   const int tot = nb * n;
   fft_twiddles(tw, n, tid, nth);
   ms_kernel_H(H, q, tid, nth);
-  float2 X[kMsElems];
+  float2 X[E];
 #pragma unroll
-  for (int j = 0; j < kMsElems; ++j) {
+  for (int j = 0; j < E; ++j) {
     const int e = tid + j * nth;
     if (e < tot) {
       X[j] = q.src_exit[(size_t)p0 * n + e];
@@ -245,7 +248,7 @@ __global__ void __launch_bounds__(kFftThreads) ms_backward_kernel(const FftPlan 
     const float2 *Tz = q.trans + (size_t)z * n;
     // g = X + s*G ; contribution g conj(T u); X <- conj(T) g = g + conj(T-1) g
 #pragma unroll
-    for (int j = 0; j < kMsElems; ++j) {
+    for (int j = 0; j < E; ++j) {
       const int e = tid + j * nth;
       if (e < tot) {
         const float2 g = make_float2(fmaf(G[e].x, s, X[j].x), fmaf(G[e].y, s, X[j].y));
@@ -367,15 +370,25 @@ extern "C" int tp_ms2d_transmission(const tp_ms2d_op *op, const void *n_field, i
                                 reinterpret_cast<cudaStream_t>(stream));
 }
 
-static int ms_rows(int n) {
-  // probes per CTA: every thread keeps kMsElems field values in registers,
-  // and the two FFT buffers per probe plus H and the twiddles must fit in
-  // 200 KB of shared memory
+// Probes per CTA: at most what kMsElems field values per thread hold and
+// what fits in 200 KB of shared memory (two FFT buffers per probe, H and the
+// twiddles), at most 4, and no more than needed to give every SM a CTA.
+static int ms_rows(int n, int num_probes) {
   int r = (kMsElems * kFftThreads) / n;
   const int rs = (200 * 1024 / (int)sizeof(float2) - 2 * n) / (2 * n);
   if (rs < r) r = rs;
   if (r > 4) r = 4;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int fill = (num_probes + sms - 1) / sms;
+  if (r > fill) r = fill < 1 ? 1 : fill;
   return r;
+}
+
+// Field values per thread for `rows` probes of length n (a compiled E).
+static int ms_elems(int n, int rows) {
+  const int e = (rows * n + kFftThreads - 1) / kFftThreads;
+  return e <= 8 ? 8 : (e <= 16 ? 16 : 32);
 }
 
 extern "C" int tp_ms2d_march(const tp_ms2d_op *op, const void *trans, const void *probes, int32_t num_probes,
@@ -392,13 +405,14 @@ extern "C" int tp_ms2d_march(const tp_ms2d_op *op, const void *trans, const void
   q.probes = static_cast<const float2 *>(probes);
   q.u_store = static_cast<float2 *>(u_store);
   q.exit_out = static_cast<float2 *>(exit_out);
-  const int rows = ms_rows(op->n);
+  const int rows = ms_rows(op->n, num_probes);
   if (rows < 1) return set_error(TP_ERR_UNSUPPORTED, "N=%d too large for the multislice kernel", op->n);
   const size_t smem = fft_smem(op->n, rows, 2);
-  rc = fft_launch_setup((const void *)ms_march_kernel, smem);
+  const int E = ms_elems(op->n, rows);
+  auto kern = E == 8 ? ms_march_kernel<8> : (E == 16 ? ms_march_kernel<16> : ms_march_kernel<32>);
+  rc = fft_launch_setup((const void *)kern, smem);
   if (rc) return rc;
-  ms_march_kernel<<<(num_probes + rows - 1) / rows, kFftThreads, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
-      pl, q, rows);
+  kern<<<(num_probes + rows - 1) / rows, kFftThreads, smem, reinterpret_cast<cudaStream_t>(stream)>>>(pl, q, rows);
   return check_cuda(cudaGetLastError(), "ms_march_kernel launch");
 }
 
@@ -416,12 +430,13 @@ extern "C" int tp_ms2d_backward(const tp_ms2d_op *op, const void *trans, const v
   q.u_fwd = static_cast<const float2 *>(u_fwd);
   q.src_exit = static_cast<const float2 *>(src_exit);
   q.grad_t = static_cast<float2 *>(grad_t);
-  const int rows = ms_rows(op->n);
+  const int rows = ms_rows(op->n, num_probes);
   if (rows < 1) return set_error(TP_ERR_UNSUPPORTED, "N=%d too large for the multislice kernel", op->n);
   const size_t smem = fft_smem(op->n, rows, 2);
-  rc = fft_launch_setup((const void *)ms_backward_kernel, smem);
+  const int E = ms_elems(op->n, rows);
+  auto kern = E == 8 ? ms_backward_kernel<8> : (E == 16 ? ms_backward_kernel<16> : ms_backward_kernel<32>);
+  rc = fft_launch_setup((const void *)kern, smem);
   if (rc) return rc;
-  ms_backward_kernel<<<(num_probes + rows - 1) / rows, kFftThreads, smem, reinterpret_cast<cudaStream_t>(stream)>>>(
-      pl, q, rows);
+  kern<<<(num_probes + rows - 1) / rows, kFftThreads, smem, reinterpret_cast<cudaStream_t>(stream)>>>(pl, q, rows);
   return check_cuda(cudaGetLastError(), "ms_backward_kernel launch");
 }
