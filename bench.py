@@ -468,7 +468,8 @@ def bench_learned_3d(dev, reps=2, train_steps=1500, pairs="mixed"):
             grad.zero_()
             e0.record(stream)
             eng.march(field, P, "forward", probes=probes, u_store=store, exit_out=ex, precond=pc, model=model)
-            eng.march(field, P, "adjoint_exact", src_exit=ex, u_fwd=store, grad_c=grad, precond=pc, model=model)
+            eng.march(field, P, "adjoint_exact", src_exit=ex, u_fwd=store, grad_c=grad, precond=pc, model=model,
+                      reuse_filters=True)
             e1.record(stream)
             torch.cuda.synchronize(dev)
             if rep >= 1:

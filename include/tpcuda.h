@@ -424,6 +424,12 @@ typedef struct tp_cn3d_march_args {
   void *train_z0, *train_sol, *train_diag;
   int32_t train_every;       /* 0 = no training pairs                           */
   int32_t train_kind;
+  int32_t learned_reuse;     /* precond == 2: 1 = the learned workspace already
+                                holds the filters of this index field and model
+                                (from the previous march with it, e.g. the
+                                forward before the adjoint): the network is not
+                                run again                                       */
+  int32_t reserved2;
 } tp_cn3d_march_args;
 
 TP_API size_t tp_cn3d_workspace_bytes(int32_t n_total, int32_t num_probes);

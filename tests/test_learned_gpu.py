@@ -144,3 +144,24 @@ def test_gradient_descent_learned_matches_plain(trained):
     diff = np.linalg.norm(runs["learned"][0] - runs[True][0]) / np.linalg.norm(runs[True][0] - n0)
     assert diff <= 0.15, diff
     assert runs["learned"][1] <= runs[True][1], (runs["learned"][1], runs[True][1])
+
+
+def test_learned_filters_reused_by_the_adjoint(trained):
+    """The adjoint march reusing the forward march's per-slice filters
+    (reuse_filters: the network is not run again for the same field) gives
+    the gradient of the march that recomputes them, to fp32 round-off."""
+    eng, model, _ = trained
+    P = 3
+    field = torch.from_numpy(_index(404)).cuda()
+    pr = torch.from_numpy(_probes(P, 4).astype(np.complex64)).cuda()
+    store = eng.new_store(P)
+    ex = torch.empty((P, NF * NB), dtype=torch.complex64, device="cuda")
+    eng.march(field, P, "forward", probes=pr, u_store=store, exit_out=ex, precond="learned", model=model)
+    grads = []
+    for reuse in (True, False):
+        gc = torch.zeros((NZ - 1, NF * NB), dtype=torch.complex64, device="cuda")
+        eng.march(field, P, "adjoint_exact", src_exit=ex, u_fwd=store, grad_c=gc, precond="learned", model=model,
+                  reuse_filters=reuse)
+        grads.append(gc.cpu().numpy())
+    assert eng.fallbacks == 0
+    assert np.linalg.norm(grads[0] - grads[1]) <= 1e-6 * np.linalg.norm(grads[1])

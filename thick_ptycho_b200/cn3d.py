@@ -82,7 +82,8 @@ class CN3D:
 
     def march(self, field: torch.Tensor, num_probes: int, mode="forward", probes=None, src_shared=None, src_exit=None,
               u_store=None, exit_out=None, u_fwd=None, grad_c=None, tol=1e-6, max_iter=20, precond=True,
-              host_check=True, is_delta=False, model=None, train=None, train_every=0, fallback=True):
+              host_check=True, is_delta=False, model=None, train=None, train_every=0, fallback=True,
+              reuse_filters=False):
         """One batched march; tensors complex64 (field complex128/complex64 (N, nz)).
 
         ``precond``: True/"fft" (periodic FFT preconditioner), False/"none", or
@@ -99,7 +100,7 @@ class CN3D:
             if fallback:
                 before = int(self.stats[2].item())
                 self._march(field, num_probes, mode, probes, src_shared, src_exit, u_store, exit_out, u_fwd, grad_c, tol,
-                            max_iter, 2, host_check, is_delta, model, train, train_every)
+                            max_iter, 2, host_check, is_delta, model, train, train_every, reuse_filters)
                 if int(self.stats[2].item()) > before:
                     self.fallbacks += 1
                     if grad_c is not None:
@@ -116,10 +117,10 @@ class CN3D:
         else:
             raise ValueError(f"unknown preconditioner {precond!r}")
         self._march(field, num_probes, mode, probes, src_shared, src_exit, u_store, exit_out, u_fwd, grad_c, tol,
-                    max_iter, code, host_check, is_delta, model, train, train_every)
+                    max_iter, code, host_check, is_delta, model, train, train_every, reuse_filters)
 
     def _march(self, field, num_probes, mode, probes, src_shared, src_exit, u_store, exit_out, u_fwd, grad_c, tol,
-               max_iter, precond, host_check, is_delta, model, train, train_every):
+               max_iter, precond, host_check, is_delta, model, train, train_every, reuse_filters=False):
         P = int(num_probes)
         field = field.reshape(self.N, self.nz).contiguous()
         mode_i = _native.MODES[mode] if isinstance(mode, str) else int(mode)
@@ -136,7 +137,9 @@ class CN3D:
         a.u_store, a.exit_out, a.u_fwd, a.grad_c = _ptr(u_store), _ptr(exit_out), _ptr(u_fwd), _ptr(grad_c)
         a.stats = ctypes.c_void_p(self.stats.data_ptr())
         if precond == 2:
+            reused = reuse_filters and self._lws is not None and self._lws_P == P
             lws = self.learned_workspace(P)
+            a.learned_reuse = 1 if reused else 0
             mdl = model.model()
             a.model = ctypes.cast(ctypes.pointer(mdl), ctypes.c_void_p)
             a.learned_ws, a.learned_ws_bytes = _ptr(lws), lws.numel()
@@ -200,6 +203,7 @@ class PWEGradient3D:
         ex = torch.empty((P, e.N), dtype=torch.complex64, device=self.device)
         e.march(field, P, "forward", probes=probes.reshape(P, e.N).contiguous(), u_store=self._store, exit_out=ex,
                 **self.kw)
+        self._filters_of = field  # the learned filters now in the engine's workspace
         return ex
 
     def backward(self, field, exit_grad):
@@ -207,7 +211,7 @@ class PWEGradient3D:
         P = exit_grad.shape[0]
         gc = torch.zeros((e.L, e.N), dtype=torch.complex64, device=self.device)
         e.march(field, P, "adjoint_exact", src_exit=exit_grad.reshape(P, e.N).contiguous(), u_fwd=self._store,
-                grad_c=gc, **self.kw)
+                grad_c=gc, reuse_filters=getattr(self, "_filters_of", None) is field, **self.kw)
         self.grad_c = gc
         return e.grad_to_n(gc, field)
 

@@ -543,40 +543,82 @@ __global__ void c3_grad_kernel(int N, int P, int nz, const C3State *st, const fl
 // with the filter of the current step's slice s (conj(F) in the adjoint
 // modes).  The filters of all slices are computed before the march, in
 // chunks of `chunk` slices: slice s uses image (s-1) % chunk of chunk
-// (s-1) / chunk, tap-major within the chunk (13, chunk * N).  A thread owns
-// one pixel for kFilterProbes probes, so each filter value is read once per
-// pixel group.  Grid (N / 256, P / kFilterProbes).
+// (s-1) / chunk, tap-major within the chunk (13, chunk * N).
+//
+// A CTA owns `rb` whole rows (rb * nf <= 2 * 256 pixels, two per thread) and
+// kFilterProbes probes.  Each thread keeps its pixels' 13 taps in registers
+// (read once for all the CTA's probes); each probe's rows with a 2-row halo
+// are copied into shared memory (cp.async, double-buffered: the next probe's
+// tile arrives while this one is filtered), so the 13 neighbour reads of a
+// pixel hit shared memory.  Grid (ceil(nb / rb), P / kFilterProbes).
 constexpr int kFilterProbes = 8;
+constexpr int kFilterPx = 2;  // pixels per thread
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
 __global__ void __launch_bounds__(k3Threads) c3_filter_kernel(const C3Params q, const C3State *st, int chunk,
                                                               const float2 *__restrict__ Fall,
                                                               const float2 *__restrict__ z, float2 *out,
-                                                              const Krylov *K) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= q.N) return;
+                                                              const Krylov *K, int rb) {
+  extern __shared__ __align__(16) float2 ztile[];  // [2][(rb + 4) * nf]
+  const int nf = q.nf, nb = q.nb;
+  const int b0 = blockIdx.x * rb;
+  const int lo = b0 - 2 < 0 ? 0 : b0 - 2, hi = b0 + rb + 2 > nb ? nb : b0 + rb + 2;
+  const int tile = (hi - lo) * nf, stride = (rb + 4) * nf;
+  const int npx = ((b0 + rb > nb ? nb : b0 + rb) - b0) * nf;
   const int sl = st->s - 1;
   const size_t np = (size_t)chunk * q.N;
   const float2 *F = Fall + (size_t)(sl / chunk) * kFilterTaps * np + (size_t)(sl % chunk) * q.N;
-  const int b = i / q.nf, f = i - b * q.nf;
-  float2 w[kFilterTaps];
-  int o[kFilterTaps];
+  float2 w[kFilterPx][kFilterTaps];
+  int o[kFilterPx][kFilterTaps], own[kFilterPx];
 #pragma unroll
-  for (int t = 0; t < kFilterTaps; ++t) {
-    const int bb = b + filter_tap_dy(t), ff = f + filter_tap_dx(t);
-    const bool in = bb >= 0 && bb < q.nb && ff >= 0 && ff < q.nf;
-    float2 v = in ? F[(size_t)t * np + i] : make_float2(0.f, 0.f);
-    if (q.conj_t) v.y = -v.y;
-    w[t] = v;
-    o[t] = in ? (bb * q.nf + ff) : i;
+  for (int k = 0; k < kFilterPx; ++k) {
+    const int e = threadIdx.x + k * blockDim.x;
+    const int b = b0 + e / nf, f = e % nf;
+    own[k] = (b - lo) * nf + f;
+#pragma unroll
+    for (int t = 0; t < kFilterTaps; ++t) {
+      const int bb = b + filter_tap_dy(t), ff = f + filter_tap_dx(t);
+      const bool in = e < npx && bb >= 0 && bb < nb && ff >= 0 && ff < nf;
+      float2 v = in ? F[(size_t)t * np + (size_t)b * nf + f] : make_float2(0.f, 0.f);
+      if (q.conj_t) v.y = -v.y;
+      w[k][t] = v;
+      o[k][t] = in ? (bb - lo) * nf + ff : own[k];
+    }
   }
   const int p0 = blockIdx.y * kFilterProbes;
-#pragma unroll 1
-  for (int pr = p0; pr < p0 + kFilterProbes && pr < q.P; ++pr) {
-    if (K != nullptr && K[pr].done) continue;
-    const float2 *zp = z + (size_t)pr * q.N;
-    float2 acc = zp[i];
+  const int p1 = p0 + kFilterProbes < q.P ? p0 + kFilterProbes : q.P;
+  auto fetch = [&](int pr, int buf) {
+    const float2 *src = z + (size_t)pr * q.N + (size_t)lo * nf;
+    float2 *dst = ztile + buf * stride;
+    for (int e = threadIdx.x; e < tile; e += blockDim.x) cp_async8(&dst[e], &src[e]);
+    cp_async_commit();
+  };
+  fetch(p0, 0);
+  for (int pr = p0; pr < p1; ++pr) {
+    const int buf = (pr - p0) & 1;
+    if (pr + 1 < p1) {
+      fetch(pr + 1, buf ^ 1);
+      cp_async_wait_prev();  // this probe's tile has landed
+    } else {
+      cp_async_wait_all();
+    }
+    __syncthreads();
+    if (K == nullptr || !K[pr].done) {
+      const float2 *zt = ztile + buf * stride;
+      float2 *dst = out + (size_t)pr * q.N + (size_t)b0 * nf;
 #pragma unroll
-    for (int t = 0; t < kFilterTaps; ++t) acc = cfma(w[t], zp[o[t]], acc);
-    out[(size_t)pr * q.N + i] = acc;
+      for (int k = 0; k < kFilterPx; ++k) {
+        const int e = threadIdx.x + k * blockDim.x;
+        if (e >= npx) continue;
+        float2 acc = zt[own[k]];
+#pragma unroll
+        for (int t = 0; t < kFilterTaps; ++t) acc = cfma(w[k][t], zt[o[k][t]], acc);
+        dst[e] = acc;
+      }
+    }
+    __syncthreads();  // the buffer is refilled two probes on
   }
 }
 
@@ -838,6 +880,8 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
       return set_error(TP_ERR_INVALID, "learned preconditioner: NULL model or workspace");
     if (!fft_on) return set_error(TP_ERR_UNSUPPORTED, "learned preconditioner needs FFT-plannable nf, nb (got %d, %d)", nf, nb);
     if (a->mode == TP_MODE_REVERSE) return set_error(TP_ERR_UNSUPPORTED, "learned preconditioner: REVERSE mode is not supported");
+    if (nf > kFilterPx * k3Threads)
+      return set_error(TP_ERR_UNSUPPORTED, "learned preconditioner: nf=%d > %d", nf, kFilterPx * k3Threads);
     if ((reinterpret_cast<uintptr_t>(a->learned_ws) & 255u) != 0)
       return set_error(TP_ERR_INVALID, "learned workspace must be 256-byte aligned");
     lw = c3_learned_layout(static_cast<char *>(a->learned_ws), nf, nb, nz, P);
@@ -868,7 +912,10 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   const int adj_exact = a->mode == TP_MODE_ADJOINT_EXACT ? 1 : 0;
   float2 *ust = static_cast<float2 *>(a->u_store);
   float2 *exit_out = static_cast<float2 *>(a->exit_out);
-  const dim3 fgrid((N + k3Threads - 1) / k3Threads, (P + kFilterProbes - 1) / kFilterProbes);
+  // learned filter: whole rows per CTA, at most two pixels per thread
+  const int frb = (kFilterPx * k3Threads) / nf >= 1 ? (kFilterPx * k3Threads) / nf : 1;
+  const dim3 fgrid((nb + frb - 1) / frb, (P + kFilterProbes - 1) / kFilterProbes);
+  const size_t smem_filter = 2 * (size_t)(frb + 4) * nf * sizeof(float2);
   const dim3 vgrid((N + 256 * 8 - 1) / (256 * 8), P);
   const int pgrid = (P + 127) / 128;
   const int one_cta = P >= 1024 ? 1024 : ((P + 31) / 32) * 32;
@@ -895,7 +942,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
                                       static_cast<const float2 *>(op->kw), static_cast<const float2 *>(op->ke),
                                       static_cast<const float2 *>(op->ks), static_cast<const float2 *>(op->kn), w.dc,
                                       w.dw, w.de, w.ds, w.dn);
-    if (learned) {
+    if (learned && !a->learned_reuse) {
       // the filters of every slice, chunk by chunk (the CNN activations' zero
       // borders are never written by the kernels)
       TP_CHECK_CUDA(cudaMemsetAsync(lw.cnn, 0, lw.cnn_bytes, s));
@@ -933,11 +980,11 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   auto iteration = [&](cudaStream_t s, int use_cond, cudaGraphConditionalHandle inner) {
     // p = r + beta (p - omega v); y = Prec(p); v = M y
     precondition(s, 0, w.r, learned ? lw.zt : w.y, w.K);
-    if (learned) c3_filter_kernel<<<fgrid, k3Threads, 0, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.y, w.K);
+    if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.y, w.K, frb);
     c3_matvec_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.cdl, w.y, w.v, w.r0, w.s, w.K, 0);
     // s = r - alpha v; z = Prec(s); t = M z
     precondition(s, 1, w.r, learned ? lw.zt : w.z, w.K);
-    if (learned) c3_filter_kernel<<<fgrid, k3Threads, 0, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.z, w.K);
+    if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.z, w.K, frb);
     c3_matvec_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K, 1);
     c3_update_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.x, w.r, w.r0, w.y, w.z, w.s, w.t, w.K, w.st);
     c3_commit_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, w.st, max_iter, use_cond, inner);
