@@ -237,6 +237,57 @@ def march(A, B, C2d, probe, mode="forward", b=None, rhs_block=None, test_rhs=Non
     return march_with_lu(lus, Bs, b, probe, mode, rhs_block, test_rhs)
 
 
+class NodePerturbation:
+    """Exit waves of a probe stack when one index node is perturbed, for
+    central finite differences at full depth.
+
+    The forward march of ``march_with_lu`` (``iterative_lu.py:185-193``) is run
+    once with every slice's factor and state kept.  Node t of n enters only the
+    object terms C[:, t−1] and C[:, t] (``base_simulation_space.py:375-381``:
+    C_j averages nodes j and j+1), i.e. slices t and t+1, so a perturbed exit
+    refactorises those two slices and re-marches from the stored state u_{t−1};
+    the arithmetic of every slice is that of the full march.
+    """
+
+    def __init__(self, A, B, n, k, dz, probes, exact_ref_coeff=False):
+        self.A, self.B, self.k, self.dz = A, B, k, dz
+        self.exact = exact_ref_coeff
+        self.n = np.array(n, dtype=complex)
+        self.C = object_contribution(self.n, k, dz, exact_ref_coeff=exact_ref_coeff)
+        self.lus, self.Bs = build_lu_factors(A, B, self.C)
+        L = self.C.shape[1]
+        u = np.asarray(probes, dtype=complex).T.copy()  # (N, P)
+        self.states = [u]
+        for j in range(1, L + 1):
+            u = self.lus[j - 1].solve(self.Bs[j - 1] @ u)
+            self.states.append(u)
+
+    def exits(self, x=None, t=None, delta=0.0):
+        """(P, N) exit waves, with n[x, t] += delta when x is given."""
+        L = self.C.shape[1]
+        if x is None:
+            return self.states[-1].T.copy()
+        cols = {}
+        for j in (t - 1, t):  # C columns that read node t
+            if 0 <= j < L:
+                seg = self.n[x, j:j + 2].copy()
+                seg[t - j] += delta
+                c = object_contribution(seg[None, :], self.k, self.dz, exact_ref_coeff=self.exact)[0, 0]
+                cols[j] = c
+        j0 = min(cols)  # first changed column: slice j0 + 1 (1-based)
+        u = self.states[j0]
+        for j in range(j0, L):
+            if j in cols:
+                Cj = self.C[:, j].copy()
+                Cj[x] = cols[j]
+                D = sp.diags(Cj)
+                lu = spla.splu((self.A - D).tocsc())
+                u = lu.solve((self.B + D) @ u)
+            else:
+                u = self.lus[j].solve(self.Bs[j] @ u)
+        return u.T.copy()
+
+
 def march_streamed(A, B, C2d, probes, keep=None):
     """Forward march of several probes, one slice factorised at a time.
 

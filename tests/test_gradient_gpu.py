@@ -5,7 +5,7 @@ reference's own (inexact) least-squares gradient.
 Tolerances: checkpointed vs full-store gradients ≤ 1e-5 relative L2 (same
 arithmetic, only the fp32 accumulation order differs); GPU vs oracle ≤ 1e-5
 relative L2; finite differences (h = 1e-7, complex128) within 1e-3 relative
-per sampled voxel; reference gradient: cosine similarity ≥ 0.98 (its adjoint
+per sampled voxel (1e-4 at the full reconstruction-gradient geometry); reference gradient: cosine similarity ≥ 0.98 (its adjoint
 is not the exact transpose of its forward: it pairs (A − C_s)ᴴ with
 (B + C_s)ᴴ of the same slice, iterative_lu.py:114-128, and its grad_A drops
 C₀u₀, forward_model.py:151-153; measured 0.992).
@@ -91,37 +91,38 @@ def test_gradient_matches_oracle_and_autograd():
 
 
 def test_gradient_matches_central_differences_config3_geometry():
-    """N = 1024, stride 4 (the reconstruction-gradient geometry), 64 nodes, 12
-    probes, √Nz checkpointing; 24 random voxels, h = 1e-7 in complex128."""
-    N, nz, P = 1024, 64, 12
+    """The reconstruction-gradient geometry at full size: N = 1024, Nz = 512
+    nodes, stride 4, ground truth of 300 seeded blobs, start δn = 0, √Nz
+    checkpointing, with 8 of its 256 probes; central differences (h = 1e-7,
+    complex128) of the oracle's amplitude loss at 64 random voxels, real and
+    imaginary parts.  A perturbed node changes only the two slices that read
+    it, so each difference re-marches the oracle from the stored state before
+    them (``NodePerturbation``).  Tolerance: 1e-4 relative per voxel, with a
+    floor of 1e-3 of the largest gradient entry (the differences themselves
+    agree with the oracle's exact adjoint gradient to 2e-6)."""
+    N, nz, P = 1024, 512, 8
     geo = SimulationGeometry.grid_2d(N, nz, 0.5, P, 4)
-    truth = 1 - blob_field_2d(N, nz, 30, 7)
+    truth = 1 - blob_field_2d(N, nz, 300, 7)
     probes = gaussian_probes_2d(N, geo.centres, 8.0)
     co = po.bc_coefficients(geo.k, 1.0, 1.0, bc_type="impedance")
     A, B = po.step_matrices_1d(N, co, "impedance", 1.0)
-
-    def exits(nn):
-        lus, Bs = po.build_lu_factors(A, B, po.object_contribution(nn, geo.k, 1.0))
-        return np.array([po.march_with_lu(lus, Bs, np.zeros(N, complex), probes[p])[:, -1] for p in range(P)])
-
-    amp = np.abs(np.fft.fft(exits(truth), axis=-1))
+    amp = np.abs(np.fft.fft(po.NodePerturbation(A, B, truth, geo.k, 1.0, probes).exits(), axis=-1))
     n0 = np.ones((N, nz), dtype=complex)  # starting guess δn = 0
     pg = PWEGradient2D(geo, checkpoint="sqrt")
     _, g = pg.loss_and_grad(n0, probes, amp)
     g = g.cpu().numpy()
+    base = po.NodePerturbation(A, B, n0, geo.k, 1.0, probes)
     rng = np.random.default_rng(0)
     h = 1e-7
     scale = np.abs(g).max()
-    for _ in range(24):
+    for _ in range(64):
         x, t = int(rng.integers(0, N)), int(rng.integers(0, nz))
         for d, part in ((1.0, 0), (1j, 1)):
-            e = np.zeros_like(n0)
-            e[x, t] = h * d
-            lp = po.amplitude_loss_and_grad(exits(n0 + e), amp)[0]
-            lm = po.amplitude_loss_and_grad(exits(n0 - e), amp)[0]
+            lp = po.amplitude_loss_and_grad(base.exits(x, t, h * d), amp)[0]
+            lm = po.amplitude_loss_and_grad(base.exits(x, t, -h * d), amp)[0]
             fd = (lp - lm) / (2 * h)
             an = g[x, t].real if part == 0 else g[x, t].imag
-            assert abs(fd - an) <= 1e-3 * max(abs(fd), 1e-2 * scale), (x, t, part, fd, an)
+            assert abs(fd - an) <= 1e-4 * max(abs(fd), 1e-3 * scale), (x, t, part, fd, an)
 
 
 def test_reference_gradient_agreement(golden):

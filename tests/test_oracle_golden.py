@@ -282,3 +282,23 @@ def test_pit_adjoint_matches_reference(golden, bc):
     # the system it solves: forward structure on (A^H, B^H, flipped conj C)
     x = po.full_system_solve(A.conj().T.tocsr(), B.conj().T.tocsr(), np.flip(np.conj(C), axis=1), rhs.T.ravel())
     assert rel(x.reshape(L, N).T, g[f"adj_rhs_{bc}"][:, 1:]) < 2e-5
+
+
+def test_node_perturbation_matches_full_march():
+    """The finite-difference helper (stored states, two refactorised slices)
+    gives the exit waves of a full re-march of the perturbed index field."""
+    rng = np.random.default_rng(3)
+    N, nz, k = 48, 16, 4 * np.pi
+    co = po.bc_coefficients(k, 1.0, 1.0, bc_type="neumann")
+    A, B = po.step_matrices_1d(N, co, "neumann", 1.0)
+    n = 1 + 1e-3 * (rng.standard_normal((N, nz)) + 0.1j * rng.standard_normal((N, nz)))
+    probes = rng.standard_normal((3, N)) + 1j * rng.standard_normal((3, N))
+    npx = po.NodePerturbation(A, B, n, k, 1.0, probes)
+    for x, t, d in ((0, 0, 1e-6), (20, 7, 1e-6j), (47, nz - 1, -2e-6)):
+        n2 = n.copy()
+        n2[x, t] += d
+        C = po.object_contribution(n2, k, 1.0)
+        ref = np.array([po.march(A, B, C, probes[p])[:, -1] for p in range(3)])
+        assert rel(npx.exits(x, t, d), ref) < 1e-13
+    assert rel(npx.exits(), np.array([po.march(A, B, po.object_contribution(n, k, 1.0), probes[p])[:, -1]
+                                      for p in range(3)])) < 1e-14
