@@ -186,7 +186,18 @@ __global__ void __launch_bounds__(k3Threads) c3_init_kernel(const C3Params q, co
   const float2 *shared = src_shared ? src_shared + (size_t)(t - 1) * q.N : nullptr;
   double acc = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
-    float2 b = use_u ? cadd(apply_P(q, cdl, u + off, i), apply_P(q, cdr, u + off, i)) : make_float2(0.f, 0.f);
+    // (P_l + P_r) u = (cd_l + cd_r) u + 2 K_off u: the two operators differ only on the diagonal
+    float2 b = make_float2(0.f, 0.f);
+    if (use_u) {
+      const float2 *uu = u + off;
+      float2 o = make_float2(0.f, 0.f);
+      const int f = i % q.nf;
+      if (f > 0) o = cfma(q.kw[i], uu[i - 1], o);
+      if (f < q.nf - 1) o = cfma(q.ke[i], uu[i + 1], o);
+      if (i >= q.nf) o = cfma(q.ks[i], uu[i - q.nf], o);
+      if (i + q.nf < q.N) o = cfma(q.kn[i], uu[i + q.nf], o);
+      b = cfma(cadd(cdl[i], cdr[i]), uu[i], cadd(o, o));
+    }
     if (src != nullptr) b = cadd(b, src[off + i]);
     if (shared != nullptr) b = cadd(b, shared[i]);
     r0[off + i] = b;
@@ -547,26 +558,34 @@ __global__ void c3_grad_kernel(int N, int P, int nz, const C3State *st, const fl
 //
 // A CTA owns `rb` whole rows (rb * nf <= 2 * 256 pixels, two per thread) and
 // kFilterProbes probes.  Each thread keeps its pixels' 13 taps in registers
-// (read once for all the CTA's probes); each probe's rows with a 2-row halo
-// are copied into shared memory (cp.async, double-buffered: the next probe's
-// tile arrives while this one is filtered), so the 13 neighbour reads of a
-// pixel hit shared memory.  Grid (ceil(nb / rb), P / kFilterProbes).
+// (read once for all the CTA's probes); the rows of all the CTA's pending
+// probes, with a 2-row halo, are copied into shared memory at once (one wave
+// of cp.async copies, so the CTA waits for one load latency, not one per
+// probe), and the 13 neighbour reads of a pixel hit shared memory.
+// Grid (ceil(nb / rb), P / kFilterProbes).
 constexpr int kFilterProbes = 8;
 constexpr int kFilterPx = 2;  // pixels per thread
-
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 __global__ void __launch_bounds__(k3Threads) c3_filter_kernel(const C3Params q, const C3State *st, int chunk,
                                                               const float2 *__restrict__ Fall,
                                                               const float2 *__restrict__ z, float2 *out,
                                                               const Krylov *K, int rb) {
-  extern __shared__ __align__(16) float2 ztile[];  // [2][(rb + 4) * nf]
+  extern __shared__ __align__(16) float2 ztile[];  // [kFilterProbes][(rb + 4) * nf]
   const int nf = q.nf, nb = q.nb;
   const int b0 = blockIdx.x * rb;
   const int lo = b0 - 2 < 0 ? 0 : b0 - 2, hi = b0 + rb + 2 > nb ? nb : b0 + rb + 2;
   const int tile = (hi - lo) * nf, stride = (rb + 4) * nf;
   const int npx = ((b0 + rb > nb ? nb : b0 + rb) - b0) * nf;
+  const int p0 = blockIdx.y * kFilterProbes;
+  const int np_cta = q.P - p0 < kFilterProbes ? q.P - p0 : kFilterProbes;
+  // every pending probe's tile, in one wave of asynchronous copies
+  for (int j = 0; j < np_cta; ++j) {
+    if (K != nullptr && K[p0 + j].done) continue;
+    const float2 *src = z + (size_t)(p0 + j) * q.N + (size_t)lo * nf;
+    float2 *dst = ztile + j * stride;
+    for (int e = threadIdx.x; e < tile; e += blockDim.x) cp_async8(&dst[e], &src[e]);
+  }
+  // the taps while the copies are in flight
   const int sl = st->s - 1;
   const size_t np = (size_t)chunk * q.N;
   const float2 *F = Fall + (size_t)(sl / chunk) * kFilterTaps * np + (size_t)(sl % chunk) * q.N;
@@ -587,38 +606,22 @@ __global__ void __launch_bounds__(k3Threads) c3_filter_kernel(const C3Params q, 
       o[k][t] = in ? (bb - lo) * nf + ff : own[k];
     }
   }
-  const int p0 = blockIdx.y * kFilterProbes;
-  const int p1 = p0 + kFilterProbes < q.P ? p0 + kFilterProbes : q.P;
-  auto fetch = [&](int pr, int buf) {
-    const float2 *src = z + (size_t)pr * q.N + (size_t)lo * nf;
-    float2 *dst = ztile + buf * stride;
-    for (int e = threadIdx.x; e < tile; e += blockDim.x) cp_async8(&dst[e], &src[e]);
-    cp_async_commit();
-  };
-  fetch(p0, 0);
-  for (int pr = p0; pr < p1; ++pr) {
-    const int buf = (pr - p0) & 1;
-    if (pr + 1 < p1) {
-      fetch(pr + 1, buf ^ 1);
-      cp_async_wait_prev();  // this probe's tile has landed
-    } else {
-      cp_async_wait_all();
-    }
-    __syncthreads();
-    if (K == nullptr || !K[pr].done) {
-      const float2 *zt = ztile + buf * stride;
-      float2 *dst = out + (size_t)pr * q.N + (size_t)b0 * nf;
+  cp_async_wait_all();
+  __syncthreads();
+  for (int j = 0; j < np_cta; ++j) {
+    const int pr = p0 + j;
+    if (K != nullptr && K[pr].done) continue;
+    const float2 *zt = ztile + j * stride;
+    float2 *dst = out + (size_t)pr * q.N + (size_t)b0 * nf;
 #pragma unroll
-      for (int k = 0; k < kFilterPx; ++k) {
-        const int e = threadIdx.x + k * blockDim.x;
-        if (e >= npx) continue;
-        float2 acc = zt[own[k]];
+    for (int k = 0; k < kFilterPx; ++k) {
+      const int e = threadIdx.x + k * blockDim.x;
+      if (e >= npx) continue;
+      float2 acc = zt[own[k]];
 #pragma unroll
-        for (int t = 0; t < kFilterTaps; ++t) acc = cfma(w[k][t], zt[o[k][t]], acc);
-        dst[e] = acc;
-      }
+      for (int t = 0; t < kFilterTaps; ++t) acc = cfma(w[k][t], zt[o[k][t]], acc);
+      dst[e] = acc;
     }
-    __syncthreads();  // the buffer is refilled two probes on
   }
 }
 
@@ -903,6 +906,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     TP_CHECK_CUDA(cudaFuncSetAttribute(pk.inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
     TP_CHECK_CUDA(cudaFuncSetAttribute(pk.cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cols));
   }
+
   const int rows_cta = use_fft ? rpc : 1;
   const int max_iter = a->max_iter > 0 ? a->max_iter : 20;
   const double tol2 = (a->tol > 0 ? a->tol : 1e-6) * (a->tol > 0 ? a->tol : 1e-6);
@@ -915,7 +919,9 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   // learned filter: whole rows per CTA, at most two pixels per thread
   const int frb = (kFilterPx * k3Threads) / nf >= 1 ? (kFilterPx * k3Threads) / nf : 1;
   const dim3 fgrid((nb + frb - 1) / frb, (P + kFilterProbes - 1) / kFilterProbes);
-  const size_t smem_filter = 2 * (size_t)(frb + 4) * nf * sizeof(float2);
+  const size_t smem_filter = (size_t)kFilterProbes * (frb + 4) * nf * sizeof(float2);
+  if (learned)
+    TP_CHECK_CUDA(cudaFuncSetAttribute(c3_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_filter));
   const dim3 vgrid((N + 256 * 8 - 1) / (256 * 8), P);
   const int pgrid = (P + 127) / 128;
   const int one_cta = P >= 1024 ? 1024 : ((P + 31) / 32) * 32;
