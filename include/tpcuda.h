@@ -429,7 +429,11 @@ typedef struct tp_cn3d_march_args {
                                 (from the previous march with it, e.g. the
                                 forward before the adjoint): the network is not
                                 run again                                       */
-  int32_t reserved2;
+  int32_t fft_kernels;       /* preconditioner transforms: 0 = register four-step
+                                kernels where nf = nb is 64, 128, 192 or 256
+                                (16 x 16, 16 x 12, 16 x 8, 8 x 8), else the
+                                shared-memory Stockham kernels; 1 = always the
+                                Stockham kernels.  Same operator either way.    */
 } tp_cn3d_march_args;
 
 TP_API size_t tp_cn3d_workspace_bytes(int32_t n_total, int32_t num_probes);

@@ -257,3 +257,51 @@ def test_graph_march_matches_step_by_step(mode):
     assert rel(out[0][0], out[1][0]) < 1e-6
     if mode == "adjoint_exact":
         assert rel(out[0][1], out[1][1]) < 1e-6
+
+
+def _apply_i_minus_p(eng, x, diag):
+    """(I - P_s) x in complex128 from the engine's forward diagonals plus the
+    slice's object diagonal (vector index b * nf + f)."""
+    kc, kw, ke, ks, kn = (d.cpu().numpy().astype(np.complex128) for d in eng._diags)
+    nf, N = eng.nx, eng.N
+    f = np.arange(N) % nf
+    px = (kc + diag) * x
+    px[f > 0] += kw[f > 0] * x[np.arange(N)[f > 0] - 1]
+    px[f < nf - 1] += ke[f < nf - 1] * x[np.arange(N)[f < nf - 1] + 1]
+    px[nf:] += ks[nf:] * x[:-nf]
+    px[:-nf] += kn[:-nf] * x[nf:]
+    return x - px
+
+
+@pytest.mark.parametrize("nf,nb", [(64, 64), (128, 128), (192, 192), (256, 256), (96, 96), (64, 128)])
+def test_fft_preconditioner_against_numpy(nf, nb):
+    """The plain preconditioner M0^{-1} v = IFFT2(FFT2(v) / lambda) through the
+    white-noise training pairs (x noise, v = (I - P_s) x, z0 = M0^{-1} v),
+    against numpy's complex128 FFT: the register four-step kernels (square 64,
+    128, 192, 256) and the shared-memory Stockham kernels (96 x 96 and 64 x 128,
+    and forced at the four-step sizes) give the same operator."""
+    from thick_ptycho_b200.cn3d import generate_pairs
+
+    rng = np.random.default_rng(nf + nb)
+    nz, k, P = 3, 2 * np.pi / 0.5, 3
+    N = nf * nb
+    field = torch.from_numpy(_field(rng, N, nz)).cuda()
+    probes = c64(_gauss(nf, nb, rng.uniform(10, min(nf, nb) - 10, (P, 2)), 6.0))
+    eng = CN3D(nf, nb, nz, k, 1.0, 1.0, 1.0, "impedance")
+    fb, ff = np.meshgrid(np.arange(nb), np.arange(nf), indexing="ij")
+    mx, my = complex(eng.co.mu_x), complex(eng.co.mu_y)
+    lam = 1 - (mx * (2 * np.cos(2 * np.pi * ff / nf) - 2) + my * (2 * np.cos(2 * np.pi * fb / nb) - 2))
+    z0 = {}
+    for kern in (0, 1):
+        eng.fft_kernels = kern
+        pairs = generate_pairs(eng, field, probes, every=1, kind="noise")
+        z0[kern] = pairs.z0.cpu().numpy().astype(np.complex128)
+        sol = pairs.sol.cpu().numpy().astype(np.complex128)
+        diag = pairs.diag.cpu().numpy().astype(np.complex128)
+        for s in range(nz - 1):
+            for p in range(P):
+                v = _apply_i_minus_p(eng, sol[s, p], diag[s]).reshape(nb, nf)
+                ref = np.fft.ifft2(np.fft.fft2(v) / lam).ravel()
+                assert rel(z0[kern][s, p], ref) < 5e-6, (kern, s, p, rel(z0[kern][s, p], ref))
+    eng.fft_kernels = 0
+    assert rel(z0[0], z0[1]) < 2e-6

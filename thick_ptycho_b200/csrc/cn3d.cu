@@ -166,44 +166,113 @@ __device__ __forceinline__ void block_reduce_add(double v, double *dst, double *
   __syncthreads();
 }
 
-// Grid (chunks, P).  r0 = rhs = (P_l + P_r) u + src and its norm; the first
-// iteration reads r0 as r and takes x = p = v = 0 without reading them.  The
-// step t decides the terms: the exact adjoint's right-hand side uses the next
-// slice's operator (cdr) and has no u term at t = 1 (lambda_{L+1} = 0); the
-// per-probe source enters at t = 1; src_shared is (L, N) by step.
+// Sum M per-thread values over the CTA; thread m < M then calls fin(m, sum).
+template <int M, class Fin>
+__device__ __forceinline__ void block_reduce_many(double (&v)[M], double *red, Fin fin) {
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    double x = v[m];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) red[m * nw + wp] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < M) {
+    double sum = 0.0;
+    for (int j = 0; j < nw; ++j) sum += red[threadIdx.x * nw + j];
+    fin(threadIdx.x, sum);
+  }
+}
+
+// The stencil kernels below give each thread one element of kStencilProbes
+// probes per loop trip: the operator's diagonals at the element are read once
+// for all of them (they are shared by the probes), the probes' loads are
+// independent.  Grid (ceil(N / (256 * kStencilElems)), ceil(P / kStencilProbes)).
+constexpr int kStencilProbes = 4;
+constexpr int kStencilElems = 4;
+
+// The off-diagonal couplings of element i (zero across an edge).
+struct Stencil {
+  float2 w, e, s, n;
+  int f;
+};
+__device__ __forceinline__ Stencil stencil_at(const C3Params &q, int i) {
+  const float2 z = make_float2(0.f, 0.f);
+  Stencil k;
+  k.f = i % q.nf;
+  k.w = k.f > 0 ? q.kw[i] : z;
+  k.e = k.f < q.nf - 1 ? q.ke[i] : z;
+  k.s = i >= q.nf ? q.ks[i] : z;
+  k.n = i + q.nf < q.N ? q.kn[i] : z;
+  return k;
+}
+// K_off x at element i (same operation order as apply_P).
+__device__ __forceinline__ float2 stencil_off(const C3Params &q, const Stencil &k, const float2 *__restrict__ x, int i,
+                                              float2 acc) {
+  if (k.f > 0) acc = cfma(k.w, x[i - 1], acc);
+  if (k.f < q.nf - 1) acc = cfma(k.e, x[i + 1], acc);
+  if (i >= q.nf) acc = cfma(k.s, x[i - q.nf], acc);
+  if (i + q.nf < q.N) acc = cfma(k.n, x[i + q.nf], acc);
+  return acc;
+}
+
+// Probes p0 .. p0 + kStencilProbes - 1 of this CTA that still iterate.
+__device__ __forceinline__ unsigned pending_mask(const Krylov *K, int p0, int P) {
+  unsigned m = 0;
+#pragma unroll
+  for (int j = 0; j < kStencilProbes; ++j)
+    if (p0 + j < P && !K[p0 + j].done) m |= 1u << j;
+  return m;
+}
+
+// r0 = rhs = (P_l + P_r) u + src and its norm; the first iteration reads r0
+// as r and takes x = p = v = 0 without reading them.  The step t decides the
+// terms: the exact adjoint's right-hand side uses the next slice's operator
+// (cdr) and has no u term at t = 1 (lambda_{L+1} = 0); the per-probe source
+// enters at t = 1; src_shared is (L, N) by step.
 __global__ void __launch_bounds__(k3Threads) c3_init_kernel(const C3Params q, const C3State *st, int adj_exact,
                                                             const float2 *__restrict__ cdl, const float2 *__restrict__ cdn,
                                                             const float2 *__restrict__ u, const float2 *__restrict__ src_exit,
                                                             const float2 *__restrict__ src_shared, float2 *r0,
                                                             Krylov *K) {
-  __shared__ double red[k3Threads / 32];
-  const int pr = blockIdx.y;
-  const size_t off = (size_t)pr * q.N;
+  __shared__ double red[kStencilProbes * (k3Threads / 32)];
+  const int p0 = blockIdx.y * kStencilProbes;
+  const int np = q.P - p0 < kStencilProbes ? q.P - p0 : kStencilProbes;
   const int t = st->t;
   const int use_u = !(adj_exact && t == 1);
   const float2 *cdr = (adj_exact && t > 1) ? cdn : cdl;
   const float2 *src = (t == 1) ? src_exit : nullptr;
   const float2 *shared = src_shared ? src_shared + (size_t)(t - 1) * q.N : nullptr;
-  double acc = 0.0;
+  double acc[kStencilProbes] = {};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
     // (P_l + P_r) u = (cd_l + cd_r) u + 2 K_off u: the two operators differ only on the diagonal
-    float2 b = make_float2(0.f, 0.f);
+    Stencil k{};
+    float2 dsum = make_float2(0.f, 0.f);
     if (use_u) {
-      const float2 *uu = u + off;
-      float2 o = make_float2(0.f, 0.f);
-      const int f = i % q.nf;
-      if (f > 0) o = cfma(q.kw[i], uu[i - 1], o);
-      if (f < q.nf - 1) o = cfma(q.ke[i], uu[i + 1], o);
-      if (i >= q.nf) o = cfma(q.ks[i], uu[i - q.nf], o);
-      if (i + q.nf < q.N) o = cfma(q.kn[i], uu[i + q.nf], o);
-      b = cfma(cadd(cdl[i], cdr[i]), uu[i], cadd(o, o));
+      k = stencil_at(q, i);
+      dsum = cadd(cdl[i], cdr[i]);
     }
-    if (src != nullptr) b = cadd(b, src[off + i]);
-    if (shared != nullptr) b = cadd(b, shared[i]);
-    r0[off + i] = b;
-    acc += (double)b.x * b.x + (double)b.y * b.y;
+    const float2 sh = shared != nullptr ? shared[i] : make_float2(0.f, 0.f);
+#pragma unroll
+    for (int j = 0; j < kStencilProbes; ++j) {
+      if (j >= np) break;
+      const size_t off = (size_t)(p0 + j) * q.N;
+      float2 b = make_float2(0.f, 0.f);
+      if (use_u) {
+        const float2 *uu = u + off;
+        const float2 o = stencil_off(q, k, uu, i, make_float2(0.f, 0.f));
+        b = cfma(dsum, uu[i], cadd(o, o));
+      }
+      if (src != nullptr) b = cadd(b, src[off + i]);
+      if (shared != nullptr) b = cadd(b, sh);
+      r0[off + i] = b;
+      acc[j] += (double)b.x * b.x + (double)b.y * b.y;
+    }
   }
-  block_reduce_add(acc, &K[pr].bnorm2, red);
+  block_reduce_many(acc, red, [&](int m, double v) {
+    if (m < np) atomicAdd(&K[p0 + m].bnorm2, v);
+  });
 }
 
 // Per probe: start a solve (rho = <r0, r0>, done when the right-hand side is zero).
@@ -266,12 +335,14 @@ __global__ void c3_twiddle_kernel(int n, float2 *tw) {
 }
 
 // Inverse of the periodic symbol, scaled by 1/(nf nb) (the normalisation of
-// the inverse 2D transform), transposed: sym[f * nb + b] =
-// 1 / ((1 - mu_x (2 cos(2 pi f/nf) - 2) - mu_y (2 cos(2 pi b/nb) - 2)) nf nb).
-__global__ void c3_symbol_kernel(const C3Params q, float2 *sym) {
+// the inverse 2D transform):
+// 1 / ((1 - mu_x (2 cos(2 pi f/nf) - 2) - mu_y (2 cos(2 pi b/nb) - 2)) nf nb),
+// at sym[f * nb + b] (transposed, for the Stockham column kernel) or at
+// sym[b * nf + f] (natural, for the four-step column kernel).
+__global__ void c3_symbol_kernel(const C3Params q, int natural, float2 *sym) {
   const double sc = 1.0 / ((double)q.nf * (double)q.nb);
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < q.N; e += gridDim.x * blockDim.x) {
-    const int f = e / q.nb, bb = e - f * q.nb;
+    const int f = natural ? e % q.nf : e / q.nb, bb = natural ? e / q.nf : e - f * q.nb;
     double sf, cf, sb, cbv;
     sincospi(2.0 * (double)f / (double)q.nf, &sf, &cf);
     sincospi(2.0 * (double)bb / (double)q.nb, &sb, &cbv);
@@ -404,39 +475,237 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_inv_kernel(const FftPl
   for (int e = threadIdx.x; e < tot; e += blockDim.x) out[off + e] = res[slot(e)];
 }
 
-// out = (I - P) y with fused fp64 dots: which 0: acc_r0v += <r0, out>;
-// which 1: acc_ts += <out, s>, acc_tt += <out, out>.
+// Padded twiddle table of the four-step transforms of length n = R1 R2:
+// tw[k1 * (R2 + 1) + n2] = W_n^{n2 k1} (fp64 sincospi, rounded once).
+__global__ void c3_twiddle4_kernel(int n, int r1, int r2, float2 *tw) {
+  for (int e = threadIdx.x; e < r1 * (r2 + 1); e += blockDim.x) {
+    const int k1 = e / (r2 + 1), n2 = e % (r2 + 1);
+    double sv, cv;
+    sincospi(-2.0 * (double)((n2 * k1) % n) / (double)n, &sv, &cv);
+    tw[e] = n2 < r2 ? make_float2((float)cv, (float)sv) : make_float2(0.f, 0.f);
+  }
+}
+
+// The preconditioner input of mode 0 / 1 / 2 at element e of a probe's vector
+// (see c3_prec_rows_kernel), storing p or s on the way.
+struct PrecInput {
+  int mode, first, second;
+  float2 bt, om, al;
+  const float2 *r, *pin, *v, *r0;
+  float2 *p, *s;
+  __device__ __forceinline__ float2 operator()(size_t e) const {
+    if (mode == 2) return r[e];
+    if (mode == 0) {
+      if (first) return r0[e];
+      const float2 pv = cfma(bt, cfnma(om, v[e], pin[e]), r[e]);
+      p[e] = pv;
+      return pv;
+    }
+    const float2 sv = cfnma(al, v[e], first ? r0[e] : r[e]);
+    s[e] = sv;
+    return sv;
+  }
+};
+
+__device__ __forceinline__ PrecInput prec_input(int mode, const float2 *r, float2 *p, const float2 *v, float2 *s,
+                                                const float2 *r0, const Krylov *K, int pr, const C3State *st) {
+  PrecInput in{};
+  in.mode = mode;
+  in.r = r;
+  in.p = p;
+  in.v = v;
+  in.s = s;
+  in.r0 = r0;
+  if (mode == 2) return in;
+  const int it = st->it;
+  in.first = it == 0;
+  const Krylov &k = K[pr];
+  if (mode == 0) {
+    if (it > 0) {
+      const double den = k.rho_prev.x * k.rho_prev.x + k.rho_prev.y * k.rho_prev.y;
+      const double2 beta = den > 0.0 ? zmul(zdiv(k.rho_cur, k.rho_prev), zdiv(k.alpha, k.omega)) : z2(0, 0);
+      in.bt = to_f2(beta);
+      in.om = to_f2(k.omega);
+      in.pin = (it == 1) ? r0 : p;
+    }
+  } else {
+    const double den = k.acc_r0v.x * k.acc_r0v.x + k.acc_r0v.y * k.acc_r0v.y;
+    in.al = to_f2(den > 0.0 ? zdiv(k.rho_cur, k.acc_r0v) : z2(0, 0));
+  }
+  return in;
+}
+
+// Four-step preconditioner kernels for nf = nb = R1 R2 (R1 >= R2): 256
+// threads, 256 / R1 rows (or columns) per CTA, one short DFT per thread and
+// stage, one shared-memory transpose per transform.
+//
+// Forward row transforms of the preconditioner input (formed as in
+// c3_prec_rows_kernel) into hat, natural frequency order.  Grid (nb / RPC, P).
+template <int R1, int R2>
+__global__ void __launch_bounds__(256) c3_rows4_kernel(const C3Params q, int mode, const float2 *r, float2 *p,
+                                                       const float2 *v, float2 *s, float2 *hat, const Krylov *K,
+                                                       const float2 *__restrict__ twg, const float2 *r0,
+                                                       const C3State *st) {
+  constexpr int N = R1 * R2, RPC = 256 / R1, S = R1 * (R2 + 1);
+  __shared__ float2 buf[RPC * S];
+  __shared__ float2 tw[R1 * (R2 + 1)];
+  const int pr = blockIdx.y;
+  if (K != nullptr && K[pr].done) return;
+  for (int e = threadIdx.x; e < R1 * (R2 + 1); e += 256) tw[e] = twg[e];
+  const PrecInput in = prec_input(mode, r, p, v, s, r0, K, pr, st);
+  const size_t off = (size_t)pr * q.N + (size_t)blockIdx.x * RPC * N;
+  __syncthreads();
+  if (threadIdx.x < RPC * R2) {  // stage A: (row, n2)
+    const int row = threadIdx.x / R2, n2 = threadIdx.x % R2;
+    float2 x[16];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) x[n1] = in(off + row * N + R2 * n1 + n2);
+    dft_reg<R1>(x, -1.f);
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1)
+      buf[row * S + k1 * (R2 + 1) + n2] = k1 ? cmul(x[k1], tw[k1 * (R2 + 1) + n2]) : x[0];
+  }
+  __syncthreads();
+  {  // stage C: (row, k1)
+    const int row = threadIdx.x / R1, k1 = threadIdx.x % R1;
+    float2 x[16];
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2) x[n2] = buf[row * S + k1 * (R2 + 1) + n2];
+    dft_reg<R2>(x, -1.f);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) hat[off + row * N + k1 + R1 * k2] = x[k2];
+  }
+}
+
+// Column transforms of hat in place: forward, times the inverse symbol
+// (natural layout), inverse.  Grid (nf / CPC, P).
+template <int R1, int R2>
+__global__ void __launch_bounds__(256, R1 * R2 == 256 ? 3 : 4) c3_cols4_kernel(const C3Params q, float2 *hat, const Krylov *K,
+                                                       const float2 *__restrict__ twg,
+                                                       const float2 *__restrict__ sym) {
+  constexpr int N = R1 * R2, CPC = 256 / R1;
+  __shared__ float2 buf[N * CPC];  // [k1][n2][c]
+  __shared__ float2 tw[R1 * (R2 + 1)];
+  const int pr = blockIdx.y;
+  if (K != nullptr && K[pr].done) return;
+  for (int e = threadIdx.x; e < R1 * (R2 + 1); e += 256) tw[e] = twg[e];
+  const int nf = q.nf, f0 = blockIdx.x * CPC;
+  float2 *base = hat + (size_t)pr * q.N + f0;
+  __syncthreads();
+  float2 x[16];
+  if (threadIdx.x < CPC * R2) {  // stage A: (c, n2), c fastest
+    const int c = threadIdx.x % CPC, n2 = threadIdx.x / CPC;
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) x[n1] = base[(size_t)(R2 * n1 + n2) * nf + c];
+    dft_reg<R1>(x, -1.f);
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1)
+      buf[(k1 * R2 + n2) * CPC + c] = k1 ? cmul(x[k1], tw[k1 * (R2 + 1) + n2]) : x[0];
+  }
+  __syncthreads();
+  {  // stage C and its inverse: (c, k1)
+    const int c = threadIdx.x % CPC, k1 = threadIdx.x / CPC;
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2) x[n2] = buf[(k1 * R2 + n2) * CPC + c];
+    dft_reg<R2>(x, -1.f);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) x[k2] = cmul(x[k2], sym[(size_t)(k1 + R1 * k2) * nf + f0 + c]);
+    dft_reg<R2>(x, 1.f);
+    __syncthreads();  // every stage-C read is done before the buffer is rewritten
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2)
+      buf[(k1 * R2 + n2) * CPC + c] = n2 ? cmulc(x[n2], tw[k1 * (R2 + 1) + n2]) : x[0];
+  }
+  __syncthreads();
+  if (threadIdx.x < CPC * R2) {  // inverse stage A: (c, n2)
+    const int c = threadIdx.x % CPC, n2 = threadIdx.x / CPC;
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) x[k1] = buf[(k1 * R2 + n2) * CPC + c];
+    dft_reg<R1>(x, 1.f);
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) base[(size_t)(R2 * n1 + n2) * nf + c] = x[n1];
+  }
+}
+
+// Inverse row transforms of hat into out (the 1/(nf nb) scale is in the
+// symbol).  Grid (nb / RPC, P).
+template <int R1, int R2>
+__global__ void __launch_bounds__(256) c3_rows4_inv_kernel(const C3Params q, const float2 *hat, float2 *out,
+                                                           const Krylov *K, const float2 *__restrict__ twg) {
+  constexpr int N = R1 * R2, RPC = 256 / R1, S = R1 * (R2 + 1);
+  __shared__ float2 buf[RPC * S];
+  __shared__ float2 tw[R1 * (R2 + 1)];
+  const int pr = blockIdx.y;
+  if (K != nullptr && K[pr].done) return;
+  for (int e = threadIdx.x; e < R1 * (R2 + 1); e += 256) tw[e] = twg[e];
+  const size_t off = (size_t)pr * q.N + (size_t)blockIdx.x * RPC * N;
+  __syncthreads();
+  {  // inverse stage C: (row, k1)
+    const int row = threadIdx.x / R1, k1 = threadIdx.x % R1;
+    float2 x[16];
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) x[k2] = hat[off + row * N + k1 + R1 * k2];
+    dft_reg<R2>(x, 1.f);
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2)
+      buf[row * S + k1 * (R2 + 1) + n2] = n2 ? cmulc(x[n2], tw[k1 * (R2 + 1) + n2]) : x[0];
+  }
+  __syncthreads();
+  if (threadIdx.x < RPC * R2) {  // inverse stage A: (row, n2)
+    const int row = threadIdx.x / R2, n2 = threadIdx.x % R2;
+    float2 x[16];
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) x[k1] = buf[row * S + k1 * (R2 + 1) + n2];
+    dft_reg<R1>(x, 1.f);
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) out[off + row * N + R2 * n1 + n2] = x[n1];
+  }
+}
+
+// out = (I - P) y with fused fp64 dots: WHICH 0: acc_r0v += <r0, out>;
+// WHICH 1: acc_ts += <out, s>, acc_tt += <out, out>.
+template <int WHICH>
 __global__ void __launch_bounds__(k3Threads) c3_matvec_kernel(const C3Params q, const float2 *__restrict__ cd,
                                                               const float2 *__restrict__ y, float2 *__restrict__ out,
                                                               const float2 *__restrict__ r0, const float2 *__restrict__ s,
-                                                              Krylov *K, int which) {
-  __shared__ double red[k3Threads / 32];
-  const int pr = blockIdx.y;
-  if (K[pr].done) return;
-  const size_t off = (size_t)pr * q.N;
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+                                                              Krylov *K) {
+  constexpr int A = WHICH == 0 ? 2 : 3;  // sums per probe
+  __shared__ double red[A * kStencilProbes * (k3Threads / 32)];
+  const int p0 = blockIdx.y * kStencilProbes;
+  const unsigned pend = pending_mask(K, p0, q.P);
+  if (pend == 0) return;
+  const float2 *c_in = WHICH == 0 ? r0 : s;
+  double acc[A * kStencilProbes] = {};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
-    const float2 t = csub(y[off + i], apply_P(q, cd, y + off, i));
-    out[off + i] = t;
-    const float2 c = (which == 0) ? r0[off + i] : s[off + i];
-    if (which == 0) {  // conj(r0) t
-      a0 += (double)c.x * t.x + (double)c.y * t.y;
-      a1 += (double)c.x * t.y - (double)c.y * t.x;
-    } else {  // conj(t) s, |t|^2
-      a0 += (double)t.x * c.x + (double)t.y * c.y;
-      a1 += (double)t.x * c.y - (double)t.y * c.x;
-      a2 += (double)t.x * t.x + (double)t.y * t.y;
+    const Stencil k = stencil_at(q, i);
+    const float2 dc = cd[i];
+#pragma unroll
+    for (int j = 0; j < kStencilProbes; ++j) {
+      if (!(pend & (1u << j))) continue;
+      const size_t off = (size_t)(p0 + j) * q.N;
+      const float2 *yy = y + off;
+      const float2 yi = yy[i];
+      const float2 t = csub(yi, stencil_off(q, k, yy, i, cmul(dc, yi)));
+      out[off + i] = t;
+      const float2 c = c_in[off + i];
+      if (WHICH == 0) {  // conj(r0) t
+        acc[A * j] += (double)c.x * t.x + (double)c.y * t.y;
+        acc[A * j + 1] += (double)c.x * t.y - (double)c.y * t.x;
+      } else {  // conj(t) s, |t|^2
+        acc[A * j] += (double)t.x * c.x + (double)t.y * c.y;
+        acc[A * j + 1] += (double)t.x * c.y - (double)t.y * c.x;
+        acc[A * j + 2] += (double)t.x * t.x + (double)t.y * t.y;
+      }
     }
   }
-  Krylov &k = K[pr];
-  if (which == 0) {
-    block_reduce_add(a0, &k.acc_r0v.x, red);
-    block_reduce_add(a1, &k.acc_r0v.y, red);
-  } else {
-    block_reduce_add(a0, &k.acc_ts.x, red);
-    block_reduce_add(a1, &k.acc_ts.y, red);
-    block_reduce_add(a2, &k.acc_tt, red);
-  }
+  block_reduce_many(acc, red, [&](int m, double v) {
+    const int j = m / A, c = m % A;
+    if (!(pend & (1u << j))) return;
+    Krylov &kr = K[p0 + j];
+    double *dst = WHICH == 0 ? (c == 0 ? &kr.acc_r0v.x : &kr.acc_r0v.y)
+                             : (c == 0 ? &kr.acc_ts.x : (c == 1 ? &kr.acc_ts.y : &kr.acc_tt));
+    atomicAdd(dst, v);
+  });
 }
 
 // omega = <t,s>/<t,t>; x += alpha y + omega z (x = 0 before the first
@@ -447,7 +716,7 @@ __global__ void __launch_bounds__(k3Threads) c3_update_kernel(const C3Params q, 
                                                               const float2 *__restrict__ z, const float2 *__restrict__ s,
                                                               const float2 *__restrict__ t, Krylov *K,
                                                               const C3State *st) {
-  __shared__ double red[k3Threads / 32];
+  __shared__ double red[3 * (k3Threads / 32)];
   const int pr = blockIdx.y;
   Krylov &k = K[pr];
   if (k.done) return;
@@ -468,41 +737,56 @@ __global__ void __launch_bounds__(k3Threads) c3_update_kernel(const C3Params q, 
     a1 += (double)c.x * rv.y - (double)c.y * rv.x;
     a2 += (double)rv.x * rv.x + (double)rv.y * rv.y;
   }
-  block_reduce_add(a0, &k.acc_r0r.x, red);
-  block_reduce_add(a1, &k.acc_r0r.y, red);
-  block_reduce_add(a2, &k.acc_rr, red);
+  double acc[3] = {a0, a1, a2};
+  block_reduce_many(acc, red, [&](int m, double v) { atomicAdd(m == 0 ? &k.acc_r0r.x : (m == 1 ? &k.acc_r0r.y : &k.acc_rr), v); });
 }
 
 // True residual of each solve: res2 = ||rhs - (I - P) d||^2 (rhs = r0, d = x),
 // then u += d, stored into node `to` of u_store (to = t, or L - t for the
 // flipped reference adjoint) and, at the last step, into exit_out.
-// Grid (chunks, P).
 __global__ void __launch_bounds__(k3Threads) c3_finish_kernel(const C3Params q, const C3State *st,
                                                               const float2 *__restrict__ cd,
                                                               const float2 *__restrict__ x, const float2 *__restrict__ r0,
                                                               float2 *u, Krylov *K, float2 *u_store, int flip,
                                                               float2 *exit_out) {
-  __shared__ double red[k3Threads / 32];
-  const int pr = blockIdx.y;
-  const size_t off = (size_t)pr * q.N;
+  __shared__ double red[kStencilProbes * (k3Threads / 32)];
+  const int p0 = blockIdx.y * kStencilProbes;
+  const int np = q.P - p0 < kStencilProbes ? q.P - p0 : kStencilProbes;
   const int t = st->t;
-  float2 *dst = u_store ? u_store + ((size_t)pr * q.nz + (flip ? q.L - t : t)) * q.N : nullptr;
-  float2 *ex = (exit_out && t == q.L) ? exit_out + off : nullptr;
+  const size_t node = flip ? q.L - t : t;
   // a probe whose right-hand side was zero did not iterate: its update is 0
   // (x then holds an earlier step's values)
-  const bool iterated = K[pr].iters > 0;
-  double acc = 0.0;
+  unsigned iterated = 0;
+#pragma unroll
+  for (int j = 0; j < kStencilProbes; ++j)
+    if (j < np && K[p0 + j].iters > 0) iterated |= 1u << j;
+  double acc[kStencilProbes] = {};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
-    const float2 xi = iterated ? x[off + i] : make_float2(0.f, 0.f);
-    const float2 mx = iterated ? csub(xi, apply_P(q, cd, x + off, i)) : xi;
-    const float2 d = csub(r0[off + i], mx);
-    acc += (double)d.x * d.x + (double)d.y * d.y;
-    const float2 un = cadd(u[off + i], xi);
-    u[off + i] = un;
-    if (dst) dst[i] = un;
-    if (ex) ex[i] = un;
+    Stencil k{};
+    float2 dc = make_float2(0.f, 0.f);
+    if (iterated) {
+      k = stencil_at(q, i);
+      dc = cd[i];
+    }
+#pragma unroll
+    for (int j = 0; j < kStencilProbes; ++j) {
+      if (j >= np) break;
+      const int pr = p0 + j;
+      const size_t off = (size_t)pr * q.N;
+      const bool it = iterated & (1u << j);
+      const float2 xi = it ? x[off + i] : make_float2(0.f, 0.f);
+      const float2 mx = it ? csub(xi, stencil_off(q, k, x + off, i, cmul(dc, xi))) : xi;
+      const float2 d = csub(r0[off + i], mx);
+      acc[j] += (double)d.x * d.x + (double)d.y * d.y;
+      const float2 un = cadd(u[off + i], xi);
+      u[off + i] = un;
+      if (u_store) u_store[((size_t)pr * q.nz + node) * q.N + i] = un;
+      if (exit_out && t == q.L) exit_out[off + i] = un;
+    }
   }
-  block_reduce_add(acc, &K[pr].res2, red);
+  block_reduce_many(acc, red, [&](int m, double v) {
+    if (m < np) atomicAdd(&K[p0 + m].res2, v);
+  });
 }
 
 // After a step (one CTA loops over the probes): accumulate the statistics
@@ -538,12 +822,24 @@ __global__ void c3_store_kernel(int N, int P, int nz, int t, const float2 *__res
 // over the probes).
 __global__ void c3_grad_kernel(int N, int P, int nz, const C3State *st, const float2 *__restrict__ lam,
                                const float2 *__restrict__ u_fwd, float2 *grad_c) {
+  constexpr int G = 8;  // probes whose loads are issued together
   const int s = st->s;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
     float2 acc = make_float2(0.f, 0.f);
-    for (int pr = 0; pr < P; ++pr) {
-      const float2 w = cadd(u_fwd[((size_t)pr * nz + s) * N + i], u_fwd[((size_t)pr * nz + s - 1) * N + i]);
-      acc = cadd(acc, cmulc(lam[(size_t)pr * N + i], w));
+    for (int p0 = 0; p0 < P; p0 += G) {
+      float2 a[G], b[G], l[G];
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        if (p0 + j < P) {
+          const size_t pr = p0 + j;
+          a[j] = u_fwd[(pr * nz + s) * N + i];
+          b[j] = u_fwd[(pr * nz + s - 1) * N + i];
+          l[j] = lam[pr * N + i];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < G; ++j)
+        if (p0 + j < P) acc = cadd(acc, cmulc(l[j], cadd(a[j], b[j])));
     }
     float2 g = grad_c[(size_t)(s - 1) * N + i];
     grad_c[(size_t)(s - 1) * N + i] = cadd(g, acc);
@@ -666,6 +962,7 @@ struct C3Work {
   float2 *cdl, *cdr;
   float2 *dc, *dw, *de, *ds, *dn;
   float2 *sym, *twf, *twb;  // preconditioner symbol (N) and twiddle tables
+  float2 *tw4;              // padded twiddle table of the four-step transforms
   Krylov *K;
   C3State *st;
   size_t bytes;
@@ -688,6 +985,7 @@ static C3Work c3_layout(char *base, int N, int P) {
   for (float2 **d : diag) *d = reinterpret_cast<float2 *>(take((size_t)N * sizeof(float2)));
   w.twf = reinterpret_cast<float2 *>(take((size_t)kFftMaxN * sizeof(float2)));
   w.twb = reinterpret_cast<float2 *>(take((size_t)kFftMaxN * sizeof(float2)));
+  w.tw4 = reinterpret_cast<float2 *>(take((size_t)four_tw_len(256) * sizeof(float2)));
   w.K = reinterpret_cast<Krylov *>(take((size_t)P * sizeof(Krylov)));
   w.st = reinterpret_cast<C3State *>(take(sizeof(C3State)));
   w.bytes = off;
@@ -725,6 +1023,35 @@ static PrecKernels prec_kernels(int nf, int nb) {
     }
   }
   return prec_kernels_t<0, 0>();
+}
+
+using Rows4Kernel = void (*)(const C3Params, int, const float2 *, float2 *, const float2 *, float2 *, float2 *,
+                            const Krylov *, const float2 *, const float2 *, const C3State *);
+using Cols4Kernel = void (*)(const C3Params, float2 *, const Krylov *, const float2 *, const float2 *);
+using Inv4Kernel = void (*)(const C3Params, const float2 *, float2 *, const Krylov *, const float2 *);
+struct Prec4Kernels {
+  Rows4Kernel rows = nullptr;
+  Cols4Kernel cols = nullptr;
+  Inv4Kernel inv = nullptr;
+  int r1 = 0, r2 = 0;
+};
+
+template <int R1, int R2>
+static Prec4Kernels prec4_kernels_t() {
+  return {c3_rows4_kernel<R1, R2>, c3_cols4_kernel<R1, R2>, c3_rows4_inv_kernel<R1, R2>, R1, R2};
+}
+
+// Register four-step kernels for square grids of 64, 128, 192 and 256 (rows
+// kernel nullptr otherwise).
+static Prec4Kernels prec4_kernels(int nf, int nb) {
+  if (nf != nb || !four_step_size(nf)) return {};
+  static_assert(four_r1(64) == 8 && four_r1(128) == 16 && four_r1(192) == 16 && four_r1(256) == 16, "plans");
+  switch (nf) {
+    case 64: return prec4_kernels_t<8, 8>();
+    case 128: return prec4_kernels_t<16, 8>();
+    case 192: return prec4_kernels_t<16, 12>();
+    default: return prec4_kernels_t<16, 16>();
+  }
 }
 
 // FFT rows per CTA: at most 16 and 4096 elements, and a divisor of the row count.
@@ -898,6 +1225,9 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   const int use_fft = fft_on;
   // kernels of the preconditioner: compile-time FFT plans for the common sizes
   PrecKernels pk = prec_kernels(nf, nb);
+  const Prec4Kernels p4 = (fft_on && a->fft_kernels == 0) ? prec4_kernels(nf, nb) : Prec4Kernels{};
+  const bool four = p4.rows != nullptr;
+  const int rpc4 = four ? 256 / p4.r1 : 1;
   const int srow_f = pk.fixed ? nf + nf / 8 + 1 : nf, srow_b = pk.fixed ? nb + nb / 8 + 1 : nb;
   const size_t smem_rows = (size_t)(nf + 2 * rpc * srow_f) * sizeof(float2);
   const size_t smem_cols = (size_t)(nb + 2 * cpc * srow_b) * sizeof(float2);
@@ -923,6 +1253,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   if (learned)
     TP_CHECK_CUDA(cudaFuncSetAttribute(c3_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_filter));
   const dim3 vgrid((N + 256 * 8 - 1) / (256 * 8), P);
+  const dim3 sgrid((N + 256 * kStencilElems - 1) / (256 * kStencilElems), (P + kStencilProbes - 1) / kStencilProbes);
   const int pgrid = (P + 127) / 128;
   const int one_cta = P >= 1024 ? 1024 : ((P + 31) / 32) * 32;
   const int eb = 296;
@@ -931,6 +1262,12 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   // ---- launch sequences (recorded into a graph, or issued step by step)
   // M0^{-1} in -> out (mode 0/1/2 input of the row kernel; Kp NULL = all probes)
   auto precondition = [&](cudaStream_t s, int mode, const float2 *rin, float2 *out, const Krylov *Kp) {
+    if (four) {
+      p4.rows<<<dim3(nb / rpc4, P), 256, 0, s>>>(q, mode, rin, w.p, w.v, w.s, w.hat, Kp, w.tw4, w.r0, w.st);
+      p4.cols<<<dim3(nf / rpc4, P), 256, 0, s>>>(q, w.hat, Kp, w.tw4, w.sym);
+      p4.inv<<<dim3(nb / rpc4, P), 256, 0, s>>>(q, w.hat, out, Kp, w.tw4);
+      return;
+    }
     pk.rows<<<dim3(nb / rows_cta, P), k3Threads, use_fft ? smem_rows : 0, s>>>(
         pf, q, mode, rin, w.p, w.v, w.s, use_fft ? w.hat : out, Kp, rows_cta, use_fft, w.twf, w.r0, w.st);
     if (use_fft) {
@@ -942,7 +1279,8 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     if (use_fft) {
       c3_twiddle_kernel<<<(nf + 255) / 256, 256, 0, s>>>(nf, w.twf);
       c3_twiddle_kernel<<<(nb + 255) / 256, 256, 0, s>>>(nb, w.twb);
-      c3_symbol_kernel<<<eb, 256, 0, s>>>(q, w.sym);
+      c3_symbol_kernel<<<eb, 256, 0, s>>>(q, four ? 1 : 0, w.sym);
+      if (four) c3_twiddle4_kernel<<<1, 256, 0, s>>>(nf, p4.r1, p4.r2, w.tw4);
     }
     c3_diag_kernel<<<eb, 256, 0, s>>>(N, nf, q.sigma, q.conj_t, static_cast<const float2 *>(op->kc),
                                       static_cast<const float2 *>(op->kw), static_cast<const float2 *>(op->ke),
@@ -977,7 +1315,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     c3_advance_kernel<<<1, 1, 0, s>>>(w.st, L, backward ? 1 : 0, use_cond, outer, inner);
     c3_center_kernel<<<eb, 256, 0, s>>>(q, w.st, 0, w.cdl);
     if (adj_exact) c3_center_kernel<<<eb, 256, 0, s>>>(q, w.st, 1, w.cdr);
-    c3_init_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.st, adj_exact, w.cdl, w.cdr, w.u,
+    c3_init_kernel<<<sgrid, k3Threads, 0, s>>>(q, w.st, adj_exact, w.cdl, w.cdr, w.u,
                                                 static_cast<const float2 *>(a->src_exit),
                                                 static_cast<const float2 *>(a->src_shared), w.r0, w.K);
     c3_start_kernel<<<pgrid, 128, 0, s>>>(w.K, P);
@@ -987,17 +1325,17 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     // p = r + beta (p - omega v); y = Prec(p); v = M y
     precondition(s, 0, w.r, learned ? lw.zt : w.y, w.K);
     if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.y, w.K, frb);
-    c3_matvec_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.cdl, w.y, w.v, w.r0, w.s, w.K, 0);
+    c3_matvec_kernel<0><<<sgrid, k3Threads, 0, s>>>(q, w.cdl, w.y, w.v, w.r0, w.s, w.K);
     // s = r - alpha v; z = Prec(s); t = M z
     precondition(s, 1, w.r, learned ? lw.zt : w.z, w.K);
     if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.z, w.K, frb);
-    c3_matvec_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K, 1);
+    c3_matvec_kernel<1><<<sgrid, k3Threads, 0, s>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K);
     c3_update_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.x, w.r, w.r0, w.y, w.z, w.s, w.t, w.K, w.st);
     c3_commit_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, w.st, max_iter, use_cond, inner);
   };
   // step tail: u += x (true residual, store), statistics, gradient
   auto step_tail = [&](cudaStream_t s) {
-    c3_finish_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.st, w.cdl, w.x, w.r0, w.u, w.K, ust, flip ? 1 : 0, exit_out);
+    c3_finish_kernel<<<sgrid, k3Threads, 0, s>>>(q, w.st, w.cdl, w.x, w.r0, w.u, w.K, ust, flip ? 1 : 0, exit_out);
     c3_stats_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, stats);
     if (a->grad_c)
       c3_grad_kernel<<<eb, 256, 0, s>>>(N, P, nz, w.st, w.u, static_cast<const float2 *>(a->u_fwd),
@@ -1116,7 +1454,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
         if (hs.pending == 0) break;
       }
     }
-    c3_finish_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.st, w.cdl, w.x, w.r0, w.u, w.K, ust, flip ? 1 : 0, exit_out);
+    c3_finish_kernel<<<sgrid, k3Threads, 0, st>>>(q, w.st, w.cdl, w.x, w.r0, w.u, w.K, ust, flip ? 1 : 0, exit_out);
     if (train && t % a->train_every == 0) {
       // training pair of this step: z0 = M0^{-1} v and x with (I - P_s) x = v,
       // v the step's right-hand side r0 and x its converged update

@@ -368,4 +368,78 @@ __device__ __forceinline__ void load_twiddles(float2 *tw, const float2 *__restri
   for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twg[t];
 }
 
+// ------------------------------------------------ register four-step transforms
+// A transform of length N = R1 * R2 with the short DFTs held in registers:
+// with n = R2 n1 + n2 and k = k1 + R1 k2,
+//   X[k1 + R1 k2] = sum_n2 W_R2^{n2 k2} W_N^{n2 k1} sum_n1 x[R2 n1 + n2] W_R1^{n1 k1}.
+// Stage A (one thread per n2): the R1-point DFT over n1 in registers, the
+// twiddles W_N^{n2 k1}, one write to shared memory; stage C (one thread per
+// k1): one read, the R2-point DFT over n2, giving X[k1 + R1 k2].  An element
+// passes through shared memory once (one write, one read) instead of once per
+// Stockham pass plus the staging copies.  The inverse runs the stages in the
+// opposite order with conjugate twiddles.  The twiddle table is padded like
+// the transpose: W_N^{n2 k1} at k1 * (R2 + 1) + n2, so that both stages read
+// it without bank conflicts.
+
+// 12-point DFT as 4 x 3 (n = 3 n1 + n2, k = k1 + 4 k2), natural order in and out.
+__device__ __forceinline__ void dft12(float2 (&v)[16], float sign) {
+  const float s3 = 0.86602540378443864676f;  // sin(pi / 3)
+  float2 y[12];
+#pragma unroll
+  for (int n2 = 0; n2 < 3; ++n2) {
+    float2 a0 = v[n2], a1 = v[3 + n2], a2 = v[6 + n2], a3 = v[9 + n2];
+    dft4_inplace(a0, a1, a2, a3, sign);
+    y[4 * n2] = a0;
+    y[4 * n2 + 1] = a1;
+    y[4 * n2 + 2] = a2;
+    y[4 * n2 + 3] = a3;
+  }
+  // W12^m = exp(sign 2 pi i m / 12) for m = n2 k1 in {1, 2, 3, 2, 4, 6}
+  const float2 w1 = make_float2(s3, sign * 0.5f), w2 = make_float2(0.5f, sign * s3), w3 = make_float2(0.f, sign);
+  const float2 w4 = make_float2(-0.5f, sign * s3), w6 = make_float2(-1.f, 0.f);
+  y[5] = cmul(y[5], w1);
+  y[6] = cmul(y[6], w2);
+  y[7] = cmul(y[7], w3);
+  y[9] = cmul(y[9], w2);
+  y[10] = cmul(y[10], w4);
+  y[11] = cmul(y[11], w6);
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    const float2 a = y[k1], b = y[4 + k1], c = y[8 + k1];
+    const float2 t = cadd(b, c);
+    const float2 d = mul_si(csub(b, c), sign * s3);
+    const float2 m = make_float2(a.x - 0.5f * t.x, a.y - 0.5f * t.y);
+    v[k1] = cadd(a, t);
+    v[k1 + 4] = cadd(m, d);
+    v[k1 + 8] = csub(m, d);
+  }
+}
+
+// R-point DFT (R = 4, 8, 12, 16) of v[0..R) in registers, natural order in and out.
+template <int R>
+__device__ __forceinline__ void dft_reg(float2 (&v)[16], float sign) {
+  static_assert(R == 4 || R == 8 || R == 12 || R == 16, "dft_reg: unsupported length");
+  if constexpr (R == 16) {
+    dft16(v, sign);
+  } else if constexpr (R == 12) {
+    dft12(v, sign);
+  } else if constexpr (R == 8) {
+    float2 w[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) w[j] = v[j];
+    dft_small<8>(w, sign);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = w[j];
+  } else {
+    dft4_inplace(v[0], v[1], v[2], v[3], sign);
+  }
+}
+
+// Factors of the lengths with a four-step plan (R1 >= R2, both <= 16).
+__host__ __device__ constexpr int four_r1(int n) { return n == 64 ? 8 : 16; }
+__host__ __device__ constexpr int four_r2(int n) { return n / four_r1(n); }
+__host__ __device__ constexpr bool four_step_size(int n) { return n == 64 || n == 128 || n == 192 || n == 256; }
+// Entries of the padded twiddle table.
+__host__ __device__ constexpr int four_tw_len(int n) { return four_r1(n) * (four_r2(n) + 1); }
+
 }  // namespace tp
