@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--small", action="store_true",
                     help="kernels case: 64 probes for the NLCG pieces and 16 for the multislice (~1 GB on the "
                          "device; the size of the profiler captures)")
+    ap.add_argument("--precond", choices=("learned", "fft"), default="learned",
+                    help="3d-march-small: the learned correction of the FFT preconditioner, or the plain one")
     ap.add_argument("--step-by-step", action="store_true",
                     help="3D cases: launch the march's kernels step by step instead of as one CUDA graph with "
                          "conditional loops (the same kernels; profilers list the kernels of such graphs only "
@@ -657,8 +659,9 @@ def run_ours(a):
 
 
 def run_case_3d_small(a):
-    """`steps` learned 3D forward marches on 256 x 256 x 5 nodes, 64 probes (config-2 probes and
-    ellipsoid distribution), after `warmup` untimed ones; an untrained network (seeded)."""
+    """`steps` 3D forward marches on 256 x 256 x 5 nodes, 64 probes (config-2 probes and ellipsoid
+    distribution), after `warmup` untimed ones; learned form with an untrained network (seeded), or the
+    plain FFT preconditioner (`--precond fft`)."""
     import torch
 
     from thick_ptycho_b200.cn3d import CN3D
@@ -680,12 +683,13 @@ def run_case_3d_small(a):
     for i in range(a.warmup + a.steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        eng.march(field, P, "forward", probes=probes, exit_out=ex, precond="learned", model=model)
+        eng.march(field, P, "forward", probes=probes, exit_out=ex, precond=a.precond if a.precond == "learned" else True,
+                  model=model)
         e1.record()
         torch.cuda.synchronize()
         if i >= a.warmup:
             ms.append(e0.elapsed_time(e1))
-    print(json.dumps({"case": "3d-march-small", "ms_per_march": statistics.median(ms) if ms else None,
+    print(json.dumps({"case": "3d-march-small", "precond": a.precond, "ms_per_march": statistics.median(ms) if ms else None,
                       "stats": eng.read_stats()}), flush=True)
 
 

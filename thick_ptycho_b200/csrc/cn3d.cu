@@ -187,10 +187,11 @@ __device__ __forceinline__ void block_reduce_many(double (&v)[M], double *red, F
 
 // The stencil kernels below give each thread one element of kStencilProbes
 // probes per loop trip: the operator's diagonals at the element are read once
-// for all of them (they are shared by the probes), the probes' loads are
-// independent.  Grid (ceil(N / (256 * kStencilElems)), ceil(P / kStencilProbes)).
+// for all of them (they are shared by the probes), and every load of the trip
+// precedes its stores, so the probes' loads are in flight together.  Grid
+// (gx, ceil(P / kStencilProbes)), gx chosen so that the grid is one wave of
+// resident CTAs (stencil_grid).
 constexpr int kStencilProbes = 4;
-constexpr int kStencilElems = 4;
 
 // The off-diagonal couplings of element i (zero across an edge).
 struct Stencil {
@@ -254,6 +255,7 @@ __global__ void __launch_bounds__(k3Threads) c3_init_kernel(const C3Params q, co
       dsum = cadd(cdl[i], cdr[i]);
     }
     const float2 sh = shared != nullptr ? shared[i] : make_float2(0.f, 0.f);
+    float2 bv[kStencilProbes];
 #pragma unroll
     for (int j = 0; j < kStencilProbes; ++j) {
       if (j >= np) break;
@@ -266,7 +268,13 @@ __global__ void __launch_bounds__(k3Threads) c3_init_kernel(const C3Params q, co
       }
       if (src != nullptr) b = cadd(b, src[off + i]);
       if (shared != nullptr) b = cadd(b, sh);
-      r0[off + i] = b;
+      bv[j] = b;
+    }
+#pragma unroll
+    for (int j = 0; j < kStencilProbes; ++j) {
+      if (j >= np) break;
+      const float2 b = bv[j];
+      r0[(size_t)(p0 + j) * q.N + i] = b;
       acc[j] += (double)b.x * b.x + (double)b.y * b.y;
     }
   }
@@ -335,14 +343,12 @@ __global__ void c3_twiddle_kernel(int n, float2 *tw) {
 }
 
 // Inverse of the periodic symbol, scaled by 1/(nf nb) (the normalisation of
-// the inverse 2D transform):
-// 1 / ((1 - mu_x (2 cos(2 pi f/nf) - 2) - mu_y (2 cos(2 pi b/nb) - 2)) nf nb),
-// at sym[f * nb + b] (transposed, for the Stockham column kernel) or at
-// sym[b * nf + f] (natural, for the four-step column kernel).
-__global__ void c3_symbol_kernel(const C3Params q, int natural, float2 *sym) {
+// the inverse 2D transform), transposed: sym[f * nb + b] =
+// 1 / ((1 - mu_x (2 cos(2 pi f/nf) - 2) - mu_y (2 cos(2 pi b/nb) - 2)) nf nb).
+__global__ void c3_symbol_kernel(const C3Params q, float2 *sym) {
   const double sc = 1.0 / ((double)q.nf * (double)q.nb);
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < q.N; e += gridDim.x * blockDim.x) {
-    const int f = natural ? e % q.nf : e / q.nb, bb = natural ? e / q.nf : e - f * q.nb;
+    const int f = e / q.nb, bb = e - f * q.nb;
     double sf, cf, sb, cbv;
     sincospi(2.0 * (double)f / (double)q.nf, &sf, &cf);
     sincospi(2.0 * (double)bb / (double)q.nb, &sb, &cbv);
@@ -475,6 +481,15 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_inv_kernel(const FftPl
   for (int e = threadIdx.x; e < tot; e += blockDim.x) out[off + e] = res[slot(e)];
 }
 
+// ab[f] = 2 cos(2 pi f / nf) - 2 (f < nf), ab[nf + b] = 2 cos(2 pi b / nb) - 2
+// (fp64, rounded once): the factors of the periodic symbol.
+__global__ void c3_symbol_factors_kernel(int nf, int nb, float *ab) {
+  for (int e = threadIdx.x; e < nf + nb; e += blockDim.x) {
+    const int j = e < nf ? e : e - nf, n = e < nf ? nf : nb;
+    ab[e] = (float)(2.0 * cospi(2.0 * (double)j / (double)n) - 2.0);
+  }
+}
+
 // Padded twiddle table of the four-step transforms of length n = R1 R2:
 // tw[k1 * (R2 + 1) + n2] = W_n^{n2 k1} (fp64 sincospi, rounded once).
 __global__ void c3_twiddle4_kernel(int n, int r1, int r2, float2 *tw) {
@@ -487,9 +502,11 @@ __global__ void c3_twiddle4_kernel(int n, int r1, int r2, float2 *tw) {
 }
 
 // The preconditioner input of mode 0 / 1 / 2 at element e of a probe's vector
-// (see c3_prec_rows_kernel), storing p or s on the way.
+// (see c3_prec_rows_kernel); loads only: the caller stores p (mode 0 after
+// the first iteration) or s (mode 1) after all its loads, so that they are
+// issued together rather than one memory latency per element.
 struct PrecInput {
-  int mode, first, second;
+  int mode, first;
   float2 bt, om, al;
   const float2 *r, *pin, *v, *r0;
   float2 *p, *s;
@@ -497,13 +514,15 @@ struct PrecInput {
     if (mode == 2) return r[e];
     if (mode == 0) {
       if (first) return r0[e];
-      const float2 pv = cfma(bt, cfnma(om, v[e], pin[e]), r[e]);
-      p[e] = pv;
-      return pv;
+      return cfma(bt, cfnma(om, v[e], pin[e]), r[e]);
     }
-    const float2 sv = cfnma(al, v[e], first ? r0[e] : r[e]);
-    s[e] = sv;
-    return sv;
+    return cfnma(al, v[e], first ? r0[e] : r[e]);
+  }
+  // where the formed input is stored (nullptr: not stored)
+  __device__ __forceinline__ float2 *dest() const {
+    if (mode == 0 && !first) return p;
+    if (mode == 1) return s;
+    return nullptr;
   }
 };
 
@@ -558,8 +577,13 @@ __global__ void __launch_bounds__(256) c3_rows4_kernel(const C3Params q, int mod
   if (threadIdx.x < RPC * R2) {  // stage A: (row, n2)
     const int row = threadIdx.x / R2, n2 = threadIdx.x % R2;
     float2 x[16];
+    const size_t e0 = off + (size_t)row * N + n2;
 #pragma unroll
-    for (int n1 = 0; n1 < R1; ++n1) x[n1] = in(off + row * N + R2 * n1 + n2);
+    for (int n1 = 0; n1 < R1; ++n1) x[n1] = in(e0 + R2 * n1);
+    if (float2 *dst = in.dest()) {
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) dst[e0 + R2 * n1] = x[n1];
+    }
     dft_reg<R1>(x, -1.f);
 #pragma unroll
     for (int k1 = 0; k1 < R1; ++k1)
@@ -577,19 +601,24 @@ __global__ void __launch_bounds__(256) c3_rows4_kernel(const C3Params q, int mod
   }
 }
 
-// Column transforms of hat in place: forward, times the inverse symbol
-// (natural layout), inverse.  Grid (nf / CPC, P).
+// Column transforms of hat in place: forward, times the inverse symbol,
+// inverse.  The symbol 1 / ((1 - mu_x a_f - mu_y a_b) nf nb) is formed on the
+// fly from the real tables a_f = 2 cos(2 pi f / nf) - 2 (ab[f]) and a_b
+// (ab[nf + b]), so no symbol array is read between the two transforms.
+// Grid (nf / CPC, P).
 template <int R1, int R2>
 __global__ void __launch_bounds__(256, R1 * R2 == 256 ? 3 : 4) c3_cols4_kernel(const C3Params q, float2 *hat, const Krylov *K,
                                                        const float2 *__restrict__ twg,
-                                                       const float2 *__restrict__ sym) {
+                                                       const float *__restrict__ ab) {
   constexpr int N = R1 * R2, CPC = 256 / R1;
   __shared__ float2 buf[N * CPC];  // [k1][n2][c]
   __shared__ float2 tw[R1 * (R2 + 1)];
+  __shared__ float bcos[N];
   const int pr = blockIdx.y;
   if (K != nullptr && K[pr].done) return;
   for (int e = threadIdx.x; e < R1 * (R2 + 1); e += 256) tw[e] = twg[e];
   const int nf = q.nf, f0 = blockIdx.x * CPC;
+  for (int e = threadIdx.x; e < N; e += 256) bcos[e] = ab[nf + e];
   float2 *base = hat + (size_t)pr * q.N + f0;
   __syncthreads();
   float2 x[16];
@@ -608,8 +637,19 @@ __global__ void __launch_bounds__(256, R1 * R2 == 256 ? 3 : 4) c3_cols4_kernel(c
 #pragma unroll
     for (int n2 = 0; n2 < R2; ++n2) x[n2] = buf[(k1 * R2 + n2) * CPC + c];
     dft_reg<R2>(x, -1.f);
+    {
+      const float sc = (float)(1.0 / ((double)nf * (double)N));
+      const float af = ab[f0 + c];
+      const float ax = (float)q.mu_x.x * af, ay = (float)q.mu_x.y * af;
+      const float mx = (float)q.mu_y.x, my = (float)q.mu_y.y;
 #pragma unroll
-    for (int k2 = 0; k2 < R2; ++k2) x[k2] = cmul(x[k2], sym[(size_t)(k1 + R1 * k2) * nf + f0 + c]);
+      for (int k2 = 0; k2 < R2; ++k2) {
+        const float bb = bcos[k1 + R1 * k2];
+        const float dr = 1.f - ax - mx * bb, di = -(ay + my * bb);
+        const float m = sc / (dr * dr + di * di);
+        x[k2] = cmul(x[k2], make_float2(dr * m, -di * m));
+      }
+    }
     dft_reg<R2>(x, 1.f);
     __syncthreads();  // every stage-C read is done before the buffer is rewritten
 #pragma unroll
@@ -665,7 +705,7 @@ __global__ void __launch_bounds__(256) c3_rows4_inv_kernel(const C3Params q, con
 // out = (I - P) y with fused fp64 dots: WHICH 0: acc_r0v += <r0, out>;
 // WHICH 1: acc_ts += <out, s>, acc_tt += <out, out>.
 template <int WHICH>
-__global__ void __launch_bounds__(k3Threads) c3_matvec_kernel(const C3Params q, const float2 *__restrict__ cd,
+__global__ void __launch_bounds__(k3Threads, WHICH == 0 ? 4 : 3) c3_matvec_kernel(const C3Params q, const float2 *__restrict__ cd,
                                                               const float2 *__restrict__ y, float2 *__restrict__ out,
                                                               const float2 *__restrict__ r0, const float2 *__restrict__ s,
                                                               Krylov *K) {
@@ -679,15 +719,21 @@ __global__ void __launch_bounds__(k3Threads) c3_matvec_kernel(const C3Params q, 
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
     const Stencil k = stencil_at(q, i);
     const float2 dc = cd[i];
+    float2 tv[kStencilProbes], cv[kStencilProbes];
 #pragma unroll
     for (int j = 0; j < kStencilProbes; ++j) {
       if (!(pend & (1u << j))) continue;
       const size_t off = (size_t)(p0 + j) * q.N;
       const float2 *yy = y + off;
       const float2 yi = yy[i];
-      const float2 t = csub(yi, stencil_off(q, k, yy, i, cmul(dc, yi)));
-      out[off + i] = t;
-      const float2 c = c_in[off + i];
+      tv[j] = csub(yi, stencil_off(q, k, yy, i, cmul(dc, yi)));
+      cv[j] = c_in[off + i];
+    }
+#pragma unroll
+    for (int j = 0; j < kStencilProbes; ++j) {
+      if (!(pend & (1u << j))) continue;
+      const float2 t = tv[j], c = cv[j];
+      out[(size_t)(p0 + j) * q.N + i] = t;
       if (WHICH == 0) {  // conj(r0) t
         acc[A * j] += (double)c.x * t.x + (double)c.y * t.y;
         acc[A * j + 1] += (double)c.x * t.y - (double)c.y * t.x;
@@ -744,7 +790,7 @@ __global__ void __launch_bounds__(k3Threads) c3_update_kernel(const C3Params q, 
 // True residual of each solve: res2 = ||rhs - (I - P) d||^2 (rhs = r0, d = x),
 // then u += d, stored into node `to` of u_store (to = t, or L - t for the
 // flipped reference adjoint) and, at the last step, into exit_out.
-__global__ void __launch_bounds__(k3Threads) c3_finish_kernel(const C3Params q, const C3State *st,
+__global__ void __launch_bounds__(k3Threads, 4) c3_finish_kernel(const C3Params q, const C3State *st,
                                                               const float2 *__restrict__ cd,
                                                               const float2 *__restrict__ x, const float2 *__restrict__ r0,
                                                               float2 *u, Krylov *K, float2 *u_store, int flip,
@@ -768,20 +814,26 @@ __global__ void __launch_bounds__(k3Threads) c3_finish_kernel(const C3Params q, 
       k = stencil_at(q, i);
       dc = cd[i];
     }
+    float2 unv[kStencilProbes];
 #pragma unroll
     for (int j = 0; j < kStencilProbes; ++j) {
       if (j >= np) break;
-      const int pr = p0 + j;
-      const size_t off = (size_t)pr * q.N;
+      const size_t off = (size_t)(p0 + j) * q.N;
       const bool it = iterated & (1u << j);
       const float2 xi = it ? x[off + i] : make_float2(0.f, 0.f);
       const float2 mx = it ? csub(xi, stencil_off(q, k, x + off, i, cmul(dc, xi))) : xi;
       const float2 d = csub(r0[off + i], mx);
       acc[j] += (double)d.x * d.x + (double)d.y * d.y;
-      const float2 un = cadd(u[off + i], xi);
-      u[off + i] = un;
-      if (u_store) u_store[((size_t)pr * q.nz + node) * q.N + i] = un;
-      if (exit_out && t == q.L) exit_out[off + i] = un;
+      unv[j] = cadd(u[off + i], xi);
+    }
+#pragma unroll
+    for (int j = 0; j < kStencilProbes; ++j) {
+      if (j >= np) break;
+      const int pr = p0 + j;
+      const size_t off = (size_t)pr * q.N;
+      u[off + i] = unv[j];
+      if (u_store) u_store[((size_t)pr * q.nz + node) * q.N + i] = unv[j];
+      if (exit_out && t == q.L) exit_out[off + i] = unv[j];
     }
   }
   block_reduce_many(acc, red, [&](int m, double v) {
@@ -963,6 +1015,7 @@ struct C3Work {
   float2 *dc, *dw, *de, *ds, *dn;
   float2 *sym, *twf, *twb;  // preconditioner symbol (N) and twiddle tables
   float2 *tw4;              // padded twiddle table of the four-step transforms
+  float *ab;                // 2 cos(2 pi f / nf) - 2, then the same for b / nb
   Krylov *K;
   C3State *st;
   size_t bytes;
@@ -986,6 +1039,7 @@ static C3Work c3_layout(char *base, int N, int P) {
   w.twf = reinterpret_cast<float2 *>(take((size_t)kFftMaxN * sizeof(float2)));
   w.twb = reinterpret_cast<float2 *>(take((size_t)kFftMaxN * sizeof(float2)));
   w.tw4 = reinterpret_cast<float2 *>(take((size_t)four_tw_len(256) * sizeof(float2)));
+  w.ab = reinterpret_cast<float *>(take((size_t)2 * kFftMaxN * sizeof(float)));
   w.K = reinterpret_cast<Krylov *>(take((size_t)P * sizeof(Krylov)));
   w.st = reinterpret_cast<C3State *>(take(sizeof(C3State)));
   w.bytes = off;
@@ -1027,7 +1081,7 @@ static PrecKernels prec_kernels(int nf, int nb) {
 
 using Rows4Kernel = void (*)(const C3Params, int, const float2 *, float2 *, const float2 *, float2 *, float2 *,
                             const Krylov *, const float2 *, const float2 *, const C3State *);
-using Cols4Kernel = void (*)(const C3Params, float2 *, const Krylov *, const float2 *, const float2 *);
+using Cols4Kernel = void (*)(const C3Params, float2 *, const Krylov *, const float2 *, const float *);
 using Inv4Kernel = void (*)(const C3Params, const float2 *, float2 *, const Krylov *, const float2 *);
 struct Prec4Kernels {
   Rows4Kernel rows = nullptr;
@@ -1052,6 +1106,23 @@ static Prec4Kernels prec4_kernels(int nf, int nb) {
     case 192: return prec4_kernels_t<16, 12>();
     default: return prec4_kernels_t<16, 16>();
   }
+}
+
+// Grid of a stencil kernel: ceil(P / kStencilProbes) probe groups times as
+// many element blocks as fill one wave of resident CTAs (at least 1, at most
+// one element per thread).
+template <class Kern>
+static dim3 stencil_grid(Kern kernel, int N, int P) {
+  int dev = 0, sms = 148, occ = 1;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, k3Threads, 0) != cudaSuccess || occ < 1) occ = 1;
+  (void)cudaGetLastError();
+  const int gy = (P + kStencilProbes - 1) / kStencilProbes;
+  int gx = (sms * occ) / gy;
+  const int gmax = (N + k3Threads - 1) / k3Threads;
+  if (gx > gmax) gx = gmax;
+  if (gx < 1) gx = 1;
+  return dim3(gx, gy);
 }
 
 // FFT rows per CTA: at most 16 and 4096 elements, and a divisor of the row count.
@@ -1253,7 +1324,8 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   if (learned)
     TP_CHECK_CUDA(cudaFuncSetAttribute(c3_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_filter));
   const dim3 vgrid((N + 256 * 8 - 1) / (256 * 8), P);
-  const dim3 sgrid((N + 256 * kStencilElems - 1) / (256 * kStencilElems), (P + kStencilProbes - 1) / kStencilProbes);
+  const dim3 sg_init = stencil_grid(c3_init_kernel, N, P), sg_fin = stencil_grid(c3_finish_kernel, N, P);
+  const dim3 sg_mv0 = stencil_grid(c3_matvec_kernel<0>, N, P), sg_mv1 = stencil_grid(c3_matvec_kernel<1>, N, P);
   const int pgrid = (P + 127) / 128;
   const int one_cta = P >= 1024 ? 1024 : ((P + 31) / 32) * 32;
   const int eb = 296;
@@ -1264,7 +1336,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   auto precondition = [&](cudaStream_t s, int mode, const float2 *rin, float2 *out, const Krylov *Kp) {
     if (four) {
       p4.rows<<<dim3(nb / rpc4, P), 256, 0, s>>>(q, mode, rin, w.p, w.v, w.s, w.hat, Kp, w.tw4, w.r0, w.st);
-      p4.cols<<<dim3(nf / rpc4, P), 256, 0, s>>>(q, w.hat, Kp, w.tw4, w.sym);
+      p4.cols<<<dim3(nf / rpc4, P), 256, 0, s>>>(q, w.hat, Kp, w.tw4, w.ab);
       p4.inv<<<dim3(nb / rpc4, P), 256, 0, s>>>(q, w.hat, out, Kp, w.tw4);
       return;
     }
@@ -1279,8 +1351,12 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     if (use_fft) {
       c3_twiddle_kernel<<<(nf + 255) / 256, 256, 0, s>>>(nf, w.twf);
       c3_twiddle_kernel<<<(nb + 255) / 256, 256, 0, s>>>(nb, w.twb);
-      c3_symbol_kernel<<<eb, 256, 0, s>>>(q, four ? 1 : 0, w.sym);
-      if (four) c3_twiddle4_kernel<<<1, 256, 0, s>>>(nf, p4.r1, p4.r2, w.tw4);
+      if (four) {
+        c3_twiddle4_kernel<<<1, 256, 0, s>>>(nf, p4.r1, p4.r2, w.tw4);
+        c3_symbol_factors_kernel<<<1, 256, 0, s>>>(nf, nb, w.ab);
+      } else {
+        c3_symbol_kernel<<<eb, 256, 0, s>>>(q, w.sym);
+      }
     }
     c3_diag_kernel<<<eb, 256, 0, s>>>(N, nf, q.sigma, q.conj_t, static_cast<const float2 *>(op->kc),
                                       static_cast<const float2 *>(op->kw), static_cast<const float2 *>(op->ke),
@@ -1315,7 +1391,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     c3_advance_kernel<<<1, 1, 0, s>>>(w.st, L, backward ? 1 : 0, use_cond, outer, inner);
     c3_center_kernel<<<eb, 256, 0, s>>>(q, w.st, 0, w.cdl);
     if (adj_exact) c3_center_kernel<<<eb, 256, 0, s>>>(q, w.st, 1, w.cdr);
-    c3_init_kernel<<<sgrid, k3Threads, 0, s>>>(q, w.st, adj_exact, w.cdl, w.cdr, w.u,
+    c3_init_kernel<<<sg_init, k3Threads, 0, s>>>(q, w.st, adj_exact, w.cdl, w.cdr, w.u,
                                                 static_cast<const float2 *>(a->src_exit),
                                                 static_cast<const float2 *>(a->src_shared), w.r0, w.K);
     c3_start_kernel<<<pgrid, 128, 0, s>>>(w.K, P);
@@ -1325,17 +1401,17 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     // p = r + beta (p - omega v); y = Prec(p); v = M y
     precondition(s, 0, w.r, learned ? lw.zt : w.y, w.K);
     if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.y, w.K, frb);
-    c3_matvec_kernel<0><<<sgrid, k3Threads, 0, s>>>(q, w.cdl, w.y, w.v, w.r0, w.s, w.K);
+    c3_matvec_kernel<0><<<sg_mv0, k3Threads, 0, s>>>(q, w.cdl, w.y, w.v, w.r0, w.s, w.K);
     // s = r - alpha v; z = Prec(s); t = M z
     precondition(s, 1, w.r, learned ? lw.zt : w.z, w.K);
     if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.z, w.K, frb);
-    c3_matvec_kernel<1><<<sgrid, k3Threads, 0, s>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K);
+    c3_matvec_kernel<1><<<sg_mv1, k3Threads, 0, s>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K);
     c3_update_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.x, w.r, w.r0, w.y, w.z, w.s, w.t, w.K, w.st);
     c3_commit_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, w.st, max_iter, use_cond, inner);
   };
   // step tail: u += x (true residual, store), statistics, gradient
   auto step_tail = [&](cudaStream_t s) {
-    c3_finish_kernel<<<sgrid, k3Threads, 0, s>>>(q, w.st, w.cdl, w.x, w.r0, w.u, w.K, ust, flip ? 1 : 0, exit_out);
+    c3_finish_kernel<<<sg_fin, k3Threads, 0, s>>>(q, w.st, w.cdl, w.x, w.r0, w.u, w.K, ust, flip ? 1 : 0, exit_out);
     c3_stats_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, stats);
     if (a->grad_c)
       c3_grad_kernel<<<eb, 256, 0, s>>>(N, P, nz, w.st, w.u, static_cast<const float2 *>(a->u_fwd),
@@ -1454,7 +1530,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
         if (hs.pending == 0) break;
       }
     }
-    c3_finish_kernel<<<sgrid, k3Threads, 0, st>>>(q, w.st, w.cdl, w.x, w.r0, w.u, w.K, ust, flip ? 1 : 0, exit_out);
+    c3_finish_kernel<<<sg_fin, k3Threads, 0, st>>>(q, w.st, w.cdl, w.x, w.r0, w.u, w.K, ust, flip ? 1 : 0, exit_out);
     if (train && t % a->train_every == 0) {
       // training pair of this step: z0 = M0^{-1} v and x with (I - P_s) x = v,
       // v the step's right-hand side r0 and x its converged update
