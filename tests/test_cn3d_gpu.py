@@ -305,3 +305,100 @@ def test_fft_preconditioner_against_numpy(nf, nb):
                 assert rel(z0[kern][s, p], ref) < 5e-6, (kern, s, p, rel(z0[kern][s, p], ref))
     eng.fft_kernels = 0
     assert rel(z0[0], z0[1]) < 2e-6
+
+
+_TAPS = [(0, 0), (0, -1), (0, 1), (-1, 0), (1, 0), (-1, -1), (-1, 1), (1, -1), (1, 1), (0, -2), (0, 2), (-2, 0), (2, 0)]
+
+
+def _slice_operator(eng, diag):
+    """P_s of one slice (forward orientation) as a sparse matrix: the engine's
+    operator diagonals plus the slice's object diagonal."""
+    import scipy.sparse as sp
+
+    kc, kw, ke, ks, kn = (d.cpu().numpy().astype(np.complex128) for d in eng._diags)
+    nf, N = eng.nx, eng.N
+    f = np.arange(N) % nf
+    w_ = np.where(f[1:] > 0, kw[1:], 0)       # (i, i-1)
+    e_ = np.where(f[:-1] < nf - 1, ke[:-1], 0)  # (i, i+1)
+    return sp.diags([kc + diag, w_, e_, ks[nf:], kn[:-nf]], [0, -1, 1, -nf, nf], format="csr")
+
+
+def _learned_filter_np(z, F, nf, nb):
+    Z = z.reshape(nb, nf)
+    Zp = np.zeros((nb + 4, nf + 4), complex)
+    Zp[2:-2, 2:-2] = Z
+    y = Z.copy()
+    for t, (dy, dx) in enumerate(_TAPS):
+        y = y + F[t].reshape(nb, nf) * Zp[2 + dy:2 + dy + nb, 2 + dx:2 + dx + nf]
+    return y.ravel()
+
+
+@pytest.mark.parametrize("nf,nb,learned,mode", [
+    (64, 64, False, "forward"), (256, 256, False, "forward"), (64, 64, True, "forward"),
+    (256, 256, True, "forward"), (192, 192, True, "adjoint"), (96, 80, True, "forward"), (320, 40, True, "adjoint"),
+])
+def test_one_bicgstab_iteration_against_numpy(nf, nb, learned, mode):
+    """One preconditioned BiCGStab iteration of one step (nz = 2, max_iter = 1)
+    against numpy in complex128: right-hand side 2 P u, y = M p, v = A y,
+    s = r - alpha v, z = M s, t = A z, x = alpha y + omega z, u + x.  M is
+    the FFT preconditioner, and for the learned form M followed by the
+    per-pixel 13-tap filter with random taps written into the learned
+    workspace (the march reuses them: the network is not run).  The cases
+    cover both transform kernels (four-step at 64, 192, 256; Stockham at
+    96 x 80 and 320 x 40), the filter's image edges, several row pairs per CTA
+    (64, 96), two column blocks (320) and the adjoint's conjugated operator,
+    symbol and taps.  The update x is compared at 5e-5 (it is ~5 % of u, held
+    in complex64)."""
+    import ctypes
+
+    from thick_ptycho_b200.cn3d import generate_pairs
+    from thick_ptycho_b200.learned import LearnedPreconditioner
+
+    rng = np.random.default_rng(nf * 7 + nb)
+    nz, k, P = 2, 2 * np.pi / 0.5, 3
+    N = nf * nb
+    field = torch.from_numpy(_field(rng, N, nz, scale=2e-2)).cuda()
+    probes = _gauss(nf, nb, np.column_stack([rng.uniform(8, nf - 8, P), rng.uniform(8, nb - 8, P)]), 6.0)
+    eng = CN3D(nf, nb, nz, k, 1.0, 1.0, 1.0, "impedance")
+    diag = generate_pairs(eng, field, c64(probes), every=1, kind="noise").diag[0].cpu().numpy().astype(np.complex128)
+    Pf = _slice_operator(eng, diag)
+    adj = mode == "adjoint"
+    Pm = Pf.conj().T.tocsr() if adj else Pf
+    fb, ff = np.meshgrid(np.arange(nb), np.arange(nf), indexing="ij")
+    mx, my = complex(eng.co.mu_x), complex(eng.co.mu_y)
+    lam = 1 - (mx * (2 * np.cos(2 * np.pi * ff / nf) - 2) + my * (2 * np.cos(2 * np.pi * fb / nb) - 2))
+    if adj:
+        lam = lam.conj()
+    model = None
+    F = None
+    if learned:
+        model = LearnedPreconditioner(nf, nb, 1.0, seed=0)
+        lws = eng.learned_workspace(P)
+        off = (int(eng.lib.tp_cnn_forward_ws_bytes(nf, nb, 1)) + 255) // 256 * 256
+        F = 0.05 * (rng.standard_normal((13, N)) + 1j * rng.standard_normal((13, N)))
+        lws[off:off + 13 * N * 8].view(torch.complex64).copy_(torch.from_numpy(F.astype(np.complex64)).cuda().ravel())
+        if adj:
+            F = F.conj()
+
+    def M(v):
+        z = np.fft.ifft2(np.fft.fft2(v.reshape(nb, nf)) / lam).ravel()
+        return _learned_filter_np(z, F, nf, nb) if learned else z
+
+    ex = torch.empty((P, N), dtype=torch.complex64, device="cuda")
+    eng.read_stats()
+    eng.march(field, P, mode, probes=c64(probes), exit_out=ex, precond="learned" if learned else True, model=model,
+              reuse_filters=learned, fallback=False, max_iter=1, tol=1e-12)
+    assert eng.read_stats()["iterations"] == P
+    got = ex.cpu().numpy().astype(np.complex128)
+    for p in range(P):
+        u0 = probes[p]
+        r0 = 2 * (Pm @ u0)
+        y = M(r0)
+        v = y - Pm @ y
+        alpha = np.vdot(r0, r0) / np.vdot(r0, v)
+        s = r0 - alpha * v
+        z = M(s)
+        t = z - Pm @ z
+        omega = np.vdot(t, s) / np.vdot(t, t)
+        x = alpha * y + omega * z
+        assert rel(got[p] - u0, x) < 5e-5, (p, rel(got[p] - u0, x))

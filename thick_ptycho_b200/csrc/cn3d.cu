@@ -904,72 +904,132 @@ __global__ void c3_grad_kernel(int N, int P, int nz, const C3State *st, const fl
 // chunks of `chunk` slices: slice s uses image (s-1) % chunk of chunk
 // (s-1) / chunk, tap-major within the chunk (13, chunk * N).
 //
-// A CTA owns `rb` whole rows (rb * nf <= 2 * 256 pixels, two per thread) and
-// kFilterProbes probes.  Each thread keeps its pixels' 13 taps in registers
-// (read once for all the CTA's probes); the rows of all the CTA's pending
-// probes, with a 2-row halo, are copied into shared memory at once (one wave
-// of cp.async copies, so the CTA waits for one load latency, not one per
-// probe), and the 13 neighbour reads of a pixel hit shared memory.
-// Grid (ceil(nb / rb), P / kFilterProbes).
+// A CTA owns a block of cw <= 256 columns and rb = 2 * (256 / cw) rows for
+// kFilterProbes probes; thread (pair, column) filters the two vertically
+// adjacent pixels (b0 + 2 pair, f) and (b0 + 2 pair + 1, f) and keeps their
+// 2 x 13 taps in registers (read once for all the CTA's probes).  The rows of
+// every pending probe, with a 2-pixel border, are copied into shared memory
+// in one wave of cp.async copies, positions outside the image set to zero, so
+// each tap reads a fixed offset and the taps reaching outside the image add
+// zero.  The two pixels' 26 taps read 18 distinct neighbours.
+// Grid (ceil(nf / cw), ceil(nb / rb), ceil(P / kFilterProbes)).
 constexpr int kFilterProbes = 8;
-constexpr int kFilterPx = 2;  // pixels per thread
 
-__global__ void __launch_bounds__(k3Threads) c3_filter_kernel(const C3Params q, const C3State *st, int chunk,
-                                                              const float2 *__restrict__ Fall,
-                                                              const float2 *__restrict__ z, float2 *out,
-                                                              const Krylov *K, int rb) {
-  extern __shared__ __align__(16) float2 ztile[];  // [kFilterProbes][(rb + 4) * nf]
+__host__ __device__ constexpr int filter_cw(int nf) { return nf < 256 ? nf : 256; }
+__host__ __device__ constexpr int filter_rb(int nf) { return 2 * (256 / filter_cw(nf)); }
+
+__global__ void __launch_bounds__(k3Threads, 2) c3_filter_kernel(const C3Params q, const C3State *st, int chunk,
+                                                                 const float2 *__restrict__ Fall,
+                                                                 const float2 *__restrict__ z, float2 *__restrict__ out,
+                                                                 const Krylov *K) {
+  extern __shared__ __align__(16) float2 ztile[];  // [kFilterProbes][rb + 4][cw + 4]
   const int nf = q.nf, nb = q.nb;
-  const int b0 = blockIdx.x * rb;
-  const int lo = b0 - 2 < 0 ? 0 : b0 - 2, hi = b0 + rb + 2 > nb ? nb : b0 + rb + 2;
-  const int tile = (hi - lo) * nf, stride = (rb + 4) * nf;
-  const int npx = ((b0 + rb > nb ? nb : b0 + rb) - b0) * nf;
-  const int p0 = blockIdx.y * kFilterProbes;
+  const int cw = filter_cw(nf), rb = filter_rb(nf), W = cw + 4, H = rb + 4;
+  const int c0 = blockIdx.x * cw, b0 = blockIdx.y * rb, p0 = blockIdx.z * kFilterProbes;
   const int np_cta = q.P - p0 < kFilterProbes ? q.P - p0 : kFilterProbes;
-  // every pending probe's tile, in one wave of asynchronous copies
+  unsigned pend = 0;
+  for (int j = 0; j < np_cta; ++j)
+    if (K == nullptr || !K[p0 + j].done) pend |= 1u << j;
+  // tile row y holds image row b0 - 2 + y, columns c0 - 2 .. c0 + cw + 1 (zero outside the image)
+  const float2 zero = make_float2(0.f, 0.f);
+  const bool pairs16 = ((nf | cw) & 1) == 0;  // 16-byte copies of column pairs
   for (int j = 0; j < np_cta; ++j) {
-    if (K != nullptr && K[p0 + j].done) continue;
-    const float2 *src = z + (size_t)(p0 + j) * q.N + (size_t)lo * nf;
-    float2 *dst = ztile + j * stride;
-    for (int e = threadIdx.x; e < tile; e += blockDim.x) cp_async8(&dst[e], &src[e]);
+    if (!((pend >> j) & 1u)) continue;
+    const float2 *src = z + (size_t)(p0 + j) * q.N;
+    for (int y = 0; y < H; ++y) {
+      const int b = b0 - 2 + y;
+      float2 *dst = ztile + (j * H + y) * W;
+      if (b < 0 || b >= nb) {
+        for (int x = threadIdx.x; x < W; x += blockDim.x) dst[x] = zero;
+        continue;
+      }
+      const float2 *srow = src + (size_t)b * nf;
+      if (pairs16) {
+        for (int m = 2 * threadIdx.x; m < cw; m += 2 * blockDim.x) {
+          if (c0 + m < nf) {
+            cp_async16(&dst[2 + m], &srow[c0 + m]);
+          } else {
+            dst[2 + m] = zero;
+            dst[3 + m] = zero;
+          }
+        }
+      } else {
+        for (int m = threadIdx.x; m < cw; m += blockDim.x) {
+          if (c0 + m < nf) cp_async8(&dst[2 + m], &srow[c0 + m]);
+          else dst[2 + m] = zero;
+        }
+      }
+      if (threadIdx.x < 4) {  // border columns x = 0, 1, cw + 2, cw + 3
+        const int x = threadIdx.x < 2 ? threadIdx.x : cw + threadIdx.x;
+        const int f = c0 - 2 + x;
+        if (f >= 0 && f < nf) cp_async8(&dst[x], &srow[f]);
+        else dst[x] = zero;
+      }
+    }
   }
-  // the taps while the copies are in flight
+  // the taps of the thread's two pixels while the copies are in flight
+  const int pr = threadIdx.x / cw, fx = threadIdx.x - pr * cw;
+  const int f = c0 + fx, ba = b0 + 2 * pr;
+  const bool act = pr < rb / 2 && f < nf;
+  const bool va = act && ba < nb, vb = act && ba + 1 < nb;
   const int sl = st->s - 1;
   const size_t np = (size_t)chunk * q.N;
   const float2 *F = Fall + (size_t)(sl / chunk) * kFilterTaps * np + (size_t)(sl % chunk) * q.N;
-  float2 w[kFilterPx][kFilterTaps];
-  int o[kFilterPx][kFilterTaps], own[kFilterPx];
+  const float cs = q.conj_t ? -1.f : 1.f;
+  float2 wa[kFilterTaps], wb[kFilterTaps];
 #pragma unroll
-  for (int k = 0; k < kFilterPx; ++k) {
-    const int e = threadIdx.x + k * blockDim.x;
-    const int b = b0 + e / nf, f = e % nf;
-    own[k] = (b - lo) * nf + f;
-#pragma unroll
-    for (int t = 0; t < kFilterTaps; ++t) {
-      const int bb = b + filter_tap_dy(t), ff = f + filter_tap_dx(t);
-      const bool in = e < npx && bb >= 0 && bb < nb && ff >= 0 && ff < nf;
-      float2 v = in ? F[(size_t)t * np + (size_t)b * nf + f] : make_float2(0.f, 0.f);
-      if (q.conj_t) v.y = -v.y;
-      w[k][t] = v;
-      o[k][t] = in ? (bb - lo) * nf + ff : own[k];
-    }
+  for (int t = 0; t < kFilterTaps; ++t) {
+    const float2 a = va ? F[(size_t)t * np + (size_t)ba * nf + f] : make_float2(0.f, 0.f);
+    const float2 b = vb ? F[(size_t)t * np + (size_t)(ba + 1) * nf + f] : make_float2(0.f, 0.f);
+    wa[t] = make_float2(a.x, cs * a.y);
+    wb[t] = make_float2(b.x, cs * b.y);
   }
   cp_async_wait_all();
   __syncthreads();
+  if (!va) return;
   for (int j = 0; j < np_cta; ++j) {
-    const int pr = p0 + j;
-    if (K != nullptr && K[pr].done) continue;
-    const float2 *zt = ztile + j * stride;
-    float2 *dst = out + (size_t)pr * q.N + (size_t)b0 * nf;
-#pragma unroll
-    for (int k = 0; k < kFilterPx; ++k) {
-      const int e = threadIdx.x + k * blockDim.x;
-      if (e >= npx) continue;
-      float2 acc = zt[own[k]];
-#pragma unroll
-      for (int t = 0; t < kFilterTaps; ++t) acc = cfma(w[k][t], zt[o[k][t]], acc);
-      dst[e] = acc;
-    }
+    const int pj = p0 + j;
+    if (!((pend >> j) & 1u)) continue;
+    // row k of the window is tile row 2 pr + k, k = 0..5; pixel a sits in row 2, b in row 3
+    const float2 *rw = ztile + j * H * W + 2 * pr * W + fx + 2;
+    const float2 m2 = rw[0];
+    const float2 m1l = rw[W - 1], m1c = rw[W], m1r = rw[W + 1];
+    const float2 a_l2 = rw[2 * W - 2], a_l1 = rw[2 * W - 1], a_c = rw[2 * W], a_r1 = rw[2 * W + 1], a_r2 = rw[2 * W + 2];
+    const float2 b_l2 = rw[3 * W - 2], b_l1 = rw[3 * W - 1], b_c = rw[3 * W], b_r1 = rw[3 * W + 1], b_r2 = rw[3 * W + 2];
+    const float2 p2l = rw[4 * W - 1], p2c = rw[4 * W], p2r = rw[4 * W + 1];
+    const float2 p3 = rw[5 * W];
+    // taps (dy, dx): (0,0) (0,-1) (0,1) (-1,0) (1,0) (-1,-1) (-1,1) (1,-1) (1,1) (0,-2) (0,2) (-2,0) (2,0)
+    float2 A = a_c;
+    A = cfma(wa[0], a_c, A);
+    A = cfma(wa[1], a_l1, A);
+    A = cfma(wa[2], a_r1, A);
+    A = cfma(wa[3], m1c, A);
+    A = cfma(wa[4], b_c, A);
+    A = cfma(wa[5], m1l, A);
+    A = cfma(wa[6], m1r, A);
+    A = cfma(wa[7], b_l1, A);
+    A = cfma(wa[8], b_r1, A);
+    A = cfma(wa[9], a_l2, A);
+    A = cfma(wa[10], a_r2, A);
+    A = cfma(wa[11], m2, A);
+    A = cfma(wa[12], p2c, A);
+    float2 B = b_c;
+    B = cfma(wb[0], b_c, B);
+    B = cfma(wb[1], b_l1, B);
+    B = cfma(wb[2], b_r1, B);
+    B = cfma(wb[3], a_c, B);
+    B = cfma(wb[4], p2c, B);
+    B = cfma(wb[5], a_l1, B);
+    B = cfma(wb[6], a_r1, B);
+    B = cfma(wb[7], p2l, B);
+    B = cfma(wb[8], p2r, B);
+    B = cfma(wb[9], b_l2, B);
+    B = cfma(wb[10], b_r2, B);
+    B = cfma(wb[11], m1c, B);
+    B = cfma(wb[12], p3, B);
+    float2 *dst = out + (size_t)pj * q.N + (size_t)ba * nf + f;
+    dst[0] = A;
+    if (vb) dst[nf] = B;
   }
 }
 
@@ -1281,8 +1341,6 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
       return set_error(TP_ERR_INVALID, "learned preconditioner: NULL model or workspace");
     if (!fft_on) return set_error(TP_ERR_UNSUPPORTED, "learned preconditioner needs FFT-plannable nf, nb (got %d, %d)", nf, nb);
     if (a->mode == TP_MODE_REVERSE) return set_error(TP_ERR_UNSUPPORTED, "learned preconditioner: REVERSE mode is not supported");
-    if (nf > kFilterPx * k3Threads)
-      return set_error(TP_ERR_UNSUPPORTED, "learned preconditioner: nf=%d > %d", nf, kFilterPx * k3Threads);
     if ((reinterpret_cast<uintptr_t>(a->learned_ws) & 255u) != 0)
       return set_error(TP_ERR_INVALID, "learned workspace must be 256-byte aligned");
     lw = c3_learned_layout(static_cast<char *>(a->learned_ws), nf, nb, nz, P);
@@ -1317,10 +1375,10 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   const int adj_exact = a->mode == TP_MODE_ADJOINT_EXACT ? 1 : 0;
   float2 *ust = static_cast<float2 *>(a->u_store);
   float2 *exit_out = static_cast<float2 *>(a->exit_out);
-  // learned filter: whole rows per CTA, at most two pixels per thread
-  const int frb = (kFilterPx * k3Threads) / nf >= 1 ? (kFilterPx * k3Threads) / nf : 1;
-  const dim3 fgrid((nb + frb - 1) / frb, (P + kFilterProbes - 1) / kFilterProbes);
-  const size_t smem_filter = (size_t)kFilterProbes * (frb + 4) * nf * sizeof(float2);
+  // learned filter: column blocks of at most 256, two rows per thread
+  const int fcw = filter_cw(nf), frb = filter_rb(nf);
+  const dim3 fgrid((nf + fcw - 1) / fcw, (nb + frb - 1) / frb, (P + kFilterProbes - 1) / kFilterProbes);
+  const size_t smem_filter = (size_t)kFilterProbes * (frb + 4) * (fcw + 4) * sizeof(float2);
   if (learned)
     TP_CHECK_CUDA(cudaFuncSetAttribute(c3_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_filter));
   const dim3 vgrid((N + 256 * 8 - 1) / (256 * 8), P);
@@ -1400,11 +1458,11 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   auto iteration = [&](cudaStream_t s, int use_cond, cudaGraphConditionalHandle inner) {
     // p = r + beta (p - omega v); y = Prec(p); v = M y
     precondition(s, 0, w.r, learned ? lw.zt : w.y, w.K);
-    if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.y, w.K, frb);
+    if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.y, w.K);
     c3_matvec_kernel<0><<<sg_mv0, k3Threads, 0, s>>>(q, w.cdl, w.y, w.v, w.r0, w.s, w.K);
     // s = r - alpha v; z = Prec(s); t = M z
     precondition(s, 1, w.r, learned ? lw.zt : w.z, w.K);
-    if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.z, w.K, frb);
+    if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.z, w.K);
     c3_matvec_kernel<1><<<sg_mv1, k3Threads, 0, s>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K);
     c3_update_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.x, w.r, w.r0, w.y, w.z, w.s, w.t, w.K, w.st);
     c3_commit_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, w.st, max_iter, use_cond, inner);
