@@ -13,6 +13,13 @@ are skipped; checked on the factor set), and a subset of the 2048 x 1024
 batched workload: its central 1024 columns, 129 nodes and 64 of its probes
 (stride 3).
 
+The same library holds the 3D march in complex128 (BiCGStab with the FFT
+preconditioner, fp64 vectors and dots), run at a Krylov tolerance of 1e-13
+against the oracle's per-slice sparse LU: 64 x 64 (register four-step
+transforms, 8 x 8), 128 x 128 (16 x 8) in the adjoint, 48 x 40 (runtime
+Stockham plan) and 32 x 32 (compile-time Stockham plan) with the exact
+adjoint and its gradient, and the reverse march.
+
 Tolerance: ≤ 1e-12 relative L2 for fields, exit waves and gradients.
 """
 
@@ -30,6 +37,7 @@ if not torch.cuda.is_available():  # pragma: no cover
     pytest.skip("needs a CUDA device", allow_module_level=True)
 
 from thick_ptycho_b200.cn2d import CN2D  # noqa: E402
+from thick_ptycho_b200.cn3d import CN3D  # noqa: E402
 from thick_ptycho_b200.workloads import CONFIG0, CONFIG1, gaussian_probes_2d  # noqa: E402
 
 TOL = 1e-12
@@ -163,3 +171,124 @@ def test_c128_batched_workload_subset():
     inside = centres[(centres >= 512 + 40) & (centres < 1536 - 40)][:64] - 512
     probes = gaussian_probes_2d(1024, inside, w.waist)
     _check_case(1024, 129, geo.k, 1 - dn, probes, "impedance", sums=True, two_slice=False)
+
+
+# ------------------------------------------------------------------ 3D march
+KTOL3 = 1e-13  # BiCGStab stopping residual of the complex128 3D march
+
+
+def _field3(rng, N, nz, scale=5e-3):
+    return 1 + scale * (rng.standard_normal((N, nz)) + 0.2j * rng.standard_normal((N, nz)))
+
+
+def _gauss3(nf, nb, centres, w):
+    f = np.arange(nf)[None, :]
+    b = np.arange(nb)[:, None]
+    return np.array([np.exp(-((f - cf) ** 2 + (b - cb) ** 2) / w**2).ravel() for cf, cb in centres]).astype(complex)
+
+
+def _oracle3(nf, nb, nz, k, dz, bc, n):
+    co = po.bc_coefficients(k, 1.0, dz, dy=1.0, bc_type=bc, dimension=3)
+    A, B = po.step_matrices_2d(nf, nb, co, bc, dz)
+    return A, B, po.object_contribution(n, k, dz)
+
+
+@pytest.mark.parametrize("nf,nb,bc", [(64, 64, "impedance"), (64, 64, "neumann"), (64, 64, "dirichlet"),
+                                      (48, 40, "impedance")])
+def test_c128_3d_forward(nf, nb, bc):
+    """Forward march of 4 probes over 12 nodes in complex128."""
+    rng = np.random.default_rng(nf + nb)
+    nz, k, P = 12, 2 * np.pi / 0.5, 4
+    N = nf * nb
+    n = _field3(rng, N, nz)
+    probes = _gauss3(nf, nb, np.column_stack([rng.uniform(10, nf - 10, P), rng.uniform(10, nb - 10, P)]), 6.0)
+    eng = CN3D(nf, nb, nz, k, 1.0, 1.0, 1.0, bc, check=True)
+    assert eng.cdtype == torch.complex128
+    store = eng.new_store(P)
+    eng.march(torch.from_numpy(n).cuda(), P, "forward", probes=c128(probes), u_store=store, tol=KTOL3, max_iter=60)
+    st = eng.read_stats()
+    assert st["failed"] == 0 and st["solves"] == P * (nz - 1), st
+    u = store.permute(0, 2, 1).cpu().numpy()
+    A, B, C = _oracle3(nf, nb, nz, k, 1.0, bc, n)
+    for p in range(P):
+        ref = po.march(A, B, C, probes[p])
+        assert rel(u[p], ref) < TOL, (p, rel(u[p], ref))
+
+
+def test_c128_3d_adjoint_128():
+    """The reference adjoint with a right-hand-side block at 128 x 128."""
+    rng = np.random.default_rng(5)
+    nf = nb = 128
+    nz, k, P = 8, 2 * np.pi / 0.5, 2
+    N = nf * nb
+    n = _field3(rng, N, nz)
+    rhs = rng.standard_normal((P, N, nz - 1)) + 1j * rng.standard_normal((P, N, nz - 1))
+    eng = CN3D(nf, nb, nz, k, 1.0, 1.0, 1.0, "impedance", check=True)
+    A, B, C = _oracle3(nf, nb, nz, k, 1.0, "impedance", n)
+    field = torch.from_numpy(n).cuda()
+    for p in range(P):
+        store = eng.new_store(1)
+        # the adjoint's source rows by step: step t solves slice L+1-t
+        sh = c128(rhs[p].T[::-1])
+        eng.march(field, 1, "adjoint", src_shared=sh, u_store=store, tol=KTOL3, max_iter=60)
+        assert eng.read_stats()["failed"] == 0
+        ref = po.march(A, B, C, None, "adjoint", rhs_block=rhs[p])
+        got = store[0].T.cpu().numpy()
+        assert rel(got, ref) < TOL, rel(got, ref)
+
+
+@pytest.mark.parametrize("exact", [False, True])
+def test_c128_3d_exact_adjoint_gradient(exact):
+    """Forward + exact adjoint with the fused gradient at 32 x 32 x 10."""
+    rng = np.random.default_rng(21)
+    nf = nb = 32
+    nz, k, P = 10, 4 * np.pi, 3
+    N = nf * nb
+    n = _field3(rng, N, nz)
+    probes = _gauss3(nf, nb, rng.uniform(10, 22, (P, 2)), 5.0)
+    eng = CN3D(nf, nb, nz, k, 1.0, 1.0, 1.0, "impedance", exact_ref_coeff=exact, check=True)
+    field = torch.from_numpy(n).cuda()
+    store = eng.new_store(P)
+    eng.march(field, P, "forward", probes=c128(probes), u_store=store, tol=KTOL3, max_iter=60)
+    srcs = rng.standard_normal((P, N)) + 1j * rng.standard_normal((P, N))
+    gc = torch.zeros((nz - 1, N), dtype=torch.complex128, device="cuda")
+    eng.march(field, P, "adjoint_exact", src_exit=c128(srcs), u_fwd=store, grad_c=gc, tol=KTOL3, max_iter=60)
+    assert eng.read_stats()["failed"] == 0
+    co = po.bc_coefficients(k, 1.0, 1.0, dy=1.0, bc_type="impedance", dimension=3)
+    A, B = po.step_matrices_2d(nf, nb, co, "impedance", 1.0)
+    C = po.object_contribution(n, k, 1.0, exact_ref_coeff=exact)
+    u = np.array([po.march(A, B, C, probes[p]) for p in range(P)])
+    assert rel(store.permute(0, 2, 1).cpu().numpy(), u) < TOL
+    src = np.zeros((P, N, nz - 1), dtype=complex)
+    src[:, :, -1] = srcs
+    lam = po.exact_adjoint_many(A, B, C, src)
+    gcr = sum(po.grad_c_from_adjoint(u[p], lam[p]) for p in range(P))
+    assert rel(gc.cpu().numpy().T, gcr) < TOL, rel(gc.cpu().numpy().T, gcr)
+    gn = eng.grad_to_n(gc, field).cpu().numpy()
+    assert rel(gn, po.chain_grad_to_n(gcr, k, 1.0, n=n, exact_ref_coeff=exact)) < TOL
+
+
+def test_c128_3d_reverse_and_learned_rejected():
+    """Reverse march (sigma = -1, dz = 0.5) in complex128; the check build has
+    no learned correction and says so."""
+    rng = np.random.default_rng(9)
+    nf = nb = 32
+    nz, k, P = 8, 4 * np.pi, 2
+    N = nf * nb
+    n = _field3(rng, N, nz)
+    probes = _gauss3(nf, nb, rng.uniform(10, 22, (P, 2)), 5.0)
+    eng = CN3D(nf, nb, nz, k, 1.0, 1.0, 0.5, "neumann", check=True)
+    store = eng.new_store(P)
+    eng.march(torch.from_numpy(n).cuda(), P, "reverse", probes=c128(probes), u_store=store, tol=KTOL3, max_iter=60)
+    assert eng.read_stats()["failed"] == 0
+    A, B, C = _oracle3(nf, nb, nz, k, 0.5, "neumann", n)
+    u = store.permute(0, 2, 1).cpu().numpy()
+    for p in range(P):
+        ref = po.march(A, B, C, probes[p], "reverse")
+        assert rel(u[p], ref) < TOL, (p, rel(u[p], ref))
+    from thick_ptycho_b200.learned import LearnedPreconditioner
+
+    model = LearnedPreconditioner(nf, nb, 1.0, seed=0)
+    with pytest.raises(Exception, match="check build"):
+        eng.march(torch.from_numpy(n).cuda(), P, "forward", probes=c128(probes), precond="learned", model=model,
+                  fallback=False)

@@ -267,8 +267,9 @@ def load() -> ctypes.CDLL:
 
 
 def load_check() -> ctypes.CDLL:
-    """Load libtpcuda_c128.so, the complex128 check build of the 2D
-    Crank–Nicolson entry points (tp_cn2d_*: every complex buffer complex128)."""
+    """Load libtpcuda_c128.so, the complex128 check build of the 2D and 3D
+    Crank–Nicolson entry points (tp_cn2d_*, tp_cn3d_*: every complex buffer
+    complex128)."""
     global _lib_c128
     if _lib_c128 is not None:
         return _lib_c128

@@ -5,12 +5,14 @@ is written to ``thick_ptycho_b200/_lib/libtpcuda.so``; it links the CUDA
 runtime statically and exports only the ``tp_*`` C symbols declared in
 ``include/tpcuda.h``.
 
-Beside it, ``libtpcuda_c128.so`` is the complex128 check build of the 2D
-Crank–Nicolson path: the same sources compiled with ``-DTP_C128_CHECK``, so
-the factorisation, the warp and team marches (partitioned solve, truncated
-spikes, PCR skip, Cayley step, pair-sum store, fused gradient) run with
-complex128 state, factor sets and fields.  It exports the ``tp_cn2d_*``
-entry points with every complex buffer complex128.
+Beside it, ``libtpcuda_c128.so`` is the complex128 check build of the
+Crank–Nicolson paths: the same sources compiled with ``-DTP_C128_CHECK``, so
+the 2D factorisation and marches (partitioned solve, truncated spikes, PCR
+skip, Cayley step, pair-sum store, fused gradient) and the 3D march
+(BiCGStab with the four-step or Stockham FFT preconditioner, exact adjoint
+and gradient; no learned correction) run with complex128 state, operators
+and fields.  It exports the ``tp_cn2d_*`` and ``tp_cn3d_*`` entry points
+with every complex buffer complex128.
 """
 
 from __future__ import annotations
@@ -41,7 +43,7 @@ def nvcc() -> str:
 
 LIB_C128 = os.path.join(LIBDIR, "libtpcuda_c128.so")
 # sources of the complex128 check build (the 2D factorisation and marches)
-C128_SOURCES = ("tp_capi.cu", "cn2d.cu", "cn2d_team.cu")
+C128_SOURCES = ("tp_capi.cu", "cn2d.cu", "cn2d_team.cu", "cn3d.cu")
 
 
 def sources():

@@ -30,10 +30,16 @@ def _c2(z: complex):
 class CN3D:
     """One 3D geometry: nx × ny transverse (N = nx·ny), nz nodes."""
 
-    def __init__(self, nx, ny, nz, k, dx, dy, dz, bc_type="impedance", exact_ref_coeff=False, device=None):
+    def __init__(self, nx, ny, nz, k, dx, dy, dz, bc_type="impedance", exact_ref_coeff=False, device=None,
+                 check=False):
+        """``check=True`` runs the geometry on the complex128 check build
+        (``libtpcuda_c128.so``): operator, vectors, stores and sources
+        complex128, the FFT-preconditioned (not the learned) march only."""
         if not torch.cuda.is_available():
             raise _native.NativeLibraryError("CN3D needs a CUDA device (there is no CPU fallback)")
-        self.lib = _native.load()
+        self.check = bool(check)
+        self.lib = _native.load_check() if self.check else _native.load()
+        self.cdtype = torch.complex128 if self.check else torch.complex64
         self.device = torch.device(device if device is not None else "cuda")
         self.nx, self.ny, self.nz, self.L = int(nx), int(ny), int(nz), int(nz) - 1
         self.N = self.nx * self.ny
@@ -42,7 +48,8 @@ class CN3D:
         self.exact_ref_coeff = bool(exact_ref_coeff)
         co = BCCoefficients.make(self.k, dx, dz, self.bc_type, dy=dy, dimension=3)
         diags = operator_2d_diagonals(self.nx, self.ny, co, self.bc_type)
-        self._diags = [torch.from_numpy(d.astype(np.complex64)).to(self.device) for d in diags]
+        npc = np.complex128 if self.check else np.complex64
+        self._diags = [torch.from_numpy(d.astype(npc)).to(self.device) for d in diags]
         self.co = co
         self._ws = None
         self._ws_P = None
@@ -82,13 +89,14 @@ class CN3D:
         return self._lws
 
     def new_store(self, P):
-        return torch.empty((P, self.nz, self.N), dtype=torch.complex64, device=self.device)
+        return torch.empty((P, self.nz, self.N), dtype=self.cdtype, device=self.device)
 
     def march(self, field: torch.Tensor, num_probes: int, mode="forward", probes=None, src_shared=None, src_exit=None,
               u_store=None, exit_out=None, u_fwd=None, grad_c=None, tol=1e-6, max_iter=20, precond=True,
               host_check=True, is_delta=False, model=None, train=None, train_every=0, fallback=True,
               reuse_filters=False):
-        """One batched march; tensors complex64 (field complex128/complex64 (N, nz)).
+        """One batched march; tensors complex64 (complex128 in the check build;
+        field complex128/complex64 (N, nz)).
 
         ``precond``: True/"fft" (periodic FFT preconditioner), False/"none", or
         "learned" (FFT preconditioner with the per-pixel correction of
@@ -131,8 +139,8 @@ class CN3D:
         for name, t, shp in (("probes", probes, (P, self.N)), ("src_shared", src_shared, (self.L, self.N)),
                              ("src_exit", src_exit, (P, self.N)), ("u_store", u_store, (P, self.nz, self.N)),
                              ("exit_out", exit_out, (P, self.N)), ("grad_c", grad_c, (self.L, self.N))):
-            if t is not None and (t.dtype != torch.complex64 or not t.is_contiguous() or tuple(t.shape) != shp):
-                raise ValueError(f"{name} must be a contiguous complex64 tensor of shape {shp}")
+            if t is not None and (t.dtype != self.cdtype or not t.is_contiguous() or tuple(t.shape) != shp):
+                raise ValueError(f"{name} must be a contiguous {self.cdtype} tensor of shape {shp}")
         a = _native.TpCn3dMarchArgs()
         a.num_probes, a.mode, a.max_iter, a.precond, a.host_check = P, mode_i, int(max_iter), int(precond), int(host_check)
         a.tol = float(tol)
@@ -161,7 +169,7 @@ class CN3D:
         o = self.op(is_delta)
         rc = self.lib.tp_cn3d_march(ctypes.byref(o), _ptr(field), dt, ctypes.byref(a), _ptr(ws), ws.numel(),
                                     ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
-        _native.check(rc, "tp_cn3d_march")
+        _native.check(rc, "tp_cn3d_march", self.lib)
 
     def read_stats(self, reset=True):
         """(total iterations, solves, failed solves, max iterations per solve,
@@ -181,8 +189,8 @@ class CN3D:
         if self.exact_ref_coeff:
             f = field.reshape(self.N, self.nz).to(torch.complex128)
             nn = f + 1 if is_delta else f
-            return (np.conj(d) * torch.conj(nn) * acc).to(torch.complex64)
-        return (np.conj(d) * acc).to(torch.complex64)
+            return (np.conj(d) * torch.conj(nn) * acc).to(self.cdtype)
+        return (np.conj(d) * acc).to(self.cdtype)
 
 
 class PWEGradient3D:

@@ -36,7 +36,7 @@ struct C3Params {
   double sigma, k, dz;
   double2 mu_x, mu_y;  // preconditioner symbol coefficients (sigma and T applied)
   const void *field;
-  const float2 *kc, *kw, *ke, *ks, *kn;  // diagonals of sigma*T(K)
+  const cx *kc, *kw, *ke, *ks, *kn;  // diagonals of sigma*T(K)
 };
 
 // Per-probe BiCGStab scalars (fp64).
@@ -77,7 +77,7 @@ __global__ void c3_advance_kernel(C3State *st, int L, int backward, int use_cond
 
 __device__ __forceinline__ double2 load_field(const C3Params &q, size_t idx) {
   if (q.dtype == TP_C128) return static_cast<const double2 *>(q.field)[idx];
-  const float2 v = static_cast<const float2 *>(q.field)[idx];
+  const cx v = static_cast<const cx *>(q.field)[idx];
   return z2(v.x, v.y);
 }
 
@@ -90,13 +90,13 @@ __device__ __forceinline__ double2 coef3(const C3Params &q, double2 v) {
 }
 
 // sigma*T(K) diagonals from K's (T = conjugate transpose for the adjoints).
-__global__ void c3_diag_kernel(int N, int nf, double sigma, int conj_t, const float2 *kc, const float2 *kw,
-                               const float2 *ke, const float2 *ks, const float2 *kn, float2 *oc, float2 *ow,
-                               float2 *oe, float2 *os, float2 *on) {
-  const float sg = (float)sigma;
-  auto tf = [&](float2 v) { return make_float2(sg * v.x, sg * (conj_t ? -v.y : v.y)); };
+__global__ void c3_diag_kernel(int N, int nf, double sigma, int conj_t, const cx *kc, const cx *kw,
+                               const cx *ke, const cx *ks, const cx *kn, cx *oc, cx *ow,
+                               cx *oe, cx *os, cx *on) {
+  const rx sg = (rx)sigma;
+  auto tf = [&](cx v) { return mkcx(sg * v.x, sg * (conj_t ? -v.y : v.y)); };
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-    const float2 z = make_float2(0.f, 0.f);
+    const cx z = mkcx(TP_R(0.0), TP_R(0.0));
     oc[i] = tf(kc[i]);
     if (!conj_t) {
       ow[i] = tf(kw[i]);
@@ -115,15 +115,15 @@ __global__ void c3_diag_kernel(int N, int nf, double sigma, int conj_t, const fl
 // cd[i] = sigma*T(K)_c[i] + sigma*T(c_s(i)) for slice s (1-based), fp64 -> fp32,
 // s = the current step's slice + next (next = 1: the slice after it, used by
 // the exact adjoint from its second step on).
-__global__ void c3_center_kernel(const C3Params q, const C3State *st, int next, float2 *__restrict__ cd) {
+__global__ void c3_center_kernel(const C3Params q, const C3State *st, int next, cx *__restrict__ cd) {
   if (next && st->t == 1) return;
   const int s = st->s + next;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
     const size_t base = (size_t)i * q.nz;
     const double2 c = zscale(zadd(coef3(q, load_field(q, base + s - 1)), coef3(q, load_field(q, base + s))), 0.25 * q.dz);
     const double2 v = zscale(q.conj_t ? zconj(c) : c, q.sigma);
-    const float2 k = q.kc[i];
-    cd[i] = make_float2((float)(k.x + v.x), (float)(k.y + v.y));
+    const cx k = q.kc[i];
+    cd[i] = mkcx((rx)(k.x + v.x), (rx)(k.y + v.y));
   }
 }
 
@@ -132,19 +132,19 @@ __global__ void c3_center_kernel(const C3Params q, const C3State *st, int next, 
 // filters' inputs.  The adjoint modes apply the conjugate of the forward
 // slice's filter (the transposed operator of a complex-symmetric K is its
 // elementwise conjugate, so its corrected inverse is the conjugate one).
-__global__ void c3_obj_diag_kernel(const C3Params q, int s0, int count, float2 *__restrict__ out) {
+__global__ void c3_obj_diag_kernel(const C3Params q, int s0, int count, cx *__restrict__ out) {
   const size_t total = (size_t)count * q.N;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
     const int s = s0 + 1 + (int)(e / q.N), i = (int)(e % q.N);
     const size_t base = (size_t)i * q.nz;
     const double2 c = zscale(zadd(coef3(q, load_field(q, base + s - 1)), coef3(q, load_field(q, base + s))), 0.25 * q.dz);
-    out[e] = to_f2(c);
+    out[e] = to_cx(c);
   }
 }
 
-__device__ __forceinline__ float2 apply_P(const C3Params &q, const float2 *__restrict__ cd, const float2 *__restrict__ x,
+__device__ __forceinline__ cx apply_P(const C3Params &q, const cx *__restrict__ cd, const cx *__restrict__ x,
                                           int i) {
-  float2 r = cmul(cd[i], x[i]);
+  cx r = cmul(cd[i], x[i]);
   const int f = i % q.nf;
   if (f > 0) r = cfma(q.kw[i], x[i - 1], r);
   if (f < q.nf - 1) r = cfma(q.ke[i], x[i + 1], r);
@@ -195,11 +195,11 @@ constexpr int kStencilProbes = 4;
 
 // The off-diagonal couplings of element i (zero across an edge).
 struct Stencil {
-  float2 w, e, s, n;
+  cx w, e, s, n;
   int f;
 };
 __device__ __forceinline__ Stencil stencil_at(const C3Params &q, int i) {
-  const float2 z = make_float2(0.f, 0.f);
+  const cx z = mkcx(TP_R(0.0), TP_R(0.0));
   Stencil k;
   k.f = i % q.nf;
   k.w = k.f > 0 ? q.kw[i] : z;
@@ -209,8 +209,8 @@ __device__ __forceinline__ Stencil stencil_at(const C3Params &q, int i) {
   return k;
 }
 // K_off x at element i (same operation order as apply_P).
-__device__ __forceinline__ float2 stencil_off(const C3Params &q, const Stencil &k, const float2 *__restrict__ x, int i,
-                                              float2 acc) {
+__device__ __forceinline__ cx stencil_off(const C3Params &q, const Stencil &k, const cx *__restrict__ x, int i,
+                                              cx acc) {
   if (k.f > 0) acc = cfma(k.w, x[i - 1], acc);
   if (k.f < q.nf - 1) acc = cfma(k.e, x[i + 1], acc);
   if (i >= q.nf) acc = cfma(k.s, x[i - q.nf], acc);
@@ -233,37 +233,37 @@ __device__ __forceinline__ unsigned pending_mask(const Krylov *K, int p0, int P)
 // (cdr) and has no u term at t = 1 (lambda_{L+1} = 0); the per-probe source
 // enters at t = 1; src_shared is (L, N) by step.
 __global__ void __launch_bounds__(k3Threads) c3_init_kernel(const C3Params q, const C3State *st, int adj_exact,
-                                                            const float2 *__restrict__ cdl, const float2 *__restrict__ cdn,
-                                                            const float2 *__restrict__ u, const float2 *__restrict__ src_exit,
-                                                            const float2 *__restrict__ src_shared, float2 *r0,
+                                                            const cx *__restrict__ cdl, const cx *__restrict__ cdn,
+                                                            const cx *__restrict__ u, const cx *__restrict__ src_exit,
+                                                            const cx *__restrict__ src_shared, cx *r0,
                                                             Krylov *K) {
   __shared__ double red[kStencilProbes * (k3Threads / 32)];
   const int p0 = blockIdx.y * kStencilProbes;
   const int np = q.P - p0 < kStencilProbes ? q.P - p0 : kStencilProbes;
   const int t = st->t;
   const int use_u = !(adj_exact && t == 1);
-  const float2 *cdr = (adj_exact && t > 1) ? cdn : cdl;
-  const float2 *src = (t == 1) ? src_exit : nullptr;
-  const float2 *shared = src_shared ? src_shared + (size_t)(t - 1) * q.N : nullptr;
+  const cx *cdr = (adj_exact && t > 1) ? cdn : cdl;
+  const cx *src = (t == 1) ? src_exit : nullptr;
+  const cx *shared = src_shared ? src_shared + (size_t)(t - 1) * q.N : nullptr;
   double acc[kStencilProbes] = {};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
     // (P_l + P_r) u = (cd_l + cd_r) u + 2 K_off u: the two operators differ only on the diagonal
     Stencil k{};
-    float2 dsum = make_float2(0.f, 0.f);
+    cx dsum = mkcx(TP_R(0.0), TP_R(0.0));
     if (use_u) {
       k = stencil_at(q, i);
       dsum = cadd(cdl[i], cdr[i]);
     }
-    const float2 sh = shared != nullptr ? shared[i] : make_float2(0.f, 0.f);
-    float2 bv[kStencilProbes];
+    const cx sh = shared != nullptr ? shared[i] : mkcx(TP_R(0.0), TP_R(0.0));
+    cx bv[kStencilProbes];
 #pragma unroll
     for (int j = 0; j < kStencilProbes; ++j) {
       if (j >= np) break;
       const size_t off = (size_t)(p0 + j) * q.N;
-      float2 b = make_float2(0.f, 0.f);
+      cx b = mkcx(TP_R(0.0), TP_R(0.0));
       if (use_u) {
-        const float2 *uu = u + off;
-        const float2 o = stencil_off(q, k, uu, i, make_float2(0.f, 0.f));
+        const cx *uu = u + off;
+        const cx o = stencil_off(q, k, uu, i, mkcx(TP_R(0.0), TP_R(0.0)));
         b = cfma(dsum, uu[i], cadd(o, o));
       }
       if (src != nullptr) b = cadd(b, src[off + i]);
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(k3Threads) c3_init_kernel(const C3Params q, co
 #pragma unroll
     for (int j = 0; j < kStencilProbes; ++j) {
       if (j >= np) break;
-      const float2 b = bv[j];
+      const cx b = bv[j];
       r0[(size_t)(p0 + j) * q.N + i] = b;
       acc[j] += (double)b.x * b.x + (double)b.y * b.y;
     }
@@ -334,18 +334,18 @@ __global__ void c3_commit_kernel(Krylov *K, int P, double tol2, C3State *st, int
 }
 
 // Twiddle table W_n^t = exp(-2 pi i t / n) (fp64 sincospi, rounded once).
-__global__ void c3_twiddle_kernel(int n, float2 *tw) {
+__global__ void c3_twiddle_kernel(int n, cx *tw) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     double sv, cv;
     sincospi(-2.0 * (double)t / (double)n, &sv, &cv);
-    tw[t] = make_float2((float)cv, (float)sv);
+    tw[t] = mkcx((rx)cv, (rx)sv);
   }
 }
 
 // Inverse of the periodic symbol, scaled by 1/(nf nb) (the normalisation of
 // the inverse 2D transform), transposed: sym[f * nb + b] =
 // 1 / ((1 - mu_x (2 cos(2 pi f/nf) - 2) - mu_y (2 cos(2 pi b/nb) - 2)) nf nb).
-__global__ void c3_symbol_kernel(const C3Params q, float2 *sym) {
+__global__ void c3_symbol_kernel(const C3Params q, cx *sym) {
   const double sc = 1.0 / ((double)q.nf * (double)q.nb);
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < q.N; e += gridDim.x * blockDim.x) {
     const int f = e / q.nb, bb = e - f * q.nb;
@@ -354,7 +354,7 @@ __global__ void c3_symbol_kernel(const C3Params q, float2 *sym) {
     sincospi(2.0 * (double)bb / (double)q.nb, &sb, &cbv);
     const double ax = 2.0 * cf - 2.0, ay = 2.0 * cbv - 2.0;
     const double2 lam = z2(1.0 - (q.mu_x.x * ax + q.mu_y.x * ay), -(q.mu_x.y * ax + q.mu_y.y * ay));
-    sym[e] = to_f2(zscale(zdiv(z2(1, 0), lam), sc));
+    sym[e] = to_cx(zscale(zdiv(z2(1, 0), lam), sc));
   }
 }
 
@@ -368,14 +368,14 @@ __global__ void c3_symbol_kernel(const C3Params q, float2 *sym) {
 // Grid (nb / rpc, P).
 template <int NF>
 __global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan pl, const C3Params q, int mode,
-                                                                 const float2 *r, float2 *p, const float2 *v, float2 *s,
-                                                                 float2 *hat, const Krylov *K, int rpc, int fft_on,
-                                                                 const float2 *twg, const float2 *r0,
+                                                                 const cx *r, cx *p, const cx *v, cx *s,
+                                                                 cx *hat, const Krylov *K, int rpc, int fft_on,
+                                                                 const cx *twg, const cx *r0,
                                                                  const C3State *st) {
-  extern __shared__ __align__(16) float2 fsm[];
+  extern __shared__ __align__(16) cx fsm[];
   const int n = NF > 0 ? NF : q.nf, pr = blockIdx.y;
   if (K != nullptr && K[pr].done) return;
-  float2 *tw = fsm, *a = tw + n, *b = a + rpc * fstride<NF>(n);
+  cx *tw = fsm, *a = tw + n, *b = a + rpc * fstride<NF>(n);
   const size_t off = (size_t)pr * q.N + (size_t)blockIdx.x * rpc * n;
   const int tot = rpc * n;
   auto slot = [&](int e) { return fslot<NF>(e / n, e % n, n); };
@@ -389,7 +389,7 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan p
     const int it = st->it;
     if (it == 0) {
       for (int e = threadIdx.x; e < tot; e += blockDim.x) {
-        const float2 pv = r0[off + e];
+        const cx pv = r0[off + e];
         if (fft_on) a[slot(e)] = pv;
         else hat[off + e] = pv;
       }
@@ -397,10 +397,10 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan p
       const Krylov &k = K[pr];
       const double den = k.rho_prev.x * k.rho_prev.x + k.rho_prev.y * k.rho_prev.y;
       const double2 beta = den > 0.0 ? zmul(zdiv(k.rho_cur, k.rho_prev), zdiv(k.alpha, k.omega)) : z2(0, 0);
-      const float2 bt = to_f2(beta), om = to_f2(k.omega);
-      const float2 *pin = (it == 1) ? r0 : p;
+      const cx bt = to_cx(beta), om = to_cx(k.omega);
+      const cx *pin = (it == 1) ? r0 : p;
       for (int e = threadIdx.x; e < tot; e += blockDim.x) {
-        const float2 pv = cfma(bt, cfnma(om, v[off + e], pin[off + e]), r[off + e]);
+        const cx pv = cfma(bt, cfnma(om, v[off + e], pin[off + e]), r[off + e]);
         p[off + e] = pv;
         if (fft_on) a[slot(e)] = pv;
         else hat[off + e] = pv;
@@ -410,10 +410,10 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan p
     const Krylov &k = K[pr];
     const double den = k.acc_r0v.x * k.acc_r0v.x + k.acc_r0v.y * k.acc_r0v.y;
     const double2 alpha = den > 0.0 ? zdiv(k.rho_cur, k.acc_r0v) : z2(0, 0);
-    const float2 al = to_f2(alpha);
-    const float2 *rin = (st->it == 0) ? r0 : r;
+    const cx al = to_cx(alpha);
+    const cx *rin = (st->it == 0) ? r0 : r;
     for (int e = threadIdx.x; e < tot; e += blockDim.x) {
-      const float2 sv = cfnma(al, v[off + e], rin[off + e]);
+      const cx sv = cfnma(al, v[off + e], rin[off + e]);
       s[off + e] = sv;
       if (fft_on) a[slot(e)] = sv;
       else hat[off + e] = sv;
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan p
   }
   if (!fft_on) return;
   __syncthreads();
-  const float2 *res = fft_rows<NF>(a, b, pl, tw, false, rpc);
+  const cx *res = fft_rows<NF>(a, b, pl, tw, false, rpc);
   for (int e = threadIdx.x; e < tot; e += blockDim.x) hat[off + e] = res[slot(e)];
 }
 
@@ -429,32 +429,32 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_kernel(const FftPlan p
 // FFTs (in place on hat).  Grid (nf / cpc, P): a CTA transposes cpc columns of
 // length nb into smem.
 template <int NB>
-__global__ void __launch_bounds__(k3Threads) c3_prec_cols_kernel(const FftPlan pl, const C3Params q, float2 *hat,
-                                                                 const Krylov *K, int cpc, const float2 *twg,
-                                                                 const float2 *__restrict__ sym) {
-  extern __shared__ __align__(16) float2 fsm[];
+__global__ void __launch_bounds__(k3Threads) c3_prec_cols_kernel(const FftPlan pl, const C3Params q, cx *hat,
+                                                                 const Krylov *K, int cpc, const cx *twg,
+                                                                 const cx *__restrict__ sym) {
+  extern __shared__ __align__(16) cx fsm[];
   const int nb = NB > 0 ? NB : q.nb, nf = q.nf, pr = blockIdx.y;
   if (K != nullptr && K[pr].done) return;
-  float2 *tw = fsm, *a = tw + nb, *b = a + cpc * fstride<NB>(nb);
+  cx *tw = fsm, *a = tw + nb, *b = a + cpc * fstride<NB>(nb);
   const int f0 = blockIdx.x * cpc;
-  float2 *base = hat + (size_t)pr * q.N;
+  cx *base = hat + (size_t)pr * q.N;
   load_twiddles(tw, twg, nb);
   for (int e = threadIdx.x; e < cpc * nb; e += blockDim.x) {
     const int c = e % cpc, bb = e / cpc;  // coalesced over c; asynchronous copies
-    cp_async8(&a[fslot<NB>(c, bb, nb)], &base[(size_t)bb * nf + f0 + c]);
+    cp_async_cx(&a[fslot<NB>(c, bb, nb)], &base[(size_t)bb * nf + f0 + c]);
   }
   cp_async_wait_all();
   __syncthreads();
-  float2 *F = fft_rows<NB>(a, b, pl, tw, false, cpc);
-  float2 *o = (F == a) ? b : a;
-  const float2 *sy = sym + (size_t)f0 * nb;
+  cx *F = fft_rows<NB>(a, b, pl, tw, false, cpc);
+  cx *o = (F == a) ? b : a;
+  const cx *sy = sym + (size_t)f0 * nb;
   for (int e = threadIdx.x; e < cpc * nb; e += blockDim.x) {
     const int c = e / nb, bb = e - c * nb;
     const int sl = fslot<NB>(c, bb, nb);
     F[sl] = cmul(F[sl], sy[e]);
   }
   __syncthreads();
-  float2 *R = fft_rows<NB>(F, o, pl, tw, true, cpc);
+  cx *R = fft_rows<NB>(F, o, pl, tw, true, cpc);
   for (int e = threadIdx.x; e < cpc * nb; e += blockDim.x) {
     const int c = e % cpc, bb = e / cpc;
     base[(size_t)bb * nf + f0 + c] = R[fslot<NB>(c, bb, nb)];
@@ -464,40 +464,40 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_cols_kernel(const FftPlan p
 // Inverse row FFTs of hat into out (the 1/(nf nb) scale is in the symbol).
 template <int NF>
 __global__ void __launch_bounds__(k3Threads) c3_prec_rows_inv_kernel(const FftPlan pl, const C3Params q,
-                                                                     const float2 *hat, float2 *out, const Krylov *K,
-                                                                     int rpc, const float2 *twg) {
-  extern __shared__ __align__(16) float2 fsm[];
+                                                                     const cx *hat, cx *out, const Krylov *K,
+                                                                     int rpc, const cx *twg) {
+  extern __shared__ __align__(16) cx fsm[];
   const int n = NF > 0 ? NF : q.nf, pr = blockIdx.y;
   if (K != nullptr && K[pr].done) return;
-  float2 *tw = fsm, *a = tw + n, *b = a + rpc * fstride<NF>(n);
+  cx *tw = fsm, *a = tw + n, *b = a + rpc * fstride<NF>(n);
   const size_t off = (size_t)pr * q.N + (size_t)blockIdx.x * rpc * n;
   const int tot = rpc * n;
   auto slot = [&](int e) { return fslot<NF>(e / n, e % n, n); };
   load_twiddles(tw, twg, n);
-  for (int e = threadIdx.x; e < tot; e += blockDim.x) cp_async8(&a[slot(e)], &hat[off + e]);
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) cp_async_cx(&a[slot(e)], &hat[off + e]);
   cp_async_wait_all();
   __syncthreads();
-  const float2 *res = fft_rows<NF>(a, b, pl, tw, true, rpc);
+  const cx *res = fft_rows<NF>(a, b, pl, tw, true, rpc);
   for (int e = threadIdx.x; e < tot; e += blockDim.x) out[off + e] = res[slot(e)];
 }
 
 // ab[f] = 2 cos(2 pi f / nf) - 2 (f < nf), ab[nf + b] = 2 cos(2 pi b / nb) - 2
 // (fp64, rounded once): the factors of the periodic symbol.
-__global__ void c3_symbol_factors_kernel(int nf, int nb, float *ab) {
+__global__ void c3_symbol_factors_kernel(int nf, int nb, rx *ab) {
   for (int e = threadIdx.x; e < nf + nb; e += blockDim.x) {
     const int j = e < nf ? e : e - nf, n = e < nf ? nf : nb;
-    ab[e] = (float)(2.0 * cospi(2.0 * (double)j / (double)n) - 2.0);
+    ab[e] = (rx)(2.0 * cospi(2.0 * (double)j / (double)n) - 2.0);
   }
 }
 
 // Padded twiddle table of the four-step transforms of length n = R1 R2:
 // tw[k1 * (R2 + 1) + n2] = W_n^{n2 k1} (fp64 sincospi, rounded once).
-__global__ void c3_twiddle4_kernel(int n, int r1, int r2, float2 *tw) {
+__global__ void c3_twiddle4_kernel(int n, int r1, int r2, cx *tw) {
   for (int e = threadIdx.x; e < r1 * (r2 + 1); e += blockDim.x) {
     const int k1 = e / (r2 + 1), n2 = e % (r2 + 1);
     double sv, cv;
     sincospi(-2.0 * (double)((n2 * k1) % n) / (double)n, &sv, &cv);
-    tw[e] = n2 < r2 ? make_float2((float)cv, (float)sv) : make_float2(0.f, 0.f);
+    tw[e] = n2 < r2 ? mkcx((rx)cv, (rx)sv) : mkcx(TP_R(0.0), TP_R(0.0));
   }
 }
 
@@ -507,10 +507,10 @@ __global__ void c3_twiddle4_kernel(int n, int r1, int r2, float2 *tw) {
 // issued together rather than one memory latency per element.
 struct PrecInput {
   int mode, first;
-  float2 bt, om, al;
-  const float2 *r, *pin, *v, *r0;
-  float2 *p, *s;
-  __device__ __forceinline__ float2 operator()(size_t e) const {
+  cx bt, om, al;
+  const cx *r, *pin, *v, *r0;
+  cx *p, *s;
+  __device__ __forceinline__ cx operator()(size_t e) const {
     if (mode == 2) return r[e];
     if (mode == 0) {
       if (first) return r0[e];
@@ -519,15 +519,15 @@ struct PrecInput {
     return cfnma(al, v[e], first ? r0[e] : r[e]);
   }
   // where the formed input is stored (nullptr: not stored)
-  __device__ __forceinline__ float2 *dest() const {
+  __device__ __forceinline__ cx *dest() const {
     if (mode == 0 && !first) return p;
     if (mode == 1) return s;
     return nullptr;
   }
 };
 
-__device__ __forceinline__ PrecInput prec_input(int mode, const float2 *r, float2 *p, const float2 *v, float2 *s,
-                                                const float2 *r0, const Krylov *K, int pr, const C3State *st) {
+__device__ __forceinline__ PrecInput prec_input(int mode, const cx *r, cx *p, const cx *v, cx *s,
+                                                const cx *r0, const Krylov *K, int pr, const C3State *st) {
   PrecInput in{};
   in.mode = mode;
   in.r = r;
@@ -543,13 +543,13 @@ __device__ __forceinline__ PrecInput prec_input(int mode, const float2 *r, float
     if (it > 0) {
       const double den = k.rho_prev.x * k.rho_prev.x + k.rho_prev.y * k.rho_prev.y;
       const double2 beta = den > 0.0 ? zmul(zdiv(k.rho_cur, k.rho_prev), zdiv(k.alpha, k.omega)) : z2(0, 0);
-      in.bt = to_f2(beta);
-      in.om = to_f2(k.omega);
+      in.bt = to_cx(beta);
+      in.om = to_cx(k.omega);
       in.pin = (it == 1) ? r0 : p;
     }
   } else {
     const double den = k.acc_r0v.x * k.acc_r0v.x + k.acc_r0v.y * k.acc_r0v.y;
-    in.al = to_f2(den > 0.0 ? zdiv(k.rho_cur, k.acc_r0v) : z2(0, 0));
+    in.al = to_cx(den > 0.0 ? zdiv(k.rho_cur, k.acc_r0v) : z2(0, 0));
   }
   return in;
 }
@@ -561,13 +561,13 @@ __device__ __forceinline__ PrecInput prec_input(int mode, const float2 *r, float
 // Forward row transforms of the preconditioner input (formed as in
 // c3_prec_rows_kernel) into hat, natural frequency order.  Grid (nb / RPC, P).
 template <int R1, int R2>
-__global__ void __launch_bounds__(256) c3_rows4_kernel(const C3Params q, int mode, const float2 *r, float2 *p,
-                                                       const float2 *v, float2 *s, float2 *hat, const Krylov *K,
-                                                       const float2 *__restrict__ twg, const float2 *r0,
+__global__ void __launch_bounds__(256) c3_rows4_kernel(const C3Params q, int mode, const cx *r, cx *p,
+                                                       const cx *v, cx *s, cx *hat, const Krylov *K,
+                                                       const cx *__restrict__ twg, const cx *r0,
                                                        const C3State *st) {
   constexpr int N = R1 * R2, RPC = 256 / R1, S = R1 * (R2 + 1);
-  __shared__ float2 buf[RPC * S];
-  __shared__ float2 tw[R1 * (R2 + 1)];
+  __shared__ cx buf[RPC * S];
+  __shared__ cx tw[R1 * (R2 + 1)];
   const int pr = blockIdx.y;
   if (K != nullptr && K[pr].done) return;
   for (int e = threadIdx.x; e < R1 * (R2 + 1); e += 256) tw[e] = twg[e];
@@ -576,15 +576,15 @@ __global__ void __launch_bounds__(256) c3_rows4_kernel(const C3Params q, int mod
   __syncthreads();
   if (threadIdx.x < RPC * R2) {  // stage A: (row, n2)
     const int row = threadIdx.x / R2, n2 = threadIdx.x % R2;
-    float2 x[16];
+    cx x[16];
     const size_t e0 = off + (size_t)row * N + n2;
 #pragma unroll
     for (int n1 = 0; n1 < R1; ++n1) x[n1] = in(e0 + R2 * n1);
-    if (float2 *dst = in.dest()) {
+    if (cx *dst = in.dest()) {
 #pragma unroll
       for (int n1 = 0; n1 < R1; ++n1) dst[e0 + R2 * n1] = x[n1];
     }
-    dft_reg<R1>(x, -1.f);
+    dft_reg<R1>(x, -TP_R(1.0));
 #pragma unroll
     for (int k1 = 0; k1 < R1; ++k1)
       buf[row * S + k1 * (R2 + 1) + n2] = k1 ? cmul(x[k1], tw[k1 * (R2 + 1) + n2]) : x[0];
@@ -592,10 +592,10 @@ __global__ void __launch_bounds__(256) c3_rows4_kernel(const C3Params q, int mod
   __syncthreads();
   {  // stage C: (row, k1)
     const int row = threadIdx.x / R1, k1 = threadIdx.x % R1;
-    float2 x[16];
+    cx x[16];
 #pragma unroll
     for (int n2 = 0; n2 < R2; ++n2) x[n2] = buf[row * S + k1 * (R2 + 1) + n2];
-    dft_reg<R2>(x, -1.f);
+    dft_reg<R2>(x, -TP_R(1.0));
 #pragma unroll
     for (int k2 = 0; k2 < R2; ++k2) hat[off + row * N + k1 + R1 * k2] = x[k2];
   }
@@ -607,26 +607,26 @@ __global__ void __launch_bounds__(256) c3_rows4_kernel(const C3Params q, int mod
 // (ab[nf + b]), so no symbol array is read between the two transforms.
 // Grid (nf / CPC, P).
 template <int R1, int R2>
-__global__ void __launch_bounds__(256, R1 * R2 == 256 ? 3 : 4) c3_cols4_kernel(const C3Params q, float2 *hat, const Krylov *K,
-                                                       const float2 *__restrict__ twg,
-                                                       const float *__restrict__ ab) {
+__global__ void __launch_bounds__(256, R1 * R2 == 256 ? 3 : 4) c3_cols4_kernel(const C3Params q, cx *hat, const Krylov *K,
+                                                       const cx *__restrict__ twg,
+                                                       const rx *__restrict__ ab) {
   constexpr int N = R1 * R2, CPC = 256 / R1;
-  __shared__ float2 buf[N * CPC];  // [k1][n2][c]
-  __shared__ float2 tw[R1 * (R2 + 1)];
-  __shared__ float bcos[N];
+  __shared__ cx buf[N * CPC];  // [k1][n2][c]
+  __shared__ cx tw[R1 * (R2 + 1)];
+  __shared__ rx bcos[N];
   const int pr = blockIdx.y;
   if (K != nullptr && K[pr].done) return;
   for (int e = threadIdx.x; e < R1 * (R2 + 1); e += 256) tw[e] = twg[e];
   const int nf = q.nf, f0 = blockIdx.x * CPC;
   for (int e = threadIdx.x; e < N; e += 256) bcos[e] = ab[nf + e];
-  float2 *base = hat + (size_t)pr * q.N + f0;
+  cx *base = hat + (size_t)pr * q.N + f0;
   __syncthreads();
-  float2 x[16];
+  cx x[16];
   if (threadIdx.x < CPC * R2) {  // stage A: (c, n2), c fastest
     const int c = threadIdx.x % CPC, n2 = threadIdx.x / CPC;
 #pragma unroll
     for (int n1 = 0; n1 < R1; ++n1) x[n1] = base[(size_t)(R2 * n1 + n2) * nf + c];
-    dft_reg<R1>(x, -1.f);
+    dft_reg<R1>(x, -TP_R(1.0));
 #pragma unroll
     for (int k1 = 0; k1 < R1; ++k1)
       buf[(k1 * R2 + n2) * CPC + c] = k1 ? cmul(x[k1], tw[k1 * (R2 + 1) + n2]) : x[0];
@@ -636,21 +636,21 @@ __global__ void __launch_bounds__(256, R1 * R2 == 256 ? 3 : 4) c3_cols4_kernel(c
     const int c = threadIdx.x % CPC, k1 = threadIdx.x / CPC;
 #pragma unroll
     for (int n2 = 0; n2 < R2; ++n2) x[n2] = buf[(k1 * R2 + n2) * CPC + c];
-    dft_reg<R2>(x, -1.f);
+    dft_reg<R2>(x, -TP_R(1.0));
     {
-      const float sc = (float)(1.0 / ((double)nf * (double)N));
-      const float af = ab[f0 + c];
-      const float ax = (float)q.mu_x.x * af, ay = (float)q.mu_x.y * af;
-      const float mx = (float)q.mu_y.x, my = (float)q.mu_y.y;
+      const rx sc = (rx)(1.0 / ((double)nf * (double)N));
+      const rx af = ab[f0 + c];
+      const rx ax = (rx)q.mu_x.x * af, ay = (rx)q.mu_x.y * af;
+      const rx mx = (rx)q.mu_y.x, my = (rx)q.mu_y.y;
 #pragma unroll
       for (int k2 = 0; k2 < R2; ++k2) {
-        const float bb = bcos[k1 + R1 * k2];
-        const float dr = 1.f - ax - mx * bb, di = -(ay + my * bb);
-        const float m = sc / (dr * dr + di * di);
-        x[k2] = cmul(x[k2], make_float2(dr * m, -di * m));
+        const rx bb = bcos[k1 + R1 * k2];
+        const rx dr = TP_R(1.0) - ax - mx * bb, di = -(ay + my * bb);
+        const rx m = sc / (dr * dr + di * di);
+        x[k2] = cmul(x[k2], mkcx(dr * m, -di * m));
       }
     }
-    dft_reg<R2>(x, 1.f);
+    dft_reg<R2>(x, TP_R(1.0));
     __syncthreads();  // every stage-C read is done before the buffer is rewritten
 #pragma unroll
     for (int n2 = 0; n2 < R2; ++n2)
@@ -661,7 +661,7 @@ __global__ void __launch_bounds__(256, R1 * R2 == 256 ? 3 : 4) c3_cols4_kernel(c
     const int c = threadIdx.x % CPC, n2 = threadIdx.x / CPC;
 #pragma unroll
     for (int k1 = 0; k1 < R1; ++k1) x[k1] = buf[(k1 * R2 + n2) * CPC + c];
-    dft_reg<R1>(x, 1.f);
+    dft_reg<R1>(x, TP_R(1.0));
 #pragma unroll
     for (int n1 = 0; n1 < R1; ++n1) base[(size_t)(R2 * n1 + n2) * nf + c] = x[n1];
   }
@@ -670,11 +670,11 @@ __global__ void __launch_bounds__(256, R1 * R2 == 256 ? 3 : 4) c3_cols4_kernel(c
 // Inverse row transforms of hat into out (the 1/(nf nb) scale is in the
 // symbol).  Grid (nb / RPC, P).
 template <int R1, int R2>
-__global__ void __launch_bounds__(256) c3_rows4_inv_kernel(const C3Params q, const float2 *hat, float2 *out,
-                                                           const Krylov *K, const float2 *__restrict__ twg) {
+__global__ void __launch_bounds__(256) c3_rows4_inv_kernel(const C3Params q, const cx *hat, cx *out,
+                                                           const Krylov *K, const cx *__restrict__ twg) {
   constexpr int N = R1 * R2, RPC = 256 / R1, S = R1 * (R2 + 1);
-  __shared__ float2 buf[RPC * S];
-  __shared__ float2 tw[R1 * (R2 + 1)];
+  __shared__ cx buf[RPC * S];
+  __shared__ cx tw[R1 * (R2 + 1)];
   const int pr = blockIdx.y;
   if (K != nullptr && K[pr].done) return;
   for (int e = threadIdx.x; e < R1 * (R2 + 1); e += 256) tw[e] = twg[e];
@@ -682,10 +682,10 @@ __global__ void __launch_bounds__(256) c3_rows4_inv_kernel(const C3Params q, con
   __syncthreads();
   {  // inverse stage C: (row, k1)
     const int row = threadIdx.x / R1, k1 = threadIdx.x % R1;
-    float2 x[16];
+    cx x[16];
 #pragma unroll
     for (int k2 = 0; k2 < R2; ++k2) x[k2] = hat[off + row * N + k1 + R1 * k2];
-    dft_reg<R2>(x, 1.f);
+    dft_reg<R2>(x, TP_R(1.0));
 #pragma unroll
     for (int n2 = 0; n2 < R2; ++n2)
       buf[row * S + k1 * (R2 + 1) + n2] = n2 ? cmulc(x[n2], tw[k1 * (R2 + 1) + n2]) : x[0];
@@ -693,10 +693,10 @@ __global__ void __launch_bounds__(256) c3_rows4_inv_kernel(const C3Params q, con
   __syncthreads();
   if (threadIdx.x < RPC * R2) {  // inverse stage A: (row, n2)
     const int row = threadIdx.x / R2, n2 = threadIdx.x % R2;
-    float2 x[16];
+    cx x[16];
 #pragma unroll
     for (int k1 = 0; k1 < R1; ++k1) x[k1] = buf[row * S + k1 * (R2 + 1) + n2];
-    dft_reg<R1>(x, 1.f);
+    dft_reg<R1>(x, TP_R(1.0));
 #pragma unroll
     for (int n1 = 0; n1 < R1; ++n1) out[off + row * N + R2 * n1 + n2] = x[n1];
   }
@@ -705,34 +705,34 @@ __global__ void __launch_bounds__(256) c3_rows4_inv_kernel(const C3Params q, con
 // out = (I - P) y with fused fp64 dots: WHICH 0: acc_r0v += <r0, out>;
 // WHICH 1: acc_ts += <out, s>, acc_tt += <out, out>.
 template <int WHICH>
-__global__ void __launch_bounds__(k3Threads, WHICH == 0 ? 4 : 3) c3_matvec_kernel(const C3Params q, const float2 *__restrict__ cd,
-                                                              const float2 *__restrict__ y, float2 *__restrict__ out,
-                                                              const float2 *__restrict__ r0, const float2 *__restrict__ s,
+__global__ void __launch_bounds__(k3Threads, WHICH == 0 ? 4 : 3) c3_matvec_kernel(const C3Params q, const cx *__restrict__ cd,
+                                                              const cx *__restrict__ y, cx *__restrict__ out,
+                                                              const cx *__restrict__ r0, const cx *__restrict__ s,
                                                               Krylov *K) {
   constexpr int A = WHICH == 0 ? 2 : 3;  // sums per probe
   __shared__ double red[A * kStencilProbes * (k3Threads / 32)];
   const int p0 = blockIdx.y * kStencilProbes;
   const unsigned pend = pending_mask(K, p0, q.P);
   if (pend == 0) return;
-  const float2 *c_in = WHICH == 0 ? r0 : s;
+  const cx *c_in = WHICH == 0 ? r0 : s;
   double acc[A * kStencilProbes] = {};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
     const Stencil k = stencil_at(q, i);
-    const float2 dc = cd[i];
-    float2 tv[kStencilProbes], cv[kStencilProbes];
+    const cx dc = cd[i];
+    cx tv[kStencilProbes], cv[kStencilProbes];
 #pragma unroll
     for (int j = 0; j < kStencilProbes; ++j) {
       if (!(pend & (1u << j))) continue;
       const size_t off = (size_t)(p0 + j) * q.N;
-      const float2 *yy = y + off;
-      const float2 yi = yy[i];
+      const cx *yy = y + off;
+      const cx yi = yy[i];
       tv[j] = csub(yi, stencil_off(q, k, yy, i, cmul(dc, yi)));
       cv[j] = c_in[off + i];
     }
 #pragma unroll
     for (int j = 0; j < kStencilProbes; ++j) {
       if (!(pend & (1u << j))) continue;
-      const float2 t = tv[j], c = cv[j];
+      const cx t = tv[j], c = cv[j];
       out[(size_t)(p0 + j) * q.N + i] = t;
       if (WHICH == 0) {  // conj(r0) t
         acc[A * j] += (double)c.x * t.x + (double)c.y * t.y;
@@ -757,10 +757,10 @@ __global__ void __launch_bounds__(k3Threads, WHICH == 0 ? 4 : 3) c3_matvec_kerne
 // omega = <t,s>/<t,t>; x += alpha y + omega z (x = 0 before the first
 // iteration of a step: not read then); r = s - omega t; accumulate <r0, r>
 // and ||r||^2 for the next iteration.
-__global__ void __launch_bounds__(k3Threads) c3_update_kernel(const C3Params q, float2 *x, float2 *r,
-                                                              const float2 *__restrict__ r0, const float2 *__restrict__ y,
-                                                              const float2 *__restrict__ z, const float2 *__restrict__ s,
-                                                              const float2 *__restrict__ t, Krylov *K,
+__global__ void __launch_bounds__(k3Threads) c3_update_kernel(const C3Params q, cx *x, cx *r,
+                                                              const cx *__restrict__ r0, const cx *__restrict__ y,
+                                                              const cx *__restrict__ z, const cx *__restrict__ s,
+                                                              const cx *__restrict__ t, Krylov *K,
                                                               const C3State *st) {
   __shared__ double red[3 * (k3Threads / 32)];
   const int pr = blockIdx.y;
@@ -770,15 +770,15 @@ __global__ void __launch_bounds__(k3Threads) c3_update_kernel(const C3Params q, 
   const double den = k.acc_r0v.x * k.acc_r0v.x + k.acc_r0v.y * k.acc_r0v.y;
   const double2 alpha = den > 0.0 ? zdiv(k.rho_cur, k.acc_r0v) : z2(0, 0);
   const double2 omega = (k.acc_tt > 0.0) ? zscale(k.acc_ts, 1.0 / k.acc_tt) : z2(0, 0);
-  const float2 al = to_f2(alpha), om = to_f2(omega);
+  const cx al = to_cx(alpha), om = to_cx(omega);
   const bool first = st->it == 0;
   double a0 = 0.0, a1 = 0.0, a2 = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
-    const float2 x0 = first ? make_float2(0.f, 0.f) : x[off + i];
+    const cx x0 = first ? mkcx(TP_R(0.0), TP_R(0.0)) : x[off + i];
     x[off + i] = cfma(om, z[off + i], cfma(al, y[off + i], x0));
-    const float2 rv = cfnma(om, t[off + i], s[off + i]);
+    const cx rv = cfnma(om, t[off + i], s[off + i]);
     r[off + i] = rv;
-    const float2 c = r0[off + i];
+    const cx c = r0[off + i];
     a0 += (double)c.x * rv.x + (double)c.y * rv.y;
     a1 += (double)c.x * rv.y - (double)c.y * rv.x;
     a2 += (double)rv.x * rv.x + (double)rv.y * rv.y;
@@ -791,10 +791,10 @@ __global__ void __launch_bounds__(k3Threads) c3_update_kernel(const C3Params q, 
 // then u += d, stored into node `to` of u_store (to = t, or L - t for the
 // flipped reference adjoint) and, at the last step, into exit_out.
 __global__ void __launch_bounds__(k3Threads, 4) c3_finish_kernel(const C3Params q, const C3State *st,
-                                                              const float2 *__restrict__ cd,
-                                                              const float2 *__restrict__ x, const float2 *__restrict__ r0,
-                                                              float2 *u, Krylov *K, float2 *u_store, int flip,
-                                                              float2 *exit_out) {
+                                                              const cx *__restrict__ cd,
+                                                              const cx *__restrict__ x, const cx *__restrict__ r0,
+                                                              cx *u, Krylov *K, cx *u_store, int flip,
+                                                              cx *exit_out) {
   __shared__ double red[kStencilProbes * (k3Threads / 32)];
   const int p0 = blockIdx.y * kStencilProbes;
   const int np = q.P - p0 < kStencilProbes ? q.P - p0 : kStencilProbes;
@@ -809,20 +809,20 @@ __global__ void __launch_bounds__(k3Threads, 4) c3_finish_kernel(const C3Params 
   double acc[kStencilProbes] = {};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x) {
     Stencil k{};
-    float2 dc = make_float2(0.f, 0.f);
+    cx dc = mkcx(TP_R(0.0), TP_R(0.0));
     if (iterated) {
       k = stencil_at(q, i);
       dc = cd[i];
     }
-    float2 unv[kStencilProbes];
+    cx unv[kStencilProbes];
 #pragma unroll
     for (int j = 0; j < kStencilProbes; ++j) {
       if (j >= np) break;
       const size_t off = (size_t)(p0 + j) * q.N;
       const bool it = iterated & (1u << j);
-      const float2 xi = it ? x[off + i] : make_float2(0.f, 0.f);
-      const float2 mx = it ? csub(xi, stencil_off(q, k, x + off, i, cmul(dc, xi))) : xi;
-      const float2 d = csub(r0[off + i], mx);
+      const cx xi = it ? x[off + i] : mkcx(TP_R(0.0), TP_R(0.0));
+      const cx mx = it ? csub(xi, stencil_off(q, k, x + off, i, cmul(dc, xi))) : xi;
+      const cx d = csub(r0[off + i], mx);
       acc[j] += (double)d.x * d.x + (double)d.y * d.y;
       unv[j] = cadd(u[off + i], xi);
     }
@@ -859,8 +859,8 @@ __global__ void c3_stats_kernel(Krylov *K, int P, double tol2, int *stats) {
 }
 
 // Store the state (P, N) into slice `t` of u_store (P, nz, N) and/or exit.
-__global__ void c3_store_kernel(int N, int P, int nz, int t, const float2 *__restrict__ u, float2 *u_store,
-                                float2 *exit_out) {
+__global__ void c3_store_kernel(int N, int P, int nz, int t, const cx *__restrict__ u, cx *u_store,
+                                cx *exit_out) {
   const size_t total = (size_t)P * N;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
     const size_t pr = e / N, i = e % N;
@@ -872,14 +872,14 @@ __global__ void c3_store_kernel(int N, int P, int nz, int t, const float2 *__res
 // grad_c[s-1][i] += sum_p lambda_p[i] conj(u_p,s[i] + u_p,s-1[i]) for the
 // current step's slice s (no atomics: one thread owns element i and loops
 // over the probes).
-__global__ void c3_grad_kernel(int N, int P, int nz, const C3State *st, const float2 *__restrict__ lam,
-                               const float2 *__restrict__ u_fwd, float2 *grad_c) {
+__global__ void c3_grad_kernel(int N, int P, int nz, const C3State *st, const cx *__restrict__ lam,
+                               const cx *__restrict__ u_fwd, cx *grad_c) {
   constexpr int G = 8;  // probes whose loads are issued together
   const int s = st->s;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-    float2 acc = make_float2(0.f, 0.f);
+    cx acc = mkcx(TP_R(0.0), TP_R(0.0));
     for (int p0 = 0; p0 < P; p0 += G) {
-      float2 a[G], b[G], l[G];
+      cx a[G], b[G], l[G];
 #pragma unroll
       for (int j = 0; j < G; ++j) {
         if (p0 + j < P) {
@@ -893,11 +893,12 @@ __global__ void c3_grad_kernel(int N, int P, int nz, const C3State *st, const fl
       for (int j = 0; j < G; ++j)
         if (p0 + j < P) acc = cadd(acc, cmulc(l[j], cadd(a[j], b[j])));
     }
-    float2 g = grad_c[(size_t)(s - 1) * N + i];
+    cx g = grad_c[(size_t)(s - 1) * N + i];
     grad_c[(size_t)(s - 1) * N + i] = cadd(g, acc);
   }
 }
 
+#ifndef TP_C128_CHECK  // the learned preconditioner is not part of the complex128 check build
 // Learned correction of the preconditioned vector: out = z + sum_t F_t z(x + o_t)
 // with the filter of the current step's slice s (conj(F) in the adjoint
 // modes).  The filters of all slices are computed before the march, in
@@ -919,10 +920,10 @@ __host__ __device__ constexpr int filter_cw(int nf) { return nf < 256 ? nf : 256
 __host__ __device__ constexpr int filter_rb(int nf) { return 2 * (256 / filter_cw(nf)); }
 
 __global__ void __launch_bounds__(k3Threads, 2) c3_filter_kernel(const C3Params q, const C3State *st, int chunk,
-                                                                 const float2 *__restrict__ Fall,
-                                                                 const float2 *__restrict__ z, float2 *__restrict__ out,
+                                                                 const cx *__restrict__ Fall,
+                                                                 const cx *__restrict__ z, cx *__restrict__ out,
                                                                  const Krylov *K) {
-  extern __shared__ __align__(16) float2 ztile[];  // [kFilterProbes][rb + 4][cw + 4]
+  extern __shared__ __align__(16) cx ztile[];  // [kFilterProbes][rb + 4][cw + 4]
   const int nf = q.nf, nb = q.nb;
   const int cw = filter_cw(nf), rb = filter_rb(nf), W = cw + 4, H = rb + 4;
   const int c0 = blockIdx.x * cw, b0 = blockIdx.y * rb, p0 = blockIdx.z * kFilterProbes;
@@ -931,19 +932,19 @@ __global__ void __launch_bounds__(k3Threads, 2) c3_filter_kernel(const C3Params 
   for (int j = 0; j < np_cta; ++j)
     if (K == nullptr || !K[p0 + j].done) pend |= 1u << j;
   // tile row y holds image row b0 - 2 + y, columns c0 - 2 .. c0 + cw + 1 (zero outside the image)
-  const float2 zero = make_float2(0.f, 0.f);
+  const cx zero = mkcx(TP_R(0.0), TP_R(0.0));
   const bool pairs16 = ((nf | cw) & 1) == 0;  // 16-byte copies of column pairs
   for (int j = 0; j < np_cta; ++j) {
     if (!((pend >> j) & 1u)) continue;
-    const float2 *src = z + (size_t)(p0 + j) * q.N;
+    const cx *src = z + (size_t)(p0 + j) * q.N;
     for (int y = 0; y < H; ++y) {
       const int b = b0 - 2 + y;
-      float2 *dst = ztile + (j * H + y) * W;
+      cx *dst = ztile + (j * H + y) * W;
       if (b < 0 || b >= nb) {
         for (int x = threadIdx.x; x < W; x += blockDim.x) dst[x] = zero;
         continue;
       }
-      const float2 *srow = src + (size_t)b * nf;
+      const cx *srow = src + (size_t)b * nf;
       if (pairs16) {
         for (int m = 2 * threadIdx.x; m < cw; m += 2 * blockDim.x) {
           if (c0 + m < nf) {
@@ -955,14 +956,14 @@ __global__ void __launch_bounds__(k3Threads, 2) c3_filter_kernel(const C3Params 
         }
       } else {
         for (int m = threadIdx.x; m < cw; m += blockDim.x) {
-          if (c0 + m < nf) cp_async8(&dst[2 + m], &srow[c0 + m]);
+          if (c0 + m < nf) cp_async_cx(&dst[2 + m], &srow[c0 + m]);
           else dst[2 + m] = zero;
         }
       }
       if (threadIdx.x < 4) {  // border columns x = 0, 1, cw + 2, cw + 3
         const int x = threadIdx.x < 2 ? threadIdx.x : cw + threadIdx.x;
         const int f = c0 - 2 + x;
-        if (f >= 0 && f < nf) cp_async8(&dst[x], &srow[f]);
+        if (f >= 0 && f < nf) cp_async_cx(&dst[x], &srow[f]);
         else dst[x] = zero;
       }
     }
@@ -974,15 +975,15 @@ __global__ void __launch_bounds__(k3Threads, 2) c3_filter_kernel(const C3Params 
   const bool va = act && ba < nb, vb = act && ba + 1 < nb;
   const int sl = st->s - 1;
   const size_t np = (size_t)chunk * q.N;
-  const float2 *F = Fall + (size_t)(sl / chunk) * kFilterTaps * np + (size_t)(sl % chunk) * q.N;
-  const float cs = q.conj_t ? -1.f : 1.f;
-  float2 wa[kFilterTaps], wb[kFilterTaps];
+  const cx *F = Fall + (size_t)(sl / chunk) * kFilterTaps * np + (size_t)(sl % chunk) * q.N;
+  const rx cs = q.conj_t ? -TP_R(1.0) : TP_R(1.0);
+  cx wa[kFilterTaps], wb[kFilterTaps];
 #pragma unroll
   for (int t = 0; t < kFilterTaps; ++t) {
-    const float2 a = va ? F[(size_t)t * np + (size_t)ba * nf + f] : make_float2(0.f, 0.f);
-    const float2 b = vb ? F[(size_t)t * np + (size_t)(ba + 1) * nf + f] : make_float2(0.f, 0.f);
-    wa[t] = make_float2(a.x, cs * a.y);
-    wb[t] = make_float2(b.x, cs * b.y);
+    const cx a = va ? F[(size_t)t * np + (size_t)ba * nf + f] : mkcx(TP_R(0.0), TP_R(0.0));
+    const cx b = vb ? F[(size_t)t * np + (size_t)(ba + 1) * nf + f] : mkcx(TP_R(0.0), TP_R(0.0));
+    wa[t] = mkcx(a.x, cs * a.y);
+    wb[t] = mkcx(b.x, cs * b.y);
   }
   cp_async_wait_all();
   __syncthreads();
@@ -991,15 +992,15 @@ __global__ void __launch_bounds__(k3Threads, 2) c3_filter_kernel(const C3Params 
     const int pj = p0 + j;
     if (!((pend >> j) & 1u)) continue;
     // row k of the window is tile row 2 pr + k, k = 0..5; pixel a sits in row 2, b in row 3
-    const float2 *rw = ztile + j * H * W + 2 * pr * W + fx + 2;
-    const float2 m2 = rw[0];
-    const float2 m1l = rw[W - 1], m1c = rw[W], m1r = rw[W + 1];
-    const float2 a_l2 = rw[2 * W - 2], a_l1 = rw[2 * W - 1], a_c = rw[2 * W], a_r1 = rw[2 * W + 1], a_r2 = rw[2 * W + 2];
-    const float2 b_l2 = rw[3 * W - 2], b_l1 = rw[3 * W - 1], b_c = rw[3 * W], b_r1 = rw[3 * W + 1], b_r2 = rw[3 * W + 2];
-    const float2 p2l = rw[4 * W - 1], p2c = rw[4 * W], p2r = rw[4 * W + 1];
-    const float2 p3 = rw[5 * W];
+    const cx *rw = ztile + j * H * W + 2 * pr * W + fx + 2;
+    const cx m2 = rw[0];
+    const cx m1l = rw[W - 1], m1c = rw[W], m1r = rw[W + 1];
+    const cx a_l2 = rw[2 * W - 2], a_l1 = rw[2 * W - 1], a_c = rw[2 * W], a_r1 = rw[2 * W + 1], a_r2 = rw[2 * W + 2];
+    const cx b_l2 = rw[3 * W - 2], b_l1 = rw[3 * W - 1], b_c = rw[3 * W], b_r1 = rw[3 * W + 1], b_r2 = rw[3 * W + 2];
+    const cx p2l = rw[4 * W - 1], p2c = rw[4 * W], p2r = rw[4 * W + 1];
+    const cx p3 = rw[5 * W];
     // taps (dy, dx): (0,0) (0,-1) (0,1) (-1,0) (1,0) (-1,-1) (-1,1) (1,-1) (1,1) (0,-2) (0,2) (-2,0) (2,0)
-    float2 A = a_c;
+    cx A = a_c;
     A = cfma(wa[0], a_c, A);
     A = cfma(wa[1], a_l1, A);
     A = cfma(wa[2], a_r1, A);
@@ -1013,7 +1014,7 @@ __global__ void __launch_bounds__(k3Threads, 2) c3_filter_kernel(const C3Params 
     A = cfma(wa[10], a_r2, A);
     A = cfma(wa[11], m2, A);
     A = cfma(wa[12], p2c, A);
-    float2 B = b_c;
+    cx B = b_c;
     B = cfma(wb[0], b_c, B);
     B = cfma(wb[1], b_l1, B);
     B = cfma(wb[2], b_r1, B);
@@ -1027,16 +1028,18 @@ __global__ void __launch_bounds__(k3Threads, 2) c3_filter_kernel(const C3Params 
     B = cfma(wb[10], b_r2, B);
     B = cfma(wb[11], m1c, B);
     B = cfma(wb[12], p3, B);
-    float2 *dst = out + (size_t)pj * q.N + (size_t)ba * nf + f;
+    cx *dst = out + (size_t)pj * q.N + (size_t)ba * nf + f;
     dst[0] = A;
     if (vb) dst[nf] = B;
   }
 }
 
+#endif  // TP_C128_CHECK
+
 // out = (I - P_s) x (no inner products): right-hand sides of the white-noise
 // training pairs.  Grid (chunks, P).
-__global__ void __launch_bounds__(k3Threads) c3_apply_a_kernel(const C3Params q, const float2 *__restrict__ cd,
-                                                               const float2 *__restrict__ x, float2 *out) {
+__global__ void __launch_bounds__(k3Threads) c3_apply_a_kernel(const C3Params q, const cx *__restrict__ cd,
+                                                               const cx *__restrict__ x, cx *out) {
   const size_t off = (size_t)blockIdx.y * q.N;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < q.N; i += gridDim.x * blockDim.x)
     out[off + i] = csub(x[off + i], apply_P(q, cd, x + off, i));
@@ -1050,12 +1053,12 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
   return z ^ (z >> 31);
 }
-__global__ void c3_noise_kernel(int N, int P, int step, float2 *x) {
+__global__ void c3_noise_kernel(int N, int P, int step, cx *x) {
   const size_t total = (size_t)P * N;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
     const uint64_t h = mix64(((uint64_t)step << 40) ^ (uint64_t)e);
-    const float a = (float)(h >> 40) * (1.f / 16777216.f), b = (float)((h >> 16) & 0xFFFFFFu) * (1.f / 16777216.f);
-    x[e] = make_float2(2.f * a - 1.f, 2.f * b - 1.f);
+    const rx a = (rx)(h >> 40) * (TP_R(1.0) / TP_R(16777216.0)), b = (rx)((h >> 16) & 0xFFFFFFu) * (TP_R(1.0) / TP_R(16777216.0));
+    x[e] = mkcx(TP_R(2.0) * a - TP_R(1.0), TP_R(2.0) * b - TP_R(1.0));
   }
 }
 
@@ -1063,19 +1066,19 @@ __global__ void c3_noise_kernel(int N, int P, int step, float2 *x) {
 __global__ void c3_flag_kernel(int *stats, int graph) { stats[4] = graph; }
 
 // out[i] = cd[i] - kc[i]: the object part sigma*T(c_s) of the slice's diagonal.
-__global__ void c3_diag_diff_kernel(int N, const float2 *__restrict__ cd, const float2 *__restrict__ kc, float2 *out) {
+__global__ void c3_diag_diff_kernel(int N, const cx *__restrict__ cd, const cx *__restrict__ kc, cx *out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
-    out[i] = make_float2(cd[i].x - kc[i].x, cd[i].y - kc[i].y);
+    out[i] = mkcx(cd[i].x - kc[i].x, cd[i].y - kc[i].y);
 }
 
 // ------------------------------------------------------------------ host
 struct C3Work {
-  float2 *u, *x, *r, *r0, *p, *v, *s, *y, *z, *t, *hat;
-  float2 *cdl, *cdr;
-  float2 *dc, *dw, *de, *ds, *dn;
-  float2 *sym, *twf, *twb;  // preconditioner symbol (N) and twiddle tables
-  float2 *tw4;              // padded twiddle table of the four-step transforms
-  float *ab;                // 2 cos(2 pi f / nf) - 2, then the same for b / nb
+  cx *u, *x, *r, *r0, *p, *v, *s, *y, *z, *t, *hat;
+  cx *cdl, *cdr;
+  cx *dc, *dw, *de, *ds, *dn;
+  cx *sym, *twf, *twb;  // preconditioner symbol (N) and twiddle tables
+  cx *tw4;              // padded twiddle table of the four-step transforms
+  rx *ab;                // 2 cos(2 pi f / nf) - 2, then the same for b / nb
   Krylov *K;
   C3State *st;
   size_t bytes;
@@ -1091,26 +1094,26 @@ static C3Work c3_layout(char *base, int N, int P) {
     off += align256(bytes);
     return ptr;
   };
-  const size_t vec = (size_t)P * N * sizeof(float2);
-  float2 **vecs[] = {&w.u, &w.x, &w.r, &w.r0, &w.p, &w.v, &w.s, &w.y, &w.z, &w.t, &w.hat};
-  for (float2 **v : vecs) *v = reinterpret_cast<float2 *>(take(vec));
-  float2 **diag[] = {&w.cdl, &w.cdr, &w.dc, &w.dw, &w.de, &w.ds, &w.dn, &w.sym};
-  for (float2 **d : diag) *d = reinterpret_cast<float2 *>(take((size_t)N * sizeof(float2)));
-  w.twf = reinterpret_cast<float2 *>(take((size_t)kFftMaxN * sizeof(float2)));
-  w.twb = reinterpret_cast<float2 *>(take((size_t)kFftMaxN * sizeof(float2)));
-  w.tw4 = reinterpret_cast<float2 *>(take((size_t)four_tw_len(256) * sizeof(float2)));
-  w.ab = reinterpret_cast<float *>(take((size_t)2 * kFftMaxN * sizeof(float)));
+  const size_t vec = (size_t)P * N * sizeof(cx);
+  cx **vecs[] = {&w.u, &w.x, &w.r, &w.r0, &w.p, &w.v, &w.s, &w.y, &w.z, &w.t, &w.hat};
+  for (cx **v : vecs) *v = reinterpret_cast<cx *>(take(vec));
+  cx **diag[] = {&w.cdl, &w.cdr, &w.dc, &w.dw, &w.de, &w.ds, &w.dn, &w.sym};
+  for (cx **d : diag) *d = reinterpret_cast<cx *>(take((size_t)N * sizeof(cx)));
+  w.twf = reinterpret_cast<cx *>(take((size_t)kFftMaxN * sizeof(cx)));
+  w.twb = reinterpret_cast<cx *>(take((size_t)kFftMaxN * sizeof(cx)));
+  w.tw4 = reinterpret_cast<cx *>(take((size_t)four_tw_len(256) * sizeof(cx)));
+  w.ab = reinterpret_cast<rx *>(take((size_t)2 * kFftMaxN * sizeof(rx)));
   w.K = reinterpret_cast<Krylov *>(take((size_t)P * sizeof(Krylov)));
   w.st = reinterpret_cast<C3State *>(take(sizeof(C3State)));
   w.bytes = off;
   return w;
 }
 
-using RowsKernel = void (*)(const FftPlan, const C3Params, int, const float2 *, float2 *, const float2 *, float2 *,
-                           float2 *, const Krylov *, int, int, const float2 *, const float2 *, const C3State *);
-using ColsKernel = void (*)(const FftPlan, const C3Params, float2 *, const Krylov *, int, const float2 *,
-                           const float2 *);
-using InvKernel = void (*)(const FftPlan, const C3Params, const float2 *, float2 *, const Krylov *, int, const float2 *);
+using RowsKernel = void (*)(const FftPlan, const C3Params, int, const cx *, cx *, const cx *, cx *,
+                           cx *, const Krylov *, int, int, const cx *, const cx *, const C3State *);
+using ColsKernel = void (*)(const FftPlan, const C3Params, cx *, const Krylov *, int, const cx *,
+                           const cx *);
+using InvKernel = void (*)(const FftPlan, const C3Params, const cx *, cx *, const Krylov *, int, const cx *);
 struct PrecKernels {
   RowsKernel rows;
   ColsKernel cols;
@@ -1139,10 +1142,10 @@ static PrecKernels prec_kernels(int nf, int nb) {
   return prec_kernels_t<0, 0>();
 }
 
-using Rows4Kernel = void (*)(const C3Params, int, const float2 *, float2 *, const float2 *, float2 *, float2 *,
-                            const Krylov *, const float2 *, const float2 *, const C3State *);
-using Cols4Kernel = void (*)(const C3Params, float2 *, const Krylov *, const float2 *, const float *);
-using Inv4Kernel = void (*)(const C3Params, const float2 *, float2 *, const Krylov *, const float2 *);
+using Rows4Kernel = void (*)(const C3Params, int, const cx *, cx *, const cx *, cx *, cx *,
+                            const Krylov *, const cx *, const cx *, const C3State *);
+using Cols4Kernel = void (*)(const C3Params, cx *, const Krylov *, const cx *, const rx *);
+using Inv4Kernel = void (*)(const C3Params, const cx *, cx *, const Krylov *, const cx *);
 struct Prec4Kernels {
   Rows4Kernel rows = nullptr;
   Cols4Kernel cols = nullptr;
@@ -1163,8 +1166,12 @@ static Prec4Kernels prec4_kernels(int nf, int nb) {
   switch (nf) {
     case 64: return prec4_kernels_t<8, 8>();
     case 128: return prec4_kernels_t<16, 8>();
+#ifndef TP_C128_CHECK  // complex128 tiles of 192 and 256 exceed 48 KB of static shared memory
     case 192: return prec4_kernels_t<16, 12>();
     default: return prec4_kernels_t<16, 16>();
+#else
+    default: return {};
+#endif
   }
 }
 
@@ -1203,7 +1210,7 @@ static int cnn_chunk(int L) { return L < kCnnChunk ? L : kCnnChunk; }
 
 struct C3Learned {
   char *cnn;
-  float2 *F, *dg, *zt;
+  cx *F, *dg, *zt;
   int chunk, nchunks;
   size_t cnn_bytes, bytes;
 };
@@ -1220,11 +1227,15 @@ static C3Learned c3_learned_layout(char *base, int nf, int nb, int nz, int P) {
   const int L = nz - 1;
   l.chunk = cnn_chunk(L);
   l.nchunks = (L + l.chunk - 1) / l.chunk;
+#ifndef TP_C128_CHECK
   l.cnn_bytes = cnn_forward_ws_bytes(conv_geom(nb, nf, l.chunk));
+#else
+  l.cnn_bytes = 0;
+#endif
   l.cnn = take(l.cnn_bytes);
-  l.F = reinterpret_cast<float2 *>(take((size_t)l.nchunks * kFilterTaps * l.chunk * N * sizeof(float2)));
-  l.dg = reinterpret_cast<float2 *>(take((size_t)l.chunk * N * sizeof(float2)));
-  l.zt = reinterpret_cast<float2 *>(take((size_t)P * N * sizeof(float2)));
+  l.F = reinterpret_cast<cx *>(take((size_t)l.nchunks * kFilterTaps * l.chunk * N * sizeof(cx)));
+  l.dg = reinterpret_cast<cx *>(take((size_t)l.chunk * N * sizeof(cx)));
+  l.zt = reinterpret_cast<cx *>(take((size_t)P * N * sizeof(cx)));
   l.bytes = off;
   return l;
 }
@@ -1337,6 +1348,9 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   const bool learned = a->precond == 2;
   C3Learned lw{};
   if (learned) {
+#ifdef TP_C128_CHECK
+    return set_error(TP_ERR_UNSUPPORTED, "the complex128 check build has no learned preconditioner");
+#endif
     if (a->model == nullptr || a->learned_ws == nullptr)
       return set_error(TP_ERR_INVALID, "learned preconditioner: NULL model or workspace");
     if (!fft_on) return set_error(TP_ERR_UNSUPPORTED, "learned preconditioner needs FFT-plannable nf, nb (got %d, %d)", nf, nb);
@@ -1358,8 +1372,8 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   const bool four = p4.rows != nullptr;
   const int rpc4 = four ? 256 / p4.r1 : 1;
   const int srow_f = pk.fixed ? nf + nf / 8 + 1 : nf, srow_b = pk.fixed ? nb + nb / 8 + 1 : nb;
-  const size_t smem_rows = (size_t)(nf + 2 * rpc * srow_f) * sizeof(float2);
-  const size_t smem_cols = (size_t)(nb + 2 * cpc * srow_b) * sizeof(float2);
+  const size_t smem_rows = (size_t)(nf + 2 * rpc * srow_f) * sizeof(cx);
+  const size_t smem_cols = (size_t)(nb + 2 * cpc * srow_b) * sizeof(cx);
   if (use_fft) {
     TP_CHECK_CUDA(cudaFuncSetAttribute(pk.rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
     TP_CHECK_CUDA(cudaFuncSetAttribute(pk.inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_rows));
@@ -1373,25 +1387,29 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   const bool backward = a->mode != TP_MODE_FORWARD;
   const bool flip = a->mode == TP_MODE_ADJOINT;
   const int adj_exact = a->mode == TP_MODE_ADJOINT_EXACT ? 1 : 0;
-  float2 *ust = static_cast<float2 *>(a->u_store);
-  float2 *exit_out = static_cast<float2 *>(a->exit_out);
+  cx *ust = static_cast<cx *>(a->u_store);
+  cx *exit_out = static_cast<cx *>(a->exit_out);
+#ifndef TP_C128_CHECK
   // learned filter: column blocks of at most 256, two rows per thread
   const int fcw = filter_cw(nf), frb = filter_rb(nf);
   const dim3 fgrid((nf + fcw - 1) / fcw, (nb + frb - 1) / frb, (P + kFilterProbes - 1) / kFilterProbes);
-  const size_t smem_filter = (size_t)kFilterProbes * (frb + 4) * (fcw + 4) * sizeof(float2);
+  const size_t smem_filter = (size_t)kFilterProbes * (frb + 4) * (fcw + 4) * sizeof(cx);
   if (learned)
     TP_CHECK_CUDA(cudaFuncSetAttribute(c3_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_filter));
+#endif
   const dim3 vgrid((N + 256 * 8 - 1) / (256 * 8), P);
   const dim3 sg_init = stencil_grid(c3_init_kernel, N, P), sg_fin = stencil_grid(c3_finish_kernel, N, P);
   const dim3 sg_mv0 = stencil_grid(c3_matvec_kernel<0>, N, P), sg_mv1 = stencil_grid(c3_matvec_kernel<1>, N, P);
   const int pgrid = (P + 127) / 128;
   const int one_cta = P >= 1024 ? 1024 : ((P + 31) / 32) * 32;
   const int eb = 296;
+#ifndef TP_C128_CHECK
   const ConvGeom gch = learned ? conv_geom(nb, nf, lw.chunk) : ConvGeom{};
+#endif
 
   // ---- launch sequences (recorded into a graph, or issued step by step)
   // M0^{-1} in -> out (mode 0/1/2 input of the row kernel; Kp NULL = all probes)
-  auto precondition = [&](cudaStream_t s, int mode, const float2 *rin, float2 *out, const Krylov *Kp) {
+  auto precondition = [&](cudaStream_t s, int mode, const cx *rin, cx *out, const Krylov *Kp) {
     if (four) {
       p4.rows<<<dim3(nb / rpc4, P), 256, 0, s>>>(q, mode, rin, w.p, w.v, w.s, w.hat, Kp, w.tw4, w.r0, w.st);
       p4.cols<<<dim3(nf / rpc4, P), 256, 0, s>>>(q, w.hat, Kp, w.tw4, w.ab);
@@ -1416,10 +1434,11 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
         c3_symbol_kernel<<<eb, 256, 0, s>>>(q, w.sym);
       }
     }
-    c3_diag_kernel<<<eb, 256, 0, s>>>(N, nf, q.sigma, q.conj_t, static_cast<const float2 *>(op->kc),
-                                      static_cast<const float2 *>(op->kw), static_cast<const float2 *>(op->ke),
-                                      static_cast<const float2 *>(op->ks), static_cast<const float2 *>(op->kn), w.dc,
+    c3_diag_kernel<<<eb, 256, 0, s>>>(N, nf, q.sigma, q.conj_t, static_cast<const cx *>(op->kc),
+                                      static_cast<const cx *>(op->kw), static_cast<const cx *>(op->ke),
+                                      static_cast<const cx *>(op->ks), static_cast<const cx *>(op->kn), w.dc,
                                       w.dw, w.de, w.ds, w.dn);
+#ifndef TP_C128_CHECK
     if (learned && !a->learned_reuse) {
       // the filters of every slice, chunk by chunk (the CNN activations' zero
       // borders are never written by the kernels)
@@ -1429,16 +1448,17 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
       qf.conj_t = 0;
       for (int c = 0; c < lw.nchunks; ++c) {
         const int s0 = c * lw.chunk, cnt = (L - s0) < lw.chunk ? (L - s0) : lw.chunk;
-        if (cnt < lw.chunk) TP_CHECK_CUDA(cudaMemsetAsync(lw.dg, 0, (size_t)lw.chunk * N * sizeof(float2), s));
+        if (cnt < lw.chunk) TP_CHECK_CUDA(cudaMemsetAsync(lw.dg, 0, (size_t)lw.chunk * N * sizeof(cx), s));
         c3_obj_diag_kernel<<<eb * 2, 256, 0, s>>>(qf, s0, cnt, lw.dg);
         const int rc = cnn_forward(gch, *a->model, lw.dg, N, nullptr, lw.cnn,
                                    lw.F + (size_t)c * kFilterTaps * lw.chunk * N, s);
         if (rc != TP_OK) return rc;
       }
     }
-    TP_CHECK_CUDA(cudaMemsetAsync(w.u, 0, (size_t)P * N * sizeof(float2), s));
+#endif
+    TP_CHECK_CUDA(cudaMemsetAsync(w.u, 0, (size_t)P * N * sizeof(cx), s));
     if (a->probes != nullptr)
-      TP_CHECK_CUDA(cudaMemcpyAsync(w.u, a->probes, (size_t)P * N * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+      TP_CHECK_CUDA(cudaMemcpyAsync(w.u, a->probes, (size_t)P * N * sizeof(cx), cudaMemcpyDeviceToDevice, s));
     TP_CHECK_CUDA(cudaMemsetAsync(w.K, 0, (size_t)P * sizeof(Krylov), s));
     TP_CHECK_CUDA(cudaMemsetAsync(w.st, 0, sizeof(C3State), s));
     if (ust) c3_store_kernel<<<eb, 256, 0, s>>>(N, P, nz, flip ? L : 0, w.u, ust, nullptr);
@@ -1450,19 +1470,23 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     c3_center_kernel<<<eb, 256, 0, s>>>(q, w.st, 0, w.cdl);
     if (adj_exact) c3_center_kernel<<<eb, 256, 0, s>>>(q, w.st, 1, w.cdr);
     c3_init_kernel<<<sg_init, k3Threads, 0, s>>>(q, w.st, adj_exact, w.cdl, w.cdr, w.u,
-                                                static_cast<const float2 *>(a->src_exit),
-                                                static_cast<const float2 *>(a->src_shared), w.r0, w.K);
+                                                static_cast<const cx *>(a->src_exit),
+                                                static_cast<const cx *>(a->src_shared), w.r0, w.K);
     c3_start_kernel<<<pgrid, 128, 0, s>>>(w.K, P);
   };
   // one BiCGStab iteration of every pending probe
   auto iteration = [&](cudaStream_t s, int use_cond, cudaGraphConditionalHandle inner) {
     // p = r + beta (p - omega v); y = Prec(p); v = M y
     precondition(s, 0, w.r, learned ? lw.zt : w.y, w.K);
+#ifndef TP_C128_CHECK
     if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.y, w.K);
+#endif
     c3_matvec_kernel<0><<<sg_mv0, k3Threads, 0, s>>>(q, w.cdl, w.y, w.v, w.r0, w.s, w.K);
     // s = r - alpha v; z = Prec(s); t = M z
     precondition(s, 1, w.r, learned ? lw.zt : w.z, w.K);
+#ifndef TP_C128_CHECK
     if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.z, w.K);
+#endif
     c3_matvec_kernel<1><<<sg_mv1, k3Threads, 0, s>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K);
     c3_update_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.x, w.r, w.r0, w.y, w.z, w.s, w.t, w.K, w.st);
     c3_commit_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, w.st, max_iter, use_cond, inner);
@@ -1472,8 +1496,8 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     c3_finish_kernel<<<sg_fin, k3Threads, 0, s>>>(q, w.st, w.cdl, w.x, w.r0, w.u, w.K, ust, flip ? 1 : 0, exit_out);
     c3_stats_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, stats);
     if (a->grad_c)
-      c3_grad_kernel<<<eb, 256, 0, s>>>(N, P, nz, w.st, w.u, static_cast<const float2 *>(a->u_fwd),
-                                        static_cast<float2 *>(a->grad_c));
+      c3_grad_kernel<<<eb, 256, 0, s>>>(N, P, nz, w.st, w.u, static_cast<const cx *>(a->u_fwd),
+                                        static_cast<cx *>(a->grad_c));
   };
 
   // ---- one graph: prologue, then WHILE(step) { head; WHILE(iteration) {..}; tail }
@@ -1576,7 +1600,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   for (int t = 1; t <= L; ++t) {
     // a training pair copies x, which a probe with a zero right-hand side
     // never writes in its step
-    if (train) TP_CHECK_CUDA(cudaMemsetAsync(w.x, 0, (size_t)P * N * sizeof(float2), st));
+    if (train) TP_CHECK_CUDA(cudaMemsetAsync(w.x, 0, (size_t)P * N * sizeof(cx), st));
     step_head(st, 0, 0, 0);
     for (int it = 0; it < max_iter; ++it) {
       iteration(st, 0, 0);
@@ -1595,23 +1619,23 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
       // (train_kind 0), or x white noise and v = (I - P_s) x (train_kind 1);
       // plus the slice's object diagonal
       const size_t k = (size_t)(t / a->train_every - 1);
-      float2 *tz = static_cast<float2 *>(a->train_z0) + k * P * N;
-      float2 *tx = static_cast<float2 *>(a->train_sol) + k * P * N;
-      const float2 *v = w.r0;
+      cx *tz = static_cast<cx *>(a->train_z0) + k * P * N;
+      cx *tx = static_cast<cx *>(a->train_sol) + k * P * N;
+      const cx *v = w.r0;
       if (a->train_kind == 1) {
         c3_noise_kernel<<<eb, 256, 0, st>>>(N, P, t, tx);
         c3_apply_a_kernel<<<vgrid, k3Threads, 0, st>>>(q, w.cdl, tx, w.t);
         v = w.t;
       } else {
-        TP_CHECK_CUDA(cudaMemcpyAsync(tx, w.x, (size_t)P * N * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+        TP_CHECK_CUDA(cudaMemcpyAsync(tx, w.x, (size_t)P * N * sizeof(cx), cudaMemcpyDeviceToDevice, st));
       }
       precondition(st, 2, v, tz, nullptr);
-      c3_diag_diff_kernel<<<eb, 256, 0, st>>>(N, w.cdl, w.dc, static_cast<float2 *>(a->train_diag) + k * N);
+      c3_diag_diff_kernel<<<eb, 256, 0, st>>>(N, w.cdl, w.dc, static_cast<cx *>(a->train_diag) + k * N);
     }
     c3_stats_kernel<<<1, one_cta, 0, st>>>(w.K, P, tol2, stats);
     if (a->grad_c)
-      c3_grad_kernel<<<eb, 256, 0, st>>>(N, P, nz, w.st, w.u, static_cast<const float2 *>(a->u_fwd),
-                                         static_cast<float2 *>(a->grad_c));
+      c3_grad_kernel<<<eb, 256, 0, st>>>(N, P, nz, w.st, w.u, static_cast<const cx *>(a->u_fwd),
+                                         static_cast<cx *>(a->grad_c));
   }
   if (stats) c3_flag_kernel<<<1, 1, 0, st>>>(stats, 0);
   return check_cuda(cudaGetLastError(), "tp_cn3d_march launches");

@@ -38,32 +38,32 @@ inline FftPlan make_fft_plan(int n) {
   return p;
 }
 
-__device__ __forceinline__ void fft_twiddles(float2 *tw, int n, int tid, int nth) {
+__device__ __forceinline__ void fft_twiddles(cx *tw, int n, int tid, int nth) {
   for (int t = tid; t < n; t += nth) {
     double s, c;
     sincospi(-2.0 * (double)t / (double)n, &s, &c);
-    tw[t] = make_float2((float)c, (float)s);
+    tw[t] = mkcx((rx)c, (rx)s);
   }
 }
 
 // R-point DFT in place (sign = -1 forward, +1 inverse).
 template <int R>
-__device__ __forceinline__ void dft_small(float2 (&v)[8], float sign);
+__device__ __forceinline__ void dft_small(cx (&v)[8], rx sign);
 
 template <>
-__device__ __forceinline__ void dft_small<2>(float2 (&v)[8], float) {
-  const float2 a = v[0], b = v[1];
+__device__ __forceinline__ void dft_small<2>(cx (&v)[8], rx) {
+  const cx a = v[0], b = v[1];
   v[0] = cadd(a, b);
   v[1] = csub(a, b);
 }
 
 // multiply by sign*i
-__device__ __forceinline__ float2 mul_si(float2 z, float sign) { return make_float2(-sign * z.y, sign * z.x); }
+__device__ __forceinline__ cx mul_si(cx z, rx sign) { return mkcx(-sign * z.y, sign * z.x); }
 
 template <>
-__device__ __forceinline__ void dft_small<4>(float2 (&v)[8], float sign) {
-  const float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
-  const float2 b0 = cadd(v[1], v[3]), b1 = mul_si(csub(v[1], v[3]), sign);
+__device__ __forceinline__ void dft_small<4>(cx (&v)[8], rx sign) {
+  const cx a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+  const cx b0 = cadd(v[1], v[3]), b1 = mul_si(csub(v[1], v[3]), sign);
   v[0] = cadd(a0, b0);
   v[2] = csub(a0, b0);
   v[1] = cadd(a1, b1);
@@ -71,16 +71,16 @@ __device__ __forceinline__ void dft_small<4>(float2 (&v)[8], float sign) {
 }
 
 template <>
-__device__ __forceinline__ void dft_small<8>(float2 (&v)[8], float sign) {
-  const float h = 0.70710678118654752440f;  // 1/sqrt(2)
-  float2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+__device__ __forceinline__ void dft_small<8>(cx (&v)[8], rx sign) {
+  const rx h = TP_R(0.70710678118654752440);  // 1/sqrt(2)
+  cx e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
   // 4-point DFTs of the even and odd samples
-  float2 a0 = cadd(e[0], e[2]), a1 = csub(e[0], e[2]), b0 = cadd(e[1], e[3]), b1 = mul_si(csub(e[1], e[3]), sign);
+  cx a0 = cadd(e[0], e[2]), a1 = csub(e[0], e[2]), b0 = cadd(e[1], e[3]), b1 = mul_si(csub(e[1], e[3]), sign);
   e[0] = cadd(a0, b0); e[2] = csub(a0, b0); e[1] = cadd(a1, b1); e[3] = csub(a1, b1);
   a0 = cadd(o[0], o[2]); a1 = csub(o[0], o[2]); b0 = cadd(o[1], o[3]); b1 = mul_si(csub(o[1], o[3]), sign);
   o[0] = cadd(a0, b0); o[2] = csub(a0, b0); o[1] = cadd(a1, b1); o[3] = csub(a1, b1);
   // twiddles W8^k = exp(sign * i * pi k / 4)
-  const float2 w1 = make_float2(h, sign * h), w3 = make_float2(-h, sign * h);
+  const cx w1 = mkcx(h, sign * h), w3 = mkcx(-h, sign * h);
   o[1] = cmul(o[1], w1);
   o[2] = mul_si(o[2], sign);
   o[3] = cmul(o[3], w3);
@@ -92,9 +92,9 @@ __device__ __forceinline__ void dft_small<8>(float2 (&v)[8], float sign) {
 }
 
 // 4-point DFT of (a0, a1, a2, a3) in place, X_m = sum_r a_r exp(sign 2 pi i r m / 4).
-__device__ __forceinline__ void dft4_inplace(float2 &a0, float2 &a1, float2 &a2, float2 &a3, float sign) {
-  const float2 s02 = cadd(a0, a2), d02 = csub(a0, a2), s13 = cadd(a1, a3);
-  const float2 jd13 = mul_si(csub(a1, a3), sign);
+__device__ __forceinline__ void dft4_inplace(cx &a0, cx &a1, cx &a2, cx &a3, rx sign) {
+  const cx s02 = cadd(a0, a2), d02 = csub(a0, a2), s13 = cadd(a1, a3);
+  const cx jd13 = mul_si(csub(a1, a3), sign);
   a0 = cadd(s02, s13);
   a2 = csub(s02, s13);
   a1 = cadd(d02, jd13);
@@ -105,14 +105,14 @@ __device__ __forceinline__ void dft4_inplace(float2 &a0, float2 &a1, float2 &a2,
 // X_m = sum_n2 W16^{n2 k1} W4^{n2 k2} sum_n1 x_{4 n1 + n2} W4^{n1 k1}:
 // DFT-4 over n1 for every n2, twiddles W16^{n2 k1}, DFT-4 over n2 for every
 // k1, then the 4 x 4 transpose of the output order.
-__device__ __forceinline__ void dft16(float2 (&v)[16], float sign) {
+__device__ __forceinline__ void dft16(cx (&v)[16], rx sign) {
   // cos and sin of 2 pi m / 16, m = 0..9 (the twiddle exponents n2 k1 used)
-  constexpr float kc[10] = {1.f, 0.92387953251128675613f, 0.70710678118654752440f, 0.38268343236508977173f, 0.f,
-                            -0.38268343236508977173f, -0.70710678118654752440f, -0.92387953251128675613f, -1.f,
-                            -0.92387953251128675613f};
-  constexpr float ks[10] = {0.f, 0.38268343236508977173f, 0.70710678118654752440f, 0.92387953251128675613f, 1.f,
-                            0.92387953251128675613f, 0.70710678118654752440f, 0.38268343236508977173f, 0.f,
-                            -0.38268343236508977173f};
+  constexpr rx kc[10] = {TP_R(1.0), TP_R(0.92387953251128675613), TP_R(0.70710678118654752440), TP_R(0.38268343236508977173), TP_R(0.0),
+                            -TP_R(0.38268343236508977173), -TP_R(0.70710678118654752440), -TP_R(0.92387953251128675613), -TP_R(1.0),
+                            -TP_R(0.92387953251128675613)};
+  constexpr rx ks[10] = {TP_R(0.0), TP_R(0.38268343236508977173), TP_R(0.70710678118654752440), TP_R(0.92387953251128675613), TP_R(1.0),
+                            TP_R(0.92387953251128675613), TP_R(0.70710678118654752440), TP_R(0.38268343236508977173), TP_R(0.0),
+                            -TP_R(0.38268343236508977173)};
 #pragma unroll
   for (int n2 = 0; n2 < 4; ++n2) dft4_inplace(v[n2], v[4 + n2], v[8 + n2], v[12 + n2], sign);
   // now v[4 k1 + n2] holds the inner DFT for (n2, k1)
@@ -121,7 +121,7 @@ __device__ __forceinline__ void dft16(float2 (&v)[16], float sign) {
 #pragma unroll
     for (int n2 = 1; n2 < 4; ++n2) {
       const int m = n2 * k1;
-      v[4 * k1 + n2] = cmul(v[4 * k1 + n2], make_float2(kc[m], sign * ks[m]));
+      v[4 * k1 + n2] = cmul(v[4 * k1 + n2], mkcx(kc[m], sign * ks[m]));
     }
 #pragma unroll
   for (int k1 = 0; k1 < 4; ++k1) dft4_inplace(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3], sign);
@@ -130,34 +130,34 @@ __device__ __forceinline__ void dft16(float2 (&v)[16], float sign) {
   for (int r = 0; r < 4; ++r)
 #pragma unroll
     for (int c = r + 1; c < 4; ++c) {
-      const float2 t = v[4 * r + c];
+      const cx t = v[4 * r + c];
       v[4 * r + c] = v[4 * c + r];
       v[4 * c + r] = t;
     }
 }
 
 template <>
-__device__ __forceinline__ void dft_small<3>(float2 (&v)[8], float sign) {
-  const float s3 = 0.86602540378443864676f;  // sin(2 pi / 3)
-  const float2 t = cadd(v[1], v[2]);
-  const float2 d = mul_si(csub(v[1], v[2]), sign * s3);
-  const float2 m = make_float2(v[0].x - 0.5f * t.x, v[0].y - 0.5f * t.y);
+__device__ __forceinline__ void dft_small<3>(cx (&v)[8], rx sign) {
+  const rx s3 = TP_R(0.86602540378443864676);  // sin(2 pi / 3)
+  const cx t = cadd(v[1], v[2]);
+  const cx d = mul_si(csub(v[1], v[2]), sign * s3);
+  const cx m = mkcx(v[0].x - TP_R(0.5) * t.x, v[0].y - TP_R(0.5) * t.y);
   v[0] = cadd(v[0], t);
   v[1] = cadd(m, d);
   v[2] = csub(m, d);
 }
 
 template <>
-__device__ __forceinline__ void dft_small<5>(float2 (&v)[8], float sign) {
-  const float c1 = 0.30901699437494742410f, c2 = -0.80901699437494742410f;  // cos(2pi/5), cos(4pi/5)
-  const float s1 = 0.95105651629515357212f, s2 = 0.58778525229247312917f;   // sin(2pi/5), sin(4pi/5)
-  const float2 a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
-  const float2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
-  const float2 x0 = v[0];
-  const float2 m1 = make_float2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
-  const float2 m2 = make_float2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
-  const float2 n1 = mul_si(make_float2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y), sign);
-  const float2 n2 = mul_si(make_float2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y), sign);
+__device__ __forceinline__ void dft_small<5>(cx (&v)[8], rx sign) {
+  const rx c1 = TP_R(0.30901699437494742410), c2 = -TP_R(0.80901699437494742410);  // cos(2pi/5), cos(4pi/5)
+  const rx s1 = TP_R(0.95105651629515357212), s2 = TP_R(0.58778525229247312917);   // sin(2pi/5), sin(4pi/5)
+  const cx a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+  const cx a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+  const cx x0 = v[0];
+  const cx m1 = mkcx(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
+  const cx m2 = mkcx(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
+  const cx n1 = mul_si(mkcx(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y), sign);
+  const cx n2 = mul_si(mkcx(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y), sign);
   v[0] = cadd(x0, cadd(a1, a2));
   v[1] = cadd(m1, n1);
   v[4] = csub(m1, n1);
@@ -166,22 +166,22 @@ __device__ __forceinline__ void dft_small<5>(float2 (&v)[8], float sign) {
 }
 
 template <int R>
-__device__ __forceinline__ void fft_pass(const float2 *a, float2 *b, int n, int Ns, const float2 *tw, float sign,
+__device__ __forceinline__ void fft_pass(const cx *a, cx *b, int n, int Ns, const cx *tw, rx sign,
                                          int nb, int tid, int nth) {
   const int T = n / R;
   const int step = n / (Ns * R);
   for (int w = tid; w < nb * T; w += nth) {
     const int bi = w / T, j = w - bi * T;
-    const float2 *src = a + bi * n;
-    float2 *dst = b + bi * n;
+    const cx *src = a + bi * n;
+    cx *dst = b + bi * n;
     const int k = j % Ns;
-    float2 v[8];
+    cx v[8];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = src[j + r * T];
 #pragma unroll
     for (int r = 1; r < R; ++r) {
-      const float2 t = tw[(r * k * step) % n];
-      v[r] = cmul(v[r], make_float2(t.x, sign < 0 ? t.y : -t.y));
+      const cx t = tw[(r * k * step) % n];
+      v[r] = cmul(v[r], mkcx(t.x, sign < 0 ? t.y : -t.y));
     }
     dft_small<R>(v, sign);
     const int idx = (j / Ns) * Ns * R + k;
@@ -195,22 +195,22 @@ __device__ __forceinline__ void fft_pass(const float2 *a, float2 *b, int n, int 
 // time, so that every index division and modulo is by a constant.  Used by
 // the 3D preconditioner for the common transverse sizes.
 template <int N, int Ns, int R>
-__device__ __forceinline__ void fft_pass_fixed(const float2 *a, float2 *b, const float2 *tw, float sign, int nb, int tid,
+__device__ __forceinline__ void fft_pass_fixed(const cx *a, cx *b, const cx *tw, rx sign, int nb, int tid,
                                                int nth) {
   constexpr int T = N / R;
   constexpr int step = N / (Ns * R);
   for (int w = tid; w < nb * T; w += nth) {
     const int bi = w / T, j = w - bi * T;
-    const float2 *src = a + bi * N;
-    float2 *dst = b + bi * N;
+    const cx *src = a + bi * N;
+    cx *dst = b + bi * N;
     const int k = j % Ns;
-    float2 v[R > 8 ? 16 : 8];
+    cx v[R > 8 ? 16 : 8];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = src[j + r * T];
 #pragma unroll
     for (int r = 1; r < R; ++r) {
-      const float2 t = tw[(r * k * step) % N];
-      v[r] = cmul(v[r], make_float2(t.x, sign < 0 ? t.y : -t.y));
+      const cx t = tw[(r * k * step) % N];
+      v[r] = cmul(v[r], mkcx(t.x, sign < 0 ? t.y : -t.y));
     }
     if constexpr (R == 16) dft16(v, sign);
     else dft_small<R>(v, sign);
@@ -221,7 +221,7 @@ __device__ __forceinline__ void fft_pass_fixed(const float2 *a, float2 *b, const
 }
 
 template <int N, int Ns, int R, int... Rest>
-__device__ __forceinline__ float2 *fft_run_fixed(float2 *a, float2 *b, const float2 *tw, float sign, int nb, int tid,
+__device__ __forceinline__ cx *fft_run_fixed(cx *a, cx *b, const cx *tw, rx sign, int nb, int tid,
                                                  int nth) {
   fft_pass_fixed<N, Ns, R>(a, b, tw, sign, nb, tid, nth);
   __syncthreads();
@@ -244,23 +244,23 @@ struct FftPad {
 __device__ __forceinline__ int fft_pad(int i) { return i + (i >> 3); }
 
 template <int N, int Ns, int R>
-__device__ __forceinline__ void fft_pass_padded(const float2 *a, float2 *b, const float2 *tw, float sign, int nb, int tid,
+__device__ __forceinline__ void fft_pass_padded(const cx *a, cx *b, const cx *tw, rx sign, int nb, int tid,
                                                 int nth) {
   constexpr int T = N / R;
   constexpr int step = N / (Ns * R);
   constexpr int S = FftPad<N>::S;
   for (int w = tid; w < nb * T; w += nth) {
     const int bi = w / T, j = w - bi * T;
-    const float2 *src = a + bi * S;
-    float2 *dst = b + bi * S;
+    const cx *src = a + bi * S;
+    cx *dst = b + bi * S;
     const int k = j % Ns;
-    float2 v[R > 8 ? 16 : 8];
+    cx v[R > 8 ? 16 : 8];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = src[fft_pad(j + r * T)];
 #pragma unroll
     for (int r = 1; r < R; ++r) {
-      const float2 t = tw[(r * k * step) % N];
-      v[r] = cmul(v[r], make_float2(t.x, sign < 0 ? t.y : -t.y));
+      const cx t = tw[(r * k * step) % N];
+      v[r] = cmul(v[r], mkcx(t.x, sign < 0 ? t.y : -t.y));
     }
     if constexpr (R == 16) dft16(v, sign);
     else dft_small<R>(v, sign);
@@ -271,7 +271,7 @@ __device__ __forceinline__ void fft_pass_padded(const float2 *a, float2 *b, cons
 }
 
 template <int N, int Ns, int R, int... Rest>
-__device__ __forceinline__ float2 *fft_run_padded(float2 *a, float2 *b, const float2 *tw, float sign, int nb, int tid,
+__device__ __forceinline__ cx *fft_run_padded(cx *a, cx *b, const cx *tw, rx sign, int nb, int tid,
                                                   int nth) {
   fft_pass_padded<N, Ns, R>(a, b, tw, sign, nb, tid, nth);
   __syncthreads();
@@ -291,9 +291,9 @@ __host__ __device__ constexpr bool fft_fixed_size(int n) {
 }
 
 template <int N>
-__device__ __forceinline__ float2 *fft_block_fixed(float2 *a, float2 *b, const float2 *tw, bool inverse, int nb,
+__device__ __forceinline__ cx *fft_block_fixed(cx *a, cx *b, const cx *tw, bool inverse, int nb,
                                                    int tid, int nth) {
-  const float sign = inverse ? 1.f : -1.f;
+  const rx sign = inverse ? TP_R(1.0) : -TP_R(1.0);
   if constexpr (N == 32) return fft_run_fixed<32, 1, 8, 4>(a, b, tw, sign, nb, tid, nth);
   else if constexpr (N == 64) return fft_run_fixed<64, 1, 8, 8>(a, b, tw, sign, nb, tid, nth);
   else if constexpr (N == 128) return fft_run_fixed<128, 1, 8, 16>(a, b, tw, sign, nb, tid, nth);
@@ -305,9 +305,9 @@ __device__ __forceinline__ float2 *fft_block_fixed(float2 *a, float2 *b, const f
 
 // The fixed-size transforms in the padded layout (FftPad).
 template <int N>
-__device__ __forceinline__ float2 *fft_block_padded(float2 *a, float2 *b, const float2 *tw, bool inverse, int nb,
+__device__ __forceinline__ cx *fft_block_padded(cx *a, cx *b, const cx *tw, bool inverse, int nb,
                                                     int tid, int nth) {
-  const float sign = inverse ? 1.f : -1.f;
+  const rx sign = inverse ? TP_R(1.0) : -TP_R(1.0);
   if constexpr (N == 32) return fft_run_padded<32, 1, 8, 4>(a, b, tw, sign, nb, tid, nth);
   else if constexpr (N == 64) return fft_run_padded<64, 1, 8, 8>(a, b, tw, sign, nb, tid, nth);
   else if constexpr (N == 128) return fft_run_padded<128, 1, 8, 16>(a, b, tw, sign, nb, tid, nth);
@@ -319,9 +319,9 @@ __device__ __forceinline__ float2 *fft_block_padded(float2 *a, float2 *b, const 
 // nb transforms of length pl.n stored back to back in `a` (scratch `b` of
 // the same size).  Returns the buffer holding the result (a or b).  Ends
 // with __syncthreads().
-__device__ __forceinline__ float2 *fft_block(float2 *a, float2 *b, const FftPlan &pl, const float2 *tw, bool inverse,
+__device__ __forceinline__ cx *fft_block(cx *a, cx *b, const FftPlan &pl, const cx *tw, bool inverse,
                                              int nb, int tid, int nth) {
-  const float sign = inverse ? 1.f : -1.f;
+  const rx sign = inverse ? TP_R(1.0) : -TP_R(1.0);
   int Ns = 1;
   for (int ps = 0; ps < pl.npass; ++ps) {
     const int R = pl.radix[ps];
@@ -333,7 +333,7 @@ __device__ __forceinline__ float2 *fft_block(float2 *a, float2 *b, const FftPlan
       default: fft_pass<5>(a, b, pl.n, Ns, tw, sign, nb, tid, nth); break;
     }
     __syncthreads();
-    float2 *t = a;
+    cx *t = a;
     a = b;
     b = t;
     Ns *= R;
@@ -345,7 +345,7 @@ __device__ __forceinline__ float2 *fft_block(float2 *a, float2 *b, const FftPlan
 // plan in the padded layout when N > 0, else the runtime plan `pl`
 // (unpadded).  Whole-CTA call.
 template <int N>
-__device__ __forceinline__ float2 *fft_rows(float2 *a, float2 *b, const FftPlan &pl, const float2 *tw, bool inverse,
+__device__ __forceinline__ cx *fft_rows(cx *a, cx *b, const FftPlan &pl, const cx *tw, bool inverse,
                                             int rows) {
   if constexpr (N > 0) return fft_block_padded<N>(a, b, tw, inverse, rows, threadIdx.x, blockDim.x);
   else return fft_block(a, b, pl, tw, inverse, rows, threadIdx.x, blockDim.x);
@@ -364,7 +364,7 @@ __host__ __device__ constexpr int fstride(int n) {
   else return n;
 }
 
-__device__ __forceinline__ void load_twiddles(float2 *tw, const float2 *__restrict__ twg, int n) {
+__device__ __forceinline__ void load_twiddles(cx *tw, const cx *__restrict__ twg, int n) {
   for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twg[t];
 }
 
@@ -382,12 +382,12 @@ __device__ __forceinline__ void load_twiddles(float2 *tw, const float2 *__restri
 // it without bank conflicts.
 
 // 12-point DFT as 4 x 3 (n = 3 n1 + n2, k = k1 + 4 k2), natural order in and out.
-__device__ __forceinline__ void dft12(float2 (&v)[16], float sign) {
-  const float s3 = 0.86602540378443864676f;  // sin(pi / 3)
-  float2 y[12];
+__device__ __forceinline__ void dft12(cx (&v)[16], rx sign) {
+  const rx s3 = TP_R(0.86602540378443864676);  // sin(pi / 3)
+  cx y[12];
 #pragma unroll
   for (int n2 = 0; n2 < 3; ++n2) {
-    float2 a0 = v[n2], a1 = v[3 + n2], a2 = v[6 + n2], a3 = v[9 + n2];
+    cx a0 = v[n2], a1 = v[3 + n2], a2 = v[6 + n2], a3 = v[9 + n2];
     dft4_inplace(a0, a1, a2, a3, sign);
     y[4 * n2] = a0;
     y[4 * n2 + 1] = a1;
@@ -395,8 +395,8 @@ __device__ __forceinline__ void dft12(float2 (&v)[16], float sign) {
     y[4 * n2 + 3] = a3;
   }
   // W12^m = exp(sign 2 pi i m / 12) for m = n2 k1 in {1, 2, 3, 2, 4, 6}
-  const float2 w1 = make_float2(s3, sign * 0.5f), w2 = make_float2(0.5f, sign * s3), w3 = make_float2(0.f, sign);
-  const float2 w4 = make_float2(-0.5f, sign * s3), w6 = make_float2(-1.f, 0.f);
+  const cx w1 = mkcx(s3, sign * TP_R(0.5)), w2 = mkcx(TP_R(0.5), sign * s3), w3 = mkcx(TP_R(0.0), sign);
+  const cx w4 = mkcx(-TP_R(0.5), sign * s3), w6 = mkcx(-TP_R(1.0), TP_R(0.0));
   y[5] = cmul(y[5], w1);
   y[6] = cmul(y[6], w2);
   y[7] = cmul(y[7], w3);
@@ -405,10 +405,10 @@ __device__ __forceinline__ void dft12(float2 (&v)[16], float sign) {
   y[11] = cmul(y[11], w6);
 #pragma unroll
   for (int k1 = 0; k1 < 4; ++k1) {
-    const float2 a = y[k1], b = y[4 + k1], c = y[8 + k1];
-    const float2 t = cadd(b, c);
-    const float2 d = mul_si(csub(b, c), sign * s3);
-    const float2 m = make_float2(a.x - 0.5f * t.x, a.y - 0.5f * t.y);
+    const cx a = y[k1], b = y[4 + k1], c = y[8 + k1];
+    const cx t = cadd(b, c);
+    const cx d = mul_si(csub(b, c), sign * s3);
+    const cx m = mkcx(a.x - TP_R(0.5) * t.x, a.y - TP_R(0.5) * t.y);
     v[k1] = cadd(a, t);
     v[k1 + 4] = cadd(m, d);
     v[k1 + 8] = csub(m, d);
@@ -417,14 +417,14 @@ __device__ __forceinline__ void dft12(float2 (&v)[16], float sign) {
 
 // R-point DFT (R = 4, 8, 12, 16) of v[0..R) in registers, natural order in and out.
 template <int R>
-__device__ __forceinline__ void dft_reg(float2 (&v)[16], float sign) {
+__device__ __forceinline__ void dft_reg(cx (&v)[16], rx sign) {
   static_assert(R == 4 || R == 8 || R == 12 || R == 16, "dft_reg: unsupported length");
   if constexpr (R == 16) {
     dft16(v, sign);
   } else if constexpr (R == 12) {
     dft12(v, sign);
   } else if constexpr (R == 8) {
-    float2 w[8];
+    cx w[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) w[j] = v[j];
     dft_small<8>(w, sign);

@@ -88,6 +88,13 @@ using cx = float2;
 using rx = float;
 using cx2 = float4;
 #endif
+// A floating-point literal of the real type (TP_R(0.5) is 0.5f, or 0.5 in
+// the complex128 check build).
+#ifdef TP_C128_CHECK
+#define TP_R(x) x
+#else
+#define TP_R(x) x##f
+#endif
 __host__ __device__ __forceinline__ cx mkcx(rx x, rx y) {
   cx v;
   v.x = x;
@@ -201,6 +208,14 @@ __device__ __forceinline__ void bulk_wait() { asm volatile("cp.async.bulk.wait_g
 // cp_async_wait_all).  Both addresses 8-byte aligned.
 __device__ __forceinline__ void cp_async8(void *dst, const void *src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+// Asynchronous global -> shared copy of one cx (8 or 16 bytes, aligned to its size).
+__device__ __forceinline__ void cp_async_cx(cx *dst, const cx *src) {
+#ifdef TP_C128_CHECK
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+#else
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+#endif
 }
 // 16-byte global -> shared asynchronous copy (L2 only).  Both addresses
 // 16-byte aligned.
