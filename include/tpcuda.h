@@ -10,6 +10,12 @@
  * except where stated, and none allocates device memory: the caller passes
  * workspaces sized by the *_bytes() queries.
  *
+ * libtpcuda_c128.so, the complex128 check build, exports the tp_cn2d_* and
+ * tp_cn3d_* entry points with the same signatures and every complex buffer
+ * (state, operator diagonals, stores, sources, workspaces' vectors)
+ * complex128; its *_bytes() queries size for that.  Its 3D march has no
+ * learned correction (precond = 2 returns TP_ERR_UNSUPPORTED).
+ *
  * Step equation (reference iterative_lu.py:185-193, operator_matrices.py:36-72):
  *   (A - C_j) u_j = (B + C_j) u_{j-1} + b_j,  A = I - K, B = I + K,
  *   K = scaled tridiagonal second difference with boundary-row edits,

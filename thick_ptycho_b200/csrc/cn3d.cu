@@ -646,7 +646,11 @@ __global__ void __launch_bounds__(256, R1 * R2 == 256 ? 3 : 4) c3_cols4_kernel(c
       for (int k2 = 0; k2 < R2; ++k2) {
         const rx bb = bcos[k1 + R1 * k2];
         const rx dr = TP_R(1.0) - ax - mx * bb, di = -(ay + my * bb);
+#ifdef TP_C128_CHECK
         const rx m = sc / (dr * dr + di * di);
+#else
+        const rx m = __fdividef(sc, dr * dr + di * di);  // a preconditioner value: the fast quotient
+#endif
         x[k2] = cmul(x[k2], mkcx(dr * m, -di * m));
       }
     }
