@@ -55,8 +55,16 @@ enum { kStatIters = 0, kStatSolves = 1, kStatFailed = 2, kStatMaxIters = 3 };
 // one CUDA graph with device-side loops) serves every step: t is the current
 // step (1..L; 0 before the first), s its slice, it the BiCGStab iterations
 // of this step, pending = 1 while a probe of the step is still iterating.
+// Learned form: cheap = 1 when every solve of the previous step took one
+// iteration (last_max, written by the step's statistics kernel); the first
+// iteration of such a step applies the learned correction to the first of
+// its two preconditioner applications only.  BiCGStab's recursions stay
+// consistent with any pair of preconditioned vectors (x += alpha y + omega z,
+// r = s - omega A z), and a solve converged in one iteration saves a filter
+// pass; solves that need more iterations keep the correction in both.
 struct __align__(16) C3State {
   int t, s, it, pending;
+  int cheap, last_max, pad0, pad1;
 };
 
 // Start step t = state.t + 1.  In a graph, `outer` is the condition of the
@@ -69,6 +77,7 @@ __global__ void c3_advance_kernel(C3State *st, int L, int backward, int use_cond
   st->s = backward ? (L + 1 - t) : t;
   st->it = 0;
   st->pending = 1;
+  st->cheap = (t > 1 && st->last_max <= 1) ? 1 : 0;
   if (use_cond) {
     cudaGraphSetConditional(outer, t < L ? 1u : 0u);
     cudaGraphSetConditional(inner, 1u);
@@ -461,11 +470,14 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_cols_kernel(const FftPlan p
   }
 }
 
-// Inverse row FFTs of hat into out (the 1/(nf nb) scale is in the symbol).
+// Inverse row FFTs of hat into out (the 1/(nf nb) scale is in the symbol);
+// into out_first instead (when given) in the first iteration of a step whose
+// state says cheap (the learned form's plain second application).
 template <int NF>
 __global__ void __launch_bounds__(k3Threads) c3_prec_rows_inv_kernel(const FftPlan pl, const C3Params q,
                                                                      const cx *hat, cx *out, const Krylov *K,
-                                                                     int rpc, const cx *twg) {
+                                                                     int rpc, const cx *twg, cx *out_first,
+                                                                     const C3State *st) {
   extern __shared__ __align__(16) cx fsm[];
   const int n = NF > 0 ? NF : q.nf, pr = blockIdx.y;
   if (K != nullptr && K[pr].done) return;
@@ -478,7 +490,8 @@ __global__ void __launch_bounds__(k3Threads) c3_prec_rows_inv_kernel(const FftPl
   cp_async_wait_all();
   __syncthreads();
   const cx *res = fft_rows<NF>(a, b, pl, tw, true, rpc);
-  for (int e = threadIdx.x; e < tot; e += blockDim.x) out[off + e] = res[slot(e)];
+  cx *dst = (out_first != nullptr && st->it == 0 && st->cheap) ? out_first : out;
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) dst[off + e] = res[slot(e)];
 }
 
 // ab[f] = 2 cos(2 pi f / nf) - 2 (f < nf), ab[nf + b] = 2 cos(2 pi b / nb) - 2
@@ -672,10 +685,11 @@ __global__ void __launch_bounds__(256, R1 * R2 == 256 ? 3 : 4) c3_cols4_kernel(c
 }
 
 // Inverse row transforms of hat into out (the 1/(nf nb) scale is in the
-// symbol).  Grid (nb / RPC, P).
+// symbol; out_first as in c3_prec_rows_inv_kernel).  Grid (nb / RPC, P).
 template <int R1, int R2>
 __global__ void __launch_bounds__(256) c3_rows4_inv_kernel(const C3Params q, const cx *hat, cx *out,
-                                                           const Krylov *K, const cx *__restrict__ twg) {
+                                                           const Krylov *K, const cx *__restrict__ twg,
+                                                           cx *out_first, const C3State *st) {
   constexpr int N = R1 * R2, RPC = 256 / R1, S = R1 * (R2 + 1);
   __shared__ cx buf[RPC * S];
   __shared__ cx tw[R1 * (R2 + 1)];
@@ -683,6 +697,7 @@ __global__ void __launch_bounds__(256) c3_rows4_inv_kernel(const C3Params q, con
   if (K != nullptr && K[pr].done) return;
   for (int e = threadIdx.x; e < R1 * (R2 + 1); e += 256) tw[e] = twg[e];
   const size_t off = (size_t)pr * q.N + (size_t)blockIdx.x * RPC * N;
+  cx *dst = (out_first != nullptr && st->it == 0 && st->cheap) ? out_first : out;
   __syncthreads();
   {  // inverse stage C: (row, k1)
     const int row = threadIdx.x / R1, k1 = threadIdx.x % R1;
@@ -702,7 +717,7 @@ __global__ void __launch_bounds__(256) c3_rows4_inv_kernel(const C3Params q, con
     for (int k1 = 0; k1 < R1; ++k1) x[k1] = buf[row * S + k1 * (R2 + 1) + n2];
     dft_reg<R1>(x, TP_R(1.0));
 #pragma unroll
-    for (int n1 = 0; n1 < R1; ++n1) out[off + row * N + R2 * n1 + n2] = x[n1];
+    for (int n1 = 0; n1 < R1; ++n1) dst[off + row * N + R2 * n1 + n2] = x[n1];
   }
 }
 
@@ -847,9 +862,13 @@ __global__ void __launch_bounds__(k3Threads, 4) c3_finish_kernel(const C3Params 
 
 // After a step (one CTA loops over the probes): accumulate the statistics
 // (when `stats` is given) and clear the per-probe sums of the next step.
-__global__ void c3_stats_kernel(Krylov *K, int P, double tol2, int *stats) {
+__global__ void c3_stats_kernel(Krylov *K, int P, double tol2, int *stats, C3State *st) {
+  __shared__ int mx;
+  if (threadIdx.x == 0) mx = 0;
+  __syncthreads();
   for (int pr = threadIdx.x; pr < P; pr += blockDim.x) {
     Krylov &k = K[pr];
+    atomicMax(&mx, k.iters);
     if (stats != nullptr) {
       atomicAdd(&stats[kStatIters], k.iters);
       atomicAdd(&stats[kStatSolves], 1);
@@ -860,6 +879,8 @@ __global__ void c3_stats_kernel(Krylov *K, int P, double tol2, int *stats) {
     k.res2 = 0.0;
     k.bnorm2 = 0.0;
   }
+  __syncthreads();
+  if (threadIdx.x == 0) st->last_max = mx;
 }
 
 // Store the state (P, N) into slice `t` of u_store (P, nz, N) and/or exit.
@@ -926,8 +947,10 @@ __host__ __device__ constexpr int filter_rb(int nf) { return 2 * (256 / filter_c
 __global__ void __launch_bounds__(k3Threads, 2) c3_filter_kernel(const C3Params q, const C3State *st, int chunk,
                                                                  const cx *__restrict__ Fall,
                                                                  const cx *__restrict__ z, cx *__restrict__ out,
-                                                                 const Krylov *K) {
+                                                                 const Krylov *K, int second) {
   extern __shared__ __align__(16) cx ztile[];  // [kFilterProbes][rb + 4][cw + 4]
+  // the second application of a cheap first iteration stays plain (C3State)
+  if (second && st->it == 0 && st->cheap) return;
   const int nf = q.nf, nb = q.nb;
   const int cw = filter_cw(nf), rb = filter_rb(nf), W = cw + 4, H = rb + 4;
   const int c0 = blockIdx.x * cw, b0 = blockIdx.y * rb, p0 = blockIdx.z * kFilterProbes;
@@ -1117,7 +1140,8 @@ using RowsKernel = void (*)(const FftPlan, const C3Params, int, const cx *, cx *
                            cx *, const Krylov *, int, int, const cx *, const cx *, const C3State *);
 using ColsKernel = void (*)(const FftPlan, const C3Params, cx *, const Krylov *, int, const cx *,
                            const cx *);
-using InvKernel = void (*)(const FftPlan, const C3Params, const cx *, cx *, const Krylov *, int, const cx *);
+using InvKernel = void (*)(const FftPlan, const C3Params, const cx *, cx *, const Krylov *, int, const cx *, cx *,
+                          const C3State *);
 struct PrecKernels {
   RowsKernel rows;
   ColsKernel cols;
@@ -1149,7 +1173,7 @@ static PrecKernels prec_kernels(int nf, int nb) {
 using Rows4Kernel = void (*)(const C3Params, int, const cx *, cx *, const cx *, cx *, cx *,
                             const Krylov *, const cx *, const cx *, const C3State *);
 using Cols4Kernel = void (*)(const C3Params, cx *, const Krylov *, const cx *, const rx *);
-using Inv4Kernel = void (*)(const C3Params, const cx *, cx *, const Krylov *, const cx *);
+using Inv4Kernel = void (*)(const C3Params, const cx *, cx *, const Krylov *, const cx *, cx *, const C3State *);
 struct Prec4Kernels {
   Rows4Kernel rows = nullptr;
   Cols4Kernel cols = nullptr;
@@ -1413,18 +1437,19 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
 
   // ---- launch sequences (recorded into a graph, or issued step by step)
   // M0^{-1} in -> out (mode 0/1/2 input of the row kernel; Kp NULL = all probes)
-  auto precondition = [&](cudaStream_t s, int mode, const cx *rin, cx *out, const Krylov *Kp) {
+  auto precondition = [&](cudaStream_t s, int mode, const cx *rin, cx *out, const Krylov *Kp,
+                          cx *out_first = nullptr) {
     if (four) {
       p4.rows<<<dim3(nb / rpc4, P), 256, 0, s>>>(q, mode, rin, w.p, w.v, w.s, w.hat, Kp, w.tw4, w.r0, w.st);
       p4.cols<<<dim3(nf / rpc4, P), 256, 0, s>>>(q, w.hat, Kp, w.tw4, w.ab);
-      p4.inv<<<dim3(nb / rpc4, P), 256, 0, s>>>(q, w.hat, out, Kp, w.tw4);
+      p4.inv<<<dim3(nb / rpc4, P), 256, 0, s>>>(q, w.hat, out, Kp, w.tw4, out_first, w.st);
       return;
     }
     pk.rows<<<dim3(nb / rows_cta, P), k3Threads, use_fft ? smem_rows : 0, s>>>(
         pf, q, mode, rin, w.p, w.v, w.s, use_fft ? w.hat : out, Kp, rows_cta, use_fft, w.twf, w.r0, w.st);
     if (use_fft) {
       pk.cols<<<dim3(nf / cpc, P), k3Threads, smem_cols, s>>>(pb, q, w.hat, Kp, cpc, w.twb, w.sym);
-      pk.inv<<<dim3(nb / rpc, P), k3Threads, smem_rows, s>>>(pf, q, w.hat, out, Kp, rpc, w.twf);
+      pk.inv<<<dim3(nb / rpc, P), k3Threads, smem_rows, s>>>(pf, q, w.hat, out, Kp, rpc, w.twf, out_first, w.st);
     }
   };
   auto prologue = [&](cudaStream_t s) -> int {
@@ -1483,13 +1508,13 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     // p = r + beta (p - omega v); y = Prec(p); v = M y
     precondition(s, 0, w.r, learned ? lw.zt : w.y, w.K);
 #ifndef TP_C128_CHECK
-    if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.y, w.K);
+    if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.y, w.K, 0);
 #endif
     c3_matvec_kernel<0><<<sg_mv0, k3Threads, 0, s>>>(q, w.cdl, w.y, w.v, w.r0, w.s, w.K);
     // s = r - alpha v; z = Prec(s); t = M z
-    precondition(s, 1, w.r, learned ? lw.zt : w.z, w.K);
+    precondition(s, 1, w.r, learned ? lw.zt : w.z, w.K, learned ? w.z : nullptr);
 #ifndef TP_C128_CHECK
-    if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.z, w.K);
+    if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.z, w.K, 1);
 #endif
     c3_matvec_kernel<1><<<sg_mv1, k3Threads, 0, s>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K);
     c3_update_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.x, w.r, w.r0, w.y, w.z, w.s, w.t, w.K, w.st);
@@ -1498,7 +1523,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   // step tail: u += x (true residual, store), statistics, gradient
   auto step_tail = [&](cudaStream_t s) {
     c3_finish_kernel<<<sg_fin, k3Threads, 0, s>>>(q, w.st, w.cdl, w.x, w.r0, w.u, w.K, ust, flip ? 1 : 0, exit_out);
-    c3_stats_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, stats);
+    c3_stats_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, stats, w.st);
     if (a->grad_c)
       c3_grad_kernel<<<eb, 256, 0, s>>>(N, P, nz, w.st, w.u, static_cast<const cx *>(a->u_fwd),
                                         static_cast<cx *>(a->grad_c));
@@ -1636,7 +1661,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
       precondition(st, 2, v, tz, nullptr);
       c3_diag_diff_kernel<<<eb, 256, 0, st>>>(N, w.cdl, w.dc, static_cast<cx *>(a->train_diag) + k * N);
     }
-    c3_stats_kernel<<<1, one_cta, 0, st>>>(w.K, P, tol2, stats);
+    c3_stats_kernel<<<1, one_cta, 0, st>>>(w.K, P, tol2, stats, w.st);
     if (a->grad_c)
       c3_grad_kernel<<<eb, 256, 0, st>>>(N, P, nz, w.st, w.u, static_cast<const cx *>(a->u_fwd),
                                          static_cast<cx *>(a->grad_c));
