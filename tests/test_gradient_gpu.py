@@ -4,8 +4,11 @@ reference's own (inexact) least-squares gradient.
 
 Tolerances: checkpointed vs full-store gradients ≤ 1e-5 relative L2 (same
 arithmetic, only the fp32 accumulation order differs); GPU vs oracle ≤ 1e-5
-relative L2; finite differences (h = 1e-7, complex128) within 1e-3 relative
-per sampled voxel (1e-4 at the full reconstruction-gradient geometry); reference gradient: cosine similarity ≥ 0.98 (its adjoint
+relative L2 (at the full reconstruction-gradient geometry on well-conditioned
+data, and stage by stage at the reconstruction's start, where the loss is
+ill-conditioned in the exit waves); finite differences (h = 1e-7, complex128)
+within 1e-3 relative per sampled voxel (1e-4 plus 1e-5 of the largest entry at
+the full reconstruction-gradient geometry); reference gradient: cosine similarity ≥ 0.98 (its adjoint
 is not the exact transpose of its forward: it pairs (A − C_s)ᴴ with
 (B + C_s)ᴴ of the same slice, iterative_lu.py:114-128, and its grad_A drops
 C₀u₀, forward_model.py:151-153; measured 0.992).
@@ -90,39 +93,94 @@ def test_gradient_matches_oracle_and_autograd():
     assert rel(field.grad.cpu().numpy(), gref) < 1e-5
 
 
-def test_gradient_matches_central_differences_config3_geometry():
-    """The reconstruction-gradient geometry at full size: N = 1024, Nz = 512
-    nodes, stride 4, ground truth of 300 seeded blobs, start δn = 0, √Nz
-    checkpointing, with 8 of its 256 probes; central differences (h = 1e-7,
-    complex128) of the oracle's amplitude loss at 64 random voxels, real and
-    imaginary parts.  A perturbed node changes only the two slices that read
-    it, so each difference re-marches the oracle from the stored state before
-    them (``NodePerturbation``).  Tolerance: 1e-4 relative per voxel, with a
-    floor of 1e-3 of the largest gradient entry (the differences themselves
-    agree with the oracle's exact adjoint gradient to 2e-6)."""
-    N, nz, P = 1024, 512, 8
+def _config3(P=8):
+    """The reconstruction-gradient geometry at full size (N = 1024, Nz = 512
+    nodes, stride 4, 300 seeded blobs) with P of its 256 probes."""
+    N, nz = 1024, 512
     geo = SimulationGeometry.grid_2d(N, nz, 0.5, P, 4)
-    truth = 1 - blob_field_2d(N, nz, 300, 7)
+    blobs = 1 - blob_field_2d(N, nz, 300, 7)
     probes = gaussian_probes_2d(N, geo.centres, 8.0)
     co = po.bc_coefficients(geo.k, 1.0, 1.0, bc_type="impedance")
     A, B = po.step_matrices_1d(N, co, "impedance", 1.0)
-    amp = np.abs(np.fft.fft(po.NodePerturbation(A, B, truth, geo.k, 1.0, probes).exits(), axis=-1))
-    n0 = np.ones((N, nz), dtype=complex)  # starting guess δn = 0
+    return geo, blobs, probes, A, B
+
+
+def _oracle_gradient(A, B, n, k, probes, src_of):
+    """The oracle's complex128 exact-adjoint gradient with the exit-wave source src_of(p, u)."""
+    C = po.object_contribution(n, k, 1.0)
+    gc = np.zeros((A.shape[0], n.shape[1] - 1), complex)
+    for p in range(probes.shape[0]):
+        u = po.march(A, B, C, probes[p])
+        src = np.zeros_like(gc)
+        src[:, -1] = src_of(p, u)
+        gc += po.grad_c_from_adjoint(u, po.exact_adjoint(A, B, C, src))
+    return po.chain_grad_to_n(gc, k, 1.0)
+
+
+def test_gradient_matches_central_differences_config3_geometry():
+    """The config-3 geometry at full depth (√Nz checkpointing, 8 probes) at the
+    300-blob index field, with data 1.25 times that field's own far-field
+    amplitude (the residual is −|U|/4 at every frequency).  (1) The GPU
+    gradient against the oracle's complex128 exact-adjoint gradient over the
+    whole field: ≤ 1e-5 relative L2.  (2) Central differences (h = 1e-7,
+    complex128) of the oracle's amplitude loss at 64 random voxels, real and
+    imaginary parts, against the GPU gradient: 1e-4 relative per voxel plus
+    1e-5 of the largest entry (a near-zero voxel carries the complex64
+    rounding of the whole field, a few 1e-6 of the largest entry when the
+    field is within 1e-5; the differences themselves agree with the exact
+    gradient to 1e-8 of the largest entry).  A perturbed node changes only the two
+    slices that read it, so each difference re-marches the oracle from the
+    stored state before them (``NodePerturbation``)."""
+    geo, n, probes, A, B = _config3()
+    base = po.NodePerturbation(A, B, n, geo.k, 1.0, probes)
+    amp = 1.25 * np.abs(np.fft.fft(base.exits(), axis=-1))
     pg = PWEGradient2D(geo, checkpoint="sqrt")
-    _, g = pg.loss_and_grad(n0, probes, amp)
+    _, g = pg.loss_and_grad(n, probes, amp)
     g = g.cpu().numpy()
-    base = po.NodePerturbation(A, B, n0, geo.k, 1.0, probes)
+    gref = _oracle_gradient(A, B, n, geo.k, probes,
+                            lambda p, u: po.amplitude_loss_and_grad(u[:, -1][None], amp[p][None])[1][0])
+    assert rel(g, gref) < 1e-5, rel(g, gref)
     rng = np.random.default_rng(0)
     h = 1e-7
     scale = np.abs(g).max()
     for _ in range(64):
-        x, t = int(rng.integers(0, N)), int(rng.integers(0, nz))
+        x, t = int(rng.integers(0, g.shape[0])), int(rng.integers(0, g.shape[1]))
         for d, part in ((1.0, 0), (1j, 1)):
             lp = po.amplitude_loss_and_grad(base.exits(x, t, h * d), amp)[0]
             lm = po.amplitude_loss_and_grad(base.exits(x, t, -h * d), amp)[0]
             fd = (lp - lm) / (2 * h)
             an = g[x, t].real if part == 0 else g[x, t].imag
-            assert abs(fd - an) <= 1e-4 * max(abs(fd), 1e-3 * scale), (x, t, part, fd, an)
+            assert abs(fd - an) <= 1e-4 * abs(fd) + 1e-5 * scale, (x, t, part, fd, an)
+
+
+def test_gradient_stages_at_the_reconstruction_start():
+    """The reconstruction's first gradient on the config-3 geometry: δn = 0,
+    amplitudes of the 300-blob field.  Where the model's and the data's
+    amplitudes cross, |U| / ||U| − a| reaches 1e4, so the amplitude-loss
+    gradient is ill-conditioned with respect to the exit waves: rounding the
+    exact exit waves to complex64 moves the complex128 gradient by 2.8e-5, an
+    exit error of 3.6e-7 (the complex64 march's) by ~1e-4, and end to end the
+    GPU gradient is 2.2e-4 from the complex128 one.  The stages are checked
+    where that sensitivity does not enter: the exit waves against the oracle
+    (≤ 1e-5), the loss (≤ 1e-5), and the exact adjoint with the gradient
+    contraction from the GPU's own exit-wave source against the oracle's
+    complex128 adjoint from the same source (≤ 1e-5)."""
+    geo, blobs, probes, A, B = _config3()
+    amp = np.abs(np.fft.fft(po.NodePerturbation(A, B, blobs, geo.k, 1.0, probes).exits(), axis=-1))
+    n0 = np.ones(blobs.shape, dtype=complex)
+    base = po.NodePerturbation(A, B, n0, geo.k, 1.0, probes)
+    pg = PWEGradient2D(geo, checkpoint="sqrt")
+    field = torch.from_numpy(n0).cuda()
+    ex = pg.forward(field, torch.from_numpy(probes.astype(np.complex64)).cuda())
+    loss, ge = amplitude_residual(ex, torch.from_numpy(amp.astype(np.float32)).cuda())
+    g = pg.backward(field, ge).cpu().numpy()
+    exits = base.exits()
+    assert rel(ex.cpu().numpy(), exits) < 1e-5
+    lref = po.amplitude_loss_and_grad(exits, amp)[0]
+    assert abs(float(loss) - lref) <= 1e-5 * abs(lref)
+    src = ge.cpu().numpy().astype(np.complex128)
+    gref = _oracle_gradient(A, B, n0, geo.k, probes, lambda p, u: src[p])
+    assert rel(g, gref) < 1e-5, rel(g, gref)
 
 
 def test_reference_gradient_agreement(golden):
