@@ -435,11 +435,16 @@ typedef struct tp_cn3d_march_args {
                                 (from the previous march with it, e.g. the
                                 forward before the adjoint): the network is not
                                 run again                                       */
-  int32_t fft_kernels;       /* preconditioner transforms: 0 = register four-step
-                                kernels where nf = nb is 64, 128, 192 or 256
-                                (16 x 16, 16 x 12, 16 x 8, 8 x 8), else the
-                                shared-memory Stockham kernels; 1 = always the
-                                Stockham kernels.  Same operator either way.    */
+  int32_t kernels;           /* kernel choice, the same arithmetic either way
+                                (0 = automatic).  Bit 0: the preconditioner's
+                                transforms always by the shared-memory Stockham
+                                kernels (automatic: register four-step kernels
+                                where nf = nb is 64, 128, 192 or 256).  Bit 1:
+                                the stencil kernels (right-hand side, matvecs,
+                                finish) always with per-thread loads
+                                (automatic: inputs staged by tensor-memory
+                                copies where nf is 64, 128, 192 or 256 and nb
+                                is even; complex64 build).                      */
 } tp_cn3d_march_args;
 
 TP_API size_t tp_cn3d_workspace_bytes(int32_t n_total, int32_t num_probes);

@@ -293,7 +293,7 @@ def test_fft_preconditioner_against_numpy(nf, nb):
     lam = 1 - (mx * (2 * np.cos(2 * np.pi * ff / nf) - 2) + my * (2 * np.cos(2 * np.pi * fb / nb) - 2))
     z0 = {}
     for kern in (0, 1):
-        eng.fft_kernels = kern
+        eng.kernels = kern
         pairs = generate_pairs(eng, field, probes, every=1, kind="noise")
         z0[kern] = pairs.z0.cpu().numpy().astype(np.complex128)
         sol = pairs.sol.cpu().numpy().astype(np.complex128)
@@ -303,7 +303,7 @@ def test_fft_preconditioner_against_numpy(nf, nb):
                 v = _apply_i_minus_p(eng, sol[s, p], diag[s]).reshape(nb, nf)
                 ref = np.fft.ifft2(np.fft.fft2(v) / lam).ravel()
                 assert rel(z0[kern][s, p], ref) < 5e-6, (kern, s, p, rel(z0[kern][s, p], ref))
-    eng.fft_kernels = 0
+    eng.kernels = 0
     assert rel(z0[0], z0[1]) < 2e-6
 
 
@@ -402,3 +402,52 @@ def test_one_bicgstab_iteration_against_numpy(nf, nb, learned, mode):
         omega = np.vdot(t, s) / np.vdot(t, t)
         x = alpha * y + omega * z
         assert rel(got[p] - u0, x) < 5e-5, (p, rel(got[p] - u0, x))
+
+
+@pytest.mark.parametrize("nf,nb,mode,bc", [(64, 64, "forward", "impedance"), (256, 32, "adjoint_exact", "neumann"),
+                                           (192, 48, "forward", "dirichlet"), (128, 66, "adjoint", "impedance")])
+def test_tma_stencils_match_per_thread_loads(nf, nb, mode, bc):
+    """The stencil kernels with their inputs staged by tensor-memory copies
+    (right-hand side, matvecs, finish; widths 64, 128, 192, 256) against the
+    same arithmetic with per-thread loads (`kernels = 2`): fields and the
+    exact-adjoint gradient equal to fp32 round-off (the fp64 dot products are
+    summed in a different order), the same iteration counts up to a
+    convergence decision that round-off may tip, and both within 1e-5 of the
+    oracle."""
+    rng = np.random.default_rng(nf + nb)
+    nz, k, P = 7, 2 * np.pi / 0.5, 6
+    N = nf * nb
+    n = _field(rng, N, nz, scale=1e-2)
+    field = torch.from_numpy(n).cuda()
+    probes = _gauss(nf, nb, np.column_stack([rng.uniform(8, nf - 8, P), rng.uniform(8, nb - 8, P)]), 5.0)
+    eng = CN3D(nf, nb, nz, k, 1.0, 1.0, 1.0, bc)
+    fwd = eng.new_store(P)
+    eng.march(field, P, "forward", probes=c64(probes), u_store=fwd, tol=1e-7)
+    src = c64(rng.standard_normal((P, N)) + 1j * rng.standard_normal((P, N)))
+    out = {}
+    for kern in (0, 2):
+        eng.kernels = kern
+        eng.read_stats()
+        store = eng.new_store(P)
+        gc = torch.zeros((nz - 1, N), dtype=torch.complex64, device="cuda")
+        if mode == "adjoint_exact":
+            eng.march(field, P, mode, src_exit=src, u_fwd=fwd, grad_c=gc, u_store=store, tol=1e-7)
+        elif mode == "adjoint":
+            eng.march(field, P, mode, src_exit=src, u_store=store, tol=1e-7)
+        else:
+            eng.march(field, P, mode, probes=c64(probes), u_store=store, tol=1e-7)
+        eng.device_status()
+        st = eng.read_stats()
+        assert st["failed"] == 0, st
+        out[kern] = (store.cpu().numpy(), gc.cpu().numpy(), st)
+    eng.kernels = 0
+    assert abs(out[0][2]["iterations"] - out[2][2]["iterations"]) <= 2
+    assert rel(out[0][0], out[2][0]) < 1e-6
+    if mode == "adjoint_exact":
+        assert rel(out[0][1], out[2][1]) < 1e-6
+    if mode == "forward":
+        co = po.bc_coefficients(k, 1.0, 1.0, dy=1.0, bc_type=bc, dimension=3)
+        A, B = po.step_matrices_2d(nf, nb, co, bc, 1.0)
+        C = po.object_contribution(n, k, 1.0)
+        for p in (0, P - 1):
+            assert rel(out[0][0][p].T, po.march(A, B, C, probes[p])) < TOL

@@ -142,7 +142,7 @@ class TpCn3dMarchArgs(ctypes.Structure):
         ("model", ctypes.c_void_p), ("learned_ws", ctypes.c_void_p), ("learned_ws_bytes", ctypes.c_size_t),
         ("train_z0", ctypes.c_void_p), ("train_sol", ctypes.c_void_p), ("train_diag", ctypes.c_void_p),
         ("train_every", ctypes.c_int32), ("train_kind", ctypes.c_int32),
-        ("learned_reuse", ctypes.c_int32), ("fft_kernels", ctypes.c_int32),
+        ("learned_reuse", ctypes.c_int32), ("kernels", ctypes.c_int32),
     ]
 
 

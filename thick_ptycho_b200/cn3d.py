@@ -60,10 +60,10 @@ class CN3D:
         # 0: each march runs as one CUDA graph with device-side step and
         # iteration loops; 1: step by step (host loop)
         self.launch = 0
-        # preconditioner transforms: 0 = register four-step kernels where
-        # nx = ny is 64, 128, 192 or 256, else shared-memory Stockham; 1 =
-        # always Stockham (the same operator)
-        self.fft_kernels = 0
+        # kernel choice (tp_cn3d_march_args.kernels; the same arithmetic):
+        # 0 = automatic; bit 0 = Stockham transforms always, bit 1 = the
+        # stencil kernels with per-thread loads instead of tensor-memory copies
+        self.kernels = 0
 
     def op(self, is_delta=False) -> _native.TpCn3dOp:
         o = _native.TpCn3dOp()
@@ -145,7 +145,7 @@ class CN3D:
         a.num_probes, a.mode, a.max_iter, a.precond, a.host_check = P, mode_i, int(max_iter), int(precond), int(host_check)
         a.tol = float(tol)
         a.launch = int(self.launch)
-        a.fft_kernels = int(self.fft_kernels)
+        a.kernels = int(self.kernels)
         a.probes, a.src_shared, a.src_exit = _ptr(probes), _ptr(src_shared), _ptr(src_exit)
         a.u_store, a.exit_out, a.u_fwd, a.grad_c = _ptr(u_store), _ptr(exit_out), _ptr(u_fwd), _ptr(grad_c)
         a.stats = ctypes.c_void_p(self.stats.data_ptr())
@@ -170,6 +170,14 @@ class CN3D:
         rc = self.lib.tp_cn3d_march(ctypes.byref(o), _ptr(field), dt, ctypes.byref(a), _ptr(ws), ws.numel(),
                                     ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
         _native.check(rc, "tp_cn3d_march", self.lib)
+
+    def device_status(self):
+        """Raise if a bounded device-side wait of this library gave up (the
+        tensor-memory stencil kernels' stage waits); synchronises the stream."""
+        code = ctypes.c_int32()
+        rc = self.lib.tp_device_status(ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream),
+                                       ctypes.byref(code))
+        _native.check(rc, "tp_device_status", self.lib)
 
     def read_stats(self, reset=True):
         """(total iterations, solves, failed solves, max iterations per solve,

@@ -10,15 +10,20 @@
 // is O(|P| |u|) ~ 4e-2 |u|, so the Krylov tolerance and the complex64
 // round-off act on the small update, not on u (the same "1 + eps" reason as
 // the 2D kernels).  BiCGStab (van der Vorst) runs on every probe of the batch
-// at once: all vectors are (P, N) complex64, inner products are accumulated
-// in fp64 per probe, and a probe stops updating once ||r|| <= tol ||rhs||;
-// after the iterations each solve is judged by its true residual
-// ||rhs - (I - P_s) d||.  Preconditioner: the periodic 5-point operator
-// diagonalised by a 2D FFT (libtpcuda's shared-memory FFT), applied as
+// at once: all vectors are (P, N) complex64 (complex128 in the check build),
+// inner products are accumulated in fp64 per probe, and a probe stops
+// updating once ||r|| <= tol ||rhs||; after the iterations each solve is
+// judged by its true residual ||rhs - (I - P_s) d||.  Preconditioner: the
+// periodic 5-point operator diagonalised by a 2D FFT, applied as
 // IFFT2(FFT2(v) / (1 - sigma*T K_per(kf, kb))),
-// K_per = mu_x (2 cos kf - 2) + mu_y (2 cos kb - 2).
+// K_per = mu_x (2 cos kf - 2) + mu_y (2 cos kb - 2), with register four-step
+// transforms for square 64..256 grids and the shared-memory Stockham FFT of
+// fft.cuh otherwise; optionally followed by the learned per-pixel correction.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include <mutex>
 
 #include "cnn_internal.cuh"
 #include "fft.cuh"
@@ -860,6 +865,243 @@ __global__ void __launch_bounds__(k3Threads, 4) c3_finish_kernel(const C3Params 
   });
 }
 
+#ifndef TP_C128_CHECK
+// ------------------------------------------------ TMA-tiled stencil kernels
+// The right-hand side, both matvecs and the finish with their inputs staged
+// by the tensor-memory accelerator: a CTA owns probe group blockIdx.y
+// (kStencilProbes probes) and the row blocks blockIdx.x, blockIdx.x +
+// gridDim.x, ... of kTmaRows image rows.  For each row block one thread
+// issues three tiled tensor loads into a shared-memory stage -- the stencil
+// input of the group's probes with a one-row halo (rows outside the image
+// read as zero), the slice's diagonal(s) and its four off-diagonals -- and
+// the stages are double-buffered, so the next block's copies are in flight
+// while this one is computed from shared memory (the kernels that read
+// their inputs from global memory wait one memory latency per loop trip).
+// The vectors of the workspace block and the slice diagonals are equally
+// spaced, so three tensor maps serve every kernel (the vector or diagonal is
+// the outer coordinate).  The arithmetic is that of c3_init_kernel,
+// c3_matvec_kernel and c3_finish_kernel, element by element; waits on the
+// stages are bounded (kDevMbarTimeout) and a CTA that gives up waits for its
+// copies in flight before it returns.
+constexpr int kTmaRows = 2;
+enum { kTmaInit = 0, kTmaMatvec0 = 1, kTmaMatvec1 = 2, kTmaFinish = 3 };
+// workspace vector and diagonal indices (c3_layout order)
+enum { kVecU = 0, kVecX = 1, kVecR0 = 3, kVecV = 5, kVecS = 6, kVecY = 7, kVecZ = 8, kVecT = 9, kNumVecs = 11 };
+enum { kDiagCdl = 0, kDiagCdr = 1, kDiagW = 3, kNumDiags = 8 };
+
+struct TmaArgs {
+  int vin;       // the staged stencil input (with its halo rows)
+  int vc0, vc1;  // the other staged vectors (tile rows only): matvec r0 or s; finish r0 and u
+  cx *out;       // init: r0; matvec: v or t; finish: u
+  const cx *src_exit, *src_shared;
+  cx *u_store, *exit_out;
+  int adj_exact, flip;
+};
+
+// vectors staged without halo: 0 (init), 1 (matvec), 2 (finish)
+template <int KIND>
+__host__ __device__ constexpr int tma_plain_vecs() {
+  return KIND == kTmaInit ? 0 : (KIND == kTmaFinish ? 2 : 1);
+}
+template <int KIND, int NF>
+__host__ __device__ constexpr uint32_t tma_stage_bytes() {
+  return (uint32_t)((kStencilProbes * (kTmaRows + 2 + tma_plain_vecs<KIND>() * kTmaRows) +
+                     (KIND == kTmaInit ? 6 : 5) * kTmaRows) *
+                    NF * sizeof(cx));
+}
+
+template <int KIND, int NF>
+__global__ void __launch_bounds__(k3Threads, 1) c3_tma_kernel(const __grid_constant__ CUtensorMap mh,
+                                                              const __grid_constant__ CUtensorMap mv,
+                                                              const __grid_constant__ CUtensorMap md,
+                                                              const __grid_constant__ CUtensorMap md4, const C3Params q,
+                                                              const C3State *st, const TmaArgs a, Krylov *K, int *err) {
+  constexpr int TR = kTmaRows, H = TR + 2, SP = kStencilProbes, TE = TR * NF;
+  constexpr int NV = tma_plain_vecs<KIND>();
+  constexpr int ND = KIND == kTmaInit ? 2 : 1;  // diagonals staged before the off-diagonals
+  constexpr uint32_t HB = SP * H * NF * sizeof(cx), VB = SP * TE * sizeof(cx), DB = TE * sizeof(cx);
+  constexpr uint32_t STAGE = tma_stage_bytes<KIND, NF>();
+  static_assert(STAGE == HB + NV * VB + (ND + 4) * DB, "stage layout");
+  constexpr int A = KIND == kTmaMatvec1 ? 3 : (KIND == kTmaMatvec0 ? 2 : 1);  // sums per probe
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ double red[A * SP * (k3Threads / 32)];
+  __shared__ __align__(8) uint64_t bar[2];
+  const int p0 = blockIdx.y * SP;
+  const int np = q.P - p0 < SP ? q.P - p0 : SP;
+  const int t = st->t;
+  unsigned act = 0, iterated = 0;
+#pragma unroll
+  for (int j = 0; j < SP; ++j) {
+    if (j >= np) continue;
+    if (KIND == kTmaMatvec0 || KIND == kTmaMatvec1) {
+      if (!K[p0 + j].done) act |= 1u << j;
+    } else {
+      act |= 1u << j;
+      if (KIND == kTmaFinish && K[p0 + j].iters > 0) iterated |= 1u << j;
+    }
+  }
+  if (act == 0) return;
+  const int nblk = q.nb / TR;
+  const int nmine = blockIdx.x < nblk ? (nblk - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  // init: the right-hand side's terms (see c3_init_kernel)
+  const int use_u = KIND == kTmaInit ? !(a.adj_exact && t == 1) : 1;
+  const int dsec = (a.adj_exact && t > 1) ? kDiagCdr : kDiagCdl;
+  const cx *src = (KIND == kTmaInit && t == 1) ? a.src_exit : nullptr;
+  const cx *shared = (KIND == kTmaInit && a.src_shared) ? a.src_shared + (size_t)(t - 1) * q.N : nullptr;
+  const size_t node = a.flip ? q.L - t : t;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int k) {  // thread 0: the stage of my k-th row block
+    const int buf = k & 1, rb = blockIdx.x + k * gridDim.x;
+    unsigned char *sb = smem + buf * STAGE;
+    mbar_arrive_expect_tx(&bar[buf], STAGE);
+    tma_load_4d(sb, &mh, 0, rb * TR - 1, p0, a.vin, &bar[buf]);
+    if (NV > 0) tma_load_4d(sb + HB, &mv, 0, rb * TR, p0, a.vc0, &bar[buf]);
+    if (NV > 1) tma_load_4d(sb + HB + VB, &mv, 0, rb * TR, p0, a.vc1, &bar[buf]);
+    tma_load_3d(sb + HB + NV * VB, &md, 0, rb * TR, kDiagCdl, &bar[buf]);
+    if (KIND == kTmaInit) tma_load_3d(sb + HB + NV * VB + DB, &md, 0, rb * TR, dsec, &bar[buf]);
+    tma_load_3d(sb + HB + NV * VB + ND * DB, &md4, 0, rb * TR, kDiagW, &bar[buf]);
+  };
+  if (threadIdx.x == 0) {
+    if (nmine > 0) issue(0);
+    if (nmine > 1) issue(1);
+  }
+  double acc[A * SP] = {};
+  const cx zero = czero();
+  for (int k = 0; k < nmine; ++k) {
+    const int buf = k & 1;
+    const bool got = mbar_wait_bounded(&bar[buf], (uint32_t)((k >> 1) & 1), err);
+    if (__syncthreads_or(!got)) {
+      // give up: the copies in flight (this stage's, and the next one's if
+      // issued) land in shared memory before the CTA exits
+      if (threadIdx.x == 0) {
+        mbar_wait_bounded(&bar[buf], (uint32_t)((k >> 1) & 1), nullptr);
+        if (k + 1 < nmine) mbar_wait_bounded(&bar[buf ^ 1], (uint32_t)(((k + 1) >> 1) & 1), nullptr);
+      }
+      __syncthreads();
+      return;
+    }
+    const unsigned char *sb = smem + buf * STAGE;
+    const cx *tl = reinterpret_cast<const cx *>(sb);                        // [SP][H][NF]
+    const cx *v0 = reinterpret_cast<const cx *>(sb + HB);                   // [SP][TR][NF]
+    const cx *v1 = reinterpret_cast<const cx *>(sb + HB + VB);              // [SP][TR][NF]
+    const cx *d1 = reinterpret_cast<const cx *>(sb + HB + NV * VB);         // [TR][NF]
+    const cx *d2 = reinterpret_cast<const cx *>(sb + HB + NV * VB + DB);    // init: second diagonal
+    const cx *dof = reinterpret_cast<const cx *>(sb + HB + NV * VB + ND * DB);  // [4][TR][NF]: w, e, s, n
+    const int rb = blockIdx.x + k * gridDim.x;
+#pragma unroll
+    for (int e = threadIdx.x; e < TE; e += k3Threads) {
+      const int row = e / NF, f = e - row * NF;
+      const int i = (rb * TR + row) * NF + f;
+      const cx kw = f > 0 ? dof[e] : zero, ke = f < NF - 1 ? dof[TE + e] : zero;
+      const cx ks = i >= NF ? dof[2 * TE + e] : zero, kn = i + NF < q.N ? dof[3 * TE + e] : zero;
+      const cx dc = d1[e];
+      // K_off x at the element from the staged rows of probe j (the order of stencil_off)
+      auto off = [&](const cx *xt, cx acc0) {
+        const int c0 = (row + 1) * NF + f;
+        if (f > 0) acc0 = cfma(kw, xt[c0 - 1], acc0);
+        if (f < NF - 1) acc0 = cfma(ke, xt[c0 + 1], acc0);
+        if (i >= NF) acc0 = cfma(ks, xt[c0 - NF], acc0);
+        if (i + NF < q.N) acc0 = cfma(kn, xt[c0 + NF], acc0);
+        return acc0;
+      };
+      if (KIND == kTmaInit) {
+        const cx dsum = cadd(dc, d2[e]);
+        const cx sh = shared != nullptr ? shared[i] : zero;
+        cx bv[SP];
+#pragma unroll
+        for (int j = 0; j < SP; ++j) {
+          if (!((act >> j) & 1u)) continue;
+          const size_t offp = (size_t)(p0 + j) * q.N;
+          cx b = zero;
+          if (use_u) {
+            const cx *xt = tl + j * H * NF;
+            const cx o = off(xt, zero);
+            b = cfma(dsum, xt[(row + 1) * NF + f], cadd(o, o));
+          }
+          if (src != nullptr) b = cadd(b, src[offp + i]);
+          if (shared != nullptr) b = cadd(b, sh);
+          bv[j] = b;
+        }
+#pragma unroll
+        for (int j = 0; j < SP; ++j) {
+          if (!((act >> j) & 1u)) continue;
+          const cx b = bv[j];
+          a.out[(size_t)(p0 + j) * q.N + i] = b;
+          acc[j] += (double)b.x * b.x + (double)b.y * b.y;
+        }
+      } else if (KIND == kTmaMatvec0 || KIND == kTmaMatvec1) {
+        cx tv[SP], cv[SP];
+#pragma unroll
+        for (int j = 0; j < SP; ++j) {
+          if (!((act >> j) & 1u)) continue;
+          const cx *xt = tl + j * H * NF;
+          const cx yi = xt[(row + 1) * NF + f];
+          tv[j] = csub(yi, off(xt, cmul(dc, yi)));
+          cv[j] = v0[j * TE + e];
+        }
+#pragma unroll
+        for (int j = 0; j < SP; ++j) {
+          if (!((act >> j) & 1u)) continue;
+          const cx tt = tv[j], c = cv[j];
+          a.out[(size_t)(p0 + j) * q.N + i] = tt;
+          if (KIND == kTmaMatvec0) {  // conj(r0) t
+            acc[A * j] += (double)c.x * tt.x + (double)c.y * tt.y;
+            acc[A * j + 1] += (double)c.x * tt.y - (double)c.y * tt.x;
+          } else {  // conj(t) s, |t|^2
+            acc[A * j] += (double)tt.x * c.x + (double)tt.y * c.y;
+            acc[A * j + 1] += (double)tt.x * c.y - (double)tt.y * c.x;
+            acc[A * j + 2] += (double)tt.x * tt.x + (double)tt.y * tt.y;
+          }
+        }
+      } else {  // finish
+        cx unv[SP];
+#pragma unroll
+        for (int j = 0; j < SP; ++j) {
+          if (!((act >> j) & 1u)) continue;
+          const bool itd = (iterated >> j) & 1u;
+          const cx *xt = tl + j * H * NF;
+          const cx xi = itd ? xt[(row + 1) * NF + f] : zero;
+          const cx mx = itd ? csub(xi, off(xt, cmul(dc, xi))) : xi;
+          const cx d = csub(v0[j * TE + e], mx);
+          acc[j] += (double)d.x * d.x + (double)d.y * d.y;
+          unv[j] = cadd(v1[j * TE + e], xi);
+        }
+#pragma unroll
+        for (int j = 0; j < SP; ++j) {
+          if (!((act >> j) & 1u)) continue;
+          const int pr = p0 + j;
+          const size_t offp = (size_t)pr * q.N;
+          a.out[offp + i] = unv[j];
+          if (a.u_store) a.u_store[((size_t)pr * q.nz + node) * q.N + i] = unv[j];
+          if (a.exit_out && t == q.L) a.exit_out[offp + i] = unv[j];
+        }
+      }
+    }
+    __syncthreads();  // every thread is done with this stage
+    if (threadIdx.x == 0 && k + 2 < nmine) {
+      fence_proxy_async_smem();
+      issue(k + 2);
+    }
+  }
+  block_reduce_many(acc, red, [&](int m, double v) {
+    const int j = m / A, c = m % A;
+    if (!((act >> j) & 1u)) return;
+    Krylov &kr = K[p0 + j];
+    double *dst;
+    if (KIND == kTmaInit) dst = &kr.bnorm2;
+    else if (KIND == kTmaFinish) dst = &kr.res2;
+    else if (KIND == kTmaMatvec0) dst = c == 0 ? &kr.acc_r0v.x : &kr.acc_r0v.y;
+    else dst = c == 0 ? &kr.acc_ts.x : (c == 1 ? &kr.acc_ts.y : &kr.acc_tt);
+    atomicAdd(dst, v);
+  });
+}
+#endif  // TP_C128_CHECK
+
 // After a step (one CTA loops over the probes): accumulate the statistics
 // (when `stats` is given) and clear the per-probe sums of the next step.
 __global__ void c3_stats_kernel(Krylov *K, int P, double tol2, int *stats, C3State *st) {
@@ -1317,6 +1559,112 @@ static int add_while(cudaStream_t rec, unsigned dflt, cudaGraphConditionalHandle
   return TP_OK;
 }
 
+#ifndef TP_C128_CHECK
+// cuTensorMapEncodeTiled, reached through the runtime (the library does not
+// link libcuda itself); nullptr when the driver does not provide it.
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiled tensor_map_encoder() {
+  static EncodeTiled fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &qr) == cudaSuccess &&
+        qr == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(f);
+    (void)cudaGetLastError();
+  });
+  return fn;
+}
+
+struct TmaMaps {
+  CUtensorMap mh, mv, md, md4;
+};
+
+// The TMA stencil kernels' tensor maps over workspace w: the vector block
+// (nf, nb, P, vector) with a (nf, kTmaRows + 2, kStencilProbes, 1) box, and
+// the slice diagonals (nf, nb, diagonal) with (nf, kTmaRows, 1) and
+// (nf, kTmaRows, 4) boxes.  False if the driver offers no encoder, the
+// workspace is not equally spaced or a map is refused.
+static bool make_tma_maps(const C3Work &w, int nf, int nb, int P, TmaMaps *m) {
+  EncodeTiled enc = tensor_map_encoder();
+  if (enc == nullptr) return false;
+  const size_t N = (size_t)nf * nb;
+  const cuuint64_t vstride = align256((size_t)P * N * sizeof(cx)), dstride = align256(N * sizeof(cx));
+  if ((size_t)(reinterpret_cast<char *>(w.x) - reinterpret_cast<char *>(w.u)) != vstride ||
+      (size_t)(reinterpret_cast<char *>(w.hat) - reinterpret_cast<char *>(w.u)) != 10 * vstride ||
+      (size_t)(reinterpret_cast<char *>(w.sym) - reinterpret_cast<char *>(w.cdl)) != 7 * dstride)
+    return false;
+  const cuuint64_t row = (cuuint64_t)nf * sizeof(cx);
+  const cuuint64_t vdims[4] = {(cuuint64_t)nf, (cuuint64_t)nb, (cuuint64_t)P, (cuuint64_t)kNumVecs};
+  const cuuint64_t vstr[3] = {row, (cuuint64_t)N * sizeof(cx), vstride};
+  const cuuint32_t vbox[4] = {(cuuint32_t)nf, (cuuint32_t)(kTmaRows + 2), (cuuint32_t)kStencilProbes, 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  const auto ok = [](CUresult r) { return r == CUDA_SUCCESS; };
+  if (!ok(enc(&m->mh, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, w.u, vdims, vstr, vbox, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)))
+    return false;
+  const cuuint32_t pbox[4] = {(cuuint32_t)nf, (cuuint32_t)kTmaRows, (cuuint32_t)kStencilProbes, 1};
+  if (!ok(enc(&m->mv, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, w.u, vdims, vstr, pbox, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)))
+    return false;
+  const cuuint64_t ddims[3] = {(cuuint64_t)nf, (cuuint64_t)nb, (cuuint64_t)kNumDiags};
+  const cuuint64_t dstr[2] = {row, dstride};
+  const cuuint32_t dbox1[3] = {(cuuint32_t)nf, (cuuint32_t)kTmaRows, 1};
+  const cuuint32_t dbox4[3] = {(cuuint32_t)nf, (cuuint32_t)kTmaRows, 4};
+  if (!ok(enc(&m->md, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, w.cdl, ddims, dstr, dbox1, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)))
+    return false;
+  if (!ok(enc(&m->md4, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, w.cdl, ddims, dstr, dbox4, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)))
+    return false;
+  return true;
+}
+
+using TmaKernel = void (*)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const CUtensorMap, const C3Params,
+                           const C3State *, const TmaArgs, Krylov *, int *);
+struct TmaLaunch {
+  TmaKernel kern = nullptr;
+  size_t smem = 0;
+  dim3 grid;
+};
+
+template <int KIND, int NF>
+static int tma_launch_t(int nb, int P, TmaLaunch *out) {
+  auto kern = c3_tma_kernel<KIND, NF>;
+  const size_t smem = 2 * (size_t)tma_stage_bytes<KIND, NF>();
+  TP_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int dev = 0, sms = 148, occ = 1;
+  TP_CHECK_CUDA(cudaGetDevice(&dev));
+  TP_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, k3Threads, smem) != cudaSuccess || occ < 1) occ = 1;
+  (void)cudaGetLastError();
+  const int gy = (P + kStencilProbes - 1) / kStencilProbes, nblk = nb / kTmaRows;
+  int gx = (sms * occ) / gy;
+  if (gx > nblk) gx = nblk;
+  if (gx < 1) gx = 1;
+  out->kern = kern;
+  out->smem = smem;
+  out->grid = dim3(gx, gy);
+  return TP_OK;
+}
+
+// The launch of stencil kind KIND at transverse width nf (kern nullptr: no
+// tensor-memory kernel for that width).
+template <int KIND>
+static int tma_launch(int nf, int nb, int P, TmaLaunch *out) {
+  switch (nf) {
+    case 64: return tma_launch_t<KIND, 64>(nb, P, out);
+    case 128: return tma_launch_t<KIND, 128>(nb, P, out);
+    case 192: return tma_launch_t<KIND, 192>(nb, P, out);
+    case 256: return tma_launch_t<KIND, 256>(nb, P, out);
+    default: return TP_OK;
+  }
+}
+#endif  // TP_C128_CHECK
+
 }  // namespace tp
 
 using namespace tp;
@@ -1396,7 +1744,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   const int use_fft = fft_on;
   // kernels of the preconditioner: compile-time FFT plans for the common sizes
   PrecKernels pk = prec_kernels(nf, nb);
-  const Prec4Kernels p4 = (fft_on && a->fft_kernels == 0) ? prec4_kernels(nf, nb) : Prec4Kernels{};
+  const Prec4Kernels p4 = (fft_on && (a->kernels & 1) == 0) ? prec4_kernels(nf, nb) : Prec4Kernels{};
   const bool four = p4.rows != nullptr;
   const int rpc4 = four ? 256 / p4.r1 : 1;
   const int srow_f = pk.fixed ? nf + nf / 8 + 1 : nf, srow_b = pk.fixed ? nb + nb / 8 + 1 : nb;
@@ -1428,6 +1776,23 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   const dim3 vgrid((N + 256 * 8 - 1) / (256 * 8), P);
   const dim3 sg_init = stencil_grid(c3_init_kernel, N, P), sg_fin = stencil_grid(c3_finish_kernel, N, P);
   const dim3 sg_mv0 = stencil_grid(c3_matvec_kernel<0>, N, P), sg_mv1 = stencil_grid(c3_matvec_kernel<1>, N, P);
+#ifndef TP_C128_CHECK
+  // stencil kernels with tensor-memory staging where the width has an instantiation
+  TmaMaps tmaps{};
+  TmaLaunch t_init, t_mv0, t_mv1, t_fin;
+  bool tma = (a->kernels & 2) == 0 && (nf == 64 || nf == 128 || nf == 192 || nf == 256) && nb % kTmaRows == 0 &&
+             make_tma_maps(w, nf, nb, P, &tmaps);
+  if (tma) {
+    int r = tma_launch<kTmaInit>(nf, nb, P, &t_init);
+    if (r == TP_OK) r = tma_launch<kTmaMatvec0>(nf, nb, P, &t_mv0);
+    if (r == TP_OK) r = tma_launch<kTmaMatvec1>(nf, nb, P, &t_mv1);
+    if (r == TP_OK) r = tma_launch<kTmaFinish>(nf, nb, P, &t_fin);
+    if (r != TP_OK) return r;
+    tma = t_init.kern && t_mv0.kern && t_mv1.kern && t_fin.kern;
+  }
+  int *derr = tma ? device_error_ptr() : nullptr;
+  if (tma && derr == nullptr) return set_error(TP_ERR_CUDA, "device error word unavailable");
+#endif
   const int pgrid = (P + 127) / 128;
   const int one_cta = P >= 1024 ? 1024 : ((P + 31) / 32) * 32;
   const int eb = 296;
@@ -1493,14 +1858,59 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
     if (ust) c3_store_kernel<<<eb, 256, 0, s>>>(N, P, nz, flip ? L : 0, w.u, ust, nullptr);
     return TP_OK;
   };
+  // (I - P) y -> v with <r0, v> (which 0), (I - P) z -> t with <t, s>, |t|^2 (which 1)
+  auto matvec = [&](cudaStream_t s, int which) {
+#ifndef TP_C128_CHECK
+    if (tma) {
+      TmaArgs ta{};
+      ta.vin = which ? kVecZ : kVecY;
+      ta.vc0 = which ? kVecS : kVecR0;
+      ta.out = which ? w.t : w.v;
+      const TmaLaunch &tl = which ? t_mv1 : t_mv0;
+      tl.kern<<<tl.grid, k3Threads, tl.smem, s>>>(tmaps.mh, tmaps.mv, tmaps.md, tmaps.md4, q, w.st, ta, w.K, derr);
+      return;
+    }
+#endif
+    if (which == 0) c3_matvec_kernel<0><<<sg_mv0, k3Threads, 0, s>>>(q, w.cdl, w.y, w.v, w.r0, w.s, w.K);
+    else c3_matvec_kernel<1><<<sg_mv1, k3Threads, 0, s>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K);
+  };
+  // true residual, u += x, store
+  auto finish = [&](cudaStream_t s) {
+#ifndef TP_C128_CHECK
+    if (tma) {
+      TmaArgs ta{};
+      ta.vin = kVecX;
+      ta.vc0 = kVecR0;
+      ta.vc1 = kVecU;
+      ta.out = w.u;
+      ta.u_store = ust;
+      ta.exit_out = exit_out;
+      ta.flip = flip ? 1 : 0;
+      t_fin.kern<<<t_fin.grid, k3Threads, t_fin.smem, s>>>(tmaps.mh, tmaps.mv, tmaps.md, tmaps.md4, q, w.st, ta, w.K, derr);
+      return;
+    }
+#endif
+    c3_finish_kernel<<<sg_fin, k3Threads, 0, s>>>(q, w.st, w.cdl, w.x, w.r0, w.u, w.K, ust, flip ? 1 : 0, exit_out);
+  };
   // step head: slice state, operators, right-hand side, Krylov start
   auto step_head = [&](cudaStream_t s, int use_cond, cudaGraphConditionalHandle outer, cudaGraphConditionalHandle inner) {
     c3_advance_kernel<<<1, 1, 0, s>>>(w.st, L, backward ? 1 : 0, use_cond, outer, inner);
     c3_center_kernel<<<eb, 256, 0, s>>>(q, w.st, 0, w.cdl);
     if (adj_exact) c3_center_kernel<<<eb, 256, 0, s>>>(q, w.st, 1, w.cdr);
-    c3_init_kernel<<<sg_init, k3Threads, 0, s>>>(q, w.st, adj_exact, w.cdl, w.cdr, w.u,
-                                                static_cast<const cx *>(a->src_exit),
-                                                static_cast<const cx *>(a->src_shared), w.r0, w.K);
+#ifndef TP_C128_CHECK
+    if (tma) {
+      TmaArgs ta{};
+      ta.vin = kVecU;
+      ta.out = w.r0;
+      ta.src_exit = static_cast<const cx *>(a->src_exit);
+      ta.src_shared = static_cast<const cx *>(a->src_shared);
+      ta.adj_exact = adj_exact;
+      t_init.kern<<<t_init.grid, k3Threads, t_init.smem, s>>>(tmaps.mh, tmaps.mv, tmaps.md, tmaps.md4, q, w.st, ta, w.K, derr);
+    } else
+#endif
+      c3_init_kernel<<<sg_init, k3Threads, 0, s>>>(q, w.st, adj_exact, w.cdl, w.cdr, w.u,
+                                                  static_cast<const cx *>(a->src_exit),
+                                                  static_cast<const cx *>(a->src_shared), w.r0, w.K);
     c3_start_kernel<<<pgrid, 128, 0, s>>>(w.K, P);
   };
   // one BiCGStab iteration of every pending probe
@@ -1510,19 +1920,19 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
 #ifndef TP_C128_CHECK
     if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.y, w.K, 0);
 #endif
-    c3_matvec_kernel<0><<<sg_mv0, k3Threads, 0, s>>>(q, w.cdl, w.y, w.v, w.r0, w.s, w.K);
+    matvec(s, 0);
     // s = r - alpha v; z = Prec(s); t = M z
     precondition(s, 1, w.r, learned ? lw.zt : w.z, w.K, learned ? w.z : nullptr);
 #ifndef TP_C128_CHECK
     if (learned) c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, w.z, w.K, 1);
 #endif
-    c3_matvec_kernel<1><<<sg_mv1, k3Threads, 0, s>>>(q, w.cdl, w.z, w.t, w.r0, w.s, w.K);
+    matvec(s, 1);
     c3_update_kernel<<<vgrid, k3Threads, 0, s>>>(q, w.x, w.r, w.r0, w.y, w.z, w.s, w.t, w.K, w.st);
     c3_commit_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, w.st, max_iter, use_cond, inner);
   };
   // step tail: u += x (true residual, store), statistics, gradient
   auto step_tail = [&](cudaStream_t s) {
-    c3_finish_kernel<<<sg_fin, k3Threads, 0, s>>>(q, w.st, w.cdl, w.x, w.r0, w.u, w.K, ust, flip ? 1 : 0, exit_out);
+    finish(s);
     c3_stats_kernel<<<1, one_cta, 0, s>>>(w.K, P, tol2, stats, w.st);
     if (a->grad_c)
       c3_grad_kernel<<<eb, 256, 0, s>>>(N, P, nz, w.st, w.u, static_cast<const cx *>(a->u_fwd),
@@ -1641,7 +2051,7 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
         if (hs.pending == 0) break;
       }
     }
-    c3_finish_kernel<<<sg_fin, k3Threads, 0, st>>>(q, w.st, w.cdl, w.x, w.r0, w.u, w.K, ust, flip ? 1 : 0, exit_out);
+    finish(st);
     if (train && t % a->train_every == 0) {
       // training pair of this step: z0 = M0^{-1} v and x with (I - P_s) x = v,
       // v the step's right-hand side r0 and x its converged update

@@ -188,6 +188,26 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       "l"(src), "r"(bytes), "r"(smem_addr(bar))
       : "memory");
 }
+// Tiled tensor loads (TMA, no multicast): the box of the tensor map `tmap`
+// (the generic address of a __grid_constant__ CUtensorMap) at coordinates
+// c0 (innermost) .. c2 / c3 into shared memory, completing on `bar`; box
+// positions outside the tensor read as zero.  c0 times the element size must
+// be a multiple of 16 bytes (callers pass c0 = 0).
+__device__ __forceinline__ void tma_load_3d(void *dst, const void *tmap, int c0, int c1, int c2, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+          smem_addr(dst)),
+      "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(void *dst, const void *tmap, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(smem_addr(dst)),
+      "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(bar))
+      : "memory");
+}
 // Shared -> global bulk copy, tracked by the issuing thread's bulk groups
 // (commit with bulk_commit; the source may be rewritten after
 // bulk_wait_read, the global result is complete after bulk_wait).  Addresses
