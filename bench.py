@@ -74,11 +74,13 @@ def parse():
                     help="3D cases: launch the march's kernels step by step instead of as one CUDA graph with "
                          "conditional loops (the same kernels; profilers list the kernels of such graphs only "
                          "as one workload)")
-    ap.add_argument("--case", choices=("headline", "3d-march-small", "3d-recon", "3d-ms", "pit", "kernels"),
+    ap.add_argument("--case", choices=("headline", "3d-march-small", "3d-recon", "3d-ms", "pit", "kernels", "cnn"),
                     default="headline",
                     help="3d-march-small: a few learned 3D forward marches (256 x 256 x 5 nodes, 64 probes), "
                          "a small profiler target for the conv and FFT kernels; 3d-recon: `steps` gradient-descent "
-                         "iterations of the 3D reconstruction (192 x 192 x 192, 256 probes), plain vs learned")
+                         "iterations of the 3D reconstruction (192 x 192 x 192, 256 probes), plain vs learned; "
+                         "cnn: the learned preconditioner's network on `--cnn-batch` 256 x 256 slices")
+    ap.add_argument("--cnn-batch", type=int, default=64, help="cnn case: slices per network launch")
     return ap.parse_args()
 
 
@@ -860,6 +862,35 @@ def run_case_3d_recon(a):
           flush=True)
 
 
+def run_case_cnn(a):
+    """The learned preconditioner's network (features and four tcgen05 3x3
+    convolutions) on `cnn_batch` seeded 256 x 256 object diagonals -- one chunk
+    of the learned march's slices: CUDA-event median of `steps` forwards after
+    `warmup`, with the FLOPs of the four layers."""
+    import torch
+
+    from thick_ptycho_b200.learned import LearnedPreconditioner
+
+    B = a.cnn_batch
+    m = LearnedPreconditioner(256, 256, 1.0, seed=0)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    d = (1e-3 * torch.randn((B, 65536), dtype=torch.complex64, device="cuda", generator=g)).contiguous()
+    for _ in range(max(1, a.warmup)):
+        m.filter(d)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(max(1, a.steps)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        m.filter(d)
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    t = statistics.median(ms)
+    flop = 2 * 65536 * 9 * 32 * (16 + 3 * 32) * B
+    print(json.dumps({"case": "cnn", "batch": B, "ms": t, "tflops": flop / (t * 1e-3) / 1e12}), flush=True)
+
+
 def run_case_kernels(a):
     """The kernels around the marches, each on a workload larger than L2 where
     its data allows, timed with CUDA events (median of `steps` launches after
@@ -1010,6 +1041,8 @@ def main():
         run_case_pit(a)
     elif a.case == "kernels":
         run_case_kernels(a)
+    elif a.case == "cnn":
+        run_case_cnn(a)
     else:
         run_ours(a)
 
