@@ -444,7 +444,10 @@ typedef struct tp_cn3d_march_args {
                                 finish) always with per-thread loads
                                 (automatic: inputs staged by tensor-memory
                                 copies where nf is 64, 128, 192 or 256 and nb
-                                is even; complex64 build).                      */
+                                is even; complex64 build).  Bit 2: the learned
+                                filter by register shuffles (automatic: rows
+                                staged by bulk copies where nf is 64, 128, 192
+                                or 256).                                        */
 } tp_cn3d_march_args;
 
 TP_API size_t tp_cn3d_workspace_bytes(int32_t n_total, int32_t num_probes);

@@ -404,6 +404,59 @@ def test_one_bicgstab_iteration_against_numpy(nf, nb, learned, mode):
         assert rel(got[p] - u0, x) < 5e-5, (p, rel(got[p] - u0, x))
 
 
+@pytest.mark.parametrize("nf,nb,mode", [(64, 64, "forward"), (256, 32, "adjoint"), (192, 45, "forward"),
+                                         (128, 60, "adjoint_exact")])
+def test_bulk_staged_filter_matches_shuffle_filter(nf, nb, mode):
+    """The learned filter with each probe's rows staged by bulk copies (the
+    default for widths 64, 128, 192, 256) against the register-shuffle kernel
+    (`kernels = 4`) over a five-step march with random per-slice taps written
+    into the learned workspace: 11 probes (a full and a partial probe group),
+    solves converging after different iteration counts (probes leaving the
+    filter's pending set), an odd row count (a last row pair of one row), the
+    adjoint's conjugated taps.  Both kernels run the same multiply-adds in the
+    same order, so the fields agree to the round-off of the fp64 dot products'
+    summation order, and the iteration counts match."""
+    from thick_ptycho_b200.learned import LearnedPreconditioner
+
+    rng = np.random.default_rng(nf + 3 * nb)
+    nz, k, P = 6, 2 * np.pi / 0.5, 11
+    N, L = nf * nb, nz - 1
+    field = torch.from_numpy(_field(rng, N, nz, scale=1e-2)).cuda()
+    probes = _gauss(nf, nb, np.column_stack([rng.uniform(8, nf - 8, P), rng.uniform(8, nb - 8, P)]), 5.0)
+    eng = CN3D(nf, nb, nz, k, 1.0, 1.0, 1.0, "impedance")
+    model = LearnedPreconditioner(nf, nb, 1.0, seed=0)
+    lws = eng.learned_workspace(P)
+    off = (int(eng.lib.tp_cnn_forward_ws_bytes(nf, nb, L)) + 255) // 256 * 256
+    F = 0.01 * (rng.standard_normal((13, L * N)) + 1j * rng.standard_normal((13, L * N)))
+    lws[off:off + 13 * L * N * 8].view(torch.complex64).copy_(torch.from_numpy(F.astype(np.complex64)).cuda().ravel())
+    fwd = eng.new_store(P)
+    eng.march(field, P, "forward", probes=c64(probes), u_store=fwd, tol=1e-7)
+    src = c64(rng.standard_normal((P, N)) + 1j * rng.standard_normal((P, N)))
+    out = {}
+    for kern in (0, 4):
+        eng.kernels = kern
+        eng.read_stats()
+        store = eng.new_store(P)
+        gc = torch.zeros((L, N), dtype=torch.complex64, device="cuda")
+        kw = dict(precond="learned", model=model, reuse_filters=True, fallback=False, tol=1e-6, u_store=store)
+        if mode == "adjoint_exact":
+            eng.march(field, P, mode, src_exit=src, u_fwd=fwd, grad_c=gc, **kw)
+        elif mode == "adjoint":
+            eng.march(field, P, mode, src_exit=src, **kw)
+        else:
+            eng.march(field, P, mode, probes=c64(probes), **kw)
+        eng.device_status()
+        st = eng.read_stats()
+        assert st["failed"] == 0, st
+        out[kern] = (store.cpu().numpy(), gc.cpu().numpy(), st)
+    eng.kernels = 0
+    assert out[0][2]["iterations"] == out[4][2]["iterations"], (out[0][2], out[4][2])
+    assert out[0][2]["iterations"] > P * L, out[0][2]  # some solves took more than one iteration
+    assert rel(out[0][0], out[4][0]) < 1e-6
+    if mode == "adjoint_exact":
+        assert rel(out[0][1], out[4][1]) < 1e-6
+
+
 @pytest.mark.parametrize("nf,nb,mode,bc", [(64, 64, "forward", "impedance"), (256, 32, "adjoint_exact", "neumann"),
                                            (192, 48, "forward", "dirichlet"), (128, 66, "adjoint", "impedance")])
 def test_tma_stencils_match_per_thread_loads(nf, nb, mode, bc):

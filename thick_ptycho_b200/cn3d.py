@@ -62,7 +62,8 @@ class CN3D:
         self.launch = 0
         # kernel choice (tp_cn3d_march_args.kernels; the same arithmetic):
         # 0 = automatic; bit 0 = Stockham transforms always, bit 1 = the
-        # stencil kernels with per-thread loads instead of tensor-memory copies
+        # stencil kernels with per-thread loads instead of tensor-memory copies,
+        # bit 2 = the learned filter by register shuffles instead of bulk-staged rows
         self.kernels = 0
 
     def op(self, is_delta=False) -> _native.TpCn3dOp:
@@ -173,7 +174,8 @@ class CN3D:
 
     def device_status(self):
         """Raise if a bounded device-side wait of this library gave up (the
-        tensor-memory stencil kernels' stage waits); synchronises the stream."""
+        tensor-memory stencil kernels' stage waits, the bulk-staged learned
+        filter's row waits); synchronises the stream."""
         code = ctypes.c_int32()
         rc = self.lib.tp_device_status(ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream),
                                        ctypes.byref(code))

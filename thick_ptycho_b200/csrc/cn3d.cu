@@ -1422,6 +1422,130 @@ __global__ void __launch_bounds__(NF, 2) c3_filter_shfl_kernel(const C3Params q,
     if (vb) dst[NF] = B;
   }
 }
+
+// The same correction with each probe's six rows b - 2 .. b + 3 staged in
+// shared memory by one bulk copy per probe: a CTA issues the copies of all
+// its pending probes at once (one mbarrier each; rows outside the image are
+// not copied but zero-filled) and filters each probe as its copy lands, so
+// the loads of the later probes overlap the arithmetic of the earlier ones.
+// Every tap reads shared memory at a fixed offset (row, column f + dx;
+// columns outside the image read zero), and the multiply-adds run in the
+// order of c3_filter_shfl_kernel, so both kernels give the same bits.  Waits
+// are bounded (kDevMbarTimeout); a thread that gives up waits for the CTA's
+// other copies before it returns.  nf = NF in {64, 128, 192, 256}, z 16-byte
+// aligned; a CTA of NF threads, one row pair, kFilterProbes probes.
+// Grid (ceil(nb / 2), ceil(P / kFilterProbes)).
+constexpr int kFilterRows = 6;
+
+template <int NF>
+__global__ void __launch_bounds__(NF, 2) c3_filter_bulk_kernel(const C3Params q, const C3State *st, int chunk,
+                                                               const cx *__restrict__ Fall,
+                                                               const cx *__restrict__ z, cx *__restrict__ out,
+                                                               const Krylov *K, int second, int *err) {
+  static_assert(NF % 32 == 0 && NF <= 256, "one thread per column, whole warps");
+  constexpr int RW = kFilterRows;
+  extern __shared__ __align__(128) cx zs[];  // [kFilterProbes][RW][NF]
+  __shared__ __align__(8) uint64_t bar[kFilterProbes];
+  if (second && st->it == 0 && st->cheap) return;
+  const int nb = q.nb, f = threadIdx.x;
+  const int ba = blockIdx.x * 2, p0 = blockIdx.y * kFilterProbes;
+  const int np_cta = q.P - p0 < kFilterProbes ? q.P - p0 : kFilterProbes;
+  unsigned pend = 0;
+  for (int j = 0; j < np_cta; ++j)
+    if (K == nullptr || !K[p0 + j].done) pend |= 1u << j;
+  if (pend == 0) return;
+  // staged rows r_lo .. r_hi - 1 (image rows ba - 2 + r) lie inside the image
+  const int r_lo = ba < 2 ? 2 - ba : 0;
+  const int r_hi = ba + 4 > nb ? nb - ba + 2 : RW;
+  if (threadIdx.x == 0) {
+    for (int j = 0; j < kFilterProbes; ++j) mbar_init(&bar[j], 1);
+    fence_mbar_init();
+  }
+  if (r_lo > 0 || r_hi < RW) {
+    for (int j = 0; j < np_cta; ++j) {
+      if (!((pend >> j) & 1u)) continue;
+      for (int r = 0; r < RW; ++r)
+        if (r < r_lo || r >= r_hi) zs[(j * RW + r) * NF + f] = czero();
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < np_cta && ((pend >> threadIdx.x) & 1u)) {
+    const int j = threadIdx.x;
+    const uint32_t bytes = (uint32_t)((r_hi - r_lo) * NF * sizeof(cx));
+    mbar_arrive_expect_tx(&bar[j], bytes);
+    bulk_g2s(&zs[(j * RW + r_lo) * NF], z + (size_t)(p0 + j) * q.N + (size_t)(ba - 2 + r_lo) * NF, bytes, &bar[j]);
+  }
+  const bool vb = ba + 1 < nb;
+  const int sl = st->s - 1;
+  const size_t npx = (size_t)chunk * q.N;
+  const cx *F = Fall + (size_t)(sl / chunk) * kFilterTaps * npx + (size_t)(sl % chunk) * q.N;
+  const float cs = q.conj_t ? -1.f : 1.f;
+  const cx zero = czero();
+  cx wa[kFilterTaps], wb[kFilterTaps];
+#pragma unroll
+  for (int t = 0; t < kFilterTaps; ++t) {
+    const cx a = F[(size_t)t * npx + (size_t)ba * NF + f];
+    const cx b = vb ? F[(size_t)t * npx + (size_t)(ba + 1) * NF + f] : zero;
+    wa[t] = mkcx(a.x, cs * a.y);
+    wb[t] = mkcx(b.x, cs * b.y);
+  }
+  const bool hw1 = f >= 1, he1 = f + 1 < NF, hw2 = f >= 2, he2 = f + 2 < NF;
+  for (int j = 0; j < np_cta; ++j) {
+    if (!((pend >> j) & 1u)) continue;
+    if (!mbar_wait_bounded(&bar[j], 0, err)) {
+      for (int k = j + 1; k < np_cta; ++k)
+        if ((pend >> k) & 1u) mbar_wait_bounded(&bar[k], 0, nullptr);
+      return;
+    }
+    const cx *zr = zs + j * RW * NF + f;  // column f of the probe's staged rows
+    cx c[RW];
+#pragma unroll
+    for (int r = 0; r < RW; ++r) c[r] = zr[r * NF];
+    cx w1[4], e1[4], w2[2], e2[2];  // columns f - 1, f + 1 (rows ba - 1 .. ba + 2), f - 2, f + 2 (rows ba, ba + 1)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      w1[k] = hw1 ? zr[(k + 1) * NF - 1] : zero;
+      e1[k] = he1 ? zr[(k + 1) * NF + 1] : zero;
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      w2[k] = hw2 ? zr[(k + 2) * NF - 2] : zero;
+      e2[k] = he2 ? zr[(k + 2) * NF + 2] : zero;
+    }
+    // taps (dy, dx): (0,0) (0,-1) (0,1) (-1,0) (1,0) (-1,-1) (-1,1) (1,-1) (1,1) (0,-2) (0,2) (-2,0) (2,0)
+    cx A = c[2];
+    A = cfma(wa[0], c[2], A);
+    A = cfma(wa[1], w1[1], A);
+    A = cfma(wa[2], e1[1], A);
+    A = cfma(wa[3], c[1], A);
+    A = cfma(wa[4], c[3], A);
+    A = cfma(wa[5], w1[0], A);
+    A = cfma(wa[6], e1[0], A);
+    A = cfma(wa[7], w1[2], A);
+    A = cfma(wa[8], e1[2], A);
+    A = cfma(wa[9], w2[0], A);
+    A = cfma(wa[10], e2[0], A);
+    A = cfma(wa[11], c[0], A);
+    A = cfma(wa[12], c[4], A);
+    cx B = c[3];
+    B = cfma(wb[0], c[3], B);
+    B = cfma(wb[1], w1[2], B);
+    B = cfma(wb[2], e1[2], B);
+    B = cfma(wb[3], c[2], B);
+    B = cfma(wb[4], c[4], B);
+    B = cfma(wb[5], w1[1], B);
+    B = cfma(wb[6], e1[1], B);
+    B = cfma(wb[7], w1[3], B);
+    B = cfma(wb[8], e1[3], B);
+    B = cfma(wb[9], w2[1], B);
+    B = cfma(wb[10], e2[1], B);
+    B = cfma(wb[11], c[1], B);
+    B = cfma(wb[12], c[5], B);
+    cx *dst = out + (size_t)(p0 + j) * q.N + (size_t)ba * NF + f;
+    dst[0] = A;
+    if (vb) dst[NF] = B;
+  }
+}
 #endif  // TP_C128_CHECK
 
 // out = (I - P_s) x (no inner products): right-hand sides of the white-noise
@@ -1891,18 +2015,36 @@ extern "C" int tp_cn3d_march(const tp_cn3d_op *op, const void *n_field, int32_t 
   const size_t smem_filter = (size_t)kFilterProbes * (frb + 4) * (fcw + 4) * sizeof(cx);
   if (learned)
     TP_CHECK_CUDA(cudaFuncSetAttribute(c3_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_filter));
-  // widths with one thread per column take the shuffle kernel
+  // widths with one thread per column take the bulk-staged kernel (bit 2 of
+  // kernels: the register-shuffle kernel), other widths the tile kernel
   using ShflFilter = void (*)(const C3Params, const C3State *, int, const cx *, const cx *, cx *, const Krylov *, int);
+  using BulkFilter = void (*)(const C3Params, const C3State *, int, const cx *, const cx *, cx *, const Krylov *, int,
+                              int *);
   const ShflFilter shfl_filter = nf == 64    ? c3_filter_shfl_kernel<64>
                                  : nf == 128 ? c3_filter_shfl_kernel<128>
                                  : nf == 192 ? c3_filter_shfl_kernel<192>
                                  : nf == 256 ? c3_filter_shfl_kernel<256>
                                              : nullptr;
+  BulkFilter bulk_filter = nf == 64    ? c3_filter_bulk_kernel<64>
+                           : nf == 128 ? c3_filter_bulk_kernel<128>
+                           : nf == 192 ? c3_filter_bulk_kernel<192>
+                           : nf == 256 ? c3_filter_bulk_kernel<256>
+                                       : nullptr;
+  int *ferr = nullptr;
+  if (!learned || (a->kernels & 4) != 0 || (reinterpret_cast<uintptr_t>(lw.zt) & 15) != 0) bulk_filter = nullptr;
+  if (bulk_filter && (ferr = device_error_ptr()) == nullptr) bulk_filter = nullptr;
+  const size_t smem_bulk_f = (size_t)kFilterProbes * kFilterRows * nf * sizeof(cx);
+  if (bulk_filter)
+    TP_CHECK_CUDA(cudaFuncSetAttribute(bulk_filter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bulk_f));
   const dim3 sgrid_f((nb + 1) / 2, (P + kFilterProbes - 1) / kFilterProbes);
   // the correction y = z + F z of application `second` (0 or 1) of an iteration
   auto filter = [&](cudaStream_t s, cx *dst, int second) {
-    if (shfl_filter) shfl_filter<<<sgrid_f, nf, 0, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, dst, w.K, second);
-    else c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, dst, w.K, second);
+    if (bulk_filter)
+      bulk_filter<<<sgrid_f, nf, smem_bulk_f, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, dst, w.K, second, ferr);
+    else if (shfl_filter)
+      shfl_filter<<<sgrid_f, nf, 0, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, dst, w.K, second);
+    else
+      c3_filter_kernel<<<fgrid, k3Threads, smem_filter, s>>>(q, w.st, lw.chunk, lw.F, lw.zt, dst, w.K, second);
   };
 #endif
   const dim3 vgrid((N + 256 * 8 - 1) / (256 * 8), P);
